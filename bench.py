@@ -1,0 +1,315 @@
+#!/usr/bin/env python
+"""Geodesics/s of the Kerr render workload on B200s (and the CPU reference arm).
+
+Workload (one "step" = one frame): Kerr a = 0.9, camera at r = 50 M and 75
+degrees inclination, 60 degree horizontal field of view, 1920x1080 pixels at
+16 samples per pixel (33,177,600 geodesics), thin Keplerian disk from the ISCO
+to 20 M at T_in = 1e4 K, 32 spectral bins over 380-780 nm, 10^5 seeded
+background stars, adaptive RKF45 at rtol = atol = 1e-7, FP32 ray state with
+FP64 step control (MIXED), escape radius 1000 M.  Synthetic, seeded input.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Under torchrun every rank renders its own frame (its own jitter seed): the
+work per GPU is fixed and the frames need no exchange, so scaling is weak and
+the value is the total of all ranks.  Rank 0 prints one JSON line.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_STARS = 100_000
+STAR_SEED = 0x57A25
+WORKLOAD = "kerr_a0.9_r50M_i75_fov60_1920x1080_16spp_32bins_1e5stars_rtol1e-7"
+METRIC = "geodesics/s on 1 B200: RKF45 FP32 vs surrogate+fallback at <=1e-3 XYZ error"
+UNIT = "geodesics/s"
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="mgk", choices=["mgk", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU sample budget per measurement")
+    return ap.parse_args()
+
+
+def scene_config(M, rank=0):
+    s = M.scene_defaults()
+    s.seed = 0x5EED + rank
+    return s
+
+
+def config_dict(s, extra=None):
+    d = {"workload": WORKLOAD, "metric_tensor": "kerr", "spin": s.spin, "width": s.width, "height": s.height,
+         "spp": s.spp, "rays_per_frame": s.width * s.height * s.spp, "n_bins": s.n_bins, "stars": N_STARS,
+         "rel_tol": s.rel_tol, "abs_tol": s.abs_tol, "precision": "mixed (fp32 state, fp64 step control)",
+         "l2": "a 512 MiB buffer is written between timed frames (frame traffic is also > L2)"}
+    if extra:
+        d.update(extra)
+    return d
+
+
+# ------------------------------------------------------------------ clocks
+class Clocks:
+    """Samples SM clocks and throttle reasons with nvidia-smi while timing."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.path = tempfile.mktemp(prefix="mgk_clocks_", suffix=".csv")
+        self.proc = None
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.f.close()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax = float(parts[2])
+                except ValueError:
+                    continue
+                for n, v in zip(names, parts[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(n)
+        os.unlink(self.path)
+        loaded = [v for v in sm if smax and v > 0.3 * smax] or sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# --------------------------------------------------------------- CPU legs
+def cpu_render_sample(s, stars, w, seconds, precision, reference=False):
+    """Renders a strided sample of the frame's pixels on the host cores and
+    returns (geodesics/s, threads, description).  The sample is sized from a
+    short calibration run so that it takes about `seconds`."""
+    from oracle import oracle_py as O
+    s = s.copy()
+    s.precision = precision
+    threads = os.cpu_count() or 1
+    npix = s.width * s.height
+    render = O.ref_render_pixels if reference else O.render_pixels
+    n_cal = min(npix, 64 * threads)
+    stride = max(1, npix // n_cal)
+    t0 = time.perf_counter()
+    render(s, stars, w, 0, n_cal, nthreads=threads, stride=stride)
+    dt = time.perf_counter() - t0
+    rate = n_cal / max(dt, 1e-6)
+    n = int(min(npix, max(n_cal, rate * seconds)))
+    stride = max(1, npix // n)
+    t0 = time.perf_counter()
+    render(s, stars, w, 0, n, nthreads=threads, stride=stride)
+    dt = time.perf_counter() - t0
+    rays = n * s.spp
+    desc = (f"{n} of {npix} pixels (every {stride}th) x {s.spp} spp = {rays} geodesics in {dt:.1f} s")
+    return rays / dt, threads, desc
+
+
+# ------------------------------------------------------------------ arms
+def run_reference(args, rank, world):
+    """The reference arm: the reference's CPU geodesic integration on the host cores."""
+    if rank != 0:
+        return None
+    import magik_b200 as M
+    from oracle import oracle_py as O
+    s = scene_config(M)
+    stars = M.star_catalog(STAR_SEED, N_STARS)
+    w = M.xyz_weights(s.n_bins)
+    use_ref = O.ref_available() and hasattr(O, "ref_render_pixels")
+    kind = "reference" if use_ref else "port"
+    per = max(2.0, min(args.cpu_seconds, 120.0 / max(1, args.steps + args.warmup)))
+    vals, desc, threads = [], "", 1
+    for i in range(args.warmup + args.steps):
+        v, threads, desc = cpu_render_sample(s, stars, w, per, M.abi.PRECISION_REF32, reference=use_ref)
+        if i >= args.warmup:
+            vals.append(v)
+    value = statistics.mean(vals)
+    what = ("the reference's own RKF45 (metric_kerr.cuh / internal_math.h compiled from its sources) per camera "
+            "ray, with the disk, escape, star and spectral stages of the CPU oracle, which the reference lacks"
+            if use_ref else "the CPU oracle in REF32 arithmetic")
+    return {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic (seeded)",
+            "config": config_dict(s), "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads,
+                                                        "kind": kind, "sample": desc, "what": what},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def run_gpu(args, rank, world, local_rank):
+    import torch
+    import magik_b200 as M
+    from magik_b200 import flops as FL
+
+    torch.cuda.set_device(local_rank)
+    dev = f"cuda:{local_rank}"
+    ctx = M.Context(local_rank)
+    s = scene_config(M, rank)
+    rays = s.width * s.height * s.spp
+    npix = s.width * s.height
+    stars = M.star_catalog(STAR_SEED, N_STARS)
+    w = M.xyz_weights(s.n_bins)
+    d_stars = torch.from_numpy(stars.view(np.uint8)).to(dev)
+    d_w = torch.from_numpy(w.ravel()).to(dev)
+    film = torch.empty(npix * 3, dtype=torch.float32, device=dev)
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)
+    peak = ctx.fp32_peak()
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        ctx.render(s, d_stars, film, d_weights=d_w, want_stats=False)
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+
+    clocks = Clocks(local_rank)
+    clocks.start()
+    times, integ, flop = [], [], []
+    st_last = None
+    for _ in range(args.steps):
+        flush.fill_(1)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        st = ctx.render(s, d_stars, film, d_weights=d_w, want_stats=True)
+        e1.record()
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+        integ.append(st.integrate_ms)
+        flop.append(FL.render_flops(s.metric, st.attempts, st.refine_evals))
+        st_last = st
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    barrier()
+
+    # end to end through the host-buffer entry point: pinned inputs in, film out
+    h_stars = torch.from_numpy(stars.view(np.uint8).copy()).pin_memory()
+    h_w = torch.from_numpy(w.ravel().copy()).pin_memory()
+    h_film = torch.empty(npix * 3, dtype=torch.float32).pin_memory()
+    ctx.render_host(s, h_stars, h_film, h_weights=h_w, want_stats=False)
+    e2e_times = []
+    for _ in range(max(1, min(args.steps, 3))):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        ctx.render_host(s, h_stars, h_film, h_weights=h_w, want_stats=False)
+        e1.record()
+        e1.synchronize()
+        e2e_times.append(e0.elapsed_time(e1))
+    film_ok = bool(torch.isfinite(h_film).all().item())
+
+    ms = statistics.mean(times)
+    e2e_ms = statistics.mean(e2e_times)
+    ms_int = statistics.mean(integ)
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([ms, e2e_ms, ms_int], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, e2e_ms, ms_int = t.tolist()
+    if rank != 0:
+        return None
+
+    achieved = statistics.mean(f / (t * 1e-3) for f, t in zip(flop, integ))
+    out = {
+        "metric": METRIC, "value": world * rays / (ms * 1e-3), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp32 (fp64 step control)",
+        "data": "synthetic (seeded camera jitter and star catalogue)",
+        "config": config_dict(s, {"parallelism": f"{world} independent frames (weak)"}),
+        "e2e": {"value": world * rays / (e2e_ms * 1e-3), "unit": UNIT,
+                "h2d_bytes_per_step": int(h_stars.numel() + h_w.numel() * 4),
+                "d2h_bytes_per_step": int(h_film.numel() * 4)},
+        "roofline": {"bound": "fp32", "kernel": "k_integrate + k_refine + k_tail (one chunk)",
+                     "achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "TFLOP/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "peak_source": "measured in this run by mgk_fp32_peak (FMA probe kernel); "
+                                    "MEASURED_PEAKS.json has no FP32 figure",
+                     "flop_per_attempt": FL.attempt_flops(s.metric),
+                     "flop_per_crossing_substep": FL.substep_flops(s.metric),
+                     "integrate_ms": ms_int},
+        "stats": {"attempts": st_last.attempts, "steps": st_last.steps, "refine_evals": st_last.refine_evals,
+                  "wide_attempts": st_last.wide_attempts,
+                  "classes": dict(zip(["alive", "disk", "escaped", "horizon", "step_limit"],
+                                      [int(c) for c in st_last.class_count])),
+                  "attempts_per_ray": st_last.attempts / rays},
+        "clocks": clk,
+        "gpu_launches": 10 * args.steps,
+        "film_finite": film_ok,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        v, thr, desc = cpu_render_sample(s, stars, w, args.cpu_seconds, M.abi.PRECISION_MIXED)
+        out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": thr, "kind": "port", "sample": desc}
+    return out
+
+
+def main():
+    args = parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        out = run_reference(args, rank, world)
+        if out is not None:
+            print(json.dumps(out), flush=True)
+        return 0
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device(f"cuda:{local_rank}"))
+    try:
+        out = run_gpu(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+    if out is not None:
+        print(json.dumps(out), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,294 @@
+/*
+ * mgk.h - C ABI of the B200-native geodesic path (libmgk.so).
+ *
+ * The library integrates null geodesics with the adaptive RKF45 scheme of
+ * Magik (Minkowski / Schwarzschild / Kerr in Kerr-Schild Cartesian form, spin
+ * axis +y), tests every accepted step against a thin accretion disk, an escape
+ * radius and the horizon, and turns the terminated rays into blackbody spectra
+ * and CIE XYZ film, all on one B200 through hand-written sm_100a kernels.
+ *
+ * Conventions follow the reference's public API (include/magik/magik.h):
+ *  - every entry point returns e_magik_result_types (magik.h:38-110); new
+ *    codes live at 10001 and above; nothing ever calls exit() or resets the
+ *    device (the reference's check_cuda does, cuda_host_utilities.h:12-20);
+ *  - caller-owned buffers are passed as plain pointers with explicit sizes;
+ *  - device work is stream-ordered on the caller's stream (NULL = legacy
+ *    default stream) and asynchronous unless stated otherwise.
+ * Plain C types only: no torch or CUDA types appear in the signatures.
+ */
+#ifndef MGK_H
+#define MGK_H
+
+#include <stddef.h>
+#include <stdint.h>
+#ifndef __cplusplus
+#include <stdbool.h>
+#endif
+
+#if defined(__GNUC__) || defined(__clang__)
+#define MGK_API __attribute__((visibility("default")))
+#else
+#define MGK_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------ results */
+/* Values 0..10000 are the reference's e_magik_result_types (magik.h:38-110). */
+typedef int32_t mgk_result;
+#define MGK_SUCCESS 0
+#define MGK_ERROR_INVALID_POINTER 2
+#define MGK_UNKNOWN_ENUM_TYPE 3
+#define MGK_INVALID_CUDA_DEVICE 4
+#define MGK_ERROR_HOST_ALLOCATION_FAILED 101
+#define MGK_ERROR_HOST_TRACE_ALLOCATED_STEPS_AND_CAPACITY_MISMATCH 102
+#define MGK_ERROR_DEVICE_OUT_OF_MEMORY 200
+#define MGK_ERROR_UNKNOWN_METRIC 707
+#define MGK_ERROR_UNKNOWN 10000
+/* New codes. */
+#define MGK_ERROR_INVALID_ARGUMENT 10001  /* a size, count or range is out of bounds */
+#define MGK_ERROR_CUDA 10002              /* a CUDA runtime call failed */
+#define MGK_ERROR_NO_DEVICE 10003         /* no sm_100 device / kernels not loadable */
+#define MGK_ERROR_DEVICE_STATUS 10004     /* a kernel reported a bad status word */
+
+/* --------------------------------------------------------------- enums */
+/* Same values as e_magik_spacetime_metric_types (magik.h:583-588). */
+#define MGK_METRIC_MINKOWSKI 0
+#define MGK_METRIC_SCHWARZSCHILD 1
+#define MGK_METRIC_KERR 2
+
+/* Arithmetic of the integrator.
+ *  REF32 - FP32 state and FP32 step control in the reference's exact operation
+ *          order (no fused multiply-add): the kernels reproduce the reference
+ *          CPU tracer's steps bit for bit.
+ *  MIXED - FP32 state with fused multiply-add, FP64 error estimate and step
+ *          control, whole attempts in FP64 within MGK_WIDE_BAND of the outer
+ *          horizon.  The production mode.
+ *  F64   - FP64 everywhere (the accuracy reference run on the GPU). */
+#define MGK_PRECISION_REF32 0
+#define MGK_PRECISION_MIXED 1
+#define MGK_PRECISION_F64 2
+
+/* Distance (in M) from the outer horizon below which MIXED attempts run in FP64. */
+#define MGK_WIDE_BAND 0.05
+
+/* Secant iterations (after the first RK sub-step) spent locating a disk or
+ * escape crossing on the geodesic. */
+#define MGK_REFINE_ITERS 4
+
+/* Termination class of a ray. */
+#define MGK_RAY_ALIVE 0
+#define MGK_RAY_DISK 1
+#define MGK_RAY_ESCAPED 2
+#define MGK_RAY_HORIZON 3
+#define MGK_RAY_STEP_LIMIT 4
+
+/* ------------------------------------------------------------ scene */
+/* Everything one render or trace needs.  Geometric units, M = 1.
+ * The integrator fields mirror the reference's metric params_t
+ * (metric_kerr.cuh:112-123) and relativity settings
+ * (relativity_settings.h:11-25). */
+typedef struct mgk_scene {
+    int32_t metric;          /* MGK_METRIC_* */
+    int32_t precision;       /* MGK_PRECISION_* */
+    int32_t time_reversed;   /* 1 for camera rays (the reference's kernels trace time-reversed) */
+    uint32_t n_max_substep;  /* RKF45 attempts per accepted step (reference default 56) */
+    double spin;             /* Kerr a, physical (flipped internally when time_reversed) */
+    double mass_sign;        /* Schwarzschild: +1 or -1 */
+    double horizon_scalar;   /* capture at horizon radius * this (reference 1.01) */
+    double abs_tol;
+    double rel_tol;
+    double h_max;            /* largest affine step (reference 1000) */
+    uint32_t max_steps;      /* accepted steps per ray before MGK_RAY_STEP_LIMIT */
+    uint32_t n_bins;         /* spectral bins, 1..MGK_MAX_BINS */
+    double escape_radius;    /* |x| at which a ray counts as escaped */
+    double disk_r_in;        /* thin disk in the plane y = 0; disk_r_out <= 0 disables it */
+    double disk_r_out;
+    double disk_T_in;        /* T(r) = disk_T_in * (r / disk_r_in)^(-3/4) */
+    double cam_r;            /* camera at cam_r * (0, cos i, sin i) */
+    double cam_incl_rad;     /* inclination i from the spin axis +y */
+    double focal_length_mm;  /* horizontal FOV = 2 atan(sensor_diag / (2 focal_length)) */
+    double sensor_diag_mm;
+    uint32_t width;
+    uint32_t height;
+    uint32_t spp;            /* samples per pixel; ray id = pixel * spp + sample */
+    uint32_t reserved0;
+    uint64_t seed;           /* counter-based RNG seed (pixel jitter, star catalogue) */
+    double lambda_min_nm;    /* bins are uniform over [lambda_min, lambda_max]; */
+    double lambda_max_nm;    /* emission is sampled at the bin centres */
+    double star_radius_rad;  /* angular radius of a star's disc on the sky, (0, 0.02] */
+} mgk_scene;
+
+#define MGK_MAX_BINS 64
+
+/* One background star (32 bytes). */
+typedef struct mgk_star {
+    float dir[3];       /* unit direction on the celestial sphere */
+    float amplitude;    /* peak radiance scale (W m^-3 sr^-1 per unit Planck) */
+    float temperature;  /* blackbody temperature, K */
+    float reserved[3];
+} mgk_star;
+
+/* Per-ray record of mgk_trace_rays (128 bytes). */
+typedef struct mgk_ray_result {
+    double x[4];        /* final four-position (x, y, z, t) */
+    double p[4];        /* final covariant four-momentum (x, y, z, t) */
+    double z;           /* redshift factor nu_obs / nu_em (disk and sky), else 0 */
+    double r_hit;       /* disk crossing radius */
+    double dir[3];      /* escape direction */
+    uint32_t cls;       /* MGK_RAY_* */
+    uint32_t steps;     /* accepted steps */
+    uint32_t attempts;  /* RKF45 attempts */
+    uint32_t wide_attempts; /* attempts run in FP64 */
+    uint32_t refine_evals;  /* RK sub-steps spent locating the crossing */
+    uint32_t reserved;
+} mgk_ray_result;
+
+/* Counters of one render. */
+typedef struct mgk_render_stats {
+    uint64_t rays;
+    uint64_t attempts;
+    uint64_t steps;
+    uint64_t wide_attempts;
+    uint64_t refine_evals;
+    uint64_t class_count[5];  /* indexed by MGK_RAY_* */
+    double integrate_ms;      /* device time of the integrator launches */
+    double total_ms;          /* device time of the whole render */
+} mgk_render_stats;
+
+typedef struct mgk_context mgk_context;
+
+/* ----------------------------------------------------------- context */
+/* Binds a device, loads the kernels and owns the scratch arena of the
+ * wavefront queues (the reference's device arena, device_arena.h:18-58). */
+MGK_API mgk_result mgk_context_create(int32_t device, mgk_context** out);
+MGK_API mgk_result mgk_context_destroy(mgk_context* ctx);
+/* Last CUDA error text seen by the context (static storage, never NULL). */
+MGK_API const char* mgk_last_error(mgk_context* ctx);
+
+/* Defaults of the Kerr render workload: a = 0.9, camera at r = 50 M and 75 degrees
+ * inclination, 60 degree horizontal field of view, 1920x1080 at 16 samples per
+ * pixel, thin disk from the ISCO to 20 M at 1e4 K, 32 bins over 380-780 nm,
+ * atol = rtol = 1e-7, 56 attempts per step (the reference default,
+ * relativity_settings.h:13), escape radius 1000 M, MIXED precision. */
+MGK_API void mgk_scene_defaults(mgk_scene* s);
+
+/* Radius of the innermost stable circular prograde orbit for spin a (M = 1),
+ * Bardeen, Press and Teukolsky (1972). */
+MGK_API double mgk_isco_radius(double spin);
+
+/* ---------------------------------------------------- host utilities */
+/* Per-bin CIE 1931 XYZ weights w[3*k + c] for n_bins uniform bins over
+ * [lambda_min, lambda_max], normalised like compute_normalized_isi_cmf_weights
+ * (host_color_utilities.cuh:145-178); the colour-matching functions are the
+ * multi-lobe Gaussian fit of Wyman, Sloan and Shirley (JCGT 2(2), 2013). */
+MGK_API mgk_result mgk_xyz_weights(uint32_t n_bins, double lambda_min_nm, double lambda_max_nm, float* w_out);
+/* Seeded star catalogue: directions uniform on the sphere, magnitudes uniform
+ * in [0, 10] (fluxes log-uniform over four decades), temperatures uniform in
+ * [3000, 30000] K. */
+MGK_API mgk_result mgk_star_catalog(uint64_t seed, uint32_t n_stars, mgk_star* out);
+/* Derived per-scene constants (camera tetrad etc.), 32 doubles; for tests. */
+MGK_API mgk_result mgk_scene_constants(const mgk_scene* s, double* out32);
+
+/* Measured peak FP32 (non-tensor) throughput of the context's device in
+ * FLOP/s (FMA = 2 FLOP), from a dependent-chain FMA probe kernel; the
+ * denominator of the integrator's roofline.  Synchronous. */
+MGK_API mgk_result mgk_fp32_peak(mgk_context* ctx, double* flops_per_s);
+
+/* ------------------------------------------------------------- render */
+/* Renders the scene's full frame: width*height*spp camera rays through the
+ * persistent integrator, shading of the hit queues, per-pixel resolve.
+ * d_stars (n_stars entries) and d_xyz_w (3*n_bins floats) are device
+ * pointers; d_xyz_w may be NULL (then mgk_xyz_weights is used).
+ * d_film_xyz receives 3 floats per pixel (X, Y, Z; mean over samples);
+ * d_film_spectral, if not NULL, receives n_bins floats per pixel.
+ * stats (host, may be NULL) is filled after the render completes; asking for
+ * it synchronises the stream. */
+MGK_API mgk_result mgk_render(mgk_context* ctx, const mgk_scene* s, const mgk_star* d_stars, uint32_t n_stars,
+                              const float* d_xyz_w, float* d_film_xyz, float* d_film_spectral,
+                              mgk_render_stats* stats, void* stream);
+
+/* The same render from host memory: copies the star catalogue and weights in,
+ * renders, copies the XYZ film out, and returns when the film is in h_film_xyz. */
+MGK_API mgk_result mgk_render_host(mgk_context* ctx, const mgk_scene* s, const mgk_star* h_stars, uint32_t n_stars,
+                                   const float* h_xyz_w, float* h_film_xyz, mgk_render_stats* stats, void* stream);
+
+/* Traces camera rays [first_ray, first_ray + n_rays) of the scene and writes
+ * one mgk_ray_result per ray to d_out (device pointer). */
+MGK_API mgk_result mgk_trace_rays(mgk_context* ctx, const mgk_scene* s, uint64_t first_ray, uint32_t n_rays,
+                                  mgk_ray_result* d_out, void* stream);
+
+/* Per-ray spectra -> XYZ of camera rays [first_ray, first_ray + n_rays):
+ * 3 floats per ray into d_xyz (device).  For parity tests of the shading. */
+MGK_API mgk_result mgk_shade_rays(mgk_context* ctx, const mgk_scene* s, const mgk_star* d_stars, uint32_t n_stars,
+                                  const float* d_xyz_w, uint64_t first_ray, uint32_t n_rays, float* d_xyz,
+                                  void* stream);
+
+/* ------------------------------------ reference-compatible trace API */
+/* Same types and layout as magik.h:583-648. */
+typedef enum e_mgk_test_particle_types { MGK_MASSIVE = 0, MGK_MASSLESS = 1 } e_mgk_test_particle_types;
+
+typedef struct magik_trace_geodesic_metric_parameters_t {
+    int32_t metric_type; /* e_magik_spacetime_metric_types */
+    bool time_reversed;
+    float event_horizon_scalar;
+    float schwarzschild_mass; /* kg */
+    float kerr_mass;          /* kg */
+    float kerr_spin;
+} magik_trace_geodesic_metric_parameters_t;
+
+typedef struct magik_trace_geodesic_integrator_parameters_t {
+    unsigned int n_integrator_max_substep;
+    float integrator_absolute_error_tolerance;
+    float integrator_relative_error_tolerance;
+} magik_trace_geodesic_integrator_parameters_t;
+
+typedef struct magik_trace_geodesic_inital_conditions_t {
+    int32_t test_particle_type; /* e_magik_test_particle_types */
+    float spatial_position_x, spatial_position_y, spatial_position_z;
+    float x_rotation, y_rotation, z_rotation;
+    float local_proper_velocity_x, local_proper_velocity_y, local_proper_velocity_z;
+    float massive_particle_speed;
+} magik_trace_geodesic_inital_conditions_t;
+
+typedef struct magik_trace_geodesic_step_t {
+    float four_position[4];
+    float four_momentum[4];
+    float moment_derivative[4];
+    float four_vector_contraction;
+    float affine_parameter;
+    float delta_affine_parameter;
+} magik_trace_geodesic_step_t;
+
+typedef struct magik_trace_geodesic_container_t {
+    uint64_t capacity;
+    uint32_t n_allocated_step;
+    uint32_t n_written;
+    magik_trace_geodesic_step_t* steps;
+} magik_trace_geodesic_container_t;
+
+/* Drop-in for the reference's magik_trace_geodesic (magik.h:656,
+ * magik.cpp:196-207): one geodesic into a caller-owned host step array, on
+ * the caller thread, synchronous.  Computed on the GPU (device 0 of the
+ * calling thread's current device) with the REF32 kernels, so the steps equal
+ * the reference CPU tracer's. */
+MGK_API int32_t magik_trace_geodesic(magik_trace_geodesic_container_t* container,
+                                     magik_trace_geodesic_inital_conditions_t initial_conditions,
+                                     magik_trace_geodesic_metric_parameters_t metric_parameters,
+                                     magik_trace_geodesic_integrator_parameters_t integrator_parameters);
+
+/* Batch form: n geodesics, one container each, traced concurrently on the GPU
+ * (one thread per geodesic). */
+MGK_API mgk_result mgk_trace_geodesic_batch(mgk_context* ctx, magik_trace_geodesic_container_t* containers,
+                                            const magik_trace_geodesic_inital_conditions_t* initial_conditions,
+                                            const magik_trace_geodesic_metric_parameters_t* metric_parameters,
+                                            const magik_trace_geodesic_integrator_parameters_t* integrator_parameters,
+                                            uint32_t n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MGK_H */

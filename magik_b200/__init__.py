@@ -1,0 +1,236 @@
+"""B200-native geodesic path: Python mirror of the C ABI in include/mgk.h.
+
+The compute path is libmgk.so (hand-written sm_100a kernels behind a C ABI);
+this module only loads it through ctypes and moves buffers.  There is no CPU
+fallback: every compute entry point raises if the library or a B200 is not
+available.  PyTorch is used for device memory and streams.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+from .abi import Scene, Star, RayResult, RenderStats  # noqa: F401
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmgk.so")
+
+_lib = None
+
+RESULT_DTYPE = np.dtype([("x", "<f8", 4), ("p", "<f8", 4), ("z", "<f8"), ("r_hit", "<f8"), ("dir", "<f8", 3),
+                         ("cls", "<u4"), ("steps", "<u4"), ("attempts", "<u4"), ("wide_attempts", "<u4"),
+                         ("refine_evals", "<u4"), ("reserved", "<u4")])
+STAR_DTYPE = np.dtype([("dir", "<f4", 3), ("amplitude", "<f4"), ("temperature", "<f4"), ("reserved", "<f4", 3)])
+STEP_DTYPE = np.dtype([("four_position", "<f4", 4), ("four_momentum", "<f4", 4), ("moment_derivative", "<f4", 4),
+                       ("four_vector_contraction", "<f4"), ("affine_parameter", "<f4"),
+                       ("delta_affine_parameter", "<f4")])
+assert RESULT_DTYPE.itemsize == 128 and STAR_DTYPE.itemsize == 32 and STEP_DTYPE.itemsize == 60
+
+EXPORTS = [
+    "mgk_context_create", "mgk_context_destroy", "mgk_last_error", "mgk_scene_defaults", "mgk_isco_radius",
+    "mgk_xyz_weights", "mgk_star_catalog", "mgk_scene_constants", "mgk_render", "mgk_render_host",
+    "mgk_trace_rays", "mgk_shade_rays", "magik_trace_geodesic", "mgk_trace_geodesic_batch", "mgk_fp32_peak",
+]
+
+
+class MgkError(RuntimeError):
+    def __init__(self, code, what, detail=""):
+        super().__init__(f"{what} failed with code {code}" + (f": {detail}" if detail else ""))
+        self.code = code
+
+
+def lib():
+    """The loaded libmgk.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m magik_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        P = C.POINTER
+        vp = C.c_void_p
+        L.mgk_context_create.argtypes = [C.c_int32, P(vp)]
+        L.mgk_context_destroy.argtypes = [vp]
+        L.mgk_last_error.argtypes = [vp]
+        L.mgk_last_error.restype = C.c_char_p
+        L.mgk_scene_defaults.argtypes = [P(Scene)]
+        L.mgk_scene_defaults.restype = None
+        L.mgk_isco_radius.argtypes = [C.c_double]
+        L.mgk_isco_radius.restype = C.c_double
+        L.mgk_xyz_weights.argtypes = [C.c_uint32, C.c_double, C.c_double, P(C.c_float)]
+        L.mgk_star_catalog.argtypes = [C.c_uint64, C.c_uint32, vp]
+        L.mgk_scene_constants.argtypes = [P(Scene), P(C.c_double)]
+        L.mgk_render.argtypes = [vp, P(Scene), vp, C.c_uint32, vp, vp, vp, P(RenderStats), vp]
+        L.mgk_render_host.argtypes = [vp, P(Scene), vp, C.c_uint32, vp, vp, P(RenderStats), vp]
+        L.mgk_trace_rays.argtypes = [vp, P(Scene), C.c_uint64, C.c_uint32, vp, vp]
+        L.mgk_shade_rays.argtypes = [vp, P(Scene), vp, C.c_uint32, vp, C.c_uint64, C.c_uint32, vp, vp]
+        L.magik_trace_geodesic.argtypes = [P(abi.TraceContainer), abi.TraceInitialConditions,
+                                           abi.TraceMetricParams, abi.TraceIntegratorParams]
+        L.magik_trace_geodesic.restype = C.c_int32
+        L.mgk_trace_geodesic_batch.argtypes = [vp, P(abi.TraceContainer), P(abi.TraceInitialConditions),
+                                               P(abi.TraceMetricParams), P(abi.TraceIntegratorParams), C.c_uint32]
+        L.mgk_fp32_peak.argtypes = [vp, P(C.c_double)]
+        for name in EXPORTS:
+            fn = getattr(L, name)
+            if fn.restype is C.c_int:  # ctypes default
+                fn.restype = C.c_int32
+        _lib = L
+    return _lib
+
+
+def _check(code, what, ctx=None):
+    if code != abi.SUCCESS:
+        detail = lib().mgk_last_error(ctx).decode() if ctx else ""
+        raise MgkError(code, what, detail)
+
+
+# ------------------------------------------------------------ host helpers
+def scene_defaults(**overrides):
+    s = Scene()
+    lib().mgk_scene_defaults(C.byref(s))
+    for k, v in overrides.items():
+        if not hasattr(s, k):
+            raise AttributeError(k)
+        setattr(s, k, v)
+    return s
+
+
+def isco_radius(spin):
+    return lib().mgk_isco_radius(float(spin))
+
+
+def xyz_weights(n_bins, lambda_min_nm=380.0, lambda_max_nm=780.0):
+    out = (C.c_float * (3 * n_bins))()
+    _check(lib().mgk_xyz_weights(n_bins, lambda_min_nm, lambda_max_nm, out), "mgk_xyz_weights")
+    return np.frombuffer(out, dtype=np.float32).reshape(n_bins, 3).copy()
+
+
+def star_catalog(seed, n):
+    out = np.zeros(n, dtype=STAR_DTYPE)
+    _check(lib().mgk_star_catalog(seed, n, out.ctypes.data_as(C.c_void_p)), "mgk_star_catalog")
+    return out
+
+
+def scene_constants(scene):
+    out = (C.c_double * 32)()
+    _check(lib().mgk_scene_constants(C.byref(scene), out), "mgk_scene_constants")
+    return np.frombuffer(out, dtype=np.float64).copy()
+
+
+def _stream_ptr(stream):
+    if stream is None:
+        import torch
+        return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    return C.c_void_p(getattr(stream, "cuda_stream", stream))
+
+
+# ----------------------------------------------------------------- context
+class Context:
+    """A device context (mgk_context): kernels, scratch arena, events."""
+
+    def __init__(self, device=0):
+        h = C.c_void_p()
+        _check(lib().mgk_context_create(device, C.byref(h)), "mgk_context_create")
+        self.handle = h
+        self.device = device
+
+    def close(self):
+        if self.handle:
+            lib().mgk_context_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def fp32_peak(self):
+        """Measured FP32 FLOP/s of this device (FMA probe)."""
+        v = C.c_double(0)
+        _check(lib().mgk_fp32_peak(self.handle, C.byref(v)), "mgk_fp32_peak", self.handle)
+        return v.value
+
+    # -- device-buffer entry points (torch CUDA tensors)
+    def render(self, scene, d_stars, d_film_xyz, d_weights=None, d_film_spectral=None, want_stats=True,
+               stream=None):
+        """mgk_render: d_stars (uint8/any CUDA tensor of n*32 bytes or None), d_film_xyz float32 [H*W*3]."""
+        n_stars = 0 if d_stars is None else d_stars.numel() * d_stars.element_size() // 32
+        st = RenderStats() if want_stats else None
+        rc = lib().mgk_render(self.handle, C.byref(scene), None if d_stars is None else d_stars.data_ptr(),
+                              n_stars, None if d_weights is None else d_weights.data_ptr(), d_film_xyz.data_ptr(),
+                              None if d_film_spectral is None else d_film_spectral.data_ptr(),
+                              C.byref(st) if st is not None else None, _stream_ptr(stream))
+        _check(rc, "mgk_render", self.handle)
+        return st
+
+    def render_host(self, scene, h_stars, h_film_xyz, h_weights=None, want_stats=True, stream=None):
+        """mgk_render_host: host pointers (numpy arrays or pinned torch tensors)."""
+        def ptr(a):
+            if a is None:
+                return None
+            return a.data_ptr() if hasattr(a, "data_ptr") else a.ctypes.data
+        n_stars = 0 if h_stars is None else (h_stars.nbytes if hasattr(h_stars, "nbytes") else
+                                             h_stars.numel() * h_stars.element_size()) // 32
+        st = RenderStats() if want_stats else None
+        rc = lib().mgk_render_host(self.handle, C.byref(scene), ptr(h_stars), n_stars, ptr(h_weights),
+                                   ptr(h_film_xyz), C.byref(st) if st is not None else None, _stream_ptr(stream))
+        _check(rc, "mgk_render_host", self.handle)
+        return st
+
+    def trace_rays(self, scene, first, n, stream=None):
+        """Per-ray results of camera rays [first, first+n) as a numpy structured array."""
+        import torch
+        buf = torch.empty(max(n, 1) * 128, dtype=torch.uint8, device=f"cuda:{self.device}")
+        _check(lib().mgk_trace_rays(self.handle, C.byref(scene), first, n, buf.data_ptr(), _stream_ptr(stream)),
+               "mgk_trace_rays", self.handle)
+        host = buf.cpu().numpy()
+        return host[: n * 128].view(RESULT_DTYPE).copy()
+
+    def shade_rays(self, scene, stars, weights, first, n, stream=None):
+        """Per-ray XYZ of camera rays [first, first+n) as a float32 [n, 3] numpy array."""
+        import torch
+        dev = f"cuda:{self.device}"
+        d_stars = None if stars is None or len(stars) == 0 else torch.from_numpy(
+            np.ascontiguousarray(stars).view(np.uint8)).to(dev)
+        d_w = None if weights is None else torch.from_numpy(np.ascontiguousarray(weights, np.float32).ravel()).to(dev)
+        out = torch.empty(max(n, 1) * 3, dtype=torch.float32, device=dev)
+        rc = lib().mgk_shade_rays(self.handle, C.byref(scene), None if d_stars is None else d_stars.data_ptr(),
+                                  0 if d_stars is None else len(stars), None if d_w is None else d_w.data_ptr(),
+                                  first, n, out.data_ptr(), _stream_ptr(stream))
+        _check(rc, "mgk_shade_rays", self.handle)
+        return out.cpu().numpy()[: 3 * n].reshape(n, 3)
+
+    def trace_geodesic_batch(self, ics, mps, ips, n_steps):
+        """Reference-compatible traces: one container of n_steps steps per geodesic."""
+        n = len(ics)
+        steps = [(abi.TraceStep * n_steps)() for _ in range(n)]
+        cs = (abi.TraceContainer * n)()
+        for i in range(n):
+            cs[i] = abi.TraceContainer(C.sizeof(abi.TraceStep) * n_steps, n_steps, 0,
+                                       C.cast(steps[i], C.POINTER(abi.TraceStep)))
+        ic_a = (abi.TraceInitialConditions * n)(*ics)
+        mp_a = (abi.TraceMetricParams * n)(*mps)
+        ip_a = (abi.TraceIntegratorParams * n)(*ips)
+        _check(lib().mgk_trace_geodesic_batch(self.handle, cs, ic_a, mp_a, ip_a, n), "mgk_trace_geodesic_batch",
+               self.handle)
+        out = []
+        for i in range(n):
+            a = np.frombuffer(steps[i], dtype=np.float32).reshape(n_steps, 15)
+            out.append(a[: cs[i].n_written].copy())
+        return out
+
+
+def trace_geodesic(ic, mp, ip, n_steps=4096):
+    """magik_trace_geodesic through libmgk (GPU).  Returns (code, steps[n_written, 15])."""
+    steps = (abi.TraceStep * n_steps)()
+    c = abi.TraceContainer(C.sizeof(abi.TraceStep) * n_steps, n_steps, 0, C.cast(steps, C.POINTER(abi.TraceStep)))
+    rc = lib().magik_trace_geodesic(C.byref(c), ic, mp, ip)
+    a = np.frombuffer(steps, dtype=np.float32).reshape(n_steps, 15)
+    return rc, a[: c.n_written].copy()

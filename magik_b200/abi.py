@@ -1,0 +1,103 @@
+"""ctypes mirror of include/mgk.h (the C ABI of libmgk.so).
+
+Only plain C layouts live here; the loader and the Python-facing functions are
+in magik_b200/__init__.py.
+"""
+import ctypes as C
+
+SUCCESS = 0
+ERROR_INVALID_POINTER = 2
+ERROR_HOST_TRACE_ALLOCATED_STEPS_AND_CAPACITY_MISMATCH = 102
+ERROR_UNKNOWN = 10000
+ERROR_INVALID_ARGUMENT = 10001
+ERROR_CUDA = 10002
+ERROR_NO_DEVICE = 10003
+ERROR_DEVICE_STATUS = 10004
+
+METRIC_MINKOWSKI, METRIC_SCHWARZSCHILD, METRIC_KERR = 0, 1, 2
+PRECISION_REF32, PRECISION_MIXED, PRECISION_F64 = 0, 1, 2
+RAY_ALIVE, RAY_DISK, RAY_ESCAPED, RAY_HORIZON, RAY_STEP_LIMIT = 0, 1, 2, 3, 4
+CLASS_NAMES = {0: "alive", 1: "disk", 2: "escaped", 3: "horizon", 4: "step_limit"}
+MASSIVE, MASSLESS = 0, 1
+MAX_BINS = 64
+WIDE_BAND = 0.05
+
+
+class Scene(C.Structure):
+    _fields_ = [
+        ("metric", C.c_int32), ("precision", C.c_int32), ("time_reversed", C.c_int32),
+        ("n_max_substep", C.c_uint32),
+        ("spin", C.c_double), ("mass_sign", C.c_double), ("horizon_scalar", C.c_double),
+        ("abs_tol", C.c_double), ("rel_tol", C.c_double), ("h_max", C.c_double),
+        ("max_steps", C.c_uint32), ("n_bins", C.c_uint32),
+        ("escape_radius", C.c_double), ("disk_r_in", C.c_double), ("disk_r_out", C.c_double),
+        ("disk_T_in", C.c_double), ("cam_r", C.c_double), ("cam_incl_rad", C.c_double),
+        ("focal_length_mm", C.c_double), ("sensor_diag_mm", C.c_double),
+        ("width", C.c_uint32), ("height", C.c_uint32), ("spp", C.c_uint32), ("reserved0", C.c_uint32),
+        ("seed", C.c_uint64), ("lambda_min_nm", C.c_double), ("lambda_max_nm", C.c_double),
+        ("star_radius_rad", C.c_double),
+    ]
+
+    def copy(self):
+        s = Scene()
+        C.pointer(s)[0] = self
+        return s
+
+    def __repr__(self):
+        return "Scene(" + ", ".join(f"{n}={getattr(self, n)!r}" for n, _ in self._fields_) + ")"
+
+
+class Star(C.Structure):
+    _fields_ = [("dir", C.c_float * 3), ("amplitude", C.c_float), ("temperature", C.c_float),
+                ("reserved", C.c_float * 3)]
+
+
+class RayResult(C.Structure):
+    _fields_ = [("x", C.c_double * 4), ("p", C.c_double * 4), ("z", C.c_double), ("r_hit", C.c_double),
+                ("dir", C.c_double * 3), ("cls", C.c_uint32), ("steps", C.c_uint32),
+                ("attempts", C.c_uint32), ("wide_attempts", C.c_uint32),
+                ("refine_evals", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class RenderStats(C.Structure):
+    _fields_ = [("rays", C.c_uint64), ("attempts", C.c_uint64), ("steps", C.c_uint64),
+                ("wide_attempts", C.c_uint64), ("refine_evals", C.c_uint64),
+                ("class_count", C.c_uint64 * 5),
+                ("integrate_ms", C.c_double), ("total_ms", C.c_double)]
+
+
+class TraceMetricParams(C.Structure):
+    _fields_ = [("metric_type", C.c_int32), ("time_reversed", C.c_bool), ("event_horizon_scalar", C.c_float),
+                ("schwarzschild_mass", C.c_float), ("kerr_mass", C.c_float), ("kerr_spin", C.c_float)]
+
+
+class TraceIntegratorParams(C.Structure):
+    _fields_ = [("n_integrator_max_substep", C.c_uint), ("integrator_absolute_error_tolerance", C.c_float),
+                ("integrator_relative_error_tolerance", C.c_float)]
+
+
+class TraceInitialConditions(C.Structure):
+    _fields_ = [("test_particle_type", C.c_int32),
+                ("spatial_position_x", C.c_float), ("spatial_position_y", C.c_float),
+                ("spatial_position_z", C.c_float),
+                ("x_rotation", C.c_float), ("y_rotation", C.c_float), ("z_rotation", C.c_float),
+                ("local_proper_velocity_x", C.c_float), ("local_proper_velocity_y", C.c_float),
+                ("local_proper_velocity_z", C.c_float), ("massive_particle_speed", C.c_float)]
+
+
+class TraceStep(C.Structure):
+    _fields_ = [("four_position", C.c_float * 4), ("four_momentum", C.c_float * 4),
+                ("moment_derivative", C.c_float * 4), ("four_vector_contraction", C.c_float),
+                ("affine_parameter", C.c_float), ("delta_affine_parameter", C.c_float)]
+
+
+class TraceContainer(C.Structure):
+    _fields_ = [("capacity", C.c_uint64), ("n_allocated_step", C.c_uint32), ("n_written", C.c_uint32),
+                ("steps", C.POINTER(TraceStep))]
+
+
+assert C.sizeof(Scene) == 184, C.sizeof(Scene)
+assert C.sizeof(Star) == 32
+assert C.sizeof(RayResult) == 128
+assert C.sizeof(TraceStep) == 60
+assert C.sizeof(TraceMetricParams) == 24

@@ -1,0 +1,292 @@
+// Device physics of the geodesic path: metrics, RKF45 attempt, step control.
+//
+// Every function is templated on the scalar T (float / double) and on an FMA
+// policy F.  The whole library is compiled with -fmad=false, so a plain
+// a*b + c always rounds twice; mad<Fuse::Fma>() fuses exactly where written.
+//   Fuse::None reproduces the reference's expression trees (metric_kerr.cuh,
+//   metric_schwarzschild.cuh, internal_math.h) with separate roundings, i.e.
+//   what the reference computes on the CPU.
+//   Fuse::Fma uses the same trees with the marked multiply-adds fused.
+// Division and sqrt are IEEE-rounded (-prec-div/-prec-sqrt, no fast math).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace mgk {
+
+enum class Fuse { None, Fma };
+
+template <Fuse F> __device__ __forceinline__ float mad(float a, float b, float c) {
+    if constexpr (F == Fuse::Fma) return __fmaf_rn(a, b, c);
+    else return __fadd_rn(__fmul_rn(a, b), c);
+}
+template <Fuse F> __device__ __forceinline__ double mad(double a, double b, double c) {
+    if constexpr (F == Fuse::Fma) return __fma_rn(a, b, c);
+    else return __dadd_rn(__dmul_rn(a, b), c);
+}
+
+// Geodesic state without the conserved p_t: position (x, y, z, t) and
+// covariant spatial momentum (px, py, pz).  p_t is carried beside it.
+template <class T> struct S7 { T x, y, z, t, px, py, pz; };
+
+template <class T> struct MP {  // per-metric integrator parameters (metric_kerr.cuh:112-123)
+    T spin;        // as integrated (flipped when time reversed)
+    T mass_sign;   // Schwarzschild
+    T horizon;     // (1 + sqrt(1 - a^2)) * horizon_scalar, or 2 * scalar (Schwarzschild)
+    T spin_abs_gt1;  // 1 if |spin| > 1 (Kerr never captures then)
+    T h_max, abs_tol, rel_tol;
+    uint32_t n_max;
+};
+
+// ------------------------------------------------------------------ RHS
+// Kerr, metric_kerr.cuh:38-105 (same tree; Fuse::None is exact).
+template <Fuse F, class T>
+__device__ __forceinline__ void rhs_kerr(const S7<T>& s, T pt, T a, S7<T>& o) {
+    const T x = s.x, y = s.y, z = s.z, px = s.px, py = s.py, pz = s.pz;
+    const T one = T(1), half = T(0.5), two = T(2);
+    T a_sq = a * a;
+    T y_sq = y * y;
+    T w_sq = mad<F>(z, z, mad<F>(y, y, x * x)) - a_sq;
+    T sigma = sqrt(mad<F>(w_sq, w_sq, (T(4) * a_sq) * y_sq));
+    T r = sqrt(half * (w_sq + sigma));
+    T r_sq = r * r;
+    T r_cu = r_sq * r;
+    T r_quad = r_sq * r_sq;
+    T r_six = r_cu * r_cu;
+    T inv_r = one / r;
+    T inv_rsq = inv_r * inv_r;
+    T inv_sigma = one / sigma;
+    T scale_xz = (half * inv_r) * mad<F>(w_sq, inv_sigma, one);
+    T scale_y = (half * inv_r) * mad<F>(w_sq + two * a_sq, inv_sigma, one);
+    T drx = x * scale_xz, dry = y * scale_y, drz = z * scale_xz;
+    T d = r_sq + a_sq;
+    T inv_d = one / d;
+    T inv_dsq = inv_d * inv_d;
+    T kx_num = mad<F>(r, x, -(a * z));
+    T kz_num = mad<F>(r, z, a * x);
+    T kx = kx_num * inv_d;
+    T kz = kz_num * inv_d;
+    T ky = y * inv_r;
+    T f_den = mad<F>(a_sq, y_sq, r_quad);
+    T inv_f_den_sq = one / (f_den * f_den);
+    T f_ = (two * r_cu) / f_den;
+    T dfdq_scale = (two * mad<F>((T(3) * a_sq) * r_sq, y_sq, -r_six)) * inv_f_den_sq;
+    T dfx = dfdq_scale * drx;
+    T dfy = mad<F>(dfdq_scale, dry, -((((T(4) * a_sq) * r_cu) * y) * inv_f_den_sq));
+    T dfz = dfdq_scale * drz;
+    T two_r = two * r;
+    T dkx_dx = mad<F>(mad<F>(x, drx, r), d, -((two_r * drx) * kx_num)) * inv_dsq;
+    T dkx_dy = mad<F>(x * dry, d, -((two_r * dry) * kx_num)) * inv_dsq;
+    T dkx_dz = mad<F>(mad<F>(x, drz, -a), d, -((two_r * drz) * kx_num)) * inv_dsq;
+    T dky_dx = ((-y) * drx) * inv_rsq;
+    T dky_dy = mad<F>(-y, dry, r) * inv_rsq;
+    T dky_dz = ((-y) * drz) * inv_rsq;
+    T dkz_dx = mad<F>(mad<F>(z, drx, a), d, -((two_r * drx) * kz_num)) * inv_dsq;
+    T dkz_dy = mad<F>(z * dry, d, -((two_r * dry) * kz_num)) * inv_dsq;
+    T dkz_dz = mad<F>(mad<F>(z, drz, r), d, -((two_r * drz) * kz_num)) * inv_dsq;
+    T kTp = mad<F>(pz, kz, mad<F>(py, ky, px * kx)) - pt;
+    T f_kTp = f_ * kTp;
+    T half_kTp_sq = (half * kTp) * kTp;
+    T bx = mad<F>(pz, dkz_dx, mad<F>(py, dky_dx, px * dkx_dx));
+    T by = mad<F>(pz, dkz_dy, mad<F>(py, dky_dy, px * dkx_dy));
+    T bz = mad<F>(pz, dkz_dz, mad<F>(py, dky_dz, px * dkx_dz));
+    o.x = mad<F>(-f_kTp, kx, px);
+    o.y = mad<F>(-f_kTp, ky, py);
+    o.z = mad<F>(-f_kTp, kz, pz);
+    o.t = -pt + f_kTp;
+    o.px = mad<F>(f_kTp, bx, half_kTp_sq * dfx);
+    o.py = mad<F>(f_kTp, by, half_kTp_sq * dfy);
+    o.pz = mad<F>(f_kTp, bz, half_kTp_sq * dfz);
+}
+
+// Schwarzschild, metric_schwarzschild.cuh:8-72.
+template <Fuse F, class T>
+__device__ __forceinline__ void rhs_schwarzschild(const S7<T>& s, T pt, T mass_sign, S7<T>& o) {
+    const T x = s.x, y = s.y, z = s.z, px = s.px, py = s.py, pz = s.pz;
+    const T one = T(1), half = T(0.5), two = T(2);
+    T w_sq = mad<F>(z, z, mad<F>(y, y, x * x));
+    T sigma = w_sq;
+    T r = sqrt(half * (w_sq + sigma));
+    T r_sq = r * r;
+    T r_cu = r_sq * r;
+    T r_quad = r_sq * r_sq;
+    T r_six = r_cu * r_cu;
+    T inv_r = one / r;
+    T inv_rsq = inv_r * inv_r;
+    T inv_sigma = one / sigma;
+    T sc = (half * inv_r) * mad<F>(w_sq, inv_sigma, one);
+    T drx = x * sc, dry = y * sc, drz = z * sc;
+    T d = r_sq;
+    T inv_d = one / d;
+    T inv_dsq = inv_d * inv_d;
+    T kx_num = r * x;
+    T kz_num = r * z;
+    T kx = kx_num * inv_d;
+    T kz = kz_num * inv_d;
+    T ky = y * inv_r;
+    T f_den = r_quad;
+    T inv_f_den_sq = one / (f_den * f_den);
+    T f_ = ((mass_sign * two) * r_cu) / f_den;
+    T dfdq_scale = ((mass_sign * two) * (-r_six)) * inv_f_den_sq;
+    T dfx = dfdq_scale * drx, dfy = dfdq_scale * dry, dfz = dfdq_scale * drz;
+    T two_r = two * r;
+    T dkx_dx = mad<F>(mad<F>(x, drx, r), d, -((two_r * drx) * kx_num)) * inv_dsq;
+    T dkx_dy = mad<F>(x * dry, d, -((two_r * dry) * kx_num)) * inv_dsq;
+    T dkx_dz = mad<F>(x * drz, d, -((two_r * drz) * kx_num)) * inv_dsq;
+    T dky_dx = ((-y) * drx) * inv_rsq;
+    T dky_dy = mad<F>(-y, dry, r) * inv_rsq;
+    T dky_dz = ((-y) * drz) * inv_rsq;
+    T dkz_dx = mad<F>(z * drx, d, -((two_r * drx) * kz_num)) * inv_dsq;
+    T dkz_dy = mad<F>(z * dry, d, -((two_r * dry) * kz_num)) * inv_dsq;
+    T dkz_dz = mad<F>(mad<F>(z, drz, r), d, -((two_r * drz) * kz_num)) * inv_dsq;
+    T kTp = mad<F>(pz, kz, mad<F>(py, ky, px * kx)) - pt;
+    T f_kTp = f_ * kTp;
+    T half_kTp_sq = (half * kTp) * kTp;
+    T bx = mad<F>(pz, dkz_dx, mad<F>(py, dky_dx, px * dkx_dx));
+    T by = mad<F>(pz, dkz_dy, mad<F>(py, dky_dy, px * dkx_dy));
+    T bz = mad<F>(pz, dkz_dz, mad<F>(py, dky_dz, px * dkx_dz));
+    o.x = mad<F>(-f_kTp, kx, px);
+    o.y = mad<F>(-f_kTp, ky, py);
+    o.z = mad<F>(-f_kTp, kz, pz);
+    o.t = -pt + f_kTp;
+    o.px = mad<F>(f_kTp, bx, half_kTp_sq * dfx);
+    o.py = mad<F>(f_kTp, by, half_kTp_sq * dfy);
+    o.pz = mad<F>(f_kTp, bz, half_kTp_sq * dfz);
+}
+
+// Minkowski, metric_minkowski.cuh:8-13.
+template <class T> __device__ __forceinline__ void rhs_minkowski(const S7<T>& s, T pt, S7<T>& o) {
+    o.x = s.px; o.y = s.py; o.z = s.pz; o.t = -pt;
+    o.px = T(0); o.py = T(0); o.pz = T(0);
+}
+
+template <int METRIC, Fuse F, class T>
+__device__ __forceinline__ void rhs(const S7<T>& s, T pt, const MP<T>& m, S7<T>& o) {
+    if constexpr (METRIC == 2) rhs_kerr<F, T>(s, pt, m.spin, o);
+    else if constexpr (METRIC == 1) rhs_schwarzschild<F, T>(s, pt, m.mass_sign, o);
+    else rhs_minkowski<T>(s, pt, o);
+}
+
+// kerr_schild_r, metric_kerr.cuh:8-13.
+template <class T> __device__ __forceinline__ T kerr_schild_r(T x, T y, T z, T a) {
+    T R = (x * x + y * y + z * z - a * a);
+    T r_squared = T(0.5) * R + T(0.5) * sqrt(R * R + T(4) * a * a * y * y);
+    return sqrt(r_squared);
+}
+
+// Horizon test (true = captured): metric_kerr.cuh:169-175 (NaN r captures),
+// metric_schwarzschild.cuh:136-141, Minkowski never.
+template <int METRIC, class T> __device__ __forceinline__ bool in_domain(T x, T y, T z, const MP<T>& m) {
+    if constexpr (METRIC == 2) {
+        if (m.spin_abs_gt1 != T(0)) return false;
+        T r = kerr_schild_r(x, y, z, m.spin);
+        if (m.horizon < r) return false;
+        return true;
+    } else if constexpr (METRIC == 1) {
+        T r = sqrt(x * x + y * y + z * z);
+        if (m.mass_sign < T(0)) return r < T(1e-3);
+        return r <= m.horizon;
+    } else {
+        return false;
+    }
+}
+
+// ------------------------------------------------------------- RKF45
+// Fehlberg 4(5) tableau as written in internal_math.h:2169-2177.
+template <class T> struct FB {
+    static constexpr T a21 = T(1) / T(4);
+    static constexpr T a31 = T(3) / T(32), a32 = T(9) / T(32);
+    static constexpr T a41 = T(1932) / T(2197), a42 = T(7200) / T(2197), a43 = T(7296) / T(2197);
+    static constexpr T a51 = T(439) / T(216), a52 = T(8), a53 = T(3680) / T(513), a54 = T(845) / T(4104);
+    static constexpr T a61 = T(8) / T(27), a62 = T(2), a63 = T(3544) / T(2565), a64 = T(1859) / T(4104),
+                       a65 = T(11) / T(40);
+    static constexpr T b1 = T(16) / T(135), b3 = T(6656) / T(12825), b4 = T(28561) / T(56430), b5 = T(9) / T(50),
+                       b6 = T(2) / T(55);
+    static constexpr T e1 = T(-1) / T(360), e3 = T(128) / T(4275), e4 = T(2197) / T(75240), e5 = T(1) / T(50),
+                       e6 = T(2) / T(55);
+};
+
+template <Fuse F, class T> __device__ __forceinline__ S7<T> axpy(T c, const S7<T>& k, const S7<T>& y) {
+    return S7<T>{mad<F>(c, k.x, y.x), mad<F>(c, k.y, y.y), mad<F>(c, k.z, y.z), mad<F>(c, k.t, y.t),
+                 mad<F>(c, k.px, y.px), mad<F>(c, k.py, y.py), mad<F>(c, k.pz, y.pz)};
+}
+template <class T> __device__ __forceinline__ S7<T> scl(T c, const S7<T>& k) {
+    return S7<T>{c * k.x, c * k.y, c * k.z, c * k.t, c * k.px, c * k.py, c * k.pz};
+}
+template <class T, class U> __device__ __forceinline__ S7<T> cvt(const S7<U>& s) {
+    return S7<T>{T(s.x), T(s.y), T(s.z), T(s.t), T(s.px), T(s.py), T(s.pz)};
+}
+
+// One attempt: six stages, the 5th-order solution y1 and the stages k.
+template <int METRIC, Fuse F, class T>
+__device__ __forceinline__ void rkf45_stages(const S7<T>& y0, T pt, T h, const MP<T>& m, S7<T>& y1, S7<T> k[6]) {
+    using C = FB<T>;
+    rhs<METRIC, F, T>(y0, pt, m, k[0]);
+    rhs<METRIC, F, T>(axpy<F>(C::a21 * h, k[0], y0), pt, m, k[1]);
+    rhs<METRIC, F, T>(axpy<F>(C::a32 * h, k[1], axpy<F>(C::a31 * h, k[0], y0)), pt, m, k[2]);
+    rhs<METRIC, F, T>(axpy<F>(C::a43 * h, k[2], axpy<F>(-(C::a42 * h), k[1], axpy<F>(C::a41 * h, k[0], y0))), pt, m,
+                      k[3]);
+    rhs<METRIC, F, T>(axpy<F>(-(C::a54 * h), k[3],
+                              axpy<F>(C::a53 * h, k[2], axpy<F>(-(C::a52 * h), k[1], axpy<F>(C::a51 * h, k[0], y0)))),
+                      pt, m, k[4]);
+    rhs<METRIC, F, T>(
+        axpy<F>(-(C::a65 * h), k[4],
+                axpy<F>(C::a64 * h, k[3],
+                        axpy<F>(-(C::a63 * h), k[2], axpy<F>(C::a62 * h, k[1], axpy<F>(-(C::a61 * h), k[0], y0))))),
+        pt, m, k[5]);
+    y1 = axpy<F>(C::b6 * h, k[5],
+                 axpy<F>(-(C::b5 * h), k[4],
+                         axpy<F>(C::b4 * h, k[3], axpy<F>(C::b3 * h, k[2], axpy<F>(C::b1 * h, k[0], y0)))));
+}
+
+template <Fuse F, class T> __device__ __forceinline__ S7<T> rkf45_error(T h, const S7<T> k[6]) {
+    using C = FB<T>;
+    return axpy<F>(-(C::e6 * h), k[5],
+                   axpy<F>(-(C::e5 * h), k[4], axpy<F>(C::e4 * h, k[3], axpy<F>(C::e3 * h, k[2], scl(C::e1 * h, k[0])))));
+}
+
+// RMS error norm, relativity_utilities.cuh:15-29 (component order t, x, y, z,
+// then momentum).  The p_t error term is identically zero (dp_t/dlambda = 0)
+// and the scale is positive (abs_tol > 0 is enforced), so it is left out.
+template <Fuse F, class T>
+__device__ __forceinline__ T rms_error(const S7<T>& e, const S7<T>& y0, const S7<T>& y1, T atol, T rtol) {
+    auto term = [&](T ei, T a0, T a1) { return ei / mad<F>(rtol, fmax(fabs(a0), fabs(a1)), atol); };
+    T s0 = term(e.t, y0.t, y1.t), s1 = term(e.x, y0.x, y1.x), s2 = term(e.y, y0.y, y1.y), s3 = term(e.z, y0.z, y1.z);
+    T s5 = term(e.px, y0.px, y1.px), s6 = term(e.py, y0.py, y1.py), s7 = term(e.pz, y0.pz, y1.pz);
+    T acc = s0 * s0;
+    acc = mad<F>(s1, s1, acc);
+    acc = mad<F>(s2, s2, acc);
+    acc = mad<F>(s3, s3, acc);
+    acc = mad<F>(s5, s5, acc);
+    acc = mad<F>(s6, s6, acc);
+    acc = mad<F>(s7, s7, acc);
+    return sqrt(acc / T(8));
+}
+
+// Error norm of the wide (FP64) controller from T-valued stages.
+template <class T>
+__device__ __forceinline__ double wide_error(const S7<T>& y0, const S7<T>& y1, const S7<T> k[6], T h, double atol,
+                                             double rtol) {
+    S7<double> kd[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) kd[i] = cvt<double>(k[i]);
+    S7<double> e = rkf45_error<Fuse::Fma, double>(double(h), kd);
+    return rms_error<Fuse::Fma, double>(e, cvt<double>(y0), cvt<double>(y1), atol, rtol);
+}
+
+// Reference step proposal 0.9*h*pow(1/err, 0.2f) (internal_math.h:2179-2195)
+// in float, with the pow evaluated in double and rounded once to float.
+__device__ __forceinline__ float propose_h_ref(float h, float err_safe, float h_max) {
+    float g = float(pow(double(1.0f / err_safe), double(0.2f)));
+    float h_new = (0.9f * h) * g;
+    if (h_new > h_max) h_new = h_max;
+    return h_new;
+}
+__device__ __forceinline__ double propose_h_wide(double h, double err_safe, double h_max) {
+    double h_new = (0.9 * h) * pow(1.0 / err_safe, 0.2);
+    if (h_new > h_max) h_new = h_max;
+    return h_new;
+}
+
+}  // namespace mgk

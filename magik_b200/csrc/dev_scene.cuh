@@ -1,0 +1,407 @@
+// Scene around the integrator: observer frames, camera rays, per-step
+// termination tests, disk emitter, blackbody, star lookup.
+//
+// Frames follow relativity_utilities.cuh:57-195 and the metric files'
+// compute_g / reference_observer; termination follows kernel_intersect.cu:55-138
+// (traceables before the horizon) and kernel_enforce_ray_limits.cu:37-64; the
+// emitter follows bxdf_utilities.cuh:89-109,156-163 (redshift, g^5 boost,
+// NaN/negative clamp) with a Keplerian thin disk in place of the reference's
+// boxes.  Functions marked MGK_HD also run on the host (scene set-up).
+#pragma once
+
+#include <cmath>
+#include <cstdint>
+
+#include "dev_physics.cuh"
+#include "../../include/mgk.h"
+
+#define MGK_HD __host__ __device__ __forceinline__
+
+namespace mgk {
+
+template <class T> struct V4 { T x, y, z, t; };
+template <class T> struct Sym4 { T tt, tx, ty, tz, xx, xy, xz, yy, yz, zz; };
+
+// ------------------------------------------------------------------ RNG
+// triplet_hash (internal_math.h:2027-2037) chained over (seed, stream, index, dim).
+MGK_HD uint32_t triplet_hash(uint32_t x) {
+    x ^= x >> 17; x *= 0xED5AD4BBu; x ^= x >> 11; x *= 0xAC4C1B51u;
+    x ^= x >> 15; x *= 0x31848BABu; x ^= x >> 14;
+    return x;
+}
+MGK_HD uint32_t rng_u32(uint64_t seed, uint32_t stream, uint32_t index, uint32_t dim) {
+    uint32_t h = triplet_hash(uint32_t(seed) ^ 0x9E3779B9u);
+    h = triplet_hash(h ^ uint32_t(seed >> 32));
+    h = triplet_hash(h ^ stream);
+    h = triplet_hash(h ^ index);
+    h = triplet_hash(h ^ (dim * 0x85EBCA6Bu + 1u));
+    return h;
+}
+MGK_HD float rng_unit(uint64_t seed, uint32_t stream, uint32_t index, uint32_t dim) {
+    return float(rng_u32(seed, stream, index, dim) >> 8) * (1.0f / 16777216.0f);
+}
+
+// ------------------------------------------------------------- frames
+template <class T> MGK_HD T ks_r(T x, T y, T z, T a) {
+    T R = (x * x + y * y + z * z - a * a);
+    T r_squared = T(0.5) * R + T(0.5) * sqrt(R * R + T(4) * a * a * y * y);
+    return sqrt(r_squared);
+}
+
+// compute_g: metric_kerr.cuh:177-190, metric_schwarzschild.cuh:143-153.
+template <class T> MGK_HD Sym4<T> compute_g(int metric, T x, T y, T z, T a, T mass_sign) {
+    if (metric == MGK_METRIC_MINKOWSKI) return Sym4<T>{T(-1), 0, 0, 0, T(1), 0, 0, T(1), 0, T(1)};
+    T f, kx, ky, kz;
+    if (metric == MGK_METRIC_KERR) {
+        const T r = ks_r(x, y, z, a);
+        f = T(2) * r * r * r / (r * r * r * r + a * a * y * y);
+        kx = (r * x - a * z) / (r * r + a * a);
+        ky = y / r;
+        kz = (r * z + a * x) / (r * r + a * a);
+    } else {
+        const T r = sqrt(x * x + y * y + z * z);
+        f = T(2) * mass_sign / r;
+        kx = x / r; ky = y / r; kz = z / r;
+    }
+    return Sym4<T>{T(-1) + f, f * kx, f * ky, f * kz, T(1) + f * kx * kx, f * kx * ky, f * kx * kz,
+                   T(1) + f * ky * ky, f * ky * kz, T(1) + f * kz * kz};
+}
+
+// reference_observer: metric_kerr.cuh:207-226, metric_schwarzschild.cuh:167-171.
+template <class T> MGK_HD V4<T> reference_observer(int metric, T x, T y, T z, T a, T mass_sign) {
+    if (metric == MGK_METRIC_MINKOWSKI) return V4<T>{0, 0, 0, T(1)};
+    if (metric == MGK_METRIC_SCHWARZSCHILD) {
+        Sym4<T> g = compute_g<T>(metric, x, y, z, a, mass_sign);
+        return V4<T>{0, 0, 0, T(1) / sqrt(-g.tt)};
+    }
+    T r = ks_r(x, y, z, a);
+    T r_sq = r * r;
+    T a_sq = a * a;
+    T cos_theta = y / r;
+    T sin2_theta = T(1) - cos_theta * cos_theta;
+    T sigma = r_sq + a_sq * cos_theta * cos_theta;
+    T delta = r_sq - T(2) * r + a_sq;
+    T Lambda = (r_sq + a_sq) * (r_sq + a_sq) - a_sq * delta * sin2_theta;
+    T u_t = sqrt(Lambda / (delta * sigma));
+    T u_phi = T(2) * a * r / sqrt(Lambda * delta * sigma);
+    return V4<T>{z * u_phi, T(0), -x * u_phi, u_t};
+}
+
+// inner_product / contract, relativity_utilities.cuh:122-139.
+template <class T> MGK_HD T inner_product(const Sym4<T>& g, const V4<T>& u, const V4<T>& v) {
+    return g.tt * u.t * v.t + g.tx * (u.t * v.x + u.x * v.t) + g.ty * (u.t * v.y + u.y * v.t) +
+           g.tz * (u.t * v.z + u.z * v.t) + g.xx * u.x * v.x + g.xy * (u.x * v.y + u.y * v.x) +
+           g.xz * (u.x * v.z + u.z * v.x) + g.yy * u.y * v.y + g.yz * (u.y * v.z + u.z * v.y) + g.zz * u.z * v.z;
+}
+template <class T> MGK_HD V4<T> contract(const Sym4<T>& g, const V4<T>& u) {
+    return V4<T>{g.tx * u.t + g.xx * u.x + g.xy * u.y + g.xz * u.z, g.ty * u.t + g.xy * u.x + g.yy * u.y + g.yz * u.z,
+                 g.tz * u.t + g.xz * u.x + g.yz * u.y + g.zz * u.z, g.tt * u.t + g.tx * u.x + g.ty * u.y + g.tz * u.z};
+}
+template <class T> MGK_HD V4<T> v_add(V4<T> a, V4<T> b) { return V4<T>{a.x + b.x, a.y + b.y, a.z + b.z, a.t + b.t}; }
+template <class T> MGK_HD V4<T> v_sub(V4<T> a, V4<T> b) { return V4<T>{a.x - b.x, a.y - b.y, a.z - b.z, a.t - b.t}; }
+template <class T> MGK_HD V4<T> v_mul(T s, V4<T> a) { return V4<T>{s * a.x, s * a.y, s * a.z, s * a.t}; }
+template <class T> MGK_HD V4<T> v_div(V4<T> a, T s) { return V4<T>{a.x / s, a.y / s, a.z / s, a.t / s}; }
+// vector_dot_product of 4-vectors (internal_math.h:1094-1097): u^mu p_mu.
+template <class T> MGK_HD T dot4(V4<T> a, V4<T> b) { return ((a.x * b.x) + (a.y * b.y) + (a.z * b.z)) + (a.t * b.t); }
+
+template <class T> struct Tetrad { V4<T> t, x, y, z; };
+// build_tetrad: Gram-Schmidt of the seeds against u in the order z, x, y
+// (relativity_utilities.cuh:141-156).
+template <class T> MGK_HD Tetrad<T> build_tetrad(const Sym4<T>& g, V4<T> X, V4<T> Y, V4<T> Z, V4<T> u) {
+    Tetrad<T> e;
+    e.t = u;
+    e.z = v_add(Z, v_mul(inner_product(g, Z, u), u));
+    e.z = v_div(e.z, T(sqrt(inner_product(g, e.z, e.z))));
+    e.x = v_sub(v_add(X, v_mul(inner_product(g, X, u), u)), v_mul(inner_product(g, X, e.z), e.z));
+    e.x = v_div(e.x, T(sqrt(inner_product(g, e.x, e.x))));
+    e.y = v_sub(v_sub(v_add(Y, v_mul(inner_product(g, Y, u), u)), v_mul(inner_product(g, Y, e.z), e.z)),
+                v_mul(inner_product(g, Y, e.x), e.x));
+    e.y = v_div(e.y, T(sqrt(inner_product(g, e.y, e.y))));
+    return e;
+}
+// local_to_global, relativity_utilities.cuh:158-161.
+template <class T> MGK_HD V4<T> local_to_global(const Tetrad<T>& e, V4<T> l) {
+    return v_add(v_add(v_add(v_mul(l.t, e.t), v_mul(l.x, e.x)), v_mul(l.y, e.y)), v_mul(l.z, e.z));
+}
+
+// ---------------------------------------------------------- scene table
+// Per-scene constants, computed once on the host in double.
+struct SceneConsts {
+    double cam_pos[4];
+    double u_obs[4];
+    double M[4][4];       // p_mu = M . (n_x, n_y, n_z, |n|)
+    double pix_a, pix_b;  // camera-frame x = (px + jx) * pix_a + pix_b
+    double pix_c, pix_d;  // camera-frame y = (py + jy) * pix_c + pix_d
+    double r_plus;
+    double spin_t;
+    double omega_sign;
+};
+
+inline SceneConsts scene_consts(const mgk_scene& s) {
+    SceneConsts c{};
+    const int metric = s.metric;
+    const double a = s.time_reversed ? -s.spin : s.spin;
+    const double ms = s.mass_sign < 0 ? -1.0 : 1.0;
+    double ci = std::cos(s.cam_incl_rad), si = std::sin(s.cam_incl_rad);
+    V4<double> q{0.0, s.cam_r * ci, s.cam_r * si, 0.0};
+    c.cam_pos[0] = q.x; c.cam_pos[1] = q.y; c.cam_pos[2] = q.z; c.cam_pos[3] = q.t;
+    V4<double> X{1, 0, 0, 0}, Y{0, si, -ci, 0}, Z{0, ci, si, 0};  // right, up, back
+    V4<double> u = reference_observer<double>(metric, q.x, q.y, q.z, a, ms);
+    Sym4<double> g = compute_g<double>(metric, q.x, q.y, q.z, a, ms);
+    Tetrad<double> e = build_tetrad<double>(g, X, Y, Z, u);
+    V4<double> cols[4] = {contract(g, e.x), contract(g, e.y), contract(g, e.z), contract(g, e.t)};
+    for (int j = 0; j < 4; ++j) {
+        c.M[0][j] = cols[j].x; c.M[1][j] = cols[j].y; c.M[2][j] = cols[j].z; c.M[3][j] = cols[j].t;
+    }
+    c.u_obs[0] = u.x; c.u_obs[1] = u.y; c.u_obs[2] = u.z; c.u_obs[3] = u.t;
+    double tan_half = s.sensor_diag_mm / (2.0 * s.focal_length_mm);
+    double W = s.width, H = s.height;
+    c.pix_a = 2.0 * tan_half / W;
+    c.pix_b = -tan_half;
+    c.pix_c = -2.0 * tan_half / W;
+    c.pix_d = tan_half * H / W;
+    double ap = metric == MGK_METRIC_KERR ? s.spin : 0.0;
+    double d1 = 1.0 - ap * ap;
+    c.r_plus = metric == MGK_METRIC_MINKOWSKI ? 0.0 : 1.0 + std::sqrt(d1 > 0.0 ? d1 : 0.0);
+    c.spin_t = a;
+    c.omega_sign = s.time_reversed ? -1.0 : 1.0;
+    return c;
+}
+
+// Device-side copy of everything a kernel needs, in the kernel's scalar T.
+template <class T> struct DevScene {
+    MP<T> m;
+    MP<double> md;     // the same parameters in double (MIXED-mode FP64 attempts)
+    T cam[4];
+    T u_obs[4];
+    T M[4][4];
+    T pix_a, pix_b, pix_c, pix_d;
+    T h0;
+    T disk_r_in, disk_r_out, disk_T_in;
+    T disk_lo, disk_hi;  // chord pre-test window of the disk
+    T escape_r2;
+    T spin_phys, omega_sign;
+    T kerr_a;          // spin used by the disk radius (0 unless Kerr)
+    double r_plus;     // for the FP64 band test
+    double band_pre2;  // (r_plus + band + margin)^2 + a^2: Euclidean pre-check of the band
+    double atol_d, rtol_d, hmax_d, spin_d;
+    T star_inv_r2;
+    T lambda[MGK_MAX_BINS];
+    float xyz_w[3 * MGK_MAX_BINS];
+    uint64_t seed;
+    uint32_t width, height, spp, n_bins, max_steps, disk_on;
+    float inv_spp;
+};
+
+// ------------------------------------------------------------ camera
+// One camera ray: jittered pinhole direction -> local photon direction in
+// the observer's tetrad -> covariant momentum; also c0 = u_obs . p.
+template <Fuse F, class T>
+__device__ __forceinline__ void camera_ray(const DevScene<T>& P, uint64_t ray_id, S7<T>& y, T& pt, T& c0) {
+    uint32_t pixel = uint32_t(ray_id / P.spp), sample = uint32_t(ray_id % P.spp);
+    uint32_t px = pixel % P.width, py = pixel / P.width;
+    T jx = T(rng_unit(P.seed, sample, pixel, 0));
+    T jy = T(rng_unit(P.seed, sample, pixel, 1));
+    T sx = mad<F>(T(px) + jx, P.pix_a, P.pix_b);
+    T sy = mad<F>(T(py) + jy, P.pix_c, P.pix_d);
+    T len = sqrt(mad<F>(sy, sy, mad<F>(sx, sx, T(1))));
+    T nx = sx / len, ny = sy / len, nz = T(-1) / len;
+    T nl = sqrt(mad<F>(nz, nz, mad<F>(ny, ny, nx * nx)));
+    T p[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        T acc = P.M[i][0] * nx;
+        acc = mad<F>(P.M[i][1], ny, acc);
+        acc = mad<F>(P.M[i][2], nz, acc);
+        acc = mad<F>(P.M[i][3], nl, acc);
+        p[i] = acc;
+    }
+    y = S7<T>{P.cam[0], P.cam[1], P.cam[2], P.cam[3], p[0], p[1], p[2]};
+    pt = p[3];
+    c0 = ((P.u_obs[0] * p[0]) + (P.u_obs[1] * p[1]) + (P.u_obs[2] * p[2])) + (P.u_obs[3] * p[3]);
+}
+
+// ----------------------------------------------------------- emitters
+template <class T> __device__ __forceinline__ T redshift_clamp(T z) {
+    if (isnan(z) || isinf(z)) z = T(1e-10);  // relativity_utilities.cuh:62-67
+    return z;
+}
+
+// Circular Keplerian orbit at (x, 0, z), normalised in the integrated frame.
+template <class T>
+__device__ __forceinline__ V4<T> disk_velocity(T xh, T zh, T r, const DevScene<T>& P, int metric) {
+    T omega = P.omega_sign / (r * sqrt(r) + P.spin_phys);
+    T vx = zh * omega, vz = -xh * omega;
+    Sym4<T> g = compute_g<T>(metric, xh, T(0), zh, P.m.spin, P.m.mass_sign);
+    T n = g.tt + T(2) * (g.tx * vx + g.tz * vz) + g.xx * vx * vx + T(2) * g.xz * vx * vz + g.zz * vz * vz;
+    T ut = T(1) / sqrt(-n);
+    return V4<T>{vx * ut, T(0), vz * ut, ut};
+}
+
+// Planck's law in SI units, internal_math.h:2511-2526.
+template <class T> __device__ __forceinline__ T planck(T wavelength_nm, T temperature) {
+    if (temperature <= T(0)) return T(0);
+    const T h = T(6.62607015E-34), c = T(299792458.0), kb = T(1.380649E-23);
+    T wl = wavelength_nm * T(1e-9);
+    T term_0 = h * c;
+    T term_1 = T(2) * term_0 * c;
+    T term_2 = wl * wl * wl * wl * wl;
+    T term_3 = exp(term_0 / (wl * kb * temperature)) - T(1);
+    return (term_1 / term_2) * (T(1) / term_3);
+}
+
+template <class T> __device__ __forceinline__ T clamp_radiance(T v) {
+    return (isnan(v) || isinf(v) || v < T(0)) ? T(0) : v;  // bxdf_utilities.cuh:158-159
+}
+
+// Termination record of a ray.
+template <class T> struct Term {
+    uint32_t cls;
+    T z, r_hit, d0, d1, d2;
+};
+
+// ------------------------------------------------------------ crossings
+// A disk or escape crossing between y0 and y1 is located on the geodesic:
+// secant iterations on the crossing function, each evaluating a fresh RK
+// sub-step of length s from y0 (explicit Euler for Minkowski), at most
+// MGK_REFINE_ITERS + 1 sub-steps.  This removes the chord error of linear
+// interpolation over a long step.
+template <int METRIC, Fuse F, class T>
+__device__ __forceinline__ S7<T> sub_step(const S7<T>& y0, T pt, T s, const MP<T>& m) {
+    S7<T> y1;
+    if constexpr (METRIC == MGK_METRIC_MINKOWSKI) {
+        S7<T> f;
+        rhs_minkowski<T>(y0, pt, f);
+        y1 = axpy<F>(s, f, y0);
+    } else {
+        S7<T> k[6];
+        rkf45_stages<METRIC, F, T>(y0, pt, s, m, y1, k);
+    }
+    return y1;
+}
+
+template <Fuse F, class T> __device__ __forceinline__ T cross_g(int kind, const S7<T>& q, T R2) {
+    return kind == 0 ? q.y : mad<F>(q.z, q.z, mad<F>(q.y, q.y, q.x * q.x)) - R2;
+}
+
+// kind 0: disk plane y = 0; kind 1: escape sphere |x| = R.
+template <int METRIC, Fuse F, class T>
+__device__ __forceinline__ S7<T> refine(int kind, const S7<T>& y0, const S7<T>& y1, T pt, T h, T R2, const MP<T>& m,
+                                        uint32_t& evals) {
+    T g0 = cross_g<F>(kind, y0, R2), g1 = cross_g<F>(kind, y1, R2);
+    T s_prev = h, g_prev = g1;
+    T s = h * (g0 / (g0 - g1));
+    S7<T> ys = sub_step<METRIC, F, T>(y0, pt, s, m);
+    ++evals;
+    T gs = cross_g<F>(kind, ys, R2);
+    for (int it = 0; it < MGK_REFINE_ITERS; ++it) {
+        T den = gs - g_prev;
+        if (gs == T(0) || den == T(0)) break;
+        T s_new = s - gs * (s - s_prev) / den;
+        if (!(s_new > T(0) && s_new < h)) break;
+        T ds = s_new - s;
+        s_prev = s;
+        g_prev = gs;
+        s = s_new;
+        ys = sub_step<METRIC, F, T>(y0, pt, s, m);
+        ++evals;
+        gs = cross_g<F>(kind, ys, R2);
+        if (fabs(ds) <= T(1e-6) * h) break;
+    }
+    return ys;
+}
+
+// Chord pre-test of the disk: the crossing radius estimated linearly lies
+// within a 2 % margin of [r_in, r_out].
+template <Fuse F, class T>
+__device__ __forceinline__ bool disk_candidate(const DevScene<T>& P, const S7<T>& y0, const S7<T>& y1) {
+    if (!P.disk_on) return false;
+    T s0 = y0.y, s1 = y1.y;
+    bool cross = (s0 > T(0)) ? (s1 <= T(0)) : ((s0 < T(0)) ? (s1 >= T(0)) : false);
+    if (!cross) return false;
+    T t = s0 / (s0 - s1);
+    T xh = mad<F>(t, y1.x - y0.x, y0.x);
+    T zh = mad<F>(t, y1.z - y0.z, y0.z);
+    T a = P.kerr_a;
+    T w = mad<F>(zh, zh, xh * xh) - a * a;
+    T rc = sqrt(w > T(0) ? w : T(0));
+    return rc >= P.disk_lo && rc <= P.disk_hi;
+}
+
+template <Fuse F, class T> __device__ __forceinline__ T radius2(const S7<T>& y) {
+    return mad<F>(y.z, y.z, mad<F>(y.y, y.y, y.x * y.x));
+}
+
+// Horizon and step-cap tests of a step without crossing candidates.
+// r_KS >= sqrt(|x|^2 - a^2): positions far outside the capture radius skip
+// the exact horizon test; NaN positions always take it.
+template <int METRIC, Fuse F, class T>
+__device__ __forceinline__ uint32_t plain_terminal(const DevScene<T>& P, const S7<T>& y1, T r2, uint32_t steps) {
+    if constexpr (METRIC != MGK_METRIC_MINKOWSKI) {
+        T q = r2 - P.kerr_a * P.kerr_a;
+        if (!(q > T(4) * P.m.horizon * P.m.horizon) && in_domain<METRIC, T>(y1.x, y1.y, y1.z, P.m))
+            return MGK_RAY_HORIZON;
+    }
+    if (steps >= P.max_steps) return MGK_RAY_STEP_LIMIT;
+    return MGK_RAY_ALIVE;
+}
+
+// All tests after the accepted step y0 -> y1 of length h, in this order:
+// thin disk (located crossing inside [r_in, r_out]), escape radius, horizon,
+// step cap.  y_end receives the located crossing for disk and sky hits.
+template <int METRIC, Fuse F, class T>
+__device__ __forceinline__ Term<T> resolve(const DevScene<T>& P, const S7<T>& y0, const S7<T>& y1, T pt, T h, T c0,
+                                           uint32_t steps, S7<T>& y_end, uint32_t& evals) {
+    Term<T> o{MGK_RAY_ALIVE, T(0), T(0), T(0), T(0), T(0)};
+    y_end = y1;
+    if (disk_candidate<F, T>(P, y0, y1)) {
+        S7<T> ys = refine<METRIC, F, T>(0, y0, y1, pt, h, T(0), P.m, evals);
+        T rh = kerr_schild_r(ys.x, ys.y, ys.z, P.kerr_a);
+        if (rh >= P.disk_r_in && rh <= P.disk_r_out) {
+            V4<T> u = disk_velocity<T>(ys.x, ys.z, rh, P, METRIC);
+            o.cls = MGK_RAY_DISK;
+            o.z = redshift_clamp<T>(c0 / dot4(u, V4<T>{ys.px, ys.py, ys.pz, pt}));
+            o.r_hit = rh;
+            y_end = ys;
+            return o;
+        }
+    }
+    T r2 = radius2<F>(y1);
+    if (r2 >= P.escape_r2) {
+        S7<T> ys = refine<METRIC, F, T>(1, y0, y1, pt, h, P.escape_r2, P.m, evals);
+        T pn = sqrt(mad<F>(ys.pz, ys.pz, mad<F>(ys.py, ys.py, ys.px * ys.px)));
+        o.cls = MGK_RAY_ESCAPED;
+        o.d0 = ys.px / pn; o.d1 = ys.py / pn; o.d2 = ys.pz / pn;
+        o.z = redshift_clamp<T>(c0 / pt);
+        y_end = ys;
+        return o;
+    }
+    o.cls = plain_terminal<METRIC, F, T>(P, y1, r2, steps);
+    return o;
+}
+
+// -------------------------------------------------------------- stars
+// Cube-map grid over the celestial sphere: face (largest |component|), then
+// N x N cells; each cell lists the stars whose disc reaches into it, in
+// ascending star index.
+struct StarGrid {
+    const uint32_t* cell_start;  // 6*N*N + 1
+    const uint32_t* cell_stars;
+    uint32_t n;
+};
+
+MGK_HD uint32_t cube_cell(float dx, float dy, float dz, uint32_t n) {
+    float ax = fabsf(dx), ay = fabsf(dy), az = fabsf(dz);
+    uint32_t face;
+    float u, v, m;
+    if (ax >= ay && ax >= az) { face = dx >= 0.f ? 0u : 1u; m = ax; u = dy; v = dz; }
+    else if (ay >= az) { face = dy >= 0.f ? 2u : 3u; m = ay; u = dx; v = dz; }
+    else { face = dz >= 0.f ? 4u : 5u; m = az; u = dx; v = dy; }
+    float fu = (u / m + 1.0f) * 0.5f * float(n), fv = (v / m + 1.0f) * 0.5f * float(n);
+    int iu = int(fu), iv = int(fv);
+    iu = iu < 0 ? 0 : (iu >= int(n) ? int(n) - 1 : iu);
+    iv = iv < 0 ? 0 : (iv >= int(n) ? int(n) - 1 : iv);
+    return (face * n + uint32_t(iv)) * n + uint32_t(iu);
+}
+
+}  // namespace mgk

@@ -1,0 +1,105 @@
+// Internal interfaces between the C-ABI layer (api.cu) and the kernels
+// (kernels.cu).  Not installed.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/mgk.h"
+
+namespace mgk {
+
+// Device-side counters of one integrator pass (one chunk of rays).
+struct Counters {
+    unsigned long long attempts;
+    unsigned long long steps;
+    unsigned long long wide_attempts;
+    unsigned long long refine_evals;
+    unsigned long long class_count[5];
+    uint32_t queue_head;    // next queue index handed to a warp
+    uint32_t hit_count;     // entries in the hit queue
+    uint32_t refine_count;  // entries in the crossing queue
+    uint32_t resume_count;  // entries in the resume queue
+    uint32_t status;        // 0 = ok; bit 0: a queue overflowed
+    uint32_t pad;
+};
+
+// Hit-queue entry (disk and sky rays; dark rays are not queued).
+template <class T> struct alignas(16) HitEntry {
+    uint32_t ray;  // index within the chunk
+    uint32_t cls;
+    T z, r_hit;
+    T d0, d1, d2;
+    T pad;
+};
+
+// Crossing-queue entry: a step whose end crossed the disk plane near the
+// disk or the escape sphere; the crossing kernel locates it.
+template <class T> struct alignas(16) RefineEntry {
+    T y0[7], y1[7];
+    T pt, h, h_next, c0;
+    uint32_t ray, steps, attempts, wide, evals, pad[3];
+};
+
+// Resume-queue entry: a ray that continues in the tail kernel (MIXED rays
+// inside the FP64 band, and rays whose disk candidate missed the disk).
+template <class T> struct alignas(16) ResumeEntry {
+    T y[7];
+    T pt, h, c0;
+    uint32_t ray, steps, attempts, wide, evals, pad[3];
+};
+
+// Views of the arena for one chunk.
+struct ChunkBuffers {
+    void* qx;              // float4 / double[4] positions
+    void* qp;              // float4 / double[4] momenta (px, py, pz, pt)
+    void* qc;              // float / double c0
+    void* hits;            // HitEntry<T>[n]
+    void* refine;          // RefineEntry<T>[n]
+    void* resume;          // ResumeEntry<T>[n]
+    float* xyz_ray;        // 3 floats per ray
+    Counters* counters;
+};
+
+struct StarGridDev {
+    const uint32_t* cell_start;
+    const uint32_t* cell_stars;
+    uint32_t n;
+};
+
+// Launchers (kernels.cu).  All asynchronous on `stream`.
+cudaError_t launch_generate(const mgk_scene& s, const void* dev_scene, uint64_t first_ray, uint32_t n,
+                            const ChunkBuffers& b, cudaStream_t stream);
+cudaError_t launch_integrate(const mgk_scene& s, const void* dev_scene, uint64_t first_ray, uint32_t n,
+                             const ChunkBuffers& b, mgk_ray_result* results, int sm_count, cudaStream_t stream);
+cudaError_t launch_shade(const mgk_scene& s, const void* dev_scene, uint64_t first_ray, uint32_t n,
+                         const ChunkBuffers& b, const mgk_star* stars, StarGridDev grid, const float* d_w,
+                         float* film_spectral, int sm_count, cudaStream_t stream);
+cudaError_t launch_resolve(const mgk_scene& s, uint64_t first_pixel, uint32_t n_pixels, const float* xyz_ray,
+                           float* film_xyz, cudaStream_t stream);
+cudaError_t launch_fma_probe(uint32_t blocks, uint32_t iters, float* sink, cudaStream_t stream);
+cudaError_t launch_trace_geodesic(const void* jobs, uint32_t n, void* steps, uint32_t* written, cudaStream_t stream);
+
+// Size of DevScene<T> for the scene's precision.
+size_t dev_scene_size(const mgk_scene& s);
+// Fills the device-scene table (host memory, dev_scene_size bytes).
+void fill_dev_scene(const mgk_scene& s, const float* xyz_w, void* out);
+
+// One geodesic of the reference-compatible trace API (host-prepared inputs).
+struct TraceJob {
+    int32_t metric;
+    int32_t n_max;
+    float spin, mass_sign, horizon, spin_abs_gt1, atol, rtol;
+    float length_scale;   // positions are multiplied by it at the end
+    float squared_norm;   // 0 for photons, -1 for massive particles
+    float x0[4];          // dimensionless start position
+    float seed[3][4];     // tetrad seeds of the observer velocity (rotated camera basis)
+    float w[3];           // local proper velocity / c, already sign-flipped if time reversed
+    float dir[3];         // spatial direction / length scale
+    uint32_t n_steps;     // capacity
+    uint32_t step_offset; // first step slot in the shared step buffer
+    uint32_t n_written;   // out
+    uint32_t pad;
+};
+
+}  // namespace mgk

@@ -1,0 +1,844 @@
+// sm_100a kernels of the geodesic path.
+//
+//  k_generate   camera rays -> SoA ray queue (float4 x, float4 p, c0)
+//               [kernel_generate_thin_lens_ray.cu + kernel_generate_initial_conditions.cu]
+//  k_integrate  persistent RKF45 integrator: each warp refills its dead lanes
+//               from the HBM queue in chunks, every lane runs one attempt per
+//               trip, accepted steps go through the termination tests, and
+//               steps that end past a disk or escape crossing are compacted
+//               by warp ballot into the crossing queue; in MIXED mode rays
+//               entering the FP64 band are compacted into the resume queue
+//               [kernel_advance_geodesic.cu + kernel_intersect.cu + kernel_enforce_ray_limits.cu]
+//  k_refine     locates the disk / escape crossings handed over by k_integrate
+//               on the geodesic (secant iterations over RK sub-steps)
+//  k_tail       resumed rays (MIXED rays inside the FP64 band near the horizon,
+//               rays whose disk candidate missed), run one thread per ray
+//  k_shade      one warp per hit: blackbody at the bin wavelengths (one lane per
+//               bin), star lookup, spectral film, XYZ by warp reduction
+//               [kernel_bxdf.cu + kernel_redistribute_radiance.cu]
+//  k_resolve    per-pixel mean over samples [kernel_splat_to_renderbuffer.cu]
+//  k_trace_geodesic  the reference-compatible single-geodesic trace
+//               [host_trace_geodesic.cu:74-117]
+//
+// Compiled with -fmad=false: no multiply-add is fused unless written as mad().
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "dev_physics.cuh"
+#include "dev_scene.cuh"
+#include "internal.h"
+
+namespace mgk {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kIntegrateThreads = 256;
+constexpr uint32_t kChunk = 64;  // queue entries a warp takes per refill
+
+template <int MODE> struct ModeT { using T = float; static constexpr Fuse F = Fuse::Fma; };
+template <> struct ModeT<MGK_PRECISION_REF32> { using T = float; static constexpr Fuse F = Fuse::None; };
+template <> struct ModeT<MGK_PRECISION_F64> { using T = double; static constexpr Fuse F = Fuse::Fma; };
+
+// Queue element loads/stores.
+__device__ __forceinline__ void q_store(void* base, uint32_t i, float a, float b, float c, float d) {
+    reinterpret_cast<float4*>(base)[i] = make_float4(a, b, c, d);
+}
+__device__ __forceinline__ void q_store(void* base, uint32_t i, double a, double b, double c, double d) {
+    double2* p = reinterpret_cast<double2*>(base) + 2 * size_t(i);
+    p[0] = make_double2(a, b);
+    p[1] = make_double2(c, d);
+}
+__device__ __forceinline__ void q_load(const void* base, uint32_t i, float v[4]) {
+    float4 q = reinterpret_cast<const float4*>(base)[i];
+    v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+}
+__device__ __forceinline__ void q_load(const void* base, uint32_t i, double v[4]) {
+    const double2* p = reinterpret_cast<const double2*>(base) + 2 * size_t(i);
+    double2 a = p[0], b = p[1];
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+
+// ---------------------------------------------------------------- generate
+template <int MODE>
+__global__ void __launch_bounds__(256) k_generate(const DevScene<typename ModeT<MODE>::T> P, uint64_t first_ray,
+                                                  uint32_t n, void* qx, void* qp, void* qc) {
+    using T = typename ModeT<MODE>::T;
+    constexpr Fuse F = ModeT<MODE>::F;
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    S7<T> y;
+    T pt, c0;
+    camera_ray<F, T>(P, first_ray + i, y, pt, c0);
+    q_store(qx, i, y.x, y.y, y.z, y.t);
+    q_store(qp, i, y.px, y.py, y.pz, pt);
+    reinterpret_cast<T*>(qc)[i] = c0;
+}
+
+// ------------------------------------------------------------ one attempt
+template <int METRIC, int MODE, class T>
+__device__ __forceinline__ void attempt(const DevScene<T>& P, const S7<T>& y, T pt, T h, S7<T>& y1, T& h_next,
+                                        bool& ok) {
+    constexpr Fuse F = ModeT<MODE>::F;
+    if constexpr (METRIC == MGK_METRIC_MINKOWSKI) {
+        // explicit Euler with a fixed step, metric_minkowski.cuh:49-53
+        S7<T> f;
+        rhs_minkowski<T>(y, pt, f);
+        y1 = axpy<F>(h, f, y);
+        h_next = h;
+        ok = true;
+    } else {
+        S7<T> k[6];
+        rkf45_stages<METRIC, F, T>(y, pt, h, P.m, y1, k);
+        if constexpr (MODE == MGK_PRECISION_REF32) {
+            S7<float> e = rkf45_error<Fuse::None, float>(h, k);
+            float err = rms_error<Fuse::None, float>(e, y, y1, P.m.abs_tol, P.m.rel_tol);
+            float safe = err > 1e-30f ? err : 1e-30f;
+            h_next = propose_h_ref(h, safe, P.m.h_max);
+            ok = safe < 1.0f;
+        } else {
+            double err = wide_error<T>(y, y1, k, h, P.atol_d, P.rtol_d);
+            double safe = err > 1e-30 ? err : 1e-30;
+            h_next = T(propose_h_wide(double(h), safe, P.hmax_d));
+            ok = safe < 1.0;
+        }
+    }
+}
+
+// FP64 attempt of the MIXED mode (state rounded back to float).
+template <int METRIC>
+__device__ __forceinline__ void attempt_wide(const DevScene<float>& P, const S7<float>& y, float pt, float h,
+                                             S7<float>& y1, float& h_next, bool& ok) {
+    S7<double> yd = cvt<double>(y), y1d;
+    S7<double> k[6];
+    rkf45_stages<METRIC, Fuse::Fma, double>(yd, double(pt), double(h), P.md, y1d, k);
+    double err = wide_error<double>(yd, y1d, k, double(h), P.atol_d, P.rtol_d);
+    double safe = err > 1e-30 ? err : 1e-30;
+    h_next = float(propose_h_wide(double(h), safe, P.hmax_d));
+    ok = safe < 1.0;
+    y1 = cvt<float>(y1d);
+}
+
+// True if the KS radius of (x, y, z) lies within MGK_WIDE_BAND of r_plus.
+// r_KS >= sqrt(|x|^2 - a^2): positions clearly outside skip the FP64 radius.
+__device__ __forceinline__ bool in_band(const DevScene<float>& P, float x, float y, float z) {
+    float q = (x * x + y * y + z * z) - P.kerr_a * P.kerr_a;
+    if (q > float(P.band_pre2)) return false;
+    double r = ks_r<double>(double(x), double(y), double(z), P.spin_d);
+    return r - P.r_plus < MGK_WIDE_BAND;
+}
+
+template <class T>
+__device__ __forceinline__ void write_result(mgk_ray_result* res, uint32_t ray, const S7<T>& y, T pt,
+                                             const Term<T>& t, uint32_t steps, uint32_t att, uint32_t wide,
+                                             uint32_t evals) {
+    mgk_ray_result r;
+    r.x[0] = double(y.x); r.x[1] = double(y.y); r.x[2] = double(y.z); r.x[3] = double(y.t);
+    r.p[0] = double(y.px); r.p[1] = double(y.py); r.p[2] = double(y.pz); r.p[3] = double(pt);
+    r.z = double(t.z); r.r_hit = double(t.r_hit);
+    r.dir[0] = double(t.d0); r.dir[1] = double(t.d1); r.dir[2] = double(t.d2);
+    r.cls = t.cls; r.steps = steps; r.attempts = att; r.wide_attempts = wide; r.refine_evals = evals;
+    r.reserved = 0;
+    res[ray] = r;
+}
+
+__device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    return v;
+}
+
+// Pushes the lanes with `flag` set into a queue with one atomic per warp;
+// returns this lane's slot (or ~0u when not flagged or the queue is full).
+__device__ __forceinline__ uint32_t warp_push(bool flag, uint32_t* count, uint32_t cap, uint32_t* status) {
+    unsigned m = __ballot_sync(kFull, flag);
+    if (m == 0) return ~0u;
+    int lane = threadIdx.x & 31;
+    int leader = __ffs(m) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(count, uint32_t(__popc(m)));
+    base = __shfl_sync(kFull, base, leader);
+    if (!flag) return ~0u;
+    uint32_t slot = base + __popc(m & ((1u << lane) - 1u));
+    if (slot >= cap) {
+        atomicOr(status, 1u);
+        return ~0u;
+    }
+    return slot;
+}
+
+// Single-thread queue push (kernels whose threads are not warp-synchronous).
+__device__ __forceinline__ uint32_t thread_push(uint32_t* count, uint32_t cap, uint32_t* status) {
+    uint32_t slot = atomicAdd(count, 1u);
+    if (slot >= cap) {
+        atomicOr(status, 1u);
+        return ~0u;
+    }
+    return slot;
+}
+
+template <class T>
+__device__ __forceinline__ void push_hit(HitEntry<T>* hits, uint32_t slot, uint32_t ray, const Term<T>& t) {
+    HitEntry<T> e;
+    e.ray = ray; e.cls = t.cls; e.z = t.z; e.r_hit = t.r_hit;
+    e.d0 = t.d0; e.d1 = t.d1; e.d2 = t.d2; e.pad = T(0);
+    hits[slot] = e;
+}
+
+template <class T>
+__device__ __forceinline__ void store_resume(ResumeEntry<T>* q, uint32_t slot, const S7<T>& y, T pt, T h, T c0,
+                                             uint32_t ray, uint32_t steps, uint32_t att, uint32_t wide,
+                                             uint32_t evals) {
+    ResumeEntry<T> e;
+    e.y[0] = y.x; e.y[1] = y.y; e.y[2] = y.z; e.y[3] = y.t; e.y[4] = y.px; e.y[5] = y.py; e.y[6] = y.pz;
+    e.pt = pt; e.h = h; e.c0 = c0;
+    e.ray = ray; e.steps = steps; e.attempts = att; e.wide = wide; e.evals = evals;
+    e.pad[0] = e.pad[1] = e.pad[2] = 0;
+    q[slot] = e;
+}
+
+template <class T> __device__ __forceinline__ S7<T> s7(const T* v) {
+    return S7<T>{v[0], v[1], v[2], v[3], v[4], v[5], v[6]};
+}
+
+// -------------------------------------------------------------- integrate
+// Persistent: every warp loops until the queue is drained.  A lane whose
+// step ends near the disk plane crossing or beyond the escape radius hands
+// the step to the crossing queue; in MIXED mode a lane entering the FP64
+// band hands its ray to the resume queue.  Both pushes are warp-ballot
+// compactions with one atomic per warp.
+template <int METRIC, int MODE>
+__global__ void __launch_bounds__(kIntegrateThreads, 2)
+    k_integrate(const DevScene<typename ModeT<MODE>::T> P, uint32_t nq, const void* __restrict__ qx,
+                const void* __restrict__ qp, const void* __restrict__ qc,
+                RefineEntry<typename ModeT<MODE>::T>* refq, ResumeEntry<typename ModeT<MODE>::T>* resq,
+                mgk_ray_result* res, Counters* cnt) {
+    using T = typename ModeT<MODE>::T;
+    constexpr Fuse F = ModeT<MODE>::F;
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+
+    bool alive = false;
+    S7<T> y{};
+    T pt = 0, c0 = 0, h = 0;
+    uint32_t ray = 0, steps = 0, tries = 0, att = 0;
+    uint32_t cbeg = 0, cend = 0;
+    bool drained = false;
+    unsigned long long n_att = 0, n_steps = 0;
+    uint32_t n_cls[5] = {0, 0, 0, 0, 0};
+
+    for (;;) {
+        // ---- refill dead lanes from the queue (warp-uniform control flow)
+        unsigned dead = __ballot_sync(kFull, !alive);
+        bool to_band = false;
+        if (dead != 0u && !(drained && cbeg == cend)) {
+            uint32_t need = __popc(dead);
+            uint32_t rem = cend - cbeg;
+            uint32_t nb = 0, ne = 0;
+            if (need > rem && !drained) {
+                uint32_t got = 0;
+                if (lane == 0) got = atomicAdd(&cnt->queue_head, kChunk);
+                got = __shfl_sync(kFull, got, 0);
+                if (got >= nq) {
+                    drained = true;
+                } else {
+                    nb = got;
+                    ne = min(got + kChunk, nq);
+                    if (ne == nq) drained = true;
+                }
+            }
+            if (!alive) {
+                uint32_t rank = __popc(dead & lt);
+                uint32_t idx = ~0u;
+                if (rank < rem) idx = cbeg + rank;
+                else if (rank - rem < ne - nb) idx = nb + (rank - rem);
+                if (idx != ~0u) {
+                    T a[4], b[4];
+                    q_load(qx, idx, a);
+                    q_load(qp, idx, b);
+                    y = S7<T>{a[0], a[1], a[2], a[3], b[0], b[1], b[2]};
+                    pt = b[3];
+                    c0 = reinterpret_cast<const T*>(qc)[idx];
+                    h = P.h0;
+                    ray = idx;
+                    steps = 0; tries = 0; att = 0;
+                    alive = true;
+                    if constexpr (MODE == MGK_PRECISION_MIXED && METRIC != MGK_METRIC_MINKOWSKI)
+                        to_band = in_band(P, y.x, y.y, y.z);
+                }
+            }
+            uint32_t used_old = min(need, rem);
+            if (ne > nb) {
+                uint32_t used_new = min(need - used_old, ne - nb);
+                cbeg = nb + used_new;
+                cend = ne;
+            } else {
+                cbeg += used_old;
+            }
+        }
+        if (__ballot_sync(kFull, alive) == 0u) break;
+
+        // ---- one RKF45 attempt per live lane
+        uint32_t cls = MGK_RAY_ALIVE;
+        bool cross = false;
+        S7<T> y0 = y;
+        T h_used = h;
+        if (alive && !to_band) {
+            S7<T> y1;
+            T hn;
+            bool ok;
+            attempt<METRIC, MODE, T>(P, y, pt, h, y1, hn, ok);
+            ++att; ++tries; ++n_att;
+            h = hn;
+            if (ok || tries >= P.m.n_max) {
+                tries = 0;
+                ++steps; ++n_steps;
+                y = y1;
+                T r2 = radius2<F>(y1);
+                cross = disk_candidate<F, T>(P, y0, y1) || r2 >= P.escape_r2;
+                if (!cross) {
+                    cls = plain_terminal<METRIC, F, T>(P, y1, r2, steps);
+                    if constexpr (MODE == MGK_PRECISION_MIXED && METRIC != MGK_METRIC_MINKOWSKI) {
+                        if (cls == MGK_RAY_ALIVE) to_band = in_band(P, y.x, y.y, y.z);
+                    }
+                }
+            }
+        }
+
+        // ---- compaction of the hand-offs
+        uint32_t slot = warp_push(cross, &cnt->refine_count, nq, &cnt->status);
+        if (slot != ~0u) {
+            RefineEntry<T> e;
+            e.y0[0] = y0.x; e.y0[1] = y0.y; e.y0[2] = y0.z; e.y0[3] = y0.t;
+            e.y0[4] = y0.px; e.y0[5] = y0.py; e.y0[6] = y0.pz;
+            e.y1[0] = y.x; e.y1[1] = y.y; e.y1[2] = y.z; e.y1[3] = y.t;
+            e.y1[4] = y.px; e.y1[5] = y.py; e.y1[6] = y.pz;
+            e.pt = pt; e.h = h_used; e.h_next = h; e.c0 = c0;
+            e.ray = ray; e.steps = steps; e.attempts = att;
+            e.wide = MODE == MGK_PRECISION_F64 ? att : 0u;
+            e.evals = 0; e.pad[0] = e.pad[1] = e.pad[2] = 0;
+            refq[slot] = e;
+        }
+        if constexpr (MODE == MGK_PRECISION_MIXED) {
+            uint32_t bslot = warp_push(to_band, &cnt->resume_count, nq, &cnt->status);
+            if (bslot != ~0u) store_resume<T>(resq, bslot, y, pt, h, c0, ray, steps, att, 0u, 0u);
+        }
+        if (cls != MGK_RAY_ALIVE) {
+            if (res) {
+                Term<T> t{cls, T(0), T(0), T(0), T(0), T(0)};
+                write_result<T>(res, ray, y, pt, t, steps, att, MODE == MGK_PRECISION_F64 ? att : 0u, 0u);
+            }
+            ++n_cls[cls];
+        }
+        if (cls != MGK_RAY_ALIVE || cross || to_band) alive = false;
+    }
+
+    // ---- counters: one atomic per warp and counter
+    n_att = warp_sum(n_att);
+    n_steps = warp_sum(n_steps);
+    unsigned long long c[5];
+#pragma unroll
+    for (int i = 0; i < 5; ++i) c[i] = warp_sum((unsigned long long)n_cls[i]);
+    if (lane == 0) {
+        atomicAdd(&cnt->attempts, n_att);
+        atomicAdd(&cnt->steps, n_steps);
+        if (MODE == MGK_PRECISION_F64) atomicAdd(&cnt->wide_attempts, n_att);
+#pragma unroll
+        for (int i = 1; i < 5; ++i)
+            if (c[i]) atomicAdd(&cnt->class_count[i], c[i]);
+    }
+}
+
+// -------------------------------------------------------------- crossings
+// One thread per handed-off step: locate the disk / escape crossing, then
+// emit the hit, or send the ray on to the tail kernel when the disk
+// candidate missed and nothing else ended it.
+template <int METRIC, int MODE>
+__global__ void __launch_bounds__(128) k_refine(const DevScene<typename ModeT<MODE>::T> P,
+                                                const RefineEntry<typename ModeT<MODE>::T>* __restrict__ refq,
+                                                uint32_t cap, HitEntry<typename ModeT<MODE>::T>* hits,
+                                                ResumeEntry<typename ModeT<MODE>::T>* resq, mgk_ray_result* res,
+                                                Counters* cnt) {
+    using T = typename ModeT<MODE>::T;
+    constexpr Fuse F = ModeT<MODE>::F;
+    const uint32_t n = min(cnt->refine_count, cap);
+    unsigned long long n_evals = 0;
+    uint32_t n_cls[5] = {0, 0, 0, 0, 0};
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    // warp-uniform trip count so the queue pushes can use warp ballots
+    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += stride) {
+        const uint32_t i = base + lane;
+        const bool valid = i < n;
+        Term<T> t{MGK_RAY_ALIVE, T(0), T(0), T(0), T(0), T(0)};
+        RefineEntry<T> e;
+        S7<T> y1{}, ye{};
+        uint32_t evals = 0;
+        if (valid) {
+            e = refq[i];
+            S7<T> y0 = s7(e.y0);
+            y1 = s7(e.y1);
+            evals = e.evals;
+            t = resolve<METRIC, F, T>(P, y0, y1, e.pt, e.h, e.c0, e.steps, ye, evals);
+            n_evals += evals - e.evals;
+        }
+        uint32_t rslot = warp_push(valid && t.cls == MGK_RAY_ALIVE, &cnt->resume_count, cap, &cnt->status);
+        if (rslot != ~0u)
+            store_resume<T>(resq, rslot, y1, e.pt, e.h_next, e.c0, e.ray, e.steps, e.attempts, e.wide, evals);
+        bool lit = valid && (t.cls == MGK_RAY_DISK || t.cls == MGK_RAY_ESCAPED);
+        uint32_t hslot = warp_push(lit, &cnt->hit_count, cap, &cnt->status);
+        if (hslot != ~0u) push_hit<T>(hits, hslot, e.ray, t);
+        if (valid && t.cls != MGK_RAY_ALIVE) {
+            if (res) write_result<T>(res, e.ray, ye, e.pt, t, e.steps, e.attempts, e.wide, evals);
+            ++n_cls[t.cls];
+        }
+    }
+    if (n_evals) atomicAdd(&cnt->refine_evals, n_evals);
+    for (int i = 1; i < 5; ++i)
+        if (n_cls[i]) atomicAdd(&cnt->class_count[i], (unsigned long long)n_cls[i]);
+}
+
+// ------------------------------------------------------------------- tail
+// One thread per resumed ray, run sequentially to termination.  MIXED mode:
+// FP64 attempts while within MGK_WIDE_BAND of r_plus, FP32 otherwise.
+template <int METRIC, int MODE>
+__global__ void __launch_bounds__(128) k_tail(const DevScene<typename ModeT<MODE>::T> P,
+                                              const ResumeEntry<typename ModeT<MODE>::T>* __restrict__ resq,
+                                              uint32_t cap, HitEntry<typename ModeT<MODE>::T>* hits,
+                                              mgk_ray_result* res, Counters* cnt) {
+    using T = typename ModeT<MODE>::T;
+    constexpr Fuse F = ModeT<MODE>::F;
+    const uint32_t n = min(cnt->resume_count, cap);
+    unsigned long long n_att = 0, n_steps = 0, n_wide = 0, n_evals = 0;
+    uint32_t n_cls[5] = {0, 0, 0, 0, 0};
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += stride) {
+        const uint32_t i = base + lane;
+        const bool valid = i < n;
+        Term<T> t{MGK_RAY_ALIVE, T(0), T(0), T(0), T(0), T(0)};
+        ResumeEntry<T> e;
+        S7<T> y{};
+        uint32_t steps = 0, att = 0, wide = 0, evals = 0;
+        if (valid) {
+            e = resq[i];
+            y = s7(e.y);
+            const T pt = e.pt, c0 = e.c0;
+            T h = e.h;
+            steps = e.steps; att = e.attempts; wide = e.wide; evals = e.evals;
+            uint32_t tries = 0;
+            double r_cur = 0.0;
+            if constexpr (MODE == MGK_PRECISION_MIXED)
+                r_cur = ks_r<double>(double(y.x), double(y.y), double(y.z), P.spin_d);
+            for (;;) {
+                S7<T> y1;
+                T hn;
+                bool ok;
+                const T h_used = h;
+                bool w = false;
+                if constexpr (MODE == MGK_PRECISION_MIXED && METRIC != MGK_METRIC_MINKOWSKI) {
+                    w = r_cur - P.r_plus < MGK_WIDE_BAND;
+                    if (w) attempt_wide<METRIC>(P, y, pt, h, y1, hn, ok);
+                    else attempt<METRIC, MODE, T>(P, y, pt, h, y1, hn, ok);
+                } else {
+                    attempt<METRIC, MODE, T>(P, y, pt, h, y1, hn, ok);
+                }
+                ++att; ++tries; ++n_att;
+                if (w || MODE == MGK_PRECISION_F64) { ++wide; ++n_wide; }
+                h = hn;
+                if (!ok && tries < P.m.n_max) continue;
+                tries = 0;
+                ++steps; ++n_steps;
+                S7<T> ye;
+                uint32_t ev0 = evals;
+                t = resolve<METRIC, F, T>(P, y, y1, pt, h_used, c0, steps, ye, evals);
+                n_evals += evals - ev0;
+                y = ye;
+                if (t.cls != MGK_RAY_ALIVE) break;
+                if constexpr (MODE == MGK_PRECISION_MIXED)
+                    r_cur = ks_r<double>(double(y.x), double(y.y), double(y.z), P.spin_d);
+            }
+        }
+        bool lit = valid && (t.cls == MGK_RAY_DISK || t.cls == MGK_RAY_ESCAPED);
+        uint32_t hslot = warp_push(lit, &cnt->hit_count, cap, &cnt->status);
+        if (hslot != ~0u) push_hit<T>(hits, hslot, e.ray, t);
+        if (valid) {
+            if (res) write_result<T>(res, e.ray, y, e.pt, t, steps, att, wide, evals);
+            ++n_cls[t.cls];
+        }
+    }
+    if (n_att) {
+        atomicAdd(&cnt->attempts, n_att);
+        atomicAdd(&cnt->steps, n_steps);
+        atomicAdd(&cnt->wide_attempts, n_wide);
+    }
+    if (n_evals) atomicAdd(&cnt->refine_evals, n_evals);
+    for (int i = 1; i < 5; ++i)
+        if (n_cls[i]) atomicAdd(&cnt->class_count[i], (unsigned long long)n_cls[i]);
+}
+
+// ------------------------------------------------------------------ shade
+// One warp per hit; lane k evaluates bins k and k + 32.
+template <class T>
+__global__ void __launch_bounds__(256) k_shade(const DevScene<T> P, const HitEntry<T>* __restrict__ hits,
+                                               uint32_t cap, const Counters* cnt, const mgk_star* __restrict__ stars,
+                                               StarGridDev grid, const float* __restrict__ d_w,
+                                               float* __restrict__ xyz_ray, float* __restrict__ film_spec,
+                                               uint64_t first_ray) {
+    __shared__ float sw[3 * MGK_MAX_BINS];
+    for (int i = threadIdx.x; i < 3 * MGK_MAX_BINS; i += blockDim.x) sw[i] = d_w ? d_w[i < 3 * int(P.n_bins) ? i : 0] : P.xyz_w[i];
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const uint32_t n = min(cnt->hit_count, cap);
+    const uint32_t nb = P.n_bins;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    const bool has0 = uint32_t(lane) < nb, has1 = uint32_t(lane) + 32u < nb;
+    const T lam0 = has0 ? P.lambda[lane] : T(0), lam1 = has1 ? P.lambda[lane + 32] : T(0);
+    for (uint32_t e = warp; e < n; e += nwarps) {
+        const HitEntry<T> h = hits[e];
+        const T z = h.z, z2 = z * z, z5 = z2 * z2 * z;
+        T s0 = T(0), s1 = T(0);
+        if (h.cls == MGK_RAY_DISK) {
+            T temp = P.disk_T_in * T(pow(double(h.r_hit / P.disk_r_in), -0.75));
+            if (has0) s0 = clamp_radiance<T>(planck<T>(z * lam0, temp) * z5);
+            if (has1) s1 = clamp_radiance<T>(planck<T>(z * lam1, temp) * z5);
+        } else if (grid.n != 0u) {
+            uint32_t cell = cube_cell(float(h.d0), float(h.d1), float(h.d2), grid.n);
+            uint32_t j0 = grid.cell_start[cell], j1 = grid.cell_start[cell + 1];
+            for (uint32_t j = j0; j < j1; ++j) {
+                const mgk_star st = stars[grid.cell_stars[j]];
+                T dx = h.d0 - T(st.dir[0]), dy = h.d1 - T(st.dir[1]), dz = h.d2 - T(st.dir[2]);
+                T q = mad<Fuse::Fma>(dz, dz, mad<Fuse::Fma>(dy, dy, dx * dx)) * P.star_inv_r2;
+                if (q >= T(1)) continue;
+                T kern = (T(1) - q) * (T(1) - q);
+                T amp = T(st.amplitude) * kern;
+                if (has0) s0 += clamp_radiance<T>(amp * planck<T>(z * lam0, T(st.temperature)) * z5);
+                if (has1) s1 += clamp_radiance<T>(amp * planck<T>(z * lam1, T(st.temperature)) * z5);
+            }
+        }
+        float f0 = float(s0), f1 = float(s1);
+        float X = 0.f, Y = 0.f, Z = 0.f;
+        if (has0) { X = f0 * sw[3 * lane]; Y = f0 * sw[3 * lane + 1]; Z = f0 * sw[3 * lane + 2]; }
+        if (has1) {
+            X = __fmaf_rn(f1, sw[3 * (lane + 32)], X);
+            Y = __fmaf_rn(f1, sw[3 * (lane + 32) + 1], Y);
+            Z = __fmaf_rn(f1, sw[3 * (lane + 32) + 2], Z);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            X += __shfl_xor_sync(kFull, X, o);
+            Y += __shfl_xor_sync(kFull, Y, o);
+            Z += __shfl_xor_sync(kFull, Z, o);
+        }
+        if (lane == 0) {
+            xyz_ray[3 * size_t(h.ray) + 0] = X;
+            xyz_ray[3 * size_t(h.ray) + 1] = Y;
+            xyz_ray[3 * size_t(h.ray) + 2] = Z;
+        }
+        if (film_spec) {
+            uint64_t pixel = (first_ray + h.ray) / P.spp;
+            if (has0) atomicAdd(&film_spec[pixel * nb + lane], f0 * P.inv_spp);
+            if (has1) atomicAdd(&film_spec[pixel * nb + lane + 32], f1 * P.inv_spp);
+        }
+    }
+}
+
+// ---------------------------------------------------------------- resolve
+__global__ void __launch_bounds__(256) k_resolve(uint64_t first_pixel, uint32_t n_pixels, uint32_t spp,
+                                                 const float* __restrict__ xyz_ray, float* __restrict__ film) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_pixels) return;
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+    const float* src = xyz_ray + 3 * size_t(i) * spp;
+    for (uint32_t s = 0; s < spp; ++s) {
+        a0 += src[3 * s + 0];
+        a1 += src[3 * s + 1];
+        a2 += src[3 * s + 2];
+    }
+    float fs = float(spp);
+    float* dst = film + 3 * (first_pixel + i);
+    dst[0] = a0 / fs;
+    dst[1] = a1 / fs;
+    dst[2] = a2 / fs;
+}
+
+// --------------------------------------------------------- trace_geodesic
+// host_trace_geodesic.cu:13-130 on the GPU, REF32 arithmetic, one thread per
+// geodesic; the observer set-up that needs sin/cos is done on the host.
+__global__ void __launch_bounds__(64) k_trace_geodesic(const TraceJob* __restrict__ jobs, uint32_t n,
+                                                       magik_trace_geodesic_step_t* steps_all, uint32_t* written) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const TraceJob J = jobs[i];
+    magik_trace_geodesic_step_t* st = steps_all + J.step_offset;
+    MP<float> m{};
+    m.spin = J.spin; m.mass_sign = J.mass_sign; m.horizon = J.horizon; m.spin_abs_gt1 = J.spin_abs_gt1;
+    m.h_max = 1000.0f; m.abs_tol = J.atol; m.rel_tol = J.rtol; m.n_max = uint32_t(J.n_max);
+    const int metric = J.metric;
+    V4<float> x0{J.x0[0], J.x0[1], J.x0[2], J.x0[3]};
+    Sym4<float> g = compute_g<float>(metric, x0.x, x0.y, x0.z, J.spin, J.mass_sign);
+    V4<float> u_ref = reference_observer<float>(metric, x0.x, x0.y, x0.z, J.spin, J.mass_sign);
+    V4<float> X{J.seed[0][0], J.seed[0][1], J.seed[0][2], J.seed[0][3]};
+    V4<float> Yv{J.seed[1][0], J.seed[1][1], J.seed[1][2], J.seed[1][3]};
+    V4<float> Z{J.seed[2][0], J.seed[2][1], J.seed[2][2], J.seed[2][3]};
+    Tetrad<float> e = build_tetrad<float>(g, X, Yv, Z, u_ref);
+    float w2 = J.w[0] * J.w[0] + J.w[1] * J.w[1] + J.w[2] * J.w[2];
+    V4<float> u = local_to_global<float>(e, V4<float>{J.w[0], J.w[1], J.w[2], sqrtf(w2 - -1.0f)});
+    Tetrad<float> e2 = build_tetrad<float>(g, V4<float>{1, 0, 0, 0}, V4<float>{0, 1, 0, 0}, V4<float>{0, 0, 1, 0}, u);
+    float d2 = J.dir[0] * J.dir[0] + J.dir[1] * J.dir[1] + J.dir[2] * J.dir[2];
+    V4<float> p_up = local_to_global<float>(e2, V4<float>{J.dir[0], J.dir[1], J.dir[2], sqrtf(d2 - J.squared_norm)});
+    V4<float> p0 = contract<float>(g, p_up);
+
+    S7<float> y{x0.x, x0.y, x0.z, x0.t, p0.x, p0.y, p0.z};
+    float pt = p0.t;
+    const float contraction = dot4<float>(u, p0);
+    float h = metric == MGK_METRIC_MINKOWSKI ? 1000.0f : 1.0f;
+    float aff = 0.0f;
+    auto put = [&](uint32_t k, const S7<float>& s, const S7<float>& ds) {
+        magik_trace_geodesic_step_t o;
+        o.four_position[0] = s.x; o.four_position[1] = s.y; o.four_position[2] = s.z; o.four_position[3] = s.t;
+        o.four_momentum[0] = s.px; o.four_momentum[1] = s.py; o.four_momentum[2] = s.pz; o.four_momentum[3] = pt;
+        o.moment_derivative[0] = ds.px; o.moment_derivative[1] = ds.py; o.moment_derivative[2] = ds.pz;
+        o.moment_derivative[3] = 0.0f;
+        o.four_vector_contraction = contraction;
+        o.affine_parameter = aff;
+        o.delta_affine_parameter = h;
+        st[k] = o;
+    };
+    auto rhs_any = [&](const S7<float>& s, S7<float>& o) {
+        if (metric == MGK_METRIC_KERR) rhs_kerr<Fuse::None, float>(s, pt, m.spin, o);
+        else if (metric == MGK_METRIC_SCHWARZSCHILD) rhs_schwarzschild<Fuse::None, float>(s, pt, m.mass_sign, o);
+        else rhs_minkowski<float>(s, pt, o);
+    };
+    S7<float> ys;
+    rhs_any(y, ys);
+    put(0, y, ys);
+    uint32_t nw = 1;
+    while (nw < J.n_steps) {
+        S7<float> y1;
+        float h_taken = h;
+        if (metric == MGK_METRIC_MINKOWSKI) {
+            S7<float> f;
+            rhs_minkowski<float>(y, pt, f);
+            y1 = axpy<Fuse::None>(h, f, y);
+        } else {
+            float temp_h = h;
+            for (uint32_t a = 0; a < m.n_max; ++a) {
+                S7<float> k[6];
+                if (metric == MGK_METRIC_KERR) rkf45_stages<MGK_METRIC_KERR, Fuse::None, float>(y, pt, temp_h, m, y1, k);
+                else rkf45_stages<MGK_METRIC_SCHWARZSCHILD, Fuse::None, float>(y, pt, temp_h, m, y1, k);
+                S7<float> er = rkf45_error<Fuse::None, float>(temp_h, k);
+                float err = rms_error<Fuse::None, float>(er, y, y1, m.abs_tol, m.rel_tol);
+                float safe = err > 1e-30f ? err : 1e-30f;
+                float hn = propose_h_ref(temp_h, safe, m.h_max);
+                h_taken = temp_h;
+                temp_h = hn;
+                if (safe < 1.0f) break;
+            }
+            h = temp_h;
+        }
+        y = y1;
+        rhs_any(y, ys);
+        aff = aff + h_taken;
+        put(nw, y, ys);
+        ++nw;
+        bool cap;
+        if (metric == MGK_METRIC_KERR) cap = in_domain<MGK_METRIC_KERR, float>(y.x, y.y, y.z, m);
+        else if (metric == MGK_METRIC_SCHWARZSCHILD) cap = in_domain<MGK_METRIC_SCHWARZSCHILD, float>(y.x, y.y, y.z, m);
+        else cap = false;
+        if (cap) break;
+    }
+    for (uint32_t k = 0; k < nw; ++k)
+        for (int c = 0; c < 4; ++c) st[k].four_position[c] *= J.length_scale;
+    written[i] = nw;
+}
+
+// --------------------------------------------------------------- FP32 probe
+// Peak FP32 throughput: 8 independent FMA chains per thread, enough warps to
+// hide the pipeline latency.  Each loop trip is 8 FMA = 16 FLOP per thread.
+__global__ void __launch_bounds__(256) k_fma_probe(uint32_t iters, float seed, float* sink) {
+    float a0 = seed + threadIdx.x, a1 = a0 + 1.f, a2 = a0 + 2.f, a3 = a0 + 3.f;
+    float a4 = a0 + 4.f, a5 = a0 + 5.f, a6 = a0 + 6.f, a7 = a0 + 7.f;
+    const float m = 0.999999f, c = 1e-7f;
+    for (uint32_t i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            a0 = __fmaf_rn(a0, m, c); a1 = __fmaf_rn(a1, m, c); a2 = __fmaf_rn(a2, m, c); a3 = __fmaf_rn(a3, m, c);
+            a4 = __fmaf_rn(a4, m, c); a5 = __fmaf_rn(a5, m, c); a6 = __fmaf_rn(a6, m, c); a7 = __fmaf_rn(a7, m, c);
+        }
+    }
+    float r = ((a0 + a1) + (a2 + a3)) + ((a4 + a5) + (a6 + a7));
+    if (r == 12345.f) sink[threadIdx.x] = r;
+}
+
+cudaError_t launch_fma_probe(uint32_t blocks, uint32_t iters, float* sink, cudaStream_t st) {
+    k_fma_probe<<<blocks, 256, 0, st>>>(iters, 1.0f, sink);
+    return cudaGetLastError();
+}
+
+// =============================================================== launchers
+template <class T> static const DevScene<T>& ds(const void* p) { return *reinterpret_cast<const DevScene<T>*>(p); }
+
+template <int MODE>
+static cudaError_t gen_t(const void* dev_scene, uint64_t first, uint32_t n, const ChunkBuffers& b, cudaStream_t st) {
+    using T = typename ModeT<MODE>::T;
+    k_generate<MODE><<<(n + 255) / 256, 256, 0, st>>>(ds<T>(dev_scene), first, n, b.qx, b.qp, b.qc);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_generate(const mgk_scene& s, const void* dev_scene, uint64_t first, uint32_t n,
+                            const ChunkBuffers& b, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    switch (s.precision) {
+        case MGK_PRECISION_REF32: return gen_t<MGK_PRECISION_REF32>(dev_scene, first, n, b, st);
+        case MGK_PRECISION_MIXED: return gen_t<MGK_PRECISION_MIXED>(dev_scene, first, n, b, st);
+        default: return gen_t<MGK_PRECISION_F64>(dev_scene, first, n, b, st);
+    }
+}
+
+template <int METRIC, int MODE>
+static cudaError_t integ_t(const void* dsc, uint32_t n, const ChunkBuffers& b, mgk_ray_result* res, int sms,
+                           cudaStream_t st) {
+    using T = typename ModeT<MODE>::T;
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_integrate<METRIC, MODE>, kIntegrateThreads, 0);
+    if (per_sm < 1) per_sm = 1;
+    uint32_t blocks = uint32_t(sms * per_sm);
+    uint32_t need = (n + kIntegrateThreads - 1) / kIntegrateThreads;
+    if (blocks > need) blocks = need;
+    auto* refq = reinterpret_cast<RefineEntry<T>*>(b.refine);
+    auto* resq = reinterpret_cast<ResumeEntry<T>*>(b.resume);
+    auto* hits = reinterpret_cast<HitEntry<T>*>(b.hits);
+    k_integrate<METRIC, MODE><<<blocks, kIntegrateThreads, 0, st>>>(ds<T>(dsc), n, b.qx, b.qp, b.qc, refq, resq, res,
+                                                                   b.counters);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_refine<METRIC, MODE><<<sms * 8, 128, 0, st>>>(ds<T>(dsc), refq, n, hits, resq, res, b.counters);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_tail<METRIC, MODE><<<sms * 2, 128, 0, st>>>(ds<T>(dsc), resq, n, hits, res, b.counters);
+    return cudaGetLastError();
+}
+
+template <int MODE>
+static cudaError_t integ_m(int metric, const void* dsc, uint32_t n, const ChunkBuffers& b, mgk_ray_result* res,
+                           int sms, cudaStream_t st) {
+    switch (metric) {
+        case MGK_METRIC_KERR: return integ_t<MGK_METRIC_KERR, MODE>(dsc, n, b, res, sms, st);
+        case MGK_METRIC_SCHWARZSCHILD: return integ_t<MGK_METRIC_SCHWARZSCHILD, MODE>(dsc, n, b, res, sms, st);
+        default: return integ_t<MGK_METRIC_MINKOWSKI, MODE>(dsc, n, b, res, sms, st);
+    }
+}
+
+cudaError_t launch_integrate(const mgk_scene& s, const void* dsc, uint64_t, uint32_t n, const ChunkBuffers& b,
+                             mgk_ray_result* res, int sms, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    switch (s.precision) {
+        case MGK_PRECISION_REF32: return integ_m<MGK_PRECISION_REF32>(s.metric, dsc, n, b, res, sms, st);
+        case MGK_PRECISION_MIXED: return integ_m<MGK_PRECISION_MIXED>(s.metric, dsc, n, b, res, sms, st);
+        default: return integ_m<MGK_PRECISION_F64>(s.metric, dsc, n, b, res, sms, st);
+    }
+}
+
+cudaError_t launch_shade(const mgk_scene& s, const void* dsc, uint64_t first, uint32_t n, const ChunkBuffers& b,
+                         const mgk_star* stars, StarGridDev grid, const float* d_w, float* film_spec, int sms,
+                         cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    uint32_t blocks = uint32_t(sms) * 8u;
+    if (s.precision == MGK_PRECISION_F64)
+        k_shade<double><<<blocks, 256, 0, st>>>(ds<double>(dsc), reinterpret_cast<const HitEntry<double>*>(b.hits),
+                                                n, b.counters, stars, grid, d_w, b.xyz_ray, film_spec, first);
+    else
+        k_shade<float><<<blocks, 256, 0, st>>>(ds<float>(dsc), reinterpret_cast<const HitEntry<float>*>(b.hits), n,
+                                               b.counters, stars, grid, d_w, b.xyz_ray, film_spec, first);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_resolve(const mgk_scene& s, uint64_t first_pixel, uint32_t n_pixels, const float* xyz_ray,
+                           float* film, cudaStream_t st) {
+    if (n_pixels == 0) return cudaSuccess;
+    k_resolve<<<(n_pixels + 255) / 256, 256, 0, st>>>(first_pixel, n_pixels, s.spp, xyz_ray, film);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_trace_geodesic(const void* jobs, uint32_t n, void* steps, uint32_t* written, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    k_trace_geodesic<<<(n + 63) / 64, 64, 0, st>>>(reinterpret_cast<const TraceJob*>(jobs), n,
+                                                   reinterpret_cast<magik_trace_geodesic_step_t*>(steps), written);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------ device scene table
+size_t dev_scene_size(const mgk_scene& s) {
+    return s.precision == MGK_PRECISION_F64 ? sizeof(DevScene<double>) : sizeof(DevScene<float>);
+}
+
+template <class T> static void fill_t(const mgk_scene& s, const float* xyz_w, DevScene<T>* P) {
+    SceneConsts c = scene_consts(s);
+    *P = DevScene<T>{};
+    const double a_t = s.time_reversed ? -s.spin : s.spin;
+    const bool kerr = s.metric == MGK_METRIC_KERR;
+    P->m.spin = T(kerr ? a_t : 0.0);
+    P->m.mass_sign = T(s.mass_sign < 0 ? -1.0 : 1.0);
+    // the reference's capture radius, evaluated in T like in_domain does
+    if (kerr) {
+        T a = T(a_t);
+        P->m.horizon = (T(1) + std::sqrt(T(1) - a * a)) * T(s.horizon_scalar);
+        P->m.spin_abs_gt1 = (a > T(1) || a < T(-1)) ? T(1) : T(0);
+    } else {
+        P->m.horizon = T(2) * T(s.horizon_scalar);
+        P->m.spin_abs_gt1 = T(0);
+    }
+    P->m.h_max = T(s.h_max);
+    P->m.abs_tol = T(s.abs_tol);
+    P->m.rel_tol = T(s.rel_tol);
+    P->m.n_max = s.n_max_substep;
+    P->md.spin = kerr ? a_t : 0.0;
+    P->md.mass_sign = s.mass_sign < 0 ? -1.0 : 1.0;
+    P->md.horizon = double(P->m.horizon);
+    P->md.spin_abs_gt1 = double(P->m.spin_abs_gt1);
+    P->md.h_max = s.h_max;
+    P->md.abs_tol = s.abs_tol;
+    P->md.rel_tol = s.rel_tol;
+    P->md.n_max = s.n_max_substep;
+    for (int i = 0; i < 4; ++i) {
+        P->cam[i] = T(c.cam_pos[i]);
+        P->u_obs[i] = T(c.u_obs[i]);
+        for (int j = 0; j < 4; ++j) P->M[i][j] = T(c.M[i][j]);
+    }
+    P->pix_a = T(c.pix_a); P->pix_b = T(c.pix_b); P->pix_c = T(c.pix_c); P->pix_d = T(c.pix_d);
+    P->h0 = s.metric == MGK_METRIC_MINKOWSKI ? T(1000) : T(1);
+    P->disk_on = s.disk_r_out > 0.0 ? 1u : 0u;
+    P->disk_r_in = T(s.disk_r_in);
+    P->disk_r_out = T(s.disk_r_out);
+    P->disk_T_in = T(s.disk_T_in);
+    P->disk_lo = T(0.98 * s.disk_r_in - 0.02);
+    P->disk_hi = T(1.02 * s.disk_r_out + 0.02);
+    T er = T(s.escape_radius);
+    P->escape_r2 = er * er;
+    P->spin_phys = T(kerr ? s.spin : 0.0);
+    P->omega_sign = T(c.omega_sign);
+    P->kerr_a = T(kerr ? a_t : 0.0);
+    P->r_plus = c.r_plus;
+    double pre = c.r_plus + MGK_WIDE_BAND + 0.01;
+    P->band_pre2 = pre * pre;
+    P->atol_d = s.abs_tol;
+    P->rtol_d = s.rel_tol;
+    P->hmax_d = s.h_max;
+    P->spin_d = kerr ? a_t : 0.0;
+    T rr = T(s.star_radius_rad);
+    P->star_inv_r2 = T(1) / (rr * rr);
+    double dl = (s.lambda_max_nm - s.lambda_min_nm) / s.n_bins;
+    for (uint32_t k = 0; k < s.n_bins && k < MGK_MAX_BINS; ++k) P->lambda[k] = T(s.lambda_min_nm + (k + 0.5) * dl);
+    for (uint32_t k = 0; k < 3 * s.n_bins && k < 3 * MGK_MAX_BINS; ++k) P->xyz_w[k] = xyz_w[k];
+    P->seed = s.seed;
+    P->width = s.width; P->height = s.height; P->spp = s.spp; P->n_bins = s.n_bins;
+    P->max_steps = s.max_steps;
+    P->inv_spp = 1.0f / float(s.spp);
+}
+
+void fill_dev_scene(const mgk_scene& s, const float* xyz_w, void* out) {
+    if (s.precision == MGK_PRECISION_F64) fill_t<double>(s, xyz_w, reinterpret_cast<DevScene<double>*>(out));
+    else fill_t<float>(s, xyz_w, reinterpret_cast<DevScene<float>*>(out));
+}
+
+}  // namespace mgk

@@ -1,0 +1,143 @@
+"""ctypes loader of the CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+Imported by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg.
+liboracle.so is the C++ restatement (oracle.hpp, oracle_scene.hpp);
+_ref/libmagikref.so is the reference's own CPU tracer compiled from its
+sources by oracle/Makefile (only present where the reference was available
+at build time).
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from magik_b200 import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libmagikref.so")
+
+_lib = None
+_ref = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(ORACLE_SO):
+            build()
+        L = C.CDLL(ORACLE_SO)
+        L.orc_trace_geodesic.argtypes = [C.POINTER(abi.TraceContainer), abi.TraceInitialConditions,
+                                         abi.TraceMetricParams, abi.TraceIntegratorParams, C.c_int]
+        L.orc_trace_geodesic.restype = C.c_int
+        L.orc_scene_constants.argtypes = [C.POINTER(abi.Scene), C.POINTER(C.c_double)]
+        L.orc_trace_rays.argtypes = [C.POINTER(abi.Scene), C.c_uint64, C.c_uint32, C.POINTER(abi.RayResult),
+                                     C.c_int]
+        L.orc_shade_rays.argtypes = [C.POINTER(abi.Scene), C.POINTER(abi.Star), C.c_uint32, C.POINTER(C.c_float),
+                                     C.c_uint32, C.POINTER(abi.RayResult), C.POINTER(C.c_double), C.c_int]
+        L.orc_render_pixels.argtypes = [C.POINTER(abi.Scene), C.POINTER(abi.Star), C.c_uint32,
+                                        C.POINTER(C.c_float), C.c_uint64, C.c_uint32, C.c_uint64,
+                                        C.POINTER(C.c_double), C.POINTER(C.c_uint64), C.c_int]
+        L.orc_count_ops.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_uint64)]
+        _lib = L
+    return _lib
+
+
+def ref_available():
+    return os.path.exists(REF_SO)
+
+
+def ref():
+    global _ref
+    if _ref is None:
+        R = C.CDLL(REF_SO)
+        R.ref_trace_geodesic.argtypes = [C.POINTER(abi.TraceContainer), abi.TraceInitialConditions,
+                                         abi.TraceMetricParams, abi.TraceIntegratorParams]
+        R.ref_trace_geodesic.restype = C.c_int
+        R.ref_cmf_weights.argtypes = [C.c_uint, C.c_float, C.c_float, C.POINTER(C.c_float)]
+        _ref = R
+    return _ref
+
+
+def new_container(n_steps):
+    steps = (abi.TraceStep * n_steps)()
+    c = abi.TraceContainer(C.sizeof(abi.TraceStep) * n_steps, n_steps, 0,
+                           C.cast(steps, C.POINTER(abi.TraceStep)))
+    return c, steps
+
+
+def steps_array(container, steps):
+    """(n_written, 15) float32 array of a filled container."""
+    n = container.n_written
+    a = np.frombuffer(steps, dtype=np.float32, count=15 * len(steps)).reshape(len(steps), 15)
+    return a[:n].copy()
+
+
+def trace_geodesic(ic, mp, ip, n_steps=4096, pow_in_double=False):
+    c, steps = new_container(n_steps)
+    rc = lib().orc_trace_geodesic(C.byref(c), ic, mp, ip, int(pow_in_double))
+    return rc, steps_array(c, steps)
+
+
+def ref_trace_geodesic(ic, mp, ip, n_steps=4096):
+    c, steps = new_container(n_steps)
+    rc = ref().ref_trace_geodesic(C.byref(c), ic, mp, ip)
+    return rc, steps_array(c, steps)
+
+
+def ref_cmf_weights(n_bins, lmin, lmax):
+    out = (C.c_float * (3 * n_bins))()
+    assert ref().ref_cmf_weights(n_bins, lmin, lmax, out) == 0
+    return np.frombuffer(out, dtype=np.float32).reshape(n_bins, 3).copy()
+
+
+def scene_constants(scene):
+    out = (C.c_double * 32)()
+    lib().orc_scene_constants(C.byref(scene), out)
+    return np.frombuffer(out, dtype=np.float64).copy()
+
+
+RESULT_DTYPE = np.dtype([("x", "<f8", 4), ("p", "<f8", 4), ("z", "<f8"), ("r_hit", "<f8"), ("dir", "<f8", 3),
+                         ("cls", "<u4"), ("steps", "<u4"), ("attempts", "<u4"), ("wide_attempts", "<u4"),
+                         ("refine_evals", "<u4"), ("reserved", "<u4")])
+assert RESULT_DTYPE.itemsize == C.sizeof(abi.RayResult)
+
+
+def trace_rays(scene, first, n, nthreads=None):
+    out = np.zeros(n, dtype=RESULT_DTYPE)
+    lib().orc_trace_rays(C.byref(scene), first, n, out.ctypes.data_as(C.POINTER(abi.RayResult)),
+                         nthreads or os.cpu_count())
+    return out
+
+
+def shade_rays(scene, stars, weights, results, nthreads=None):
+    stars = np.ascontiguousarray(stars)
+    w = np.ascontiguousarray(weights, dtype=np.float32)
+    out = np.zeros((len(results), 3), dtype=np.float64)
+    lib().orc_shade_rays(C.byref(scene), stars.ctypes.data_as(C.POINTER(abi.Star)), len(stars),
+                         w.ctypes.data_as(C.POINTER(C.c_float)), len(results),
+                         np.ascontiguousarray(results).ctypes.data_as(C.POINTER(abi.RayResult)),
+                         out.ctypes.data_as(C.POINTER(C.c_double)), nthreads or os.cpu_count())
+    return out
+
+
+def render_pixels(scene, stars, weights, first_pixel, n_pixels, nthreads=None, stride=1):
+    stars = np.ascontiguousarray(stars)
+    w = np.ascontiguousarray(weights, dtype=np.float32)
+    out = np.zeros((n_pixels, 3), dtype=np.float64)
+    att = C.c_uint64(0)
+    lib().orc_render_pixels(C.byref(scene), stars.ctypes.data_as(C.POINTER(abi.Star)), len(stars),
+                            w.ctypes.data_as(C.POINTER(C.c_float)), first_pixel, n_pixels, stride,
+                            out.ctypes.data_as(C.POINTER(C.c_double)), C.byref(att), nthreads or os.cpu_count())
+    return out, att.value
+
+
+def count_ops(metric, fused):
+    out = (C.c_uint64 * 2)()
+    lib().orc_count_ops(metric, int(fused), out)
+    return out[0], out[1]
