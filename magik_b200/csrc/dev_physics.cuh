@@ -264,15 +264,76 @@ __device__ __forceinline__ T rms_error(const S7<T>& e, const S7<T>& y0, const S7
     return sqrt(acc / T(8));
 }
 
-// Error norm of the wide (FP64) controller from T-valued stages.
-template <class T>
-__device__ __forceinline__ double wide_error(const S7<T>& y0, const S7<T>& y1, const S7<T> k[6], T h, double atol,
-                                             double rtol) {
+// ---------------------------------------------------------- step control
+// Step-size factor err^(-1/5) for the proposal h_new = 0.9 h err^(-1/5)
+// (internal_math.h:2190 writes it as pow(1/err, 0.2)).  Computed with IEEE
+// operations only, so the CPU oracle reproduces it bit for bit: split
+// a = m 2^e with m in [1, 2), e = 5q + r; start from a quadratic fit of
+// m^(-1/5) times 2^(-r/5) 2^(-q), then Newton steps y <- y (6 - a y^5) / 5.
+__device__ __forceinline__ float inv_root5(float a) {
+    if (!(a <= 3.4028235e38f)) return 0.0f;  // err = inf: no step
+    const uint32_t b = __float_as_uint(a);
+    const int ex = int(b >> 23) - 127;
+    const float m = __uint_as_float((b & 0x7fffffu) | 0x3f800000u);
+    const int q = ex >= 0 ? ex / 5 : -((4 - ex) / 5);
+    const int r = ex - 5 * q;
+    const float D[5] = {1.0f, 0.8705505632961241f, 0.757858283255199f, 0.6597539553864471f, 0.5743491774985174f};
+    float y = __fmaf_rn(__fmaf_rn(0.05264997f, m, -0.28570902f), m, 1.23209767f);
+    y = y * D[r];
+    y = y * __uint_as_float(uint32_t(127 - q) << 23);
+#pragma unroll
+    for (int it = 0; it < 2; ++it) {
+        float y2 = y * y, y4 = y2 * y2, t = a * (y4 * y);
+        y = y * __fmaf_rn(-0.2f, t, 1.2f);
+    }
+    return y;
+}
+__device__ __forceinline__ double inv_root5(double a) {
+    if (!(a <= 1.7976931348623157e308)) return 0.0;
+    const uint64_t b = uint64_t(__double_as_longlong(a));
+    const int ex = int(b >> 52) - 1023;
+    const double m = __longlong_as_double((long long)((b & 0xfffffffffffffull) | 0x3ff0000000000000ull));
+    const int q = ex >= 0 ? ex / 5 : -((4 - ex) / 5);
+    const int r = ex - 5 * q;
+    const double D[5] = {1.0, 0.8705505632961241, 0.757858283255199, 0.6597539553864471, 0.5743491774985174};
+    double y = __fma_rn(__fma_rn(0.05264997, m, -0.28570902), m, 1.23209767);
+    y = y * D[r];
+    y = y * __longlong_as_double((long long)(uint64_t(1023 - q) << 52));
+#pragma unroll
+    for (int it = 0; it < 3; ++it) {
+        double y2 = y * y, y4 = y2 * y2, t = a * (y4 * y);
+        y = y * __fma_rn(-0.2, t, 1.2);
+    }
+    return y;
+}
+
+// MIXED control: the error estimate (difference of the 5th- and 4th-order
+// solutions, which cancels badly in FP32) is formed in FP64 from the FP32
+// stages; its norm and the proposal need only a few digits and run in FP32.
+__device__ __forceinline__ void control_mixed(const S7<float>& y0, const S7<float>& y1, const S7<float> k[6],
+                                              float h, const MP<float>& m, float& h_next, bool& ok) {
     S7<double> kd[6];
 #pragma unroll
     for (int i = 0; i < 6; ++i) kd[i] = cvt<double>(k[i]);
-    S7<double> e = rkf45_error<Fuse::Fma, double>(double(h), kd);
-    return rms_error<Fuse::Fma, double>(e, cvt<double>(y0), cvt<double>(y1), atol, rtol);
+    S7<float> e = cvt<float>(rkf45_error<Fuse::Fma, double>(double(h), kd));
+    float err = rms_error<Fuse::Fma, float>(e, y0, y1, m.abs_tol, m.rel_tol);
+    float safe = err > 1e-30f ? err : 1e-30f;
+    float hn = (0.9f * h) * inv_root5(safe);
+    if (hn > m.h_max) hn = m.h_max;
+    h_next = hn;
+    ok = safe < 1.0f;
+}
+
+// FP64 control (F64 mode, and MIXED attempts inside the FP64 band).
+__device__ __forceinline__ void control_f64(const S7<double>& y0, const S7<double>& y1, const S7<double> k[6],
+                                            double h, const MP<double>& m, double& h_next, bool& ok) {
+    S7<double> e = rkf45_error<Fuse::Fma, double>(h, k);
+    double err = rms_error<Fuse::Fma, double>(e, y0, y1, m.abs_tol, m.rel_tol);
+    double safe = err > 1e-30 ? err : 1e-30;
+    double hn = (0.9 * h) * inv_root5(safe);
+    if (hn > m.h_max) hn = m.h_max;
+    h_next = hn;
+    ok = safe < 1.0;
 }
 
 // Reference step proposal 0.9*h*pow(1/err, 0.2f) (internal_math.h:2179-2195)
@@ -280,11 +341,6 @@ __device__ __forceinline__ double wide_error(const S7<T>& y0, const S7<T>& y1, c
 __device__ __forceinline__ float propose_h_ref(float h, float err_safe, float h_max) {
     float g = float(pow(double(1.0f / err_safe), double(0.2f)));
     float h_new = (0.9f * h) * g;
-    if (h_new > h_max) h_new = h_max;
-    return h_new;
-}
-__device__ __forceinline__ double propose_h_wide(double h, double err_safe, double h_max) {
-    double h_new = (0.9 * h) * pow(1.0 / err_safe, 0.2);
     if (h_new > h_max) h_new = h_max;
     return h_new;
 }

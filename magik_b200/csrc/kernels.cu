@@ -94,11 +94,10 @@ __device__ __forceinline__ void attempt(const DevScene<T>& P, const S7<T>& y, T 
             float safe = err > 1e-30f ? err : 1e-30f;
             h_next = propose_h_ref(h, safe, P.m.h_max);
             ok = safe < 1.0f;
+        } else if constexpr (MODE == MGK_PRECISION_MIXED) {
+            control_mixed(y, y1, k, h, P.m, h_next, ok);
         } else {
-            double err = wide_error<T>(y, y1, k, h, P.atol_d, P.rtol_d);
-            double safe = err > 1e-30 ? err : 1e-30;
-            h_next = T(propose_h_wide(double(h), safe, P.hmax_d));
-            ok = safe < 1.0;
+            control_f64(y, y1, k, h, P.m, h_next, ok);
         }
     }
 }
@@ -110,10 +109,9 @@ __device__ __forceinline__ void attempt_wide(const DevScene<float>& P, const S7<
     S7<double> yd = cvt<double>(y), y1d;
     S7<double> k[6];
     rkf45_stages<METRIC, Fuse::Fma, double>(yd, double(pt), double(h), P.md, y1d, k);
-    double err = wide_error<double>(yd, y1d, k, double(h), P.atol_d, P.rtol_d);
-    double safe = err > 1e-30 ? err : 1e-30;
-    h_next = float(propose_h_wide(double(h), safe, P.hmax_d));
-    ok = safe < 1.0;
+    double hn;
+    control_f64(yd, y1d, k, double(h), P.md, hn, ok);
+    h_next = float(hn);
     y1 = cvt<float>(y1d);
 }
 

@@ -347,20 +347,82 @@ template <Ctl K, class T> inline T propose_h(T h, T err_safe, T h_max) {
     return h_new;
 }
 
-// Wide-controller step proposal (all double): 0.9*h*(1/err)^(1/5).
-inline double propose_h_wide(double h, double err_safe, double h_max) {
-    double h_new = (0.9 * h) * std::pow(1.0 / err_safe, 0.2);
-    if (h_new > h_max) h_new = h_max;
-    return h_new;
+// Step-size factor err^(-1/5) of the MIXED and F64 controllers, IEEE
+// operations only (the CUDA kernels compute the same bits): a = m 2^e with
+// m in [1, 2), e = 5q + r; a quadratic fit of m^(-1/5) times 2^(-r/5) 2^(-q),
+// then Newton steps y <- y (6 - a y^5) / 5 (two in float, three in double).
+inline float inv_root5(float a) {
+    if (!(a <= 3.4028235e38f)) return 0.0f;
+    uint32_t b;
+    std::memcpy(&b, &a, 4);
+    const int ex = int(b >> 23) - 127;
+    uint32_t mb = (b & 0x7fffffu) | 0x3f800000u;
+    float m;
+    std::memcpy(&m, &mb, 4);
+    const int q = ex >= 0 ? ex / 5 : -((4 - ex) / 5);
+    const int r = ex - 5 * q;
+    const float D[5] = {1.0f, 0.8705505632961241f, 0.757858283255199f, 0.6597539553864471f, 0.5743491774985174f};
+    float y = std::fma(std::fma(0.05264997f, m, -0.28570902f), m, 1.23209767f);
+    y = y * D[r];
+    uint32_t pb = uint32_t(127 - q) << 23;
+    float p2;
+    std::memcpy(&p2, &pb, 4);
+    y = y * p2;
+    for (int it = 0; it < 2; ++it) {
+        float y2 = y * y, y4 = y2 * y2, t = a * (y4 * y);
+        y = y * std::fma(-0.2f, t, 1.2f);
+    }
+    return y;
+}
+inline double inv_root5(double a) {
+    if (!(a <= 1.7976931348623157e308)) return 0.0;
+    uint64_t b;
+    std::memcpy(&b, &a, 8);
+    const int ex = int(b >> 52) - 1023;
+    uint64_t mb = (b & 0xfffffffffffffull) | 0x3ff0000000000000ull;
+    double m;
+    std::memcpy(&m, &mb, 8);
+    const int q = ex >= 0 ? ex / 5 : -((4 - ex) / 5);
+    const int r = ex - 5 * q;
+    const double D[5] = {1.0, 0.8705505632961241, 0.757858283255199, 0.6597539553864471, 0.5743491774985174};
+    double y = std::fma(std::fma(0.05264997, m, -0.28570902), m, 1.23209767);
+    y = y * D[r];
+    uint64_t pb = uint64_t(1023 - q) << 52;
+    double p2;
+    std::memcpy(&p2, &pb, 8);
+    y = y * p2;
+    for (int it = 0; it < 3; ++it) {
+        double y2 = y * y, y4 = y2 * y2, t = a * (y4 * y);
+        y = y * std::fma(-0.2, t, 1.2);
+    }
+    return y;
 }
 
-// Error norm of the wide controller from T-valued stages, all in double.
-template <class T>
-inline double wide_error(const GState<T>& y0, const GState<T>& y1, const GState<T> k[6], T h, double atol, double rtol) {
+// FP64 control: error estimate, norm and proposal all in double.
+inline void control_f64(const GState<double>& y0, const GState<double>& y1, const GState<double> k[6], double h,
+                        const MetricParams<double>& m, double* h_next, bool* ok) {
+    GState<double> e = rkf45_error<Fuse::Fma, double>(h, k);
+    double err = rms_error<Fuse::Fma, double>(e, y0, y1, m.abs_tol, m.rel_tol);
+    double safe = err > 1e-30 ? err : 1e-30;
+    double hn = (0.9 * h) * inv_root5(safe);
+    if (hn > m.h_max) hn = m.h_max;
+    *h_next = hn;
+    *ok = safe < 1.0;
+}
+
+// MIXED control: the error estimate in double from the float stages; its
+// norm and the proposal in float.
+inline void control_mixed(const GState<float>& y0, const GState<float>& y1, const GState<float> k[6], float h,
+                          const MetricParams<float>& m, float* h_next, bool* ok) {
     GState<double> kd[6];
     for (int i = 0; i < 6; ++i) kd[i] = to_double(k[i]);
-    GState<double> e = rkf45_error<Fuse::Fma, double>(double(h), kd);
-    return rms_error<Fuse::Fma, double>(e, to_double(y0), to_double(y1), atol, rtol);
+    GState<float> e = widen<float>(rkf45_error<Fuse::Fma, double>(double(h), kd));
+    float err = rms_error<Fuse::Fma, float>(e, y0, y1, m.abs_tol, m.rel_tol);
+    float safe = err > 1e-30f ? err : 1e-30f;
+    float hn = (0.9f * h) * inv_root5(safe);
+    if (hn > m.h_max) hn = m.h_max;
+    *h_next = hn;
+    *ok = safe < 1.0f;
 }
 
 // Result of one attempt sequence (= one accepted step of the reference).
@@ -393,12 +455,11 @@ inline StepOut<T> solve_step(const GState<T>& y0, T h, const MetricParams<T>& m)
         ++o.attempts;
         bool ok;
         if constexpr (K == Ctl::Wide) {
-            double err = wide_error<T>(y0, o.y1, k, temp_h, double(m.abs_tol), double(m.rel_tol));
-            double safe = err > 1e-30 ? err : 1e-30;
-            double hn = propose_h_wide(double(temp_h), safe, double(m.h_max));
+            static_assert(std::is_same_v<T, double>, "the FP64 controller runs on double state");
+            double hn;
+            control_f64(y0, o.y1, k, temp_h, m, &hn, &ok);
             o.h_taken = temp_h;
-            temp_h = T(hn);
-            ok = safe < 1.0;
+            temp_h = hn;
         } else {
             GState<T> e = rkf45_error<F, T>(temp_h, k);
             T err = rms_error<F, T>(e, y0, o.y1, m.abs_tol, m.rel_tol);

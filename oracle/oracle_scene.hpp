@@ -309,21 +309,19 @@ inline MixedAttempt mixed_attempt(const GState<float>& y0, float h, const Metric
     MixedAttempt o{};
     bool wide = (mf.metric != MINKOWSKI) && (r_cur - r_plus < MGK_WIDE_BAND);
     o.wide = wide;
-    double err;
     if (wide) {
         GState<double> yd = to_double(y0), y1d;
         GState<double> k[6];
         rkf45_attempt<Fuse::Fma, double>(yd, double(h), md, &y1d, k);
-        err = wide_error<double>(yd, y1d, k, double(h), md.abs_tol, md.rel_tol);
+        double hn;
+        control_f64(yd, y1d, k, double(h), md, &hn, &o.accept_ok);
+        o.h_next = float(hn);
         o.y1 = widen<float>(y1d);
     } else {
         GState<float> k[6];
         rkf45_attempt<Fuse::Fma, float>(y0, h, mf, &o.y1, k);
-        err = wide_error<float>(y0, o.y1, k, h, md.abs_tol, md.rel_tol);
+        control_mixed(y0, o.y1, k, h, mf, &o.h_next, &o.accept_ok);
     }
-    double safe = err > 1e-30 ? err : 1e-30;
-    o.h_next = float(propose_h_wide(double(h), safe, md.h_max));
-    o.accept_ok = safe < 1.0;
     return o;
 }
 
