@@ -55,8 +55,9 @@ ARGS = None
 
 
 def scene_config(M, rank=0):
+    from magik_b200.dist import frame_seed
     s = M.scene_defaults()
-    s.seed = 0x5EED + rank
+    s.seed = frame_seed(0x5EED, rank)
     if ARGS is not None:
         for k in ("width", "height", "spp"):
             v = getattr(ARGS, k)
@@ -261,10 +262,8 @@ def run_gpu(args, rank, world, local_rank):
     e2e_ms = statistics.mean(e2e_times)
     ms_int = statistics.mean(integ)
     if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([ms, e2e_ms, ms_int], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, e2e_ms, ms_int = t.tolist()
+        from magik_b200.dist import max_over_ranks
+        ms, e2e_ms, ms_int = max_over_ranks([ms, e2e_ms, ms_int], device=dev)
     if rank != 0:
         return None
 
@@ -287,7 +286,8 @@ def run_gpu(args, rank, world, local_rank):
                      "flop_per_crossing_substep": FL.substep_flops(s.metric),
                      "integrate_ms": ms_int},
         "stats": {"attempts": st_last.attempts, "steps": st_last.steps, "refine_evals": st_last.refine_evals,
-                  "wide_attempts": st_last.wide_attempts,
+                  "wide_attempts": st_last.wide_attempts, "crossings": st_last.crossings,
+                  "resumed": st_last.resumed,
                   "classes": dict(zip(["alive", "disk", "escaped", "horizon", "step_limit"],
                                       [int(c) for c in st_last.class_count])),
                   "attempts_per_ray": st_last.attempts / rays},

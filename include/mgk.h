@@ -74,8 +74,9 @@ typedef int32_t mgk_result;
 /* Distance (in M) from the outer horizon below which MIXED attempts run in FP64. */
 #define MGK_WIDE_BAND 0.05
 
-/* Secant iterations (after the first RK sub-step) spent locating a disk or
- * escape crossing on the geodesic. */
+/* Secant iterations (after the first RK sub-step to the chord estimate)
+ * spent locating a disk crossing on the geodesic; an escape crossing takes
+ * the first sub-step only. */
 #define MGK_REFINE_ITERS 4
 
 /* Termination class of a ray. */
@@ -156,6 +157,8 @@ typedef struct mgk_render_stats {
     uint64_t class_count[5];  /* indexed by MGK_RAY_* */
     double integrate_ms;      /* device time of the integrator launches */
     double total_ms;          /* device time of the whole render */
+    uint64_t crossings;       /* steps handed to the crossing kernel */
+    uint64_t resumed;         /* rays continued by the tail kernel */
 } mgk_render_stats;
 
 typedef struct mgk_context mgk_context;

@@ -63,7 +63,8 @@ class RenderStats(C.Structure):
     _fields_ = [("rays", C.c_uint64), ("attempts", C.c_uint64), ("steps", C.c_uint64),
                 ("wide_attempts", C.c_uint64), ("refine_evals", C.c_uint64),
                 ("class_count", C.c_uint64 * 5),
-                ("integrate_ms", C.c_double), ("total_ms", C.c_double)]
+                ("integrate_ms", C.c_double), ("total_ms", C.c_double), ("crossings", C.c_uint64),
+                ("resumed", C.c_uint64)]
 
 
 class TraceMetricParams(C.Structure):

@@ -365,6 +365,8 @@ mgk_result run(mgk_context* ctx, const mgk_scene& s, const mgk_star* d_stars, ui
             stats->steps += k.steps;
             stats->wide_attempts += k.wide_attempts;
             stats->refine_evals += k.refine_evals;
+            stats->crossings += k.refine_count;
+            stats->resumed += k.resume_count;
             for (int i = 0; i < 5; ++i) stats->class_count[i] += k.class_count[i];
             status |= k.status;
         }

@@ -6,7 +6,8 @@
 //   Fuse::None reproduces the reference's expression trees (metric_kerr.cuh,
 //   metric_schwarzschild.cuh, internal_math.h) with separate roundings, i.e.
 //   what the reference computes on the CPU.
-//   Fuse::Fma uses the same trees with the marked multiply-adds fused.
+//   Fuse::Fma uses the same trees with the marked multiply-adds fused, and
+//   forms the RHS quotients from two reciprocals instead of five divisions.
 // Division and sqrt are IEEE-rounded (-prec-div/-prec-sqrt, no fast math).
 #pragma once
 
@@ -54,23 +55,37 @@ __device__ __forceinline__ void rhs_kerr(const S7<T>& s, T pt, T a, S7<T>& o) {
     T r_cu = r_sq * r;
     T r_quad = r_sq * r_sq;
     T r_six = r_cu * r_cu;
-    T inv_r = one / r;
+    T d = r_sq + a_sq;
+    T f_den = mad<F>(a_sq, y_sq, r_quad);
+    T inv_r, inv_sigma, inv_d, inv_f_den_sq, f_;
+    if constexpr (F == Fuse::Fma) {
+        // two reciprocals give all five quotients: 1/(r sigma d) and 1/f_den
+        T rs = r * sigma;
+        T inv_rsd = one / (rs * d);
+        T inv_fden = one / f_den;
+        inv_d = rs * inv_rsd;
+        T inv_rs = d * inv_rsd;
+        inv_r = sigma * inv_rs;
+        inv_sigma = r * inv_rs;
+        inv_f_den_sq = inv_fden * inv_fden;
+        f_ = (two * r_cu) * inv_fden;
+    } else {
+        inv_r = one / r;
+        inv_sigma = one / sigma;
+        inv_d = one / d;
+        inv_f_den_sq = one / (f_den * f_den);
+        f_ = (two * r_cu) / f_den;
+    }
     T inv_rsq = inv_r * inv_r;
-    T inv_sigma = one / sigma;
     T scale_xz = (half * inv_r) * mad<F>(w_sq, inv_sigma, one);
     T scale_y = (half * inv_r) * mad<F>(w_sq + two * a_sq, inv_sigma, one);
     T drx = x * scale_xz, dry = y * scale_y, drz = z * scale_xz;
-    T d = r_sq + a_sq;
-    T inv_d = one / d;
     T inv_dsq = inv_d * inv_d;
     T kx_num = mad<F>(r, x, -(a * z));
     T kz_num = mad<F>(r, z, a * x);
     T kx = kx_num * inv_d;
     T kz = kz_num * inv_d;
     T ky = y * inv_r;
-    T f_den = mad<F>(a_sq, y_sq, r_quad);
-    T inv_f_den_sq = one / (f_den * f_den);
-    T f_ = (two * r_cu) / f_den;
     T dfdq_scale = (two * mad<F>((T(3) * a_sq) * r_sq, y_sq, -r_six)) * inv_f_den_sq;
     T dfx = dfdq_scale * drx;
     T dfy = mad<F>(dfdq_scale, dry, -((((T(4) * a_sq) * r_cu) * y) * inv_f_den_sq));
@@ -112,22 +127,35 @@ __device__ __forceinline__ void rhs_schwarzschild(const S7<T>& s, T pt, T mass_s
     T r_cu = r_sq * r;
     T r_quad = r_sq * r_sq;
     T r_six = r_cu * r_cu;
-    T inv_r = one / r;
+    T d = r_sq;
+    T f_den = r_quad;
+    T inv_r, inv_sigma, inv_d, inv_f_den_sq, f_;
+    if constexpr (F == Fuse::Fma) {
+        T rs = r * sigma;
+        T inv_rsd = one / (rs * d);
+        T inv_fden = one / f_den;
+        inv_d = rs * inv_rsd;
+        T inv_rs = d * inv_rsd;
+        inv_r = sigma * inv_rs;
+        inv_sigma = r * inv_rs;
+        inv_f_den_sq = inv_fden * inv_fden;
+        f_ = ((mass_sign * two) * r_cu) * inv_fden;
+    } else {
+        inv_r = one / r;
+        inv_sigma = one / sigma;
+        inv_d = one / d;
+        inv_f_den_sq = one / (f_den * f_den);
+        f_ = ((mass_sign * two) * r_cu) / f_den;
+    }
     T inv_rsq = inv_r * inv_r;
-    T inv_sigma = one / sigma;
     T sc = (half * inv_r) * mad<F>(w_sq, inv_sigma, one);
     T drx = x * sc, dry = y * sc, drz = z * sc;
-    T d = r_sq;
-    T inv_d = one / d;
     T inv_dsq = inv_d * inv_d;
     T kx_num = r * x;
     T kz_num = r * z;
     T kx = kx_num * inv_d;
     T kz = kz_num * inv_d;
     T ky = y * inv_r;
-    T f_den = r_quad;
-    T inv_f_den_sq = one / (f_den * f_den);
-    T f_ = ((mass_sign * two) * r_cu) / f_den;
     T dfdq_scale = ((mass_sign * two) * (-r_six)) * inv_f_den_sq;
     T dfx = dfdq_scale * drx, dfy = dfdq_scale * dry, dfz = dfdq_scale * drz;
     T two_r = two * r;

@@ -294,7 +294,11 @@ __device__ __forceinline__ S7<T> refine(int kind, const S7<T>& y0, const S7<T>& 
     S7<T> ys = sub_step<METRIC, F, T>(y0, pt, s, m);
     ++evals;
     T gs = cross_g<F>(kind, ys, R2);
-    for (int it = 0; it < MGK_REFINE_ITERS; ++it) {
+    // The escape sphere lies in the far field, where one sub-step to the chord
+    // estimate already puts the direction within 1e-9 of the located one;
+    // the disk plane is met in strong field and iterates.
+    const int iters = kind == 0 ? MGK_REFINE_ITERS : 0;
+    for (int it = 0; it < iters; ++it) {
         T den = gs - g_prev;
         if (gs == T(0) || den == T(0)) break;
         T s_new = s - gs * (s - s_prev) / den;

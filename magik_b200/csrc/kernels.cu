@@ -350,7 +350,7 @@ __global__ void __launch_bounds__(kIntegrateThreads, 2)
 // emit the hit, or send the ray on to the tail kernel when the disk
 // candidate missed and nothing else ended it.
 template <int METRIC, int MODE>
-__global__ void __launch_bounds__(128) k_refine(const DevScene<typename ModeT<MODE>::T> P,
+__global__ void __launch_bounds__(128, 4) k_refine(const DevScene<typename ModeT<MODE>::T> P,
                                                 const RefineEntry<typename ModeT<MODE>::T>* __restrict__ refq,
                                                 uint32_t cap, HitEntry<typename ModeT<MODE>::T>* hits,
                                                 ResumeEntry<typename ModeT<MODE>::T>* resq, mgk_ray_result* res,
@@ -398,7 +398,7 @@ __global__ void __launch_bounds__(128) k_refine(const DevScene<typename ModeT<MO
 // One thread per resumed ray, run sequentially to termination.  MIXED mode:
 // FP64 attempts while within MGK_WIDE_BAND of r_plus, FP32 otherwise.
 template <int METRIC, int MODE>
-__global__ void __launch_bounds__(128) k_tail(const DevScene<typename ModeT<MODE>::T> P,
+__global__ void __launch_bounds__(128, 4) k_tail(const DevScene<typename ModeT<MODE>::T> P,
                                               const ResumeEntry<typename ModeT<MODE>::T>* __restrict__ resq,
                                               uint32_t cap, HitEntry<typename ModeT<MODE>::T>* hits,
                                               mgk_ray_result* res, Counters* cnt) {
@@ -474,7 +474,9 @@ __global__ void __launch_bounds__(128) k_tail(const DevScene<typename ModeT<MODE
 }
 
 // ------------------------------------------------------------------ shade
-// One warp per hit; lane k evaluates bins k and k + 32.
+// One thread per hit (a warp shades 32 hits at once, so the dependent loads of
+// the entry, the star cell and the stars overlap across lanes).  The bin
+// wavelengths and XYZ weights are staged in shared memory.
 template <class T>
 __global__ void __launch_bounds__(256) k_shade(const DevScene<T> P, const HitEntry<T>* __restrict__ hits,
                                                uint32_t cap, const Counters* cnt, const mgk_star* __restrict__ stars,
@@ -482,61 +484,49 @@ __global__ void __launch_bounds__(256) k_shade(const DevScene<T> P, const HitEnt
                                                float* __restrict__ xyz_ray, float* __restrict__ film_spec,
                                                uint64_t first_ray) {
     __shared__ float sw[3 * MGK_MAX_BINS];
-    for (int i = threadIdx.x; i < 3 * MGK_MAX_BINS; i += blockDim.x) sw[i] = d_w ? d_w[i < 3 * int(P.n_bins) ? i : 0] : P.xyz_w[i];
-    __syncthreads();
-    const int lane = threadIdx.x & 31;
-    const uint32_t n = min(cnt->hit_count, cap);
+    __shared__ T slam[MGK_MAX_BINS];
     const uint32_t nb = P.n_bins;
-    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-    const bool has0 = uint32_t(lane) < nb, has1 = uint32_t(lane) + 32u < nb;
-    const T lam0 = has0 ? P.lambda[lane] : T(0), lam1 = has1 ? P.lambda[lane + 32] : T(0);
-    for (uint32_t e = warp; e < n; e += nwarps) {
+    for (uint32_t i = threadIdx.x; i < 3 * MGK_MAX_BINS; i += blockDim.x)
+        sw[i] = i < 3 * nb ? (d_w ? d_w[i] : P.xyz_w[i]) : 0.f;
+    for (uint32_t i = threadIdx.x; i < MGK_MAX_BINS; i += blockDim.x) slam[i] = P.lambda[i];
+    __syncthreads();
+    const uint32_t n = min(cnt->hit_count, cap);
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
         const HitEntry<T> h = hits[e];
         const T z = h.z, z2 = z * z, z5 = z2 * z2 * z;
-        T s0 = T(0), s1 = T(0);
+        float X = 0.f, Y = 0.f, Z = 0.f;
+        float* spec = film_spec ? film_spec + ((first_ray + h.ray) / P.spp) * nb : nullptr;
         if (h.cls == MGK_RAY_DISK) {
-            T temp = P.disk_T_in * T(pow(double(h.r_hit / P.disk_r_in), -0.75));
-            if (has0) s0 = clamp_radiance<T>(planck<T>(z * lam0, temp) * z5);
-            if (has1) s1 = clamp_radiance<T>(planck<T>(z * lam1, temp) * z5);
+            const T temp = P.disk_T_in * T(pow(double(h.r_hit / P.disk_r_in), -0.75));
+            for (uint32_t k = 0; k < nb; ++k) {
+                float sv = float(clamp_radiance<T>(planck<T>(z * slam[k], temp) * z5));
+                X = __fmaf_rn(sv, sw[3 * k], X);
+                Y = __fmaf_rn(sv, sw[3 * k + 1], Y);
+                Z = __fmaf_rn(sv, sw[3 * k + 2], Z);
+                if (spec) atomicAdd(spec + k, sv * P.inv_spp);
+            }
         } else if (grid.n != 0u) {
-            uint32_t cell = cube_cell(float(h.d0), float(h.d1), float(h.d2), grid.n);
-            uint32_t j0 = grid.cell_start[cell], j1 = grid.cell_start[cell + 1];
-            for (uint32_t j = j0; j < j1; ++j) {
+            const uint32_t cell = cube_cell(float(h.d0), float(h.d1), float(h.d2), grid.n);
+            const uint32_t j1 = grid.cell_start[cell + 1];
+            for (uint32_t j = grid.cell_start[cell]; j < j1; ++j) {
                 const mgk_star st = stars[grid.cell_stars[j]];
                 T dx = h.d0 - T(st.dir[0]), dy = h.d1 - T(st.dir[1]), dz = h.d2 - T(st.dir[2]);
                 T q = mad<Fuse::Fma>(dz, dz, mad<Fuse::Fma>(dy, dy, dx * dx)) * P.star_inv_r2;
                 if (q >= T(1)) continue;
-                T kern = (T(1) - q) * (T(1) - q);
-                T amp = T(st.amplitude) * kern;
-                if (has0) s0 += clamp_radiance<T>(amp * planck<T>(z * lam0, T(st.temperature)) * z5);
-                if (has1) s1 += clamp_radiance<T>(amp * planck<T>(z * lam1, T(st.temperature)) * z5);
+                const T amp = T(st.amplitude) * ((T(1) - q) * (T(1) - q));
+                const T ts = T(st.temperature);
+                for (uint32_t k = 0; k < nb; ++k) {
+                    float sv = float(clamp_radiance<T>(amp * planck<T>(z * slam[k], ts) * z5));
+                    X = __fmaf_rn(sv, sw[3 * k], X);
+                    Y = __fmaf_rn(sv, sw[3 * k + 1], Y);
+                    Z = __fmaf_rn(sv, sw[3 * k + 2], Z);
+                    if (spec) atomicAdd(spec + k, sv * P.inv_spp);
+                }
             }
         }
-        float f0 = float(s0), f1 = float(s1);
-        float X = 0.f, Y = 0.f, Z = 0.f;
-        if (has0) { X = f0 * sw[3 * lane]; Y = f0 * sw[3 * lane + 1]; Z = f0 * sw[3 * lane + 2]; }
-        if (has1) {
-            X = __fmaf_rn(f1, sw[3 * (lane + 32)], X);
-            Y = __fmaf_rn(f1, sw[3 * (lane + 32) + 1], Y);
-            Z = __fmaf_rn(f1, sw[3 * (lane + 32) + 2], Z);
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            X += __shfl_xor_sync(kFull, X, o);
-            Y += __shfl_xor_sync(kFull, Y, o);
-            Z += __shfl_xor_sync(kFull, Z, o);
-        }
-        if (lane == 0) {
-            xyz_ray[3 * size_t(h.ray) + 0] = X;
-            xyz_ray[3 * size_t(h.ray) + 1] = Y;
-            xyz_ray[3 * size_t(h.ray) + 2] = Z;
-        }
-        if (film_spec) {
-            uint64_t pixel = (first_ray + h.ray) / P.spp;
-            if (has0) atomicAdd(&film_spec[pixel * nb + lane], f0 * P.inv_spp);
-            if (has1) atomicAdd(&film_spec[pixel * nb + lane + 32], f1 * P.inv_spp);
-        }
+        xyz_ray[3 * size_t(h.ray) + 0] = X;
+        xyz_ray[3 * size_t(h.ray) + 1] = Y;
+        xyz_ray[3 * size_t(h.ray) + 2] = Z;
     }
 }
 

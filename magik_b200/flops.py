@@ -7,14 +7,16 @@ the same expressions with an op-counting scalar (8 components, p_t included);
 tests/test_host.py checks that the figures below equal its counts minus the
 p_t work, which is identically zero and skipped by the kernels.
 
-  RHS                           Kerr 156   Schwarzschild 126
+  RHS                           Kerr 160   Schwarzschild 130 (the fused
+                                formulation: two reciprocals and six
+                                products in place of five quotients)
   one RKF45 attempt             6 RHS + 25 coefficient products + 210 stage
                                 combinations + 70 (5th-order solution)
                                 + 63 (error) + 36 (norm) + 4 (proposal)
   one crossing sub-step         6 RHS + 20 coefficient products + 210 + 70
 """
 
-RHS = {2: 156, 1: 126, 0: 0}
+RHS = {2: 160, 1: 130, 0: 0}
 ATTEMPT_OVERHEAD = 25 + 210 + 70 + 63 + 36 + 4
 SUBSTEP_OVERHEAD = 20 + 210 + 70
 # p_t terms the 8-component count includes and the kernels skip

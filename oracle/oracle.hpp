@@ -16,7 +16,8 @@
 //   Fuse::None - every a*b+c is a separately rounded multiply and add, in the
 //                reference's expression order (what g++ emits for x86-64).
 //   Fuse::Fma  - the same expression tree with the multiply-add pairs marked
-//                by mad() fused into one correctly rounded fma().  The CUDA
+//                by mad() fused into one correctly rounded fma(), and the
+//                five RHS quotients formed from two reciprocals.  The CUDA
 //                kernels use the same tree with __fmaf_rn / __fma_rn at the
 //                same sites, so both sides round identically.
 // Build with -ffp-contract=off so the compiler adds no fusion of its own.
@@ -67,25 +68,38 @@ template <Fuse F, class T> inline GState<T> rhs_kerr(const GState<T>& s, T a) {
     T r_quad = r_sq * r_sq;
     T r_six = r_cu * r_cu;
 
-    T inv_r = one / r;
+    T d = r_sq + a_sq;
+    T f_den = mad<F>(a_sq, y_sq, r_quad);
+    T inv_r, inv_sigma, inv_d, inv_f_den_sq, f_;
+    if constexpr (F == Fuse::Fma) {
+        // fused formulation: 1/(r sigma d) and 1/f_den give all five quotients
+        T rs = r * sigma;
+        T inv_rsd = one / (rs * d);
+        T inv_fden = one / f_den;
+        inv_d = rs * inv_rsd;
+        T inv_rs = d * inv_rsd;
+        inv_r = sigma * inv_rs;
+        inv_sigma = r * inv_rs;
+        inv_f_den_sq = inv_fden * inv_fden;
+        f_ = (two * r_cu) * inv_fden;
+    } else {
+        inv_r = one / r;
+        inv_sigma = one / sigma;
+        inv_d = one / d;
+        inv_f_den_sq = one / (f_den * f_den);
+        f_ = (two * r_cu) / f_den;
+    }
     T inv_rsq = inv_r * inv_r;
-    T inv_sigma = one / sigma;
     T scale_xz = (half * inv_r) * mad<F>(w_sq, inv_sigma, one);
     T scale_y = (half * inv_r) * mad<F>(w_sq + two * a_sq, inv_sigma, one);
     T drx = x * scale_xz, dry = y * scale_y, drz = z * scale_xz;
 
-    T d = r_sq + a_sq;
-    T inv_d = one / d;
     T inv_dsq = inv_d * inv_d;
     T kx_num = mad<F>(r, x, -(a * z));
     T kz_num = mad<F>(r, z, a * x);
     T kx = kx_num * inv_d;
     T kz = kz_num * inv_d;
     T ky = y * inv_r;
-
-    T f_den = mad<F>(a_sq, y_sq, r_quad);
-    T inv_f_den_sq = one / (f_den * f_den);
-    T f_ = (two * r_cu) / f_den;
 
     T dfdq_scale = (two * mad<F>((T(3) * a_sq) * r_sq, y_sq, -r_six)) * inv_f_den_sq;
     T dfx = dfdq_scale * drx;
@@ -134,24 +148,36 @@ template <Fuse F, class T> inline GState<T> rhs_schwarzschild(const GState<T>& s
     T r_quad = r_sq * r_sq;
     T r_six = r_cu * r_cu;
 
-    T inv_r = one / r;
+    T d = r_sq;
+    T f_den = r_quad;
+    T inv_r, inv_sigma, inv_d, inv_f_den_sq, f_;
+    if constexpr (F == Fuse::Fma) {
+        T rs = r * sigma;
+        T inv_rsd = one / (rs * d);
+        T inv_fden = one / f_den;
+        inv_d = rs * inv_rsd;
+        T inv_rs = d * inv_rsd;
+        inv_r = sigma * inv_rs;
+        inv_sigma = r * inv_rs;
+        inv_f_den_sq = inv_fden * inv_fden;
+        f_ = ((mass_sign * two) * r_cu) * inv_fden;
+    } else {
+        inv_r = one / r;
+        inv_sigma = one / sigma;
+        inv_d = one / d;
+        inv_f_den_sq = one / (f_den * f_den);
+        f_ = ((mass_sign * two) * r_cu) / f_den;
+    }
     T inv_rsq = inv_r * inv_r;
-    T inv_sigma = one / sigma;
     T scale = (half * inv_r) * mad<F>(w_sq, inv_sigma, one);
     T drx = x * scale, dry = y * scale, drz = z * scale;
 
-    T d = r_sq;
-    T inv_d = one / d;
     T inv_dsq = inv_d * inv_d;
     T kx_num = r * x;
     T kz_num = r * z;
     T kx = kx_num * inv_d;
     T kz = kz_num * inv_d;
     T ky = y * inv_r;
-
-    T f_den = r_quad;
-    T inv_f_den_sq = one / (f_den * f_den);
-    T f_ = ((mass_sign * two) * r_cu) / f_den;
 
     T dfdq_scale = ((mass_sign * two) * (-r_six)) * inv_f_den_sq;
     T dfx = dfdq_scale * drx, dfy = dfdq_scale * dry, dfz = dfdq_scale * drz;
