@@ -104,7 +104,8 @@ typedef struct mgk_scene {
     double h_max;            /* largest affine step (reference 1000) */
     uint32_t max_steps;      /* accepted steps per ray before MGK_RAY_STEP_LIMIT */
     uint32_t n_bins;         /* spectral bins, 1..MGK_MAX_BINS */
-    double escape_radius;    /* |x| at which a ray counts as escaped */
+    double escape_radius;    /* |x| at which a ray counts as escaped; MIXED needs
+                                escape_radius + 2 h_max <= 1.5e4 */
     double disk_r_in;        /* thin disk in the plane y = 0; disk_r_out <= 0 disables it */
     double disk_r_out;
     double disk_T_in;        /* T(r) = disk_T_in * (r / disk_r_in)^(-3/4) */

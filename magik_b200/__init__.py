@@ -14,7 +14,8 @@ from . import abi
 from .abi import Scene, Star, RayResult, RenderStats  # noqa: F401
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libmgk.so")
+# MGK_LIB selects another build of the library (e.g. a launch-shape variant)
+LIB_PATH = os.environ.get("MGK_LIB", os.path.join(HERE, "libmgk.so"))
 
 _lib = None
 

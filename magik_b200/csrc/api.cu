@@ -77,6 +77,10 @@ mgk_result validate(const mgk_scene* s) {
     if (!(s->focal_length_mm > 0.0) || !(s->sensor_diag_mm > 0.0) || !(s->cam_r > 0.0))
         return MGK_ERROR_INVALID_ARGUMENT;
     if (!(s->star_radius_rad > 0.0 && s->star_radius_rad <= 0.02)) return MGK_ERROR_INVALID_ARGUMENT;
+    // MIXED evaluates the RHS with one float reciprocal of ~r^9, finite below
+    // r ~ 1.9e4; a ray moves at most about h_max past the escape radius
+    if (s->precision == MGK_PRECISION_MIXED && s->escape_radius + 2.0 * s->h_max > 1.5e4)
+        return MGK_ERROR_INVALID_ARGUMENT;
     return MGK_SUCCESS;
 }
 
@@ -365,7 +369,7 @@ mgk_result run(mgk_context* ctx, const mgk_scene& s, const mgk_star* d_stars, ui
             stats->steps += k.steps;
             stats->wide_attempts += k.wide_attempts;
             stats->refine_evals += k.refine_evals;
-            stats->crossings += k.refine_count;
+            stats->crossings += k.refine_count + k.escape_count;
             stats->resumed += k.resume_count;
             for (int i = 0; i < 5; ++i) stats->class_count[i] += k.class_count[i];
             status |= k.status;

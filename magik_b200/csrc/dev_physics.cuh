@@ -7,7 +7,7 @@
 //   metric_schwarzschild.cuh, internal_math.h) with separate roundings, i.e.
 //   what the reference computes on the CPU.
 //   Fuse::Fma uses the same trees with the marked multiply-adds fused, and
-//   forms the RHS quotients from two reciprocals instead of five divisions.
+//   forms the five RHS quotients from one reciprocal.
 // Division and sqrt are IEEE-rounded (-prec-div/-prec-sqrt, no fast math).
 #pragma once
 
@@ -59,10 +59,12 @@ __device__ __forceinline__ void rhs_kerr(const S7<T>& s, T pt, T a, S7<T>& o) {
     T f_den = mad<F>(a_sq, y_sq, r_quad);
     T inv_r, inv_sigma, inv_d, inv_f_den_sq, f_;
     if constexpr (F == Fuse::Fma) {
-        // two reciprocals give all five quotients: 1/(r sigma d) and 1/f_den
+        // one reciprocal, 1/(r sigma d f_den), gives all five quotients
         T rs = r * sigma;
-        T inv_rsd = one / (rs * d);
-        T inv_fden = one / f_den;
+        T rsd = rs * d;
+        T inv_all = one / (rsd * f_den);  // ~r^9: finite for r below ~1.9e4 in float
+        T inv_rsd = f_den * inv_all;
+        T inv_fden = rsd * inv_all;
         inv_d = rs * inv_rsd;
         T inv_rs = d * inv_rsd;
         inv_r = sigma * inv_rs;
@@ -132,8 +134,10 @@ __device__ __forceinline__ void rhs_schwarzschild(const S7<T>& s, T pt, T mass_s
     T inv_r, inv_sigma, inv_d, inv_f_den_sq, f_;
     if constexpr (F == Fuse::Fma) {
         T rs = r * sigma;
-        T inv_rsd = one / (rs * d);
-        T inv_fden = one / f_den;
+        T rsd = rs * d;
+        T inv_all = one / (rsd * f_den);  // ~r^9: finite for r below ~1.9e4 in float
+        T inv_rsd = f_den * inv_all;
+        T inv_fden = rsd * inv_all;
         inv_d = rs * inv_rsd;
         T inv_rs = d * inv_rsd;
         inv_r = sigma * inv_rs;
@@ -335,6 +339,37 @@ __device__ __forceinline__ double inv_root5(double a) {
     return y;
 }
 
+// Reciprocal of a positive normal float from integer and FMA operations only
+// (bit-identical on the CPU): the seed 0x7EF311C3 - bits(x) is within 12 %,
+// two Newton steps y <- y (2 - x y) bring it within 2e-4.  The MIXED error
+// norm needs no more than that.
+__device__ __forceinline__ float rcp_norm(float x) {
+    float y = __uint_as_float(0x7EF311C3u - __float_as_uint(x));
+    y = y * __fmaf_rn(-x, y, 2.0f);
+    y = y * __fmaf_rn(-x, y, 2.0f);
+    return y;
+}
+
+// MIXED RMS norm: as rms_error<Fuse::Fma, float> with the divisions replaced
+// by rcp_norm.
+__device__ __forceinline__ float rms_error_mixed(const S7<float>& e, const S7<float>& y0, const S7<float>& y1,
+                                                 float atol, float rtol) {
+    auto term = [&](float ei, float a0, float a1) {
+        return ei * rcp_norm(__fmaf_rn(rtol, fmaxf(fabsf(a0), fabsf(a1)), atol));
+    };
+    float s0 = term(e.t, y0.t, y1.t), s1 = term(e.x, y0.x, y1.x), s2 = term(e.y, y0.y, y1.y);
+    float s3 = term(e.z, y0.z, y1.z);
+    float s5 = term(e.px, y0.px, y1.px), s6 = term(e.py, y0.py, y1.py), s7 = term(e.pz, y0.pz, y1.pz);
+    float acc = s0 * s0;
+    acc = __fmaf_rn(s1, s1, acc);
+    acc = __fmaf_rn(s2, s2, acc);
+    acc = __fmaf_rn(s3, s3, acc);
+    acc = __fmaf_rn(s5, s5, acc);
+    acc = __fmaf_rn(s6, s6, acc);
+    acc = __fmaf_rn(s7, s7, acc);
+    return sqrtf(acc / 8.0f);
+}
+
 // MIXED control: the error estimate (difference of the 5th- and 4th-order
 // solutions, which cancels badly in FP32) is formed in FP64 from the FP32
 // stages; its norm and the proposal need only a few digits and run in FP32.
@@ -344,7 +379,7 @@ __device__ __forceinline__ void control_mixed(const S7<float>& y0, const S7<floa
 #pragma unroll
     for (int i = 0; i < 6; ++i) kd[i] = cvt<double>(k[i]);
     S7<float> e = cvt<float>(rkf45_error<Fuse::Fma, double>(double(h), kd));
-    float err = rms_error<Fuse::Fma, float>(e, y0, y1, m.abs_tol, m.rel_tol);
+    float err = rms_error_mixed(e, y0, y1, m.abs_tol, m.rel_tol);
     float safe = err > 1e-30f ? err : 1e-30f;
     float hn = (0.9f * h) * inv_root5(safe);
     if (hn > m.h_max) hn = m.h_max;

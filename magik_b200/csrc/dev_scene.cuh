@@ -187,6 +187,8 @@ template <class T> struct DevScene {
     double atol_d, rtol_d, hmax_d, spin_d;
     T star_inv_r2;
     T lambda[MGK_MAX_BINS];
+    T planck_a[MGK_MAX_BINS];  // 2 h c^2 / lambda_k^5
+    T planck_b[MGK_MAX_BINS];  // h c / (k_B lambda_k)
     float xyz_w[3 * MGK_MAX_BINS];
     uint64_t seed;
     uint32_t width, height, spp, n_bins, max_steps, disk_on;

@@ -18,10 +18,10 @@ struct Counters {
     unsigned long long class_count[5];
     uint32_t queue_head;    // next queue index handed to a warp
     uint32_t hit_count;     // entries in the hit queue
-    uint32_t refine_count;  // entries in the crossing queue
+    uint32_t refine_count;  // disk-crossing entries (from the front of the crossing queue)
+    uint32_t escape_count;  // escape-crossing entries (from the back of the crossing queue)
     uint32_t resume_count;  // entries in the resume queue
     uint32_t status;        // 0 = ok; bit 0: a queue overflowed
-    uint32_t pad;
 };
 
 // Hit-queue entry (disk and sky rays; dark rays are not queued).

@@ -31,7 +31,13 @@
 namespace mgk {
 
 constexpr unsigned kFull = 0xffffffffu;
-constexpr int kIntegrateThreads = 256;
+#ifndef MGK_INTEGRATE_THREADS
+#define MGK_INTEGRATE_THREADS 256
+#endif
+#ifndef MGK_INTEGRATE_MIN_BLOCKS
+#define MGK_INTEGRATE_MIN_BLOCKS 2
+#endif
+constexpr int kIntegrateThreads = MGK_INTEGRATE_THREADS;
 constexpr uint32_t kChunk = 64;  // queue entries a warp takes per refill
 
 template <int MODE> struct ModeT { using T = float; static constexpr Fuse F = Fuse::Fma; };
@@ -204,7 +210,7 @@ template <class T> __device__ __forceinline__ S7<T> s7(const T* v) {
 // band hands its ray to the resume queue.  Both pushes are warp-ballot
 // compactions with one atomic per warp.
 template <int METRIC, int MODE>
-__global__ void __launch_bounds__(kIntegrateThreads, 2)
+__global__ void __launch_bounds__(kIntegrateThreads, MGK_INTEGRATE_MIN_BLOCKS)
     k_integrate(const DevScene<typename ModeT<MODE>::T> P, uint32_t nq, const void* __restrict__ qx,
                 const void* __restrict__ qp, const void* __restrict__ qc,
                 RefineEntry<typename ModeT<MODE>::T>* refq, ResumeEntry<typename ModeT<MODE>::T>* resq,
@@ -276,7 +282,7 @@ __global__ void __launch_bounds__(kIntegrateThreads, 2)
 
         // ---- one RKF45 attempt per live lane
         uint32_t cls = MGK_RAY_ALIVE;
-        bool cross = false;
+        bool cross = false, disk = false;
         S7<T> y0 = y;
         T h_used = h;
         if (alive && !to_band) {
@@ -291,7 +297,8 @@ __global__ void __launch_bounds__(kIntegrateThreads, 2)
                 ++steps; ++n_steps;
                 y = y1;
                 T r2 = radius2<F>(y1);
-                cross = disk_candidate<F, T>(P, y0, y1) || r2 >= P.escape_r2;
+                disk = disk_candidate<F, T>(P, y0, y1);
+                cross = disk || r2 >= P.escape_r2;
                 if (!cross) {
                     cls = plain_terminal<METRIC, F, T>(P, y1, r2, steps);
                     if constexpr (MODE == MGK_PRECISION_MIXED && METRIC != MGK_METRIC_MINKOWSKI) {
@@ -301,8 +308,12 @@ __global__ void __launch_bounds__(kIntegrateThreads, 2)
             }
         }
 
-        // ---- compaction of the hand-offs
-        uint32_t slot = warp_push(cross, &cnt->refine_count, nq, &cnt->status);
+        // ---- compaction of the hand-offs: disk candidates fill the crossing
+        // queue from the front, escapes from the back, so that the crossing
+        // kernel's warps see one kind (escapes take one sub-step, disks iterate)
+        uint32_t slot = warp_push(cross && disk, &cnt->refine_count, nq, &cnt->status);
+        uint32_t eslot = warp_push(cross && !disk, &cnt->escape_count, nq, &cnt->status);
+        if (eslot != ~0u) slot = nq - 1u - eslot;
         if (slot != ~0u) {
             RefineEntry<T> e;
             e.y0[0] = y0.x; e.y0[1] = y0.y; e.y0[2] = y0.z; e.y0[3] = y0.t;
@@ -357,15 +368,18 @@ __global__ void __launch_bounds__(128, 4) k_refine(const DevScene<typename ModeT
                                                 Counters* cnt) {
     using T = typename ModeT<MODE>::T;
     constexpr Fuse F = ModeT<MODE>::F;
-    const uint32_t n = min(cnt->refine_count, cap);
+    const uint32_t nd = min(cnt->refine_count, cap);
+    const uint32_t n = min(nd + min(cnt->escape_count, cap), cap);
     unsigned long long n_evals = 0;
     uint32_t n_cls[5] = {0, 0, 0, 0, 0};
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t stride = gridDim.x * blockDim.x;
-    // warp-uniform trip count so the queue pushes can use warp ballots
+    // warp-uniform trip count so the queue pushes can use warp ballots;
+    // indices [0, nd) are the disk entries, the rest the escapes at the back
     for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += stride) {
-        const uint32_t i = base + lane;
-        const bool valid = i < n;
+        const uint32_t v = base + lane;
+        const bool valid = v < n;
+        const uint32_t i = v < nd ? v : cap - 1u - (v - nd);
         Term<T> t{MGK_RAY_ALIVE, T(0), T(0), T(0), T(0), T(0)};
         RefineEntry<T> e;
         S7<T> y1{}, ye{};
@@ -475,8 +489,12 @@ __global__ void __launch_bounds__(128, 4) k_tail(const DevScene<typename ModeT<M
 
 // ------------------------------------------------------------------ shade
 // One thread per hit (a warp shades 32 hits at once, so the dependent loads of
-// the entry, the star cell and the stars overlap across lanes).  The bin
-// wavelengths and XYZ weights are staged in shared memory.
+// the entry, the star cell and the stars overlap across lanes).  The boosted
+// blackbody I(lambda_obs) = B(z lambda_obs, T) z^5 is evaluated as
+//   a_k / (exp(b_k / (z T)) - 1),  a_k = 2 h c^2 / lambda_k^5,  b_k = h c / (k_B lambda_k),
+// since the z^5 of the boost cancels the z^-5 of B at the shifted wavelength:
+// one exponential and one quotient per bin.  a_k, b_k and the XYZ weights are
+// staged in shared memory.
 template <class T>
 __global__ void __launch_bounds__(256) k_shade(const DevScene<T> P, const HitEntry<T>* __restrict__ hits,
                                                uint32_t cap, const Counters* cnt, const mgk_star* __restrict__ stars,
@@ -484,27 +502,33 @@ __global__ void __launch_bounds__(256) k_shade(const DevScene<T> P, const HitEnt
                                                float* __restrict__ xyz_ray, float* __restrict__ film_spec,
                                                uint64_t first_ray) {
     __shared__ float sw[3 * MGK_MAX_BINS];
-    __shared__ T slam[MGK_MAX_BINS];
+    __shared__ T sa[MGK_MAX_BINS], sb[MGK_MAX_BINS];
     const uint32_t nb = P.n_bins;
     for (uint32_t i = threadIdx.x; i < 3 * MGK_MAX_BINS; i += blockDim.x)
         sw[i] = i < 3 * nb ? (d_w ? d_w[i] : P.xyz_w[i]) : 0.f;
-    for (uint32_t i = threadIdx.x; i < MGK_MAX_BINS; i += blockDim.x) slam[i] = P.lambda[i];
+    for (uint32_t i = threadIdx.x; i < MGK_MAX_BINS; i += blockDim.x) {
+        sa[i] = P.planck_a[i];
+        sb[i] = P.planck_b[i];
+    }
     __syncthreads();
     const uint32_t n = min(cnt->hit_count, cap);
     for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
         const HitEntry<T> h = hits[e];
-        const T z = h.z, z2 = z * z, z5 = z2 * z2 * z;
         float X = 0.f, Y = 0.f, Z = 0.f;
         float* spec = film_spec ? film_spec + ((first_ray + h.ray) / P.spp) * nb : nullptr;
-        if (h.cls == MGK_RAY_DISK) {
-            const T temp = P.disk_T_in * T(pow(double(h.r_hit / P.disk_r_in), -0.75));
+        auto add = [&](T amp, T temp) {
+            const T u = T(1) / (h.z * temp);
             for (uint32_t k = 0; k < nb; ++k) {
-                float sv = float(clamp_radiance<T>(planck<T>(z * slam[k], temp) * z5));
+                float sv = float(clamp_radiance<T>(amp * (sa[k] / (exp(sb[k] * u) - T(1)))));
                 X = __fmaf_rn(sv, sw[3 * k], X);
                 Y = __fmaf_rn(sv, sw[3 * k + 1], Y);
                 Z = __fmaf_rn(sv, sw[3 * k + 2], Z);
                 if (spec) atomicAdd(spec + k, sv * P.inv_spp);
             }
+        };
+        if (h.cls == MGK_RAY_DISK) {
+            // T(r) = T_in (r / r_in)^(-3/4)
+            add(T(1), P.disk_T_in * exp2(T(-0.75) * log2(h.r_hit / P.disk_r_in)));
         } else if (grid.n != 0u) {
             const uint32_t cell = cube_cell(float(h.d0), float(h.d1), float(h.d2), grid.n);
             const uint32_t j1 = grid.cell_start[cell + 1];
@@ -513,15 +537,7 @@ __global__ void __launch_bounds__(256) k_shade(const DevScene<T> P, const HitEnt
                 T dx = h.d0 - T(st.dir[0]), dy = h.d1 - T(st.dir[1]), dz = h.d2 - T(st.dir[2]);
                 T q = mad<Fuse::Fma>(dz, dz, mad<Fuse::Fma>(dy, dy, dx * dx)) * P.star_inv_r2;
                 if (q >= T(1)) continue;
-                const T amp = T(st.amplitude) * ((T(1) - q) * (T(1) - q));
-                const T ts = T(st.temperature);
-                for (uint32_t k = 0; k < nb; ++k) {
-                    float sv = float(clamp_radiance<T>(amp * planck<T>(z * slam[k], ts) * z5));
-                    X = __fmaf_rn(sv, sw[3 * k], X);
-                    Y = __fmaf_rn(sv, sw[3 * k + 1], Y);
-                    Z = __fmaf_rn(sv, sw[3 * k + 2], Z);
-                    if (spec) atomicAdd(spec + k, sv * P.inv_spp);
-                }
+                add(T(st.amplitude) * ((T(1) - q) * (T(1) - q)), T(st.temperature));
             }
         }
         xyz_ray[3 * size_t(h.ray) + 0] = X;
@@ -816,7 +832,15 @@ template <class T> static void fill_t(const mgk_scene& s, const float* xyz_w, De
     T rr = T(s.star_radius_rad);
     P->star_inv_r2 = T(1) / (rr * rr);
     double dl = (s.lambda_max_nm - s.lambda_min_nm) / s.n_bins;
-    for (uint32_t k = 0; k < s.n_bins && k < MGK_MAX_BINS; ++k) P->lambda[k] = T(s.lambda_min_nm + (k + 0.5) * dl);
+    for (uint32_t k = 0; k < s.n_bins && k < MGK_MAX_BINS; ++k) {
+        const double lam = s.lambda_min_nm + (k + 0.5) * dl;
+        P->lambda[k] = T(lam);
+        // boosted blackbody a_k / (exp(b_k / (z T)) - 1), internal_math.h:2511-2526 with the
+        // wavelength in metres
+        const double h = 6.62607015E-34, c = 299792458.0, kb = 1.380649E-23, wl = lam * 1e-9;
+        P->planck_a[k] = T(2.0 * h * c * c / (wl * wl * wl * wl * wl));
+        P->planck_b[k] = T(h * c / (wl * kb));
+    }
     for (uint32_t k = 0; k < 3 * s.n_bins && k < 3 * MGK_MAX_BINS; ++k) P->xyz_w[k] = xyz_w[k];
     P->seed = s.seed;
     P->width = s.width; P->height = s.height; P->spp = s.spp; P->n_bins = s.n_bins;

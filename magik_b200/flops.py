@@ -1,14 +1,15 @@
 """Algorithmic operation counts of the integrator, used for the roofline.
 
 Source-level counts (+, -, *, /, sqrt = 1; fused multiply-add = 2; pow = 1)
-of the formulation the kernels execute: the 7-component state (x, y, z, t,
+of the formulation the kernels execute (a division or a square root counts
+as one operation however it is implemented): the 7-component state (x, y, z, t,
 px, py, pz) with the conserved p_t carried beside it.  The CPU oracle counts
 the same expressions with an op-counting scalar (8 components, p_t included);
 tests/test_host.py checks that the figures below equal its counts minus the
 p_t work, which is identically zero and skipped by the kernels.
 
-  RHS                           Kerr 160   Schwarzschild 130 (the fused
-                                formulation: two reciprocals and six
+  RHS                           Kerr 162   Schwarzschild 132 (the fused
+                                formulation: one reciprocal and eight
                                 products in place of five quotients)
   one RKF45 attempt             6 RHS + 25 coefficient products + 210 stage
                                 combinations + 70 (5th-order solution)
@@ -16,7 +17,7 @@ p_t work, which is identically zero and skipped by the kernels.
   one crossing sub-step         6 RHS + 20 coefficient products + 210 + 70
 """
 
-RHS = {2: 160, 1: 130, 0: 0}
+RHS = {2: 162, 1: 132, 0: 0}
 ATTEMPT_OVERHEAD = 25 + 210 + 70 + 63 + 36 + 4
 SUBSTEP_OVERHEAD = 20 + 210 + 70
 # p_t terms the 8-component count includes and the kernels skip

@@ -17,7 +17,7 @@
 //                reference's expression order (what g++ emits for x86-64).
 //   Fuse::Fma  - the same expression tree with the multiply-add pairs marked
 //                by mad() fused into one correctly rounded fma(), and the
-//                five RHS quotients formed from two reciprocals.  The CUDA
+//                five RHS quotients formed from one reciprocal.  The CUDA
 //                kernels use the same tree with __fmaf_rn / __fma_rn at the
 //                same sites, so both sides round identically.
 // Build with -ffp-contract=off so the compiler adds no fusion of its own.
@@ -72,10 +72,12 @@ template <Fuse F, class T> inline GState<T> rhs_kerr(const GState<T>& s, T a) {
     T f_den = mad<F>(a_sq, y_sq, r_quad);
     T inv_r, inv_sigma, inv_d, inv_f_den_sq, f_;
     if constexpr (F == Fuse::Fma) {
-        // fused formulation: 1/(r sigma d) and 1/f_den give all five quotients
+        // fused formulation: 1/(r sigma d f_den) gives all five quotients
         T rs = r * sigma;
-        T inv_rsd = one / (rs * d);
-        T inv_fden = one / f_den;
+        T rsd = rs * d;
+        T inv_all = one / (rsd * f_den);  // ~r^9: finite for r below ~1.9e4 in float
+        T inv_rsd = f_den * inv_all;
+        T inv_fden = rsd * inv_all;
         inv_d = rs * inv_rsd;
         T inv_rs = d * inv_rsd;
         inv_r = sigma * inv_rs;
@@ -153,8 +155,10 @@ template <Fuse F, class T> inline GState<T> rhs_schwarzschild(const GState<T>& s
     T inv_r, inv_sigma, inv_d, inv_f_den_sq, f_;
     if constexpr (F == Fuse::Fma) {
         T rs = r * sigma;
-        T inv_rsd = one / (rs * d);
-        T inv_fden = one / f_den;
+        T rsd = rs * d;
+        T inv_all = one / (rsd * f_den);  // ~r^9: finite for r below ~1.9e4 in float
+        T inv_rsd = f_den * inv_all;
+        T inv_fden = rsd * inv_all;
         inv_d = rs * inv_rsd;
         T inv_rs = d * inv_rsd;
         inv_r = sigma * inv_rs;
@@ -436,6 +440,39 @@ inline void control_f64(const GState<double>& y0, const GState<double>& y1, cons
     *ok = safe < 1.0;
 }
 
+// Reciprocal for the MIXED norm: integer seed 0x7EF311C3 - bits(x) and two
+// Newton steps with fma (identical to the kernels' rcp_norm).
+inline float rcp_norm(float x) {
+    uint32_t b;
+    std::memcpy(&b, &x, 4);
+    b = 0x7EF311C3u - b;
+    float y;
+    std::memcpy(&y, &b, 4);
+    y = y * std::fma(-x, y, 2.0f);
+    y = y * std::fma(-x, y, 2.0f);
+    return y;
+}
+
+// MIXED RMS norm (relativity_utilities.cuh:15-29 with e_i / scale_i formed as
+// e_i * rcp_norm(scale_i)); component order t, x, y, z, then momentum.
+inline float rms_error_mixed(const GState<float>& e, const GState<float>& y0, const GState<float>& y1, float atol,
+                             float rtol) {
+    auto term = [&](float ei, float a0, float a1) {
+        return ei * rcp_norm(std::fma(rtol, std::fmax(std::fabs(a0), std::fabs(a1)), atol));
+    };
+    float s0 = term(e.x.t, y0.x.t, y1.x.t), s1 = term(e.x.x, y0.x.x, y1.x.x), s2 = term(e.x.y, y0.x.y, y1.x.y);
+    float s3 = term(e.x.z, y0.x.z, y1.x.z);
+    float s5 = term(e.p.x, y0.p.x, y1.p.x), s6 = term(e.p.y, y0.p.y, y1.p.y), s7 = term(e.p.z, y0.p.z, y1.p.z);
+    float acc = s0 * s0;
+    acc = std::fma(s1, s1, acc);
+    acc = std::fma(s2, s2, acc);
+    acc = std::fma(s3, s3, acc);
+    acc = std::fma(s5, s5, acc);
+    acc = std::fma(s6, s6, acc);
+    acc = std::fma(s7, s7, acc);
+    return std::sqrt(acc / 8.0f);
+}
+
 // MIXED control: the error estimate in double from the float stages; its
 // norm and the proposal in float.
 inline void control_mixed(const GState<float>& y0, const GState<float>& y1, const GState<float> k[6], float h,
@@ -443,7 +480,7 @@ inline void control_mixed(const GState<float>& y0, const GState<float>& y1, cons
     GState<double> kd[6];
     for (int i = 0; i < 6; ++i) kd[i] = to_double(k[i]);
     GState<float> e = widen<float>(rkf45_error<Fuse::Fma, double>(double(h), kd));
-    float err = rms_error<Fuse::Fma, float>(e, y0, y1, m.abs_tol, m.rel_tol);
+    float err = rms_error_mixed(e, y0, y1, m.abs_tol, m.rel_tol);
     float safe = err > 1e-30f ? err : 1e-30f;
     float hn = (0.9f * h) * inv_root5(safe);
     if (hn > m.h_max) hn = m.h_max;
