@@ -231,7 +231,9 @@ MGK_API mgk_result mgk_shade_rays(mgk_context* ctx, const mgk_scene* s, const mg
                                   void* stream);
 
 /* ------------------------------------ reference-compatible trace API */
-/* Same types and layout as magik.h:583-648. */
+/* Same types and layout as magik.h:583-648; when the reference's magik.h is
+ * included first its declarations are used instead. */
+#ifndef MAGIK_H
 typedef enum e_mgk_test_particle_types { MGK_MASSIVE = 0, MGK_MASSLESS = 1 } e_mgk_test_particle_types;
 
 typedef struct magik_trace_geodesic_metric_parameters_t {
@@ -282,6 +284,7 @@ MGK_API int32_t magik_trace_geodesic(magik_trace_geodesic_container_t* container
                                      magik_trace_geodesic_inital_conditions_t initial_conditions,
                                      magik_trace_geodesic_metric_parameters_t metric_parameters,
                                      magik_trace_geodesic_integrator_parameters_t integrator_parameters);
+#endif /* MAGIK_H */
 
 /* Batch form: n geodesics, one container each, traced concurrently on the GPU
  * (one thread per geodesic). */

@@ -35,7 +35,7 @@ constexpr unsigned kFull = 0xffffffffu;
 #define MGK_INTEGRATE_THREADS 256
 #endif
 #ifndef MGK_INTEGRATE_MIN_BLOCKS
-#define MGK_INTEGRATE_MIN_BLOCKS 2
+#define MGK_INTEGRATE_MIN_BLOCKS 3
 #endif
 constexpr int kIntegrateThreads = MGK_INTEGRATE_THREADS;
 constexpr uint32_t kChunk = 64;  // queue entries a warp takes per refill
