@@ -224,6 +224,22 @@ MGK_API mgk_result mgk_render_host(mgk_context* ctx, const mgk_scene* s, const m
 MGK_API mgk_result mgk_trace_rays(mgk_context* ctx, const mgk_scene* s, uint64_t first_ray, uint32_t n_rays,
                                   mgk_ray_result* d_out, void* stream);
 
+/* mgk_trace_rays without any device allocation (no counterpart in the
+ * reference).  For callers that cannot call cudaMalloc once running: a host
+ * application that gives the renderer a fixed share of the GPU and forbids
+ * later allocations, or an interactive loop that cannot take the device-wide
+ * synchronisation cudaMalloc / cudaFree may cause.  No context is needed: the
+ * scratch is a file-scope __device__ array of 8 MiB inside the library, held
+ * by every device that loads the library until the process exits.  At most
+ * MGK_STATIC_MAX_RAYS rays per call (more returns MGK_ERROR_INVALID_ARGUMENT).
+ * Runs on the current device; its first call there looks up the array's
+ * device address (cudaGetSymbolAddress) and should come before any stream
+ * capture.  All calls share the array: calls whose work overlaps on the GPU
+ * race, so issue them on one stream.  d_out as for mgk_trace_rays. */
+#define MGK_STATIC_MAX_RAYS 16384
+MGK_API mgk_result mgk_trace_rays_static(const mgk_scene* s, uint64_t first_ray, uint32_t n_rays,
+                                         mgk_ray_result* d_out, void* stream);
+
 /* Per-ray spectra -> XYZ of camera rays [first_ray, first_ray + n_rays):
  * 3 floats per ray into d_xyz (device).  For parity tests of the shading. */
 MGK_API mgk_result mgk_shade_rays(mgk_context* ctx, const mgk_scene* s, const mgk_star* d_stars, uint32_t n_stars,

@@ -32,6 +32,7 @@ EXPORTS = [
     "mgk_context_create", "mgk_context_destroy", "mgk_last_error", "mgk_scene_defaults", "mgk_isco_radius",
     "mgk_xyz_weights", "mgk_star_catalog", "mgk_scene_constants", "mgk_render", "mgk_render_host",
     "mgk_trace_rays", "mgk_shade_rays", "magik_trace_geodesic", "mgk_trace_geodesic_batch", "mgk_fp32_peak",
+    "mgk_trace_rays_static",
 ]
 
 
@@ -71,6 +72,7 @@ def lib():
         L.mgk_trace_geodesic_batch.argtypes = [vp, P(abi.TraceContainer), P(abi.TraceInitialConditions),
                                                P(abi.TraceMetricParams), P(abi.TraceIntegratorParams), C.c_uint32]
         L.mgk_fp32_peak.argtypes = [vp, P(C.c_double)]
+        L.mgk_trace_rays_static.argtypes = [P(Scene), C.c_uint64, C.c_uint32, vp, vp]
         for name in EXPORTS:
             fn = getattr(L, name)
             if fn.restype is C.c_int:  # ctypes default
@@ -226,6 +228,16 @@ class Context:
             a = np.frombuffer(steps[i], dtype=np.float32).reshape(n_steps, 15)
             out.append(a[: cs[i].n_written].copy())
         return out
+
+
+STATIC_MAX_RAYS = 16384
+
+
+def trace_rays_static(scene, first, n, d_out, stream=None):
+    """mgk_trace_rays_static: traces camera rays [first, first+n) into the CUDA
+    buffer d_out (n * 128 bytes) with no device allocation; n <= 16384."""
+    _check(lib().mgk_trace_rays_static(C.byref(scene), first, n, d_out.data_ptr(), _stream_ptr(stream)),
+           "mgk_trace_rays_static")
 
 
 def trace_geodesic(ic, mp, ip, n_steps=4096):

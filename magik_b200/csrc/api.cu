@@ -396,6 +396,11 @@ mgk_context* g_default[64] = {};
 
 }  // namespace
 
+namespace mgk {
+// Scene checks shared with the allocation-free entry point (static_scratch.cu).
+mgk_result validate_scene(const mgk_scene* s) { return validate(s); }
+}  // namespace mgk
+
 // ====================================================================== ABI
 extern "C" {
 
