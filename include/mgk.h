@@ -160,6 +160,8 @@ typedef struct mgk_render_stats {
     double total_ms;          /* device time of the whole render */
     uint64_t crossings;       /* steps handed to the crossing kernel */
     uint64_t resumed;         /* rays continued by the tail kernel */
+    uint64_t fallback_rays;   /* surrogate renders: rays routed to RKF45 */
+    double surrogate_ms;      /* surrogate renders: device time of network + routing */
 } mgk_render_stats;
 
 typedef struct mgk_context mgk_context;
@@ -245,6 +247,76 @@ MGK_API mgk_result mgk_trace_rays_static(const mgk_scene* s, uint64_t first_ray,
 MGK_API mgk_result mgk_shade_rays(mgk_context* ctx, const mgk_scene* s, const mgk_star* d_stars, uint32_t n_stars,
                                   const float* d_xyz_w, uint64_t first_ray, uint32_t n_rays, float* d_xyz,
                                   void* stream);
+
+/* --------------------------------------------------- deflection surrogate */
+/* A learned stand-in for the integrator: an MLP 7 -> 256 -> 256 -> 256 -> 256 -> 8
+ * with SiLU activations, BF16 weights and activations, FP32 accumulation, run on
+ * tensor cores by the library's own forward / backward / Adam kernels.
+ * Inputs: [(r_obs - 55) / 45, cos i, sin i, 2 a / 0.998 - 1, n_x, n_y, n_z],
+ * with n the photon direction in the observer's frame.
+ * Outputs: [disk logit, escape logit (horizon logit 0), (r_hit - 10) / 10,
+ * disk redshift, escape direction (3), confidence logit].
+ * Rays with low confidence or near the critical curve go to RKF45. */
+typedef struct mgk_sample_label {
+    int32_t cls;    /* 0 disk, 1 escape, 2 dark */
+    float r;        /* (r_hit - 10) / 10 */
+    float g;        /* disk redshift factor */
+    float dir[3];   /* escape direction */
+    float reserved[2];
+} mgk_sample_label;
+
+typedef struct mgk_train_config {
+    uint32_t batch;          /* samples per step, multiple of 1024 (65536) */
+    uint32_t epochs;         /* passes over the sample set (20) */
+    float lr, beta1, beta2, eps;  /* Adam (1e-3, 0.9, 0.999, 1e-8) */
+    uint64_t seed;           /* shuffling */
+    float w_cls, w_r, w_g, w_dir, w_conf;  /* loss weights */
+    float tol_r, tol_g, tol_dir;           /* confidence target: prediction within these */
+} mgk_train_config;
+
+typedef struct mgk_surrogate mgk_surrogate;
+
+MGK_API void mgk_train_defaults(mgk_train_config* c);
+/* Number of FP32 parameters (with the padding of the first and last layer). */
+MGK_API uint64_t mgk_surrogate_param_count(void);
+/* Creates a network with seeded uniform initial weights on the context's device. */
+MGK_API mgk_result mgk_surrogate_create(mgk_context* ctx, uint64_t seed, mgk_surrogate** out);
+MGK_API mgk_result mgk_surrogate_destroy(mgk_surrogate* net);
+MGK_API mgk_result mgk_surrogate_get_params(mgk_surrogate* net, float* h_params);
+MGK_API mgk_result mgk_surrogate_set_params(mgk_surrogate* net, const float* h_params);
+/* n training samples (features n x 7, labels n) traced by the F64 integrator.
+ * n_spin_buckets == 0: camera rays of `base` (its observer, spin and field of
+ *   view), from frames seeded seed, seed + 1, ... - a surrogate for one view.
+ * n_spin_buckets >= 1: observers uniform in r [10, 100] M and inclination
+ *   [0, 90] deg, directions uniform on the camera's forward hemisphere, spins
+ *   uniform in [0, 0.998] over the buckets (base.spin for one bucket), disk
+ *   r_in at the ISCO of each spin; needs base->escape_radius >= 100.
+ * The metric, disk, escape radius and tolerances come from `base`. */
+MGK_API mgk_result mgk_make_samples(mgk_context* ctx, const mgk_scene* base, uint64_t seed, uint32_t n,
+                                    uint32_t n_spin_buckets, float* d_features, mgk_sample_label* d_labels,
+                                    void* stream);
+/* Forward pass: d_out receives 16 floats per sample (8 outputs + padding). */
+MGK_API mgk_result mgk_surrogate_forward(mgk_surrogate* net, const float* d_features, uint32_t n, float* d_out,
+                                         void* stream);
+/* Loss and gradient of one batch (n a multiple of 1024) into host memory
+ * (mgk_surrogate_param_count floats); synchronous. */
+MGK_API mgk_result mgk_surrogate_gradient(mgk_surrogate* net, const mgk_train_config* cfg, const float* d_features,
+                                          const mgk_sample_label* d_labels, uint32_t n, float* h_grad,
+                                          float* h_loss);
+/* Adam training over the sample set; h_epoch_loss (may be NULL) receives the
+ * mean batch loss of each epoch.  Synchronous. */
+MGK_API mgk_result mgk_surrogate_train(mgk_surrogate* net, const mgk_train_config* cfg, const float* d_features,
+                                       const mgk_sample_label* d_labels, uint32_t n, float* h_epoch_loss,
+                                       void* stream);
+/* mgk_render with the surrogate in front of the integrator: every camera ray
+ * goes through the network; rays whose confidence is below conf_min, or whose
+ * impact parameter lies within crit_frac of the critical curve, are
+ * integrated with RKF45 (the scene's precision); the rest are shaded from the
+ * network's outputs. */
+MGK_API mgk_result mgk_render_surrogate(mgk_context* ctx, mgk_surrogate* net, const mgk_scene* s,
+                                        const mgk_star* d_stars, uint32_t n_stars, const float* d_xyz_w,
+                                        float conf_min, float crit_frac, float* d_film_xyz,
+                                        mgk_render_stats* stats, void* stream);
 
 /* ------------------------------------ reference-compatible trace API */
 /* Same types and layout as magik.h:583-648; when the reference's magik.h is

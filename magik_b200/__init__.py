@@ -32,7 +32,9 @@ EXPORTS = [
     "mgk_context_create", "mgk_context_destroy", "mgk_last_error", "mgk_scene_defaults", "mgk_isco_radius",
     "mgk_xyz_weights", "mgk_star_catalog", "mgk_scene_constants", "mgk_render", "mgk_render_host",
     "mgk_trace_rays", "mgk_shade_rays", "magik_trace_geodesic", "mgk_trace_geodesic_batch", "mgk_fp32_peak",
-    "mgk_trace_rays_static",
+    "mgk_trace_rays_static", "mgk_train_defaults", "mgk_surrogate_param_count", "mgk_surrogate_create",
+    "mgk_surrogate_destroy", "mgk_surrogate_get_params", "mgk_surrogate_set_params", "mgk_make_samples",
+    "mgk_surrogate_forward", "mgk_surrogate_gradient", "mgk_surrogate_train", "mgk_render_surrogate",
 ]
 
 
@@ -73,6 +75,21 @@ def lib():
                                                P(abi.TraceMetricParams), P(abi.TraceIntegratorParams), C.c_uint32]
         L.mgk_fp32_peak.argtypes = [vp, P(C.c_double)]
         L.mgk_trace_rays_static.argtypes = [P(Scene), C.c_uint64, C.c_uint32, vp, vp]
+        L.mgk_train_defaults.argtypes = [P(abi.TrainConfig)]
+        L.mgk_train_defaults.restype = None
+        L.mgk_surrogate_param_count.argtypes = []
+        L.mgk_surrogate_param_count.restype = C.c_uint64
+        L.mgk_surrogate_create.argtypes = [vp, C.c_uint64, P(vp)]
+        L.mgk_surrogate_destroy.argtypes = [vp]
+        L.mgk_surrogate_get_params.argtypes = [vp, P(C.c_float)]
+        L.mgk_surrogate_set_params.argtypes = [vp, P(C.c_float)]
+        L.mgk_make_samples.argtypes = [vp, P(Scene), C.c_uint64, C.c_uint32, C.c_uint32, vp, vp, vp]
+        L.mgk_surrogate_forward.argtypes = [vp, vp, C.c_uint32, vp, vp]
+        L.mgk_surrogate_gradient.argtypes = [vp, P(abi.TrainConfig), vp, vp, C.c_uint32, P(C.c_float),
+                                             P(C.c_float)]
+        L.mgk_surrogate_train.argtypes = [vp, P(abi.TrainConfig), vp, vp, C.c_uint32, P(C.c_float), vp]
+        L.mgk_render_surrogate.argtypes = [vp, vp, P(Scene), vp, C.c_uint32, vp, C.c_float, C.c_float, vp,
+                                           P(RenderStats), vp]
         for name in EXPORTS:
             fn = getattr(L, name)
             if fn.restype is C.c_int:  # ctypes default
@@ -247,3 +264,105 @@ def trace_geodesic(ic, mp, ip, n_steps=4096):
     rc = lib().magik_trace_geodesic(C.byref(c), ic, mp, ip)
     a = np.frombuffer(steps, dtype=np.float32).reshape(n_steps, 15)
     return rc, a[: c.n_written].copy()
+
+
+# --------------------------------------------------------------- surrogate
+LABEL_DTYPE = np.dtype([("cls", "<i4"), ("r", "<f4"), ("g", "<f4"), ("dir", "<f4", (3,)),
+                        ("reserved", "<f4", (2,))])
+assert LABEL_DTYPE.itemsize == 32
+
+
+def train_defaults(**overrides):
+    c = abi.TrainConfig()
+    lib().mgk_train_defaults(C.byref(c))
+    for k, v in overrides.items():
+        setattr(c, k, v)
+    return c
+
+
+def surrogate_param_count():
+    return int(lib().mgk_surrogate_param_count())
+
+
+class Surrogate:
+    """The deflection surrogate network (mgk_surrogate) on a context's device."""
+
+    def __init__(self, ctx, seed=1):
+        h = C.c_void_p()
+        _check(lib().mgk_surrogate_create(ctx.handle, seed, C.byref(h)), "mgk_surrogate_create", ctx.handle)
+        self.handle = h
+        self.ctx = ctx
+
+    def close(self):
+        if self.handle:
+            lib().mgk_surrogate_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def get_params(self):
+        out = np.empty(surrogate_param_count(), np.float32)
+        _check(lib().mgk_surrogate_get_params(self.handle, out.ctypes.data_as(C.POINTER(C.c_float))),
+               "mgk_surrogate_get_params")
+        return out
+
+    def set_params(self, params):
+        a = np.ascontiguousarray(params, np.float32)
+        assert a.size == surrogate_param_count()
+        _check(lib().mgk_surrogate_set_params(self.handle, a.ctypes.data_as(C.POINTER(C.c_float))),
+               "mgk_surrogate_set_params")
+
+    def forward(self, d_feat, stream=None):
+        """d_feat: CUDA float32 [n, 7] -> CUDA float32 [n, 16]."""
+        import torch
+        n = d_feat.shape[0]
+        out = torch.empty((max(n, 1), 16), dtype=torch.float32, device=d_feat.device)
+        _check(lib().mgk_surrogate_forward(self.handle, d_feat.data_ptr(), n, out.data_ptr(), _stream_ptr(stream)),
+               "mgk_surrogate_forward")
+        return out[:n]
+
+    def gradient(self, cfg, d_feat, d_lab):
+        """Loss and gradient of one batch (host float32 vector)."""
+        g = np.empty(surrogate_param_count(), np.float32)
+        loss = C.c_float(0)
+        _check(lib().mgk_surrogate_gradient(self.handle, C.byref(cfg), d_feat.data_ptr(), d_lab.data_ptr(),
+                                            d_feat.shape[0], g.ctypes.data_as(C.POINTER(C.c_float)),
+                                            C.byref(loss)), "mgk_surrogate_gradient")
+        return float(loss.value), g
+
+    def train(self, cfg, d_feat, d_lab, stream=None):
+        """Adam training; returns the mean loss of each epoch."""
+        losses = np.zeros(max(cfg.epochs, 1), np.float32)
+        _check(lib().mgk_surrogate_train(self.handle, C.byref(cfg), d_feat.data_ptr(), d_lab.data_ptr(),
+                                         d_feat.shape[0], losses.ctypes.data_as(C.POINTER(C.c_float)),
+                                         _stream_ptr(stream)), "mgk_surrogate_train")
+        return losses[: cfg.epochs]
+
+
+def make_samples(ctx, base, seed, n, n_spin_buckets=0, stream=None):
+    """Training samples traced by the F64 integrator: (features [n, 7] float32,
+    labels [n, 8] int32/float32 view of mgk_sample_label) as CUDA tensors."""
+    import torch
+    dev = f"cuda:{ctx.device}"
+    feat = torch.empty((max(n, 1), 7), dtype=torch.float32, device=dev)
+    lab = torch.empty((max(n, 1), 8), dtype=torch.int32, device=dev)
+    _check(lib().mgk_make_samples(ctx.handle, C.byref(base), seed, n, n_spin_buckets, feat.data_ptr(),
+                                  lab.data_ptr(), _stream_ptr(stream)), "mgk_make_samples", ctx.handle)
+    return feat[:n], lab[:n]
+
+
+def render_surrogate(ctx, net, scene, d_stars, d_film_xyz, conf_min=0.99, crit_frac=0.02, d_weights=None,
+                     stream=None):
+    """mgk_render_surrogate; returns the RenderStats."""
+    n_stars = 0 if d_stars is None else d_stars.numel() * d_stars.element_size() // 32
+    st = RenderStats()
+    rc = lib().mgk_render_surrogate(ctx.handle, net.handle, C.byref(scene),
+                                    None if d_stars is None else d_stars.data_ptr(), n_stars,
+                                    None if d_weights is None else d_weights.data_ptr(), conf_min, crit_frac,
+                                    d_film_xyz.data_ptr(), C.byref(st), _stream_ptr(stream))
+    _check(rc, "mgk_render_surrogate", ctx.handle)
+    return st

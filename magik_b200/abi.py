@@ -64,7 +64,22 @@ class RenderStats(C.Structure):
                 ("wide_attempts", C.c_uint64), ("refine_evals", C.c_uint64),
                 ("class_count", C.c_uint64 * 5),
                 ("integrate_ms", C.c_double), ("total_ms", C.c_double), ("crossings", C.c_uint64),
-                ("resumed", C.c_uint64)]
+                ("resumed", C.c_uint64), ("fallback_rays", C.c_uint64), ("surrogate_ms", C.c_double)]
+
+
+class SampleLabel(C.Structure):
+    _fields_ = [("cls", C.c_int32), ("r", C.c_float), ("g", C.c_float), ("dir", C.c_float * 3),
+                ("reserved", C.c_float * 2)]
+
+
+class TrainConfig(C.Structure):
+    _fields_ = [("batch", C.c_uint32), ("epochs", C.c_uint32), ("lr", C.c_float), ("beta1", C.c_float),
+                ("beta2", C.c_float), ("eps", C.c_float), ("seed", C.c_uint64),
+                ("w_cls", C.c_float), ("w_r", C.c_float), ("w_g", C.c_float), ("w_dir", C.c_float),
+                ("w_conf", C.c_float), ("tol_r", C.c_float), ("tol_g", C.c_float), ("tol_dir", C.c_float)]
+
+
+assert C.sizeof(SampleLabel) == 32
 
 
 class TraceMetricParams(C.Structure):

@@ -397,6 +397,7 @@ mgk_context* g_default[64] = {};
 }  // namespace
 
 namespace mgk {
+int context_device(mgk_context* ctx) { return ctx->device; }
 // Scene checks shared with the allocation-free entry point (static_scratch.cu).
 mgk_result validate_scene(const mgk_scene* s) { return validate(s); }
 }  // namespace mgk
@@ -783,6 +784,225 @@ MGK_API int32_t magik_trace_geodesic(magik_trace_geodesic_container_t* container
     mgk_result rc = mgk_trace_geodesic_batch(ctx, container, &ic, &mp, &ip, 1);
     if (rc == MGK_ERROR_INVALID_ARGUMENT || rc == MGK_ERROR_UNKNOWN) return MGK_ERROR_UNKNOWN;
     return rc;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------- surrogate
+namespace {
+
+constexpr uint32_t kSampleChunk = 1u << 22;
+constexpr uint32_t kRouteBatch = 1u << 20;
+
+ChunkBuffers chunk_buffers(void* A, const Layout& L, Counters* cnt) {
+    ChunkBuffers B;
+    B.qx = at<void>(A, L.qx);
+    B.qp = at<void>(A, L.qp);
+    B.qc = at<void>(A, L.qc);
+    B.hits = at<void>(A, L.hits);
+    B.refine = at<void>(A, L.refine);
+    B.resume = at<void>(A, L.resume);
+    B.xyz_ray = at<float>(A, L.xyz);
+    B.counters = cnt;
+    return B;
+}
+
+}  // namespace
+
+extern "C" {
+
+MGK_API mgk_result mgk_make_samples(mgk_context* ctx, const mgk_scene* base, uint64_t seed, uint32_t n,
+                                    uint32_t n_spin_buckets, float* d_feat, mgk_sample_label* d_lab, void* stream) {
+    if (!ctx || !base || !d_feat || !d_lab) return MGK_ERROR_INVALID_POINTER;
+    if (n == 0) return MGK_SUCCESS;
+    mgk_scene s0 = *base;
+    s0.precision = MGK_PRECISION_F64;
+    mgk_result rc = validate(&s0);
+    if (rc != MGK_SUCCESS) return rc;
+    if (n_spin_buckets > 1024 || (n_spin_buckets && s0.escape_radius < 100.0)) return MGK_ERROR_INVALID_ARGUMENT;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    MGK_CUDA(ctx, cudaSetDevice(ctx->device));
+    const uint32_t chunk = std::min(n, kSampleChunk);
+    Layout L = make_layout(s0, chunk, 1, 0, 8);
+    const size_t res_off = align_up(L.total, 256);
+    rc = ensure_arena(ctx, res_off + size_t(chunk) * sizeof(mgk_ray_result));
+    if (rc != MGK_SUCCESS) return rc;
+    void* A = ctx->arena;
+    Counters* cnt = at<Counters>(A, L.counters);
+    mgk_ray_result* res = at<mgk_ray_result>(A, res_off);
+    std::vector<float> w(3 * MGK_MAX_BINS, 0.f);
+    alignas(16) unsigned char table[sizeof(DevScene<double>)];
+    const uint64_t frame_rays = uint64_t(s0.width) * s0.height * s0.spp;
+    const uint32_t nb = n_spin_buckets ? n_spin_buckets : 1;
+    uint32_t status = 0;
+    for (uint32_t k = 0; k < nb; ++k) {
+        const uint32_t lo = uint32_t(uint64_t(n) * k / nb), hi = uint32_t(uint64_t(n) * (k + 1) / nb);
+        mgk_scene s = s0;
+        if (n_spin_buckets > 1) s.spin = 0.998 * double(k) / double(nb - 1);
+        if (n_spin_buckets) s.disk_r_in = mgk_isco_radius(s.spin);
+        if (s.disk_r_in >= s.disk_r_out) return MGK_ERROR_INVALID_ARGUMENT;
+        for (uint32_t j = lo; j < hi;) {
+            uint32_t m = std::min(chunk, hi - j);
+            uint64_t first = j;
+            if (!n_spin_buckets) {  // camera rays of frame j / frame_rays
+                s.seed = seed + j / frame_rays;
+                first = j % frame_rays;
+                m = uint32_t(std::min<uint64_t>(m, frame_rays - first));
+            }
+            fill_dev_scene(s, w.data(), table);
+            ChunkBuffers B = chunk_buffers(A, L, cnt);
+            MGK_CUDA(ctx, cudaMemsetAsync(cnt, 0, sizeof(Counters), st));
+            if (n_spin_buckets) {
+                MGK_CUDA(ctx, launch_generate_samples(s, table, seed, j, m, B, d_feat + size_t(j) * 7, st));
+            } else {
+                MGK_CUDA(ctx, launch_generate(s, table, first, m, B, st));
+                MGK_CUDA(ctx, launch_camera_features(s, table, first, m, B, d_feat + size_t(j) * 7, st));
+            }
+            MGK_CUDA(ctx, launch_integrate(s, table, first, m, B, res, ctx->sm_count, st));
+            MGK_CUDA(ctx, launch_labels(res, m, d_lab + j, st));
+            Counters h;
+            MGK_CUDA(ctx, cudaMemcpyAsync(&h, cnt, sizeof(h), cudaMemcpyDeviceToHost, st));
+            MGK_CUDA(ctx, cudaStreamSynchronize(st));
+            status |= h.status;
+            j += m;
+        }
+    }
+    if (status) {
+        ctx->last_error = "queue overflow reported by the integrator";
+        return MGK_ERROR_DEVICE_STATUS;
+    }
+    return MGK_SUCCESS;
+}
+
+MGK_API mgk_result mgk_render_surrogate(mgk_context* ctx, mgk_surrogate* net, const mgk_scene* sp,
+                                        const mgk_star* d_stars, uint32_t n_stars, const float* d_w, float conf_min,
+                                        float crit_frac, float* film, mgk_render_stats* stats, void* stream) {
+    if (!ctx || !net || !sp || !film) return MGK_ERROR_INVALID_POINTER;
+    const mgk_scene& s = *sp;
+    mgk_result rc = validate(&s);
+    if (rc != MGK_SUCCESS) return rc;
+    if (s.precision == MGK_PRECISION_REF32) return MGK_ERROR_INVALID_ARGUMENT;
+    if (n_stars && !d_stars) return MGK_ERROR_INVALID_POINTER;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    MGK_CUDA(ctx, cudaSetDevice(ctx->device));
+    const uint64_t n = uint64_t(s.width) * s.height * s.spp;
+    uint32_t chunk = kMaxChunkRays / s.spp * s.spp;
+    if (chunk == 0) return MGK_ERROR_INVALID_ARGUMENT;
+    if (n < chunk) chunk = uint32_t(n);
+    const uint32_t n_chunks = uint32_t((n + chunk - 1) / chunk);
+    const uint32_t gn = grid_n(s.star_radius_rad);
+    Layout L = make_layout(s, chunk, n_chunks, n_stars, gn);
+    const size_t T = s.precision == MGK_PRECISION_F64 ? 8 : 4;
+    const size_t fq_off = align_up(L.total, 256);
+    const size_t ids_off = align_up(fq_off + size_t(chunk) * 9 * T, 256);
+    const size_t feat_off = align_up(ids_off + size_t(chunk) * 4, 256);
+    const size_t out_off = align_up(feat_off + size_t(kRouteBatch) * 7 * 4, 256);
+    rc = ensure_arena(ctx, out_off + size_t(kRouteBatch) * 16 * 4);
+    if (rc != MGK_SUCCESS) return rc;
+    void* A = ctx->arena;
+    std::vector<float> w(3 * MGK_MAX_BINS, 0.f);
+    if (!d_w) mgk_xyz_weights(s.n_bins, s.lambda_min_nm, s.lambda_max_nm, w.data());
+    alignas(16) unsigned char table[sizeof(DevScene<double>)];
+    fill_dev_scene(s, w.data(), table);
+
+    StarGridDev grid{nullptr, nullptr, 0};
+    if (n_stars) {
+        const uint32_t cells = 6 * gn * gn;
+        uint32_t* counts = at<uint32_t>(A, L.g_counts);
+        uint32_t* start = at<uint32_t>(A, L.g_start);
+        uint32_t* cursor = at<uint32_t>(A, L.g_cursor);
+        uint32_t* list = at<uint32_t>(A, L.g_list);
+        MGK_CUDA(ctx, cudaMemsetAsync(counts, 0, size_t(cells) * 4, st));
+        MGK_CUDA(ctx, cudaMemsetAsync(cursor, 0, size_t(cells) * 4, st));
+        float rad = float(s.star_radius_rad);
+        k_grid_count<<<(n_stars + 255) / 256, 256, 0, st>>>(d_stars, n_stars, rad, gn, counts);
+        k_grid_scan<<<1, 1024, 0, st>>>(counts, cells, start);
+        k_grid_fill<<<(n_stars + 255) / 256, 256, 0, st>>>(d_stars, n_stars, rad, gn, start, cursor, list);
+        k_grid_sort<<<(cells + 255) / 256, 256, 0, st>>>(start, cells, list);
+        MGK_CUDA(ctx, cudaGetLastError());
+        grid = StarGridDev{start, list, gn};
+    }
+    while (ctx->events.size() < 4 * size_t(n_chunks) + 2) {
+        cudaEvent_t e;
+        MGK_CUDA(ctx, cudaEventCreate(&e));
+        ctx->events.push_back(e);
+    }
+    Counters* cnt_all = at<Counters>(A, L.counters);
+    MGK_CUDA(ctx, cudaMemsetAsync(cnt_all, 0, size_t(n_chunks) * sizeof(Counters), st));
+    MGK_CUDA(ctx, cudaEventRecord(ctx->events[0], st));
+    std::vector<Counters> h(n_chunks);
+    for (uint32_t c = 0; c < n_chunks; ++c) {
+        const uint64_t b = uint64_t(c) * chunk;
+        const uint32_t m = uint32_t(std::min<uint64_t>(chunk, n - b));
+        ChunkBuffers B = chunk_buffers(A, L, cnt_all + c);
+        void* fq = at<void>(A, fq_off);
+        uint32_t* ids = at<uint32_t>(A, ids_off);
+        float* feat = at<float>(A, feat_off);
+        float* out = at<float>(A, out_off);
+        cudaEvent_t* ev = &ctx->events[2 + 4 * c];
+        MGK_CUDA(ctx, launch_generate(s, table, b, m, B, st));
+        MGK_CUDA(ctx, cudaEventRecord(ev[0], st));
+        for (uint32_t r0 = 0; r0 < m; r0 += kRouteBatch) {
+            const uint32_t k = std::min(kRouteBatch, m - r0);
+            MGK_CUDA(ctx, launch_camera_features(s, table, b + r0, k, B, feat, st));
+            MGK_CUDA(ctx, surrogate_infer(net, feat, k, out, st));
+            MGK_CUDA(ctx, launch_route(s, table, r0, k, m, out, conf_min, crit_frac, B, ids, fq, st));
+        }
+        MGK_CUDA(ctx, cudaEventRecord(ev[1], st));
+        Counters hc;
+        MGK_CUDA(ctx, cudaMemcpyAsync(&hc, cnt_all + c, sizeof(hc), cudaMemcpyDeviceToHost, st));
+        MGK_CUDA(ctx, cudaStreamSynchronize(st));
+        const uint32_t nf = std::min(hc.fallback_count, m);
+        ChunkBuffers F = B;
+        F.qx = fq;
+        F.qp = static_cast<char*>(fq) + size_t(m) * 4 * T;
+        F.qc = static_cast<char*>(fq) + size_t(m) * 8 * T;
+        F.ray_ids = ids;
+        F.hit_cap = m;
+        MGK_CUDA(ctx, cudaEventRecord(ev[2], st));
+        MGK_CUDA(ctx, launch_integrate(s, table, b, nf, F, nullptr, ctx->sm_count, st));
+        MGK_CUDA(ctx, cudaEventRecord(ev[3], st));
+        MGK_CUDA(ctx, cudaMemsetAsync(B.xyz_ray, 0, size_t(m) * 12, st));
+        MGK_CUDA(ctx, launch_shade(s, table, b, m, B, d_stars, grid, d_w, nullptr, ctx->sm_count, st));
+        MGK_CUDA(ctx, launch_resolve(s, b / s.spp, m / s.spp, B.xyz_ray, film, st));
+    }
+    MGK_CUDA(ctx, cudaEventRecord(ctx->events[1], st));
+    MGK_CUDA(ctx, cudaMemcpyAsync(h.data(), cnt_all, n_chunks * sizeof(Counters), cudaMemcpyDeviceToHost, st));
+    MGK_CUDA(ctx, cudaStreamSynchronize(st));
+    uint32_t status = 0;
+    for (auto& k : h) status |= k.status;
+    if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        stats->rays = n;
+        for (auto& k : h) {
+            stats->attempts += k.attempts;
+            stats->steps += k.steps;
+            stats->wide_attempts += k.wide_attempts;
+            stats->refine_evals += k.refine_evals;
+            stats->crossings += k.refine_count + k.escape_count;
+            stats->resumed += k.resume_count;
+            stats->fallback_rays += k.fallback_count;
+            for (int i = 0; i < 5; ++i) stats->class_count[i] += k.class_count[i];
+        }
+        float ms = 0.f;
+        MGK_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->events[0], ctx->events[1]));
+        stats->total_ms = ms;
+        double im = 0.0, sm = 0.0;
+        for (uint32_t c = 0; c < n_chunks; ++c) {
+            cudaEvent_t* ev = &ctx->events[2 + 4 * c];
+            MGK_CUDA(ctx, cudaEventElapsedTime(&ms, ev[0], ev[1]));
+            sm += ms;
+            MGK_CUDA(ctx, cudaEventElapsedTime(&ms, ev[2], ev[3]));
+            im += ms;
+        }
+        stats->integrate_ms = im;
+        stats->surrogate_ms = sm;
+    }
+    if (status) {
+        ctx->last_error = "queue overflow reported by the integrator";
+        return MGK_ERROR_DEVICE_STATUS;
+    }
+    return MGK_SUCCESS;
 }
 
 }  // extern "C"

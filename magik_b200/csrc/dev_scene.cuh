@@ -192,6 +192,7 @@ template <class T> struct DevScene {
     float xyz_w[3 * MGK_MAX_BINS];
     uint64_t seed;
     uint32_t width, height, spp, n_bins, max_steps, disk_on;
+    int32_t metric;
     float inv_spp;
 };
 

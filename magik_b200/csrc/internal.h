@@ -22,6 +22,8 @@ struct Counters {
     uint32_t escape_count;  // escape-crossing entries (from the back of the crossing queue)
     uint32_t resume_count;  // entries in the resume queue
     uint32_t status;        // 0 = ok; bit 0: a queue overflowed
+    uint32_t fallback_count;  // surrogate renders: rays routed to RKF45
+    uint32_t pad;
 };
 
 // Hit-queue entry (disk and sky rays; dark rays are not queued).
@@ -59,6 +61,8 @@ struct ChunkBuffers {
     void* resume;          // ResumeEntry<T>[n]
     float* xyz_ray;        // 3 floats per ray
     Counters* counters;
+    const uint32_t* ray_ids = nullptr;  // queue position -> ray index (null: identity)
+    uint32_t hit_cap = 0;               // hit-queue capacity (0: the launch's ray count)
 };
 
 struct StarGridDev {
@@ -77,6 +81,18 @@ cudaError_t launch_shade(const mgk_scene& s, const void* dev_scene, uint64_t fir
                          float* film_spectral, int sm_count, cudaStream_t stream);
 cudaError_t launch_resolve(const mgk_scene& s, uint64_t first_pixel, uint32_t n_pixels, const float* xyz_ray,
                            float* film_xyz, cudaStream_t stream);
+// Surrogate support (kernels.cu).
+cudaError_t launch_generate_samples(const mgk_scene& s, const void* dev_scene, uint64_t seed, uint32_t first,
+                                    uint32_t n, const ChunkBuffers& b, float* feat, cudaStream_t stream);
+cudaError_t launch_labels(const mgk_ray_result* res, uint32_t n, void* labels, cudaStream_t stream);
+cudaError_t launch_camera_features(const mgk_scene& s, const void* dev_scene, uint64_t first_ray, uint32_t n,
+                                   const ChunkBuffers& b, float* feat, cudaStream_t stream);
+cudaError_t launch_route(const mgk_scene& s, const void* dev_scene, uint32_t base, uint32_t n, uint32_t cap,
+                         const float* out, float conf_min, float crit_frac, const ChunkBuffers& b,
+                         uint32_t* fallback_ids, void* fallback_q, cudaStream_t stream);
+// Inference of the surrogate network (surrogate.cu): 16 floats per row of out.
+cudaError_t surrogate_infer(mgk_surrogate* net, const float* feat, uint32_t n, float* out, cudaStream_t stream);
+int context_device(mgk_context* ctx);
 cudaError_t launch_fma_probe(uint32_t blocks, uint32_t iters, float* sink, cudaStream_t stream);
 cudaError_t launch_trace_geodesic(const void* jobs, uint32_t n, void* steps, uint32_t* written, cudaStream_t stream);
 

@@ -214,7 +214,7 @@ __global__ void __launch_bounds__(kIntegrateThreads, MGK_INTEGRATE_MIN_BLOCKS)
     k_integrate(const DevScene<typename ModeT<MODE>::T> P, uint32_t nq, const void* __restrict__ qx,
                 const void* __restrict__ qp, const void* __restrict__ qc,
                 RefineEntry<typename ModeT<MODE>::T>* refq, ResumeEntry<typename ModeT<MODE>::T>* resq,
-                mgk_ray_result* res, Counters* cnt) {
+                mgk_ray_result* res, Counters* cnt, const uint32_t* __restrict__ ray_ids) {
     using T = typename ModeT<MODE>::T;
     constexpr Fuse F = ModeT<MODE>::F;
     const int lane = threadIdx.x & 31;
@@ -262,7 +262,7 @@ __global__ void __launch_bounds__(kIntegrateThreads, MGK_INTEGRATE_MIN_BLOCKS)
                     pt = b[3];
                     c0 = reinterpret_cast<const T*>(qc)[idx];
                     h = P.h0;
-                    ray = idx;
+                    ray = ray_ids ? ray_ids[idx] : idx;
                     steps = 0; tries = 0; att = 0;
                     alive = true;
                     if constexpr (MODE == MGK_PRECISION_MIXED && METRIC != MGK_METRIC_MINKOWSKI)
@@ -365,7 +365,7 @@ __global__ void __launch_bounds__(128, 4) k_refine(const DevScene<typename ModeT
                                                 const RefineEntry<typename ModeT<MODE>::T>* __restrict__ refq,
                                                 uint32_t cap, HitEntry<typename ModeT<MODE>::T>* hits,
                                                 ResumeEntry<typename ModeT<MODE>::T>* resq, mgk_ray_result* res,
-                                                Counters* cnt) {
+                                                Counters* cnt, uint32_t hit_cap) {
     using T = typename ModeT<MODE>::T;
     constexpr Fuse F = ModeT<MODE>::F;
     const uint32_t nd = min(cnt->refine_count, cap);
@@ -396,7 +396,7 @@ __global__ void __launch_bounds__(128, 4) k_refine(const DevScene<typename ModeT
         if (rslot != ~0u)
             store_resume<T>(resq, rslot, y1, e.pt, e.h_next, e.c0, e.ray, e.steps, e.attempts, e.wide, evals);
         bool lit = valid && (t.cls == MGK_RAY_DISK || t.cls == MGK_RAY_ESCAPED);
-        uint32_t hslot = warp_push(lit, &cnt->hit_count, cap, &cnt->status);
+        uint32_t hslot = warp_push(lit, &cnt->hit_count, hit_cap, &cnt->status);
         if (hslot != ~0u) push_hit<T>(hits, hslot, e.ray, t);
         if (valid && t.cls != MGK_RAY_ALIVE) {
             if (res) write_result<T>(res, e.ray, ye, e.pt, t, e.steps, e.attempts, e.wide, evals);
@@ -415,7 +415,7 @@ template <int METRIC, int MODE>
 __global__ void __launch_bounds__(128, 4) k_tail(const DevScene<typename ModeT<MODE>::T> P,
                                               const ResumeEntry<typename ModeT<MODE>::T>* __restrict__ resq,
                                               uint32_t cap, HitEntry<typename ModeT<MODE>::T>* hits,
-                                              mgk_ray_result* res, Counters* cnt) {
+                                              mgk_ray_result* res, Counters* cnt, uint32_t hit_cap) {
     using T = typename ModeT<MODE>::T;
     constexpr Fuse F = ModeT<MODE>::F;
     const uint32_t n = min(cnt->resume_count, cap);
@@ -470,7 +470,7 @@ __global__ void __launch_bounds__(128, 4) k_tail(const DevScene<typename ModeT<M
             }
         }
         bool lit = valid && (t.cls == MGK_RAY_DISK || t.cls == MGK_RAY_ESCAPED);
-        uint32_t hslot = warp_push(lit, &cnt->hit_count, cap, &cnt->status);
+        uint32_t hslot = warp_push(lit, &cnt->hit_count, hit_cap, &cnt->status);
         if (hslot != ~0u) push_hit<T>(hits, hslot, e.ray, t);
         if (valid) {
             if (res) write_result<T>(res, e.ray, y, e.pt, t, steps, att, wide, evals);
@@ -656,6 +656,232 @@ __global__ void __launch_bounds__(64) k_trace_geodesic(const TraceJob* __restric
     written[i] = nw;
 }
 
+// Device-scene table passed by value to the kernels.
+template <class T> static const DevScene<T>& ds(const void* p) { return *reinterpret_cast<const DevScene<T>*>(p); }
+
+// ------------------------------------------------------------- surrogate
+// Features of the surrogate network, shared by training and rendering:
+// [(r_obs - 55) / 45, cos i, sin i, 2 a / 0.998 - 1, n_x, n_y, n_z] with n the
+// photon's direction in the observer's frame (camera looks along -z).
+__device__ __forceinline__ void write_features(float* f, double r_obs, double ci, double si, double spin, double nx,
+                                               double ny, double nz) {
+    f[0] = float((r_obs - 55.0) / 45.0);
+    f[1] = float(ci);
+    f[2] = float(si);
+    f[3] = float(2.0 * spin / 0.998 - 1.0);
+    f[4] = float(nx);
+    f[5] = float(ny);
+    f[6] = float(nz);
+}
+
+// Training samples: each ray has its own observer (r in [10, 100] M,
+// inclination in [0, 90] degrees) and a direction uniform on the camera's
+// forward hemisphere; the spin is the launch's.  The observer tetrad is built
+// per ray in double, like scene_consts does once per frame.
+template <int MODE>
+__global__ void __launch_bounds__(128) k_generate_samples(const DevScene<typename ModeT<MODE>::T> P, uint64_t seed,
+                                                          uint32_t first, uint32_t n, void* qx, void* qp, void* qc,
+                                                          float* feat) {
+    using T = typename ModeT<MODE>::T;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t id = first + i;
+    const double u0 = rng_unit(seed, 0x5A3Bu, id, 0), u1 = rng_unit(seed, 0x5A3Bu, id, 1);
+    const double u2 = rng_unit(seed, 0x5A3Bu, id, 2), u3 = rng_unit(seed, 0x5A3Bu, id, 3);
+    const double r_obs = 10.0 + 90.0 * u0, incl = 0.5 * 3.14159265358979323846 * u1;
+    const double ci = cos(incl), si = sin(incl);
+    const double ct = u2, st = sqrt(fmax(0.0, 1.0 - ct * ct)), ph = 2.0 * 3.14159265358979323846 * u3;
+    const double nx = st * cos(ph), ny = st * sin(ph), nz = -ct;
+    const int metric = P.metric;
+    const double a = P.spin_d, ms = double(P.m.mass_sign);
+    V4<double> q{0.0, r_obs * ci, r_obs * si, 0.0};
+    V4<double> X{1, 0, 0, 0}, Y{0, si, -ci, 0}, Z{0, ci, si, 0};
+    V4<double> u = reference_observer<double>(metric, q.x, q.y, q.z, a, ms);
+    Sym4<double> g = compute_g<double>(metric, q.x, q.y, q.z, a, ms);
+    Tetrad<double> e = build_tetrad<double>(g, X, Y, Z, u);
+    V4<double> pu = local_to_global<double>(e, V4<double>{nx, ny, nz, 1.0});
+    V4<double> p = contract<double>(g, pu);
+    q_store(qx, i, T(q.x), T(q.y), T(q.z), T(0));
+    q_store(qp, i, T(p.x), T(p.y), T(p.z), T(p.t));
+    reinterpret_cast<T*>(qc)[i] = T(dot4<double>(u, p));
+    write_features(feat + size_t(i) * 7, r_obs, ci, si, double(P.spin_phys), nx, ny, nz);
+}
+
+cudaError_t launch_generate_samples(const mgk_scene& s, const void* dsc, uint64_t seed, uint32_t first, uint32_t n,
+                                    const ChunkBuffers& b, float* feat, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    if (s.precision == MGK_PRECISION_F64)
+        k_generate_samples<MGK_PRECISION_F64><<<(n + 127) / 128, 128, 0, st>>>(ds<double>(dsc), seed, first, n, b.qx,
+                                                                               b.qp, b.qc, feat);
+    else if (s.precision == MGK_PRECISION_MIXED)
+        k_generate_samples<MGK_PRECISION_MIXED><<<(n + 127) / 128, 128, 0, st>>>(ds<float>(dsc), seed, first, n, b.qx,
+                                                                                 b.qp, b.qc, feat);
+    else
+        k_generate_samples<MGK_PRECISION_REF32><<<(n + 127) / 128, 128, 0, st>>>(ds<float>(dsc), seed, first, n, b.qx,
+                                                                                 b.qp, b.qc, feat);
+    return cudaGetLastError();
+}
+
+// Labels of the traced samples (layout of mgk_sample_label).
+__global__ void k_labels(const mgk_ray_result* __restrict__ res, uint32_t n, mgk_sample_label* __restrict__ lab) {
+    static_assert(sizeof(mgk_sample_label) == 32, "label layout");
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const mgk_ray_result r = res[i];
+    mgk_sample_label L;
+    L.cls = r.cls == MGK_RAY_DISK ? 0 : (r.cls == MGK_RAY_ESCAPED ? 1 : 2);
+    L.r = r.cls == MGK_RAY_DISK ? float((r.r_hit - 10.0) / 10.0) : 0.f;
+    L.g = r.cls == MGK_RAY_DISK ? float(r.z) : 0.f;
+    for (int k = 0; k < 3; ++k) L.dir[k] = r.cls == MGK_RAY_ESCAPED ? float(r.dir[k]) : 0.f;
+    L.reserved[0] = L.reserved[1] = 0.f;
+    lab[i] = L;
+}
+
+cudaError_t launch_labels(const mgk_ray_result* res, uint32_t n, void* labels, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    k_labels<<<(n + 255) / 256, 256, 0, st>>>(res, n, reinterpret_cast<mgk_sample_label*>(labels));
+    return cudaGetLastError();
+}
+
+// Features of the camera rays of a frame (same direction as camera_ray).
+template <class T>
+__global__ void k_camera_features(const DevScene<T> P, uint64_t first_ray, uint32_t n, float* feat) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint64_t ray_id = first_ray + i;
+    const uint32_t pixel = uint32_t(ray_id / P.spp), sample = uint32_t(ray_id % P.spp);
+    const uint32_t px = pixel % P.width, py = pixel / P.width;
+    const double sx = (double(px) + rng_unit(P.seed, sample, pixel, 0)) * double(P.pix_a) + double(P.pix_b);
+    const double sy = (double(py) + rng_unit(P.seed, sample, pixel, 1)) * double(P.pix_c) + double(P.pix_d);
+    const double len = sqrt(sx * sx + sy * sy + 1.0);
+    const double cy = double(P.cam[1]), cz = double(P.cam[2]);
+    const double r = sqrt(cy * cy + cz * cz);
+    write_features(feat + size_t(i) * 7, r, cy / r, cz / r, double(P.spin_phys), sx / len, sy / len, -1.0 / len);
+}
+
+cudaError_t launch_camera_features(const mgk_scene& s, const void* dsc, uint64_t first, uint32_t n,
+                                   const ChunkBuffers&, float* feat, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    if (s.precision == MGK_PRECISION_F64) k_camera_features<double><<<(n + 255) / 256, 256, 0, st>>>(ds<double>(dsc), first, n, feat);
+    else k_camera_features<float><<<(n + 255) / 256, 256, 0, st>>>(ds<float>(dsc), first, n, feat);
+    return cudaGetLastError();
+}
+
+// Distance of a photon's conserved quantities from the Kerr critical curve.
+// lambda = L/E, eta = Q/E^2 from the Kerr-Schild state (spin axis y; the
+// oblate-spheroidal theta has dx^i/dtheta = (x cot, r-sin, z cot) terms);
+// the critical curve is the spherical photon orbits' (Bardeen 1973):
+//   lambda_c(r) = -(r^3 - 3 r^2 + a^2 r + a^2) / (a (r - 1)),
+//   eta_c(r)    = r^3 (4 a^2 - r (r - 3)^2) / (a^2 (r - 1)^2),
+// r between the prograde and retrograde circular photon orbits.  Returns
+// |b - b_c| / b_c with b = sqrt(eta + lambda^2) (1e30 when lambda lies
+// outside the curve's range).
+__device__ __forceinline__ double critical_distance(double x, double y, double z, double px, double py, double pz,
+                                                    double pt, double a) {
+    const double E = -pt, L = z * px - x * pz;
+    const double r = ks_r<double>(x, y, z, a);
+    const double ct = y / r, st2 = fmax(1e-300, 1.0 - ct * ct), st = sqrt(st2);
+    const double pth = (ct / st) * (x * px + z * pz) - r * st * py;
+    const double Q = pth * pth + ct * ct * (L * L / st2 - a * a * E * E);
+    const double lam = L / E, eta = Q / (E * E), b = sqrt(fmax(0.0, eta + lam * lam));
+    if (fabs(a) < 1e-3) {
+        const double bc = sqrt(27.0);
+        return fabs(b - bc) / bc;
+    }
+    const double aa = fabs(a);
+    double r1 = 2.0 * (1.0 + cos(2.0 / 3.0 * acos(-aa))), r2 = 2.0 * (1.0 + cos(2.0 / 3.0 * acos(aa)));
+    auto lc = [&](double rr) { return -(rr * rr * rr - 3.0 * rr * rr + a * a * rr + a * a) / (a * (rr - 1.0)); };
+    double l1 = lc(r1), l2 = lc(r2);
+    if (!((lam - l1) * (lam - l2) <= 0.0)) return 1e30;
+    for (int it = 0; it < 60; ++it) {
+        double rm = 0.5 * (r1 + r2), lm = lc(rm);
+        if ((lm - lam) * (l1 - lam) > 0.0) { r1 = rm; l1 = lm; } else { r2 = rm; }
+    }
+    const double rs = 0.5 * (r1 + r2);
+    const double etac = rs * rs * rs * (4.0 * a * a - rs * (rs - 3.0) * (rs - 3.0)) / (a * a * (rs - 1.0) * (rs - 1.0));
+    const double bc = sqrt(fmax(1e-300, etac + lam * lam));
+    return fabs(b - bc) / bc;
+}
+
+// Routing of a frame chunk after the surrogate's forward pass: rays with low
+// confidence or near the critical curve go to the RKF45 fallback queue
+// (compacted by warp ballot, with their ray index); the others become hits
+// straight from the network's outputs.
+template <int MODE>
+__global__ void __launch_bounds__(256) k_route(const DevScene<typename ModeT<MODE>::T> P, uint32_t base_ray, uint32_t n,
+                                               uint32_t cap, const float* __restrict__ out, float conf_min,
+                                               float crit_frac, const void* __restrict__ qx,
+                                               const void* __restrict__ qp, const void* __restrict__ qc, void* fqx,
+                                               void* fqp, void* fqc, uint32_t* fallback_ids,
+                                               HitEntry<typename ModeT<MODE>::T>* hits, Counters* cnt) {
+    using T = typename ModeT<MODE>::T;
+    const uint32_t lane = threadIdx.x & 31;
+    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += gridDim.x * blockDim.x) {
+        const uint32_t i = base + lane;
+        const uint32_t ray = base_ray + i;
+        const bool valid = i < n;
+        bool fall = false, lit = false;
+        Term<T> t{MGK_RAY_ALIVE, T(0), T(0), T(0), T(0), T(0)};
+        T a4[4] = {T(0), T(0), T(0), T(0)}, b4[4] = {T(0), T(0), T(0), T(0)}, c0 = T(0);
+        if (valid) {
+            const float* o = out + size_t(i) * 16;
+            q_load(qx, ray, a4);
+            q_load(qp, ray, b4);
+            c0 = reinterpret_cast<const T*>(qc)[ray];
+            const float conf = 1.0f / (1.0f + expf(-o[7]));
+            const double dc = critical_distance(double(a4[0]), double(a4[1]), double(a4[2]), double(b4[0]),
+                                                double(b4[1]), double(b4[2]), double(b4[3]), P.spin_d);
+            fall = conf < conf_min || dc < double(crit_frac);
+            if (!fall) {
+                const int cls = (o[0] >= o[1] && o[0] >= 0.f) ? 0 : (o[1] >= 0.f ? 1 : 2);
+                if (cls == 0) {
+                    t.cls = MGK_RAY_DISK;
+                    t.r_hit = T(10.0f + 10.0f * o[2]);
+                    t.z = T(o[3]);
+                    lit = t.r_hit >= P.disk_r_in && t.r_hit <= P.disk_r_out;
+                } else if (cls == 1) {
+                    const float dn = sqrtf(o[4] * o[4] + o[5] * o[5] + o[6] * o[6]);
+                    t.cls = MGK_RAY_ESCAPED;
+                    t.d0 = T(o[4] / dn); t.d1 = T(o[5] / dn); t.d2 = T(o[6] / dn);
+                    t.z = redshift_clamp<T>(c0 / b4[3]);
+                    lit = true;
+                }
+            }
+        }
+        uint32_t fslot = warp_push(valid && fall, &cnt->fallback_count, cap, &cnt->status);
+        if (fslot != ~0u) {
+            q_store(fqx, fslot, a4[0], a4[1], a4[2], a4[3]);
+            q_store(fqp, fslot, b4[0], b4[1], b4[2], b4[3]);
+            reinterpret_cast<T*>(fqc)[fslot] = c0;
+            fallback_ids[fslot] = ray;
+        }
+        uint32_t hslot = warp_push(lit, &cnt->hit_count, cap, &cnt->status);
+        if (hslot != ~0u) push_hit<T>(hits, hslot, ray, t);
+    }
+}
+
+cudaError_t launch_route(const mgk_scene& s, const void* dsc, uint32_t base, uint32_t n, uint32_t cap,
+                         const float* out, float conf_min, float crit_frac, const ChunkBuffers& b,
+                         uint32_t* fallback_ids, void* fallback_q, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    const bool f64 = s.precision == MGK_PRECISION_F64;
+    const size_t T = f64 ? 8 : 4;
+    char* fq = static_cast<char*>(fallback_q);
+    void* fqx = fq;
+    void* fqp = fq + size_t(cap) * 4 * T;
+    void* fqc = fq + size_t(cap) * 8 * T;
+    const uint32_t blocks = (n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096;
+    if (f64)
+        k_route<MGK_PRECISION_F64><<<blocks, 256, 0, st>>>(ds<double>(dsc), base, n, cap, out, conf_min, crit_frac,
+                                                           b.qx, b.qp, b.qc, fqx, fqp, fqc, fallback_ids,
+                                                           reinterpret_cast<HitEntry<double>*>(b.hits), b.counters);
+    else
+        k_route<MGK_PRECISION_MIXED><<<blocks, 256, 0, st>>>(ds<float>(dsc), base, n, cap, out, conf_min, crit_frac,
+                                                             b.qx, b.qp, b.qc, fqx, fqp, fqc, fallback_ids,
+                                                             reinterpret_cast<HitEntry<float>*>(b.hits), b.counters);
+    return cudaGetLastError();
+}
+
 // --------------------------------------------------------------- FP32 probe
 // Peak FP32 throughput: 8 independent FMA chains per thread, enough warps to
 // hide the pipeline latency.  Each loop trip is 8 FMA = 16 FLOP per thread.
@@ -680,7 +906,6 @@ cudaError_t launch_fma_probe(uint32_t blocks, uint32_t iters, float* sink, cudaS
 }
 
 // =============================================================== launchers
-template <class T> static const DevScene<T>& ds(const void* p) { return *reinterpret_cast<const DevScene<T>*>(p); }
 
 template <int MODE>
 static cudaError_t gen_t(const void* dev_scene, uint64_t first, uint32_t n, const ChunkBuffers& b, cudaStream_t st) {
@@ -713,13 +938,14 @@ static cudaError_t integ_t(const void* dsc, uint32_t n, const ChunkBuffers& b, m
     auto* resq = reinterpret_cast<ResumeEntry<T>*>(b.resume);
     auto* hits = reinterpret_cast<HitEntry<T>*>(b.hits);
     k_integrate<METRIC, MODE><<<blocks, kIntegrateThreads, 0, st>>>(ds<T>(dsc), n, b.qx, b.qp, b.qc, refq, resq, res,
-                                                                   b.counters);
+                                                                   b.counters, b.ray_ids);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    k_refine<METRIC, MODE><<<sms * 8, 128, 0, st>>>(ds<T>(dsc), refq, n, hits, resq, res, b.counters);
+    const uint32_t hit_cap = b.hit_cap ? b.hit_cap : n;
+    k_refine<METRIC, MODE><<<sms * 8, 128, 0, st>>>(ds<T>(dsc), refq, n, hits, resq, res, b.counters, hit_cap);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    k_tail<METRIC, MODE><<<sms * 2, 128, 0, st>>>(ds<T>(dsc), resq, n, hits, res, b.counters);
+    k_tail<METRIC, MODE><<<sms * 2, 128, 0, st>>>(ds<T>(dsc), resq, n, hits, res, b.counters, hit_cap);
     return cudaGetLastError();
 }
 
@@ -845,6 +1071,7 @@ template <class T> static void fill_t(const mgk_scene& s, const float* xyz_w, De
     P->seed = s.seed;
     P->width = s.width; P->height = s.height; P->spp = s.spp; P->n_bins = s.n_bins;
     P->max_steps = s.max_steps;
+    P->metric = s.metric;
     P->inv_spp = 1.0f / float(s.spp);
 }
 

@@ -1,0 +1,414 @@
+// Driver of the deflection surrogate: parameters, sample generation,
+// training (forward, loss, backward, Adam on the library's tensor-core
+// kernels), inference and the routed render.
+#include <algorithm>
+#include <cmath>
+#include <new>
+#include <cstring>
+#include <vector>
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include "dev_scene.cuh"
+#include "internal.h"
+#include "mlp.h"
+
+using namespace mgk;
+
+namespace {
+
+// Offsets (in floats) of the layers in the flat parameter vector; weights are
+// stored [out][in] (the K-major B operand of the forward GEMMs).
+struct Layout {
+    size_t w[MLP_LAYERS], b[MLP_LAYERS], total;
+    int in[MLP_LAYERS], out[MLP_LAYERS];
+};
+Layout param_layout() {
+    Layout L{};
+    const int ins[MLP_LAYERS] = {MLP_IN_PAD, MLP_HID, MLP_HID, MLP_HID, MLP_HID};
+    const int outs[MLP_LAYERS] = {MLP_HID, MLP_HID, MLP_HID, MLP_HID, MLP_OUT_PAD};
+    size_t o = 0;
+    for (int l = 0; l < MLP_LAYERS; ++l) {
+        L.in[l] = ins[l];
+        L.out[l] = outs[l];
+        L.w[l] = o;
+        o += size_t(ins[l]) * outs[l];
+        L.b[l] = o;
+        o += outs[l];
+    }
+    L.total = o;
+    return L;
+}
+
+}  // namespace
+
+struct mgk_surrogate {
+    mgk_context* ctx = nullptr;
+    int device = 0;
+    Layout L{};
+    float* p = nullptr;        // FP32 master parameters
+    float* grad = nullptr;
+    float* m = nullptr;
+    float* v = nullptr;
+    __nv_bfloat16* wb = nullptr;  // BF16 copies (same offsets)
+    uint64_t step = 0;
+    // training buffers for batch `tb`
+    int tb = 0;
+    __nv_bfloat16 *x0 = nullptr, *Z[4] = {}, *H[4] = {}, *dza = nullptr, *dzb = nullptr, *dout = nullptr;
+    float *out = nullptr, *dout32 = nullptr, *loss = nullptr;
+    mgk_sample_label* blab = nullptr;
+    uint32_t* perm = nullptr;
+    uint32_t perm_n = 0;
+    // inference buffers for batch `ib`
+    int ib = 0;
+    __nv_bfloat16 *ix0 = nullptr, *iha = nullptr, *ihb = nullptr;
+    float* iout = nullptr;
+    float* feat_tmp = nullptr;
+    std::vector<void*> owned;
+};
+
+namespace {
+
+template <class P> cudaError_t dalloc(mgk_surrogate* s, P** ptr, size_t bytes) {
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, bytes);
+    if (e != cudaSuccess) return e;
+    s->owned.push_back(q);
+    *ptr = static_cast<P*>(q);
+    return cudaSuccess;
+}
+
+#define TRY(call)                                          \
+    do {                                                   \
+        cudaError_t _e = (call);                           \
+        if (_e != cudaSuccess) {                           \
+            cudaGetLastError();                            \
+            return MGK_ERROR_CUDA;                         \
+        }                                                  \
+    } while (0)
+
+mgk_result ensure_train_buffers(mgk_surrogate* s, int B) {
+    if (s->tb >= B) return MGK_SUCCESS;
+    if (s->tb) return MGK_ERROR_INVALID_ARGUMENT;  // one batch size per network
+    const size_t act = size_t(B) * MLP_HID * sizeof(__nv_bfloat16);
+    TRY(dalloc(s, &s->x0, size_t(B) * MLP_IN_PAD * 2));
+    for (int l = 0; l < 4; ++l) {
+        TRY(dalloc(s, &s->Z[l], act));
+        TRY(dalloc(s, &s->H[l], act));
+    }
+    TRY(dalloc(s, &s->dza, act));
+    TRY(dalloc(s, &s->dzb, act));
+    TRY(dalloc(s, &s->dout, size_t(B) * MLP_OUT_PAD * 2));
+    TRY(dalloc(s, &s->out, size_t(B) * MLP_OUT_PAD * 4));
+    TRY(dalloc(s, &s->dout32, size_t(B) * MLP_OUT_PAD * 4));
+    TRY(dalloc(s, &s->loss, 64));
+    TRY(dalloc(s, &s->blab, size_t(B) * sizeof(mgk_sample_label)));
+    s->tb = B;
+    return MGK_SUCCESS;
+}
+
+mgk_result ensure_infer_buffers(mgk_surrogate* s, int B) {
+    if (s->ib >= B) return MGK_SUCCESS;
+    if (s->ib) return MGK_ERROR_INVALID_ARGUMENT;
+    TRY(dalloc(s, &s->ix0, size_t(B) * MLP_IN_PAD * 2));
+    TRY(dalloc(s, &s->iha, size_t(B) * MLP_HID * 2));
+    TRY(dalloc(s, &s->ihb, size_t(B) * MLP_HID * 2));
+    TRY(dalloc(s, &s->iout, size_t(B) * MLP_OUT_PAD * 4));
+    s->ib = B;
+    return MGK_SUCCESS;
+}
+
+// Permutation buffer of the sample set (grown by reallocation).
+mgk_result ensure_perm(mgk_surrogate* s, uint32_t n) {
+    if (s->perm_n >= n) return MGK_SUCCESS;
+    if (s->perm) {
+        for (auto& q : s->owned)
+            if (q == s->perm) q = nullptr;
+        cudaFree(s->perm);
+        s->perm = nullptr;
+        s->perm_n = 0;
+    }
+    TRY(dalloc(s, &s->perm, size_t(n) * 4));
+    s->perm_n = n;
+    return MGK_SUCCESS;
+}
+
+GemmArgs gemm(const __nv_bfloat16* A, const __nv_bfloat16* B, int M, int N, int K, int lda, int ldb, int ldc) {
+    GemmArgs g{};
+    g.A = A; g.B = B; g.M = M; g.N = N; g.K = K; g.lda = lda; g.ldb = ldb; g.ldc = ldc; g.k_split = K;
+    return g;
+}
+
+// Forward pass of a batch of B rows from x0; with Z == nullptr (inference)
+// only the activations are written, ping-ponging between ha and hb.
+cudaError_t forward(mgk_surrogate* s, const __nv_bfloat16* x0, int B, __nv_bfloat16* const* Z,
+                    __nv_bfloat16* const* H, float* out, cudaStream_t st) {
+    const Layout& L = s->L;
+    GemmArgs g = gemm(x0, s->wb + L.w[0], B, MLP_HID, MLP_IN_PAD, MLP_IN_PAD, MLP_IN_PAD, MLP_HID);
+    g.bias = s->p + L.b[0];
+    g.Z = Z ? Z[0] : nullptr;
+    g.H = H[0];
+    cudaError_t e = launch_gemm(GEMM_FWD_FIRST, g, st);
+    for (int l = 1; l < 4 && e == cudaSuccess; ++l) {
+        g = gemm(H[l - 1], s->wb + L.w[l], B, MLP_HID, MLP_HID, MLP_HID, MLP_HID, MLP_HID);
+        g.bias = s->p + L.b[l];
+        g.Z = Z ? Z[l] : nullptr;
+        g.H = H[l];
+        e = launch_gemm(GEMM_FWD_HIDDEN, g, st);
+    }
+    if (e != cudaSuccess) return e;
+    g = gemm(H[3], s->wb + L.w[4], B, MLP_OUT_PAD, MLP_HID, MLP_HID, MLP_HID, MLP_OUT_PAD);
+    g.bias = s->p + L.b[4];
+    g.out = out;
+    return launch_gemm(GEMM_FWD_OUT, g, st);
+}
+
+// Loss, backward pass and gradient accumulation of the batch in the training
+// buffers (grad is zeroed first).
+cudaError_t backward(mgk_surrogate* s, int B, const LossWeights& w, cudaStream_t st) {
+    const Layout& L = s->L;
+    cudaError_t e = cudaMemsetAsync(s->grad, 0, L.total * sizeof(float), st);
+    if (e == cudaSuccess) e = launch_loss(s->out, s->blab, B, w, s->dout, s->dout32, s->loss, st);
+    if (e != cudaSuccess) return e;
+    const int ks = B >= 1024 && B % 1024 == 0 ? 1024 : B;
+    // output layer
+    GemmArgs g = gemm(s->dout, s->H[3], MLP_OUT_PAD, MLP_HID, B, MLP_OUT_PAD, MLP_HID, MLP_HID);
+    g.k_split = ks;
+    g.out = s->grad + L.w[4];
+    if ((e = launch_gemm(GEMM_DW_OUT, g, st)) != cudaSuccess) return e;
+    if ((e = launch_colsum_f32(s->dout32, B, MLP_OUT_PAD, s->grad + L.b[4], st)) != cudaSuccess) return e;
+    g = gemm(s->dout, s->wb + L.w[4], B, MLP_HID, MLP_OUT_PAD, MLP_OUT_PAD, MLP_HID, MLP_HID);
+    g.Zp = s->Z[3];
+    g.H = s->dza;
+    if ((e = launch_gemm(GEMM_DX_FROM_OUT, g, st)) != cudaSuccess) return e;
+    // hidden layers 4, 3, 2 (index l = 3, 2, 1): dz of layer l is in `cur`
+    __nv_bfloat16* cur = s->dza;
+    __nv_bfloat16* nxt = s->dzb;
+    for (int l = 3; l >= 1; --l) {
+        g = gemm(cur, s->H[l - 1], MLP_HID, MLP_HID, B, MLP_HID, MLP_HID, MLP_HID);
+        g.k_split = ks;
+        g.out = s->grad + L.w[l];
+        if ((e = launch_gemm(GEMM_DW_HIDDEN, g, st)) != cudaSuccess) return e;
+        if ((e = launch_colsum(cur, B, MLP_HID, MLP_HID, s->grad + L.b[l], st)) != cudaSuccess) return e;
+        g = gemm(cur, s->wb + L.w[l], B, MLP_HID, MLP_HID, MLP_HID, MLP_HID, MLP_HID);
+        g.Zp = s->Z[l - 1];
+        g.H = nxt;
+        if ((e = launch_gemm(GEMM_DX_HIDDEN, g, st)) != cudaSuccess) return e;
+        __nv_bfloat16* t = cur;
+        cur = nxt;
+        nxt = t;
+    }
+    // first layer
+    g = gemm(cur, s->x0, MLP_HID, MLP_IN_PAD, B, MLP_HID, MLP_IN_PAD, MLP_IN_PAD);
+    g.k_split = ks;
+    g.out = s->grad + L.w[0];
+    if ((e = launch_gemm(GEMM_DW_FIRST, g, st)) != cudaSuccess) return e;
+    return launch_colsum(cur, B, MLP_HID, MLP_HID, s->grad + L.b[0], st);
+}
+
+}  // namespace
+
+namespace mgk {
+
+// Inference in sub-batches of the network's inference buffers; a sub-batch
+// whose row count is a multiple of the GEMM tile writes straight into out.
+cudaError_t surrogate_infer(mgk_surrogate* s, const float* feat, uint32_t n, float* out, cudaStream_t st) {
+    constexpr uint32_t IB = 1u << 20;
+    if (ensure_infer_buffers(s, int(IB)) != MGK_SUCCESS) return cudaErrorMemoryAllocation;
+    for (uint32_t b0 = 0; b0 < n; b0 += IB) {
+        const uint32_t cnt = std::min<uint32_t>(IB, n - b0);
+        const uint32_t padded = (cnt + 127) / 128 * 128;
+        float* dst = out + size_t(b0) * MLP_OUT_PAD;
+        cudaError_t e = launch_features_bf16(feat + size_t(b0) * MLP_IN, cnt, padded, s->ix0, st);
+        if (e != cudaSuccess) return e;
+        __nv_bfloat16* H[4] = {s->iha, s->ihb, s->iha, s->ihb};
+        e = forward(s, s->ix0, int(padded), nullptr, H, padded == cnt ? dst : s->iout, st);
+        if (e != cudaSuccess) return e;
+        if (padded != cnt) {
+            e = cudaMemcpyAsync(dst, s->iout, size_t(cnt) * MLP_OUT_PAD * 4, cudaMemcpyDeviceToDevice, st);
+            if (e != cudaSuccess) return e;
+        }
+    }
+    return cudaSuccess;
+}
+
+}  // namespace mgk
+
+namespace {
+
+LossWeights loss_weights(const mgk_train_config& c) {
+    return LossWeights{c.w_cls, c.w_r, c.w_g, c.w_dir, c.w_conf, c.tol_r, c.tol_g, c.tol_dir};
+}
+
+uint32_t host_hash(uint64_t seed, uint32_t a, uint32_t b) { return rng_u32(seed, 0x7E11u, a, b); }
+
+}  // namespace
+
+extern "C" {
+
+MGK_API void mgk_train_defaults(mgk_train_config* c) {
+    if (!c) return;
+    std::memset(c, 0, sizeof(*c));
+    c->batch = 65536;
+    c->epochs = 20;
+    c->lr = 1e-3f;
+    c->beta1 = 0.9f;
+    c->beta2 = 0.999f;
+    c->eps = 1e-8f;
+    c->seed = 0x7EA1;
+    c->w_cls = 1.0f;
+    c->w_r = 10.0f;
+    c->w_g = 100.0f;
+    c->w_dir = 100.0f;
+    c->w_conf = 0.1f;
+    c->tol_r = 1e-3f;    // 0.01 M in r_hit
+    c->tol_g = 1e-3f;
+    c->tol_dir = 1e-3f;  // ~1 mrad
+}
+
+MGK_API uint64_t mgk_surrogate_param_count(void) { return param_layout().total; }
+
+MGK_API mgk_result mgk_surrogate_destroy(mgk_surrogate* s) {
+    if (!s) return MGK_ERROR_INVALID_POINTER;
+    cudaSetDevice(s->device);
+    for (void* q : s->owned) cudaFree(q);
+    delete s;
+    return MGK_SUCCESS;
+}
+
+MGK_API mgk_result mgk_surrogate_set_params(mgk_surrogate* s, const float* h) {
+    if (!s || !h) return MGK_ERROR_INVALID_POINTER;
+    cudaSetDevice(s->device);
+    const size_t n = s->L.total;
+    std::vector<__nv_bfloat16> b(n);
+    for (size_t i = 0; i < n; ++i) b[i] = __float2bfloat16_rn(h[i]);
+    TRY(cudaMemcpy(s->p, h, n * 4, cudaMemcpyHostToDevice));
+    TRY(cudaMemcpy(s->wb, b.data(), n * 2, cudaMemcpyHostToDevice));
+    TRY(cudaMemset(s->m, 0, n * 4));
+    TRY(cudaMemset(s->v, 0, n * 4));
+    s->step = 0;
+    return MGK_SUCCESS;
+}
+
+MGK_API mgk_result mgk_surrogate_get_params(mgk_surrogate* s, float* h) {
+    if (!s || !h) return MGK_ERROR_INVALID_POINTER;
+    cudaSetDevice(s->device);
+    TRY(cudaMemcpy(h, s->p, s->L.total * 4, cudaMemcpyDeviceToHost));
+    return MGK_SUCCESS;
+}
+
+MGK_API mgk_result mgk_surrogate_create(mgk_context* ctx, uint64_t seed, mgk_surrogate** out) {
+    if (!ctx || !out) return MGK_ERROR_INVALID_POINTER;
+    *out = nullptr;
+    mgk_surrogate* s = new (std::nothrow) mgk_surrogate();
+    if (!s) return MGK_ERROR_HOST_ALLOCATION_FAILED;
+    s->ctx = ctx;
+    s->device = context_device(ctx);
+    s->L = param_layout();
+    cudaSetDevice(s->device);
+    const size_t n = s->L.total;
+    if (dalloc(s, &s->p, n * 4) != cudaSuccess || dalloc(s, &s->grad, n * 4) != cudaSuccess ||
+        dalloc(s, &s->m, n * 4) != cudaSuccess || dalloc(s, &s->v, n * 4) != cudaSuccess ||
+        dalloc(s, &s->wb, n * 2) != cudaSuccess) {
+        cudaGetLastError();
+        mgk_surrogate_destroy(s);
+        return MGK_ERROR_DEVICE_OUT_OF_MEMORY;
+    }
+    // uniform(-1/sqrt(fan_in), 1/sqrt(fan_in)) on the real (unpadded) inputs
+    std::vector<float> h(n, 0.f);
+    const Layout& L = s->L;
+    for (int l = 0; l < MLP_LAYERS; ++l) {
+        const int real_in = l == 0 ? MLP_IN : MLP_HID, real_out = l == MLP_LAYERS - 1 ? MLP_OUT : MLP_HID;
+        const float k = 1.0f / std::sqrt(float(real_in));
+        for (int o = 0; o < real_out; ++o)
+            for (int i = 0; i < real_in; ++i)
+                h[L.w[l] + size_t(o) * L.in[l] + i] = k * (2.0f * rng_unit(seed, 0xB17Au + l, o, i) - 1.0f);
+    }
+    mgk_result rc = mgk_surrogate_set_params(s, h.data());
+    if (rc != MGK_SUCCESS) {
+        mgk_surrogate_destroy(s);
+        return rc;
+    }
+    *out = s;
+    return MGK_SUCCESS;
+}
+
+MGK_API mgk_result mgk_surrogate_forward(mgk_surrogate* s, const float* d_feat, uint32_t n, float* d_out,
+                                         void* stream) {
+    if (!s || !d_feat || !d_out) return MGK_ERROR_INVALID_POINTER;
+    cudaSetDevice(s->device);
+    TRY(surrogate_infer(s, d_feat, n, d_out, static_cast<cudaStream_t>(stream)));
+    return MGK_SUCCESS;
+}
+
+MGK_API mgk_result mgk_surrogate_gradient(mgk_surrogate* s, const mgk_train_config* cfg, const float* d_feat,
+                                          const mgk_sample_label* d_lab, uint32_t n, float* h_grad, float* h_loss) {
+    if (!s || !cfg || !d_feat || !d_lab || !h_grad) return MGK_ERROR_INVALID_POINTER;
+    if (n == 0 || n % 1024) return MGK_ERROR_INVALID_ARGUMENT;
+    cudaSetDevice(s->device);
+    mgk_result rc = ensure_train_buffers(s, int(n));
+    if (rc != MGK_SUCCESS) return rc;
+    if (s->tb != int(n)) return MGK_ERROR_INVALID_ARGUMENT;
+    cudaStream_t st = nullptr;
+    rc = ensure_perm(s, n);
+    if (rc != MGK_SUCCESS) return rc;
+    std::vector<uint32_t> perm(n);
+    for (uint32_t i = 0; i < n; ++i) perm[i] = i;
+    TRY(cudaMemcpyAsync(s->perm, perm.data(), size_t(n) * 4, cudaMemcpyHostToDevice, st));
+    TRY(launch_gather(d_feat, d_lab, s->perm, 0, int(n), s->x0, s->blab, st));
+    TRY(cudaMemsetAsync(s->loss, 0, 4, st));
+    TRY(forward(s, s->x0, int(n), s->Z, s->H, s->out, st));
+    TRY(backward(s, int(n), loss_weights(*cfg), st));
+    TRY(cudaMemcpyAsync(h_grad, s->grad, s->L.total * 4, cudaMemcpyDeviceToHost, st));
+    float loss = 0.f;
+    TRY(cudaMemcpyAsync(&loss, s->loss, 4, cudaMemcpyDeviceToHost, st));
+    TRY(cudaStreamSynchronize(st));
+    if (h_loss) *h_loss = loss;
+    return MGK_SUCCESS;
+}
+
+MGK_API mgk_result mgk_surrogate_train(mgk_surrogate* s, const mgk_train_config* cfg, const float* d_feat,
+                                       const mgk_sample_label* d_lab, uint32_t n, float* h_epoch_loss,
+                                       void* stream) {
+    if (!s || !cfg || !d_feat || !d_lab) return MGK_ERROR_INVALID_POINTER;
+    const uint32_t B = cfg->batch;
+    if (B == 0 || B % 1024 || n < B) return MGK_ERROR_INVALID_ARGUMENT;
+    cudaSetDevice(s->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    mgk_result rc = ensure_train_buffers(s, int(B));
+    if (rc != MGK_SUCCESS) return rc;
+    if (s->tb != int(B)) return MGK_ERROR_INVALID_ARGUMENT;
+    rc = ensure_perm(s, n);
+    if (rc != MGK_SUCCESS) return rc;
+    const LossWeights w = loss_weights(*cfg);
+    const uint32_t nb = n / B;
+    std::vector<uint32_t> perm(n);
+    for (uint32_t ep = 0; ep < cfg->epochs; ++ep) {
+        // Fisher-Yates with the counter-based hash
+        for (uint32_t i = 0; i < n; ++i) perm[i] = i;
+        for (uint32_t i = n - 1; i > 0; --i) {
+            uint32_t j = uint32_t((uint64_t(host_hash(cfg->seed, ep, i)) * (i + 1)) >> 32);
+            std::swap(perm[i], perm[j]);
+        }
+        TRY(cudaMemcpyAsync(s->perm, perm.data(), size_t(n) * 4, cudaMemcpyHostToDevice, st));
+        TRY(cudaMemsetAsync(s->loss, 0, 4, st));
+        for (uint32_t b = 0; b < nb; ++b) {
+            TRY(launch_gather(d_feat, d_lab, s->perm, int(b * B), int(B), s->x0, s->blab, st));
+            TRY(forward(s, s->x0, int(B), s->Z, s->H, s->out, st));
+            TRY(backward(s, int(B), w, st));
+            ++s->step;
+            AdamStep a{cfg->lr, cfg->beta1, cfg->beta2, cfg->eps,
+                       float(1.0 / (1.0 - std::pow(double(cfg->beta1), double(s->step)))),
+                       float(1.0 / (1.0 - std::pow(double(cfg->beta2), double(s->step))))};
+            TRY(launch_adam(s->p, s->grad, s->m, s->v, s->wb, int(s->L.total), a, st));
+        }
+        float loss = 0.f;
+        TRY(cudaMemcpyAsync(&loss, s->loss, 4, cudaMemcpyDeviceToHost, st));
+        TRY(cudaStreamSynchronize(st));
+        if (h_epoch_loss) h_epoch_loss[ep] = loss / float(nb);
+    }
+    return MGK_SUCCESS;
+}
+
+}  // extern "C"
