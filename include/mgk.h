@@ -295,9 +295,17 @@ MGK_API mgk_result mgk_surrogate_set_params(mgk_surrogate* net, const float* h_p
 MGK_API mgk_result mgk_make_samples(mgk_context* ctx, const mgk_scene* base, uint64_t seed, uint32_t n,
                                     uint32_t n_spin_buckets, float* d_features, mgk_sample_label* d_labels,
                                     void* stream);
-/* Forward pass: d_out receives 16 floats per sample (8 outputs + padding). */
+/* Forward pass (fused tcgen05 kernel, asynchronous): d_out receives 16 floats
+ * per sample (8 outputs + padding). */
 MGK_API mgk_result mgk_surrogate_forward(mgk_surrogate* net, const float* d_features, uint32_t n, float* d_out,
                                          void* stream);
+/* The same forward pass on the tiled mma.sync GEMM kernels of the training
+ * path (for comparisons; the fused tcgen05 kernel above is the fast path). */
+MGK_API mgk_result mgk_surrogate_forward_tiled(mgk_surrogate* net, const float* d_features, uint32_t n,
+                                               float* d_out, void* stream);
+/* Status word of the fused inference kernel: 0, or bit 1 when one of its
+ * bounded waits gave up (its outputs are then invalid).  Synchronous. */
+MGK_API mgk_result mgk_surrogate_status(mgk_surrogate* net, uint32_t* status);
 /* Loss and gradient of one batch (n a multiple of 1024) into host memory
  * (mgk_surrogate_param_count floats); synchronous. */
 MGK_API mgk_result mgk_surrogate_gradient(mgk_surrogate* net, const mgk_train_config* cfg, const float* d_features,

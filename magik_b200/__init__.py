@@ -34,7 +34,7 @@ EXPORTS = [
     "mgk_trace_rays", "mgk_shade_rays", "magik_trace_geodesic", "mgk_trace_geodesic_batch", "mgk_fp32_peak",
     "mgk_trace_rays_static", "mgk_train_defaults", "mgk_surrogate_param_count", "mgk_surrogate_create",
     "mgk_surrogate_destroy", "mgk_surrogate_get_params", "mgk_surrogate_set_params", "mgk_make_samples",
-    "mgk_surrogate_forward", "mgk_surrogate_gradient", "mgk_surrogate_train", "mgk_render_surrogate",
+    "mgk_surrogate_forward", "mgk_surrogate_forward_tiled", "mgk_surrogate_status", "mgk_surrogate_gradient", "mgk_surrogate_train", "mgk_render_surrogate",
 ]
 
 
@@ -85,6 +85,8 @@ def lib():
         L.mgk_surrogate_set_params.argtypes = [vp, P(C.c_float)]
         L.mgk_make_samples.argtypes = [vp, P(Scene), C.c_uint64, C.c_uint32, C.c_uint32, vp, vp, vp]
         L.mgk_surrogate_forward.argtypes = [vp, vp, C.c_uint32, vp, vp]
+        L.mgk_surrogate_forward_tiled.argtypes = [vp, vp, C.c_uint32, vp, vp]
+        L.mgk_surrogate_status.argtypes = [vp, P(C.c_uint32)]
         L.mgk_surrogate_gradient.argtypes = [vp, P(abi.TrainConfig), vp, vp, C.c_uint32, P(C.c_float),
                                              P(C.c_float)]
         L.mgk_surrogate_train.argtypes = [vp, P(abi.TrainConfig), vp, vp, C.c_uint32, P(C.c_float), vp]
@@ -324,6 +326,20 @@ class Surrogate:
         _check(lib().mgk_surrogate_forward(self.handle, d_feat.data_ptr(), n, out.data_ptr(), _stream_ptr(stream)),
                "mgk_surrogate_forward")
         return out[:n]
+
+    def forward_tiled(self, d_feat, stream=None):
+        """The forward pass on the training path's tiled GEMM kernels."""
+        import torch
+        n = d_feat.shape[0]
+        out = torch.empty((max(n, 1), 16), dtype=torch.float32, device=d_feat.device)
+        _check(lib().mgk_surrogate_forward_tiled(self.handle, d_feat.data_ptr(), n, out.data_ptr(),
+                                                 _stream_ptr(stream)), "mgk_surrogate_forward_tiled")
+        return out[:n]
+
+    def status(self):
+        v = C.c_uint32(0)
+        _check(lib().mgk_surrogate_status(self.handle, C.byref(v)), "mgk_surrogate_status")
+        return v.value
 
     def gradient(self, cfg, d_feat, d_lab):
         """Loss and gradient of one batch (host float32 vector)."""

@@ -969,7 +969,7 @@ MGK_API mgk_result mgk_render_surrogate(mgk_context* ctx, mgk_surrogate* net, co
     MGK_CUDA(ctx, cudaEventRecord(ctx->events[1], st));
     MGK_CUDA(ctx, cudaMemcpyAsync(h.data(), cnt_all, n_chunks * sizeof(Counters), cudaMemcpyDeviceToHost, st));
     MGK_CUDA(ctx, cudaStreamSynchronize(st));
-    uint32_t status = 0;
+    uint32_t status = surrogate_status(net);
     for (auto& k : h) status |= k.status;
     if (stats) {
         std::memset(stats, 0, sizeof(*stats));
@@ -999,7 +999,7 @@ MGK_API mgk_result mgk_render_surrogate(mgk_context* ctx, mgk_surrogate* net, co
         stats->surrogate_ms = sm;
     }
     if (status) {
-        ctx->last_error = "queue overflow reported by the integrator";
+        ctx->last_error = "queue overflow or surrogate wait timeout reported on the device";
         return MGK_ERROR_DEVICE_STATUS;
     }
     return MGK_SUCCESS;

@@ -92,6 +92,7 @@ cudaError_t launch_route(const mgk_scene& s, const void* dev_scene, uint32_t bas
                          uint32_t* fallback_ids, void* fallback_q, cudaStream_t stream);
 // Inference of the surrogate network (surrogate.cu): 16 floats per row of out.
 cudaError_t surrogate_infer(mgk_surrogate* net, const float* feat, uint32_t n, float* out, cudaStream_t stream);
+uint32_t surrogate_status(mgk_surrogate* net);
 int context_device(mgk_context* ctx);
 cudaError_t launch_fma_probe(uint32_t blocks, uint32_t iters, float* sink, cudaStream_t stream);
 cudaError_t launch_trace_geodesic(const void* jobs, uint32_t n, void* steps, uint32_t* written, cudaStream_t stream);

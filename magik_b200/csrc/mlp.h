@@ -15,6 +15,14 @@ namespace mgk {
 // padding columns of W1 and rows of W5 start at zero and receive zero
 // gradients, so they stay zero.
 constexpr int MLP_IN = 7, MLP_IN_PAD = 16, MLP_HID = 256, MLP_OUT = 8, MLP_OUT_PAD = 16, MLP_LAYERS = 5;
+// Offsets (floats) of the weights ([out][in]) and biases in the flat parameter vector.
+__host__ __device__ constexpr uint32_t mlp_w_off(int l) {
+    return l == 0 ? 0u : (l == 1 ? 4352u : (l == 2 ? 70144u : (l == 3 ? 135936u : 201728u)));
+}
+__host__ __device__ constexpr uint32_t mlp_b_off(int l) {
+    return l == 0 ? 4096u : (l == 1 ? 69888u : (l == 2 ? 135680u : (l == 3 ? 201472u : 205824u)));
+}
+constexpr uint32_t MLP_PARAMS = 205840;
 
 enum GemmEpilogue { EPI_FWD_SILU = 0, EPI_FWD_OUT = 1, EPI_DX = 2, EPI_DW = 3 };
 enum GemmKind {
@@ -57,5 +65,11 @@ cudaError_t launch_adam(float* p, const float* g, float* m, float* v, __nv_bfloa
 cudaError_t launch_gather(const float* feat, const SampleLabel* lab, const uint32_t* perm, int b0, int B,
                           __nv_bfloat16* x0, SampleLabel* blab, cudaStream_t st);
 cudaError_t launch_features_bf16(const float* feat, uint32_t n, uint32_t rows, __nv_bfloat16* x0, cudaStream_t st);
+
+// Fused tensor-core inference (mlp_tc.cu).
+size_t mlp_image_bytes();
+cudaError_t launch_weight_image(const __nv_bfloat16* wb, void* img, cudaStream_t st);
+cudaError_t launch_mlp_infer_tc(const float* feat, uint32_t n, const void* img, const float* params, float* out,
+                                uint32_t* status, int sm_count, cudaStream_t st);
 
 }  // namespace mgk

@@ -64,7 +64,11 @@ struct mgk_surrogate {
     int ib = 0;
     __nv_bfloat16 *ix0 = nullptr, *iha = nullptr, *ihb = nullptr;
     float* iout = nullptr;
-    float* feat_tmp = nullptr;
+    // fused tensor-core inference: weight image (rebuilt after each update)
+    void* img = nullptr;
+    bool img_valid = false;
+    uint32_t* status = nullptr;  // bit 1: a bounded wait of the fused kernel gave up
+    int sm_count = 0;
     std::vector<void*> owned;
 };
 
@@ -211,9 +215,26 @@ cudaError_t backward(mgk_surrogate* s, int B, const LossWeights& w, cudaStream_t
 
 namespace mgk {
 
-// Inference in sub-batches of the network's inference buffers; a sub-batch
-// whose row count is a multiple of the GEMM tile writes straight into out.
+// Inference: the fused tensor-core kernel over all n rows.
 cudaError_t surrogate_infer(mgk_surrogate* s, const float* feat, uint32_t n, float* out, cudaStream_t st) {
+    if (!s->img_valid) {
+        cudaError_t e = launch_weight_image(s->wb, s->img, st);
+        if (e != cudaSuccess) return e;
+        s->img_valid = true;
+    }
+    return launch_mlp_infer_tc(feat, n, s->img, s->p, out, s->status, s->sm_count, st);
+}
+
+// Status word of the fused kernel (0: no wait gave up); synchronous.
+uint32_t surrogate_status(mgk_surrogate* s) {
+    uint32_t h = 0;
+    if (cudaMemcpy(&h, s->status, 4, cudaMemcpyDeviceToHost) != cudaSuccess) return ~0u;
+    return h;
+}
+
+// Inference with the tiled GEMM kernels of the training path, in sub-batches
+// of the network's inference buffers (used to compare the two paths).
+cudaError_t surrogate_infer_tiled(mgk_surrogate* s, const float* feat, uint32_t n, float* out, cudaStream_t st) {
     constexpr uint32_t IB = 1u << 20;
     if (ensure_infer_buffers(s, int(IB)) != MGK_SUCCESS) return cudaErrorMemoryAllocation;
     for (uint32_t b0 = 0; b0 < n; b0 += IB) {
@@ -285,6 +306,7 @@ MGK_API mgk_result mgk_surrogate_set_params(mgk_surrogate* s, const float* h) {
     for (size_t i = 0; i < n; ++i) b[i] = __float2bfloat16_rn(h[i]);
     TRY(cudaMemcpy(s->p, h, n * 4, cudaMemcpyHostToDevice));
     TRY(cudaMemcpy(s->wb, b.data(), n * 2, cudaMemcpyHostToDevice));
+    s->img_valid = false;
     TRY(cudaMemset(s->m, 0, n * 4));
     TRY(cudaMemset(s->v, 0, n * 4));
     s->step = 0;
@@ -310,7 +332,9 @@ MGK_API mgk_result mgk_surrogate_create(mgk_context* ctx, uint64_t seed, mgk_sur
     const size_t n = s->L.total;
     if (dalloc(s, &s->p, n * 4) != cudaSuccess || dalloc(s, &s->grad, n * 4) != cudaSuccess ||
         dalloc(s, &s->m, n * 4) != cudaSuccess || dalloc(s, &s->v, n * 4) != cudaSuccess ||
-        dalloc(s, &s->wb, n * 2) != cudaSuccess) {
+        dalloc(s, &s->wb, n * 2) != cudaSuccess || dalloc(s, &s->img, mlp_image_bytes()) != cudaSuccess ||
+        dalloc(s, &s->status, 16) != cudaSuccess || cudaMemset(s->status, 0, 16) != cudaSuccess ||
+        cudaDeviceGetAttribute(&s->sm_count, cudaDevAttrMultiProcessorCount, s->device) != cudaSuccess) {
         cudaGetLastError();
         mgk_surrogate_destroy(s);
         return MGK_ERROR_DEVICE_OUT_OF_MEMORY;
@@ -340,6 +364,21 @@ MGK_API mgk_result mgk_surrogate_forward(mgk_surrogate* s, const float* d_feat, 
     cudaSetDevice(s->device);
     TRY(surrogate_infer(s, d_feat, n, d_out, static_cast<cudaStream_t>(stream)));
     return MGK_SUCCESS;
+}
+
+MGK_API mgk_result mgk_surrogate_forward_tiled(mgk_surrogate* s, const float* d_feat, uint32_t n, float* d_out,
+                                               void* stream) {
+    if (!s || !d_feat || !d_out) return MGK_ERROR_INVALID_POINTER;
+    cudaSetDevice(s->device);
+    TRY(surrogate_infer_tiled(s, d_feat, n, d_out, static_cast<cudaStream_t>(stream)));
+    return MGK_SUCCESS;
+}
+
+MGK_API mgk_result mgk_surrogate_status(mgk_surrogate* s, uint32_t* status) {
+    if (!s || !status) return MGK_ERROR_INVALID_POINTER;
+    cudaSetDevice(s->device);
+    *status = surrogate_status(s);
+    return *status == ~0u ? MGK_ERROR_CUDA : MGK_SUCCESS;
 }
 
 MGK_API mgk_result mgk_surrogate_gradient(mgk_surrogate* s, const mgk_train_config* cfg, const float* d_feat,
@@ -402,6 +441,7 @@ MGK_API mgk_result mgk_surrogate_train(mgk_surrogate* s, const mgk_train_config*
                        float(1.0 / (1.0 - std::pow(double(cfg->beta1), double(s->step)))),
                        float(1.0 / (1.0 - std::pow(double(cfg->beta2), double(s->step))))};
             TRY(launch_adam(s->p, s->grad, s->m, s->v, s->wb, int(s->L.total), a, st));
+            s->img_valid = false;
         }
         float loss = 0.f;
         TRY(cudaMemcpyAsync(&loss, s->loss, 4, cudaMemcpyDeviceToHost, st));

@@ -76,17 +76,40 @@ def _rel(a, b):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("n", [1000, 4096])
-def test_forward_matches_oracle(ctx, n):
+@pytest.mark.parametrize("path", ["fused", "tiled"])
+def test_forward_matches_oracle(ctx, n, path):
+    """Both inference paths (the fused tcgen05 kernel and the tiled mma.sync
+    GEMMs of the training path) against the BF16-emulating oracle."""
     net = M.Surrogate(ctx, seed=7)
     p = O.init_params(11)
     net.set_params(p)
     f, _ = O.random_batch(n, 12)
-    got = net.forward(_dev(f)).cpu().numpy()
+    fwd = net.forward if path == "fused" else net.forward_tiled
+    got = fwd(_dev(f)).cpu().numpy()
     want, _ = O.forward(p, f, bf16_mode=True)
     err = np.abs(got - want)
     assert err.max() <= 2e-2 + 2e-2 * np.abs(want).max(), err.max()
     assert np.median(err) <= 1e-3
     assert np.all(got[:, O.OUT:] == 0.0)  # padding outputs
+    assert net.status() == 0
+    net.close()
+
+
+@pytest.mark.gpu
+def test_fused_forward_many_tiles_per_block(ctx):
+    """300,000 rows: every block of the persistent fused kernel runs many
+    tiles, so the weight ring and all barrier phases wrap around; the result
+    must agree with the tiled path row for row, and follow a weight update."""
+    net = M.Surrogate(ctx, seed=7)
+    f, _ = O.random_batch(300_000, 13)
+    x = _dev(f)
+    for seed in (31, 32):
+        net.set_params(O.init_params(seed))
+        a = net.forward(x).cpu().numpy()
+        b = net.forward_tiled(x).cpu().numpy()
+        err = np.abs(a - b)
+        assert err.max() <= 2e-2 + 2e-2 * np.abs(b).max() and np.median(err) <= 1e-3
+    assert net.status() == 0
     net.close()
 
 
