@@ -252,16 +252,19 @@ MGK_API mgk_result mgk_shade_rays(mgk_context* ctx, const mgk_scene* s, const mg
 /* A learned stand-in for the integrator: an MLP 7 -> 256 -> 256 -> 256 -> 256 -> 8
  * with SiLU activations, BF16 weights and activations, FP32 accumulation, run on
  * tensor cores by the library's own forward / backward / Adam kernels.
- * Inputs: [(r_obs - 55) / 45, cos i, sin i, 2 a / 0.998 - 1, n_x, n_y, n_z],
- * with n the photon direction in the observer's frame.
+ * Inputs: [(r_obs - 55) / 45, cos i, sin i, 2 a / 0.998 - 1, 2 n_x, 2 n_y,
+ * 4 n_z + 3], with n the photon direction in the observer's frame (camera
+ * looking along -z).
  * Outputs: [disk logit, escape logit (horizon logit 0), (r_hit - 10) / 10,
- * disk redshift, escape direction (3), confidence logit].
+ * disk redshift, escape direction minus the undeflected direction (3),
+ * confidence logit].  The undeflected direction is n in the flat camera basis
+ * right = +x, up = (0, sin i, -cos i), back = (0, cos i, sin i).
  * Rays with low confidence or near the critical curve go to RKF45. */
 typedef struct mgk_sample_label {
     int32_t cls;    /* 0 disk, 1 escape, 2 dark */
     float r;        /* (r_hit - 10) / 10 */
     float g;        /* disk redshift factor */
-    float dir[3];   /* escape direction */
+    float dir[3];   /* escape direction minus the undeflected direction */
     float reserved[2];
 } mgk_sample_label;
 
@@ -272,6 +275,9 @@ typedef struct mgk_train_config {
     uint64_t seed;           /* shuffling */
     float w_cls, w_r, w_g, w_dir, w_conf;  /* loss weights */
     float tol_r, tol_g, tol_dir;           /* confidence target: prediction within these */
+    float lr_final;          /* cosine decay of the step size from lr to lr_final over
+                                all steps (default lr_final = lr: constant) */
+    uint32_t reserved;
 } mgk_train_config;
 
 typedef struct mgk_surrogate mgk_surrogate;
@@ -286,7 +292,10 @@ MGK_API mgk_result mgk_surrogate_get_params(mgk_surrogate* net, float* h_params)
 MGK_API mgk_result mgk_surrogate_set_params(mgk_surrogate* net, const float* h_params);
 /* n training samples (features n x 7, labels n) traced by the F64 integrator.
  * n_spin_buckets == 0: camera rays of `base` (its observer, spin and field of
- *   view), from frames seeded seed, seed + 1, ... - a surrogate for one view.
+ *   view), from frames seeded seed, seed + 1, ... that each cover the whole
+ *   field of view: n / (width height) samples per pixel, or a coarser pixel
+ *   grid over the same sensor when n is below the pixel count - a surrogate
+ *   for one view.
  * n_spin_buckets >= 1: observers uniform in r [10, 100] M and inclination
  *   [0, 90] deg, directions uniform on the camera's forward hemisphere, spins
  *   uniform in [0, 0.998] over the buckets (base.spin for one bucket), disk

@@ -76,7 +76,8 @@ class TrainConfig(C.Structure):
     _fields_ = [("batch", C.c_uint32), ("epochs", C.c_uint32), ("lr", C.c_float), ("beta1", C.c_float),
                 ("beta2", C.c_float), ("eps", C.c_float), ("seed", C.c_uint64),
                 ("w_cls", C.c_float), ("w_r", C.c_float), ("w_g", C.c_float), ("w_dir", C.c_float),
-                ("w_conf", C.c_float), ("tol_r", C.c_float), ("tol_g", C.c_float), ("tol_dir", C.c_float)]
+                ("w_conf", C.c_float), ("tol_r", C.c_float), ("tol_g", C.c_float), ("tol_dir", C.c_float),
+                ("lr_final", C.c_float), ("reserved", C.c_uint32)]
 
 
 assert C.sizeof(SampleLabel) == 32

@@ -832,6 +832,20 @@ MGK_API mgk_result mgk_make_samples(mgk_context* ctx, const mgk_scene* base, uin
     mgk_ray_result* res = at<mgk_ray_result>(A, res_off);
     std::vector<float> w(3 * MGK_MAX_BINS, 0.f);
     alignas(16) unsigned char table[sizeof(DevScene<double>)];
+    if (!n_spin_buckets) {
+        // Frames that cover the whole field of view: n / pixels samples per
+        // pixel, or a coarser pixel grid over the same sensor when n is
+        // smaller than the pixel count.
+        const uint64_t pixels = uint64_t(s0.width) * s0.height;
+        if (n >= pixels) {
+            s0.spp = uint32_t(n / pixels);
+        } else {
+            const double f = std::sqrt(double(n) / double(pixels));
+            s0.width = std::max<uint32_t>(1, uint32_t(s0.width * f));
+            s0.height = std::max<uint32_t>(1, uint32_t(s0.height * f));
+            s0.spp = 1;
+        }
+    }
     const uint64_t frame_rays = uint64_t(s0.width) * s0.height * s0.spp;
     const uint32_t nb = n_spin_buckets ? n_spin_buckets : 1;
     uint32_t status = 0;
@@ -859,7 +873,7 @@ MGK_API mgk_result mgk_make_samples(mgk_context* ctx, const mgk_scene* base, uin
                 MGK_CUDA(ctx, launch_camera_features(s, table, first, m, B, d_feat + size_t(j) * 7, st));
             }
             MGK_CUDA(ctx, launch_integrate(s, table, first, m, B, res, ctx->sm_count, st));
-            MGK_CUDA(ctx, launch_labels(res, m, d_lab + j, st));
+            MGK_CUDA(ctx, launch_labels(res, d_feat + size_t(j) * 7, m, d_lab + j, st));
             Counters h;
             MGK_CUDA(ctx, cudaMemcpyAsync(&h, cnt, sizeof(h), cudaMemcpyDeviceToHost, st));
             MGK_CUDA(ctx, cudaStreamSynchronize(st));
@@ -946,7 +960,7 @@ MGK_API mgk_result mgk_render_surrogate(mgk_context* ctx, mgk_surrogate* net, co
             const uint32_t k = std::min(kRouteBatch, m - r0);
             MGK_CUDA(ctx, launch_camera_features(s, table, b + r0, k, B, feat, st));
             MGK_CUDA(ctx, surrogate_infer(net, feat, k, out, st));
-            MGK_CUDA(ctx, launch_route(s, table, r0, k, m, out, conf_min, crit_frac, B, ids, fq, st));
+            MGK_CUDA(ctx, launch_route(s, table, r0, k, m, out, feat, conf_min, crit_frac, B, ids, fq, st));
         }
         MGK_CUDA(ctx, cudaEventRecord(ev[1], st));
         Counters hc;

@@ -84,11 +84,11 @@ cudaError_t launch_resolve(const mgk_scene& s, uint64_t first_pixel, uint32_t n_
 // Surrogate support (kernels.cu).
 cudaError_t launch_generate_samples(const mgk_scene& s, const void* dev_scene, uint64_t seed, uint32_t first,
                                     uint32_t n, const ChunkBuffers& b, float* feat, cudaStream_t stream);
-cudaError_t launch_labels(const mgk_ray_result* res, uint32_t n, void* labels, cudaStream_t stream);
+cudaError_t launch_labels(const mgk_ray_result* res, const float* feat, uint32_t n, void* labels, cudaStream_t stream);
 cudaError_t launch_camera_features(const mgk_scene& s, const void* dev_scene, uint64_t first_ray, uint32_t n,
                                    const ChunkBuffers& b, float* feat, cudaStream_t stream);
 cudaError_t launch_route(const mgk_scene& s, const void* dev_scene, uint32_t base, uint32_t n, uint32_t cap,
-                         const float* out, float conf_min, float crit_frac, const ChunkBuffers& b,
+                         const float* out, const float* feat, float conf_min, float crit_frac, const ChunkBuffers& b,
                          uint32_t* fallback_ids, void* fallback_q, cudaStream_t stream);
 // Inference of the surrogate network (surrogate.cu): 16 floats per row of out.
 cudaError_t surrogate_infer(mgk_surrogate* net, const float* feat, uint32_t n, float* out, cudaStream_t stream);

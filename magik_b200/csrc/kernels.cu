@@ -661,17 +661,18 @@ template <class T> static const DevScene<T>& ds(const void* p) { return *reinter
 
 // ------------------------------------------------------------- surrogate
 // Features of the surrogate network, shared by training and rendering:
-// [(r_obs - 55) / 45, cos i, sin i, 2 a / 0.998 - 1, n_x, n_y, n_z] with n the
-// photon's direction in the observer's frame (camera looks along -z).
+// [(r_obs - 55) / 45, cos i, sin i, 2 a / 0.998 - 1, 2 n_x, 2 n_y, 4 n_z + 3]
+// with n the photon's direction in the observer's frame (camera looks along
+// -z); the direction is scaled so that a camera's field of view spans O(1).
 __device__ __forceinline__ void write_features(float* f, double r_obs, double ci, double si, double spin, double nx,
                                                double ny, double nz) {
     f[0] = float((r_obs - 55.0) / 45.0);
     f[1] = float(ci);
     f[2] = float(si);
     f[3] = float(2.0 * spin / 0.998 - 1.0);
-    f[4] = float(nx);
-    f[5] = float(ny);
-    f[6] = float(nz);
+    f[4] = float(2.0 * nx);
+    f[5] = float(2.0 * ny);
+    f[6] = float(4.0 * nz + 3.0);
 }
 
 // Training samples: each ray has its own observer (r in [10, 100] M,
@@ -722,8 +723,21 @@ cudaError_t launch_generate_samples(const mgk_scene& s, const void* dsc, uint64_
     return cudaGetLastError();
 }
 
-// Labels of the traced samples (layout of mgk_sample_label).
-__global__ void k_labels(const mgk_ray_result* __restrict__ res, uint32_t n, mgk_sample_label* __restrict__ lab) {
+// Undeflected direction of a photon from its features: the camera-frame
+// direction n in the flat camera basis right = +x, up = (0, sin i, -cos i),
+// back = (0, cos i, sin i).  The network predicts the escape direction as a
+// residual from it, which is small away from the black hole.
+__device__ __forceinline__ void flat_direction(const float* f, float d[3]) {
+    const float ci = f[1], si = f[2], nx = 0.5f * f[4], ny = 0.5f * f[5], nz = 0.25f * (f[6] - 3.0f);
+    d[0] = nx;
+    d[1] = ny * si + nz * ci;
+    d[2] = -ny * ci + nz * si;
+}
+
+// Labels of the traced samples (layout of mgk_sample_label); feat holds the
+// samples' features (7 floats each).
+__global__ void k_labels(const mgk_ray_result* __restrict__ res, const float* __restrict__ feat, uint32_t n,
+                         mgk_sample_label* __restrict__ lab) {
     static_assert(sizeof(mgk_sample_label) == 32, "label layout");
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -732,14 +746,16 @@ __global__ void k_labels(const mgk_ray_result* __restrict__ res, uint32_t n, mgk
     L.cls = r.cls == MGK_RAY_DISK ? 0 : (r.cls == MGK_RAY_ESCAPED ? 1 : 2);
     L.r = r.cls == MGK_RAY_DISK ? float((r.r_hit - 10.0) / 10.0) : 0.f;
     L.g = r.cls == MGK_RAY_DISK ? float(r.z) : 0.f;
-    for (int k = 0; k < 3; ++k) L.dir[k] = r.cls == MGK_RAY_ESCAPED ? float(r.dir[k]) : 0.f;
+    float d0[3];
+    flat_direction(feat + size_t(i) * 7, d0);
+    for (int k = 0; k < 3; ++k) L.dir[k] = r.cls == MGK_RAY_ESCAPED ? float(r.dir[k] - double(d0[k])) : 0.f;
     L.reserved[0] = L.reserved[1] = 0.f;
     lab[i] = L;
 }
 
-cudaError_t launch_labels(const mgk_ray_result* res, uint32_t n, void* labels, cudaStream_t st) {
+cudaError_t launch_labels(const mgk_ray_result* res, const float* feat, uint32_t n, void* labels, cudaStream_t st) {
     if (n == 0) return cudaSuccess;
-    k_labels<<<(n + 255) / 256, 256, 0, st>>>(res, n, reinterpret_cast<mgk_sample_label*>(labels));
+    k_labels<<<(n + 255) / 256, 256, 0, st>>>(res, feat, n, reinterpret_cast<mgk_sample_label*>(labels));
     return cudaGetLastError();
 }
 
@@ -809,7 +825,8 @@ __device__ __forceinline__ double critical_distance(double x, double y, double z
 // straight from the network's outputs.
 template <int MODE>
 __global__ void __launch_bounds__(256) k_route(const DevScene<typename ModeT<MODE>::T> P, uint32_t base_ray, uint32_t n,
-                                               uint32_t cap, const float* __restrict__ out, float conf_min,
+                                               uint32_t cap, const float* __restrict__ out,
+                                               const float* __restrict__ feat, float conf_min,
                                                float crit_frac, const void* __restrict__ qx,
                                                const void* __restrict__ qp, const void* __restrict__ qc, void* fqx,
                                                void* fqp, void* fqc, uint32_t* fallback_ids,
@@ -840,9 +857,12 @@ __global__ void __launch_bounds__(256) k_route(const DevScene<typename ModeT<MOD
                     t.z = T(o[3]);
                     lit = t.r_hit >= P.disk_r_in && t.r_hit <= P.disk_r_out;
                 } else if (cls == 1) {
-                    const float dn = sqrtf(o[4] * o[4] + o[5] * o[5] + o[6] * o[6]);
+                    float d[3];
+                    flat_direction(feat + size_t(i) * 7, d);
+                    d[0] += o[4]; d[1] += o[5]; d[2] += o[6];
+                    const float dn = sqrtf(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
                     t.cls = MGK_RAY_ESCAPED;
-                    t.d0 = T(o[4] / dn); t.d1 = T(o[5] / dn); t.d2 = T(o[6] / dn);
+                    t.d0 = T(d[0] / dn); t.d1 = T(d[1] / dn); t.d2 = T(d[2] / dn);
                     t.z = redshift_clamp<T>(c0 / b4[3]);
                     lit = true;
                 }
@@ -861,7 +881,7 @@ __global__ void __launch_bounds__(256) k_route(const DevScene<typename ModeT<MOD
 }
 
 cudaError_t launch_route(const mgk_scene& s, const void* dsc, uint32_t base, uint32_t n, uint32_t cap,
-                         const float* out, float conf_min, float crit_frac, const ChunkBuffers& b,
+                         const float* out, const float* feat, float conf_min, float crit_frac, const ChunkBuffers& b,
                          uint32_t* fallback_ids, void* fallback_q, cudaStream_t st) {
     if (n == 0) return cudaSuccess;
     const bool f64 = s.precision == MGK_PRECISION_F64;
@@ -872,11 +892,11 @@ cudaError_t launch_route(const mgk_scene& s, const void* dsc, uint32_t base, uin
     void* fqc = fq + size_t(cap) * 8 * T;
     const uint32_t blocks = (n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096;
     if (f64)
-        k_route<MGK_PRECISION_F64><<<blocks, 256, 0, st>>>(ds<double>(dsc), base, n, cap, out, conf_min, crit_frac,
+        k_route<MGK_PRECISION_F64><<<blocks, 256, 0, st>>>(ds<double>(dsc), base, n, cap, out, feat, conf_min, crit_frac,
                                                            b.qx, b.qp, b.qc, fqx, fqp, fqc, fallback_ids,
                                                            reinterpret_cast<HitEntry<double>*>(b.hits), b.counters);
     else
-        k_route<MGK_PRECISION_MIXED><<<blocks, 256, 0, st>>>(ds<float>(dsc), base, n, cap, out, conf_min, crit_frac,
+        k_route<MGK_PRECISION_MIXED><<<blocks, 256, 0, st>>>(ds<float>(dsc), base, n, cap, out, feat, conf_min, crit_frac,
                                                              b.qx, b.qp, b.qc, fqx, fqp, fqc, fallback_ids,
                                                              reinterpret_cast<HitEntry<float>*>(b.hits), b.counters);
     return cudaGetLastError();

@@ -286,6 +286,7 @@ MGK_API void mgk_train_defaults(mgk_train_config* c) {
     c->tol_r = 1e-3f;    // 0.01 M in r_hit
     c->tol_g = 1e-3f;
     c->tol_dir = 1e-3f;  // ~1 mrad
+    c->lr_final = c->lr;
 }
 
 MGK_API uint64_t mgk_surrogate_param_count(void) { return param_layout().total; }
@@ -437,7 +438,10 @@ MGK_API mgk_result mgk_surrogate_train(mgk_surrogate* s, const mgk_train_config*
             TRY(forward(s, s->x0, int(B), s->Z, s->H, s->out, st));
             TRY(backward(s, int(B), w, st));
             ++s->step;
-            AdamStep a{cfg->lr, cfg->beta1, cfg->beta2, cfg->eps,
+            const double prog = double(ep * nb + b) / double(cfg->epochs * nb);
+            const float lr = float(double(cfg->lr_final) +
+                                   0.5 * double(cfg->lr - cfg->lr_final) * (1.0 + std::cos(3.14159265358979323846 * prog)));
+            AdamStep a{lr, cfg->beta1, cfg->beta2, cfg->eps,
                        float(1.0 / (1.0 - std::pow(double(cfg->beta1), double(s->step)))),
                        float(1.0 / (1.0 - std::pow(double(cfg->beta2), double(s->step))))};
             TRY(launch_adam(s->p, s->grad, s->m, s->v, s->wb, int(s->L.total), a, st));

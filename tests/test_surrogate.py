@@ -161,8 +161,9 @@ def test_samples_are_f64_traces_of_camera_rays(ctx):
     disk = cls == 0
     assert np.allclose(lab["r"][disk], ((rec["r_hit"][disk] - 10.0) / 10.0).astype(np.float32))
     f = feat.cpu().numpy()
-    assert np.allclose(np.linalg.norm(f[:, 4:7], axis=1), 1.0, atol=1e-6)
-    assert np.all(f[:, 6] < 0)
+    n = np.stack([f[:, 4] / 2, f[:, 5] / 2, (f[:, 6] - 3) / 4], 1)  # feature scaling of the direction
+    assert np.allclose(np.linalg.norm(n, axis=1), 1.0, atol=1e-6)
+    assert np.all(n[:, 2] < 0)
 
 
 @pytest.mark.gpu
