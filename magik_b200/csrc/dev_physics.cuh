@@ -7,7 +7,7 @@
 //   metric_schwarzschild.cuh, internal_math.h) with separate roundings, i.e.
 //   what the reference computes on the CPU.
 //   Fuse::Fma uses the same trees with the marked multiply-adds fused, and
-//   forms the five RHS quotients from one reciprocal.
+//   the rearranged RHS below (rhs_kerr_fused, rhs_schwarzschild_fused).
 // Division and sqrt are IEEE-rounded (-prec-div/-prec-sqrt, no fast math).
 #pragma once
 
@@ -41,7 +41,8 @@ template <class T> struct MP {  // per-metric integrator parameters (metric_kerr
 };
 
 // ------------------------------------------------------------------ RHS
-// Kerr, metric_kerr.cuh:38-105 (same tree; Fuse::None is exact).
+// Kerr, metric_kerr.cuh:38-105: the reference's expression tree (REF32 runs
+// it with Fuse::None and reproduces the reference's roundings).
 template <Fuse F, class T>
 __device__ __forceinline__ void rhs_kerr(const S7<T>& s, T pt, T a, S7<T>& o) {
     const T x = s.x, y = s.y, z = s.z, px = s.px, py = s.py, pz = s.pz;
@@ -57,27 +58,11 @@ __device__ __forceinline__ void rhs_kerr(const S7<T>& s, T pt, T a, S7<T>& o) {
     T r_six = r_cu * r_cu;
     T d = r_sq + a_sq;
     T f_den = mad<F>(a_sq, y_sq, r_quad);
-    T inv_r, inv_sigma, inv_d, inv_f_den_sq, f_;
-    if constexpr (F == Fuse::Fma) {
-        // one reciprocal, 1/(r sigma d f_den), gives all five quotients
-        T rs = r * sigma;
-        T rsd = rs * d;
-        T inv_all = one / (rsd * f_den);  // ~r^9: finite for r below ~1.9e4 in float
-        T inv_rsd = f_den * inv_all;
-        T inv_fden = rsd * inv_all;
-        inv_d = rs * inv_rsd;
-        T inv_rs = d * inv_rsd;
-        inv_r = sigma * inv_rs;
-        inv_sigma = r * inv_rs;
-        inv_f_den_sq = inv_fden * inv_fden;
-        f_ = (two * r_cu) * inv_fden;
-    } else {
-        inv_r = one / r;
-        inv_sigma = one / sigma;
-        inv_d = one / d;
-        inv_f_den_sq = one / (f_den * f_den);
-        f_ = (two * r_cu) / f_den;
-    }
+    T inv_r = one / r;
+    T inv_sigma = one / sigma;
+    T inv_d = one / d;
+    T inv_f_den_sq = one / (f_den * f_den);
+    T f_ = (two * r_cu) / f_den;
     T inv_rsq = inv_r * inv_r;
     T scale_xz = (half * inv_r) * mad<F>(w_sq, inv_sigma, one);
     T scale_y = (half * inv_r) * mad<F>(w_sq + two * a_sq, inv_sigma, one);
@@ -117,7 +102,7 @@ __device__ __forceinline__ void rhs_kerr(const S7<T>& s, T pt, T a, S7<T>& o) {
     o.pz = mad<F>(f_kTp, bz, half_kTp_sq * dfz);
 }
 
-// Schwarzschild, metric_schwarzschild.cuh:8-72.
+// Schwarzschild, metric_schwarzschild.cuh:8-72: the reference's tree.
 template <Fuse F, class T>
 __device__ __forceinline__ void rhs_schwarzschild(const S7<T>& s, T pt, T mass_sign, S7<T>& o) {
     const T x = s.x, y = s.y, z = s.z, px = s.px, py = s.py, pz = s.pz;
@@ -131,26 +116,11 @@ __device__ __forceinline__ void rhs_schwarzschild(const S7<T>& s, T pt, T mass_s
     T r_six = r_cu * r_cu;
     T d = r_sq;
     T f_den = r_quad;
-    T inv_r, inv_sigma, inv_d, inv_f_den_sq, f_;
-    if constexpr (F == Fuse::Fma) {
-        T rs = r * sigma;
-        T rsd = rs * d;
-        T inv_all = one / (rsd * f_den);  // ~r^9: finite for r below ~1.9e4 in float
-        T inv_rsd = f_den * inv_all;
-        T inv_fden = rsd * inv_all;
-        inv_d = rs * inv_rsd;
-        T inv_rs = d * inv_rsd;
-        inv_r = sigma * inv_rs;
-        inv_sigma = r * inv_rs;
-        inv_f_den_sq = inv_fden * inv_fden;
-        f_ = ((mass_sign * two) * r_cu) * inv_fden;
-    } else {
-        inv_r = one / r;
-        inv_sigma = one / sigma;
-        inv_d = one / d;
-        inv_f_den_sq = one / (f_den * f_den);
-        f_ = ((mass_sign * two) * r_cu) / f_den;
-    }
+    T inv_r = one / r;
+    T inv_sigma = one / sigma;
+    T inv_d = one / d;
+    T inv_f_den_sq = one / (f_den * f_den);
+    T f_ = ((mass_sign * two) * r_cu) / f_den;
     T inv_rsq = inv_r * inv_r;
     T sc = (half * inv_r) * mad<F>(w_sq, inv_sigma, one);
     T drx = x * sc, dry = y * sc, drz = z * sc;
@@ -187,6 +157,92 @@ __device__ __forceinline__ void rhs_schwarzschild(const S7<T>& s, T pt, T mass_s
     o.pz = mad<F>(f_kTp, bz, half_kTp_sq * dfz);
 }
 
+
+// Kerr, fused formulation (MIXED and F64): the same Hamiltonian RHS,
+//   dx/dl = p - f (k.p) k,   dp/dl = f (k.p) (grad k).p + (k.p)^2 grad f / 2,
+// k = ((r x - a z)/d, y/r, (r z + a x)/d), d = r^2 + a^2, f = 2 r^3/(r^4 + a^2 y^2),
+// rearranged to need fewer operations:
+//  * one reciprocal 1/(r sigma d f_den) gives 1/d, 1/(r sigma), 1/r, 1/f_den;
+//  * dr/dx_i = (x r/sigma, y d/(r sigma), z r/sigma), using r^2 = (w + sigma)/2;
+//  * sum_j p_j dk_j/dx_i is formed without the nine derivatives: with
+//    g_x = x d - 2 r (r x - a z), g_z = z d - 2 r (r z + a x) and
+//    G = px g_x + pz g_z,  px dkx/dx_i + pz dkz/dx_i = (dr_i G + U_i)/d^2,
+//    U = d (px r + pz a, 0, pz r - px a), and py dky/dx_i = py (r delta_iy - y dr_i)/r^2.
+template <class T> __device__ __forceinline__ void rhs_kerr_fused(const S7<T>& s, T pt, T a, S7<T>& o) {
+    constexpr Fuse F = Fuse::Fma;
+    const T x = s.x, y = s.y, z = s.z, px = s.px, py = s.py, pz = s.pz;
+    const T a_sq = a * a;
+    const T y_sq = y * y;
+    const T w_sq = mad<F>(z, z, mad<F>(x, x, y_sq)) - a_sq;
+    const T sigma = sqrt(mad<F>(w_sq, w_sq, (T(4) * a_sq) * y_sq));
+    const T r = sqrt(T(0.5) * (w_sq + sigma));
+    const T r_sq = r * r;
+    const T d = r_sq + a_sq;
+    const T f_den = mad<F>(a_sq, y_sq, r_sq * r_sq);
+    const T rs = r * sigma;
+    const T rsd = rs * d;
+    const T inv_all = T(1) / (rsd * f_den);  // ~r^9: finite for r below ~1.9e4 in float
+    const T inv_rsd = f_den * inv_all;
+    const T inv_fden = rsd * inv_all;
+    const T inv_d = rs * inv_rsd;
+    const T inv_rs = d * inv_rsd;
+    const T inv_r = sigma * inv_rs;
+    const T sxz = r_sq * inv_rs;
+    const T drx = x * sxz, dry = y * (d * inv_rs), drz = z * sxz;
+    const T r_cu = r_sq * r;
+    const T f_ = (T(2) * r_cu) * inv_fden;
+    const T kx_num = mad<F>(r, x, -(a * z));
+    const T kz_num = mad<F>(r, z, a * x);
+    const T kx = kx_num * inv_d, kz = kz_num * inv_d, ky = y * inv_r;
+    const T kTp = mad<F>(pz, kz, mad<F>(py, ky, px * kx)) - pt;
+    const T f_kTp = f_ * kTp;
+    const T hk2 = (T(0.5) * kTp) * kTp;
+    const T two_r = r + r;
+    const T gx = mad<F>(x, d, -(two_r * kx_num));
+    const T gz = mad<F>(z, d, -(two_r * kz_num));
+    const T G = mad<F>(px, gx, pz * gz);
+    const T Ux = d * mad<F>(px, r, pz * a);
+    const T Uz = d * mad<F>(pz, r, -(px * a));
+    const T c = py * (inv_r * inv_r);
+    const T cy = c * y;
+    const T inv_fden_sq = inv_fden * inv_fden;
+    const T dfdq = (T(2) * mad<F>((T(3) * a_sq) * r_sq, y_sq, -(r_cu * r_cu))) * inv_fden_sq;
+    const T A = f_kTp * (inv_d * inv_d);
+    const T B = mad<F>(hk2, dfdq, -(f_kTp * cy));
+    const T E = mad<F>(-hk2, (((T(4) * a_sq) * r_cu) * y) * inv_fden_sq, f_kTp * (c * r));
+    o.x = mad<F>(-f_kTp, kx, px);
+    o.y = mad<F>(-f_kTp, ky, py);
+    o.z = mad<F>(-f_kTp, kz, pz);
+    o.t = f_kTp - pt;
+    o.px = mad<F>(A, mad<F>(drx, G, Ux), B * drx);
+    o.py = mad<F>(A, dry * G, mad<F>(B, dry, E));
+    o.pz = mad<F>(A, mad<F>(drz, G, Uz), B * drz);
+}
+
+// Schwarzschild, fused formulation: with a = 0, k = x/r, f = 2 m/r,
+// dk_i/dx_j = (delta_ij - k_i k_j)/r and df/dx_i = -f k_i/r, so
+//   dp_i/dl = (f (k.p)/r) (p_i - k_i (k.p_s + (k.p)/2)),  k.p = k.p_s - p_t.
+template <class T>
+__device__ __forceinline__ void rhs_schwarzschild_fused(const S7<T>& s, T pt, T mass_sign, S7<T>& o) {
+    constexpr Fuse F = Fuse::Fma;
+    const T x = s.x, y = s.y, z = s.z, px = s.px, py = s.py, pz = s.pz;
+    const T r = sqrt(mad<F>(z, z, mad<F>(y, y, x * x)));
+    const T inv_r = T(1) / r;
+    const T kx = x * inv_r, ky = y * inv_r, kz = z * inv_r;
+    const T kp = mad<F>(pz, kz, mad<F>(py, ky, px * kx));
+    const T kTp = kp - pt;
+    const T fk = ((mass_sign * T(2)) * inv_r) * kTp;
+    o.x = mad<F>(-fk, kx, px);
+    o.y = mad<F>(-fk, ky, py);
+    o.z = mad<F>(-fk, kz, pz);
+    o.t = fk - pt;
+    const T sc = fk * inv_r;
+    const T q = mad<F>(T(0.5), kTp, kp);
+    o.px = sc * mad<F>(-kx, q, px);
+    o.py = sc * mad<F>(-ky, q, py);
+    o.pz = sc * mad<F>(-kz, q, pz);
+}
+
 // Minkowski, metric_minkowski.cuh:8-13.
 template <class T> __device__ __forceinline__ void rhs_minkowski(const S7<T>& s, T pt, S7<T>& o) {
     o.x = s.px; o.y = s.py; o.z = s.pz; o.t = -pt;
@@ -195,8 +251,13 @@ template <class T> __device__ __forceinline__ void rhs_minkowski(const S7<T>& s,
 
 template <int METRIC, Fuse F, class T>
 __device__ __forceinline__ void rhs(const S7<T>& s, T pt, const MP<T>& m, S7<T>& o) {
-    if constexpr (METRIC == 2) rhs_kerr<F, T>(s, pt, m.spin, o);
-    else if constexpr (METRIC == 1) rhs_schwarzschild<F, T>(s, pt, m.mass_sign, o);
+    if constexpr (METRIC == 2) {
+        if constexpr (F == Fuse::Fma) rhs_kerr_fused<T>(s, pt, m.spin, o);
+        else rhs_kerr<F, T>(s, pt, m.spin, o);
+    } else if constexpr (METRIC == 1) {
+        if constexpr (F == Fuse::Fma) rhs_schwarzschild_fused<T>(s, pt, m.mass_sign, o);
+        else rhs_schwarzschild<F, T>(s, pt, m.mass_sign, o);
+    }
     else rhs_minkowski<T>(s, pt, o);
 }
 

@@ -1,31 +1,37 @@
 """Algorithmic operation counts of the integrator, used for the roofline.
 
-Source-level counts (+, -, *, /, sqrt = 1; fused multiply-add = 2; pow = 1)
-of the formulation the kernels execute (a division or a square root counts
-as one operation however it is implemented): the 7-component state (x, y, z, t,
-px, py, pz) with the conserved p_t carried beside it.  The CPU oracle counts
-the same expressions with an op-counting scalar (8 components, p_t included);
-tests/test_host.py checks that the figures below equal its counts minus the
-p_t work, which is identically zero and skipped by the kernels.
+The roofline counts the work of the reference's algorithm, not of this
+library's formulation: source-level counts (+, -, *, /, sqrt = 1; a fused
+multiply-add = 2) of the reference's expression trees for the RHS
+(metric_kerr.cuh:38-105, metric_schwarzschild.cuh:8-72) and the RKF45
+attempt (internal_math.h:2160-2205, relativity_utilities.cuh:10-55) on its
+8-component state.  The CPU oracle evaluates those trees with an
+op-counting scalar; tests/test_host.py checks the figures below against it.
 
-  RHS                           Kerr 162   Schwarzschild 132 (the fused
-                                formulation: one reciprocal and eight
-                                products in place of five quotients)
-  one RKF45 attempt             6 RHS + 25 coefficient products + 210 stage
-                                combinations + 70 (5th-order solution)
-                                + 63 (error) + 36 (norm) + 4 (proposal)
-  one crossing sub-step         6 RHS + 20 coefficient products + 210 + 70
+  RHS            Kerr 156          Schwarzschild 126
+  RKF45 attempt  Kerr 1398         Schwarzschild 1218  (6 RHS + stage
+                 combinations, 5th-order solution, error, norm, proposal)
+
+A crossing sub-step (the secant refinement of a disk or escape crossing, an
+addition of this library) is counted as 6 RHS of the reference tree plus
+its 300 stage-combination operations.
+
+The kernels execute fewer operations than that (the fused RHS of the MIXED
+and F64 modes, and 7 state components: dp_t/dl = 0 is not integrated);
+IMPLEMENTATION holds those counts (RHS, attempt) for information.
 """
 
-RHS = {2: 162, 1: 132, 0: 0}
-ATTEMPT_OVERHEAD = 25 + 210 + 70 + 63 + 36 + 4
-SUBSTEP_OVERHEAD = 20 + 210 + 70
-# p_t terms the 8-component count includes and the kernels skip
-PT_TERMS_PER_ATTEMPT = 54
+RHS = {2: 156, 1: 126, 0: 0}
+ATTEMPT = {2: 1398, 1: 1218, 0: 0}
+SUBSTEP_OVERHEAD = 300
+
+# operations of the fused formulation the MIXED / F64 kernels run, counted by
+# the oracle on its 8-component state: (RHS, attempt)
+IMPLEMENTATION = {2: (119, 1176), 1: (38, 690)}
 
 
 def attempt_flops(metric):
-    return 6 * RHS[metric] + ATTEMPT_OVERHEAD
+    return ATTEMPT[metric]
 
 
 def substep_flops(metric):

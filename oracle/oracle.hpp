@@ -70,27 +70,11 @@ template <Fuse F, class T> inline GState<T> rhs_kerr(const GState<T>& s, T a) {
 
     T d = r_sq + a_sq;
     T f_den = mad<F>(a_sq, y_sq, r_quad);
-    T inv_r, inv_sigma, inv_d, inv_f_den_sq, f_;
-    if constexpr (F == Fuse::Fma) {
-        // fused formulation: 1/(r sigma d f_den) gives all five quotients
-        T rs = r * sigma;
-        T rsd = rs * d;
-        T inv_all = one / (rsd * f_den);  // ~r^9: finite for r below ~1.9e4 in float
-        T inv_rsd = f_den * inv_all;
-        T inv_fden = rsd * inv_all;
-        inv_d = rs * inv_rsd;
-        T inv_rs = d * inv_rsd;
-        inv_r = sigma * inv_rs;
-        inv_sigma = r * inv_rs;
-        inv_f_den_sq = inv_fden * inv_fden;
-        f_ = (two * r_cu) * inv_fden;
-    } else {
-        inv_r = one / r;
-        inv_sigma = one / sigma;
-        inv_d = one / d;
-        inv_f_den_sq = one / (f_den * f_den);
-        f_ = (two * r_cu) / f_den;
-    }
+    T inv_r = one / r;
+    T inv_sigma = one / sigma;
+    T inv_d = one / d;
+    T inv_f_den_sq = one / (f_den * f_den);
+    T f_ = (two * r_cu) / f_den;
     T inv_rsq = inv_r * inv_r;
     T scale_xz = (half * inv_r) * mad<F>(w_sq, inv_sigma, one);
     T scale_y = (half * inv_r) * mad<F>(w_sq + two * a_sq, inv_sigma, one);
@@ -152,26 +136,11 @@ template <Fuse F, class T> inline GState<T> rhs_schwarzschild(const GState<T>& s
 
     T d = r_sq;
     T f_den = r_quad;
-    T inv_r, inv_sigma, inv_d, inv_f_den_sq, f_;
-    if constexpr (F == Fuse::Fma) {
-        T rs = r * sigma;
-        T rsd = rs * d;
-        T inv_all = one / (rsd * f_den);  // ~r^9: finite for r below ~1.9e4 in float
-        T inv_rsd = f_den * inv_all;
-        T inv_fden = rsd * inv_all;
-        inv_d = rs * inv_rsd;
-        T inv_rs = d * inv_rsd;
-        inv_r = sigma * inv_rs;
-        inv_sigma = r * inv_rs;
-        inv_f_den_sq = inv_fden * inv_fden;
-        f_ = ((mass_sign * two) * r_cu) * inv_fden;
-    } else {
-        inv_r = one / r;
-        inv_sigma = one / sigma;
-        inv_d = one / d;
-        inv_f_den_sq = one / (f_den * f_den);
-        f_ = ((mass_sign * two) * r_cu) / f_den;
-    }
+    T inv_r = one / r;
+    T inv_sigma = one / sigma;
+    T inv_d = one / d;
+    T inv_f_den_sq = one / (f_den * f_den);
+    T f_ = ((mass_sign * two) * r_cu) / f_den;
     T inv_rsq = inv_r * inv_r;
     T scale = (half * inv_r) * mad<F>(w_sq, inv_sigma, one);
     T drx = x * scale, dry = y * scale, drz = z * scale;
@@ -213,6 +182,84 @@ template <Fuse F, class T> inline GState<T> rhs_schwarzschild(const GState<T>& s
     return o;
 }
 
+// Fused formulation of the Kerr RHS (the library's MIXED and F64 modes): the
+// same Hamiltonian right-hand side as rhs_kerr, rearranged so that one
+// reciprocal gives 1/d, 1/(r sigma), 1/r and 1/f_den, dr/dx_i = (x r/sigma,
+// y d/(r sigma), z r/sigma), and sum_j p_j dk_j/dx_i comes from
+// G = px (x d - 2 r kx_num) + pz (z d - 2 r kz_num):
+//   px dkx/dx_i + pz dkz/dx_i = (dr_i G + U_i)/d^2, U = d (px r + pz a, 0, pz r - px a),
+//   py dky/dx_i = py (r delta_iy - y dr_i)/r^2.
+// The device code evaluates exactly these operations in this order.
+template <class T> inline GState<T> rhs_kerr_fused(const GState<T>& s, T a) {
+    constexpr Fuse F = Fuse::Fma;
+    const T x = s.x.x, y = s.x.y, z = s.x.z;
+    const T pt = s.p.t, px = s.p.x, py = s.p.y, pz = s.p.z;
+    const T a_sq = a * a;
+    const T y_sq = y * y;
+    const T w_sq = mad<F>(z, z, mad<F>(x, x, y_sq)) - a_sq;
+    const T sigma = sq_root(mad<F>(w_sq, w_sq, (T(4) * a_sq) * y_sq));
+    const T r = sq_root(T(0.5) * (w_sq + sigma));
+    const T r_sq = r * r;
+    const T d = r_sq + a_sq;
+    const T f_den = mad<F>(a_sq, y_sq, r_sq * r_sq);
+    const T rs = r * sigma;
+    const T rsd = rs * d;
+    const T inv_all = T(1) / (rsd * f_den);
+    const T inv_rsd = f_den * inv_all;
+    const T inv_fden = rsd * inv_all;
+    const T inv_d = rs * inv_rsd;
+    const T inv_rs = d * inv_rsd;
+    const T inv_r = sigma * inv_rs;
+    const T sxz = r_sq * inv_rs;
+    const T drx = x * sxz, dry = y * (d * inv_rs), drz = z * sxz;
+    const T r_cu = r_sq * r;
+    const T f_ = (T(2) * r_cu) * inv_fden;
+    const T kx_num = mad<F>(r, x, -(a * z));
+    const T kz_num = mad<F>(r, z, a * x);
+    const T kx = kx_num * inv_d, kz = kz_num * inv_d, ky = y * inv_r;
+    const T kTp = mad<F>(pz, kz, mad<F>(py, ky, px * kx)) - pt;
+    const T f_kTp = f_ * kTp;
+    const T hk2 = (T(0.5) * kTp) * kTp;
+    const T two_r = r + r;
+    const T gx = mad<F>(x, d, -(two_r * kx_num));
+    const T gz = mad<F>(z, d, -(two_r * kz_num));
+    const T G = mad<F>(px, gx, pz * gz);
+    const T Ux = d * mad<F>(px, r, pz * a);
+    const T Uz = d * mad<F>(pz, r, -(px * a));
+    const T c = py * (inv_r * inv_r);
+    const T cy = c * y;
+    const T inv_fden_sq = inv_fden * inv_fden;
+    const T dfdq = (T(2) * mad<F>((T(3) * a_sq) * r_sq, y_sq, -(r_cu * r_cu))) * inv_fden_sq;
+    const T A = f_kTp * (inv_d * inv_d);
+    const T B = mad<F>(hk2, dfdq, -(f_kTp * cy));
+    const T E = mad<F>(-hk2, (((T(4) * a_sq) * r_cu) * y) * inv_fden_sq, f_kTp * (c * r));
+    GState<T> o;
+    o.x = V4<T>{mad<F>(-f_kTp, kx, px), mad<F>(-f_kTp, ky, py), mad<F>(-f_kTp, kz, pz), f_kTp - pt};
+    o.p = V4<T>{mad<F>(A, mad<F>(drx, G, Ux), B * drx), mad<F>(A, dry * G, mad<F>(B, dry, E)),
+                mad<F>(A, mad<F>(drz, G, Uz), B * drz), T(0)};
+    return o;
+}
+
+// Fused formulation of the Schwarzschild RHS: with a = 0, k = x/r, f = 2 m/r,
+//   dp_i/dl = (f (k.p)/r) (p_i - k_i (k.p_s + (k.p)/2)),  k.p = k.p_s - p_t.
+template <class T> inline GState<T> rhs_schwarzschild_fused(const GState<T>& s, T mass_sign) {
+    constexpr Fuse F = Fuse::Fma;
+    const T x = s.x.x, y = s.x.y, z = s.x.z;
+    const T pt = s.p.t, px = s.p.x, py = s.p.y, pz = s.p.z;
+    const T r = sq_root(mad<F>(z, z, mad<F>(y, y, x * x)));
+    const T inv_r = T(1) / r;
+    const T kx = x * inv_r, ky = y * inv_r, kz = z * inv_r;
+    const T kp = mad<F>(pz, kz, mad<F>(py, ky, px * kx));
+    const T kTp = kp - pt;
+    const T fk = ((mass_sign * T(2)) * inv_r) * kTp;
+    const T sc = fk * inv_r;
+    const T q = mad<F>(T(0.5), kTp, kp);
+    GState<T> o;
+    o.x = V4<T>{mad<F>(-fk, kx, px), mad<F>(-fk, ky, py), mad<F>(-fk, kz, pz), fk - pt};
+    o.p = V4<T>{sc * mad<F>(-kx, q, px), sc * mad<F>(-ky, q, py), sc * mad<F>(-kz, q, pz), T(0)};
+    return o;
+}
+
 // Minkowski RHS; src/renderer/relativity/metric_minkowski.cuh:8-13.
 template <class T> inline GState<T> rhs_minkowski(const GState<T>& s) {
     GState<T> o;
@@ -237,8 +284,13 @@ template <class T> struct MetricParams {
 };
 
 template <Fuse F, class T> inline GState<T> rhs(const GState<T>& s, const MetricParams<T>& m) {
-    if (m.metric == KERR) return rhs_kerr<F, T>(s, m.spin);
-    if (m.metric == SCHWARZSCHILD) return rhs_schwarzschild<F, T>(s, m.mass_sign);
+    if constexpr (F == Fuse::Fma) {
+        if (m.metric == KERR) return rhs_kerr_fused<T>(s, m.spin);
+        if (m.metric == SCHWARZSCHILD) return rhs_schwarzschild_fused<T>(s, m.mass_sign);
+    } else {
+        if (m.metric == KERR) return rhs_kerr<F, T>(s, m.spin);
+        if (m.metric == SCHWARZSCHILD) return rhs_schwarzschild<F, T>(s, m.mass_sign);
+    }
     return rhs_minkowski<T>(s);
 }
 
