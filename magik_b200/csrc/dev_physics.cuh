@@ -38,7 +38,17 @@ template <class T> struct MP {  // per-metric integrator parameters (metric_kerr
     T spin_abs_gt1;  // 1 if |spin| > 1 (Kerr never captures then)
     T h_max, abs_tol, rel_tol;
     uint32_t n_max;
+    T a_sq, two_a_sq, three_a_sq, four_a_sq;  // a^2 and multiples, rounded in T (fused RHS)
 };
+
+// Fills the spin constants of m from m.spin (host or device; the same
+// roundings as evaluating a * a, 2 a^2, 3 a^2, 4 a^2 in T).
+template <class T> __host__ __device__ inline void set_spin_consts(MP<T>& m) {
+    m.a_sq = m.spin * m.spin;
+    m.two_a_sq = T(2) * m.a_sq;
+    m.three_a_sq = T(3) * m.a_sq;
+    m.four_a_sq = T(4) * m.a_sq;
+}
 
 // ------------------------------------------------------------------ RHS
 // Kerr, metric_kerr.cuh:38-105: the reference's expression tree (REF32 runs
@@ -168,13 +178,13 @@ __device__ __forceinline__ void rhs_schwarzschild(const S7<T>& s, T pt, T mass_s
 //    g_x = x d - 2 r (r x - a z), g_z = z d - 2 r (r z + a x) and
 //    G = px g_x + pz g_z,  px dkx/dx_i + pz dkz/dx_i = (dr_i G + U_i)/d^2,
 //    U = d (px r + pz a, 0, pz r - px a), and py dky/dx_i = py (r delta_iy - y dr_i)/r^2.
-template <class T> __device__ __forceinline__ void rhs_kerr_fused(const S7<T>& s, T pt, T a, S7<T>& o) {
+template <class T> __device__ __forceinline__ void rhs_kerr_fused(const S7<T>& s, T pt, const MP<T>& m, S7<T>& o) {
     constexpr Fuse F = Fuse::Fma;
     const T x = s.x, y = s.y, z = s.z, px = s.px, py = s.py, pz = s.pz;
-    const T a_sq = a * a;
+    const T a = m.spin, a_sq = m.a_sq;
     const T y_sq = y * y;
     const T w_sq = mad<F>(z, z, mad<F>(x, x, y_sq)) - a_sq;
-    const T sigma = sqrt(mad<F>(w_sq, w_sq, (T(4) * a_sq) * y_sq));
+    const T sigma = sqrt(mad<F>(w_sq, w_sq, m.four_a_sq * y_sq));
     const T r = sqrt(T(0.5) * (w_sq + sigma));
     const T r_sq = r * r;
     const T d = r_sq + a_sq;
@@ -196,7 +206,7 @@ template <class T> __device__ __forceinline__ void rhs_kerr_fused(const S7<T>& s
     const T kx = kx_num * inv_d, kz = kz_num * inv_d, ky = y * inv_r;
     const T kTp = mad<F>(pz, kz, mad<F>(py, ky, px * kx)) - pt;
     const T f_kTp = f_ * kTp;
-    const T hk2 = (T(0.5) * kTp) * kTp;
+    const T kTp2 = kTp * kTp;
     const T two_r = r + r;
     const T gx = mad<F>(x, d, -(two_r * kx_num));
     const T gz = mad<F>(z, d, -(two_r * kz_num));
@@ -206,10 +216,12 @@ template <class T> __device__ __forceinline__ void rhs_kerr_fused(const S7<T>& s
     const T c = py * (inv_r * inv_r);
     const T cy = c * y;
     const T inv_fden_sq = inv_fden * inv_fden;
-    const T dfdq = (T(2) * mad<F>((T(3) * a_sq) * r_sq, y_sq, -(r_cu * r_cu))) * inv_fden_sq;
+    // (k.p)^2/2 df/dx_i = (k.p)^2 (dq dr_i - delta_iy 2 a^2 r^3 y / f_den^2),
+    // dq = (3 a^2 r^2 y^2 - r^6) / f_den^2
+    const T dq = mad<F>(m.three_a_sq * r_sq, y_sq, -(r_cu * r_cu)) * inv_fden_sq;
     const T A = f_kTp * (inv_d * inv_d);
-    const T B = mad<F>(hk2, dfdq, -(f_kTp * cy));
-    const T E = mad<F>(-hk2, (((T(4) * a_sq) * r_cu) * y) * inv_fden_sq, f_kTp * (c * r));
+    const T B = mad<F>(kTp2, dq, -(f_kTp * cy));
+    const T E = mad<F>(-kTp2, ((m.two_a_sq * r_cu) * y) * inv_fden_sq, f_kTp * (c * r));
     o.x = mad<F>(-f_kTp, kx, px);
     o.y = mad<F>(-f_kTp, ky, py);
     o.z = mad<F>(-f_kTp, kz, pz);
@@ -252,7 +264,7 @@ template <class T> __device__ __forceinline__ void rhs_minkowski(const S7<T>& s,
 template <int METRIC, Fuse F, class T>
 __device__ __forceinline__ void rhs(const S7<T>& s, T pt, const MP<T>& m, S7<T>& o) {
     if constexpr (METRIC == 2) {
-        if constexpr (F == Fuse::Fma) rhs_kerr_fused<T>(s, pt, m.spin, o);
+        if constexpr (F == Fuse::Fma) rhs_kerr_fused<T>(s, pt, m, o);
         else rhs_kerr<F, T>(s, pt, m.spin, o);
     } else if constexpr (METRIC == 1) {
         if constexpr (F == Fuse::Fma) rhs_schwarzschild_fused<T>(s, pt, m.mass_sign, o);

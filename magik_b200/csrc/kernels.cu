@@ -32,12 +32,14 @@ namespace mgk {
 
 constexpr unsigned kFull = 0xffffffffu;
 #ifndef MGK_INTEGRATE_THREADS
-#define MGK_INTEGRATE_THREADS 256
+#define MGK_INTEGRATE_THREADS 128
 #endif
 #ifndef MGK_INTEGRATE_MIN_BLOCKS
-#define MGK_INTEGRATE_MIN_BLOCKS 3
+#define MGK_INTEGRATE_MIN_BLOCKS 7
 #endif
 constexpr int kIntegrateThreads = MGK_INTEGRATE_THREADS;
+// FP64 state needs about twice the registers: fewer resident blocks
+constexpr int kIntegrateMinBlocksF64 = 4;
 constexpr uint32_t kChunk = 64;  // queue entries a warp takes per refill
 
 template <int MODE> struct ModeT { using T = float; static constexpr Fuse F = Fuse::Fma; };
@@ -210,7 +212,7 @@ template <class T> __device__ __forceinline__ S7<T> s7(const T* v) {
 // band hands its ray to the resume queue.  Both pushes are warp-ballot
 // compactions with one atomic per warp.
 template <int METRIC, int MODE>
-__global__ void __launch_bounds__(kIntegrateThreads, MGK_INTEGRATE_MIN_BLOCKS)
+__global__ void __launch_bounds__(kIntegrateThreads, MODE == MGK_PRECISION_F64 ? kIntegrateMinBlocksF64 : MGK_INTEGRATE_MIN_BLOCKS)
     k_integrate(const DevScene<typename ModeT<MODE>::T> P, uint32_t nq, const void* __restrict__ qx,
                 const void* __restrict__ qp, const void* __restrict__ qc,
                 RefineEntry<typename ModeT<MODE>::T>* refq, ResumeEntry<typename ModeT<MODE>::T>* resq,
@@ -577,6 +579,7 @@ __global__ void __launch_bounds__(64) k_trace_geodesic(const TraceJob* __restric
     MP<float> m{};
     m.spin = J.spin; m.mass_sign = J.mass_sign; m.horizon = J.horizon; m.spin_abs_gt1 = J.spin_abs_gt1;
     m.h_max = 1000.0f; m.abs_tol = J.atol; m.rel_tol = J.rtol; m.n_max = uint32_t(J.n_max);
+    set_spin_consts(m);
     const int metric = J.metric;
     V4<float> x0{J.x0[0], J.x0[1], J.x0[2], J.x0[3]};
     Sym4<float> g = compute_g<float>(metric, x0.x, x0.y, x0.z, J.spin, J.mass_sign);
@@ -1050,6 +1053,8 @@ template <class T> static void fill_t(const mgk_scene& s, const float* xyz_w, De
     P->md.abs_tol = s.abs_tol;
     P->md.rel_tol = s.rel_tol;
     P->md.n_max = s.n_max_substep;
+    set_spin_consts(P->m);
+    set_spin_consts(P->md);
     for (int i = 0; i < 4; ++i) {
         P->cam[i] = T(c.cam_pos[i]);
         P->u_obs[i] = T(c.u_obs[i]);

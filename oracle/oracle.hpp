@@ -219,7 +219,7 @@ template <class T> inline GState<T> rhs_kerr_fused(const GState<T>& s, T a) {
     const T kx = kx_num * inv_d, kz = kz_num * inv_d, ky = y * inv_r;
     const T kTp = mad<F>(pz, kz, mad<F>(py, ky, px * kx)) - pt;
     const T f_kTp = f_ * kTp;
-    const T hk2 = (T(0.5) * kTp) * kTp;
+    const T kTp2 = kTp * kTp;
     const T two_r = r + r;
     const T gx = mad<F>(x, d, -(two_r * kx_num));
     const T gz = mad<F>(z, d, -(two_r * kz_num));
@@ -229,10 +229,10 @@ template <class T> inline GState<T> rhs_kerr_fused(const GState<T>& s, T a) {
     const T c = py * (inv_r * inv_r);
     const T cy = c * y;
     const T inv_fden_sq = inv_fden * inv_fden;
-    const T dfdq = (T(2) * mad<F>((T(3) * a_sq) * r_sq, y_sq, -(r_cu * r_cu))) * inv_fden_sq;
+    const T dq = mad<F>((T(3) * a_sq) * r_sq, y_sq, -(r_cu * r_cu)) * inv_fden_sq;
     const T A = f_kTp * (inv_d * inv_d);
-    const T B = mad<F>(hk2, dfdq, -(f_kTp * cy));
-    const T E = mad<F>(-hk2, (((T(4) * a_sq) * r_cu) * y) * inv_fden_sq, f_kTp * (c * r));
+    const T B = mad<F>(kTp2, dq, -(f_kTp * cy));
+    const T E = mad<F>(-kTp2, ((T(2) * a_sq) * r_cu) * y * inv_fden_sq, f_kTp * (c * r));
     GState<T> o;
     o.x = V4<T>{mad<F>(-f_kTp, kx, px), mad<F>(-f_kTp, ky, py), mad<F>(-f_kTp, kz, pz), f_kTp - pt};
     o.p = V4<T>{mad<F>(A, mad<F>(drx, G, Ux), B * drx), mad<F>(A, dry * G, mad<F>(B, dry, E)),
