@@ -395,8 +395,13 @@ def run_gpu(args, rank, world, local_rank):
         # runs after the timed region; its own timings are inside "surrogate"
         out["surrogate"] = run_surrogate(args, ctx, s, d_stars, d_w, ms, max(1, min(args.steps, 3)))
     if world == 1 and not args.no_cpu_baseline:
-        v, thr, desc = cpu_render_sample(s, stars, w, args.cpu_seconds, M.abi.PRECISION_MIXED)
-        out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": thr, "kind": "port", "sample": desc}
+        from oracle import oracle_py as O
+        use_ref = O.ref_available()
+        v, thr, desc = cpu_render_sample(s, stars, w, args.cpu_seconds,
+                                         M.abi.PRECISION_REF32 if use_ref else M.abi.PRECISION_MIXED,
+                                         reference=use_ref)
+        out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": thr, "kind": "reference" if use_ref else "port",
+                               "sample": desc}
     return out
 
 

@@ -60,6 +60,9 @@ def ref():
                                          abi.TraceMetricParams, abi.TraceIntegratorParams]
         R.ref_trace_geodesic.restype = C.c_int
         R.ref_cmf_weights.argtypes = [C.c_uint, C.c_float, C.c_float, C.POINTER(C.c_float)]
+        R.ref_render_pixels.argtypes = [C.POINTER(abi.Scene), C.POINTER(abi.Star), C.c_uint32, C.POINTER(C.c_float),
+                                        C.c_uint64, C.c_uint32, C.c_uint64, C.POINTER(C.c_double), C.c_int]
+        R.ref_render_pixels.restype = C.c_int
         _ref = R
     return _ref
 
@@ -135,6 +138,20 @@ def render_pixels(scene, stars, weights, first_pixel, n_pixels, nthreads=None, s
                             w.ctypes.data_as(C.POINTER(C.c_float)), first_pixel, n_pixels, stride,
                             out.ctypes.data_as(C.POINTER(C.c_double)), C.byref(att), nthreads or os.cpu_count())
     return out, att.value
+
+
+def ref_render_pixels(scene, stars, weights, first_pixel, n_pixels, nthreads=None, stride=1):
+    """Pixels rendered with the reference's own RKF45 step (oracle/_ref) inside
+    the oracle's camera, termination and spectral stages; REF32 semantics.
+    Returns (xyz [n, 3] float64, None): the reference reports no retries."""
+    stars = np.ascontiguousarray(stars)
+    w = np.ascontiguousarray(weights, dtype=np.float32)
+    out = np.zeros((n_pixels, 3), dtype=np.float64)
+    rc = ref().ref_render_pixels(C.byref(scene), stars.ctypes.data_as(C.POINTER(abi.Star)), len(stars),
+                                 w.ctypes.data_as(C.POINTER(C.c_float)), first_pixel, n_pixels, stride,
+                                 out.ctypes.data_as(C.POINTER(C.c_double)), nthreads or os.cpu_count())
+    assert rc == 0, rc
+    return out, None
 
 
 def count_ops(metric, fused):

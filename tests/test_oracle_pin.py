@@ -98,3 +98,20 @@ def test_reference_colour_weights_golden():
         width = (float(hi) - float(lo)) / int(n)
         assert abs(ref[:, 1].sum() * width - 1.0) < 1e-5
         assert abs(ours[:, 1].sum() * width - 1.0) < 1e-5
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference tracer not built (needs the reference sources)")
+@pytest.mark.parametrize("metric", [abi.METRIC_KERR, abi.METRIC_SCHWARZSCHILD])
+def test_oracle_render_matches_reference_step_render(metric):
+    """The oracle's REF32 render against the same render driven by the
+    reference's own compiled RKF45 step: the two differ only where the
+    reference's powf and the oracle's double pow round a step size apart."""
+    import magik_b200 as M
+    s = M.scene_defaults(width=48, height=27, spp=1, precision=abi.PRECISION_REF32, metric=metric)
+    stars = M.star_catalog(0x57A25, 20000)
+    w = M.xyz_weights(s.n_bins)
+    n = s.width * s.height
+    a, _ = O.render_pixels(s, stars, w, 0, n, nthreads=4)
+    b, _ = O.ref_render_pixels(s, stars, w, 0, n, nthreads=4)
+    assert np.mean(np.all(a == b, axis=1)) >= 0.98
+    assert np.abs(a - b).sum() <= 1e-5 * np.abs(a).sum()
