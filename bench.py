@@ -28,6 +28,12 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+# DRAM bytes per ray of k_integrate and per row of k_mlp_infer_tc, from one
+# ncu capture each of a smaller case (profiles/k_integrate_kerr_640x360x16.md,
+# profiles/k_mlp_infer_tc_1M_rows.md); the traffic grows with the units, so
+# the roofline scales it to the launch.
+INTEGRATE_DRAM_BYTES_PER_RAY = 618.6e6 / 3_686_400
+MLP_DRAM_BYTES_PER_ROW = 44.2e6 / 1_048_576
 N_STARS = 100_000
 STAR_SEED = 0x57A25
 WORKLOAD = "kerr_a0.9_r50M_i75_fov60_1920x1080_16spp_32bins_1e5stars_rtol1e-7"
@@ -248,8 +254,9 @@ def run_surrogate(args, ctx, s, d_stars, d_w, film_mixed_ms, steps):
 
     # fused inference kernel alone (tensor-core roofline)
     x = feat[: 1 << 22].contiguous()
+    n_rows = int(x.shape[0])
     fwd_ms, _ = timed(lambda: net.forward(x))
-    fwd_tflops = (1 << 22) * 400_896 / (fwd_ms * 1e-3) / 1e12
+    fwd_tflops = n_rows * 400_896 / (fwd_ms * 1e-3) / 1e12
     peaks = measured_peaks()
     bf16_peak = peaks.get("bf16_tflops")
 
@@ -277,8 +284,9 @@ def run_surrogate(args, ctx, s, d_stars, d_w, film_mixed_ms, steps):
         "inference_roofline": {"bound": "tensor", "kernel": "k_mlp_infer_tc (tcgen05, fused 5 layers)",
                                "achieved": fwd_tflops, "peak": bf16_peak, "unit": "TFLOP/s",
                                "frac": (fwd_tflops / bf16_peak) if bf16_peak else None,
+                               "traffic": MLP_DRAM_BYTES_PER_ROW * n_rows,
                                "peak_source": "MEASURED_PEAKS.json bf16_tflops (cuBLAS burst), of measured",
-                               "flop_per_ray": 400_896, "rows": 1 << 22, "ms": fwd_ms},
+                               "flop_per_ray": 400_896, "rows": n_rows, "ms": fwd_ms},
     }
 
 
@@ -375,7 +383,9 @@ def run_gpu(args, rank, world, local_rank):
                 "d2h_bytes_per_step": int(h_film.numel() * 4)},
         "roofline": {"bound": "fp32", "kernel": "k_integrate + k_refine + k_tail (one chunk)",
                      "achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "TFLOP/s",
-                     "frac": achieved / peak, "traffic": None,
+                     "frac": achieved / peak, "traffic": INTEGRATE_DRAM_BYTES_PER_RAY * rays,
+                     "traffic_note": "bytes per launch of k_integrate: ncu DRAM bytes per ray of a 640x360x16 "
+                                     "capture x rays of this frame",
                      "peak_source": "measured in this run by mgk_fp32_peak (FMA probe kernel); "
                                     "MEASURED_PEAKS.json has no FP32 figure",
                      "flop_per_attempt": FL.attempt_flops(s.metric),

@@ -220,11 +220,18 @@ def test_trained_surrogate_render_error_and_fallback(ctx):
     n_pix = s.width * s.height
     ref = torch.zeros(n_pix * 3, dtype=torch.float32, device="cuda")
     ctx.render(base, d_stars, ref)
-    errs, fb = [], []
-    for conf_min in (0.0, 0.9, 0.99):
+    plain = torch.zeros_like(ref)
+    plain_attempts = ctx.render(s, d_stars, plain).attempts
+    errs, fb, att = [], [], []
+    for conf_min in (-1.0, 0.0, 0.9, 0.99, 2.0):
         film = torch.zeros_like(ref)
-        st = M.render_surrogate(ctx, net, s, d_stars, film, conf_min=conf_min, crit_frac=0.02)
+        st = M.render_surrogate(ctx, net, s, d_stars, film, conf_min=conf_min, crit_frac=0.02 if conf_min >= 0 else 0.0)
         errs.append(float((film - ref).abs().view(-1, 3).mean().item()))
         fb.append(st.fallback_rays / (n_pix * s.spp))
-    assert fb[0] <= fb[1] <= fb[2] <= 1.0
-    assert errs[2] <= errs[0] + 1e-6
+        att.append(st.attempts)
+    # what the network gains: the integrator work it takes away ...
+    assert att[0] == 0 and fb[0] == 0.0
+    assert fb[1] <= fb[2] <= fb[3] <= fb[4] == 1.0
+    assert att[1] <= att[2] <= att[3] <= att[4] == plain_attempts
+    # ... and what that costs in accuracy: the stricter the routing the closer to RKF45
+    assert errs[4] <= errs[3] + 1e-6 <= errs[0] + 2e-6
