@@ -57,6 +57,8 @@ def parse_args():
     ap.add_argument("--no-surrogate", action="store_true", help="skip the surrogate+fallback leg")
     ap.add_argument("--surrogate-samples", type=int, default=1 << 24)
     ap.add_argument("--surrogate-epochs", type=int, default=20)
+    ap.add_argument("--no-stress", action="store_true", help="skip the refill-stress frame (Kerr a=0.998)")
+    ap.add_argument("--stress-spp", type=int, default=64)
     return ap.parse_args()
 
 
@@ -290,6 +292,41 @@ def run_surrogate(args, ctx, s, d_stars, d_w, film_mixed_ms, steps):
     }
 
 
+def run_stress(args, ctx, d_stars, d_w, peak):
+    """BASELINE's refill-stress configuration: Kerr a = 0.998, observer at
+    r = 20 M and 85 degrees, 3840x2160 at 64 spp (530,841,600 geodesics),
+    up to 5e4 steps per ray, FP32 integration with the FP64 band near the
+    horizon.  One warm-up and one timed frame; reports geodesics/s, the
+    fraction of attempts taken in FP64 and the FP32 roofline."""
+    import torch
+    import magik_b200 as M
+    from magik_b200 import flops as FL
+    s = M.scene_defaults(width=3840, height=2160, spp=args.stress_spp, spin=0.998, cam_r=20.0,
+                         cam_incl_rad=85.0 * 3.141592653589793 / 180.0, max_steps=50_000)
+    s.disk_r_in = M.isco_radius(0.998)
+    film = torch.empty(s.width * s.height * 3, dtype=torch.float32, device=f"cuda:{ctx.device}")
+    ctx.render(s, d_stars, film, d_weights=d_w, want_stats=False)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    st = ctx.render(s, d_stars, film, d_weights=d_w, want_stats=True)
+    e1.record()
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    rays = s.width * s.height * s.spp
+    flop = FL.render_flops(s.metric, st.attempts, st.refine_evals)
+    return {"workload": f"kerr_a0.998_r20M_i85_fov60_3840x2160_{s.spp}spp_32bins_1e5stars_rtol1e-7",
+            "value": rays / (ms * 1e-3), "unit": UNIT, "ms_per_frame": ms, "rays": rays,
+            "attempts_per_ray": st.attempts / rays, "max_steps": s.max_steps,
+            "fp64_attempt_fraction": st.wide_attempts / max(1, st.attempts),
+            "rays_resumed_in_tail": st.resumed, "step_limit_rays": int(st.class_count[4]),
+            "classes": dict(zip(["alive", "disk", "escaped", "horizon", "step_limit"],
+                                [int(c) for c in st.class_count])),
+            "roofline": {"bound": "fp32", "achieved": flop / (st.integrate_ms * 1e-3) / 1e12,
+                         "peak": peak / 1e12, "unit": "TFLOP/s",
+                         "frac": flop / (st.integrate_ms * 1e-3) / peak}}
+
+
 def run_gpu(args, rank, world, local_rank):
     import torch
     import magik_b200 as M
@@ -401,6 +438,8 @@ def run_gpu(args, rank, world, local_rank):
         "gpu_launches": 10 * args.steps,
         "film_finite": film_ok,
     }
+    if world == 1 and not args.no_stress:
+        out["refill_stress"] = run_stress(args, ctx, d_stars, d_w, peak)
     if world == 1 and not args.no_surrogate:
         # runs after the timed region; its own timings are inside "surrogate"
         out["surrogate"] = run_surrogate(args, ctx, s, d_stars, d_w, ms, max(1, min(args.steps, 3)))
