@@ -375,6 +375,12 @@ __device__ __forceinline__ T rms_error(const S7<T>& e, const S7<T>& y0, const S7
 // operations only, so the CPU oracle reproduces it bit for bit: split
 // a = m 2^e with m in [1, 2), e = 5q + r; start from a quadratic fit of
 // m^(-1/5) times 2^(-r/5) 2^(-q), then Newton steps y <- y (6 - a y^5) / 5.
+// 2^(-r/5), r = 0..4, for inv_root5 (constant memory: one indexed load).
+__constant__ float kRoot5Scale[5] = {1.0f, 0.8705505632961241f, 0.757858283255199f, 0.6597539553864471f,
+                                     0.5743491774985174f};
+__constant__ double kRoot5ScaleD[5] = {1.0, 0.8705505632961241, 0.757858283255199, 0.6597539553864471,
+                                       0.5743491774985174};
+
 __device__ __forceinline__ float inv_root5(float a) {
     if (!(a <= 3.4028235e38f)) return 0.0f;  // err = inf: no step
     const uint32_t b = __float_as_uint(a);
@@ -382,9 +388,8 @@ __device__ __forceinline__ float inv_root5(float a) {
     const float m = __uint_as_float((b & 0x7fffffu) | 0x3f800000u);
     const int q = ex >= 0 ? ex / 5 : -((4 - ex) / 5);
     const int r = ex - 5 * q;
-    const float D[5] = {1.0f, 0.8705505632961241f, 0.757858283255199f, 0.6597539553864471f, 0.5743491774985174f};
     float y = __fmaf_rn(__fmaf_rn(0.05264997f, m, -0.28570902f), m, 1.23209767f);
-    y = y * D[r];
+    y = y * kRoot5Scale[r];
     y = y * __uint_as_float(uint32_t(127 - q) << 23);
 #pragma unroll
     for (int it = 0; it < 2; ++it) {
@@ -400,9 +405,8 @@ __device__ __forceinline__ double inv_root5(double a) {
     const double m = __longlong_as_double((long long)((b & 0xfffffffffffffull) | 0x3ff0000000000000ull));
     const int q = ex >= 0 ? ex / 5 : -((4 - ex) / 5);
     const int r = ex - 5 * q;
-    const double D[5] = {1.0, 0.8705505632961241, 0.757858283255199, 0.6597539553864471, 0.5743491774985174};
     double y = __fma_rn(__fma_rn(0.05264997, m, -0.28570902), m, 1.23209767);
-    y = y * D[r];
+    y = y * kRoot5ScaleD[r];
     y = y * __longlong_as_double((long long)(uint64_t(1023 - q) << 52));
 #pragma unroll
     for (int it = 0; it < 3; ++it) {

@@ -228,7 +228,7 @@ __global__ void __launch_bounds__(kIntegrateThreads, MODE == MGK_PRECISION_F64 ?
     uint32_t ray = 0, steps = 0, tries = 0, att = 0;
     uint32_t cbeg = 0, cend = 0;
     bool drained = false;
-    unsigned long long n_att = 0, n_steps = 0;
+    uint32_t n_att = 0, n_steps = 0;  // per lane: below 2^32 (a lane runs at most max_steps x n_max per ray)
     uint32_t n_cls[5] = {0, 0, 0, 0, 0};
 
     for (;;) {
@@ -313,25 +313,6 @@ __global__ void __launch_bounds__(kIntegrateThreads, MODE == MGK_PRECISION_F64 ?
         // ---- compaction of the hand-offs: disk candidates fill the crossing
         // queue from the front, escapes from the back, so that the crossing
         // kernel's warps see one kind (escapes take one sub-step, disks iterate)
-        uint32_t slot = warp_push(cross && disk, &cnt->refine_count, nq, &cnt->status);
-        uint32_t eslot = warp_push(cross && !disk, &cnt->escape_count, nq, &cnt->status);
-        if (eslot != ~0u) slot = nq - 1u - eslot;
-        if (slot != ~0u) {
-            RefineEntry<T> e;
-            e.y0[0] = y0.x; e.y0[1] = y0.y; e.y0[2] = y0.z; e.y0[3] = y0.t;
-            e.y0[4] = y0.px; e.y0[5] = y0.py; e.y0[6] = y0.pz;
-            e.y1[0] = y.x; e.y1[1] = y.y; e.y1[2] = y.z; e.y1[3] = y.t;
-            e.y1[4] = y.px; e.y1[5] = y.py; e.y1[6] = y.pz;
-            e.pt = pt; e.h = h_used; e.h_next = h; e.c0 = c0;
-            e.ray = ray; e.steps = steps; e.attempts = att;
-            e.wide = MODE == MGK_PRECISION_F64 ? att : 0u;
-            e.evals = 0; e.pad[0] = e.pad[1] = e.pad[2] = 0;
-            refq[slot] = e;
-        }
-        if constexpr (MODE == MGK_PRECISION_MIXED) {
-            uint32_t bslot = warp_push(to_band, &cnt->resume_count, nq, &cnt->status);
-            if (bslot != ~0u) store_resume<T>(resq, bslot, y, pt, h, c0, ray, steps, att, 0u, 0u);
-        }
         if (cls != MGK_RAY_ALIVE) {
             if (res) {
                 Term<T> t{cls, T(0), T(0), T(0), T(0), T(0)};
@@ -339,19 +320,41 @@ __global__ void __launch_bounds__(kIntegrateThreads, MODE == MGK_PRECISION_F64 ?
             }
             ++n_cls[cls];
         }
+        // one ballot skips the three pushes on the (common) trips with no hand-off
+        if (__ballot_sync(kFull, cross || to_band) != 0u) {
+            uint32_t slot = warp_push(cross && disk, &cnt->refine_count, nq, &cnt->status);
+            uint32_t eslot = warp_push(cross && !disk, &cnt->escape_count, nq, &cnt->status);
+            if (eslot != ~0u) slot = nq - 1u - eslot;
+            if (slot != ~0u) {
+                RefineEntry<T> e;
+                e.y0[0] = y0.x; e.y0[1] = y0.y; e.y0[2] = y0.z; e.y0[3] = y0.t;
+                e.y0[4] = y0.px; e.y0[5] = y0.py; e.y0[6] = y0.pz;
+                e.y1[0] = y.x; e.y1[1] = y.y; e.y1[2] = y.z; e.y1[3] = y.t;
+                e.y1[4] = y.px; e.y1[5] = y.py; e.y1[6] = y.pz;
+                e.pt = pt; e.h = h_used; e.h_next = h; e.c0 = c0;
+                e.ray = ray; e.steps = steps; e.attempts = att;
+                e.wide = MODE == MGK_PRECISION_F64 ? att : 0u;
+                e.evals = 0; e.pad[0] = e.pad[1] = e.pad[2] = 0;
+                refq[slot] = e;
+            }
+            if constexpr (MODE == MGK_PRECISION_MIXED) {
+                uint32_t bslot = warp_push(to_band, &cnt->resume_count, nq, &cnt->status);
+                if (bslot != ~0u) store_resume<T>(resq, bslot, y, pt, h, c0, ray, steps, att, 0u, 0u);
+            }
+        }
         if (cls != MGK_RAY_ALIVE || cross || to_band) alive = false;
     }
 
     // ---- counters: one atomic per warp and counter
-    n_att = warp_sum(n_att);
-    n_steps = warp_sum(n_steps);
+    const unsigned long long w_att = warp_sum((unsigned long long)n_att);
+    const unsigned long long w_steps = warp_sum((unsigned long long)n_steps);
     unsigned long long c[5];
 #pragma unroll
     for (int i = 0; i < 5; ++i) c[i] = warp_sum((unsigned long long)n_cls[i]);
     if (lane == 0) {
-        atomicAdd(&cnt->attempts, n_att);
-        atomicAdd(&cnt->steps, n_steps);
-        if (MODE == MGK_PRECISION_F64) atomicAdd(&cnt->wide_attempts, n_att);
+        atomicAdd(&cnt->attempts, w_att);
+        atomicAdd(&cnt->steps, w_steps);
+        if (MODE == MGK_PRECISION_F64) atomicAdd(&cnt->wide_attempts, w_att);
 #pragma unroll
         for (int i = 1; i < 5; ++i)
             if (c[i]) atomicAdd(&cnt->class_count[i], c[i]);
