@@ -10,9 +10,10 @@ FP64 step control (MIXED), escape radius 1000 M.  Synthetic, seeded input.
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
-Under torchrun every rank renders its own frame (its own jitter seed): the
-work per GPU is fixed and the frames need no exchange, so scaling is weak and
-the value is the total of all ranks.  Rank 0 prints one JSON line.
+Under torchrun every rank renders a sample slice of the frame (all pixels,
+its own jitter seed) and the films are sum-reduced into rank 0 inside the
+timed region: the work per GPU is fixed, so scaling is weak and the value is
+the total of all ranks.  Rank 0 prints one JSON line.
 """
 import argparse
 import json
@@ -332,6 +333,7 @@ def run_gpu(args, rank, world, local_rank):
     import magik_b200 as M
     from magik_b200 import flops as FL
 
+    from magik_b200.dist import reduce_film
     torch.cuda.set_device(local_rank)
     dev = f"cuda:{local_rank}"
     ctx = M.Context(local_rank)
@@ -367,6 +369,8 @@ def run_gpu(args, rank, world, local_rank):
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record()
         st = ctx.render(s, d_stars, film, d_weights=d_w, want_stats=True)
+        if world > 1:
+            reduce_film(film)  # the sample slices of all ranks into rank 0's image
         e1.record()
         e1.synchronize()
         times.append(e0.elapsed_time(e1))
@@ -414,7 +418,7 @@ def run_gpu(args, rank, world, local_rank):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "fp32 (fp64 step control)",
         "data": "synthetic (seeded camera jitter and star catalogue)",
-        "config": config_dict(s, {"parallelism": f"{world} independent frames (weak)"}),
+        "config": config_dict(s, {"parallelism": f"{world} sample slices of one frame, film sum-reduced into rank 0 (weak)"}),
         "e2e": {"value": world * rays / (e2e_ms * 1e-3), "unit": UNIT,
                 "h2d_bytes_per_step": int(h_stars.numel() + h_w.numel() * 4),
                 "d2h_bytes_per_step": int(h_film.numel() * 4)},

@@ -1,8 +1,9 @@
-"""Multi-GPU plumbing of the render: one process per GPU, no data-path
-collective.  Rays are independent and frames need no exchange, so each rank
-renders whole frames of its own (its own jitter seed, i.e. a different set of
-samples of the same image); the only collective is the max over ranks of the
-measured times, over torch.distributed (NCCL on GPUs, gloo on CPU)."""
+"""Multi-GPU plumbing of the render: one process per GPU over
+torch.distributed (NCCL on GPUs, gloo on CPU).  Rays are independent, so the
+frame is split into sample slices: every rank renders all pixels with its own
+jitter seed (a different set of samples of the same image) and the one
+exchange step is a sum-reduce of the XYZ films into rank 0, which divides by
+the number of ranks.  Timings are combined with a max over ranks."""
 
 
 def frame_seed(base_seed, rank):
@@ -29,3 +30,20 @@ def sum_over_ranks(values, device="cpu"):
     if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
         dist.all_reduce(t, op=dist.ReduceOp.SUM)
     return t.tolist()
+
+
+def reduce_film(film, dst=0):
+    """Mean of the ranks' films into rank `dst`, in place: a sum-reduce
+    (NCCL reduce over NVLink on GPUs) then a division by the world size.
+    Each rank rendered a sample slice of the same image with its own seed,
+    so the result is the image at world x spp samples per pixel.  The other
+    ranks' films are scratch afterwards (gloo reduces through them).
+    Identity when torch.distributed is not initialised or has one rank."""
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return film
+    world = dist.get_world_size()
+    dist.reduce(film, dst=dst, op=dist.ReduceOp.SUM)
+    if dist.get_rank() == dst:
+        film.mul_(1.0 / world)
+    return film

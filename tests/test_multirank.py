@@ -1,5 +1,6 @@
 """The N > 1 path of bench.py on CPU: two gloo ranks, each with its own frame
-seed, combine their timings with a max and their ray counts with a sum."""
+seed, combine their timings with a max, their ray counts with a sum, and
+their films (sample slices of one image) with a sum-reduce into rank 0."""
 import os
 import socket
 
@@ -25,7 +26,11 @@ def _worker(rank, world, port, q):
         ms = [10.0 + rank, 5.0 * (2 - rank)]  # per-rank step times
         mx = D.max_over_ranks(ms)
         rays = D.sum_over_ranks([1000 * (rank + 1)])
-        q.put((rank, D.frame_seed(0x5EED, rank), mx, rays))
+        import torch
+        film = torch.full((6,), float(rank + 1), dtype=torch.float32)
+        film[0] = 10.0 * (rank + 1)
+        D.reduce_film(film)
+        q.put((rank, D.frame_seed(0x5EED, rank), mx, rays, film.tolist()))
     finally:
         dist.destroy_process_group()
 
@@ -44,9 +49,11 @@ def test_two_rank_weak_scaling_aggregation():
     out.sort()
     seeds = {o[1] for o in out}
     assert len(seeds) == 2
-    for _, _, mx, rays in out:
+    for rank, _, mx, rays, film in out:
         assert mx == [11.0, 10.0]
         assert rays == [3000.0]
+        if rank == 0:  # mean of the two sample slices
+            assert film == [15.0, 1.5, 1.5, 1.5, 1.5, 1.5]
 
 
 def test_frame_seed_rank0_is_base():
