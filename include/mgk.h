@@ -203,6 +203,17 @@ MGK_API mgk_result mgk_scene_constants(const mgk_scene* s, double* out32);
  * denominator of the integrator's roofline.  Synchronous. */
 MGK_API mgk_result mgk_fp32_peak(mgk_context* ctx, double* flops_per_s);
 
+/* Self-check of the MIXED mode's square root and reciprocal (no counterpart
+ * in the reference).  The fused RHS takes them from the hardware
+ * approximations with one FMA correction each; they are defined as
+ *   msqrt(a) = IEEE sqrt(max(a, 2^-100)), NaN for a = +inf,
+ *   mrcp(b)  = IEEE 1/b for normal b with a normal reciprocal, +-0 for
+ *              |b| > 2^126, NaN for b = +-0, subnormal or infinite,
+ * which the CPU oracle restates.  Evaluates both on the device for all 2^32
+ * float inputs and writes the number of inputs where each differs from its
+ * definition (0 on a conforming device).  Synchronous; about a millisecond. */
+MGK_API mgk_result mgk_check_rounding(mgk_context* ctx, uint64_t mismatches[2]);
+
 /* ------------------------------------------------------------- render */
 /* Renders the scene's full frame: width*height*spp camera rays through the
  * persistent integrator, shading of the hit queues, per-pixel resolve.

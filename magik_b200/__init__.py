@@ -32,6 +32,7 @@ EXPORTS = [
     "mgk_context_create", "mgk_context_destroy", "mgk_last_error", "mgk_scene_defaults", "mgk_isco_radius",
     "mgk_xyz_weights", "mgk_star_catalog", "mgk_scene_constants", "mgk_render", "mgk_render_host",
     "mgk_trace_rays", "mgk_shade_rays", "magik_trace_geodesic", "mgk_trace_geodesic_batch", "mgk_fp32_peak",
+    "mgk_check_rounding",
     "mgk_trace_rays_static", "mgk_train_defaults", "mgk_surrogate_param_count", "mgk_surrogate_create",
     "mgk_surrogate_destroy", "mgk_surrogate_get_params", "mgk_surrogate_set_params", "mgk_make_samples",
     "mgk_surrogate_forward", "mgk_surrogate_forward_tiled", "mgk_surrogate_status", "mgk_surrogate_gradient", "mgk_surrogate_train", "mgk_render_surrogate",
@@ -74,6 +75,7 @@ def lib():
         L.mgk_trace_geodesic_batch.argtypes = [vp, P(abi.TraceContainer), P(abi.TraceInitialConditions),
                                                P(abi.TraceMetricParams), P(abi.TraceIntegratorParams), C.c_uint32]
         L.mgk_fp32_peak.argtypes = [vp, P(C.c_double)]
+        L.mgk_check_rounding.argtypes = [vp, P(C.c_uint64)]
         L.mgk_trace_rays_static.argtypes = [P(Scene), C.c_uint64, C.c_uint32, vp, vp]
         L.mgk_train_defaults.argtypes = [P(abi.TrainConfig)]
         L.mgk_train_defaults.restype = None
@@ -178,6 +180,12 @@ class Context:
         v = C.c_double(0)
         _check(lib().mgk_fp32_peak(self.handle, C.byref(v)), "mgk_fp32_peak", self.handle)
         return v.value
+
+    def check_rounding(self):
+        """mgk_check_rounding: (msqrt, mrcp) mismatch counts over all 2^32 floats."""
+        out = (C.c_uint64 * 2)()
+        _check(lib().mgk_check_rounding(self.handle, out), "mgk_check_rounding", self.handle)
+        return int(out[0]), int(out[1])
 
     # -- device-buffer entry points (torch CUDA tensors)
     def render(self, scene, d_stars, d_film_xyz, d_weights=None, d_film_spectral=None, want_stats=True,

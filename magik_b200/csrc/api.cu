@@ -564,6 +564,21 @@ MGK_API mgk_result mgk_fp32_peak(mgk_context* ctx, double* flops_per_s) {
     return MGK_SUCCESS;
 }
 
+MGK_API mgk_result mgk_check_rounding(mgk_context* ctx, uint64_t mismatches[2]) {
+    if (!ctx || !mismatches) return MGK_ERROR_INVALID_POINTER;
+    MGK_CUDA(ctx, cudaSetDevice(ctx->device));
+    mgk_result rc = ensure_arena(ctx, 4096);
+    if (rc != MGK_SUCCESS) return rc;
+    auto* out = static_cast<unsigned long long*>(ctx->arena);
+    MGK_CUDA(ctx, cudaMemsetAsync(out, 0, 2 * sizeof(unsigned long long), nullptr));
+    MGK_CUDA(ctx, launch_check_rounding(ctx->sm_count, out, nullptr));
+    unsigned long long h[2] = {0, 0};
+    MGK_CUDA(ctx, cudaMemcpy(h, out, sizeof h, cudaMemcpyDeviceToHost));
+    mismatches[0] = h[0];
+    mismatches[1] = h[1];
+    return MGK_SUCCESS;
+}
+
 MGK_API mgk_result mgk_render(mgk_context* ctx, const mgk_scene* s, const mgk_star* d_stars, uint32_t n_stars,
                               const float* d_xyz_w, float* d_film_xyz, float* d_film_spectral,
                               mgk_render_stats* stats, void* stream) {

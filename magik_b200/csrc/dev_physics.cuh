@@ -8,7 +8,8 @@
 //   what the reference computes on the CPU.
 //   Fuse::Fma uses the same trees with the marked multiply-adds fused, and
 //   the rearranged RHS below (rhs_kerr_fused, rhs_schwarzschild_fused).
-// Division and sqrt are IEEE-rounded (-prec-div/-prec-sqrt, no fast math).
+// Division and sqrt are IEEE-rounded (-prec-div/-prec-sqrt, no fast math),
+// except in the float fused RHS (msqrt / mrcp below).
 #pragma once
 
 #include <cstdint>
@@ -26,6 +27,54 @@ template <Fuse F> __device__ __forceinline__ double mad(double a, double b, doub
     if constexpr (F == Fuse::Fma) return __fma_rn(a, b, c);
     else return __dadd_rn(__dmul_rn(a, b), c);
 }
+
+// ------------------------------------------------- MIXED sqrt / reciprocal
+// The fused RHS of the MIXED mode takes its square roots and its reciprocal
+// from the hardware approximations (rsqrt.approx / rcp.approx, flush to zero)
+// and one FMA correction each, after P. Markstein, "Computation of elementary
+// functions on the IBM RISC System/6000 processor", IBM J. Res. Dev. 34(1),
+// 1990:
+//   sqrt(a): y ~ 1/sqrt(a), g = a y, h = y/2, d = a - g^2 (one rounding), g + d h
+//   1/b:     y ~ 1/b, e = 1 - b y (one rounding), y + e y
+// Neither needs the range checks and slow-path branches of the IEEE
+// sequences, and their results are these functions exactly (mgk_check_rounding
+// compares every float input on the device):
+//   msqrt(a) = IEEE sqrt(max(a, 2^-100)), except NaN for a = +inf;
+//   mrcp(b)  = IEEE 1/b for normal b with a normal reciprocal, +-0 for
+//              |b| > 2^126, NaN for b = +-0, subnormal or infinite.
+// The clamp keeps d = a - g^2 out of the subnormal range, where a single
+// correction is not enough.  In the RHS the clamp and the special values are
+// reached by degenerate states only (at the ring singularity); the oracle
+// defines both functions the same way.
+constexpr float kSqrtFloor = 7.888609052210118e-31f;  // 2^-100
+
+__device__ __forceinline__ float rsqrt_approx(float a) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(a));
+    return y;
+}
+__device__ __forceinline__ float rcp_approx(float b) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(b));
+    return y;
+}
+__device__ __forceinline__ float msqrt(float a) {
+    a = fmaxf(a, kSqrtFloor);
+    const float y = rsqrt_approx(a);
+    const float g = a * y, h = 0.5f * y;
+    const float d = __fmaf_rn(-g, g, a);
+    return __fmaf_rn(d, h, g);
+}
+__device__ __forceinline__ float mrcp(float b) {
+    const float y = rcp_approx(b);
+    const float e = __fmaf_rn(-b, y, 1.0f);
+    return __fmaf_rn(e, y, y);
+}
+// The fused RHS in T: msqrt / mrcp in float, IEEE sqrt and division in double.
+__device__ __forceinline__ float fused_sqrt(float a) { return msqrt(a); }
+__device__ __forceinline__ double fused_sqrt(double a) { return sqrt(a); }
+__device__ __forceinline__ float fused_rcp(float b) { return mrcp(b); }
+__device__ __forceinline__ double fused_rcp(double b) { return 1.0 / b; }
 
 // Geodesic state without the conserved p_t: position (x, y, z, t) and
 // covariant spatial momentum (px, py, pz).  p_t is carried beside it.
@@ -174,24 +223,29 @@ __device__ __forceinline__ void rhs_schwarzschild(const S7<T>& s, T pt, T mass_s
 // rearranged to need fewer operations:
 //  * one reciprocal 1/(r sigma d f_den) gives 1/d, 1/(r sigma), 1/r, 1/f_den;
 //  * dr/dx_i = (x r/sigma, y d/(r sigma), z r/sigma), using r^2 = (w + sigma)/2;
-//  * sum_j p_j dk_j/dx_i is formed without the nine derivatives: with
-//    g_x = x d - 2 r (r x - a z), g_z = z d - 2 r (r z + a x) and
-//    G = px g_x + pz g_z,  px dkx/dx_i + pz dkz/dx_i = (dr_i G + U_i)/d^2,
-//    U = d (px r + pz a, 0, pz r - px a), and py dky/dx_i = py (r delta_iy - y dr_i)/r^2.
+//  * sum_j p_j dk_j/dx_i is formed without the nine derivatives:
+//      px dkx/dx_i + pz dkz/dx_i = (dr_i G' + U'_i)/d,  py dky/dx_i = c (r delta_iy - y dr_i),
+//    with S = px kx + pz kz (a partial sum of k.p), G' = (px x + pz z) - 2 r S,
+//    U' = (px r + pz a, 0, pz r - px a) and c = py/r^2;
+//  * (k.p)^2 df/dx_i / 2 = (k.p)^2 (dq dr_i - delta_iy 2 a^2 r^3 y / f_den^2),
+//    dq = (3 a^2 r^2 y^2 - r^6) / f_den^2;
+// so that with F = f (k.p), Ad = F/d, B = (k.p)^2 dq - F c y, Q = Ad G' + B and
+// E = F c r - (k.p)^2 2 a^2 r^3 y / f_den^2:
+//      dp_i/dl = Q dr_i + Ad U'_i + delta_iy E.
 template <class T> __device__ __forceinline__ void rhs_kerr_fused(const S7<T>& s, T pt, const MP<T>& m, S7<T>& o) {
     constexpr Fuse F = Fuse::Fma;
     const T x = s.x, y = s.y, z = s.z, px = s.px, py = s.py, pz = s.pz;
     const T a = m.spin, a_sq = m.a_sq;
     const T y_sq = y * y;
     const T w_sq = mad<F>(z, z, mad<F>(x, x, y_sq)) - a_sq;
-    const T sigma = sqrt(mad<F>(w_sq, w_sq, m.four_a_sq * y_sq));
-    const T r = sqrt(T(0.5) * (w_sq + sigma));
+    const T sigma = fused_sqrt(mad<F>(w_sq, w_sq, m.four_a_sq * y_sq));
+    const T r = fused_sqrt(T(0.5) * (w_sq + sigma));
     const T r_sq = r * r;
     const T d = r_sq + a_sq;
     const T f_den = mad<F>(a_sq, y_sq, r_sq * r_sq);
     const T rs = r * sigma;
     const T rsd = rs * d;
-    const T inv_all = T(1) / (rsd * f_den);  // ~r^9: finite for r below ~1.9e4 in float
+    const T inv_all = fused_rcp(rsd * f_den);  // ~r^9: finite for r below ~1.9e4 in float
     const T inv_rsd = f_den * inv_all;
     const T inv_fden = rsd * inv_all;
     const T inv_d = rs * inv_rsd;
@@ -204,31 +258,29 @@ template <class T> __device__ __forceinline__ void rhs_kerr_fused(const S7<T>& s
     const T kx_num = mad<F>(r, x, -(a * z));
     const T kz_num = mad<F>(r, z, a * x);
     const T kx = kx_num * inv_d, kz = kz_num * inv_d, ky = y * inv_r;
-    const T kTp = mad<F>(pz, kz, mad<F>(py, ky, px * kx)) - pt;
+    const T S = mad<F>(pz, kz, px * kx);
+    const T kTp = mad<F>(py, ky, S) - pt;
     const T f_kTp = f_ * kTp;
     const T kTp2 = kTp * kTp;
     const T two_r = r + r;
-    const T gx = mad<F>(x, d, -(two_r * kx_num));
-    const T gz = mad<F>(z, d, -(two_r * kz_num));
-    const T G = mad<F>(px, gx, pz * gz);
-    const T Ux = d * mad<F>(px, r, pz * a);
-    const T Uz = d * mad<F>(pz, r, -(px * a));
+    const T Gp = mad<F>(-two_r, S, mad<F>(pz, z, px * x));
+    const T Ad = f_kTp * inv_d;
+    const T Ux = mad<F>(px, r, pz * a);
+    const T Uz = mad<F>(pz, r, -(px * a));
     const T c = py * (inv_r * inv_r);
     const T cy = c * y;
     const T inv_fden_sq = inv_fden * inv_fden;
-    // (k.p)^2/2 df/dx_i = (k.p)^2 (dq dr_i - delta_iy 2 a^2 r^3 y / f_den^2),
-    // dq = (3 a^2 r^2 y^2 - r^6) / f_den^2
     const T dq = mad<F>(m.three_a_sq * r_sq, y_sq, -(r_cu * r_cu)) * inv_fden_sq;
-    const T A = f_kTp * (inv_d * inv_d);
     const T B = mad<F>(kTp2, dq, -(f_kTp * cy));
     const T E = mad<F>(-kTp2, ((m.two_a_sq * r_cu) * y) * inv_fden_sq, f_kTp * (c * r));
+    const T Q = mad<F>(Ad, Gp, B);
     o.x = mad<F>(-f_kTp, kx, px);
     o.y = mad<F>(-f_kTp, ky, py);
     o.z = mad<F>(-f_kTp, kz, pz);
     o.t = f_kTp - pt;
-    o.px = mad<F>(A, mad<F>(drx, G, Ux), B * drx);
-    o.py = mad<F>(A, dry * G, mad<F>(B, dry, E));
-    o.pz = mad<F>(A, mad<F>(drz, G, Uz), B * drz);
+    o.px = mad<F>(Q, drx, Ad * Ux);
+    o.py = mad<F>(Q, dry, E);
+    o.pz = mad<F>(Q, drz, Ad * Uz);
 }
 
 // Schwarzschild, fused formulation: with a = 0, k = x/r, f = 2 m/r,
@@ -238,8 +290,8 @@ template <class T>
 __device__ __forceinline__ void rhs_schwarzschild_fused(const S7<T>& s, T pt, T mass_sign, S7<T>& o) {
     constexpr Fuse F = Fuse::Fma;
     const T x = s.x, y = s.y, z = s.z, px = s.px, py = s.py, pz = s.pz;
-    const T r = sqrt(mad<F>(z, z, mad<F>(y, y, x * x)));
-    const T inv_r = T(1) / r;
+    const T r = fused_sqrt(mad<F>(z, z, mad<F>(y, y, x * x)));
+    const T inv_r = fused_rcp(r);
     const T kx = x * inv_r, ky = y * inv_r, kz = z * inv_r;
     const T kp = mad<F>(pz, kz, mad<F>(py, ky, px * kx));
     const T kTp = kp - pt;
@@ -391,12 +443,9 @@ __device__ __forceinline__ float inv_root5(float a) {
     float y = __fmaf_rn(__fmaf_rn(0.05264997f, m, -0.28570902f), m, 1.23209767f);
     y = y * kRoot5Scale[r];
     y = y * __uint_as_float(uint32_t(127 - q) << 23);
-#pragma unroll
-    for (int it = 0; it < 2; ++it) {
-        float y2 = y * y, y4 = y2 * y2, t = a * (y4 * y);
-        y = y * __fmaf_rn(-0.2f, t, 1.2f);
-    }
-    return y;
+    // the fit is within 1e-3; one Newton step leaves 3e-6, ample for a step proposal
+    const float y2 = y * y, y4 = y2 * y2, t = a * (y4 * y);
+    return y * __fmaf_rn(-0.2f, t, 1.2f);
 }
 __device__ __forceinline__ double inv_root5(double a) {
     if (!(a <= 1.7976931348623157e308)) return 0.0;
@@ -418,19 +467,19 @@ __device__ __forceinline__ double inv_root5(double a) {
 
 // Reciprocal of a positive normal float from integer and FMA operations only
 // (bit-identical on the CPU): the seed 0x7EF311C3 - bits(x) is within 12 %,
-// two Newton steps y <- y (2 - x y) bring it within 2e-4.  The MIXED error
-// norm needs no more than that.
+// one Newton step y <- y (2 - x y) brings it within 1.44 %, from below.  A
+// norm term e_i / scale_i is then at most 1.44 % small: the MIXED error
+// control accepts steps whose error is up to 1.5 % above the tolerance.
 __device__ __forceinline__ float rcp_norm(float x) {
-    float y = __uint_as_float(0x7EF311C3u - __float_as_uint(x));
-    y = y * __fmaf_rn(-x, y, 2.0f);
-    y = y * __fmaf_rn(-x, y, 2.0f);
-    return y;
+    const float y = __uint_as_float(0x7EF311C3u - __float_as_uint(x));
+    return y * __fmaf_rn(-x, y, 2.0f);
 }
 
-// MIXED RMS norm: as rms_error<Fuse::Fma, float> with the divisions replaced
-// by rcp_norm.
+// MIXED RMS norm of the unscaled error E (the step's error is h E): as
+// rms_error<Fuse::Fma, float> of h E, with the divisions replaced by rcp_norm
+// and h applied once, to the sum of squares.
 __device__ __forceinline__ float rms_error_mixed(const S7<float>& e, const S7<float>& y0, const S7<float>& y1,
-                                                 float atol, float rtol) {
+                                                 float h, float atol, float rtol) {
     auto term = [&](float ei, float a0, float a1) {
         return ei * rcp_norm(__fmaf_rn(rtol, fmaxf(fabsf(a0), fabsf(a1)), atol));
     };
@@ -444,19 +493,27 @@ __device__ __forceinline__ float rms_error_mixed(const S7<float>& e, const S7<fl
     acc = __fmaf_rn(s5, s5, acc);
     acc = __fmaf_rn(s6, s6, acc);
     acc = __fmaf_rn(s7, s7, acc);
-    return sqrtf(acc / 8.0f);
+    return sqrtf(acc * ((h * h) * 0.125f));
 }
 
-// MIXED control: the error estimate (difference of the 5th- and 4th-order
-// solutions, which cancels badly in FP32) is formed in FP64 from the FP32
-// stages; its norm and the proposal need only a few digits and run in FP32.
+// The unscaled error estimate E = sum_j (b5_j - b4_j) k_j of the Fehlberg
+// pair in FP64 from the FP32 stages (the step's error is h E).
+template <class T> __device__ __forceinline__ S7<T> rkf45_error_unscaled(const S7<T> k[6]) {
+    using C = FB<T>;
+    return axpy<Fuse::Fma>(-C::e6, k[5], axpy<Fuse::Fma>(-C::e5, k[4], axpy<Fuse::Fma>(C::e4, k[3],
+                           axpy<Fuse::Fma>(C::e3, k[2], scl(C::e1, k[0])))));
+}
+
+// MIXED control: the error estimate (whose terms cancel badly in FP32) is
+// formed in FP64 from the FP32 stages; its norm and the proposal need only a
+// few digits and run in FP32.
 __device__ __forceinline__ void control_mixed(const S7<float>& y0, const S7<float>& y1, const S7<float> k[6],
                                               float h, const MP<float>& m, float& h_next, bool& ok) {
     S7<double> kd[6];
 #pragma unroll
     for (int i = 0; i < 6; ++i) kd[i] = cvt<double>(k[i]);
-    S7<float> e = cvt<float>(rkf45_error<Fuse::Fma, double>(double(h), kd));
-    float err = rms_error_mixed(e, y0, y1, m.abs_tol, m.rel_tol);
+    S7<float> e = cvt<float>(rkf45_error_unscaled<double>(kd));
+    float err = rms_error_mixed(e, y0, y1, h, m.abs_tol, m.rel_tol);
     float safe = err > 1e-30f ? err : 1e-30f;
     float hn = (0.9f * h) * inv_root5(safe);
     if (hn > m.h_max) hn = m.h_max;

@@ -95,6 +95,7 @@ cudaError_t surrogate_infer(mgk_surrogate* net, const float* feat, uint32_t n, f
 uint32_t surrogate_status(mgk_surrogate* net);
 int context_device(mgk_context* ctx);
 cudaError_t launch_fma_probe(uint32_t blocks, uint32_t iters, float* sink, cudaStream_t stream);
+cudaError_t launch_check_rounding(int sm_count, unsigned long long* out, cudaStream_t stream);
 cudaError_t launch_trace_geodesic(const void* jobs, uint32_t n, void* steps, uint32_t* written, cudaStream_t stream);
 
 // Size of DevScene<T> for the scene's precision.

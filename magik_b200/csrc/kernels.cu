@@ -24,6 +24,9 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
+#include "dev_pair.cuh"
 #include "dev_physics.cuh"
 #include "dev_scene.cuh"
 #include "internal.h"
@@ -40,6 +43,14 @@ constexpr unsigned kFull = 0xffffffffu;
 constexpr int kIntegrateThreads = MGK_INTEGRATE_THREADS;
 // FP64 state needs about twice the registers: fewer resident blocks
 constexpr int kIntegrateMinBlocksF64 = 4;
+// two rays per thread (k_integrate_x2): about twice the registers as well
+#ifndef MGK_X2_MIN_BLOCKS
+#define MGK_X2_MIN_BLOCKS 3
+#endif
+// MIXED Kerr / Schwarzschild frames run k_integrate_x2 (1) or k_integrate (0)
+#ifndef MGK_MIXED_X2
+#define MGK_MIXED_X2 0
+#endif
 constexpr uint32_t kChunk = 64;  // queue entries a warp takes per refill
 
 template <int MODE> struct ModeT { using T = float; static constexpr Fuse F = Fuse::Fma; };
@@ -355,6 +366,190 @@ __global__ void __launch_bounds__(kIntegrateThreads, MODE == MGK_PRECISION_F64 ?
         atomicAdd(&cnt->attempts, w_att);
         atomicAdd(&cnt->steps, w_steps);
         if (MODE == MGK_PRECISION_F64) atomicAdd(&cnt->wide_attempts, w_att);
+#pragma unroll
+        for (int i = 1; i < 5; ++i)
+            if (c[i]) atomicAdd(&cnt->class_count[i], c[i]);
+    }
+}
+
+// ------------------------------------------------- integrate, two rays per thread
+// MIXED Kerr and Schwarzschild: k_integrate with two rays per thread (slots
+// 0 and 1, the halves of every float2 in dev_pair.cuh), so that each FP32
+// operation of an attempt is one packed f32x2 instruction for both rays.
+// The refill, the termination tests and the hand-offs are k_integrate's,
+// per slot: a warp refills its dead slots (slot 0 of every lane before slot 1)
+// from chunks of the queue, and each hand-off queue gets one ballot per slot.
+// Both slots run an attempt on every trip; a dead slot's result is ignored.
+template <int S>
+__device__ __forceinline__ void x2_refill(const DevScene<float>& P, const void* __restrict__ qx,
+                                          const void* __restrict__ qp, const void* __restrict__ qc,
+                                          const uint32_t* __restrict__ ray_ids, uint32_t idx, S7<F2>& y, F2& pt,
+                                          F2& c0, F2& h, uint32_t& ray, bool& to_band) {
+    const float4 a = reinterpret_cast<const float4*>(qx)[idx];
+    const float4 b = reinterpret_cast<const float4*>(qp)[idx];
+    set_slot<S>(y, S7<float>{a.x, a.y, a.z, a.w, b.x, b.y, b.z});
+    set_lane<S>(pt, b.w);
+    set_lane<S>(c0, reinterpret_cast<const float*>(qc)[idx]);
+    set_lane<S>(h, P.h0);
+    ray = ray_ids ? ray_ids[idx] : idx;
+    to_band = in_band(P, a.x, a.y, a.z);
+}
+
+template <int METRIC>
+__global__ void __launch_bounds__(kIntegrateThreads, MGK_X2_MIN_BLOCKS)
+    k_integrate_x2(const DevScene<float> P, uint32_t nq, const void* __restrict__ qx, const void* __restrict__ qp,
+                   const void* __restrict__ qc, RefineEntry<float>* refq, ResumeEntry<float>* resq,
+                   mgk_ray_result* res, Counters* cnt, const uint32_t* __restrict__ ray_ids) {
+    constexpr Fuse F = Fuse::Fma;
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+
+    bool alive[2] = {false, false};
+    S7<F2> y{};
+    F2 pt = b2(0.f), c0 = b2(0.f), h = b2(0.f);
+    uint32_t ray[2] = {0, 0}, steps[2] = {0, 0}, tries[2] = {0, 0}, att[2] = {0, 0};
+    uint32_t cbeg = 0, cend = 0;
+    bool drained = false;
+    uint32_t n_att = 0, n_steps = 0;
+    uint32_t n_cls[5] = {0, 0, 0, 0, 0};
+
+    for (;;) {
+        // ---- refill dead slots (warp-uniform control flow)
+        const unsigned d0 = __ballot_sync(kFull, !alive[0]);
+        const unsigned d1 = __ballot_sync(kFull, !alive[1]);
+        bool to_band[2] = {false, false};
+        if ((d0 | d1) != 0u && !(drained && cbeg == cend)) {
+            const uint32_t n0 = __popc(d0);
+            const uint32_t need = n0 + __popc(d1);
+            const uint32_t rem = cend - cbeg;
+            uint32_t nb = 0, ne = 0;
+            if (need > rem && !drained) {
+                uint32_t got = 0;
+                if (lane == 0) got = atomicAdd(&cnt->queue_head, kChunk);
+                got = __shfl_sync(kFull, got, 0);
+                if (got >= nq) {
+                    drained = true;
+                } else {
+                    nb = got;
+                    ne = min(got + kChunk, nq);
+                    if (ne == nq) drained = true;
+                }
+            }
+            auto pick = [&](uint32_t rank) {
+                if (rank < rem) return cbeg + rank;
+                if (rank - rem < ne - nb) return nb + (rank - rem);
+                return ~0u;
+            };
+            if (!alive[0]) {
+                const uint32_t idx = pick(__popc(d0 & lt));
+                if (idx != ~0u) {
+                    x2_refill<0>(P, qx, qp, qc, ray_ids, idx, y, pt, c0, h, ray[0], to_band[0]);
+                    steps[0] = 0; tries[0] = 0; att[0] = 0;
+                    alive[0] = true;
+                }
+            }
+            if (!alive[1]) {
+                const uint32_t idx = pick(n0 + __popc(d1 & lt));
+                if (idx != ~0u) {
+                    x2_refill<1>(P, qx, qp, qc, ray_ids, idx, y, pt, c0, h, ray[1], to_band[1]);
+                    steps[1] = 0; tries[1] = 0; att[1] = 0;
+                    alive[1] = true;
+                }
+            }
+            const uint32_t used_old = min(need, rem);
+            if (ne > nb) {
+                cbeg = nb + min(need - used_old, ne - nb);
+                cend = ne;
+            } else {
+                cbeg += used_old;
+            }
+        }
+        if (__ballot_sync(kFull, alive[0] || alive[1]) == 0u) break;
+
+        // ---- one RKF45 attempt for both slots
+        const S7<F2> y0 = y;
+        const F2 h_used = h;
+        S7<F2> y1;
+        F2 hn;
+        bool ok[2];
+        attempt_x2<METRIC>(P.m, y, pt, h, y1, hn, ok);
+
+        uint32_t cls[2] = {MGK_RAY_ALIVE, MGK_RAY_ALIVE};
+        bool cross[2] = {false, false}, disk[2] = {false, false};
+        auto accept = [&](auto sc) {
+            constexpr int s = decltype(sc)::value;
+            if (!(alive[s] && !to_band[s])) return;
+            ++att[s]; ++tries[s]; ++n_att;
+            set_lane<s>(h, lane_of<s>(hn));
+            if (!(ok[s] || tries[s] >= P.m.n_max)) return;
+            tries[s] = 0;
+            ++steps[s]; ++n_steps;
+            const S7<float> a0 = slot_of<s>(y0), a1 = slot_of<s>(y1);
+            set_slot<s>(y, a1);
+            const float r2 = radius2<F>(a1);
+            disk[s] = disk_candidate<F, float>(P, a0, a1);
+            cross[s] = disk[s] || r2 >= P.escape_r2;
+            if (!cross[s]) {
+                cls[s] = plain_terminal<METRIC, F, float>(P, a1, r2, steps[s]);
+                if (cls[s] == MGK_RAY_ALIVE) to_band[s] = in_band(P, a1.x, a1.y, a1.z);
+            }
+        };
+        accept(std::integral_constant<int, 0>{});
+        accept(std::integral_constant<int, 1>{});
+
+        auto finish = [&](auto sc) {
+            constexpr int s = decltype(sc)::value;
+            if (cls[s] == MGK_RAY_ALIVE) return;
+            if (res) {
+                Term<float> t{cls[s], 0.f, 0.f, 0.f, 0.f, 0.f};
+                write_result<float>(res, ray[s], slot_of<s>(y), lane_of<s>(pt), t, steps[s], att[s], 0u, 0u);
+            }
+            ++n_cls[cls[s]];
+        };
+        finish(std::integral_constant<int, 0>{});
+        finish(std::integral_constant<int, 1>{});
+
+        // ---- hand-offs: disk candidates from the front of the crossing queue,
+        // escapes from the back, FP64-band rays to the resume queue
+        if (__ballot_sync(kFull, cross[0] || cross[1] || to_band[0] || to_band[1]) != 0u) {
+            auto hand_off = [&](auto sc) {
+                constexpr int s = decltype(sc)::value;
+                uint32_t slot = warp_push(cross[s] && disk[s], &cnt->refine_count, nq, &cnt->status);
+                const uint32_t eslot = warp_push(cross[s] && !disk[s], &cnt->escape_count, nq, &cnt->status);
+                if (eslot != ~0u) slot = nq - 1u - eslot;
+                if (slot != ~0u) {
+                    const S7<float> a0 = slot_of<s>(y0), a1 = slot_of<s>(y);
+                    RefineEntry<float> e;
+                    e.y0[0] = a0.x; e.y0[1] = a0.y; e.y0[2] = a0.z; e.y0[3] = a0.t;
+                    e.y0[4] = a0.px; e.y0[5] = a0.py; e.y0[6] = a0.pz;
+                    e.y1[0] = a1.x; e.y1[1] = a1.y; e.y1[2] = a1.z; e.y1[3] = a1.t;
+                    e.y1[4] = a1.px; e.y1[5] = a1.py; e.y1[6] = a1.pz;
+                    e.pt = lane_of<s>(pt); e.h = lane_of<s>(h_used); e.h_next = lane_of<s>(h); e.c0 = lane_of<s>(c0);
+                    e.ray = ray[s]; e.steps = steps[s]; e.attempts = att[s];
+                    e.wide = 0u; e.evals = 0; e.pad[0] = e.pad[1] = e.pad[2] = 0;
+                    refq[slot] = e;
+                }
+                const uint32_t bslot = warp_push(to_band[s], &cnt->resume_count, nq, &cnt->status);
+                if (bslot != ~0u)
+                    store_resume<float>(resq, bslot, slot_of<s>(y), lane_of<s>(pt), lane_of<s>(h), lane_of<s>(c0),
+                                        ray[s], steps[s], att[s], 0u, 0u);
+            };
+            hand_off(std::integral_constant<int, 0>{});
+            hand_off(std::integral_constant<int, 1>{});
+        }
+#pragma unroll
+        for (int s = 0; s < 2; ++s)
+            if (cls[s] != MGK_RAY_ALIVE || cross[s] || to_band[s]) alive[s] = false;
+    }
+
+    const unsigned long long w_att = warp_sum((unsigned long long)n_att);
+    const unsigned long long w_steps = warp_sum((unsigned long long)n_steps);
+    unsigned long long c[5];
+#pragma unroll
+    for (int i = 0; i < 5; ++i) c[i] = warp_sum((unsigned long long)n_cls[i]);
+    if (lane == 0) {
+        atomicAdd(&cnt->attempts, w_att);
+        atomicAdd(&cnt->steps, w_steps);
 #pragma unroll
         for (int i = 1; i < 5; ++i)
             if (c[i]) atomicAdd(&cnt->class_count[i], c[i]);
@@ -926,6 +1121,46 @@ __global__ void __launch_bounds__(256) k_fma_probe(uint32_t iters, float seed, f
     if (r == 12345.f) sink[threadIdx.x] = r;
 }
 
+// ----------------------------------------------------- rounding self-check
+// msqrt / mrcp (dev_physics.cuh) against their definitions, on every one of
+// the 2^32 float inputs: the definitions use the IEEE-rounded __fsqrt_rn and
+// __frcp_rn with the stated clamp and special values.  out[0] / out[1]
+// receive the number of inputs where msqrt / mrcp differ (NaNs compare equal).
+__device__ __forceinline__ float msqrt_definition(float a) {
+    a = fmaxf(a, kSqrtFloor);
+    if (isinf(a)) return __int_as_float(0x7fc00000);
+    return __fsqrt_rn(a);
+}
+__device__ __forceinline__ float mrcp_definition(float b) {
+    const float ab = fabsf(b);
+    if (isnan(b) || ab < 1.17549435e-38f || isinf(b)) return __int_as_float(0x7fc00000);
+    if (ab > 8.507059173023462e37f) return copysignf(0.0f, b);  // 1/b subnormal: |b| > 2^126
+    return __frcp_rn(b);
+}
+__device__ __forceinline__ bool same_bits(float a, float b) {
+    return __float_as_uint(a) == __float_as_uint(b) || (isnan(a) && isnan(b));
+}
+__global__ void __launch_bounds__(256) k_check_rounding(unsigned long long* out) {
+    unsigned long long bad_s = 0, bad_r = 0;
+    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < (1ull << 32); i += stride) {
+        const float a = __uint_as_float(uint32_t(i));
+        bad_s += !same_bits(msqrt(a), msqrt_definition(a));
+        bad_r += !same_bits(mrcp(a), mrcp_definition(a));
+    }
+    bad_s = warp_sum(bad_s);
+    bad_r = warp_sum(bad_r);
+    if ((threadIdx.x & 31) == 0) {
+        if (bad_s) atomicAdd(&out[0], bad_s);
+        if (bad_r) atomicAdd(&out[1], bad_r);
+    }
+}
+
+cudaError_t launch_check_rounding(int sms, unsigned long long* out, cudaStream_t st) {
+    k_check_rounding<<<sms * 8, 256, 0, st>>>(out);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_fma_probe(uint32_t blocks, uint32_t iters, float* sink, cudaStream_t st) {
     k_fma_probe<<<blocks, 256, 0, st>>>(iters, 1.0f, sink);
     return cudaGetLastError();
@@ -963,8 +1198,20 @@ static cudaError_t integ_t(const void* dsc, uint32_t n, const ChunkBuffers& b, m
     auto* refq = reinterpret_cast<RefineEntry<T>*>(b.refine);
     auto* resq = reinterpret_cast<ResumeEntry<T>*>(b.resume);
     auto* hits = reinterpret_cast<HitEntry<T>*>(b.hits);
-    k_integrate<METRIC, MODE><<<blocks, kIntegrateThreads, 0, st>>>(ds<T>(dsc), n, b.qx, b.qp, b.qc, refq, resq, res,
-                                                                   b.counters, b.ray_ids);
+    if constexpr (MGK_MIXED_X2 && MODE == MGK_PRECISION_MIXED && METRIC != MGK_METRIC_MINKOWSKI) {
+        // two rays per thread: half the threads for the same rays
+        per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_integrate_x2<METRIC>, kIntegrateThreads, 0);
+        if (per_sm < 1) per_sm = 1;
+        blocks = uint32_t(sms * per_sm);
+        need = (n + 2 * kIntegrateThreads - 1) / (2 * kIntegrateThreads);
+        if (blocks > need) blocks = need;
+        k_integrate_x2<METRIC><<<blocks, kIntegrateThreads, 0, st>>>(ds<T>(dsc), n, b.qx, b.qp, b.qc, refq, resq, res,
+                                                                     b.counters, b.ray_ids);
+    } else {
+        k_integrate<METRIC, MODE><<<blocks, kIntegrateThreads, 0, st>>>(ds<T>(dsc), n, b.qx, b.qp, b.qc, refq, resq,
+                                                                       res, b.counters, b.ray_ids);
+    }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     const uint32_t hit_cap = b.hit_cap ? b.hit_cap : n;

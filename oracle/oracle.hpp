@@ -24,6 +24,7 @@
 #pragma once
 
 #include <cmath>
+#include <limits>
 #include <cstdint>
 #include <cstring>
 #include <type_traits>
@@ -42,6 +43,29 @@ template <Fuse F, class T> inline T mad(T a, T b, T c) {
     }
 }
 template <class T> inline T sq_root(T v) { using std::sqrt; return sqrt(v); }
+
+// The square root and reciprocal of the fused RHS in float (the library's
+// MIXED mode evaluates them from hardware approximations with one FMA
+// correction each; dev_physics.cuh: msqrt, mrcp), defined by their results:
+//   msqrt(a) = IEEE sqrt(max(a, 2^-100)), NaN for a = +inf;
+//   mrcp(b)  = IEEE 1/b for normal b with a normal reciprocal, +-0 for
+//              |b| > 2^126, NaN for b = +-0, subnormal or infinite.
+// std::fmax, like the device's fmaxf, returns the other operand for a NaN.
+inline float msqrt(float a) {
+    a = std::fmax(a, 0x1p-100f);
+    if (std::isinf(a)) return std::numeric_limits<float>::quiet_NaN();
+    return std::sqrt(a);
+}
+inline float mrcp(float b) {
+    const float ab = std::fabs(b);
+    if (std::isnan(b) || ab < 0x1p-126f || std::isinf(b)) return std::numeric_limits<float>::quiet_NaN();
+    if (ab > 0x1p126f) return std::copysign(0.0f, b);
+    return 1.0f / b;
+}
+template <class T> inline T fused_sqrt(T v) { return sq_root(v); }
+template <> inline float fused_sqrt<float>(float v) { return msqrt(v); }
+template <class T> inline T fused_rcp(T v) { return T(1) / v; }
+template <> inline float fused_rcp<float>(float v) { return mrcp(v); }
 template <class T> inline T fmax_(T a, T b) { using std::fmax; return fmax(a, b); }
 template <class T> inline T fabs_(T a) { using std::fabs; return fabs(a); }
 
@@ -185,10 +209,12 @@ template <Fuse F, class T> inline GState<T> rhs_schwarzschild(const GState<T>& s
 // Fused formulation of the Kerr RHS (the library's MIXED and F64 modes): the
 // same Hamiltonian right-hand side as rhs_kerr, rearranged so that one
 // reciprocal gives 1/d, 1/(r sigma), 1/r and 1/f_den, dr/dx_i = (x r/sigma,
-// y d/(r sigma), z r/sigma), and sum_j p_j dk_j/dx_i comes from
-// G = px (x d - 2 r kx_num) + pz (z d - 2 r kz_num):
-//   px dkx/dx_i + pz dkz/dx_i = (dr_i G + U_i)/d^2, U = d (px r + pz a, 0, pz r - px a),
-//   py dky/dx_i = py (r delta_iy - y dr_i)/r^2.
+// y d/(r sigma), z r/sigma), and sum_j p_j dk_j/dx_i needs no derivative of k:
+//   px dkx/dx_i + pz dkz/dx_i = (dr_i G' + U'_i)/d,  py dky/dx_i = (py/r^2)(r delta_iy - y dr_i),
+// S = px kx + pz kz, G' = (px x + pz z) - 2 r S, U' = (px r + pz a, 0, pz r - px a),
+// so that dp_i/dl = Q dr_i + Ad U'_i + delta_iy E with F = f (k.p), Ad = F/d,
+// B = (k.p)^2 dq - F c y, Q = Ad G' + B, E = F c r - (k.p)^2 2 a^2 r^3 y/f_den^2,
+// c = py/r^2, dq = (3 a^2 r^2 y^2 - r^6)/f_den^2.
 // The device code evaluates exactly these operations in this order.
 template <class T> inline GState<T> rhs_kerr_fused(const GState<T>& s, T a) {
     constexpr Fuse F = Fuse::Fma;
@@ -197,14 +223,14 @@ template <class T> inline GState<T> rhs_kerr_fused(const GState<T>& s, T a) {
     const T a_sq = a * a;
     const T y_sq = y * y;
     const T w_sq = mad<F>(z, z, mad<F>(x, x, y_sq)) - a_sq;
-    const T sigma = sq_root(mad<F>(w_sq, w_sq, (T(4) * a_sq) * y_sq));
-    const T r = sq_root(T(0.5) * (w_sq + sigma));
+    const T sigma = fused_sqrt(mad<F>(w_sq, w_sq, (T(4) * a_sq) * y_sq));
+    const T r = fused_sqrt(T(0.5) * (w_sq + sigma));
     const T r_sq = r * r;
     const T d = r_sq + a_sq;
     const T f_den = mad<F>(a_sq, y_sq, r_sq * r_sq);
     const T rs = r * sigma;
     const T rsd = rs * d;
-    const T inv_all = T(1) / (rsd * f_den);
+    const T inv_all = fused_rcp(rsd * f_den);
     const T inv_rsd = f_den * inv_all;
     const T inv_fden = rsd * inv_all;
     const T inv_d = rs * inv_rsd;
@@ -217,26 +243,25 @@ template <class T> inline GState<T> rhs_kerr_fused(const GState<T>& s, T a) {
     const T kx_num = mad<F>(r, x, -(a * z));
     const T kz_num = mad<F>(r, z, a * x);
     const T kx = kx_num * inv_d, kz = kz_num * inv_d, ky = y * inv_r;
-    const T kTp = mad<F>(pz, kz, mad<F>(py, ky, px * kx)) - pt;
+    const T S = mad<F>(pz, kz, px * kx);
+    const T kTp = mad<F>(py, ky, S) - pt;
     const T f_kTp = f_ * kTp;
     const T kTp2 = kTp * kTp;
     const T two_r = r + r;
-    const T gx = mad<F>(x, d, -(two_r * kx_num));
-    const T gz = mad<F>(z, d, -(two_r * kz_num));
-    const T G = mad<F>(px, gx, pz * gz);
-    const T Ux = d * mad<F>(px, r, pz * a);
-    const T Uz = d * mad<F>(pz, r, -(px * a));
+    const T Gp = mad<F>(-two_r, S, mad<F>(pz, z, px * x));
+    const T Ad = f_kTp * inv_d;
+    const T Ux = mad<F>(px, r, pz * a);
+    const T Uz = mad<F>(pz, r, -(px * a));
     const T c = py * (inv_r * inv_r);
     const T cy = c * y;
     const T inv_fden_sq = inv_fden * inv_fden;
     const T dq = mad<F>((T(3) * a_sq) * r_sq, y_sq, -(r_cu * r_cu)) * inv_fden_sq;
-    const T A = f_kTp * (inv_d * inv_d);
     const T B = mad<F>(kTp2, dq, -(f_kTp * cy));
     const T E = mad<F>(-kTp2, ((T(2) * a_sq) * r_cu) * y * inv_fden_sq, f_kTp * (c * r));
+    const T Q = mad<F>(Ad, Gp, B);
     GState<T> o;
     o.x = V4<T>{mad<F>(-f_kTp, kx, px), mad<F>(-f_kTp, ky, py), mad<F>(-f_kTp, kz, pz), f_kTp - pt};
-    o.p = V4<T>{mad<F>(A, mad<F>(drx, G, Ux), B * drx), mad<F>(A, dry * G, mad<F>(B, dry, E)),
-                mad<F>(A, mad<F>(drz, G, Uz), B * drz), T(0)};
+    o.p = V4<T>{mad<F>(Q, drx, Ad * Ux), mad<F>(Q, dry, E), mad<F>(Q, drz, Ad * Uz), T(0)};
     return o;
 }
 
@@ -246,8 +271,8 @@ template <class T> inline GState<T> rhs_schwarzschild_fused(const GState<T>& s, 
     constexpr Fuse F = Fuse::Fma;
     const T x = s.x.x, y = s.x.y, z = s.x.z;
     const T pt = s.p.t, px = s.p.x, py = s.p.y, pz = s.p.z;
-    const T r = sq_root(mad<F>(z, z, mad<F>(y, y, x * x)));
-    const T inv_r = T(1) / r;
+    const T r = fused_sqrt(mad<F>(z, z, mad<F>(y, y, x * x)));
+    const T inv_r = fused_rcp(r);
     const T kx = x * inv_r, ky = y * inv_r, kz = z * inv_r;
     const T kp = mad<F>(pz, kz, mad<F>(py, ky, px * kx));
     const T kTp = kp - pt;
@@ -431,8 +456,9 @@ template <Ctl K, class T> inline T propose_h(T h, T err_safe, T h_max) {
 
 // Step-size factor err^(-1/5) of the MIXED and F64 controllers, IEEE
 // operations only (the CUDA kernels compute the same bits): a = m 2^e with
-// m in [1, 2), e = 5q + r; a quadratic fit of m^(-1/5) times 2^(-r/5) 2^(-q),
-// then Newton steps y <- y (6 - a y^5) / 5 (two in float, three in double).
+// m in [1, 2), e = 5q + r; a quadratic fit of m^(-1/5) (within 1e-3) times
+// 2^(-r/5) 2^(-q), then Newton steps y <- y (6 - a y^5) / 5 (one in float,
+// three in double).
 inline float inv_root5(float a) {
     if (!(a <= 3.4028235e38f)) return 0.0f;
     uint32_t b;
@@ -450,11 +476,8 @@ inline float inv_root5(float a) {
     float p2;
     std::memcpy(&p2, &pb, 4);
     y = y * p2;
-    for (int it = 0; it < 2; ++it) {
-        float y2 = y * y, y4 = y2 * y2, t = a * (y4 * y);
-        y = y * std::fma(-0.2f, t, 1.2f);
-    }
-    return y;
+    const float y2 = y * y, y4 = y2 * y2, t = a * (y4 * y);
+    return y * std::fma(-0.2f, t, 1.2f);
 }
 inline double inv_root5(double a) {
     if (!(a <= 1.7976931348623157e308)) return 0.0;
@@ -492,23 +515,24 @@ inline void control_f64(const GState<double>& y0, const GState<double>& y1, cons
     *ok = safe < 1.0;
 }
 
-// Reciprocal for the MIXED norm: integer seed 0x7EF311C3 - bits(x) and two
-// Newton steps with fma (identical to the kernels' rcp_norm).
+// Reciprocal for the MIXED norm: integer seed 0x7EF311C3 - bits(x) and one
+// Newton step with fma (identical to the kernels' rcp_norm; within 1.44 %,
+// from below).
 inline float rcp_norm(float x) {
     uint32_t b;
     std::memcpy(&b, &x, 4);
     b = 0x7EF311C3u - b;
     float y;
     std::memcpy(&y, &b, 4);
-    y = y * std::fma(-x, y, 2.0f);
-    y = y * std::fma(-x, y, 2.0f);
-    return y;
+    return y * std::fma(-x, y, 2.0f);
 }
 
-// MIXED RMS norm (relativity_utilities.cuh:15-29 with e_i / scale_i formed as
-// e_i * rcp_norm(scale_i)); component order t, x, y, z, then momentum.
-inline float rms_error_mixed(const GState<float>& e, const GState<float>& y0, const GState<float>& y1, float atol,
-                             float rtol) {
+// MIXED RMS norm of the unscaled error E (the step's error is h E):
+// relativity_utilities.cuh:15-29 with e_i / scale_i formed as
+// E_i * rcp_norm(scale_i) and h applied once, to the sum of squares;
+// component order t, x, y, z, then momentum.
+inline float rms_error_mixed(const GState<float>& e, const GState<float>& y0, const GState<float>& y1, float h,
+                             float atol, float rtol) {
     auto term = [&](float ei, float a0, float a1) {
         return ei * rcp_norm(std::fma(rtol, std::fmax(std::fabs(a0), std::fabs(a1)), atol));
     };
@@ -522,7 +546,15 @@ inline float rms_error_mixed(const GState<float>& e, const GState<float>& y0, co
     acc = std::fma(s5, s5, acc);
     acc = std::fma(s6, s6, acc);
     acc = std::fma(s7, s7, acc);
-    return std::sqrt(acc / 8.0f);
+    return std::sqrt(acc * ((h * h) * 0.125f));
+}
+
+// The unscaled error estimate E = sum_j (b5_j - b4_j) k_j of the Fehlberg
+// pair (internal_math.h:2177 without the factor h).
+template <class T> inline GState<T> rkf45_error_unscaled(const GState<T> k[6]) {
+    using C = Fehlberg<T>;
+    return axpy<Fuse::Fma>(-C::e6, k[5], axpy<Fuse::Fma>(-C::e5, k[4], axpy<Fuse::Fma>(C::e4, k[3],
+                           axpy<Fuse::Fma>(C::e3, k[2], scale(C::e1, k[0])))));
 }
 
 // MIXED control: the error estimate in double from the float stages; its
@@ -531,8 +563,8 @@ inline void control_mixed(const GState<float>& y0, const GState<float>& y1, cons
                           const MetricParams<float>& m, float* h_next, bool* ok) {
     GState<double> kd[6];
     for (int i = 0; i < 6; ++i) kd[i] = to_double(k[i]);
-    GState<float> e = widen<float>(rkf45_error<Fuse::Fma, double>(double(h), kd));
-    float err = rms_error_mixed(e, y0, y1, m.abs_tol, m.rel_tol);
+    GState<float> e = widen<float>(rkf45_error_unscaled<double>(kd));
+    float err = rms_error_mixed(e, y0, y1, h, m.abs_tol, m.rel_tol);
     float safe = err > 1e-30f ? err : 1e-30f;
     float hn = (0.9f * h) * inv_root5(safe);
     if (hn > m.h_max) hn = m.h_max;

@@ -65,6 +65,13 @@ def test_trace_rays_bit_exact(ctx, metric, precision):
     assert (gpu["cls"] != abi.RAY_ALIVE).all()
 
 
+def test_mixed_sqrt_and_reciprocal_match_their_definitions(ctx):
+    """The MIXED fused RHS's square root and reciprocal (hardware approximation
+    plus one FMA correction) equal their definitions, which the oracle
+    restates, on every one of the 2^32 float inputs."""
+    assert ctx.check_rounding() == (0, 0)
+
+
 def test_trace_rays_offset_range(ctx):
     """A range that starts mid-frame and is not pixel aligned."""
     s = small_scene(spp=3)
