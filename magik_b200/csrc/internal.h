@@ -23,7 +23,7 @@ struct Counters {
     uint32_t resume_count;  // entries in the resume queue
     uint32_t status;        // 0 = ok; bit 0: a queue overflowed
     uint32_t fallback_count;  // surrogate renders: rays routed to RKF45
-    uint32_t pad;
+    uint32_t resume_head;     // next resume-queue index handed to a warp of the tail kernel
 };
 
 // Hit-queue entry (disk and sky rays; dark rays are not queued).

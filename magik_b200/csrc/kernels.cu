@@ -47,6 +47,10 @@ constexpr int kIntegrateMinBlocksF64 = 4;
 #ifndef MGK_X2_MIN_BLOCKS
 #define MGK_X2_MIN_BLOCKS 3
 #endif
+// resident blocks of the crossing kernel (one thread per crossing)
+#ifndef MGK_REFINE_MIN_BLOCKS
+#define MGK_REFINE_MIN_BLOCKS 4
+#endif
 // MIXED Kerr / Schwarzschild frames run k_integrate_x2 (1) or k_integrate (0)
 #ifndef MGK_MIXED_X2
 #define MGK_MIXED_X2 0
@@ -561,7 +565,7 @@ __global__ void __launch_bounds__(kIntegrateThreads, MGK_X2_MIN_BLOCKS)
 // emit the hit, or send the ray on to the tail kernel when the disk
 // candidate missed and nothing else ended it.
 template <int METRIC, int MODE>
-__global__ void __launch_bounds__(128, 4) k_refine(const DevScene<typename ModeT<MODE>::T> P,
+__global__ void __launch_bounds__(128, MGK_REFINE_MIN_BLOCKS) k_refine(const DevScene<typename ModeT<MODE>::T> P,
                                                 const RefineEntry<typename ModeT<MODE>::T>* __restrict__ refq,
                                                 uint32_t cap, HitEntry<typename ModeT<MODE>::T>* hits,
                                                 ResumeEntry<typename ModeT<MODE>::T>* resq, mgk_ray_result* res,
@@ -609,8 +613,12 @@ __global__ void __launch_bounds__(128, 4) k_refine(const DevScene<typename ModeT
 }
 
 // ------------------------------------------------------------------- tail
-// One thread per resumed ray, run sequentially to termination.  MIXED mode:
-// FP64 attempts while within MGK_WIDE_BAND of r_plus, FP32 otherwise.
+// Resumed rays (MIXED rays inside the FP64 band, rays whose disk candidate
+// missed), run to termination.  Persistent like k_integrate: every lane
+// holds one ray and takes one attempt per trip, and a warp refills its
+// finished lanes from the resume queue in chunks, so that no lane waits for
+// the longest ray of its warp.  MIXED mode: FP64 attempts while within
+// MGK_WIDE_BAND of r_plus, FP32 otherwise.
 template <int METRIC, int MODE>
 __global__ void __launch_bounds__(128, 4) k_tail(const DevScene<typename ModeT<MODE>::T> P,
                                               const ResumeEntry<typename ModeT<MODE>::T>* __restrict__ resq,
@@ -619,62 +627,105 @@ __global__ void __launch_bounds__(128, 4) k_tail(const DevScene<typename ModeT<M
     using T = typename ModeT<MODE>::T;
     constexpr Fuse F = ModeT<MODE>::F;
     const uint32_t n = min(cnt->resume_count, cap);
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
     unsigned long long n_att = 0, n_steps = 0, n_wide = 0, n_evals = 0;
     uint32_t n_cls[5] = {0, 0, 0, 0, 0};
-    const uint32_t lane = threadIdx.x & 31;
-    const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += stride) {
-        const uint32_t i = base + lane;
-        const bool valid = i < n;
-        Term<T> t{MGK_RAY_ALIVE, T(0), T(0), T(0), T(0), T(0)};
-        ResumeEntry<T> e;
-        S7<T> y{};
-        uint32_t steps = 0, att = 0, wide = 0, evals = 0;
-        if (valid) {
-            e = resq[i];
-            y = s7(e.y);
-            const T pt = e.pt, c0 = e.c0;
-            T h = e.h;
-            steps = e.steps; att = e.attempts; wide = e.wide; evals = e.evals;
-            uint32_t tries = 0;
-            double r_cur = 0.0;
-            if constexpr (MODE == MGK_PRECISION_MIXED)
-                r_cur = ks_r<double>(double(y.x), double(y.y), double(y.z), P.spin_d);
-            for (;;) {
-                S7<T> y1;
-                T hn;
-                bool ok;
-                const T h_used = h;
-                bool w = false;
-                if constexpr (MODE == MGK_PRECISION_MIXED && METRIC != MGK_METRIC_MINKOWSKI) {
-                    w = r_cur - P.r_plus < MGK_WIDE_BAND;
-                    if (w) attempt_wide<METRIC>(P, y, pt, h, y1, hn, ok);
-                    else attempt<METRIC, MODE, T>(P, y, pt, h, y1, hn, ok);
+
+    bool alive = false;
+    S7<T> y{};
+    T pt = 0, c0 = 0, h = 0;
+    uint32_t ray = 0, steps = 0, att = 0, wide = 0, evals = 0, tries = 0;
+    double r_cur = 0.0;
+    uint32_t cbeg = 0, cend = 0;
+    bool drained = false;
+
+    for (;;) {
+        // ---- refill finished lanes (warp-uniform control flow)
+        const unsigned dead = __ballot_sync(kFull, !alive);
+        if (dead != 0u && !(drained && cbeg == cend)) {
+            const uint32_t need = __popc(dead);
+            const uint32_t rem = cend - cbeg;
+            uint32_t nb = 0, ne = 0;
+            if (need > rem && !drained) {
+                uint32_t got = 0;
+                if (lane == 0) got = atomicAdd(&cnt->resume_head, kChunk);
+                got = __shfl_sync(kFull, got, 0);
+                if (got >= n) {
+                    drained = true;
                 } else {
-                    attempt<METRIC, MODE, T>(P, y, pt, h, y1, hn, ok);
+                    nb = got;
+                    ne = min(got + kChunk, n);
+                    if (ne == n) drained = true;
                 }
-                ++att; ++tries; ++n_att;
-                if (w || MODE == MGK_PRECISION_F64) { ++wide; ++n_wide; }
-                h = hn;
-                if (!ok && tries < P.m.n_max) continue;
+            }
+            if (!alive) {
+                const uint32_t rank = __popc(dead & lt);
+                uint32_t idx = ~0u;
+                if (rank < rem) idx = cbeg + rank;
+                else if (rank - rem < ne - nb) idx = nb + (rank - rem);
+                if (idx != ~0u) {
+                    const ResumeEntry<T> e = resq[idx];
+                    y = s7(e.y);
+                    pt = e.pt; c0 = e.c0; h = e.h;
+                    ray = e.ray; steps = e.steps; att = e.attempts; wide = e.wide; evals = e.evals;
+                    tries = 0;
+                    if constexpr (MODE == MGK_PRECISION_MIXED)
+                        r_cur = ks_r<double>(double(y.x), double(y.y), double(y.z), P.spin_d);
+                    alive = true;
+                }
+            }
+            const uint32_t used_old = min(need, rem);
+            if (ne > nb) {
+                cbeg = nb + min(need - used_old, ne - nb);
+                cend = ne;
+            } else {
+                cbeg += used_old;
+            }
+        }
+        if (__ballot_sync(kFull, alive) == 0u) break;
+
+        // ---- one attempt per live lane
+        Term<T> t{MGK_RAY_ALIVE, T(0), T(0), T(0), T(0), T(0)};
+        bool done = false;
+        if (alive) {
+            S7<T> y1;
+            T hn;
+            bool ok;
+            const T h_used = h;
+            bool w = false;
+            if constexpr (MODE == MGK_PRECISION_MIXED && METRIC != MGK_METRIC_MINKOWSKI) {
+                w = r_cur - P.r_plus < MGK_WIDE_BAND;
+                if (w) attempt_wide<METRIC>(P, y, pt, h, y1, hn, ok);
+                else attempt<METRIC, MODE, T>(P, y, pt, h, y1, hn, ok);
+            } else {
+                attempt<METRIC, MODE, T>(P, y, pt, h, y1, hn, ok);
+            }
+            ++att; ++tries; ++n_att;
+            if (w || MODE == MGK_PRECISION_F64) { ++wide; ++n_wide; }
+            h = hn;
+            if (ok || tries >= P.m.n_max) {
                 tries = 0;
                 ++steps; ++n_steps;
                 S7<T> ye;
-                uint32_t ev0 = evals;
+                const uint32_t ev0 = evals;
                 t = resolve<METRIC, F, T>(P, y, y1, pt, h_used, c0, steps, ye, evals);
                 n_evals += evals - ev0;
                 y = ye;
-                if (t.cls != MGK_RAY_ALIVE) break;
-                if constexpr (MODE == MGK_PRECISION_MIXED)
+                if (t.cls != MGK_RAY_ALIVE) done = true;
+                else if constexpr (MODE == MGK_PRECISION_MIXED)
                     r_cur = ks_r<double>(double(y.x), double(y.y), double(y.z), P.spin_d);
             }
         }
-        bool lit = valid && (t.cls == MGK_RAY_DISK || t.cls == MGK_RAY_ESCAPED);
-        uint32_t hslot = warp_push(lit, &cnt->hit_count, hit_cap, &cnt->status);
-        if (hslot != ~0u) push_hit<T>(hits, hslot, e.ray, t);
-        if (valid) {
-            if (res) write_result<T>(res, e.ray, y, e.pt, t, steps, att, wide, evals);
+
+        // ---- finished rays: hit queue (one ballot per warp) and per-ray records
+        const bool lit = done && (t.cls == MGK_RAY_DISK || t.cls == MGK_RAY_ESCAPED);
+        const uint32_t hslot = warp_push(lit, &cnt->hit_count, hit_cap, &cnt->status);
+        if (hslot != ~0u) push_hit<T>(hits, hslot, ray, t);
+        if (done) {
+            if (res) write_result<T>(res, ray, y, pt, t, steps, att, wide, evals);
             ++n_cls[t.cls];
+            alive = false;
         }
     }
     if (n_att) {
@@ -1215,10 +1266,17 @@ static cudaError_t integ_t(const void* dsc, uint32_t n, const ChunkBuffers& b, m
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     const uint32_t hit_cap = b.hit_cap ? b.hit_cap : n;
-    k_refine<METRIC, MODE><<<sms * 8, 128, 0, st>>>(ds<T>(dsc), refq, n, hits, resq, res, b.counters, hit_cap);
+    int refine_per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&refine_per_sm, k_refine<METRIC, MODE>, 128, 0);
+    if (refine_per_sm < 1) refine_per_sm = 1;
+    k_refine<METRIC, MODE><<<sms * refine_per_sm * 2, 128, 0, st>>>(ds<T>(dsc), refq, n, hits, resq, res, b.counters,
+                                                                   hit_cap);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    k_tail<METRIC, MODE><<<sms * 2, 128, 0, st>>>(ds<T>(dsc), resq, n, hits, res, b.counters, hit_cap);
+    int tail_per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tail_per_sm, k_tail<METRIC, MODE>, 128, 0);
+    if (tail_per_sm < 1) tail_per_sm = 1;
+    k_tail<METRIC, MODE><<<sms * tail_per_sm, 128, 0, st>>>(ds<T>(dsc), resq, n, hits, res, b.counters, hit_cap);
     return cudaGetLastError();
 }
 
