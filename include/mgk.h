@@ -116,14 +116,35 @@ typedef struct mgk_scene {
     uint32_t width;
     uint32_t height;
     uint32_t spp;            /* samples per pixel; ray id = pixel * spp + sample */
-    uint32_t reserved0;
+    uint32_t spectral_mode;  /* MGK_SPECTRAL_BINS or MGK_SPECTRAL_SAMPLED */
     uint64_t seed;           /* counter-based RNG seed (pixel jitter, star catalogue) */
-    double lambda_min_nm;    /* bins are uniform over [lambda_min, lambda_max]; */
-    double lambda_max_nm;    /* emission is sampled at the bin centres */
+    double lambda_min_nm;    /* bins are uniform over [lambda_min, lambda_max] */
+    double lambda_max_nm;
     double star_radius_rad;  /* angular radius of a star's disc on the sky, (0, 0.02] */
+    /* MGK_SPECTRAL_SAMPLED only: the reference's sensor (optical_system_settings.h,
+     * color_settings.h) */
+    double iso;                     /* reference default 500 */
+    double fps;                     /* 24 */
+    double shutter_angle_deg;       /* 180 */
+    double redistribution_sigma_nm; /* Gaussian spread of a sample over the bins, 10 */
 } mgk_scene;
 
 #define MGK_MAX_BINS 64
+
+/* Spectral modes.
+ *  MGK_SPECTRAL_BINS (default): the emission is evaluated at the n_bins bin
+ *    centres and the film holds radiance per bin.
+ *  MGK_SPECTRAL_SAMPLED: the reference renderer's stochastic mode.  Each ray
+ *    draws one wavelength from the CIE inverse CDF table
+ *    (device_sensor_utilities.cuh:25-33; 256 entries, built like
+ *    host_color_utilities.cuh:188-233 from the analytic colour-matching
+ *    functions), its radiance there carries the throughput 1/pdf, is turned
+ *    into sensor irradiance (device_color_utilities.cuh:22-29) and spread over
+ *    the bins with a Gaussian of redistribution_sigma_nm
+ *    (kernel_redistribute_radiance.cu:55-92).  The film holds irradiance. */
+#define MGK_SPECTRAL_BINS 0
+#define MGK_SPECTRAL_SAMPLED 1
+#define MGK_CMF_ICDF_ENTRIES 256
 
 /* One background star (32 bytes). */
 typedef struct mgk_star {
@@ -191,6 +212,13 @@ MGK_API double mgk_isco_radius(double spin);
  * (host_color_utilities.cuh:145-178); the colour-matching functions are the
  * multi-lobe Gaussian fit of Wyman, Sloan and Shirley (JCGT 2(2), 2013). */
 MGK_API mgk_result mgk_xyz_weights(uint32_t n_bins, double lambda_min_nm, double lambda_max_nm, float* w_out);
+/* The CIE inverse CDF table of the sampled spectral mode (MGK_SPECTRAL_SAMPLED)
+ * for [lambda_min_nm, lambda_max_nm]: MGK_CMF_ICDF_ENTRIES wavelengths (nm) at
+ * equidistant probabilities, built as the reference's
+ * compute_tabulated_cmf_inverse_cdf (host_color_utilities.cuh:188-233,
+ * floor 5 %) from the analytic colour-matching functions.  Host only. */
+MGK_API mgk_result mgk_cmf_inverse_cdf(double lambda_min_nm, double lambda_max_nm, float* table_out);
+
 /* Seeded star catalogue: directions uniform on the sphere, magnitudes uniform
  * in [0, 10] (fluxes log-uniform over four decades), temperatures uniform in
  * [3000, 30000] K. */

@@ -32,7 +32,7 @@ EXPORTS = [
     "mgk_context_create", "mgk_context_destroy", "mgk_last_error", "mgk_scene_defaults", "mgk_isco_radius",
     "mgk_xyz_weights", "mgk_star_catalog", "mgk_scene_constants", "mgk_render", "mgk_render_host",
     "mgk_trace_rays", "mgk_shade_rays", "magik_trace_geodesic", "mgk_trace_geodesic_batch", "mgk_fp32_peak",
-    "mgk_check_rounding",
+    "mgk_check_rounding", "mgk_cmf_inverse_cdf",
     "mgk_trace_rays_static", "mgk_train_defaults", "mgk_surrogate_param_count", "mgk_surrogate_create",
     "mgk_surrogate_destroy", "mgk_surrogate_get_params", "mgk_surrogate_set_params", "mgk_make_samples",
     "mgk_surrogate_forward", "mgk_surrogate_forward_tiled", "mgk_surrogate_status", "mgk_surrogate_gradient", "mgk_surrogate_train", "mgk_render_surrogate",
@@ -76,6 +76,7 @@ def lib():
                                                P(abi.TraceMetricParams), P(abi.TraceIntegratorParams), C.c_uint32]
         L.mgk_fp32_peak.argtypes = [vp, P(C.c_double)]
         L.mgk_check_rounding.argtypes = [vp, P(C.c_uint64)]
+        L.mgk_cmf_inverse_cdf.argtypes = [C.c_double, C.c_double, P(C.c_float)]
         L.mgk_trace_rays_static.argtypes = [P(Scene), C.c_uint64, C.c_uint32, vp, vp]
         L.mgk_train_defaults.argtypes = [P(abi.TrainConfig)]
         L.mgk_train_defaults.restype = None
@@ -127,6 +128,14 @@ def xyz_weights(n_bins, lambda_min_nm=380.0, lambda_max_nm=780.0):
     out = (C.c_float * (3 * n_bins))()
     _check(lib().mgk_xyz_weights(n_bins, lambda_min_nm, lambda_max_nm, out), "mgk_xyz_weights")
     return np.frombuffer(out, dtype=np.float32).reshape(n_bins, 3).copy()
+
+
+def cmf_inverse_cdf(lambda_min_nm=380.0, lambda_max_nm=780.0):
+    """mgk_cmf_inverse_cdf: the sampled spectral mode's CIE inverse CDF table
+    (256 wavelengths in nm)."""
+    out = (C.c_float * abi.CMF_ICDF_ENTRIES)()
+    _check(lib().mgk_cmf_inverse_cdf(lambda_min_nm, lambda_max_nm, out), "mgk_cmf_inverse_cdf")
+    return np.frombuffer(out, dtype=np.float32).copy()
 
 
 def star_catalog(seed, n):

@@ -20,6 +20,8 @@ RAY_ALIVE, RAY_DISK, RAY_ESCAPED, RAY_HORIZON, RAY_STEP_LIMIT = 0, 1, 2, 3, 4
 CLASS_NAMES = {0: "alive", 1: "disk", 2: "escaped", 3: "horizon", 4: "step_limit"}
 MASSIVE, MASSLESS = 0, 1
 MAX_BINS = 64
+SPECTRAL_BINS, SPECTRAL_SAMPLED = 0, 1
+CMF_ICDF_ENTRIES = 256
 WIDE_BAND = 0.05
 
 
@@ -33,9 +35,11 @@ class Scene(C.Structure):
         ("escape_radius", C.c_double), ("disk_r_in", C.c_double), ("disk_r_out", C.c_double),
         ("disk_T_in", C.c_double), ("cam_r", C.c_double), ("cam_incl_rad", C.c_double),
         ("focal_length_mm", C.c_double), ("sensor_diag_mm", C.c_double),
-        ("width", C.c_uint32), ("height", C.c_uint32), ("spp", C.c_uint32), ("reserved0", C.c_uint32),
+        ("width", C.c_uint32), ("height", C.c_uint32), ("spp", C.c_uint32), ("spectral_mode", C.c_uint32),
         ("seed", C.c_uint64), ("lambda_min_nm", C.c_double), ("lambda_max_nm", C.c_double),
         ("star_radius_rad", C.c_double),
+        ("iso", C.c_double), ("fps", C.c_double), ("shutter_angle_deg", C.c_double),
+        ("redistribution_sigma_nm", C.c_double),
     ]
 
     def copy(self):
@@ -113,7 +117,7 @@ class TraceContainer(C.Structure):
                 ("steps", C.POINTER(TraceStep))]
 
 
-assert C.sizeof(Scene) == 184, C.sizeof(Scene)
+assert C.sizeof(Scene) == 216, C.sizeof(Scene)
 assert C.sizeof(Star) == 32
 assert C.sizeof(RayResult) == 128
 assert C.sizeof(TraceStep) == 60

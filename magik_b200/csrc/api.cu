@@ -77,6 +77,10 @@ mgk_result validate(const mgk_scene* s) {
     if (!(s->focal_length_mm > 0.0) || !(s->sensor_diag_mm > 0.0) || !(s->cam_r > 0.0))
         return MGK_ERROR_INVALID_ARGUMENT;
     if (!(s->star_radius_rad > 0.0 && s->star_radius_rad <= 0.02)) return MGK_ERROR_INVALID_ARGUMENT;
+    if (s->spectral_mode > MGK_SPECTRAL_SAMPLED) return MGK_UNKNOWN_ENUM_TYPE;
+    if (s->spectral_mode == MGK_SPECTRAL_SAMPLED &&
+        !(s->iso > 0.0 && s->fps > 0.0 && s->shutter_angle_deg > 0.0 && s->redistribution_sigma_nm > 0.0))
+        return MGK_ERROR_INVALID_ARGUMENT;
     // MIXED evaluates the RHS with one float reciprocal of ~r^9, finite below
     // r ~ 1.9e4; a ray moves at most about h_max past the escape radius
     if (s->precision == MGK_PRECISION_MIXED && s->escape_radius + 2.0 * s->h_max > 1.5e4)
@@ -115,6 +119,43 @@ uint32_t grid_n(double radius) {
 }
 
 }  // namespace
+
+namespace mgk {
+// CIE inverse CDF table of the sampled spectral mode, as the reference builds
+// it (host_color_utilities.cuh:188-233) in float: the colour-matching
+// functions resampled at 471 points over [lmin, lmax] (the reference's 1 nm
+// CIE 1931 table has 471 entries), s = x + y + z, a trapezoid CDF with a
+// floor of 5 % of the mean of s per unit wavelength, normalised, inverted at
+// 256 equidistant probabilities by linear interpolation.
+void cmf_inverse_cdf_table(double lmin_d, double lmax_d, float* out) {
+    constexpr uint32_t n_entries = 471;
+    const uint32_t n = n_entries - 1;
+    const float lmin = float(lmin_d), lmax = float(lmax_d);
+    const float dl = (lmax - lmin) / float(n);
+    std::vector<float> s(n_entries);
+    for (uint32_t i = 0; i < n_entries; ++i) {
+        double c[3];
+        cmf_1931(double(lmin + float(i) * dl), c);
+        s[i] = (float(c[0]) + float(c[1])) + float(c[2]);
+    }
+    float mean = 0.0f;
+    for (uint32_t i = 0; i < n_entries; ++i) mean += s[i];
+    mean /= float(n_entries);
+    const float floor = 0.05f * mean;
+    std::vector<float> cdf(n + 1, 0.0f);
+    for (uint32_t i = 0; i < n; ++i) cdf[i + 1] = cdf[i] + (0.5f * (s[i] + s[i + 1]) + floor) * dl;
+    const float total = cdf[n];
+    for (uint32_t j = 0; j <= n; ++j) cdf[j] /= total;
+    uint32_t j = 0;
+    for (uint32_t k = 0; k < MGK_CMF_ICDF_ENTRIES; ++k) {
+        const float u = float(k) / float(MGK_CMF_ICDF_ENTRIES - 1);
+        while (j < n - 1 && cdf[j + 1] < u) ++j;
+        const float tt = (u - cdf[j]) / std::fmax(cdf[j + 1] - cdf[j], 1e-12f);
+        out[k] = lmin + (float(j) + tt) * dl;
+    }
+}
+
+}  // namespace mgk
 
 constexpr int kStarBox = 4;
 
@@ -481,6 +522,11 @@ MGK_API void mgk_scene_defaults(mgk_scene* s) {
     s->lambda_min_nm = 380.0;
     s->lambda_max_nm = 780.0;
     s->star_radius_rad = 2.0e-3;
+    s->spectral_mode = MGK_SPECTRAL_BINS;
+    s->iso = 500.0;
+    s->fps = 24.0;
+    s->shutter_angle_deg = 180.0;
+    s->redistribution_sigma_nm = 10.0;
 }
 
 MGK_API mgk_result mgk_xyz_weights(uint32_t n_bins, double lmin, double lmax, float* w_out) {
@@ -502,6 +548,13 @@ MGK_API mgk_result mgk_xyz_weights(uint32_t n_bins, double lmin, double lmax, fl
         sum_y += acc[3 * i + 1];
     }
     for (uint32_t i = 0; i < 3 * n_bins; ++i) w_out[i] = float(acc[i] / sum_y / bin);
+    return MGK_SUCCESS;
+}
+
+MGK_API mgk_result mgk_cmf_inverse_cdf(double lmin, double lmax, float* table_out) {
+    if (!table_out) return MGK_ERROR_INVALID_POINTER;
+    if (!(lmax > lmin) || !(lmin > 0.0)) return MGK_ERROR_INVALID_ARGUMENT;
+    cmf_inverse_cdf_table(lmin, lmax, table_out);
     return MGK_SUCCESS;
 }
 

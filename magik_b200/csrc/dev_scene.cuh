@@ -194,6 +194,13 @@ template <class T> struct DevScene {
     uint32_t width, height, spp, n_bins, max_steps, disk_on;
     int32_t metric;
     float inv_spp;
+    // MGK_SPECTRAL_SAMPLED
+    uint32_t spectral_mode;
+    float cmf_icdf[MGK_CMF_ICDF_ENTRIES];  // CIE inverse CDF, nm
+    T planck_c1, planck_c2;  // 2 h c^2 and h c / k_B (SI), for the sampled wavelength
+    T sensor_gain;           // radiance * throughput -> sensor irradiance (device_color_utilities.cuh:22-29)
+    T lambda_lo, dlambda;    // bin edges lambda_lo + k dlambda, nm
+    T inv_sigma_sqrt2;       // 1 / (redistribution sigma * sqrt 2), 1/nm
 };
 
 // ------------------------------------------------------------ camera

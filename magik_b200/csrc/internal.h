@@ -102,6 +102,9 @@ cudaError_t launch_trace_geodesic(const void* jobs, uint32_t n, void* steps, uin
 size_t dev_scene_size(const mgk_scene& s);
 // Fills the device-scene table (host memory, dev_scene_size bytes).
 void fill_dev_scene(const mgk_scene& s, const float* xyz_w, void* out);
+// The CIE inverse CDF table of the sampled spectral mode (api.cu):
+// MGK_CMF_ICDF_ENTRIES wavelengths in nm.
+void cmf_inverse_cdf_table(double lmin_nm, double lmax_nm, float* out);
 
 // One geodesic of the reference-compatible trace API (host-prepared inputs).
 struct TraceJob {

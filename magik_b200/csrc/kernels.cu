@@ -21,9 +21,9 @@
 //               [host_trace_geodesic.cu:74-117]
 //
 // Compiled with -fmad=false: no multiply-add is fused unless written as mad().
+#include <cmath>
 #include <cstdint>
 #include <cuda_runtime.h>
-
 #include <type_traits>
 
 #include "dev_pair.cuh"
@@ -742,10 +742,18 @@ __global__ void __launch_bounds__(128, 4) k_tail(const DevScene<typename ModeT<M
 // One thread per hit (a warp shades 32 hits at once, so the dependent loads of
 // the entry, the star cell and the stars overlap across lanes).  The boosted
 // blackbody I(lambda_obs) = B(z lambda_obs, T) z^5 is evaluated as
-//   a_k / (exp(b_k / (z T)) - 1),  a_k = 2 h c^2 / lambda_k^5,  b_k = h c / (k_B lambda_k),
+//   a / (exp(b / (z T)) - 1),  a = 2 h c^2 / lambda^5,  b = h c / (k_B lambda),
 // since the z^5 of the boost cancels the z^-5 of B at the shifted wavelength:
-// one exponential and one quotient per bin.  a_k, b_k and the XYZ weights are
-// staged in shared memory.
+// one exponential and one quotient per wavelength.
+//  MGK_SPECTRAL_BINS: the emission at every bin centre (a_k, b_k and the XYZ
+//    weights staged in shared memory); the film holds radiance per bin.
+//  MGK_SPECTRAL_SAMPLED: the reference's stochastic sensor.  The ray's
+//    wavelength comes from the CIE inverse CDF (device_sensor_utilities.cuh:
+//    25-33, u = rng(seed, sample, pixel, 2)) with throughput 1/pdf; its
+//    radiance times throughput times the sensor gain is the sampled
+//    irradiance (device_color_utilities.cuh:22-29), spread over the bins by
+//    the Gaussian CDF differences at the bin edges
+//    (kernel_redistribute_radiance.cu:55-92).
 template <class T>
 __global__ void __launch_bounds__(256) k_shade(const DevScene<T> P, const HitEntry<T>* __restrict__ hits,
                                                uint32_t cap, const Counters* cnt, const mgk_star* __restrict__ stars,
@@ -754,21 +762,43 @@ __global__ void __launch_bounds__(256) k_shade(const DevScene<T> P, const HitEnt
                                                uint64_t first_ray) {
     __shared__ float sw[3 * MGK_MAX_BINS];
     __shared__ T sa[MGK_MAX_BINS], sb[MGK_MAX_BINS];
+    __shared__ float sicdf[MGK_CMF_ICDF_ENTRIES];
     const uint32_t nb = P.n_bins;
+    const bool sampled = P.spectral_mode == MGK_SPECTRAL_SAMPLED;
     for (uint32_t i = threadIdx.x; i < 3 * MGK_MAX_BINS; i += blockDim.x)
         sw[i] = i < 3 * nb ? (d_w ? d_w[i] : P.xyz_w[i]) : 0.f;
     for (uint32_t i = threadIdx.x; i < MGK_MAX_BINS; i += blockDim.x) {
         sa[i] = P.planck_a[i];
         sb[i] = P.planck_b[i];
     }
+    for (uint32_t i = threadIdx.x; i < MGK_CMF_ICDF_ENTRIES; i += blockDim.x) sicdf[i] = sampled ? P.cmf_icdf[i] : 0.f;
     __syncthreads();
     const uint32_t n = min(cnt->hit_count, cap);
     for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
         const HitEntry<T> h = hits[e];
+        const uint64_t ray_id = first_ray + h.ray;
         float X = 0.f, Y = 0.f, Z = 0.f;
-        float* spec = film_spec ? film_spec + ((first_ray + h.ray) / P.spp) * nb : nullptr;
+        float* spec = film_spec ? film_spec + (ray_id / P.spp) * nb : nullptr;
+        // sampled mode: the ray's wavelength, throughput and Planck factors there
+        T lam = T(0), tput = T(0), a_s = T(0), b_s = T(0), rad = T(0);
+        if (sampled) {
+            const uint32_t pixel = uint32_t(ray_id / P.spp), sample = uint32_t(ray_id % P.spp);
+            const float x = rng_unit(P.seed, sample, pixel, 2) * float(MGK_CMF_ICDF_ENTRIES - 1);
+            const uint32_t k = uint32_t(fminf(x, float(MGK_CMF_ICDF_ENTRIES) - 2.0f));
+            const float f = x - float(k);
+            const float t0 = sicdf[k], t1 = sicdf[k + 1];
+            lam = T((t0 * (1.0f - f)) + (t1 * f));  // lerp, internal_math.h:2040-2043
+            tput = T(float(MGK_CMF_ICDF_ENTRIES - 1) * (t1 - t0));
+            const T lm = lam * T(1e-9), l2 = lm * lm, l4 = l2 * l2, l5 = l4 * lm;
+            a_s = P.planck_c1 / l5;
+            b_s = P.planck_c2 / lm;
+        }
         auto add = [&](T amp, T temp) {
             const T u = T(1) / (h.z * temp);
+            if (sampled) {
+                rad += clamp_radiance<T>(amp * (a_s / (exp(b_s * u) - T(1))));
+                return;
+            }
             for (uint32_t k = 0; k < nb; ++k) {
                 float sv = float(clamp_radiance<T>(amp * (sa[k] / (exp(sb[k] * u) - T(1)))));
                 X = __fmaf_rn(sv, sw[3 * k], X);
@@ -789,6 +819,22 @@ __global__ void __launch_bounds__(256) k_shade(const DevScene<T> P, const HitEnt
                 T q = mad<Fuse::Fma>(dz, dz, mad<Fuse::Fma>(dy, dy, dx * dx)) * P.star_inv_r2;
                 if (q >= T(1)) continue;
                 add(T(st.amplitude) * ((T(1) - q) * (T(1) - q)), T(st.temperature));
+            }
+        }
+        if (sampled) {
+            const T irr = (rad * tput) * P.sensor_gain;
+            if (irr > T(0)) {
+                T phi0 = T(0.5) * (T(1) + erf((P.lambda_lo - lam) * P.inv_sigma_sqrt2));
+                for (uint32_t k = 0; k < nb; ++k) {
+                    const T e1 = P.lambda_lo + T(k + 1) * P.dlambda;
+                    const T phi1 = T(0.5) * (T(1) + erf((e1 - lam) * P.inv_sigma_sqrt2));
+                    const float sv = float(irr * (phi1 - phi0));
+                    phi0 = phi1;
+                    X = __fmaf_rn(sv, sw[3 * k], X);
+                    Y = __fmaf_rn(sv, sw[3 * k + 1], Y);
+                    Z = __fmaf_rn(sv, sw[3 * k + 2], Z);
+                    if (spec) atomicAdd(spec + k, sv * P.inv_spp);
+                }
             }
         }
         xyz_ray[3 * size_t(h.ray) + 0] = X;
@@ -1406,6 +1452,24 @@ template <class T> static void fill_t(const mgk_scene& s, const float* xyz_w, De
     P->max_steps = s.max_steps;
     P->metric = s.metric;
     P->inv_spp = 1.0f / float(s.spp);
+    P->spectral_mode = s.spectral_mode;
+    if (s.spectral_mode == MGK_SPECTRAL_SAMPLED) {
+        cmf_inverse_cdf_table(s.lambda_min_nm, s.lambda_max_nm, P->cmf_icdf);
+        const double h = 6.62607015E-34, c = 299792458.0, kb = 1.380649E-23;
+        P->planck_c1 = T(2.0 * h * c * c);
+        P->planck_c2 = T(h * c / kb);
+        // radiance_to_irradiance (device_color_utilities.cuh:22-29): the sensor of
+        // sensor_diag_mm with the frame's aspect (compute_inv_b,
+        // device_sensor_utilities.cuh:59-62), area per pixel times
+        // iso 2 pi / ((360 fps) / shutter angle)
+        const double W = s.width, H = s.height;
+        const double inv_b = s.sensor_diag_mm / std::sqrt(W * W + H * H);
+        const double area_m2 = (W * inv_b) * (H * inv_b) / 1e6;
+        P->sensor_gain = T((area_m2 / (W * H)) * s.iso * 2.0 * M_PI / ((360.0 * s.fps) / s.shutter_angle_deg));
+        P->lambda_lo = T(s.lambda_min_nm);
+        P->dlambda = T(dl);
+        P->inv_sigma_sqrt2 = T(1.0 / (s.redistribution_sigma_nm * std::sqrt(2.0)));
+    }
 }
 
 void fill_dev_scene(const mgk_scene& s, const float* xyz_w, void* out) {

@@ -239,7 +239,8 @@ int orc_trace_rays(const mgk_scene* s, uint64_t first, uint32_t n, mgk_ray_resul
 
 // Spectrum -> XYZ of given ray results (shading stage alone).
 int orc_shade_rays(const mgk_scene* s, const mgk_star* stars, uint32_t n_stars, const float* w, uint32_t n,
-                   const mgk_ray_result* in, double* xyz_out, int nthreads) {
+                   const mgk_ray_result* in, uint64_t first_ray, const float* icdf, double* xyz_out, int nthreads) {
+    if (s->spectral_mode == MGK_SPECTRAL_SAMPLED && !icdf) return 1;
     StarIndex idx;
     idx.build(stars, n_stars, s->star_radius_rad);
     const uint32_t nb = s->n_bins;
@@ -252,14 +253,16 @@ int orc_shade_rays(const mgk_scene* s, const mgk_star* stars, uint32_t n_stars, 
             for (uint32_t k = 0; k < nb; ++k) lam[k] = s->lambda_min_nm + (k + 0.5) * dl;
             Hit<double> h; h.cls = r.cls; h.z = r.z; h.r_hit = r.r_hit;
             h.dir[0] = r.dir[0]; h.dir[1] = r.dir[1]; h.dir[2] = r.dir[2];
-            ray_spectrum<double>(*s, &idx, h, lam, spec);
+            if (s->spectral_mode == MGK_SPECTRAL_SAMPLED) sampled_spectrum<double>(*s, &idx, h, first_ray + i, icdf, spec);
+            else ray_spectrum<double>(*s, &idx, h, lam, spec);
             spectrum_xyz<double>(nb, spec, w, out3);
         } else {
             float lam[MGK_MAX_BINS], spec[MGK_MAX_BINS], o[3];
             for (uint32_t k = 0; k < nb; ++k) lam[k] = float(s->lambda_min_nm + (k + 0.5) * dl);
             Hit<float> h; h.cls = r.cls; h.z = float(r.z); h.r_hit = float(r.r_hit);
             h.dir[0] = float(r.dir[0]); h.dir[1] = float(r.dir[1]); h.dir[2] = float(r.dir[2]);
-            ray_spectrum<float>(*s, &idx, h, lam, spec);
+            if (s->spectral_mode == MGK_SPECTRAL_SAMPLED) sampled_spectrum<float>(*s, &idx, h, first_ray + i, icdf, spec);
+            else ray_spectrum<float>(*s, &idx, h, lam, spec);
             spectrum_xyz<float>(nb, spec, w, o);
             out3[0] = o[0]; out3[1] = o[1]; out3[2] = o[2];
         }
@@ -272,8 +275,9 @@ int orc_shade_rays(const mgk_scene* s, const mgk_star* stars, uint32_t n_stars, 
 // trace every sample, shade, average.  xyz_out: 3 doubles per pixel.
 // attempts_out (may be NULL) receives the RKF45 attempt total.
 int orc_render_pixels(const mgk_scene* s, const mgk_star* stars, uint32_t n_stars, const float* w,
-                      uint64_t first_pixel, uint32_t n_pixels, uint64_t pixel_stride, double* xyz_out,
-                      uint64_t* attempts_out, int nthreads) {
+                      uint64_t first_pixel, uint32_t n_pixels, uint64_t pixel_stride, const float* icdf,
+                      double* xyz_out, uint64_t* attempts_out, int nthreads) {
+    if (s->spectral_mode == MGK_SPECTRAL_SAMPLED && !icdf) return 1;
     SceneConsts c = scene_consts(*s);
     StarIndex idx;
     idx.build(stars, n_stars, s->star_radius_rad);
@@ -293,7 +297,9 @@ int orc_render_pixels(const mgk_scene* s, const mgk_star* stars, uint32_t n_star
                 for (uint32_t k = 0; k < nb; ++k) lam[k] = s->lambda_min_nm + (k + 0.5) * dl;
                 Hit<double> h; h.cls = r.cls; h.z = r.z; h.r_hit = r.r_hit;
                 h.dir[0] = r.dir[0]; h.dir[1] = r.dir[1]; h.dir[2] = r.dir[2];
-                ray_spectrum<double>(*s, &idx, h, lam, spec);
+                if (s->spectral_mode == MGK_SPECTRAL_SAMPLED)
+                    sampled_spectrum<double>(*s, &idx, h, pix * spp + smp, icdf, spec);
+                else ray_spectrum<double>(*s, &idx, h, lam, spec);
                 spectrum_xyz<double>(nb, spec, w, o);
                 for (int k = 0; k < 3; ++k) acc[k] += o[k];
             } else {
@@ -301,7 +307,9 @@ int orc_render_pixels(const mgk_scene* s, const mgk_star* stars, uint32_t n_star
                 for (uint32_t k = 0; k < nb; ++k) lam[k] = float(s->lambda_min_nm + (k + 0.5) * dl);
                 Hit<float> h; h.cls = r.cls; h.z = float(r.z); h.r_hit = float(r.r_hit);
                 h.dir[0] = float(r.dir[0]); h.dir[1] = float(r.dir[1]); h.dir[2] = float(r.dir[2]);
-                ray_spectrum<float>(*s, &idx, h, lam, spec);
+                if (s->spectral_mode == MGK_SPECTRAL_SAMPLED)
+                    sampled_spectrum<float>(*s, &idx, h, pix * spp + smp, icdf, spec);
+                else ray_spectrum<float>(*s, &idx, h, lam, spec);
                 spectrum_xyz<float>(nb, spec, w, o);
                 for (int k = 0; k < 3; ++k) accf[k] += o[k];
             }

@@ -39,10 +39,11 @@ def lib():
         L.orc_trace_rays.argtypes = [C.POINTER(abi.Scene), C.c_uint64, C.c_uint32, C.POINTER(abi.RayResult),
                                      C.c_int]
         L.orc_shade_rays.argtypes = [C.POINTER(abi.Scene), C.POINTER(abi.Star), C.c_uint32, C.POINTER(C.c_float),
-                                     C.c_uint32, C.POINTER(abi.RayResult), C.POINTER(C.c_double), C.c_int]
+                                     C.c_uint32, C.POINTER(abi.RayResult), C.c_uint64, C.POINTER(C.c_float),
+                                     C.POINTER(C.c_double), C.c_int]
         L.orc_render_pixels.argtypes = [C.POINTER(abi.Scene), C.POINTER(abi.Star), C.c_uint32,
                                         C.POINTER(C.c_float), C.c_uint64, C.c_uint32, C.c_uint64,
-                                        C.POINTER(C.c_double), C.POINTER(C.c_uint64), C.c_int]
+                                        C.POINTER(C.c_float), C.POINTER(C.c_double), C.POINTER(C.c_uint64), C.c_int]
         L.orc_count_ops.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_uint64)]
         _lib = L
     return _lib
@@ -60,6 +61,7 @@ def ref():
                                          abi.TraceMetricParams, abi.TraceIntegratorParams]
         R.ref_trace_geodesic.restype = C.c_int
         R.ref_cmf_weights.argtypes = [C.c_uint, C.c_float, C.c_float, C.POINTER(C.c_float)]
+        R.ref_cmf_inverse_cdf.argtypes = [C.c_float, C.c_float, C.POINTER(C.c_float)]
         R.ref_render_pixels.argtypes = [C.POINTER(abi.Scene), C.POINTER(abi.Star), C.c_uint32, C.POINTER(C.c_float),
                                         C.c_uint64, C.c_uint32, C.c_uint64, C.POINTER(C.c_double), C.c_int]
         R.ref_render_pixels.restype = C.c_int
@@ -99,6 +101,12 @@ def ref_cmf_weights(n_bins, lmin, lmax):
     return np.frombuffer(out, dtype=np.float32).reshape(n_bins, 3).copy()
 
 
+def ref_cmf_inverse_cdf(lmin, lmax):
+    out = (C.c_float * abi.CMF_ICDF_ENTRIES)()
+    assert ref().ref_cmf_inverse_cdf(lmin, lmax, out) == abi.CMF_ICDF_ENTRIES
+    return np.frombuffer(out, dtype=np.float32).copy()
+
+
 def scene_constants(scene):
     out = (C.c_double * 32)()
     lib().orc_scene_constants(C.byref(scene), out)
@@ -118,25 +126,45 @@ def trace_rays(scene, first, n, nthreads=None):
     return out
 
 
-def shade_rays(scene, stars, weights, results, nthreads=None):
+def _icdf_ptr(scene, icdf):
+    """The sampled spectral mode's inverse CDF table (256 float32) as a
+    pointer, or None in the bin mode."""
+    if scene.spectral_mode != abi.SPECTRAL_SAMPLED:
+        return None, None
+    if icdf is None:
+        raise ValueError("the sampled spectral mode needs its inverse CDF table (icdf=...)")
+    a = np.ascontiguousarray(icdf, dtype=np.float32)
+    assert a.size == abi.CMF_ICDF_ENTRIES
+    return a, a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def shade_rays(scene, stars, weights, results, nthreads=None, first_ray=0, icdf=None):
+    """XYZ of per-ray records of camera rays first_ray, first_ray + 1, ...
+    (icdf: the inverse CDF table, sampled spectral mode only)."""
     stars = np.ascontiguousarray(stars)
     w = np.ascontiguousarray(weights, dtype=np.float32)
     out = np.zeros((len(results), 3), dtype=np.float64)
-    lib().orc_shade_rays(C.byref(scene), stars.ctypes.data_as(C.POINTER(abi.Star)), len(stars),
-                         w.ctypes.data_as(C.POINTER(C.c_float)), len(results),
-                         np.ascontiguousarray(results).ctypes.data_as(C.POINTER(abi.RayResult)),
-                         out.ctypes.data_as(C.POINTER(C.c_double)), nthreads or os.cpu_count())
+    keep, p = _icdf_ptr(scene, icdf)
+    rc = lib().orc_shade_rays(C.byref(scene), stars.ctypes.data_as(C.POINTER(abi.Star)), len(stars),
+                              w.ctypes.data_as(C.POINTER(C.c_float)), len(results),
+                              np.ascontiguousarray(results).ctypes.data_as(C.POINTER(abi.RayResult)), first_ray, p,
+                              out.ctypes.data_as(C.POINTER(C.c_double)), nthreads or os.cpu_count())
+    assert rc == 0
+    del keep
     return out
 
 
-def render_pixels(scene, stars, weights, first_pixel, n_pixels, nthreads=None, stride=1):
+def render_pixels(scene, stars, weights, first_pixel, n_pixels, nthreads=None, stride=1, icdf=None):
     stars = np.ascontiguousarray(stars)
     w = np.ascontiguousarray(weights, dtype=np.float32)
     out = np.zeros((n_pixels, 3), dtype=np.float64)
     att = C.c_uint64(0)
-    lib().orc_render_pixels(C.byref(scene), stars.ctypes.data_as(C.POINTER(abi.Star)), len(stars),
-                            w.ctypes.data_as(C.POINTER(C.c_float)), first_pixel, n_pixels, stride,
-                            out.ctypes.data_as(C.POINTER(C.c_double)), C.byref(att), nthreads or os.cpu_count())
+    keep, p = _icdf_ptr(scene, icdf)
+    rc = lib().orc_render_pixels(C.byref(scene), stars.ctypes.data_as(C.POINTER(abi.Star)), len(stars),
+                                 w.ctypes.data_as(C.POINTER(C.c_float)), first_pixel, n_pixels, stride, p,
+                                 out.ctypes.data_as(C.POINTER(C.c_double)), C.byref(att), nthreads or os.cpu_count())
+    assert rc == 0
+    del keep
     return out, att.value
 
 

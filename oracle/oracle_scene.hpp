@@ -472,6 +472,71 @@ inline void ray_spectrum(const mgk_scene& s, const StarIndex* stars, const Hit<T
     }
 }
 
+// Sampled spectral mode (MGK_SPECTRAL_SAMPLED, the reference's stochastic
+// sensor): the ray's wavelength from the inverse CDF table icdf (256 entries)
+// with u = rng(seed, sample, pixel, 2) as device_sensor_utilities.cuh:25-33
+// draws it, throughput 1/pdf = 255 (t[k+1] - t[k]); the boosted blackbody of
+// every emitter there (planck above, independent of the library's a / (exp - 1)
+// form); sampled irradiance = radiance * throughput * sensor gain
+// (device_color_utilities.cuh:22-29); spread over the bins by the
+// differences of the Gaussian CDF at the bin edges
+// (kernel_redistribute_radiance.cu:55-92, internal_math.h:2019-2024).
+// spec (n_bins values) receives the per-bin irradiance.
+template <class T>
+inline void sampled_spectrum(const mgk_scene& s, const StarIndex* stars, const Hit<T>& h, uint64_t ray_id,
+                             const float* icdf, T* spec) {
+    const uint32_t nb = s.n_bins;
+    for (uint32_t k = 0; k < nb; ++k) spec[k] = T(0);
+    const uint32_t pixel = uint32_t(ray_id / s.spp), sample = uint32_t(ray_id % s.spp);
+    const float x = rng_unit(s.seed, sample, pixel, 2) * float(MGK_CMF_ICDF_ENTRIES - 1);
+    const uint32_t k0 = uint32_t(std::fmin(x, float(MGK_CMF_ICDF_ENTRIES) - 2.0f));
+    const float f = x - float(k0);
+    const float t0 = icdf[k0], t1 = icdf[k0 + 1];
+    const T lam = T((t0 * (1.0f - f)) + (t1 * f));
+    const T tput = T(float(MGK_CMF_ICDF_ENTRIES - 1) * (t1 - t0));
+    T z = h.z;
+    T z2 = z * z;
+    T z5 = z2 * z2 * z;
+    auto clamp = [](T v) { return (std::isnan(v) || std::isinf(v) || v < T(0)) ? T(0) : v; };
+    T rad = T(0);
+    if (h.cls == MGK_RAY_DISK) {
+        T temp = T(s.disk_T_in) * T(std::pow(double(h.r_hit / T(s.disk_r_in)), -0.75));
+        rad = clamp(planck<T>(z * lam, temp) * z5);
+    } else if (h.cls == MGK_RAY_ESCAPED && stars && stars->n) {
+        double th = std::acos(std::max(-1.0, std::min(1.0, double(h.dir[1]))));
+        double radius = s.star_radius_rad;
+        long lo = long((th - radius) / stars->band) - 1, hi = long((th + radius) / stars->band) + 1;
+        std::vector<uint32_t> hits;
+        T inv_r2 = T(1) / (T(radius) * T(radius));
+        for (long b = std::max(0L, lo); b <= std::min(long(stars->bands.size()) - 1, hi); ++b)
+            for (uint32_t i : stars->bands[size_t(b)]) hits.push_back(i);
+        std::sort(hits.begin(), hits.end());
+        for (uint32_t i : hits) {
+            const mgk_star& st = stars->stars[i];
+            T dx = h.dir[0] - T(st.dir[0]), dy = h.dir[1] - T(st.dir[1]), dz = h.dir[2] - T(st.dir[2]);
+            T q = mad<Fuse::Fma>(dz, dz, mad<Fuse::Fma>(dy, dy, dx * dx)) * inv_r2;
+            if (q >= T(1)) continue;
+            T kern = (T(1) - q) * (T(1) - q);
+            rad += clamp(T(st.amplitude) * kern * planck<T>(z * lam, T(st.temperature)) * z5);
+        }
+    }
+    const double W = s.width, H = s.height;
+    const double inv_b = s.sensor_diag_mm / std::sqrt(W * W + H * H);
+    const double area_m2 = (W * inv_b) * (H * inv_b) / 1e6;
+    const T gain = T((area_m2 / (W * H)) * s.iso * 2.0 * M_PI / ((360.0 * s.fps) / s.shutter_angle_deg));
+    const T irr = (rad * tput) * gain;
+    if (!(irr > T(0))) return;
+    const T lo = T(s.lambda_min_nm), dl = T((s.lambda_max_nm - s.lambda_min_nm) / s.n_bins);
+    const T inv_s2 = T(1.0 / (s.redistribution_sigma_nm * std::sqrt(2.0)));
+    T phi0 = T(0.5) * (T(1) + std::erf((lo - lam) * inv_s2));
+    for (uint32_t k = 0; k < nb; ++k) {
+        const T e1 = lo + T(k + 1) * dl;
+        const T phi1 = T(0.5) * (T(1) + std::erf((e1 - lam) * inv_s2));
+        spec[k] = irr * (phi1 - phi0);
+        phi0 = phi1;
+    }
+}
+
 // XYZ of a spectrum with per-bin weights w[3*k + c].
 template <class T> inline void spectrum_xyz(uint32_t nb, const T* spec, const float* w, T xyz[3]) {
     T X = 0, Y = 0, Z = 0;

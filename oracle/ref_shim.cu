@@ -46,6 +46,14 @@ extern "C" __attribute__((visibility("default"))) int ref_cmf_weights(unsigned n
     return 0;
 }
 
+// The reference's inverse CDF table of the CIE 1931 colour-matching
+// functions (compute_tabulated_cmf_inverse_cdf, floor 0.05 as
+// color_pipeline.cuh:36 calls it): MAGIK_N_CMF_INVERSE_CDF_BIN wavelengths.
+extern "C" __attribute__((visibility("default"))) int ref_cmf_inverse_cdf(float lmin, float lmax, float* out) {
+    magik::compute_tabulated_cmf_inverse_cdf(out, 0.05f, lmin, lmax, magik::fetch_cmf_info(MAGIK_CMF_CIE_1931));
+    return MAGIK_N_CMF_INVERSE_CDF_BIN;
+}
+
 namespace {
 
 void ref_parallel_for(uint64_t n, int nthreads, const std::function<void(uint64_t)>& fn) {

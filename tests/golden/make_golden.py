@@ -12,6 +12,10 @@ Writes
   ref_cmf_weights.npz  the reference's per-bin CIE 1931 XYZ weights
                        (compute_normalized_isi_cmf_weights) for the bin
                        layouts the workloads use
+  ref_cmf_icdf.npz     the reference's CIE inverse CDF table of its
+                       stochastic spectral mode
+                       (compute_tabulated_cmf_inverse_cdf) for the same
+                       wavelength ranges
 """
 import ctypes as C
 import math
@@ -87,7 +91,9 @@ def main():
     w = {f"w{n}_{int(lo)}_{int(hi)}": O.ref_cmf_weights(n, lo, hi)
          for n, lo, hi in [(16, 380.0, 780.0), (32, 380.0, 780.0), (24, 360.0, 830.0)]}
     np.savez_compressed(os.path.join(HERE, "ref_cmf_weights.npz"), **w)
-    print("wrote", N_CASES, "traces and", len(w), "weight tables")
+    icdf = {f"icdf_{int(lo)}_{int(hi)}": O.ref_cmf_inverse_cdf(lo, hi) for lo, hi in [(380.0, 780.0), (360.0, 830.0)]}
+    np.savez_compressed(os.path.join(HERE, "ref_cmf_icdf.npz"), **icdf)
+    print("wrote", N_CASES, "traces,", len(w), "weight tables and", len(icdf), "inverse CDF tables")
 
 
 if __name__ == "__main__":

@@ -142,6 +142,35 @@ def test_render_film_matches_oracle(ctx, precision):
     assert (ref[:, 1] > 0).mean() > 0.2
 
 
+@pytest.mark.parametrize("precision", [abi.PRECISION_MIXED, abi.PRECISION_F64])
+def test_render_sampled_spectral_mode_matches_oracle(ctx, precision):
+    """The reference's stochastic sensor (MGK_SPECTRAL_SAMPLED): one CIE
+    inverse-CDF wavelength per ray, Gaussian redistribution over the bins."""
+    import torch
+    s = small_scene(precision=precision, star_radius_rad=0.02, spectral_mode=abi.SPECTRAL_SAMPLED, n_bins=24)
+    stars = _stars(20000)
+    w = M.xyz_weights(s.n_bins)
+    icdf = M.cmf_inverse_cdf(s.lambda_min_nm, s.lambda_max_nm)
+    npix = s.width * s.height
+    film = torch.empty(npix * 3, dtype=torch.float32, device="cuda")
+    spec = torch.empty(npix * s.n_bins, dtype=torch.float32, device="cuda")
+    d_stars = torch.from_numpy(stars.view(np.uint8)).cuda()
+    d_w = torch.from_numpy(w.ravel()).cuda()
+    ctx.render(s, d_stars, film, d_weights=d_w, d_film_spectral=spec)
+    got = film.cpu().numpy().reshape(npix, 3).astype(np.float64)
+    ref, _ = O.render_pixels(s, stars, w, 0, npix, icdf=icdf)
+    assert np.isfinite(got).all() and (got >= 0).all()
+    assert _film_rel_err(got, ref).max() <= 1e-4
+    sp = spec.cpu().numpy().reshape(npix, s.n_bins).astype(np.float64)
+    assert _film_rel_err(sp @ w.astype(np.float64), got).max() <= 1e-4
+    assert (ref[:, 1] > 0).mean() > 0.2
+    # the per-ray path as well
+    n = s.width * s.height * s.spp
+    xyz = ctx.shade_rays(s, stars, w, 0, n).astype(np.float64)
+    rec = O.trace_rays(s, 0, n)
+    assert _film_rel_err(xyz, O.shade_rays(s, stars, w, rec, icdf=icdf)).max() <= 1e-4
+
+
 def test_shade_rays_matches_oracle(ctx):
     s = small_scene(star_radius_rad=0.02)
     stars = _stars(20000)

@@ -226,3 +226,63 @@ def test_disk_emitter_is_normalised():
     # redshift factor g = nu_obs / nu_em of a thin disk seen at 75 degrees lies in (0, ~1.6)
     assert (r["z"][disk] > 0).all() and (r["z"][disk] < 2).all()
     assert np.all((r["r_hit"][disk] >= s.disk_r_in) & (r["r_hit"][disk] <= s.disk_r_out))
+
+
+def test_sampled_spectral_mode_oracle_splat():
+    """The oracle's sampled spectral mode against a numpy restatement: a disk
+    hit's wavelength from the inverse CDF table with u = rng(seed, sample,
+    pixel, 2), throughput 1/pdf, the boosted blackbody there, the sensor gain,
+    and the Gaussian spread over the bins, which with unit X weights sums to
+    irradiance * (Phi(lambda_max) - Phi(lambda_min))."""
+    s = M.scene_defaults(width=8, height=4, spp=2, precision=abi.PRECISION_F64,
+                         spectral_mode=abi.SPECTRAL_SAMPLED, n_bins=24)
+    icdf = M.cmf_inverse_cdf(s.lambda_min_nm, s.lambda_max_nm)
+    n = 20
+    rec = np.zeros(n, dtype=M.RESULT_DTYPE)
+    rec["cls"] = abi.RAY_DISK
+    rng = np.random.default_rng(5)
+    rec["z"] = rng.uniform(0.5, 1.4, n)
+    rec["r_hit"] = rng.uniform(s.disk_r_in, s.disk_r_out, n)
+    w = np.zeros((s.n_bins, 3), dtype=np.float32)
+    w[:, 0] = 1.0
+    first = 3
+    got = O.shade_rays(s, np.zeros(0, dtype=M.STAR_DTYPE), w, rec, first_ray=first, icdf=icdf)
+    h, c, kb = 6.62607015e-34, 299792458.0, 1.380649e-23
+    W, H = s.width, s.height
+    inv_b = s.sensor_diag_mm / math.sqrt(W * W + H * H)
+    gain = (W * inv_b) * (H * inv_b) / 1e6 / (W * H) * s.iso * 2 * math.pi / (360 * s.fps / s.shutter_angle_deg)
+    for i in range(n):
+        ray = first + i
+        u = np.float32(_jitter_dim(s, ray // s.spp, ray % s.spp, 2))
+        x = np.float32(u * np.float32(255))
+        k = int(min(x, np.float32(254)))
+        f = np.float32(x - np.float32(k))
+        lam = float(np.float32(icdf[k] * (np.float32(1) - f)) + np.float32(icdf[k + 1] * f))
+        tput = float(np.float32(255) * (icdf[k + 1] - icdf[k]))
+        z, r = rec["z"][i], rec["r_hit"][i]
+        T = s.disk_T_in * (r / s.disk_r_in) ** -0.75
+        wl = z * lam * 1e-9
+        rad = 2 * h * c * c / wl ** 5 / math.expm1(h * c / (wl * kb * T)) * z ** 5
+        irr = rad * tput * gain
+        sig = s.redistribution_sigma_nm * math.sqrt(2)
+        phi = lambda e: 0.5 * (1 + math.erf((e - lam) / sig))
+        expect = irr * (phi(s.lambda_max_nm) - phi(s.lambda_min_nm))
+        assert got[i, 0] == pytest.approx(expect, rel=1e-9)
+        assert got[i, 1] == 0 and got[i, 2] == 0
+
+
+def _jitter_dim(s, pixel, sample, dim):
+    """rng_unit(seed, sample, pixel, dim) of the library, restated."""
+    def h32(x):
+        x &= 0xFFFFFFFF
+        x ^= x >> 17; x = (x * 0xED5AD4BB) & 0xFFFFFFFF
+        x ^= x >> 11; x = (x * 0xAC4C1B51) & 0xFFFFFFFF
+        x ^= x >> 15; x = (x * 0x31848BAB) & 0xFFFFFFFF
+        x ^= x >> 14
+        return x
+    v = h32((s.seed & 0xFFFFFFFF) ^ 0x9E3779B9)
+    v = h32(v ^ (s.seed >> 32))
+    v = h32(v ^ sample)
+    v = h32(v ^ pixel)
+    v = h32(v ^ ((dim * 0x85EBCA6B + 1) & 0xFFFFFFFF))
+    return (v >> 8) / 16777216.0

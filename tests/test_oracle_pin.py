@@ -115,3 +115,22 @@ def test_oracle_render_matches_reference_step_render(metric):
     b, _ = O.ref_render_pixels(s, stars, w, 0, n, nthreads=4)
     assert np.mean(np.all(a == b, axis=1)) >= 0.98
     assert np.abs(a - b).sum() <= 1e-5 * np.abs(a).sum()
+
+
+def test_reference_inverse_cdf_golden():
+    """The sampled spectral mode's CIE inverse CDF table against the
+    reference's own (compute_tabulated_cmf_inverse_cdf on its tabulated CIE
+    1931 data): the library builds it the same way from the analytic fit."""
+    import magik_b200 as M
+    g = np.load(os.path.join(GOLD, "ref_cmf_icdf.npz"))
+    for key in g.files:
+        lo, hi = map(float, key.split("_")[1:])
+        ref = g[key]
+        ours = M.cmf_inverse_cdf(lo, hi)
+        assert ours.shape == ref.shape == (256,)
+        assert ours[0] == lo and ours[-1] == hi
+        assert np.all(np.diff(ours) >= 0)
+        d = np.abs(ours.astype(np.float64) - ref)
+        # 0.12 nm on average; the last entries, where the CMFs vanish and the
+        # inverse CDF is steep, differ by up to 3 nm
+        assert d.mean() < 0.25 and d.max() < 4.0, key
