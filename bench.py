@@ -328,6 +328,50 @@ def run_stress(args, ctx, d_stars, d_w, peak):
                          "frac": flop / (st.integrate_ms * 1e-3) / peak}}
 
 
+def run_display(args, ctx):
+    """The colour resolve after the film (mgk_display) over 16.8 M seeded XYZ
+    pixels (403 MB moved per launch, above the 126 MB L2): the reference's
+    default settings (linear Rec.709 scene, white balance 5600 K, the GT7 tone
+    mapper in Jzazbz, Rec.709 display), which spend ~36 float transcendentals
+    per pixel and are compute-bound, and the same resolve without a view
+    transform to sRGB, which is HBM-bound (24 bytes per pixel)."""
+    import torch
+    import magik_b200 as M
+    n = 1 << 24
+    dev = f"cuda:{ctx.device}"
+    g = torch.Generator(device=dev)
+    g.manual_seed(0xD15)
+    xyz = torch.rand(n * 3, generator=g, device=dev) * 4.0
+    rgb = torch.empty_like(xyz)
+    peak = measured_peaks().get("hbm_gbs")
+
+    def timed(pipe, reps=20):
+        for _ in range(3):
+            ctx.display(pipe, xyz, rgb)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            ctx.display(pipe, xyz, rgb)
+        e1.record()
+        e1.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    out = {}
+    for key, ds, what in (("gt7", M.display_defaults(),
+                           "GT7 (Jzazbz) view transform, Rec.709 scene and display"),
+                          ("none_srgb", M.display_defaults(view_transform="NONE", display_colorspace="SRGB"),
+                           "no view transform, Rec.709 scene, sRGB display")):
+        ms = timed(M.display_prepare(ds))
+        gbs = 24.0 * n / (ms * 1e-3) / 1e9
+        out[key] = {"workload": f"{what}, 16,777,216 XYZ pixels", "value": n / (ms * 1e-3), "unit": "pixels/s",
+                    "ms_per_launch": ms,
+                    "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s",
+                                 "frac": gbs / peak if peak else None,
+                                 "peak_source": "MEASURED_PEAKS.json hbm_gbs, of measured"}}
+    return out
+
+
 def run_gpu(args, rank, world, local_rank):
     import torch
     import magik_b200 as M
@@ -444,6 +488,8 @@ def run_gpu(args, rank, world, local_rank):
     }
     if world == 1 and not args.no_stress:
         out["refill_stress"] = run_stress(args, ctx, d_stars, d_w, peak)
+    if world == 1:
+        out["display"] = run_display(args, ctx)
     if world == 1 and not args.no_surrogate:
         # runs after the timed region; its own timings are inside "surrogate"
         out["surrogate"] = run_surrogate(args, ctx, s, d_stars, d_w, ms, max(1, min(args.steps, 3)))

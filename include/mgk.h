@@ -260,6 +260,97 @@ MGK_API mgk_result mgk_render(mgk_context* ctx, const mgk_scene* s, const mgk_st
 MGK_API mgk_result mgk_render_host(mgk_context* ctx, const mgk_scene* s, const mgk_star* h_stars, uint32_t n_stars,
                                    const float* h_xyz_w, float* h_film_xyz, mgk_render_stats* stats, void* stream);
 
+/* ------------------------------------------------------------ display */
+/* The colour resolve after the XYZ film: white balance and the scene
+ * colourspace, a view transform, the display colourspace and its transfer
+ * function (color_pipeline.cuh:21-48, device_color_utilities.cuh:56-70,
+ * view_transform.cuh, colorspaces.cuh).  The enumerations keep the
+ * reference's values (magik.h:328-367). */
+#define MGK_SCENE_COLORSPACE_CIE_XYZ 0
+#define MGK_SCENE_COLORSPACE_CIE_RGB 1
+#define MGK_SCENE_COLORSPACE_LINEAR_REC709 2
+#define MGK_SCENE_COLORSPACE_LINEAR_REC2020 3
+#define MGK_SCENE_COLORSPACE_ACES_CG 4
+#define MGK_SCENE_COLORSPACE_ADOBE_RGB_1998 5
+#define MGK_DISPLAY_COLORSPACE_SRGB 0
+#define MGK_DISPLAY_COLORSPACE_REC709 1
+#define MGK_DISPLAY_COLORSPACE_REC2100_PQ 2
+#define MGK_DISPLAY_COLORSPACE_REC2100_HLG 3
+#define MGK_DISPLAY_COLORSPACE_DCI_P3_THEATRICAL_WHITE_POINT 4
+#define MGK_DISPLAY_COLORSPACE_DISPLAY_P3 5
+#define MGK_DISPLAY_COLORSPACE_ADOBE_RGB 6
+#define MGK_VIEW_TRANSFORM_NONE 0
+#define MGK_VIEW_TRANSFORM_REINHARD_SIMPLE 1
+#define MGK_VIEW_TRANSFORM_REINHARD_EXTENDED 2
+#define MGK_VIEW_TRANSFORM_GRAN_TURISMO_7 3
+#define MGK_VIEW_TRANSFORM_AGX 4
+#define MGK_VIEW_TRANSFORM_KHRONOS_PBR_NEUTRAL 5
+#define MGK_GT7_MODE_ICTCP 0
+#define MGK_GT7_MODE_JZAZBZ 1
+#define MGK_AGX_LOOK_NONE 0
+#define MGK_AGX_LOOK_GOLDEN 1
+#define MGK_AGX_LOOK_PUNCHY 2
+
+/* The colour settings of the resolve (color_settings.h:9-35; defaults from
+ * mgk_display_defaults are the reference's). */
+typedef struct mgk_display_settings {
+    int32_t scene_colorspace;    /* MGK_SCENE_COLORSPACE_* (LINEAR_REC709) */
+    int32_t view_transform;      /* MGK_VIEW_TRANSFORM_* (GRAN_TURISMO_7) */
+    int32_t display_colorspace;  /* MGK_DISPLAY_COLORSPACE_* (REC709) */
+    int32_t gt7_mode;            /* MGK_GT7_MODE_* (JZAZBZ) */
+    int32_t agx_look;            /* MGK_AGX_LOOK_* (GOLDEN) */
+    int32_t reserved;
+    double white_point_K;        /* white balance: blackbody temperature (5600) */
+    double tint;                 /* offset normal to the Planckian locus in CIE 1960 uv (0) */
+    double reinhard_white_luminance;   /* 4 */
+    double khronos_start_compression;  /* 0.8 */
+    double khronos_desaturation;       /* 0.15 */
+    double gt7_sdr_paper_white;        /* 250 cd/m^2 */
+    double gt7_reference_luminance;    /* 100 cd/m^2 */
+    double gt7_jzazbz_exponent_scale;  /* 1.7 */
+} mgk_display_settings;
+
+/* Everything the display kernel needs, prepared on the host from the
+ * settings (mgk_display_prepare) or filled by the caller.  Matrices are
+ * row-major 3 x 3; the colour of a pixel goes
+ *   XYZ -> xyz_to_scene -> view transform -> scene_to_display -> transfer function.
+ * The view transforms work in Rec.709 (Khronos PBR neutral) or Rec.2020
+ * (GT7, AgX) linear light: vt_to_working / vt_from_working. */
+typedef struct mgk_display_pipeline {
+    int32_t view_transform, display_colorspace, gt7_mode, agx_look;
+    float xyz_to_scene[9];      /* white-balanced XYZ -> scene colourspace */
+    float scene_to_display[9];  /* scene colourspace -> display colourspace, with its chromatic adaptation */
+    float vt_to_working[9];
+    float vt_from_working[9];
+    float agx_inset[9];
+    float agx_outset[9];
+    float luminance_weights[3]; /* scene colourspace -> Y (Reinhard extended) */
+    float reinhard_white_luminance;
+    float khronos_start_compression, khronos_desaturation;
+    /* GT7 tone curve (view_transform.cuh:115-462) */
+    float gt7_reference_luminance, gt7_jzazbz_exponent_scale;
+    float gt7_peak_intensity, gt7_alpha, gt7_mid_point, gt7_linear_section, gt7_toe_strength;
+    float gt7_kA, gt7_kB, gt7_kC;
+    float gt7_sdr_correction, gt7_fb_luminance_target, gt7_fb_luminance_target_ucs;
+    float gt7_blend_ratio, gt7_fade_start, gt7_fade_end;
+    float reserved[3];
+} mgk_display_pipeline;
+
+MGK_API void mgk_display_defaults(mgk_display_settings* ds);
+
+/* Host: the pipeline of the settings, as color_pipeline_descriptor_t::create
+ * and the view transforms' make_params build it (the white point integrates
+ * the blackbody against the analytic colour-matching functions at the 471
+ * wavelengths of the reference's CIE table). */
+MGK_API mgk_result mgk_display_prepare(const mgk_display_settings* ds, mgk_display_pipeline* out);
+
+/* Device: n_pixels XYZ triples (d_xyz, e.g. an mgk_render film) -> display
+ * RGB triples (d_rgb, float32).  d_xyz and d_rgb may be the same buffer.
+ * Stream-ordered.  Replaces kernel_splat_to_renderbuffer's colour part
+ * (kernel_splat_to_renderbuffer.cu:37-57). */
+MGK_API mgk_result mgk_display(mgk_context* ctx, const mgk_display_pipeline* p, const float* d_xyz, uint64_t n_pixels,
+                               float* d_rgb, void* stream);
+
 /* Traces camera rays [first_ray, first_ray + n_rays) of the scene and writes
  * one mgk_ray_result per ray to d_out (device pointer). */
 MGK_API mgk_result mgk_trace_rays(mgk_context* ctx, const mgk_scene* s, uint64_t first_ray, uint32_t n_rays,

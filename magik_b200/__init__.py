@@ -32,7 +32,7 @@ EXPORTS = [
     "mgk_context_create", "mgk_context_destroy", "mgk_last_error", "mgk_scene_defaults", "mgk_isco_radius",
     "mgk_xyz_weights", "mgk_star_catalog", "mgk_scene_constants", "mgk_render", "mgk_render_host",
     "mgk_trace_rays", "mgk_shade_rays", "magik_trace_geodesic", "mgk_trace_geodesic_batch", "mgk_fp32_peak",
-    "mgk_check_rounding", "mgk_cmf_inverse_cdf",
+    "mgk_check_rounding", "mgk_cmf_inverse_cdf", "mgk_display_defaults", "mgk_display_prepare", "mgk_display",
     "mgk_trace_rays_static", "mgk_train_defaults", "mgk_surrogate_param_count", "mgk_surrogate_create",
     "mgk_surrogate_destroy", "mgk_surrogate_get_params", "mgk_surrogate_set_params", "mgk_make_samples",
     "mgk_surrogate_forward", "mgk_surrogate_forward_tiled", "mgk_surrogate_status", "mgk_surrogate_gradient", "mgk_surrogate_train", "mgk_render_surrogate",
@@ -77,6 +77,10 @@ def lib():
         L.mgk_fp32_peak.argtypes = [vp, P(C.c_double)]
         L.mgk_check_rounding.argtypes = [vp, P(C.c_uint64)]
         L.mgk_cmf_inverse_cdf.argtypes = [C.c_double, C.c_double, P(C.c_float)]
+        L.mgk_display_defaults.argtypes = [P(abi.DisplaySettings)]
+        L.mgk_display_defaults.restype = None
+        L.mgk_display_prepare.argtypes = [P(abi.DisplaySettings), P(abi.DisplayPipeline)]
+        L.mgk_display.argtypes = [vp, P(abi.DisplayPipeline), vp, C.c_uint64, vp, vp]
         L.mgk_trace_rays_static.argtypes = [P(Scene), C.c_uint64, C.c_uint32, vp, vp]
         L.mgk_train_defaults.argtypes = [P(abi.TrainConfig)]
         L.mgk_train_defaults.restype = None
@@ -138,6 +142,28 @@ def cmf_inverse_cdf(lambda_min_nm=380.0, lambda_max_nm=780.0):
     return np.frombuffer(out, dtype=np.float32).copy()
 
 
+def display_defaults(**overrides):
+    """mgk_display_defaults (the reference's colour settings) with overrides;
+    enum fields accept the names of abi.SCENE_CS / DISPLAY_CS / VIEW_TRANSFORM /
+    GT7_MODE / AGX_LOOK."""
+    d = abi.DisplaySettings()
+    lib().mgk_display_defaults(C.byref(d))
+    names = dict(scene_colorspace=abi.SCENE_CS, display_colorspace=abi.DISPLAY_CS, view_transform=abi.VIEW_TRANSFORM,
+                 gt7_mode=abi.GT7_MODE, agx_look=abi.AGX_LOOK)
+    for k, v in overrides.items():
+        if not hasattr(d, k):
+            raise AttributeError(k)
+        setattr(d, k, names[k][v] if isinstance(v, str) else v)
+    return d
+
+
+def display_prepare(settings):
+    """mgk_display_prepare: the display pipeline of the settings."""
+    p = abi.DisplayPipeline()
+    _check(lib().mgk_display_prepare(C.byref(settings), C.byref(p)), "mgk_display_prepare")
+    return p
+
+
 def star_catalog(seed, n):
     out = np.zeros(n, dtype=STAR_DTYPE)
     _check(lib().mgk_star_catalog(seed, n, out.ctypes.data_as(C.c_void_p)), "mgk_star_catalog")
@@ -195,6 +221,12 @@ class Context:
         out = (C.c_uint64 * 2)()
         _check(lib().mgk_check_rounding(self.handle, out), "mgk_check_rounding", self.handle)
         return int(out[0]), int(out[1])
+
+    def display(self, pipeline, d_xyz, d_rgb, stream=None):
+        """mgk_display: d_xyz (float32 CUDA tensor of n*3) -> d_rgb (same shape)."""
+        n = d_xyz.numel() // 3
+        _check(lib().mgk_display(self.handle, C.byref(pipeline), d_xyz.data_ptr(), n, d_rgb.data_ptr(),
+                                 _stream_ptr(stream)), "mgk_display", self.handle)
 
     # -- device-buffer entry points (torch CUDA tensors)
     def render(self, scene, d_stars, d_film_xyz, d_weights=None, d_film_spectral=None, want_stats=True,

@@ -51,6 +51,41 @@ class Scene(C.Structure):
         return "Scene(" + ", ".join(f"{n}={getattr(self, n)!r}" for n, _ in self._fields_) + ")"
 
 
+SCENE_CS = dict(CIE_XYZ=0, CIE_RGB=1, LINEAR_REC709=2, LINEAR_REC2020=3, ACES_CG=4, ADOBE_RGB_1998=5)
+DISPLAY_CS = dict(SRGB=0, REC709=1, REC2100_PQ=2, REC2100_HLG=3, DCI_P3_THEATRICAL_WHITE_POINT=4, DISPLAY_P3=5,
+                  ADOBE_RGB=6)
+VIEW_TRANSFORM = dict(NONE=0, REINHARD_SIMPLE=1, REINHARD_EXTENDED=2, GRAN_TURISMO_7=3, AGX=4, KHRONOS_PBR_NEUTRAL=5)
+GT7_MODE = dict(ICTCP=0, JZAZBZ=1)
+AGX_LOOK = dict(NONE=0, GOLDEN=1, PUNCHY=2)
+
+
+class DisplaySettings(C.Structure):
+    _fields_ = [("scene_colorspace", C.c_int32), ("view_transform", C.c_int32), ("display_colorspace", C.c_int32),
+                ("gt7_mode", C.c_int32), ("agx_look", C.c_int32), ("reserved", C.c_int32),
+                ("white_point_K", C.c_double), ("tint", C.c_double), ("reinhard_white_luminance", C.c_double),
+                ("khronos_start_compression", C.c_double), ("khronos_desaturation", C.c_double),
+                ("gt7_sdr_paper_white", C.c_double), ("gt7_reference_luminance", C.c_double),
+                ("gt7_jzazbz_exponent_scale", C.c_double)]
+
+
+class DisplayPipeline(C.Structure):
+    _fields_ = [("view_transform", C.c_int32), ("display_colorspace", C.c_int32), ("gt7_mode", C.c_int32),
+                ("agx_look", C.c_int32),
+                ("xyz_to_scene", C.c_float * 9), ("scene_to_display", C.c_float * 9),
+                ("vt_to_working", C.c_float * 9), ("vt_from_working", C.c_float * 9),
+                ("agx_inset", C.c_float * 9), ("agx_outset", C.c_float * 9),
+                ("luminance_weights", C.c_float * 3), ("reinhard_white_luminance", C.c_float),
+                ("khronos_start_compression", C.c_float), ("khronos_desaturation", C.c_float),
+                ("gt7_reference_luminance", C.c_float), ("gt7_jzazbz_exponent_scale", C.c_float),
+                ("gt7_peak_intensity", C.c_float), ("gt7_alpha", C.c_float), ("gt7_mid_point", C.c_float),
+                ("gt7_linear_section", C.c_float), ("gt7_toe_strength", C.c_float),
+                ("gt7_kA", C.c_float), ("gt7_kB", C.c_float), ("gt7_kC", C.c_float),
+                ("gt7_sdr_correction", C.c_float), ("gt7_fb_luminance_target", C.c_float),
+                ("gt7_fb_luminance_target_ucs", C.c_float),
+                ("gt7_blend_ratio", C.c_float), ("gt7_fade_start", C.c_float), ("gt7_fade_end", C.c_float),
+                ("reserved", C.c_float * 3)]
+
+
 class Star(C.Structure):
     _fields_ = [("dir", C.c_float * 3), ("amplitude", C.c_float), ("temperature", C.c_float),
                 ("reserved", C.c_float * 3)]

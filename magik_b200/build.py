@@ -16,7 +16,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmgk.so")
-SOURCES = ["kernels.cu", "api.cu", "static_scratch.cu", "mlp.cu", "mlp_tc.cu", "surrogate.cu"]
+SOURCES = ["kernels.cu", "api.cu", "static_scratch.cu", "mlp.cu", "mlp_tc.cu", "surrogate.cu", "display.cu"]
 HEADERS = ["dev_physics.cuh", "dev_pair.cuh", "dev_scene.cuh", "internal.h", os.path.join("..", "..", "include", "mgk.h")]
 
 NVCC_FLAGS = [

@@ -19,6 +19,8 @@ struct mgk_context {
     int sm_count = 0;
     void* arena = nullptr;
     size_t arena_bytes = 0;
+    void* stage = nullptr;            // device staging of mgk_render_host's inputs and film
+    size_t stage_bytes = 0;
     std::vector<cudaEvent_t> events;  // pairs around the integrator launches
     std::string last_error = "no error";
 };
@@ -121,6 +123,8 @@ uint32_t grid_n(double radius) {
 }  // namespace
 
 namespace mgk {
+void cmf_1931_values(double nm, double out[3]) { cmf_1931(nm, out); }
+
 // CIE inverse CDF table of the sampled spectral mode, as the reference builds
 // it (host_color_utilities.cuh:188-233) in float: the colour-matching
 // functions resampled at 471 points over [lmin, lmax] (the reference's 1 nm
@@ -479,6 +483,7 @@ MGK_API mgk_result mgk_context_destroy(mgk_context* ctx) {
     cudaSetDevice(ctx->device);
     for (auto e : ctx->events) cudaEventDestroy(e);
     if (ctx->arena) cudaFree(ctx->arena);
+    if (ctx->stage) cudaFree(ctx->stage);
     delete ctx;
     return MGK_SUCCESS;
 }
@@ -632,6 +637,26 @@ MGK_API mgk_result mgk_check_rounding(mgk_context* ctx, uint64_t mismatches[2]) 
     return MGK_SUCCESS;
 }
 
+MGK_API void mgk_display_defaults(mgk_display_settings* ds) {
+    if (ds) display_defaults(ds);
+}
+
+MGK_API mgk_result mgk_display_prepare(const mgk_display_settings* ds, mgk_display_pipeline* out) {
+    if (!ds || !out) return MGK_ERROR_INVALID_POINTER;
+    return display_prepare(*ds, out);
+}
+
+MGK_API mgk_result mgk_display(mgk_context* ctx, const mgk_display_pipeline* p, const float* d_xyz, uint64_t n_pixels,
+                               float* d_rgb, void* stream) {
+    if (!ctx || !p || ((!d_xyz || !d_rgb) && n_pixels)) return MGK_ERROR_INVALID_POINTER;
+    if (p->view_transform < 0 || p->view_transform > MGK_VIEW_TRANSFORM_KHRONOS_PBR_NEUTRAL ||
+        p->display_colorspace < 0 || p->display_colorspace > MGK_DISPLAY_COLORSPACE_ADOBE_RGB)
+        return MGK_UNKNOWN_ENUM_TYPE;
+    MGK_CUDA(ctx, cudaSetDevice(ctx->device));
+    MGK_CUDA(ctx, launch_display(*p, d_xyz, n_pixels, d_rgb, static_cast<cudaStream_t>(stream)));
+    return MGK_SUCCESS;
+}
+
 MGK_API mgk_result mgk_render(mgk_context* ctx, const mgk_scene* s, const mgk_star* d_stars, uint32_t n_stars,
                               const float* d_xyz_w, float* d_film_xyz, float* d_film_spectral,
                               mgk_render_stats* stats, void* stream) {
@@ -651,21 +676,27 @@ MGK_API mgk_result mgk_render_host(mgk_context* ctx, const mgk_scene* s, const m
     const size_t film_bytes = size_t(s->width) * s->height * 12;
     const size_t star_bytes = size_t(n_stars) * sizeof(mgk_star);
     const size_t w_bytes = h_xyz_w ? size_t(s->n_bins) * 12 : 0;
-    // host-side inputs and outputs travel through one device staging block
-    void* stage = nullptr;
-    size_t stage_bytes = align_up(film_bytes, 256) + align_up(star_bytes, 256) + align_up(w_bytes, 256) + 256;
-    MGK_CUDA(ctx, cudaMallocAsync(&stage, stage_bytes, st));
-    char* p = static_cast<char*>(stage);
+    // host-side inputs and outputs travel through one device staging block,
+    // kept by the context and grown when a frame needs more (a block freed
+    // back to the stream-ordered pool would be unmapped at the next
+    // synchronisation and mapped again by every call)
+    const size_t stage_bytes = align_up(film_bytes, 256) + align_up(star_bytes, 256) + align_up(w_bytes, 256) + 256;
+    if (ctx->stage_bytes < stage_bytes) {
+        MGK_CUDA(ctx, cudaStreamSynchronize(st));
+        if (ctx->stage) cudaFree(ctx->stage);
+        ctx->stage = nullptr;
+        ctx->stage_bytes = 0;
+        MGK_CUDA(ctx, cudaMalloc(&ctx->stage, stage_bytes));
+        ctx->stage_bytes = stage_bytes;
+    }
+    char* p = static_cast<char*>(ctx->stage);
     float* d_film = reinterpret_cast<float*>(p);
     mgk_star* d_stars = reinterpret_cast<mgk_star*>(p + align_up(film_bytes, 256));
     float* d_w = h_xyz_w ? reinterpret_cast<float*>(p + align_up(film_bytes, 256) + align_up(star_bytes, 256)) : nullptr;
     cudaError_t e = cudaSuccess;
     if (star_bytes) e = cudaMemcpyAsync(d_stars, h_stars, star_bytes, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess && w_bytes) e = cudaMemcpyAsync(d_w, h_xyz_w, w_bytes, cudaMemcpyHostToDevice, st);
-    if (e != cudaSuccess) {
-        cudaFreeAsync(stage, st);
-        return cuda_fail(ctx, e, "cudaMemcpyAsync(H2D)");
-    }
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMemcpyAsync(H2D)");
     uint64_t n = uint64_t(s->width) * s->height * s->spp;
     rc = run(ctx, *s, d_stars, n_stars, d_w, 0, n, nullptr, nullptr, d_film, nullptr, stats, st, true);
     if (rc == MGK_SUCCESS) {
@@ -673,7 +704,6 @@ MGK_API mgk_result mgk_render_host(mgk_context* ctx, const mgk_scene* s, const m
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) rc = cuda_fail(ctx, e, "cudaMemcpyAsync(D2H)");
     }
-    cudaFreeAsync(stage, st);
     return rc;
 }
 

@@ -62,6 +62,9 @@ def ref():
         R.ref_trace_geodesic.restype = C.c_int
         R.ref_cmf_weights.argtypes = [C.c_uint, C.c_float, C.c_float, C.POINTER(C.c_float)]
         R.ref_cmf_inverse_cdf.argtypes = [C.c_float, C.c_float, C.POINTER(C.c_float)]
+        R.ref_display_pipeline.argtypes = [C.POINTER(abi.DisplaySettings), C.POINTER(abi.DisplayPipeline)]
+        R.ref_display_pixels.argtypes = [C.POINTER(abi.DisplaySettings), C.POINTER(C.c_float), C.c_uint32,
+                                         C.POINTER(C.c_float)]
         R.ref_render_pixels.argtypes = [C.POINTER(abi.Scene), C.POINTER(abi.Star), C.c_uint32, C.POINTER(C.c_float),
                                         C.c_uint64, C.c_uint32, C.c_uint64, C.POINTER(C.c_double), C.c_int]
         R.ref_render_pixels.restype = C.c_int
@@ -105,6 +108,23 @@ def ref_cmf_inverse_cdf(lmin, lmax):
     out = (C.c_float * abi.CMF_ICDF_ENTRIES)()
     assert ref().ref_cmf_inverse_cdf(lmin, lmax, out) == abi.CMF_ICDF_ENTRIES
     return np.frombuffer(out, dtype=np.float32).copy()
+
+
+def ref_display_pipeline(settings):
+    """The reference's colour pipeline for the settings, in the library's
+    mgk_display_pipeline layout."""
+    p = abi.DisplayPipeline()
+    assert ref().ref_display_pipeline(C.byref(settings), C.byref(p)) == 0
+    return p
+
+
+def ref_display_pixels(settings, xyz):
+    """Display RGB of XYZ triples (float32 [n, 3]) by the reference's own colour code."""
+    x = np.ascontiguousarray(xyz, dtype=np.float32).reshape(-1, 3)
+    out = np.zeros_like(x)
+    assert ref().ref_display_pixels(C.byref(settings), x.ctypes.data_as(C.POINTER(C.c_float)), len(x),
+                                    out.ctypes.data_as(C.POINTER(C.c_float))) == 0
+    return out
 
 
 def scene_constants(scene):

@@ -14,6 +14,7 @@
 
 #include "host_trace_geodesic.h"
 #include "host_color_utilities.cuh"
+#include "color_pipeline.cuh"
 #include "cuda_host_utilities.h"
 #include "magik.h"
 #include "kernel_advance_geodesic.cuh"
@@ -52,6 +53,126 @@ extern "C" __attribute__((visibility("default"))) int ref_cmf_weights(unsigned n
 extern "C" __attribute__((visibility("default"))) int ref_cmf_inverse_cdf(float lmin, float lmax, float* out) {
     magik::compute_tabulated_cmf_inverse_cdf(out, 0.05f, lmin, lmax, magik::fetch_cmf_info(MAGIK_CMF_CIE_1931));
     return MAGIK_N_CMF_INVERSE_CDF_BIN;
+}
+
+// The reference's colour resolve (color_pipeline.cuh:21-48 with the view
+// transforms' make_params / apply and the display colourspaces' encode,
+// composed as scene_to_display_referred_color composes them,
+// device_color_utilities.cuh:56-70), for the library's display tests.
+namespace {
+magik::color_settings_t ref_color_settings(const mgk_display_settings* ds) {
+    magik::color_settings_t cs;
+    cs.scene_colorspace_type = e_magik_scene_colorspace_types(ds->scene_colorspace);
+    cs.view_transform_type = e_magik_view_transform_types(ds->view_transform);
+    cs.display_colorspace_type = e_magik_display_colorspace_types(ds->display_colorspace);
+    cs.vt_gt7_mode = e_magik_gran_turismo_7_mode_types(ds->gt7_mode);
+    cs.vt_agx_look = e_magik_agx_look_types(ds->agx_look);
+    cs.white_point = float(ds->white_point_K);
+    cs.tint = float(ds->tint);
+    cs.vt_reinhard_extended_white_luminance = float(ds->reinhard_white_luminance);
+    cs.vt_khronos_pbr_neutral_start_compression = float(ds->khronos_start_compression);
+    cs.vt_khronos_pbr_neutral_desaturation = float(ds->khronos_desaturation);
+    cs.vt_gt7_sdr_paper_white = float(ds->gt7_sdr_paper_white);
+    cs.vt_gt7_reference_luminance = float(ds->gt7_reference_luminance);
+    cs.vt_gt7_jzazbz_exponent_scale_factor = float(ds->gt7_jzazbz_exponent_scale);
+    return cs;
+}
+void put_m(float* d, const magik::mat3f& m) {
+    const float v[9] = {m.m11, m.m12, m.m13, m.m21, m.m22, m.m23, m.m31, m.m32, m.m33};
+    for (int i = 0; i < 9; ++i) d[i] = v[i];
+}
+magik::mat3f ref_xyz_to_scene(const magik::color_settings_t& cs) {
+    auto sc = magik::fetch_scene_colorspace(cs.scene_colorspace_type);
+    auto cmf = magik::fetch_cmf_info(cs.cmf_type);
+    magik::vec3f src = magik::compute_white_point_xyz(cs.white_point, cs.tint, cmf);
+    magik::vec3f dst = magik::cie_xy_to_cie_XYZ(sc.white_point_cie_xy);
+    return sc.cie_XYZ_to_colorspace * magik::chromatic_adaptation(src, dst);
+}
+template <e_magik_view_transform_types V>
+magik::vec3f ref_display_one(const magik::color_settings_t& cs, const magik::color_pipeline_descriptor_t& d,
+                             const typename magik::generic_view_transform_t<V>::params_t& vp, magik::vec3f scene) {
+    magik::vec3f c = magik::generic_view_transform_t<V>::apply(scene, vp);
+    c = d.scene_to_display_referred * c;
+    magik::vec3f out{0, 0, 0};
+    magik::dispatch_list(magik::supported_display_colorspaces{}, d.display_colorspace_type, [&](auto tag) {
+        constexpr auto D = decltype(tag)::value;
+        out = magik::generic_display_colorspace_t<D>::encode(c);
+    });
+    return out;
+}
+}  // namespace
+
+extern "C" __attribute__((visibility("default"))) int ref_display_pipeline(const mgk_display_settings* ds,
+                                                                           mgk_display_pipeline* out) {
+    using namespace magik;
+    color_settings_t cs = ref_color_settings(ds);
+    color_pipeline_descriptor_t d = color_pipeline_descriptor_t::create(cs);
+    *out = mgk_display_pipeline{};
+    out->view_transform = ds->view_transform;
+    out->display_colorspace = ds->display_colorspace;
+    out->gt7_mode = ds->gt7_mode;
+    out->agx_look = ds->agx_look;
+    put_m(out->xyz_to_scene, ref_xyz_to_scene(cs));
+    put_m(out->scene_to_display, d.scene_to_display_referred);
+    auto re = generic_view_transform_t<MAGIK_VIEW_TRANSFORM_REINHARD_EXTENDED>::make_params(cs);
+    out->luminance_weights[0] = re.luminance_weights.x;
+    out->luminance_weights[1] = re.luminance_weights.y;
+    out->luminance_weights[2] = re.luminance_weights.z;
+    out->reinhard_white_luminance = re.white_luminance;
+    auto kh = generic_view_transform_t<MAGIK_VIEW_TRANSFORM_KHRONOS_PBR_NEUTRAL>::make_params(cs);
+    out->khronos_start_compression = kh.start_compression;
+    out->khronos_desaturation = kh.desaturation;
+    auto gt = generic_view_transform_t<MAGIK_VIEW_TRANSFORM_GRAN_TURISMO_7>::make_params(cs);
+    auto ag = generic_view_transform_t<MAGIK_VIEW_TRANSFORM_AGX>::make_params(cs);
+    if (ds->view_transform == MAGIK_VIEW_TRANSFORM_KHRONOS_PBR_NEUTRAL) {
+        put_m(out->vt_to_working, kh.to_linear_rec_709);
+        put_m(out->vt_from_working, kh.to_scene_colorspace);
+    } else {
+        put_m(out->vt_to_working, gt.to_linear_rec_2020);
+        put_m(out->vt_from_working, gt.to_scene_colorspace);
+    }
+    put_m(out->agx_inset, ag.agx_inset_matrix);
+    put_m(out->agx_outset, ag.agx_outset_matrix);
+    out->gt7_reference_luminance = gt.reference_luminance;
+    out->gt7_jzazbz_exponent_scale = gt.jzazbz_exponent_scale_factor;
+    out->gt7_peak_intensity = gt.peak_intensity_;
+    out->gt7_alpha = gt.alpha_;
+    out->gt7_mid_point = gt.mid_point_;
+    out->gt7_linear_section = gt.linear_section_;
+    out->gt7_toe_strength = gt.toe_strength_;
+    out->gt7_kA = gt.kA_;
+    out->gt7_kB = gt.kB_;
+    out->gt7_kC = gt.kC_;
+    out->gt7_sdr_correction = gt.sdr_correction_factor_;
+    out->gt7_fb_luminance_target = gt.framebuffer_luminance_target_;
+    out->gt7_fb_luminance_target_ucs = gt.framebuffer_luminance_target_ucs;
+    out->gt7_blend_ratio = gt.blend_ratio_;
+    out->gt7_fade_start = gt.fade_start_;
+    out->gt7_fade_end = gt.fade_end_;
+    return 0;
+}
+
+// Display RGB of n XYZ triples with the reference's own functions: the
+// white-balanced XYZ -> scene matrix, the view transform, the scene ->
+// display matrix and the display's transfer function.
+extern "C" __attribute__((visibility("default"))) int ref_display_pixels(const mgk_display_settings* ds,
+                                                                         const float* xyz, uint32_t n, float* out) {
+    using namespace magik;
+    color_settings_t cs = ref_color_settings(ds);
+    color_pipeline_descriptor_t d = color_pipeline_descriptor_t::create(cs);
+    const mat3f m = ref_xyz_to_scene(cs);
+    bool ok = dispatch_list(supported_view_transforms{}, cs.view_transform_type, [&](auto tag) {
+        constexpr auto V = decltype(tag)::value;
+        auto vp = generic_view_transform_t<V>::make_params(cs);
+        for (uint32_t i = 0; i < n; ++i) {
+            vec3f scene = m * vec3f{xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]};
+            vec3f o = ref_display_one<V>(cs, d, vp, scene);
+            out[3 * i] = o.x;
+            out[3 * i + 1] = o.y;
+            out[3 * i + 2] = o.z;
+        }
+    });
+    return ok ? 0 : 1;
 }
 
 namespace {

@@ -12,6 +12,11 @@ Writes
   ref_cmf_weights.npz  the reference's per-bin CIE 1931 XYZ weights
                        (compute_normalized_isi_cmf_weights) for the bin
                        layouts the workloads use
+  ref_display.npz      the reference's colour resolve: for combinations of
+                       scene colourspace, view transform, display colourspace,
+                       GT7 mode and AgX look, its pipeline (in the library's
+                       mgk_display_pipeline layout) and the display RGB of a
+                       seeded set of XYZ colours by its own functions
   ref_cmf_icdf.npz     the reference's CIE inverse CDF table of its
                        stochastic spectral mode
                        (compute_tabulated_cmf_inverse_cdf) for the same
@@ -93,7 +98,54 @@ def main():
     np.savez_compressed(os.path.join(HERE, "ref_cmf_weights.npz"), **w)
     icdf = {f"icdf_{int(lo)}_{int(hi)}": O.ref_cmf_inverse_cdf(lo, hi) for lo, hi in [(380.0, 780.0), (360.0, 830.0)]}
     np.savez_compressed(os.path.join(HERE, "ref_cmf_icdf.npz"), **icdf)
-    print("wrote", N_CASES, "traces,", len(w), "weight tables and", len(icdf), "inverse CDF tables")
+    combos, settings, pipes, outs = display_golden()
+    xyz = display_inputs()
+    np.savez_compressed(os.path.join(HERE, "ref_display.npz"), combos=np.array(combos), settings=settings,
+                        pipelines=pipes, xyz=xyz, rgb=outs)
+    print("wrote", N_CASES, "traces,", len(w), "weight tables,", len(icdf), "inverse CDF tables and",
+          len(combos), "display pipelines")
+
+
+def display_inputs(n=384, seed=77):
+    """XYZ colours for the display fixtures: luminance log-uniform over
+    1e-4 .. 30 at chromaticities inside the spectral locus (x, y drawn in the
+    triangle of the Rec.2020 primaries), and a few exact blacks."""
+    rng = np.random.default_rng(seed)
+    prim = np.array([[0.708, 0.292], [0.170, 0.797], [0.131, 0.046]])
+    w = rng.dirichlet([1.0, 1.0, 1.0], n)
+    xy = w @ prim
+    Y = 10 ** rng.uniform(-4, math.log10(30.0), n)
+    X = xy[:, 0] / xy[:, 1] * Y
+    Z = (1 - xy[:, 0] - xy[:, 1]) / xy[:, 1] * Y
+    xyz = np.stack([X, Y, Z], 1).astype(np.float32)
+    xyz[:4] = 0.0
+    return xyz
+
+
+def display_golden():
+    import ctypes as C
+    import magik_b200 as M
+    combos = []
+    for vt in abi.VIEW_TRANSFORM:
+        for dc in abi.DISPLAY_CS:
+            combos.append(("LINEAR_REC709", vt, dc, "JZAZBZ", "GOLDEN"))
+    for sc in abi.SCENE_CS:
+        if sc != "LINEAR_REC709":
+            combos.append((sc, "GRAN_TURISMO_7", "REC709", "JZAZBZ", "GOLDEN"))
+            combos.append((sc, "AGX", "SRGB", "JZAZBZ", "GOLDEN"))
+    for dc in ("REC709", "REC2100_PQ"):
+        combos.append(("LINEAR_REC709", "GRAN_TURISMO_7", dc, "ICTCP", "GOLDEN"))
+    for look in ("NONE", "PUNCHY"):
+        combos.append(("LINEAR_REC709", "AGX", "SRGB", "JZAZBZ", look))
+    xyz = display_inputs()
+    settings, pipes, outs = [], [], []
+    for sc, vt, dc, mode, look in combos:
+        ds = M.display_defaults(scene_colorspace=sc, view_transform=vt, display_colorspace=dc, gt7_mode=mode,
+                                agx_look=look)
+        settings.append(np.frombuffer(bytes(ds), dtype=np.uint8))
+        pipes.append(np.frombuffer(bytes(O.ref_display_pipeline(ds)), dtype=np.uint8))
+        outs.append(O.ref_display_pixels(ds, xyz))
+    return ["/".join(c) for c in combos], np.stack(settings), np.stack(pipes), np.stack(outs)
 
 
 if __name__ == "__main__":

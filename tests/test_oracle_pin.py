@@ -134,3 +134,35 @@ def test_reference_inverse_cdf_golden():
         # 0.12 nm on average; the last entries, where the CMFs vanish and the
         # inverse CDF is steep, differ by up to 3 nm
         assert d.mean() < 0.25 and d.max() < 4.0, key
+
+
+def _display_golden():
+    g = np.load(os.path.join(GOLD, "ref_display.npz"))
+    from magik_b200 import abi
+    settings = [abi.DisplaySettings.from_buffer_copy(s.tobytes()) for s in g["settings"]]
+    pipes = [abi.DisplayPipeline.from_buffer_copy(p.tobytes()) for p in g["pipelines"]]
+    return g, settings, pipes
+
+
+def test_display_pipeline_against_reference_golden():
+    """mgk_display_prepare against the reference's colour pipeline
+    (color_pipeline_descriptor_t::create and the view transforms'
+    make_params, from oracle/_ref): every matrix and parameter is the same
+    float, except the white-balance matrix, whose white point integrates the
+    blackbody against the analytic colour-matching functions instead of the
+    tabulated CIE 1931 ones (1.2e-3 at 5600 K)."""
+    import ctypes as C
+    import magik_b200 as M
+    from magik_b200 import abi
+    g, settings, pipes = _display_golden()
+    names = []
+    for f, t in abi.DisplayPipeline._fields_[4:]:
+        names += [f] * (C.sizeof(t) // 4)
+    names = np.array(names)
+    other = names != "xyz_to_scene"
+    for combo, ds, ref in zip(g["combos"], settings, pipes):
+        ours = np.frombuffer(bytes(M.display_prepare(ds)), dtype=np.float32)[4:]
+        theirs = np.frombuffer(bytes(ref), dtype=np.float32)[4:]
+        assert np.array_equal(ours[other], theirs[other]), combo
+        rel = np.abs(ours[~other] - theirs[~other]).max() / np.abs(theirs[~other]).max()
+        assert rel < 2e-3, (combo, rel)
