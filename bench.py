@@ -321,7 +321,7 @@ def run_stress(args, ctx, d_stars, d_w, peak):
             "attempts_per_ray": st.attempts / rays, "max_steps": s.max_steps,
             "fp64_attempt_fraction": st.wide_attempts / max(1, st.attempts),
             "rays_resumed_in_tail": st.resumed, "step_limit_rays": int(st.class_count[4]),
-            "classes": dict(zip(["alive", "disk", "escaped", "horizon", "step_limit"],
+            "classes": dict(zip(["alive", "disk", "escaped", "horizon", "step_limit", "light"],
                                 [int(c) for c in st.class_count])),
             "roofline": {"bound": "fp32", "achieved": flop / (st.integrate_ms * 1e-3) / 1e12,
                          "peak": peak / 1e12, "unit": "TFLOP/s",
@@ -479,7 +479,7 @@ def run_gpu(args, rank, world, local_rank):
         "stats": {"attempts": st_last.attempts, "steps": st_last.steps, "refine_evals": st_last.refine_evals,
                   "wide_attempts": st_last.wide_attempts, "crossings": st_last.crossings,
                   "resumed": st_last.resumed,
-                  "classes": dict(zip(["alive", "disk", "escaped", "horizon", "step_limit"],
+                  "classes": dict(zip(["alive", "disk", "escaped", "horizon", "step_limit", "light"],
                                       [int(c) for c in st_last.class_count])),
                   "attempts_per_ray": st_last.attempts / rays},
         "clocks": clk,

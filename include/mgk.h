@@ -84,7 +84,9 @@ typedef int32_t mgk_result;
 #define MGK_RAY_DISK 1
 #define MGK_RAY_ESCAPED 2
 #define MGK_RAY_HORIZON 3
-#define MGK_RAY_STEP_LIMIT 4
+#define MGK_RAY_STEP_LIMIT 4  /* also: more reflections than room_reflection_limit */
+#define MGK_RAY_LIGHT 5       /* the room's light (MGK_SCENE room traceables) */
+#define MGK_RAY_CLASSES 6
 
 /* ------------------------------------------------------------ scene */
 /* Everything one render or trace needs.  Geometric units, M = 1.
@@ -127,6 +129,16 @@ typedef struct mgk_scene {
     double fps;                     /* 24 */
     double shutter_angle_deg;       /* 180 */
     double redistribution_sigma_nm; /* Gaussian spread of a sample over the bins, 10 */
+    /* The reference's box-and-light test scene (stage.h:19-22, matter_examples.cuh:33-77),
+     * in units of M (the reference's metres divided by its length scale 0.5 m):
+     * a diffuse box the camera sits in (walls normal to x reflect like mirrors,
+     * the others are Lambertian, matter_examples.cuh:38-51) and a white-LED light
+     * box (matter_examples.cuh:64-76).  room_on = 0 disables both. */
+    uint32_t room_on;
+    uint32_t room_reflection_limit;  /* reflections before MGK_RAY_STEP_LIMIT (render_settings.h:17, 10) */
+    double room_min[3], room_max[3];    /* (-40, -20, -40), (40, 20, 40) */
+    double light_min[3], light_max[3];  /* (-20, 19, -20), (20, 21, 20) */
+    double light_scale;                 /* white-LED spectral radiance scale, 7e5 */
 } mgk_scene;
 
 #define MGK_MAX_BINS 64
@@ -166,7 +178,7 @@ typedef struct mgk_ray_result {
     uint32_t attempts;  /* RKF45 attempts */
     uint32_t wide_attempts; /* attempts run in FP64 */
     uint32_t refine_evals;  /* RK sub-steps spent locating the crossing */
-    uint32_t reserved;
+    uint32_t bounces;       /* reflections off the room's walls */
 } mgk_ray_result;
 
 /* Counters of one render. */
@@ -176,7 +188,7 @@ typedef struct mgk_render_stats {
     uint64_t steps;
     uint64_t wide_attempts;
     uint64_t refine_evals;
-    uint64_t class_count[5];  /* indexed by MGK_RAY_* */
+    uint64_t class_count[MGK_RAY_CLASSES];  /* indexed by MGK_RAY_* */
     double integrate_ms;      /* device time of the integrator launches */
     double total_ms;          /* device time of the whole render */
     uint64_t crossings;       /* steps handed to the crossing kernel */

@@ -21,7 +21,7 @@ _lib = None
 
 RESULT_DTYPE = np.dtype([("x", "<f8", 4), ("p", "<f8", 4), ("z", "<f8"), ("r_hit", "<f8"), ("dir", "<f8", 3),
                          ("cls", "<u4"), ("steps", "<u4"), ("attempts", "<u4"), ("wide_attempts", "<u4"),
-                         ("refine_evals", "<u4"), ("reserved", "<u4")])
+                         ("refine_evals", "<u4"), ("bounces", "<u4")])
 STAR_DTYPE = np.dtype([("dir", "<f4", 3), ("amplitude", "<f4"), ("temperature", "<f4"), ("reserved", "<f4", 3)])
 STEP_DTYPE = np.dtype([("four_position", "<f4", 4), ("four_momentum", "<f4", 4), ("moment_derivative", "<f4", 4),
                        ("four_vector_contraction", "<f4"), ("affine_parameter", "<f4"),

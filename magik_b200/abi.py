@@ -16,8 +16,9 @@ ERROR_DEVICE_STATUS = 10004
 
 METRIC_MINKOWSKI, METRIC_SCHWARZSCHILD, METRIC_KERR = 0, 1, 2
 PRECISION_REF32, PRECISION_MIXED, PRECISION_F64 = 0, 1, 2
-RAY_ALIVE, RAY_DISK, RAY_ESCAPED, RAY_HORIZON, RAY_STEP_LIMIT = 0, 1, 2, 3, 4
-CLASS_NAMES = {0: "alive", 1: "disk", 2: "escaped", 3: "horizon", 4: "step_limit"}
+RAY_ALIVE, RAY_DISK, RAY_ESCAPED, RAY_HORIZON, RAY_STEP_LIMIT, RAY_LIGHT = 0, 1, 2, 3, 4, 5
+RAY_CLASSES = 6
+CLASS_NAMES = {0: "alive", 1: "disk", 2: "escaped", 3: "horizon", 4: "step_limit", 5: "light"}
 MASSIVE, MASSLESS = 0, 1
 MAX_BINS = 64
 SPECTRAL_BINS, SPECTRAL_SAMPLED = 0, 1
@@ -40,6 +41,9 @@ class Scene(C.Structure):
         ("star_radius_rad", C.c_double),
         ("iso", C.c_double), ("fps", C.c_double), ("shutter_angle_deg", C.c_double),
         ("redistribution_sigma_nm", C.c_double),
+        ("room_on", C.c_uint32), ("room_reflection_limit", C.c_uint32),
+        ("room_min", C.c_double * 3), ("room_max", C.c_double * 3),
+        ("light_min", C.c_double * 3), ("light_max", C.c_double * 3), ("light_scale", C.c_double),
     ]
 
     def copy(self):
@@ -95,13 +99,13 @@ class RayResult(C.Structure):
     _fields_ = [("x", C.c_double * 4), ("p", C.c_double * 4), ("z", C.c_double), ("r_hit", C.c_double),
                 ("dir", C.c_double * 3), ("cls", C.c_uint32), ("steps", C.c_uint32),
                 ("attempts", C.c_uint32), ("wide_attempts", C.c_uint32),
-                ("refine_evals", C.c_uint32), ("reserved", C.c_uint32)]
+                ("refine_evals", C.c_uint32), ("bounces", C.c_uint32)]
 
 
 class RenderStats(C.Structure):
     _fields_ = [("rays", C.c_uint64), ("attempts", C.c_uint64), ("steps", C.c_uint64),
                 ("wide_attempts", C.c_uint64), ("refine_evals", C.c_uint64),
-                ("class_count", C.c_uint64 * 5),
+                ("class_count", C.c_uint64 * 6),
                 ("integrate_ms", C.c_double), ("total_ms", C.c_double), ("crossings", C.c_uint64),
                 ("resumed", C.c_uint64), ("fallback_rays", C.c_uint64), ("surrogate_ms", C.c_double)]
 
@@ -152,7 +156,7 @@ class TraceContainer(C.Structure):
                 ("steps", C.POINTER(TraceStep))]
 
 
-assert C.sizeof(Scene) == 216, C.sizeof(Scene)
+assert C.sizeof(Scene) == 328, C.sizeof(Scene)
 assert C.sizeof(Star) == 32
 assert C.sizeof(RayResult) == 128
 assert C.sizeof(TraceStep) == 60

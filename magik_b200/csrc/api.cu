@@ -83,6 +83,25 @@ mgk_result validate(const mgk_scene* s) {
     if (s->spectral_mode == MGK_SPECTRAL_SAMPLED &&
         !(s->iso > 0.0 && s->fps > 0.0 && s->shutter_angle_deg > 0.0 && s->redistribution_sigma_nm > 0.0))
         return MGK_ERROR_INVALID_ARGUMENT;
+    if (s->room_on) {
+        // both boxes proper, the camera inside the room and outside the light
+        // (rays start inside the room: kernel_intersect.cu:81-100 takes the
+        // room's far face)
+        for (int a = 0; a < 3; ++a)
+            if (!(s->room_min[a] < s->room_max[a] && s->light_min[a] < s->light_max[a]) ||
+                !std::isfinite(s->room_min[a]) || !std::isfinite(s->room_max[a]) ||
+                !std::isfinite(s->light_min[a]) || !std::isfinite(s->light_max[a]))
+                return MGK_ERROR_INVALID_ARGUMENT;
+        if (!(s->light_scale >= 0.0 && std::isfinite(s->light_scale)) || s->room_reflection_limit > 1024u)
+            return MGK_ERROR_INVALID_ARGUMENT;
+        const double q[3] = {0.0, s->cam_r * std::cos(s->cam_incl_rad), s->cam_r * std::sin(s->cam_incl_rad)};
+        bool in_room = true, in_light = true;
+        for (int a = 0; a < 3; ++a) {
+            in_room = in_room && q[a] > s->room_min[a] && q[a] < s->room_max[a];
+            in_light = in_light && q[a] >= s->light_min[a] && q[a] <= s->light_max[a];
+        }
+        if (!in_room || in_light) return MGK_ERROR_INVALID_ARGUMENT;
+    }
     // MIXED evaluates the RHS with one float reciprocal of ~r^9, finite below
     // r ~ 1.9e4; a ray moves at most about h_max past the escape radius
     if (s->precision == MGK_PRECISION_MIXED && s->escape_radius + 2.0 * s->h_max > 1.5e4)
@@ -416,7 +435,7 @@ mgk_result run(mgk_context* ctx, const mgk_scene& s, const mgk_star* d_stars, ui
             stats->refine_evals += k.refine_evals;
             stats->crossings += k.refine_count + k.escape_count;
             stats->resumed += k.resume_count;
-            for (int i = 0; i < 5; ++i) stats->class_count[i] += k.class_count[i];
+            for (int i = 0; i < MGK_RAY_CLASSES; ++i) stats->class_count[i] += k.class_count[i];
             status |= k.status;
         }
         float ms = 0.f;
@@ -532,6 +551,17 @@ MGK_API void mgk_scene_defaults(mgk_scene* s) {
     s->fps = 24.0;
     s->shutter_angle_deg = 180.0;
     s->redistribution_sigma_nm = 10.0;
+    // the reference's stage (stage.h:19-22, optical_system_settings.h:33) in
+    // units of M = G M / c^2 = 0.5 m (relativity_settings.h:21-24)
+    s->room_on = 0;
+    s->room_reflection_limit = 10;
+    const double lo[3] = {-40.0, -20.0, -40.0}, hi[3] = {40.0, 20.0, 40.0};
+    const double llo[3] = {-20.0, 19.0, -20.0}, lhi[3] = {20.0, 21.0, 20.0};
+    for (int a = 0; a < 3; ++a) {
+        s->room_min[a] = lo[a]; s->room_max[a] = hi[a];
+        s->light_min[a] = llo[a]; s->light_max[a] = lhi[a];
+    }
+    s->light_scale = 7.0e5;
 }
 
 MGK_API mgk_result mgk_xyz_weights(uint32_t n_bins, double lmin, double lmax, float* w_out) {
@@ -918,6 +948,7 @@ MGK_API mgk_result mgk_make_samples(mgk_context* ctx, const mgk_scene* base, uin
     mgk_result rc = validate(&s0);
     if (rc != MGK_SUCCESS) return rc;
     if (n_spin_buckets > 1024 || (n_spin_buckets && s0.escape_radius < 100.0)) return MGK_ERROR_INVALID_ARGUMENT;
+    if (s0.room_on) return MGK_ERROR_INVALID_ARGUMENT;  // the surrogate learns sky directions only
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     MGK_CUDA(ctx, cudaSetDevice(ctx->device));
     const uint32_t chunk = std::min(n, kSampleChunk);
@@ -994,6 +1025,7 @@ MGK_API mgk_result mgk_render_surrogate(mgk_context* ctx, mgk_surrogate* net, co
     mgk_result rc = validate(&s);
     if (rc != MGK_SUCCESS) return rc;
     if (s.precision == MGK_PRECISION_REF32) return MGK_ERROR_INVALID_ARGUMENT;
+    if (s.room_on) return MGK_ERROR_INVALID_ARGUMENT;  // the surrogate learns sky directions only
     if (n_stars && !d_stars) return MGK_ERROR_INVALID_POINTER;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     MGK_CUDA(ctx, cudaSetDevice(ctx->device));
@@ -1094,7 +1126,7 @@ MGK_API mgk_result mgk_render_surrogate(mgk_context* ctx, mgk_surrogate* net, co
             stats->crossings += k.refine_count + k.escape_count;
             stats->resumed += k.resume_count;
             stats->fallback_rays += k.fallback_count;
-            for (int i = 0; i < 5; ++i) stats->class_count[i] += k.class_count[i];
+            for (int i = 0; i < MGK_RAY_CLASSES; ++i) stats->class_count[i] += k.class_count[i];
         }
         float ms = 0.f;
         MGK_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->events[0], ctx->events[1]));

@@ -201,6 +201,12 @@ template <class T> struct DevScene {
     T sensor_gain;           // radiance * throughput -> sensor irradiance (device_color_utilities.cuh:22-29)
     T lambda_lo, dlambda;    // bin edges lambda_lo + k dlambda, nm
     T inv_sigma_sqrt2;       // 1 / (redistribution sigma * sqrt 2), 1/nm
+    // room scene (walls and light as axis-aligned boxes)
+    uint32_t room_on, room_limit;
+    T room_lo[3], room_hi[3];
+    T light_lo[3], light_hi[3];
+    T light_scale;
+    uint64_t ray_base;  // global index of the launch's ray 0 (per-ray random numbers)
 };
 
 // ------------------------------------------------------------ camera
@@ -290,24 +296,28 @@ __device__ __forceinline__ S7<T> sub_step(const S7<T>& y0, T pt, T s, const MP<T
     return y1;
 }
 
-template <Fuse F, class T> __device__ __forceinline__ T cross_g(int kind, const S7<T>& q, T R2) {
-    return kind == 0 ? q.y : mad<F>(q.z, q.z, mad<F>(q.y, q.y, q.x * q.x)) - R2;
+template <class T> MGK_HD T axis_of(const S7<T>& q, int axis) { return axis == 0 ? q.x : (axis == 1 ? q.y : q.z); }
+template <class T> MGK_HD T axis_of(const V4<T>& q, int axis) { return axis == 0 ? q.x : (axis == 1 ? q.y : q.z); }
+
+// kind 0, 1, 2: the plane x, y or z = v; kind 3: the sphere |x|^2 = v.
+template <Fuse F, class T> __device__ __forceinline__ T cross_g(int kind, const S7<T>& q, T v) {
+    return kind == 3 ? mad<F>(q.z, q.z, mad<F>(q.y, q.y, q.x * q.x)) - v : axis_of(q, kind) - v;
 }
 
-// kind 0: disk plane y = 0; kind 1: escape sphere |x| = R.
+// Disk: kind 1, v = 0; escape sphere: kind 3, v = R^2; room faces: planes.
 template <int METRIC, Fuse F, class T>
-__device__ __forceinline__ S7<T> refine(int kind, const S7<T>& y0, const S7<T>& y1, T pt, T h, T R2, const MP<T>& m,
+__device__ __forceinline__ S7<T> refine(int kind, const S7<T>& y0, const S7<T>& y1, T pt, T h, T v, const MP<T>& m,
                                         uint32_t& evals) {
-    T g0 = cross_g<F>(kind, y0, R2), g1 = cross_g<F>(kind, y1, R2);
+    T g0 = cross_g<F>(kind, y0, v), g1 = cross_g<F>(kind, y1, v);
     T s_prev = h, g_prev = g1;
     T s = h * (g0 / (g0 - g1));
     S7<T> ys = sub_step<METRIC, F, T>(y0, pt, s, m);
     ++evals;
-    T gs = cross_g<F>(kind, ys, R2);
+    T gs = cross_g<F>(kind, ys, v);
     // The escape sphere lies in the far field, where one sub-step to the chord
     // estimate already puts the direction within 1e-9 of the located one;
-    // the disk plane is met in strong field and iterates.
-    const int iters = kind == 0 ? MGK_REFINE_ITERS : 0;
+    // planes (the disk in strong field, the room's faces) iterate.
+    const int iters = kind < 3 ? MGK_REFINE_ITERS : 0;
     for (int it = 0; it < iters; ++it) {
         T den = gs - g_prev;
         if (gs == T(0) || den == T(0)) break;
@@ -319,7 +329,7 @@ __device__ __forceinline__ S7<T> refine(int kind, const S7<T>& y0, const S7<T>& 
         s = s_new;
         ys = sub_step<METRIC, F, T>(y0, pt, s, m);
         ++evals;
-        gs = cross_g<F>(kind, ys, R2);
+        gs = cross_g<F>(kind, ys, v);
         if (fabs(ds) <= T(1e-6) * h) break;
     }
     return ys;
@@ -342,6 +352,167 @@ __device__ __forceinline__ bool disk_candidate(const DevScene<T>& P, const S7<T>
     return rc >= P.disk_lo && rc <= P.disk_hi;
 }
 
+// ---------------------------------------------------------------- room
+// The reference's test scene (matter_examples.cuh:33-77, kernel_intersect.cu:
+// 81-100, traceables.cuh:17-74): the camera inside a box whose walls reflect
+// (walls normal to x like mirrors, the others Lambertian) and a light box that
+// absorbs and emits a white-LED spectrum.
+//
+// Cheap test after every step (integrator): the step ends outside the room,
+// or its chord's bounding box overlaps the light.  Conservative; the crossing
+// kernel runs the exact chord test.
+template <class T>
+__device__ __forceinline__ bool room_candidate(const DevScene<T>& P, const S7<T>& y0, const S7<T>& y1) {
+    if (!P.room_on) return false;
+    const bool inside = y1.x >= P.room_lo[0] && y1.x <= P.room_hi[0] && y1.y >= P.room_lo[1] &&
+                        y1.y <= P.room_hi[1] && y1.z >= P.room_lo[2] && y1.z <= P.room_hi[2];
+    const bool light = fmax(y0.x, y1.x) >= P.light_lo[0] && fmin(y0.x, y1.x) <= P.light_hi[0] &&
+                       fmax(y0.y, y1.y) >= P.light_lo[1] && fmin(y0.y, y1.y) <= P.light_hi[1] &&
+                       fmax(y0.z, y1.z) >= P.light_lo[2] && fmin(y0.z, y1.z) <= P.light_hi[2];
+    return !inside || light;
+}
+
+// First room event on the chord a0 -> a1 (chord parameter t in [0, 1]):
+// leaving the room through a wall (the face whose plane the chord crosses
+// first among the axes on which a1 lies outside), or entering the light
+// (slab test, traceables.cuh:17-74 with the chord as the segment).  axis < 0:
+// none.  side 0 / 1: the face at the box's minimum / maximum on that axis.
+template <class T> struct RoomEvent {
+    T t;
+    int axis, side;
+    bool light;
+};
+template <class T>
+MGK_HD RoomEvent<T> room_chord(const T* lo, const T* hi, const T* llo, const T* lhi, const T* a0, const T* a1) {
+    RoomEvent<T> ev{T(2), -1, 0, false};
+    for (int a = 0; a < 3; ++a) {
+        const bool above = a1[a] > hi[a], below = a1[a] < lo[a];
+        if (!(above || below)) continue;
+        const T b = above ? hi[a] : lo[a];
+        T t = (b - a0[a]) / (a1[a] - a0[a]);
+        if (!(t >= T(0))) t = T(0);  // started outside on this axis
+        if (t < ev.t) { ev.t = t; ev.axis = a; ev.side = above ? 1 : 0; }
+    }
+    T tn = T(0), tf = T(1);
+    int an = -1, sn = 0;
+    bool miss = false;
+    // the chord's bounding box must overlap the light (the integrator's pre-test)
+    for (int a = 0; a < 3; ++a)
+        if (!(fmax(a0[a], a1[a]) >= llo[a] && fmin(a0[a], a1[a]) <= lhi[a])) miss = true;
+    for (int a = 0; a < 3 && !miss; ++a) {
+        const T d = a1[a] - a0[a];
+        if (d == T(0)) {
+            if (a0[a] < llo[a] || a0[a] > lhi[a]) miss = true;
+            continue;
+        }
+        const T t_lo = (llo[a] - a0[a]) / d, t_hi = (lhi[a] - a0[a]) / d;
+        const T t_near = d > T(0) ? t_lo : t_hi, t_far = d > T(0) ? t_hi : t_lo;
+        if (t_near > tn) { tn = t_near; an = a; sn = d > T(0) ? 0 : 1; }
+        if (t_far < tf) tf = t_far;
+    }
+    // an < 0: the chord starts inside the light (not an entry)
+    if (!miss && an >= 0 && tn <= tf && tn < ev.t) {
+        ev.t = tn; ev.axis = an; ev.side = sn; ev.light = true;
+    }
+    return ev;
+}
+
+// White-LED spectral radiance: five Gaussians s exp(-(x - o)^2 / (2 w^2))
+// with the reference's centres, widths and weights (internal_math.h:
+// 2441-2445, 2501-2509).
+template <class T> __device__ __forceinline__ T white_led(T x) {
+    const T o[5] = {T(577.0), T(451.0), T(455.0), T(528.0), T(690.0)};
+    const T w[5] = {T(50.7937003968), T(7.07106781187), T(14.1421356237), T(13.7840487521), T(44.72135955)};
+    const T s[5] = {T(157.0), T(200.0), T(50.0), T(20.0), T(10.0)};
+    T acc = T(0);
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+        const T d = x - o[i];
+        acc = acc + exp(T(-0.5) * ((d * d) / (w[i] * w[i]))) * s[i];
+    }
+    return acc;
+}
+
+// Uniform direction on the unit sphere from the ray's random numbers
+// (dimensions base .. base + 32): cos(theta) = 1 - 2 u as in
+// sample_lambertian_brdf (brdf.cuh:12-29), the azimuth's (cos, sin) from a
+// point of the unit disc found by rejection (up to 16 tries; IEEE square
+// root and division only, so host and device agree bit for bit).
+template <class T> MGK_HD void sphere_dir(uint64_t seed, uint32_t sample, uint32_t pixel, uint32_t base, T out[3]) {
+    const T cz = T(1) - T(2) * T(rng_unit(seed, sample, pixel, base));
+    const T q = T(1) - cz * cz;
+    const T sz = sqrt(q > T(0) ? q : T(0));
+    T cx = T(1), cy = T(0);
+    for (uint32_t j = 0; j < 16; ++j) {
+        const T vx = T(2) * T(rng_unit(seed, sample, pixel, base + 1u + 2u * j)) - T(1);
+        const T vy = T(2) * T(rng_unit(seed, sample, pixel, base + 2u + 2u * j)) - T(1);
+        const T r2 = vx * vx + vy * vy;
+        if (r2 <= T(1) && r2 > T(1e-12)) {
+            const T r = sqrt(r2);
+            cx = vx / r;
+            cy = vy / r;
+            break;
+        }
+    }
+    out[0] = cx * sz; out[1] = cy * sz; out[2] = cz;
+}
+
+// Reflection off a wall at the located point X with covariant momentum p
+// (apply_reflected, bxdf_utilities.cuh:53-109,139-154): the wall's observer
+// is the reference observer (zero proper velocity, matter_examples.cuh:35-38);
+// the ray's direction and the wall normal are taken to its rest frame
+// (tetrad seeds x, y, z), the normal is turned to face the ray, the
+// direction is mirrored (walls normal to x) or replaced by a cosine-weighted
+// one around the normal (Lambertian: normalised uniform sphere direction plus
+// normal), and mapped back to a null covariant momentum.  c0 becomes
+// (u . p_out) times the redshift at the wall, so that redshifts multiply
+// along the path.
+template <class T>
+__device__ __forceinline__ void reflect_wall(const DevScene<T>& P, int axis, int side, const S7<T>& X, T& pt, T& c0,
+                                             uint32_t bounce, uint64_t ray_id, S7<T>& out) {
+    const int metric = P.metric;
+    const Sym4<T> g = compute_g<T>(metric, X.x, X.y, X.z, P.m.spin, P.m.mass_sign);
+    const V4<T> u = reference_observer<T>(metric, X.x, X.y, X.z, P.m.spin, P.m.mass_sign);
+    const Tetrad<T> e = build_tetrad<T>(g, V4<T>{T(1), T(0), T(0), T(0)}, V4<T>{T(0), T(1), T(0), T(0)},
+                                        V4<T>{T(0), T(0), T(1), T(0)}, u);
+    const V4<T> p{X.px, X.py, X.pz, pt};
+    const T zr = redshift_clamp<T>(c0 / dot4(u, p));
+    T d[3] = {dot4(e.x, p), dot4(e.y, p), dot4(e.z, p)};
+    const T dl = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    d[0] = d[0] / dl; d[1] = d[1] / dl; d[2] = d[2] / dl;
+    // facing normal in the global frame points into the room; its rest-frame
+    // components are e_i^mu n_mu
+    const T ns = side ? T(-1) : T(1);
+    T n[3] = {axis_of(e.x, axis) * ns, axis_of(e.y, axis) * ns, axis_of(e.z, axis) * ns};
+    const T nl = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+    n[0] = n[0] / nl; n[1] = n[1] / nl; n[2] = n[2] / nl;
+    if (n[0] * d[0] + n[1] * d[1] + n[2] * d[2] > T(0)) { n[0] = -n[0]; n[1] = -n[1]; n[2] = -n[2]; }
+    T o[3];
+    if (axis == 0) {
+        const T k = T(2) * (d[0] * n[0] + d[1] * n[1] + d[2] * n[2]);
+        o[0] = d[0] - k * n[0]; o[1] = d[1] - k * n[1]; o[2] = d[2] - k * n[2];
+    } else {
+        const uint32_t pixel = uint32_t(ray_id / P.spp), sample = uint32_t(ray_id % P.spp);
+        T q[3];
+        sphere_dir<T>(P.seed, sample, pixel, 8u + 64u * bounce, q);
+        o[0] = q[0] + n[0]; o[1] = q[1] + n[1]; o[2] = q[2] + n[2];
+        if (!(o[0] * o[0] + o[1] * o[1] + o[2] * o[2] > T(1e-12))) { o[0] = n[0]; o[1] = n[1]; o[2] = n[2]; }
+    }
+    const T ol = sqrt(o[0] * o[0] + o[1] * o[1] + o[2] * o[2]);
+    o[0] = o[0] / ol; o[1] = o[1] / ol; o[2] = o[2] / ol;
+    const T l = sqrt(o[0] * o[0] + o[1] * o[1] + o[2] * o[2]);
+    const V4<T> pu = local_to_global<T>(e, V4<T>{o[0], o[1], o[2], l});
+    const V4<T> po = contract<T>(g, pu);
+    c0 = dot4(u, po) * zr;
+    pt = po.t;
+    // restart 1/256 inside the wall, on the face (offset_geodesic,
+    // bxdf_utilities.cuh:111-137, with a fixed offset)
+    T x[3] = {X.x, X.y, X.z};
+    for (int a = 0; a < 3; ++a) x[a] = fmin(fmax(x[a], P.room_lo[a]), P.room_hi[a]);
+    x[axis] = side ? P.room_hi[axis] - T(0.00390625) : P.room_lo[axis] + T(0.00390625);
+    out = S7<T>{x[0], x[1], x[2], X.t, po.x, po.y, po.z};
+}
+
 template <Fuse F, class T> __device__ __forceinline__ T radius2(const S7<T>& y) {
     return mad<F>(y.z, y.z, mad<F>(y.y, y.y, y.x * y.x));
 }
@@ -360,16 +531,31 @@ __device__ __forceinline__ uint32_t plain_terminal(const DevScene<T>& P, const S
     return MGK_RAY_ALIVE;
 }
 
+// Ray state that a room reflection changes.
+struct Bounce {
+    uint32_t count;  // reflections so far
+    uint64_t ray_id;  // global ray index (random numbers)
+    bool reflected;  // set by resolve: the ray continues from y_end with the new pt, c0
+};
+
 // All tests after the accepted step y0 -> y1 of length h, in this order:
-// thin disk (located crossing inside [r_in, r_out]), escape radius, horizon,
-// step cap.  y_end receives the located crossing for disk and sky hits.
+// thin disk (located crossing inside [r_in, r_out]) unless a room event comes
+// first on the chord, room walls and light, escape radius, horizon, step cap.
+// y_end receives the located crossing for disk, light and sky hits, and the
+// restart state after a reflection (pt and c0 then change too).
 template <int METRIC, Fuse F, class T>
-__device__ __forceinline__ Term<T> resolve(const DevScene<T>& P, const S7<T>& y0, const S7<T>& y1, T pt, T h, T c0,
-                                           uint32_t steps, S7<T>& y_end, uint32_t& evals) {
+__device__ __forceinline__ Term<T> resolve(const DevScene<T>& P, const S7<T>& y0, const S7<T>& y1, T& pt, T h,
+                                           T& c0, uint32_t steps, Bounce& bn, S7<T>& y_end, uint32_t& evals) {
     Term<T> o{MGK_RAY_ALIVE, T(0), T(0), T(0), T(0), T(0)};
     y_end = y1;
-    if (disk_candidate<F, T>(P, y0, y1)) {
-        S7<T> ys = refine<METRIC, F, T>(0, y0, y1, pt, h, T(0), P.m, evals);
+    bn.reflected = false;
+    RoomEvent<T> ev{T(2), -1, 0, false};
+    if (P.room_on) {
+        const T a0[3] = {y0.x, y0.y, y0.z}, a1[3] = {y1.x, y1.y, y1.z};
+        ev = room_chord<T>(P.room_lo, P.room_hi, P.light_lo, P.light_hi, a0, a1);
+    }
+    if (disk_candidate<F, T>(P, y0, y1) && !(ev.axis >= 0 && ev.t < y0.y / (y0.y - y1.y))) {
+        S7<T> ys = refine<METRIC, F, T>(1, y0, y1, pt, h, T(0), P.m, evals);
         T rh = kerr_schild_r(ys.x, ys.y, ys.z, P.kerr_a);
         if (rh >= P.disk_r_in && rh <= P.disk_r_out) {
             V4<T> u = disk_velocity<T>(ys.x, ys.z, rh, P, METRIC);
@@ -380,9 +566,33 @@ __device__ __forceinline__ Term<T> resolve(const DevScene<T>& P, const S7<T>& y0
             return o;
         }
     }
+    if (ev.axis >= 0) {
+        const T* face = ev.light ? (ev.side ? P.light_hi : P.light_lo) : (ev.side ? P.room_hi : P.room_lo);
+        const S7<T> ys = ev.t > T(0) ? refine<METRIC, F, T>(ev.axis, y0, y1, pt, h, face[ev.axis], P.m, evals) : y0;
+        y_end = ys;
+        if (ev.light) {
+            // absorbed: the light's spectrum at the redshift seen by its (static) observer
+            const V4<T> u = reference_observer<T>(P.metric, ys.x, ys.y, ys.z, P.m.spin, P.m.mass_sign);
+            o.cls = MGK_RAY_LIGHT;
+            o.z = redshift_clamp<T>(c0 / dot4(u, V4<T>{ys.px, ys.py, ys.pz, pt}));
+            return o;
+        }
+        if (bn.count >= P.room_limit) {
+            // one reflection more than the limit ends the ray
+            // (kernel_enforce_ray_limits.cu:49)
+            bn.count += 1u;
+            o.cls = MGK_RAY_STEP_LIMIT;
+            return o;
+        }
+        reflect_wall<T>(P, ev.axis, ev.side, ys, pt, c0, bn.count, bn.ray_id, y_end);
+        bn.count += 1u;
+        bn.reflected = true;
+        if (steps >= P.max_steps) o.cls = MGK_RAY_STEP_LIMIT;
+        return o;
+    }
     T r2 = radius2<F>(y1);
     if (r2 >= P.escape_r2) {
-        S7<T> ys = refine<METRIC, F, T>(1, y0, y1, pt, h, P.escape_r2, P.m, evals);
+        S7<T> ys = refine<METRIC, F, T>(3, y0, y1, pt, h, P.escape_r2, P.m, evals);
         T pn = sqrt(mad<F>(ys.pz, ys.pz, mad<F>(ys.py, ys.py, ys.px * ys.px)));
         o.cls = MGK_RAY_ESCAPED;
         o.d0 = ys.px / pn; o.d1 = ys.py / pn; o.d2 = ys.pz / pn;

@@ -15,7 +15,7 @@ struct Counters {
     unsigned long long steps;
     unsigned long long wide_attempts;
     unsigned long long refine_evals;
-    unsigned long long class_count[5];
+    unsigned long long class_count[MGK_RAY_CLASSES];
     uint32_t queue_head;    // next queue index handed to a warp
     uint32_t hit_count;     // entries in the hit queue
     uint32_t refine_count;  // disk-crossing entries (from the front of the crossing queue)
@@ -36,19 +36,21 @@ template <class T> struct alignas(16) HitEntry {
 };
 
 // Crossing-queue entry: a step whose end crossed the disk plane near the
-// disk or the escape sphere; the crossing kernel locates it.
+// disk, the escape sphere or (room scene) a wall or the light; the crossing
+// kernel locates it.
 template <class T> struct alignas(16) RefineEntry {
     T y0[7], y1[7];
     T pt, h, h_next, c0;
-    uint32_t ray, steps, attempts, wide, evals, pad[3];
+    uint32_t ray, steps, attempts, wide, evals, bounces, pad[2];
 };
 
 // Resume-queue entry: a ray that continues in the tail kernel (MIXED rays
-// inside the FP64 band, and rays whose disk candidate missed the disk).
+// inside the FP64 band, rays whose disk candidate missed the disk, rays
+// reflected off a wall of the room).
 template <class T> struct alignas(16) ResumeEntry {
     T y[7];
     T pt, h, c0;
-    uint32_t ray, steps, attempts, wide, evals, pad[3];
+    uint32_t ray, steps, attempts, wide, evals, bounces, pad[2];
 };
 
 // Views of the arena for one chunk.

@@ -5,17 +5,21 @@
 //  k_integrate  persistent RKF45 integrator: each warp refills its dead lanes
 //               from the HBM queue in chunks, every lane runs one attempt per
 //               trip, accepted steps go through the termination tests, and
-//               steps that end past a disk or escape crossing are compacted
-//               by warp ballot into the crossing queue; in MIXED mode rays
-//               entering the FP64 band are compacted into the resume queue
+//               steps that end past a disk, escape or room crossing are
+//               compacted by warp ballot into the crossing queue; in MIXED
+//               mode rays entering the FP64 band are compacted into the
+//               resume queue
 //               [kernel_advance_geodesic.cu + kernel_intersect.cu + kernel_enforce_ray_limits.cu]
-//  k_refine     locates the disk / escape crossings handed over by k_integrate
-//               on the geodesic (secant iterations over RK sub-steps)
+//  k_refine     locates the disk / escape / wall / light crossings handed over
+//               by k_integrate on the geodesic (secant iterations over RK
+//               sub-steps); reflects rays off the room's walls
+//               [kernel_bxdf.cu, bxdf_utilities.cuh:139-154]
 //  k_tail       resumed rays (MIXED rays inside the FP64 band near the horizon,
-//               rays whose disk candidate missed), run one thread per ray
-//  k_shade      one warp per hit: blackbody at the bin wavelengths (one lane per
-//               bin), star lookup, spectral film, XYZ by warp reduction
-//               [kernel_bxdf.cu + kernel_redistribute_radiance.cu]
+//               rays whose disk candidate missed, reflected rays), persistent
+//               with per-lane refill
+//  k_shade      one thread per hit: blackbody or white-LED emission at the bin
+//               wavelengths (or the sampled wavelength), star lookup, spectral
+//               film, XYZ [kernel_bxdf.cu + kernel_redistribute_radiance.cu]
 //  k_resolve    per-pixel mean over samples [kernel_splat_to_renderbuffer.cu]
 //  k_trace_geodesic  the reference-compatible single-geodesic trace
 //               [host_trace_geodesic.cu:74-117]
@@ -150,14 +154,14 @@ __device__ __forceinline__ bool in_band(const DevScene<float>& P, float x, float
 template <class T>
 __device__ __forceinline__ void write_result(mgk_ray_result* res, uint32_t ray, const S7<T>& y, T pt,
                                              const Term<T>& t, uint32_t steps, uint32_t att, uint32_t wide,
-                                             uint32_t evals) {
+                                             uint32_t evals, uint32_t bounces) {
     mgk_ray_result r;
     r.x[0] = double(y.x); r.x[1] = double(y.y); r.x[2] = double(y.z); r.x[3] = double(y.t);
     r.p[0] = double(y.px); r.p[1] = double(y.py); r.p[2] = double(y.pz); r.p[3] = double(pt);
     r.z = double(t.z); r.r_hit = double(t.r_hit);
     r.dir[0] = double(t.d0); r.dir[1] = double(t.d1); r.dir[2] = double(t.d2);
     r.cls = t.cls; r.steps = steps; r.attempts = att; r.wide_attempts = wide; r.refine_evals = evals;
-    r.reserved = 0;
+    r.bounces = bounces;
     res[ray] = r;
 }
 
@@ -207,12 +211,12 @@ __device__ __forceinline__ void push_hit(HitEntry<T>* hits, uint32_t slot, uint3
 template <class T>
 __device__ __forceinline__ void store_resume(ResumeEntry<T>* q, uint32_t slot, const S7<T>& y, T pt, T h, T c0,
                                              uint32_t ray, uint32_t steps, uint32_t att, uint32_t wide,
-                                             uint32_t evals) {
+                                             uint32_t evals, uint32_t bounces) {
     ResumeEntry<T> e;
     e.y[0] = y.x; e.y[1] = y.y; e.y[2] = y.z; e.y[3] = y.t; e.y[4] = y.px; e.y[5] = y.py; e.y[6] = y.pz;
     e.pt = pt; e.h = h; e.c0 = c0;
     e.ray = ray; e.steps = steps; e.attempts = att; e.wide = wide; e.evals = evals;
-    e.pad[0] = e.pad[1] = e.pad[2] = 0;
+    e.bounces = bounces; e.pad[0] = e.pad[1] = 0;
     q[slot] = e;
 }
 
@@ -244,7 +248,7 @@ __global__ void __launch_bounds__(kIntegrateThreads, MODE == MGK_PRECISION_F64 ?
     uint32_t cbeg = 0, cend = 0;
     bool drained = false;
     uint32_t n_att = 0, n_steps = 0;  // per lane: below 2^32 (a lane runs at most max_steps x n_max per ray)
-    uint32_t n_cls[5] = {0, 0, 0, 0, 0};
+    uint32_t n_cls[MGK_RAY_CLASSES] = {0, 0, 0, 0, 0, 0};
 
     for (;;) {
         // ---- refill dead lanes from the queue (warp-uniform control flow)
@@ -314,7 +318,7 @@ __global__ void __launch_bounds__(kIntegrateThreads, MODE == MGK_PRECISION_F64 ?
                 ++steps; ++n_steps;
                 y = y1;
                 T r2 = radius2<F>(y1);
-                disk = disk_candidate<F, T>(P, y0, y1);
+                disk = disk_candidate<F, T>(P, y0, y1) || room_candidate<T>(P, y0, y1);
                 cross = disk || r2 >= P.escape_r2;
                 if (!cross) {
                     cls = plain_terminal<METRIC, F, T>(P, y1, r2, steps);
@@ -331,7 +335,7 @@ __global__ void __launch_bounds__(kIntegrateThreads, MODE == MGK_PRECISION_F64 ?
         if (cls != MGK_RAY_ALIVE) {
             if (res) {
                 Term<T> t{cls, T(0), T(0), T(0), T(0), T(0)};
-                write_result<T>(res, ray, y, pt, t, steps, att, MODE == MGK_PRECISION_F64 ? att : 0u, 0u);
+                write_result<T>(res, ray, y, pt, t, steps, att, MODE == MGK_PRECISION_F64 ? att : 0u, 0u, 0u);
             }
             ++n_cls[cls];
         }
@@ -349,12 +353,12 @@ __global__ void __launch_bounds__(kIntegrateThreads, MODE == MGK_PRECISION_F64 ?
                 e.pt = pt; e.h = h_used; e.h_next = h; e.c0 = c0;
                 e.ray = ray; e.steps = steps; e.attempts = att;
                 e.wide = MODE == MGK_PRECISION_F64 ? att : 0u;
-                e.evals = 0; e.pad[0] = e.pad[1] = e.pad[2] = 0;
+                e.evals = 0; e.bounces = 0; e.pad[0] = e.pad[1] = 0;
                 refq[slot] = e;
             }
             if constexpr (MODE == MGK_PRECISION_MIXED) {
                 uint32_t bslot = warp_push(to_band, &cnt->resume_count, nq, &cnt->status);
-                if (bslot != ~0u) store_resume<T>(resq, bslot, y, pt, h, c0, ray, steps, att, 0u, 0u);
+                if (bslot != ~0u) store_resume<T>(resq, bslot, y, pt, h, c0, ray, steps, att, 0u, 0u, 0u);
             }
         }
         if (cls != MGK_RAY_ALIVE || cross || to_band) alive = false;
@@ -363,15 +367,15 @@ __global__ void __launch_bounds__(kIntegrateThreads, MODE == MGK_PRECISION_F64 ?
     // ---- counters: one atomic per warp and counter
     const unsigned long long w_att = warp_sum((unsigned long long)n_att);
     const unsigned long long w_steps = warp_sum((unsigned long long)n_steps);
-    unsigned long long c[5];
+    unsigned long long c[MGK_RAY_CLASSES];
 #pragma unroll
-    for (int i = 0; i < 5; ++i) c[i] = warp_sum((unsigned long long)n_cls[i]);
+    for (int i = 0; i < MGK_RAY_CLASSES; ++i) c[i] = warp_sum((unsigned long long)n_cls[i]);
     if (lane == 0) {
         atomicAdd(&cnt->attempts, w_att);
         atomicAdd(&cnt->steps, w_steps);
         if (MODE == MGK_PRECISION_F64) atomicAdd(&cnt->wide_attempts, w_att);
 #pragma unroll
-        for (int i = 1; i < 5; ++i)
+        for (int i = 1; i < MGK_RAY_CLASSES; ++i)
             if (c[i]) atomicAdd(&cnt->class_count[i], c[i]);
     }
 }
@@ -415,7 +419,7 @@ __global__ void __launch_bounds__(kIntegrateThreads, MGK_X2_MIN_BLOCKS)
     uint32_t cbeg = 0, cend = 0;
     bool drained = false;
     uint32_t n_att = 0, n_steps = 0;
-    uint32_t n_cls[5] = {0, 0, 0, 0, 0};
+    uint32_t n_cls[MGK_RAY_CLASSES] = {0, 0, 0, 0, 0, 0};
 
     for (;;) {
         // ---- refill dead slots (warp-uniform control flow)
@@ -491,7 +495,7 @@ __global__ void __launch_bounds__(kIntegrateThreads, MGK_X2_MIN_BLOCKS)
             const S7<float> a0 = slot_of<s>(y0), a1 = slot_of<s>(y1);
             set_slot<s>(y, a1);
             const float r2 = radius2<F>(a1);
-            disk[s] = disk_candidate<F, float>(P, a0, a1);
+            disk[s] = disk_candidate<F, float>(P, a0, a1) || room_candidate<float>(P, a0, a1);
             cross[s] = disk[s] || r2 >= P.escape_r2;
             if (!cross[s]) {
                 cls[s] = plain_terminal<METRIC, F, float>(P, a1, r2, steps[s]);
@@ -506,7 +510,7 @@ __global__ void __launch_bounds__(kIntegrateThreads, MGK_X2_MIN_BLOCKS)
             if (cls[s] == MGK_RAY_ALIVE) return;
             if (res) {
                 Term<float> t{cls[s], 0.f, 0.f, 0.f, 0.f, 0.f};
-                write_result<float>(res, ray[s], slot_of<s>(y), lane_of<s>(pt), t, steps[s], att[s], 0u, 0u);
+                write_result<float>(res, ray[s], slot_of<s>(y), lane_of<s>(pt), t, steps[s], att[s], 0u, 0u, 0u);
             }
             ++n_cls[cls[s]];
         };
@@ -530,13 +534,13 @@ __global__ void __launch_bounds__(kIntegrateThreads, MGK_X2_MIN_BLOCKS)
                     e.y1[4] = a1.px; e.y1[5] = a1.py; e.y1[6] = a1.pz;
                     e.pt = lane_of<s>(pt); e.h = lane_of<s>(h_used); e.h_next = lane_of<s>(h); e.c0 = lane_of<s>(c0);
                     e.ray = ray[s]; e.steps = steps[s]; e.attempts = att[s];
-                    e.wide = 0u; e.evals = 0; e.pad[0] = e.pad[1] = e.pad[2] = 0;
+                    e.wide = 0u; e.evals = 0; e.bounces = 0; e.pad[0] = e.pad[1] = 0;
                     refq[slot] = e;
                 }
                 const uint32_t bslot = warp_push(to_band[s], &cnt->resume_count, nq, &cnt->status);
                 if (bslot != ~0u)
                     store_resume<float>(resq, bslot, slot_of<s>(y), lane_of<s>(pt), lane_of<s>(h), lane_of<s>(c0),
-                                        ray[s], steps[s], att[s], 0u, 0u);
+                                        ray[s], steps[s], att[s], 0u, 0u, 0u);
             };
             hand_off(std::integral_constant<int, 0>{});
             hand_off(std::integral_constant<int, 1>{});
@@ -548,14 +552,14 @@ __global__ void __launch_bounds__(kIntegrateThreads, MGK_X2_MIN_BLOCKS)
 
     const unsigned long long w_att = warp_sum((unsigned long long)n_att);
     const unsigned long long w_steps = warp_sum((unsigned long long)n_steps);
-    unsigned long long c[5];
+    unsigned long long c[MGK_RAY_CLASSES];
 #pragma unroll
-    for (int i = 0; i < 5; ++i) c[i] = warp_sum((unsigned long long)n_cls[i]);
+    for (int i = 0; i < MGK_RAY_CLASSES; ++i) c[i] = warp_sum((unsigned long long)n_cls[i]);
     if (lane == 0) {
         atomicAdd(&cnt->attempts, w_att);
         atomicAdd(&cnt->steps, w_steps);
 #pragma unroll
-        for (int i = 1; i < 5; ++i)
+        for (int i = 1; i < MGK_RAY_CLASSES; ++i)
             if (c[i]) atomicAdd(&cnt->class_count[i], c[i]);
     }
 }
@@ -575,7 +579,7 @@ __global__ void __launch_bounds__(128, MGK_REFINE_MIN_BLOCKS) k_refine(const Dev
     const uint32_t nd = min(cnt->refine_count, cap);
     const uint32_t n = min(nd + min(cnt->escape_count, cap), cap);
     unsigned long long n_evals = 0;
-    uint32_t n_cls[5] = {0, 0, 0, 0, 0};
+    uint32_t n_cls[MGK_RAY_CLASSES] = {0, 0, 0, 0, 0, 0};
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t stride = gridDim.x * blockDim.x;
     // warp-uniform trip count so the queue pushes can use warp ballots;
@@ -586,29 +590,34 @@ __global__ void __launch_bounds__(128, MGK_REFINE_MIN_BLOCKS) k_refine(const Dev
         const uint32_t i = v < nd ? v : cap - 1u - (v - nd);
         Term<T> t{MGK_RAY_ALIVE, T(0), T(0), T(0), T(0), T(0)};
         RefineEntry<T> e;
-        S7<T> y1{}, ye{};
+        S7<T> ye{};
         uint32_t evals = 0;
+        Bounce bn{0u, 0ull, false};
         if (valid) {
             e = refq[i];
             S7<T> y0 = s7(e.y0);
-            y1 = s7(e.y1);
+            S7<T> y1 = s7(e.y1);
             evals = e.evals;
-            t = resolve<METRIC, F, T>(P, y0, y1, e.pt, e.h, e.c0, e.steps, ye, evals);
+            bn.count = e.bounces;
+            bn.ray_id = P.ray_base + e.ray;
+            t = resolve<METRIC, F, T>(P, y0, y1, e.pt, e.h, e.c0, e.steps, bn, ye, evals);
             n_evals += evals - e.evals;
         }
+        // a ray that goes on (candidate missed, or reflected: restart with the first step size)
         uint32_t rslot = warp_push(valid && t.cls == MGK_RAY_ALIVE, &cnt->resume_count, cap, &cnt->status);
         if (rslot != ~0u)
-            store_resume<T>(resq, rslot, y1, e.pt, e.h_next, e.c0, e.ray, e.steps, e.attempts, e.wide, evals);
-        bool lit = valid && (t.cls == MGK_RAY_DISK || t.cls == MGK_RAY_ESCAPED);
+            store_resume<T>(resq, rslot, ye, e.pt, bn.reflected ? P.h0 : e.h_next, e.c0, e.ray, e.steps, e.attempts,
+                            e.wide, evals, bn.count);
+        bool lit = valid && (t.cls == MGK_RAY_DISK || t.cls == MGK_RAY_ESCAPED || t.cls == MGK_RAY_LIGHT);
         uint32_t hslot = warp_push(lit, &cnt->hit_count, hit_cap, &cnt->status);
         if (hslot != ~0u) push_hit<T>(hits, hslot, e.ray, t);
         if (valid && t.cls != MGK_RAY_ALIVE) {
-            if (res) write_result<T>(res, e.ray, ye, e.pt, t, e.steps, e.attempts, e.wide, evals);
+            if (res) write_result<T>(res, e.ray, ye, e.pt, t, e.steps, e.attempts, e.wide, evals, bn.count);
             ++n_cls[t.cls];
         }
     }
     if (n_evals) atomicAdd(&cnt->refine_evals, n_evals);
-    for (int i = 1; i < 5; ++i)
+    for (int i = 1; i < MGK_RAY_CLASSES; ++i)
         if (n_cls[i]) atomicAdd(&cnt->class_count[i], (unsigned long long)n_cls[i]);
 }
 
@@ -630,12 +639,13 @@ __global__ void __launch_bounds__(128, 4) k_tail(const DevScene<typename ModeT<M
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
     unsigned long long n_att = 0, n_steps = 0, n_wide = 0, n_evals = 0;
-    uint32_t n_cls[5] = {0, 0, 0, 0, 0};
+    uint32_t n_cls[MGK_RAY_CLASSES] = {0, 0, 0, 0, 0, 0};
 
     bool alive = false;
     S7<T> y{};
     T pt = 0, c0 = 0, h = 0;
     uint32_t ray = 0, steps = 0, att = 0, wide = 0, evals = 0, tries = 0;
+    Bounce bn{0u, 0ull, false};
     double r_cur = 0.0;
     uint32_t cbeg = 0, cend = 0;
     bool drained = false;
@@ -669,6 +679,8 @@ __global__ void __launch_bounds__(128, 4) k_tail(const DevScene<typename ModeT<M
                     y = s7(e.y);
                     pt = e.pt; c0 = e.c0; h = e.h;
                     ray = e.ray; steps = e.steps; att = e.attempts; wide = e.wide; evals = e.evals;
+                    bn.count = e.bounces;
+                    bn.ray_id = P.ray_base + e.ray;
                     tries = 0;
                     if constexpr (MODE == MGK_PRECISION_MIXED)
                         r_cur = ks_r<double>(double(y.x), double(y.y), double(y.z), P.spin_d);
@@ -709,9 +721,10 @@ __global__ void __launch_bounds__(128, 4) k_tail(const DevScene<typename ModeT<M
                 ++steps; ++n_steps;
                 S7<T> ye;
                 const uint32_t ev0 = evals;
-                t = resolve<METRIC, F, T>(P, y, y1, pt, h_used, c0, steps, ye, evals);
+                t = resolve<METRIC, F, T>(P, y, y1, pt, h_used, c0, steps, bn, ye, evals);
                 n_evals += evals - ev0;
                 y = ye;
+                if (bn.reflected) h = P.h0;
                 if (t.cls != MGK_RAY_ALIVE) done = true;
                 else if constexpr (MODE == MGK_PRECISION_MIXED)
                     r_cur = ks_r<double>(double(y.x), double(y.y), double(y.z), P.spin_d);
@@ -719,11 +732,11 @@ __global__ void __launch_bounds__(128, 4) k_tail(const DevScene<typename ModeT<M
         }
 
         // ---- finished rays: hit queue (one ballot per warp) and per-ray records
-        const bool lit = done && (t.cls == MGK_RAY_DISK || t.cls == MGK_RAY_ESCAPED);
+        const bool lit = done && (t.cls == MGK_RAY_DISK || t.cls == MGK_RAY_ESCAPED || t.cls == MGK_RAY_LIGHT);
         const uint32_t hslot = warp_push(lit, &cnt->hit_count, hit_cap, &cnt->status);
         if (hslot != ~0u) push_hit<T>(hits, hslot, ray, t);
         if (done) {
-            if (res) write_result<T>(res, ray, y, pt, t, steps, att, wide, evals);
+            if (res) write_result<T>(res, ray, y, pt, t, steps, att, wide, evals, bn.count);
             ++n_cls[t.cls];
             alive = false;
         }
@@ -734,7 +747,7 @@ __global__ void __launch_bounds__(128, 4) k_tail(const DevScene<typename ModeT<M
         atomicAdd(&cnt->wide_attempts, n_wide);
     }
     if (n_evals) atomicAdd(&cnt->refine_evals, n_evals);
-    for (int i = 1; i < 5; ++i)
+    for (int i = 1; i < MGK_RAY_CLASSES; ++i)
         if (n_cls[i]) atomicAdd(&cnt->class_count[i], (unsigned long long)n_cls[i]);
 }
 
@@ -810,6 +823,21 @@ __global__ void __launch_bounds__(256) k_shade(const DevScene<T> P, const HitEnt
         if (h.cls == MGK_RAY_DISK) {
             // T(r) = T_in (r / r_in)^(-3/4)
             add(T(1), P.disk_T_in * exp2(T(-0.75) * log2(h.r_hit / P.disk_r_in)));
+        } else if (h.cls == MGK_RAY_LIGHT) {
+            // white LED at the shifted wavelength, boosted by z^5
+            // (matter_examples.cuh:67-76, bxdf_utilities.cuh:156-163)
+            const T z2 = h.z * h.z, z5 = z2 * z2 * h.z;
+            if (sampled) {
+                rad = clamp_radiance<T>(white_led<T>(h.z * lam) * P.light_scale * z5);
+            } else {
+                for (uint32_t k = 0; k < nb; ++k) {
+                    float sv = float(clamp_radiance<T>(white_led<T>(h.z * P.lambda[k]) * P.light_scale * z5));
+                    X = __fmaf_rn(sv, sw[3 * k], X);
+                    Y = __fmaf_rn(sv, sw[3 * k + 1], Y);
+                    Z = __fmaf_rn(sv, sw[3 * k + 2], Z);
+                    if (spec) atomicAdd(spec + k, sv * P.inv_spp);
+                }
+            }
         } else if (grid.n != 0u) {
             const uint32_t cell = cube_cell(float(h.d0), float(h.d1), float(h.d2), grid.n);
             const uint32_t j1 = grid.cell_start[cell + 1];
@@ -1283,9 +1311,11 @@ cudaError_t launch_generate(const mgk_scene& s, const void* dev_scene, uint64_t 
 }
 
 template <int METRIC, int MODE>
-static cudaError_t integ_t(const void* dsc, uint32_t n, const ChunkBuffers& b, mgk_ray_result* res, int sms,
-                           cudaStream_t st) {
+static cudaError_t integ_t(const void* dsc, uint64_t first, uint32_t n, const ChunkBuffers& b, mgk_ray_result* res,
+                           int sms, cudaStream_t st) {
     using T = typename ModeT<MODE>::T;
+    DevScene<T> P = ds<T>(dsc);
+    P.ray_base = first;
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_integrate<METRIC, MODE>, kIntegrateThreads, 0);
     if (per_sm < 1) per_sm = 1;
@@ -1303,10 +1333,10 @@ static cudaError_t integ_t(const void* dsc, uint32_t n, const ChunkBuffers& b, m
         blocks = uint32_t(sms * per_sm);
         need = (n + 2 * kIntegrateThreads - 1) / (2 * kIntegrateThreads);
         if (blocks > need) blocks = need;
-        k_integrate_x2<METRIC><<<blocks, kIntegrateThreads, 0, st>>>(ds<T>(dsc), n, b.qx, b.qp, b.qc, refq, resq, res,
+        k_integrate_x2<METRIC><<<blocks, kIntegrateThreads, 0, st>>>(P, n, b.qx, b.qp, b.qc, refq, resq, res,
                                                                      b.counters, b.ray_ids);
     } else {
-        k_integrate<METRIC, MODE><<<blocks, kIntegrateThreads, 0, st>>>(ds<T>(dsc), n, b.qx, b.qp, b.qc, refq, resq,
+        k_integrate<METRIC, MODE><<<blocks, kIntegrateThreads, 0, st>>>(P, n, b.qx, b.qp, b.qc, refq, resq,
                                                                        res, b.counters, b.ray_ids);
     }
     cudaError_t e = cudaGetLastError();
@@ -1315,34 +1345,34 @@ static cudaError_t integ_t(const void* dsc, uint32_t n, const ChunkBuffers& b, m
     int refine_per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&refine_per_sm, k_refine<METRIC, MODE>, 128, 0);
     if (refine_per_sm < 1) refine_per_sm = 1;
-    k_refine<METRIC, MODE><<<sms * refine_per_sm * 2, 128, 0, st>>>(ds<T>(dsc), refq, n, hits, resq, res, b.counters,
+    k_refine<METRIC, MODE><<<sms * refine_per_sm * 2, 128, 0, st>>>(P, refq, n, hits, resq, res, b.counters,
                                                                    hit_cap);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     int tail_per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tail_per_sm, k_tail<METRIC, MODE>, 128, 0);
     if (tail_per_sm < 1) tail_per_sm = 1;
-    k_tail<METRIC, MODE><<<sms * tail_per_sm, 128, 0, st>>>(ds<T>(dsc), resq, n, hits, res, b.counters, hit_cap);
+    k_tail<METRIC, MODE><<<sms * tail_per_sm, 128, 0, st>>>(P, resq, n, hits, res, b.counters, hit_cap);
     return cudaGetLastError();
 }
 
 template <int MODE>
-static cudaError_t integ_m(int metric, const void* dsc, uint32_t n, const ChunkBuffers& b, mgk_ray_result* res,
-                           int sms, cudaStream_t st) {
+static cudaError_t integ_m(int metric, const void* dsc, uint64_t first, uint32_t n, const ChunkBuffers& b,
+                           mgk_ray_result* res, int sms, cudaStream_t st) {
     switch (metric) {
-        case MGK_METRIC_KERR: return integ_t<MGK_METRIC_KERR, MODE>(dsc, n, b, res, sms, st);
-        case MGK_METRIC_SCHWARZSCHILD: return integ_t<MGK_METRIC_SCHWARZSCHILD, MODE>(dsc, n, b, res, sms, st);
-        default: return integ_t<MGK_METRIC_MINKOWSKI, MODE>(dsc, n, b, res, sms, st);
+        case MGK_METRIC_KERR: return integ_t<MGK_METRIC_KERR, MODE>(dsc, first, n, b, res, sms, st);
+        case MGK_METRIC_SCHWARZSCHILD: return integ_t<MGK_METRIC_SCHWARZSCHILD, MODE>(dsc, first, n, b, res, sms, st);
+        default: return integ_t<MGK_METRIC_MINKOWSKI, MODE>(dsc, first, n, b, res, sms, st);
     }
 }
 
-cudaError_t launch_integrate(const mgk_scene& s, const void* dsc, uint64_t, uint32_t n, const ChunkBuffers& b,
+cudaError_t launch_integrate(const mgk_scene& s, const void* dsc, uint64_t first, uint32_t n, const ChunkBuffers& b,
                              mgk_ray_result* res, int sms, cudaStream_t st) {
     if (n == 0) return cudaSuccess;
     switch (s.precision) {
-        case MGK_PRECISION_REF32: return integ_m<MGK_PRECISION_REF32>(s.metric, dsc, n, b, res, sms, st);
-        case MGK_PRECISION_MIXED: return integ_m<MGK_PRECISION_MIXED>(s.metric, dsc, n, b, res, sms, st);
-        default: return integ_m<MGK_PRECISION_F64>(s.metric, dsc, n, b, res, sms, st);
+        case MGK_PRECISION_REF32: return integ_m<MGK_PRECISION_REF32>(s.metric, dsc, first, n, b, res, sms, st);
+        case MGK_PRECISION_MIXED: return integ_m<MGK_PRECISION_MIXED>(s.metric, dsc, first, n, b, res, sms, st);
+        default: return integ_m<MGK_PRECISION_F64>(s.metric, dsc, first, n, b, res, sms, st);
     }
 }
 
@@ -1470,6 +1500,16 @@ template <class T> static void fill_t(const mgk_scene& s, const float* xyz_w, De
         P->dlambda = T(dl);
         P->inv_sigma_sqrt2 = T(1.0 / (s.redistribution_sigma_nm * std::sqrt(2.0)));
     }
+    P->room_on = s.room_on ? 1u : 0u;
+    P->room_limit = s.room_reflection_limit;
+    for (int a = 0; a < 3; ++a) {
+        P->room_lo[a] = T(s.room_min[a]);
+        P->room_hi[a] = T(s.room_max[a]);
+        P->light_lo[a] = T(s.light_min[a]);
+        P->light_hi[a] = T(s.light_max[a]);
+    }
+    P->light_scale = T(s.light_scale);
+    P->ray_base = 0;
 }
 
 void fill_dev_scene(const mgk_scene& s, const float* xyz_w, void* out) {

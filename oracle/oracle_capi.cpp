@@ -351,4 +351,30 @@ int orc_count_ops(int metric, int fused, uint64_t* out) {
     return 0;
 }
 
+// Room scene parts, for the CPU tests: the chord event (double), the
+// white-LED spectrum (double) and one wall reflection of a float state.
+int orc_room_event(const mgk_scene* s, const double* p0, const double* p1, double* t, int* axis_side_light) {
+    RoomEvent<double> ev = room_event<double>(*s, V4<double>{p0[0], p0[1], p0[2], 0.0},
+                                              V4<double>{p1[0], p1[1], p1[2], 0.0});
+    *t = ev.t;
+    axis_side_light[0] = ev.axis; axis_side_light[1] = ev.side; axis_side_light[2] = ev.light ? 1 : 0;
+    return 0;
+}
+
+double orc_white_led(double lambda_nm) { return white_led<double>(lambda_nm); }
+
+int orc_reflect_wall(const mgk_scene* s, const float* x, const float* p, int axis, int side, float c0,
+                     uint32_t bounce, uint64_t ray_id, float* x_out, float* p_out, float* c0_out) {
+    MetricParams<float> m = metric_params<float>(*s);
+    GState<float> ys;
+    ys.x = V4<float>{x[0], x[1], x[2], x[3]};
+    ys.p = V4<float>{p[0], p[1], p[2], p[3]};
+    float c = c0;
+    GState<float> o = reflect_wall<float>(*s, m, axis, side, ys, &c, bounce, ray_id);
+    x_out[0] = o.x.x; x_out[1] = o.x.y; x_out[2] = o.x.z; x_out[3] = o.x.t;
+    p_out[0] = o.p.x; p_out[1] = o.p.y; p_out[2] = o.p.z; p_out[3] = o.p.t;
+    *c0_out = c;
+    return 0;
+}
+
 }  // extern "C"

@@ -45,6 +45,13 @@ def lib():
                                         C.POINTER(C.c_float), C.c_uint64, C.c_uint32, C.c_uint64,
                                         C.POINTER(C.c_float), C.POINTER(C.c_double), C.POINTER(C.c_uint64), C.c_int]
         L.orc_count_ops.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_uint64)]
+        D3 = C.POINTER(C.c_double)
+        F4 = C.POINTER(C.c_float)
+        L.orc_room_event.argtypes = [C.POINTER(abi.Scene), D3, D3, D3, C.POINTER(C.c_int)]
+        L.orc_white_led.argtypes = [C.c_double]
+        L.orc_white_led.restype = C.c_double
+        L.orc_reflect_wall.argtypes = [C.POINTER(abi.Scene), F4, F4, C.c_int, C.c_int, C.c_float, C.c_uint32,
+                                       C.c_uint64, F4, F4, F4]
         _lib = L
     return _lib
 
@@ -68,6 +75,11 @@ def ref():
         R.ref_render_pixels.argtypes = [C.POINTER(abi.Scene), C.POINTER(abi.Star), C.c_uint32, C.POINTER(C.c_float),
                                         C.c_uint64, C.c_uint32, C.c_uint64, C.POINTER(C.c_double), C.c_int]
         R.ref_render_pixels.restype = C.c_int
+        R.ref_white_led.argtypes = [C.c_float]
+        R.ref_white_led.restype = C.c_float
+        F4 = C.POINTER(C.c_float)
+        R.ref_reflect_mirror.argtypes = [C.POINTER(abi.Scene), F4, F4, F4, C.c_float, F4, F4]
+        R.ref_reflect_mirror.restype = C.c_int
         _ref = R
     return _ref
 
@@ -135,7 +147,7 @@ def scene_constants(scene):
 
 RESULT_DTYPE = np.dtype([("x", "<f8", 4), ("p", "<f8", 4), ("z", "<f8"), ("r_hit", "<f8"), ("dir", "<f8", 3),
                          ("cls", "<u4"), ("steps", "<u4"), ("attempts", "<u4"), ("wide_attempts", "<u4"),
-                         ("refine_evals", "<u4"), ("reserved", "<u4")])
+                         ("refine_evals", "<u4"), ("bounces", "<u4")])
 assert RESULT_DTYPE.itemsize == C.sizeof(abi.RayResult)
 
 
@@ -206,3 +218,50 @@ def count_ops(metric, fused):
     out = (C.c_uint64 * 2)()
     lib().orc_count_ops(metric, int(fused), out)
     return out[0], out[1]
+
+
+def _fptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def room_event(scene, p0, p1):
+    """First room event on the chord p0 -> p1: (t, axis, side, light)."""
+    a0 = np.ascontiguousarray(p0, dtype=np.float64)
+    a1 = np.ascontiguousarray(p1, dtype=np.float64)
+    t = C.c_double()
+    asl = (C.c_int * 3)()
+    lib().orc_room_event(C.byref(scene), a0.ctypes.data_as(C.POINTER(C.c_double)),
+                         a1.ctypes.data_as(C.POINTER(C.c_double)), C.byref(t), asl)
+    return t.value, asl[0], asl[1], bool(asl[2])
+
+
+def white_led(lam):
+    return lib().orc_white_led(float(lam))
+
+
+def reflect_wall(scene, x, p, axis, side, c0, bounce=0, ray_id=0):
+    """One wall reflection of a float state: (x_out[4], p_out[4], c0_out)."""
+    xi = np.ascontiguousarray(x, dtype=np.float32)
+    pi = np.ascontiguousarray(p, dtype=np.float32)
+    xo = np.zeros(4, np.float32)
+    po = np.zeros(4, np.float32)
+    co = C.c_float()
+    lib().orc_reflect_wall(C.byref(scene), _fptr(xi), _fptr(pi), axis, side, c0, bounce, ray_id, _fptr(xo),
+                           _fptr(po), C.byref(co))
+    return xo, po, co.value
+
+
+def ref_white_led(lam):
+    return ref().ref_white_led(float(lam))
+
+
+def ref_reflect_mirror(scene, x, p, n, c0):
+    """The reference's mirror reflection: (p_out[4], c0_out)."""
+    xi = np.ascontiguousarray(x, dtype=np.float32)
+    pi = np.ascontiguousarray(p, dtype=np.float32)
+    ni = np.ascontiguousarray(n, dtype=np.float32)
+    po = np.zeros(4, np.float32)
+    co = C.c_float()
+    rc = ref().ref_reflect_mirror(C.byref(scene), _fptr(xi), _fptr(pi), _fptr(ni), c0, _fptr(po), C.byref(co))
+    assert rc == 0
+    return po, co.value

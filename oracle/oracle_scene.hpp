@@ -5,11 +5,14 @@
 //  * pinhole camera with seeded jitter; observer = the metric's reference
 //    observer (kernel_generate_initial_conditions.cu:54-74,
 //    relativity_utilities.cuh:163-195)
-//  * per accepted step: thin-disk crossing, escape radius, horizon
-//    (kernel_intersect.cu:55-138 order: traceables before the horizon),
-//    step cap (kernel_enforce_ray_limits.cu:37-64)
+//  * per accepted step: thin-disk crossing, room walls and light, escape
+//    radius, horizon (kernel_intersect.cu:55-138 order: traceables before the
+//    horizon), step cap and reflection cap (kernel_enforce_ray_limits.cu:37-64)
+//  * wall reflection in the wall's rest frame, mirror on walls normal to x,
+//    Lambertian elsewhere (matter_examples.cuh:33-58, bxdf_utilities.cuh:53-154)
 //  * Keplerian disk emitter, redshift (bxdf_utilities.cuh:89-109,156-163),
-//    blackbody (internal_math.h:2511-2526) at N wavelengths, star field
+//    blackbody (internal_math.h:2511-2526) at N wavelengths, star field,
+//    white-LED light (matter_examples.cuh:60-77, internal_math.h:2441-2509)
 //  * spectral -> XYZ with per-bin CMF weights (device_color_utilities.cuh:40-54)
 //
 // The "mixed" precision mode (FP32 state, FP64 step control, FP64 attempts
@@ -184,7 +187,7 @@ struct RayResult {
     uint32_t attempts;
     uint32_t wide_attempts;
     uint32_t refine_evals;  // RK sub-steps spent locating a crossing
-    uint32_t reserved;
+    uint32_t bounces;       // reflections off the room's walls
 };
 
 // ------------------------------------------------------------ crossings
@@ -201,12 +204,15 @@ template <Fuse F, class T> inline GState<T> sub_step(const GState<T>& y0, T s, c
     return y1;
 }
 
-// kind 0: disk plane (g = y); kind 1: escape sphere (g = |x|^2 - R^2).
+template <class T> inline T coord(const V4<T>& q, int axis) { return axis == 0 ? q.x : (axis == 1 ? q.y : q.z); }
+
+// kind 0, 1, 2: the plane x, y or z = v (disk: y = 0; room faces);
+// kind 3: the escape sphere |x|^2 = v.
 template <Fuse F, class T>
-inline GState<T> refine(int kind, const GState<T>& y0, const GState<T>& y1, T h, T R2, const MetricParams<T>& m,
+inline GState<T> refine(int kind, const GState<T>& y0, const GState<T>& y1, T h, T v, const MetricParams<T>& m,
                         uint32_t* evals) {
     auto g = [&](const GState<T>& q) {
-        return kind == 0 ? q.x.y : mad<F>(q.x.z, q.x.z, mad<F>(q.x.y, q.x.y, q.x.x * q.x.x)) - R2;
+        return kind == 3 ? mad<F>(q.x.z, q.x.z, mad<F>(q.x.y, q.x.y, q.x.x * q.x.x)) - v : coord(q.x, kind) - v;
     };
     T g0 = g(y0), g1 = g(y1);
     T s_prev = h, g_prev = g1;
@@ -216,8 +222,8 @@ inline GState<T> refine(int kind, const GState<T>& y0, const GState<T>& y1, T h,
     T gs = g(ys);
     // The escape sphere lies in the far field, where one sub-step to the chord
     // estimate already puts the direction within 1e-9 of the located one;
-    // the disk plane is met in strong field and iterates.
-    const int iters = kind == 0 ? MGK_REFINE_ITERS : 0;
+    // planes (the disk in strong field, the room's faces) iterate.
+    const int iters = kind < 3 ? MGK_REFINE_ITERS : 0;
     for (int it = 0; it < iters; ++it) {
         T den = gs - g_prev;
         if (gs == T(0) || den == T(0)) break;
@@ -263,34 +269,195 @@ inline bool disk_candidate(const mgk_scene& s, const MetricParams<T>& m, const G
     return rc >= T(0.98 * s.disk_r_in - 0.02) && rc <= T(1.02 * s.disk_r_out + 0.02);
 }
 
+// ------------------------------------------------------------------ room
+// The reference's box-and-light scene (stage.h:19-22, matter_examples.cuh:
+// 33-77, kernel_intersect.cu:81-100).  First event on the chord a0 -> a1:
+// leaving the room (the face crossed first among the axes on which a1 lies
+// outside) or entering the light (slab test as traceables.cuh:17-74, on the
+// chord segment).  axis < 0: none; side 0 / 1: face at the minimum / maximum.
+template <class T> struct RoomEvent {
+    T t = T(2);
+    int axis = -1, side = 0;
+    bool light = false;
+};
+template <class T> inline RoomEvent<T> room_event(const mgk_scene& s, const V4<T>& p0, const V4<T>& p1) {
+    RoomEvent<T> ev;
+    if (!s.room_on) return ev;
+    const T a0[3] = {p0.x, p0.y, p0.z}, a1[3] = {p1.x, p1.y, p1.z};
+    for (int a = 0; a < 3; ++a) {
+        const T lo = T(s.room_min[a]), hi = T(s.room_max[a]);
+        const bool above = a1[a] > hi, below = a1[a] < lo;
+        if (!(above || below)) continue;
+        const T b = above ? hi : lo;
+        T t = (b - a0[a]) / (a1[a] - a0[a]);
+        if (!(t >= T(0))) t = T(0);
+        if (t < ev.t) { ev.t = t; ev.axis = a; ev.side = above ? 1 : 0; }
+    }
+    T tn = T(0), tf = T(1);
+    int an = -1, sn = 0;
+    bool miss = false;
+    for (int a = 0; a < 3; ++a)  // chord bounding box overlaps the light
+        if (!(std::fmax(a0[a], a1[a]) >= T(s.light_min[a]) && std::fmin(a0[a], a1[a]) <= T(s.light_max[a])))
+            miss = true;
+    for (int a = 0; a < 3 && !miss; ++a) {
+        const T llo = T(s.light_min[a]), lhi = T(s.light_max[a]);
+        const T d = a1[a] - a0[a];
+        if (d == T(0)) {
+            if (a0[a] < llo || a0[a] > lhi) miss = true;
+            continue;
+        }
+        const T t_lo = (llo - a0[a]) / d, t_hi = (lhi - a0[a]) / d;
+        const T t_near = d > T(0) ? t_lo : t_hi, t_far = d > T(0) ? t_hi : t_lo;
+        if (t_near > tn) { tn = t_near; an = a; sn = d > T(0) ? 0 : 1; }
+        if (t_far < tf) tf = t_far;
+    }
+    if (!miss && an >= 0 && tn <= tf && tn < ev.t) {
+        ev.t = tn; ev.axis = an; ev.side = sn; ev.light = true;
+    }
+    return ev;
+}
+
+// evaluate_white_led_spectrum, internal_math.h:2501-2509, with
+// gaussian_distribution (internal_math.h:2441-2445).
+template <class T> inline T white_led(T x) {
+    auto gauss = [](T v, T o, T w, T sc) { return T(std::exp(T(-0.5) * (((v - o) * (v - o)) / (w * w)))) * sc; };
+    T acc = T(0);
+    acc = acc + gauss(x, T(577.0), T(50.7937003968), T(157.0));
+    acc = acc + gauss(x, T(451.0), T(7.07106781187), T(200.0));
+    acc = acc + gauss(x, T(455.0), T(14.1421356237), T(50.0));
+    acc = acc + gauss(x, T(528.0), T(13.7840487521), T(20.0));
+    acc = acc + gauss(x, T(690.0), T(44.72135955), T(10.0));
+    return acc;
+}
+
+// Uniform unit-sphere direction (the distribution of sample_lambertian_brdf's
+// p, brdf.cuh:18-25): cos(theta) = 1 - 2 u, azimuth from a rejection-sampled
+// point of the unit disc, from the ray's random dimensions base .. base + 32.
+template <class T> inline void sphere_dir(uint64_t seed, uint32_t sample, uint32_t pixel, uint32_t base, T out[3]) {
+    const T cz = T(1) - T(2) * T(rng_unit(seed, sample, pixel, base));
+    const T q = T(1) - cz * cz;
+    const T sz = sq_root(q > T(0) ? q : T(0));
+    T cx = T(1), cy = T(0);
+    for (uint32_t j = 0; j < 16; ++j) {
+        const T vx = T(2) * T(rng_unit(seed, sample, pixel, base + 1u + 2u * j)) - T(1);
+        const T vy = T(2) * T(rng_unit(seed, sample, pixel, base + 2u + 2u * j)) - T(1);
+        const T r2 = vx * vx + vy * vy;
+        if (r2 <= T(1) && r2 > T(1e-12)) {
+            const T r = sq_root(r2);
+            cx = vx / r;
+            cy = vy / r;
+            break;
+        }
+    }
+    out[0] = cx * sz; out[1] = cy * sz; out[2] = cz;
+}
+
+// Reflection at the located wall point ys (apply_reflected and its context,
+// bxdf_utilities.cuh:53-109,139-154): rest frame of the reference observer,
+// facing normal, mirror (walls normal to x) or normalised(uniform sphere
+// direction + normal), back to a null covariant momentum; c0 takes the
+// redshift at the wall along; the ray restarts 1/256 inside the face.
+template <class T>
+inline GState<T> reflect_wall(const mgk_scene& s, const MetricParams<T>& m, int axis, int side, const GState<T>& ys,
+                              T* c0, uint32_t bounce, uint64_t ray_id) {
+    const Sym4<T> g = compute_g(ys.x, m);
+    const V4<T> u = reference_observer(ys.x, m);
+    const Tetrad<T> e = build_tetrad(g, V4<T>{T(1), T(0), T(0), T(0)}, V4<T>{T(0), T(1), T(0), T(0)},
+                                     V4<T>{T(0), T(0), T(1), T(0)}, u);
+    const V4<T>& p = ys.p;
+    const T zr = redshift_clamp<T>(*c0 / dot4(u, p));
+    T d[3] = {dot4(e.x, p), dot4(e.y, p), dot4(e.z, p)};
+    const T dl = sq_root(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    for (T& v : d) v = v / dl;
+    const T ns = side ? T(-1) : T(1);
+    T n[3] = {coord(e.x, axis) * ns, coord(e.y, axis) * ns, coord(e.z, axis) * ns};
+    const T nl = sq_root(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+    for (T& v : n) v = v / nl;
+    if (n[0] * d[0] + n[1] * d[1] + n[2] * d[2] > T(0))
+        for (T& v : n) v = -v;
+    T o[3];
+    if (axis == 0) {
+        const T k = T(2) * (d[0] * n[0] + d[1] * n[1] + d[2] * n[2]);
+        for (int i = 0; i < 3; ++i) o[i] = d[i] - k * n[i];
+    } else {
+        T q[3];
+        sphere_dir<T>(s.seed, uint32_t(ray_id % s.spp), uint32_t(ray_id / s.spp), 8u + 64u * bounce, q);
+        for (int i = 0; i < 3; ++i) o[i] = q[i] + n[i];
+        if (!(o[0] * o[0] + o[1] * o[1] + o[2] * o[2] > T(1e-12)))
+            for (int i = 0; i < 3; ++i) o[i] = n[i];
+    }
+    const T ol = sq_root(o[0] * o[0] + o[1] * o[1] + o[2] * o[2]);
+    for (T& v : o) v = v / ol;
+    const T l = sq_root(o[0] * o[0] + o[1] * o[1] + o[2] * o[2]);
+    const V4<T> po = contract(g, local_to_global(e, V4<T>{o[0], o[1], o[2], l}));
+    *c0 = dot4(u, po) * zr;
+    T x[3] = {ys.x.x, ys.x.y, ys.x.z};
+    for (int a = 0; a < 3; ++a) x[a] = std::fmin(std::fmax(x[a], T(s.room_min[a])), T(s.room_max[a]));
+    x[axis] = side ? T(s.room_max[axis]) - T(0.00390625) : T(s.room_min[axis]) + T(0.00390625);
+    GState<T> out;
+    out.x = V4<T>{x[0], x[1], x[2], ys.x.t};
+    out.p = po;
+    return out;
+}
+
+struct Bounce {
+    uint32_t count = 0;
+    uint64_t ray_id = 0;
+    bool reflected = false;
+};
+
 // Tests after the accepted step y0 -> y1 of length h, in this order: thin
-// disk, escape radius, horizon, step cap.
+// disk (unless a room event comes first on the chord), room walls and light,
+// escape radius, horizon, step cap.  A wall reflection leaves the ray alive
+// with y_end its restart state and *c0 updated.
 template <Fuse F, class T>
 inline Resolved<T> resolve(const mgk_scene& s, const MetricParams<T>& m, const GState<T>& y0, const GState<T>& y1,
-                           T h, T c0, uint32_t steps, T spin_phys, T omega_sign) {
+                           T h, T* c0, uint32_t steps, T spin_phys, T omega_sign, Bounce* bn) {
     Resolved<T> o;
     o.y_end = y1;
+    bn->reflected = false;
     T a = m.metric == KERR ? m.spin : T(0);
-    if (disk_candidate<F, T>(s, m, y0, y1)) {
-        GState<T> ys = refine<F, T>(0, y0, y1, h, T(0), m, &o.evals);
+    const RoomEvent<T> ev = room_event<T>(s, y0.x, y1.x);
+    if (disk_candidate<F, T>(s, m, y0, y1) && !(ev.axis >= 0 && ev.t < y0.x.y / (y0.x.y - y1.x.y))) {
+        GState<T> ys = refine<F, T>(1, y0, y1, h, T(0), m, &o.evals);
         T rh = kerr_schild_r(ys.x.x, ys.x.y, ys.x.z, a);
         if (rh >= T(s.disk_r_in) && rh <= T(s.disk_r_out)) {
             V4<T> u = disk_velocity<T>(ys.x.x, ys.x.z, rh, m, spin_phys, omega_sign);
             o.hit.cls = MGK_RAY_DISK;
-            o.hit.z = redshift_clamp<T>(c0 / dot4(u, ys.p));
+            o.hit.z = redshift_clamp<T>(*c0 / dot4(u, ys.p));
             o.hit.r_hit = rh;
             o.y_end = ys;
             return o;
         }
     }
+    if (ev.axis >= 0) {
+        const double* face = ev.light ? (ev.side ? s.light_max : s.light_min) : (ev.side ? s.room_max : s.room_min);
+        const GState<T> ys = ev.t > T(0) ? refine<F, T>(ev.axis, y0, y1, h, T(face[ev.axis]), m, &o.evals) : y0;
+        o.y_end = ys;
+        if (ev.light) {
+            o.hit.cls = MGK_RAY_LIGHT;
+            o.hit.z = redshift_clamp<T>(*c0 / dot4(reference_observer(ys.x, m), ys.p));
+            return o;
+        }
+        if (bn->count >= s.room_reflection_limit) {
+            bn->count += 1;
+            o.hit.cls = MGK_RAY_STEP_LIMIT;
+            return o;
+        }
+        o.y_end = reflect_wall<T>(s, m, ev.axis, ev.side, ys, c0, bn->count, bn->ray_id);
+        bn->count += 1;
+        bn->reflected = true;
+        if (steps >= s.max_steps) o.hit.cls = MGK_RAY_STEP_LIMIT;
+        return o;
+    }
     T R2 = T(s.escape_radius) * T(s.escape_radius);
     T r2 = mad<F>(y1.x.z, y1.x.z, mad<F>(y1.x.y, y1.x.y, y1.x.x * y1.x.x));
     if (r2 >= R2) {
-        GState<T> ys = refine<F, T>(1, y0, y1, h, R2, m, &o.evals);
+        GState<T> ys = refine<F, T>(3, y0, y1, h, R2, m, &o.evals);
         T pn = sq_root(mad<F>(ys.p.z, ys.p.z, mad<F>(ys.p.y, ys.p.y, ys.p.x * ys.p.x)));
         o.hit.cls = MGK_RAY_ESCAPED;
         o.hit.dir[0] = ys.p.x / pn; o.hit.dir[1] = ys.p.y / pn; o.hit.dir[2] = ys.p.z / pn;
-        o.hit.z = redshift_clamp<T>(c0 / ys.p.t);  // static emitter at infinity: u . p = p_t
+        o.hit.z = redshift_clamp<T>(*c0 / ys.p.t);  // static emitter at infinity: u . p = p_t
         o.y_end = ys;
         return o;
     }
@@ -336,13 +503,13 @@ template <class T> inline double ks_radius(const V4<T>& q, const MetricParams<do
 }
 
 template <class T> inline void store_result(RayResult* r, const GState<T>& y, const Hit<T>& h, uint32_t steps,
-                                            uint32_t attempts, uint32_t wide, uint32_t evals) {
+                                            uint32_t attempts, uint32_t wide, uint32_t evals, uint32_t bounces) {
     r->x[0] = y.x.x; r->x[1] = y.x.y; r->x[2] = y.x.z; r->x[3] = y.x.t;
     r->p[0] = y.p.x; r->p[1] = y.p.y; r->p[2] = y.p.z; r->p[3] = y.p.t;
     r->z = h.z; r->r_hit = h.r_hit;
     r->dir[0] = h.dir[0]; r->dir[1] = h.dir[1]; r->dir[2] = h.dir[2];
     r->cls = h.cls; r->steps = steps; r->attempts = attempts; r->wide_attempts = wide; r->refine_evals = evals;
-    r->reserved = 0;
+    r->bounces = bounces;
 }
 
 // Trace one camera ray of the scene to termination in the given precision.
@@ -358,7 +525,10 @@ inline RayResult trace_ray(const mgk_scene& s, const SceneConsts& c, uint64_t ra
             else ri = camera_ray<Fuse::None, T>(s, c, ray_id);
             GState<T> y = ri.y;
             T h = ri.h0;
+            T c0 = ri.c0;
             uint32_t steps = 0, attempts = 0, evals = 0;
+            Bounce bn;
+            bn.ray_id = ray_id;
             Resolved<T> rs;
             while (true) {
                 StepOut<T> so;
@@ -367,17 +537,18 @@ inline RayResult trace_ray(const mgk_scene& s, const SceneConsts& c, uint64_t ra
                 attempts += so.attempts;
                 ++steps;
                 if constexpr (std::is_same_v<T, double>)
-                    rs = resolve<Fuse::Fma, T>(s, m, y, so.y1, so.h_taken, ri.c0, steps,
-                                               T(s.metric == KERR ? s.spin : 0.0), T(c.omega_sign));
+                    rs = resolve<Fuse::Fma, T>(s, m, y, so.y1, so.h_taken, &c0, steps,
+                                               T(s.metric == KERR ? s.spin : 0.0), T(c.omega_sign), &bn);
                 else
-                    rs = resolve<Fuse::None, T>(s, m, y, so.y1, so.h_taken, ri.c0, steps,
-                                                T(s.metric == KERR ? s.spin : 0.0), T(c.omega_sign));
+                    rs = resolve<Fuse::None, T>(s, m, y, so.y1, so.h_taken, &c0, steps,
+                                                T(s.metric == KERR ? s.spin : 0.0), T(c.omega_sign), &bn);
                 evals += rs.evals;
                 y = rs.y_end;
-                h = so.h_next;
+                h = bn.reflected ? ri.h0 : so.h_next;
                 if (rs.hit.cls != MGK_RAY_ALIVE) break;
             }
-            store_result(&res, y, rs.hit, steps, attempts, std::is_same_v<T, double> ? attempts : 0u, evals);
+            store_result(&res, y, rs.hit, steps, attempts, std::is_same_v<T, double> ? attempts : 0u, evals,
+                         bn.count);
         };
         if (f64) run(double{}); else run(float{});
     } else {
@@ -388,6 +559,9 @@ inline RayResult trace_ray(const mgk_scene& s, const SceneConsts& c, uint64_t ra
         GState<T> y = ri.y;
         T h = ri.h0;
         uint32_t steps = 0, attempts = 0, wide = 0, tries = 0, evals = 0;
+        T c0 = ri.c0;
+        Bounce bn;
+        bn.ray_id = ray_id;
         double r_cur = ks_radius(y.x, md);
         Resolved<T> rs;
         while (true) {
@@ -406,14 +580,15 @@ inline RayResult trace_ray(const mgk_scene& s, const SceneConsts& c, uint64_t ra
             }
             tries = 0;
             ++steps;
-            rs = resolve<Fuse::Fma, T>(s, mf, y, y1, h_used, ri.c0, steps, T(s.metric == KERR ? s.spin : 0.0),
-                                       T(c.omega_sign));
+            rs = resolve<Fuse::Fma, T>(s, mf, y, y1, h_used, &c0, steps, T(s.metric == KERR ? s.spin : 0.0),
+                                       T(c.omega_sign), &bn);
             evals += rs.evals;
             y = rs.y_end;
+            if (bn.reflected) h = ri.h0;
             if (rs.hit.cls != MGK_RAY_ALIVE) break;
             r_cur = ks_radius(y.x, md);
         }
-        store_result(&res, y, rs.hit, steps, attempts, wide, evals);
+        store_result(&res, y, rs.hit, steps, attempts, wide, evals, bn.count);
     }
     return res;
 }
@@ -451,6 +626,10 @@ inline void ray_spectrum(const mgk_scene& s, const StarIndex* stars, const Hit<T
     if (h.cls == MGK_RAY_DISK) {
         T temp = T(s.disk_T_in) * T(std::pow(double(h.r_hit / T(s.disk_r_in)), -0.75));
         for (uint32_t k = 0; k < nb; ++k) out[k] = clamp(planck<T>(z * lambda[k], temp) * z5);
+    } else if (h.cls == MGK_RAY_LIGHT) {
+        // ABSORBED with the LED spectrum at the shifted wavelength, times z^5
+        // (matter_examples.cuh:67-76, bxdf_utilities.cuh:156-163)
+        for (uint32_t k = 0; k < nb; ++k) out[k] = clamp(white_led<T>(z * lambda[k]) * T(s.light_scale) * z5);
     } else if (h.cls == MGK_RAY_ESCAPED && stars && stars->n) {
         double th = std::acos(std::max(-1.0, std::min(1.0, double(h.dir[1]))));
         double rad = s.star_radius_rad;
@@ -502,6 +681,8 @@ inline void sampled_spectrum(const mgk_scene& s, const StarIndex* stars, const H
     if (h.cls == MGK_RAY_DISK) {
         T temp = T(s.disk_T_in) * T(std::pow(double(h.r_hit / T(s.disk_r_in)), -0.75));
         rad = clamp(planck<T>(z * lam, temp) * z5);
+    } else if (h.cls == MGK_RAY_LIGHT) {
+        rad = clamp(white_led<T>(z * lam) * T(s.light_scale) * z5);
     } else if (h.cls == MGK_RAY_ESCAPED && stars && stars->n) {
         double th = std::acos(std::max(-1.0, std::min(1.0, double(h.dir[1]))));
         double radius = s.star_radius_rad;

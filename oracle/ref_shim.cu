@@ -196,9 +196,35 @@ void ref_parallel_for(uint64_t n, int nthreads, const std::function<void(uint64_
     for (auto& t : th) t.join();
 }
 
+// The reference's mirror reflection at a wall (bxdf_diffuse_matter_t on a
+// wall normal to x, matter_examples.cuh:40-48) composed from its own frame
+// code as generate_velocity_context / generate_material_context /
+// apply_reflected do (bxdf_utilities.cuh:53-109,139-154), for a covariant
+// momentum p at x and the global facing normal n: the outgoing covariant
+// momentum and the new initial contraction.
+template <e_magik_spacetime_metric_types MT>
+void reflect_mirror_ref(typename magik::metric<MT>::params_t mp, const float* x, const float* p, const float* n,
+                        float c0, float* p_out, float* c0_out) {
+    using namespace magik;
+    contravariant_seed_vectors_t seeds;
+    const vec4f X{x[0], x[1], x[2], x[3]}, P{p[0], p[1], p[2], p[3]};
+    const vec4f u = rest_frame_four_velocity<MT>(X, seeds, vec3f{0.0f, 0.0f, 0.0f}, mp);
+    const sym4_t g_inv = metric<MT>::compute_inv_g(X, mp);
+    const vec4f rest = global_to_observer_rest_frame<MT>(X, seeds, contract(g_inv, P), u, mp);
+    const vec3f incoming = vec3f{rest.x, rest.y, rest.z}.norm();
+    const float z = compute_redshift_factor(c0, u, P);
+    const vec4f n_rest4 = global_to_observer_rest_frame<MT>(X, seeds, contract(g_inv, vec4f{n[0], n[1], n[2], 0.0f}), u, mp);
+    const vec3f n_rest = vec3f{n_rest4.x, n_rest4.y, n_rest4.z}.norm();
+    const vec3f facing = vector_dot_product(n_rest, incoming) > 0.0f ? -n_rest : n_rest;
+    const vec3f out = vector_reflect(incoming, facing).make_norm();
+    const vec4f po = rest_frame_direction_to_global_four_momentum<MT>(X, seeds, out, u, 0.0f, mp);
+    p_out[0] = po.x; p_out[1] = po.y; p_out[2] = po.z; p_out[3] = po.t;
+    *c0_out = vector_dot_product(u, po) * z;
+}
+
 // One camera ray: the oracle's REF32 initial conditions, then per accepted
 // step the reference's own solve_step (float, its op order and its powf) and
-// the oracle's disk / escape / horizon / step-cap tests.
+// the oracle's disk / room / escape / horizon / step-cap tests.
 template <e_magik_spacetime_metric_types MT>
 orc::RayResult trace_ref(const mgk_scene& s, const orc::SceneConsts& c, uint64_t ray_id,
                          typename magik::metric<MT>::params_t p) {
@@ -208,6 +234,9 @@ orc::RayResult trace_ref(const mgk_scene& s, const orc::SceneConsts& c, uint64_t
     GState<float> y = ri.y;
     float h = ri.h0;
     uint32_t steps = 0, attempts = 0, evals = 0;
+    float c0 = ri.c0;
+    Bounce bn;
+    bn.ray_id = ray_id;
     Resolved<float> rs;
     const float spin = float(s.metric == MGK_METRIC_KERR ? s.spin : 0.0);
     for (;;) {
@@ -220,18 +249,46 @@ orc::RayResult trace_ref(const mgk_scene& s, const orc::SceneConsts& c, uint64_t
         y1.p = V4<float>{y1r.four_momentum.x, y1r.four_momentum.y, y1r.four_momentum.z, y1r.four_momentum.t};
         ++attempts;  // the reference does not report its retries
         ++steps;
-        rs = resolve<Fuse::None, float>(s, m, y, y1, h_taken, ri.c0, steps, spin, float(c.omega_sign));
+        rs = resolve<Fuse::None, float>(s, m, y, y1, h_taken, &c0, steps, spin, float(c.omega_sign), &bn);
         evals += rs.evals;
         y = rs.y_end;
-        h = h_step;
+        h = bn.reflected ? ri.h0 : h_step;
         if (rs.hit.cls != MGK_RAY_ALIVE) break;
     }
     RayResult res{};
-    store_result(&res, y, rs.hit, steps, attempts, 0u, evals);
+    store_result(&res, y, rs.hit, steps, attempts, 0u, evals, bn.count);
     return res;
 }
 
 }  // namespace
+
+// evaluate_white_led_spectrum (internal_math.h:2501-2509) in float.
+extern "C" __attribute__((visibility("default"))) float ref_white_led(float lambda_nm) {
+    return magik::evaluate_white_led_spectrum(lambda_nm);
+}
+
+// reflect_mirror_ref for a Kerr (spin a, time-reversed) or Schwarzschild scene.
+extern "C" __attribute__((visibility("default"))) int ref_reflect_mirror(const mgk_scene* s, const float* x,
+                                                                         const float* p, const float* n, float c0,
+                                                                         float* p_out, float* c0_out) {
+    const bool tr = s->time_reversed != 0;
+    if (s->metric == MGK_METRIC_KERR) {
+        magik::kerr_metric::params_t pk{tr, 1.0f, float(tr ? -s->spin : s->spin), float(s->horizon_scalar),
+                                        float(s->h_max), float(s->abs_tol), float(s->rel_tol), s->n_max_substep};
+        reflect_mirror_ref<e_magik_spacetime_metric_types::KERR>(pk, x, p, n, c0, p_out, c0_out);
+        return 0;
+    }
+    if (s->metric == MGK_METRIC_SCHWARZSCHILD) {
+        magik::metric<e_magik_spacetime_metric_types::SCHWARZSCHILD>::params_t ps{};
+        ps.time_reversed = tr;
+        ps.mass_parameter = 1.0f;
+        ps.mass_sign = float(s->mass_sign < 0 ? -1.0 : 1.0);
+        ps.event_horizon_scalar = float(s->horizon_scalar);
+        reflect_mirror_ref<e_magik_spacetime_metric_types::SCHWARZSCHILD>(ps, x, p, n, c0, p_out, c0_out);
+        return 0;
+    }
+    return 1;
+}
 
 // Pixels [first, first + n*stride) of the scene (stride apart) rendered with
 // the reference's RKF45 step: mean XYZ per pixel into xyz_out (3 doubles per

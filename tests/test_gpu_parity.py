@@ -14,11 +14,11 @@ import pytest
 import magik_b200 as M
 from magik_b200 import abi
 from oracle import oracle_py as O
-from tests.conftest import small_scene
+from tests.conftest import room_scene, small_scene
 
 pytestmark = pytest.mark.gpu
 
-FIELDS = ["cls", "steps", "attempts", "wide_attempts", "refine_evals", "x", "p", "z", "r_hit", "dir"]
+FIELDS = ["cls", "steps", "attempts", "wide_attempts", "refine_evals", "bounces", "x", "p", "z", "r_hit", "dir"]
 
 
 def scene_for(metric, precision, **kw):
@@ -104,7 +104,7 @@ def test_render_stats_match_per_ray_records(ctx):
     assert st.attempts == int(rec["attempts"].sum())
     assert st.steps == int(rec["steps"].sum())
     assert st.refine_evals == int(rec["refine_evals"].sum())
-    counts = np.bincount(rec["cls"], minlength=5)
+    counts = np.bincount(rec["cls"], minlength=abi.RAY_CLASSES)
     assert list(st.class_count) == [int(c) for c in counts]
 
 
@@ -258,3 +258,72 @@ def test_magik_trace_geodesic_entry_point():
     # capacity mismatch is reported like the reference (magik.cpp:198-200)
     bad = abi.TraceContainer(7, 512, 0, None)
     assert M.lib().magik_trace_geodesic(bad, ic, mp, ip) == abi.ERROR_INVALID_POINTER
+
+
+# ------------------------------------------------------------------ room
+@pytest.mark.parametrize("metric", [abi.METRIC_KERR, abi.METRIC_SCHWARZSCHILD, abi.METRIC_MINKOWSKI])
+@pytest.mark.parametrize("precision", [abi.PRECISION_REF32, abi.PRECISION_MIXED, abi.PRECISION_F64])
+def test_room_trace_rays_bit_exact(ctx, metric, precision):
+    """The box-and-light scene: wall and light crossings located on the
+    geodesic, reflections in the wall's rest frame (mirror / Lambertian with
+    the ray's own random numbers), the reflection cap; every record equal to
+    the oracle's, bounces included."""
+    s = room_scene(metric=metric, spin=0.9 if metric == abi.METRIC_KERR else 0.0, precision=precision)
+    n = s.width * s.height * s.spp
+    gpu = ctx.trace_rays(s, 0, n)
+    orc = O.trace_rays(s, 0, n)
+    compare_records(gpu, orc)
+    counts = np.bincount(gpu["cls"], minlength=abi.RAY_CLASSES)
+    assert counts[abi.RAY_ALIVE] == 0 and counts[abi.RAY_LIGHT] > 0
+    assert gpu["bounces"].max() == s.room_reflection_limit + 1
+
+
+def test_room_offset_range_and_disk(ctx):
+    """A mid-frame range (the reflection random numbers follow the global ray
+    index) in a room that also holds the disk (disk hits before wall exits)."""
+    s = room_scene(disk_r_out=12.0, spp=3)
+    gpu = ctx.trace_rays(s, 1001, 777)
+    orc = O.trace_rays(s, 1001, 777)
+    compare_records(gpu, orc)
+    assert (gpu["cls"] == abi.RAY_DISK).any() and (gpu["cls"] == abi.RAY_LIGHT).any()
+
+
+@pytest.mark.parametrize("sampled", [False, True])
+@pytest.mark.parametrize("precision", [abi.PRECISION_MIXED, abi.PRECISION_F64])
+def test_room_render_film_matches_oracle(ctx, precision, sampled):
+    import torch
+    kw = dict(spectral_mode=abi.SPECTRAL_SAMPLED, n_bins=24) if sampled else {}
+    s = room_scene(precision=precision, **kw)
+    w = M.xyz_weights(s.n_bins)
+    icdf = M.cmf_inverse_cdf(s.lambda_min_nm, s.lambda_max_nm) if sampled else None
+    npix = s.width * s.height
+    film = torch.empty(npix * 3, dtype=torch.float32, device="cuda")
+    st = ctx.render(s, None, film, d_weights=torch.from_numpy(w.ravel()).cuda())
+    got = film.cpu().numpy().reshape(npix, 3).astype(np.float64)
+    ref, _ = O.render_pixels(s, np.zeros(0, M.STAR_DTYPE), w, 0, npix, icdf=icdf)
+    assert np.isfinite(got).all() and (got >= 0).all()
+    assert _film_rel_err(got, ref).max() <= 1e-4
+    assert (ref[:, 1] > 0).mean() > 0.1
+    rec = ctx.trace_rays(s, 0, npix * s.spp)
+    counts = np.bincount(rec["cls"], minlength=abi.RAY_CLASSES)
+    assert list(st.class_count) == [int(c) for c in counts]
+
+
+def test_room_scene_validation(ctx):
+    import torch
+    film = torch.empty(48 * 27 * 3, dtype=torch.float32, device="cuda")
+    bad = [dict(cam_r=60.0),                                   # camera outside the room
+           dict(cam_r=19.5, cam_incl_rad=0.0),                 # camera inside the light
+           dict(room_min=(40.0, -20.0, -40.0)),                # empty room
+           dict(light_scale=float("nan")),
+           dict(room_reflection_limit=5000)]
+    for kw in bad:
+        s = room_scene()
+        for k, v in kw.items():
+            if isinstance(v, tuple):
+                getattr(s, k)[:] = v
+            else:
+                setattr(s, k, v)
+        with pytest.raises(M.MgkError) as e:
+            ctx.render(s, None, film)
+        assert e.value.code == abi.ERROR_INVALID_ARGUMENT, kw
