@@ -328,6 +328,49 @@ def run_stress(args, ctx, d_stars, d_w, peak):
                          "frac": flop / (st.integrate_ms * 1e-3) / peak}}
 
 
+def run_room(args, ctx, d_w, peak):
+    """The reference's box-and-light stage around the Kerr a = 0.9 hole
+    (walls at x, z = +-40 M, floor and ceiling at y = -+20 M, white-LED light
+    straddling the ceiling, up to 10 reflections, mirror walls normal to x,
+    Lambertian elsewhere), camera 18 M out and 10 degrees above the equator,
+    1920x1080 at 4 spp, MIXED precision.  One warm-up and three timed frames;
+    geodesics/s (camera rays), path segments/s (rays + reflections), the
+    FP32 roofline of the integration and the oracle port on a strided sample
+    of the same frame on the host cores."""
+    import torch
+    import magik_b200 as M
+    from magik_b200 import flops as FL
+    s = M.scene_defaults(width=1920, height=1080, spp=4, room_on=1, cam_r=18.0,
+                         cam_incl_rad=80.0 * 3.141592653589793 / 180.0, disk_r_out=0.0)
+    film = torch.empty(s.width * s.height * 3, dtype=torch.float32, device=f"cuda:{ctx.device}")
+    ctx.render(s, None, film, d_weights=d_w, want_stats=False)
+    torch.cuda.synchronize()
+    reps = 3
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        st = ctx.render(s, None, film, d_weights=d_w, want_stats=True)
+    e1.record()
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    rays = s.width * s.height * s.spp
+    flop = FL.render_flops(s.metric, st.attempts, st.refine_evals)
+    out = {"workload": "room_kerr_a0.9_r18M_i80_fov60_1920x1080_4spp_32bins_10reflections",
+           "value": rays / (ms * 1e-3), "unit": UNIT, "ms_per_frame": ms, "rays": rays,
+           "segments_per_s": (rays + st.reflections) / (ms * 1e-3),
+           "reflections_per_ray": st.reflections / rays, "attempts_per_ray": st.attempts / rays,
+           "classes": dict(zip(["alive", "disk", "escaped", "horizon", "step_limit", "light"],
+                               [int(c) for c in st.class_count])),
+           "film_finite": bool(torch.isfinite(film).all().item()),
+           "roofline": {"bound": "fp32", "achieved": flop / (st.integrate_ms * 1e-3) / 1e12,
+                        "peak": peak / 1e12, "unit": "TFLOP/s", "frac": flop / (st.integrate_ms * 1e-3) / peak}}
+    if not args.no_cpu_baseline:
+        v, thr, desc = cpu_render_sample(s, np.zeros(0, M.STAR_DTYPE), M.xyz_weights(s.n_bins), 3.0,
+                                         M.abi.PRECISION_MIXED)
+        out["cpu_port"] = {"value": v, "unit": UNIT, "cores": thr, "kind": "port", "sample": desc}
+    return out
+
+
 def run_display(args, ctx):
     """The colour resolve after the film (mgk_display) over 16.8 M seeded XYZ
     pixels (403 MB moved per launch, above the 126 MB L2): the reference's
@@ -489,6 +532,7 @@ def run_gpu(args, rank, world, local_rank):
     if world == 1 and not args.no_stress:
         out["refill_stress"] = run_stress(args, ctx, d_stars, d_w, peak)
     if world == 1:
+        out["room"] = run_room(args, ctx, d_w, peak)
         out["display"] = run_display(args, ctx)
     if world == 1 and not args.no_surrogate:
         # runs after the timed region; its own timings are inside "surrogate"

@@ -195,6 +195,7 @@ typedef struct mgk_render_stats {
     uint64_t resumed;         /* rays continued by the tail kernel */
     uint64_t fallback_rays;   /* surrogate renders: rays routed to RKF45 */
     double surrogate_ms;      /* surrogate renders: device time of network + routing */
+    uint64_t reflections;     /* room scene: reflections off the walls */
 } mgk_render_stats;
 
 typedef struct mgk_context mgk_context;

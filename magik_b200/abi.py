@@ -107,7 +107,8 @@ class RenderStats(C.Structure):
                 ("wide_attempts", C.c_uint64), ("refine_evals", C.c_uint64),
                 ("class_count", C.c_uint64 * 6),
                 ("integrate_ms", C.c_double), ("total_ms", C.c_double), ("crossings", C.c_uint64),
-                ("resumed", C.c_uint64), ("fallback_rays", C.c_uint64), ("surrogate_ms", C.c_double)]
+                ("resumed", C.c_uint64), ("fallback_rays", C.c_uint64), ("surrogate_ms", C.c_double),
+                ("reflections", C.c_uint64)]
 
 
 class SampleLabel(C.Structure):

@@ -435,6 +435,7 @@ mgk_result run(mgk_context* ctx, const mgk_scene& s, const mgk_star* d_stars, ui
             stats->refine_evals += k.refine_evals;
             stats->crossings += k.refine_count + k.escape_count;
             stats->resumed += k.resume_count;
+            stats->reflections += k.reflections;
             for (int i = 0; i < MGK_RAY_CLASSES; ++i) stats->class_count[i] += k.class_count[i];
             status |= k.status;
         }
@@ -1125,6 +1126,7 @@ MGK_API mgk_result mgk_render_surrogate(mgk_context* ctx, mgk_surrogate* net, co
             stats->refine_evals += k.refine_evals;
             stats->crossings += k.refine_count + k.escape_count;
             stats->resumed += k.resume_count;
+            stats->reflections += k.reflections;
             stats->fallback_rays += k.fallback_count;
             for (int i = 0; i < MGK_RAY_CLASSES; ++i) stats->class_count[i] += k.class_count[i];
         }

@@ -16,6 +16,7 @@ struct Counters {
     unsigned long long wide_attempts;
     unsigned long long refine_evals;
     unsigned long long class_count[MGK_RAY_CLASSES];
+    unsigned long long reflections;  // room-wall reflections
     uint32_t queue_head;    // next queue index handed to a warp
     uint32_t hit_count;     // entries in the hit queue
     uint32_t refine_count;  // disk-crossing entries (from the front of the crossing queue)

@@ -580,6 +580,7 @@ __global__ void __launch_bounds__(128, MGK_REFINE_MIN_BLOCKS) k_refine(const Dev
     const uint32_t n = min(nd + min(cnt->escape_count, cap), cap);
     unsigned long long n_evals = 0;
     uint32_t n_cls[MGK_RAY_CLASSES] = {0, 0, 0, 0, 0, 0};
+    uint32_t n_refl = 0;
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t stride = gridDim.x * blockDim.x;
     // warp-uniform trip count so the queue pushes can use warp ballots;
@@ -602,6 +603,7 @@ __global__ void __launch_bounds__(128, MGK_REFINE_MIN_BLOCKS) k_refine(const Dev
             bn.ray_id = P.ray_base + e.ray;
             t = resolve<METRIC, F, T>(P, y0, y1, e.pt, e.h, e.c0, e.steps, bn, ye, evals);
             n_evals += evals - e.evals;
+            n_refl += bn.reflected ? 1u : 0u;
         }
         // a ray that goes on (candidate missed, or reflected: restart with the first step size)
         uint32_t rslot = warp_push(valid && t.cls == MGK_RAY_ALIVE, &cnt->resume_count, cap, &cnt->status);
@@ -617,6 +619,7 @@ __global__ void __launch_bounds__(128, MGK_REFINE_MIN_BLOCKS) k_refine(const Dev
         }
     }
     if (n_evals) atomicAdd(&cnt->refine_evals, n_evals);
+    if (n_refl) atomicAdd(&cnt->reflections, (unsigned long long)n_refl);
     for (int i = 1; i < MGK_RAY_CLASSES; ++i)
         if (n_cls[i]) atomicAdd(&cnt->class_count[i], (unsigned long long)n_cls[i]);
 }
@@ -638,7 +641,7 @@ __global__ void __launch_bounds__(128, 4) k_tail(const DevScene<typename ModeT<M
     const uint32_t n = min(cnt->resume_count, cap);
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
-    unsigned long long n_att = 0, n_steps = 0, n_wide = 0, n_evals = 0;
+    unsigned long long n_att = 0, n_steps = 0, n_wide = 0, n_evals = 0, n_refl = 0;
     uint32_t n_cls[MGK_RAY_CLASSES] = {0, 0, 0, 0, 0, 0};
 
     bool alive = false;
@@ -724,7 +727,10 @@ __global__ void __launch_bounds__(128, 4) k_tail(const DevScene<typename ModeT<M
                 t = resolve<METRIC, F, T>(P, y, y1, pt, h_used, c0, steps, bn, ye, evals);
                 n_evals += evals - ev0;
                 y = ye;
-                if (bn.reflected) h = P.h0;
+                if (bn.reflected) {
+                    h = P.h0;
+                    ++n_refl;
+                }
                 if (t.cls != MGK_RAY_ALIVE) done = true;
                 else if constexpr (MODE == MGK_PRECISION_MIXED)
                     r_cur = ks_r<double>(double(y.x), double(y.y), double(y.z), P.spin_d);
@@ -747,6 +753,7 @@ __global__ void __launch_bounds__(128, 4) k_tail(const DevScene<typename ModeT<M
         atomicAdd(&cnt->wide_attempts, n_wide);
     }
     if (n_evals) atomicAdd(&cnt->refine_evals, n_evals);
+    if (n_refl) atomicAdd(&cnt->reflections, n_refl);
     for (int i = 1; i < MGK_RAY_CLASSES; ++i)
         if (n_cls[i]) atomicAdd(&cnt->class_count[i], (unsigned long long)n_cls[i]);
 }

@@ -307,6 +307,8 @@ def test_room_render_film_matches_oracle(ctx, precision, sampled):
     rec = ctx.trace_rays(s, 0, npix * s.spp)
     counts = np.bincount(rec["cls"], minlength=abi.RAY_CLASSES)
     assert list(st.class_count) == [int(c) for c in counts]
+    # a ray stopped by the cap counts limit + 1 bounces but did not reflect the last time
+    assert st.reflections == int(np.minimum(rec["bounces"], s.room_reflection_limit).sum())
 
 
 def test_room_scene_validation(ctx):
