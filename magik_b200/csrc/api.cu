@@ -308,7 +308,8 @@ __global__ void k_grid_sort(const uint32_t* start, uint32_t m, uint32_t* list) {
 namespace {
 
 struct Layout {
-    size_t qx, qp, qc, hits, refine, resume, xyz, counters, g_counts, g_start, g_cursor, g_list, total;
+    size_t qx, qp, qc, hits, refine, resume, cont0, cont1, xyz, counters, g_counts, g_start, g_cursor, g_list, total;
+    bool cont;
 };
 
 Layout make_layout(const mgk_scene& s, uint32_t chunk, uint32_t n_chunks, uint32_t n_stars, uint32_t gn) {
@@ -326,6 +327,10 @@ Layout make_layout(const mgk_scene& s, uint32_t chunk, uint32_t n_chunks, uint32
     L.hits = take(size_t(chunk) * hit);
     L.refine = take(size_t(chunk) * ref);
     L.resume = take(size_t(chunk) * rsm);
+    // room scenes: two continuation queues for the integrator's reflection passes
+    L.cont = s.room_on != 0;
+    L.cont0 = take(L.cont ? size_t(chunk) * rsm : 0);
+    L.cont1 = take(L.cont ? size_t(chunk) * rsm : 0);
     L.xyz = take(size_t(chunk) * 12);
     L.counters = take(size_t(n_chunks) * sizeof(Counters));
     size_t cells = n_stars ? size_t(6) * gn * gn : 0;
@@ -407,6 +412,10 @@ mgk_result run(mgk_context* ctx, const mgk_scene& s, const mgk_star* d_stars, ui
         B.hits = at<void>(A, L.hits);
         B.refine = at<void>(A, L.refine);
         B.resume = at<void>(A, L.resume);
+        if (L.cont) {
+            B.cont[0] = at<void>(A, L.cont0);
+            B.cont[1] = at<void>(A, L.cont1);
+        }
         B.xyz_ray = ray_xyz ? ray_xyz + 3 * (b - first) : at<float>(A, L.xyz);
         B.counters = cnt_all + c;
         MGK_CUDA(ctx, launch_generate(s, table, b, m, B, st));
@@ -433,7 +442,7 @@ mgk_result run(mgk_context* ctx, const mgk_scene& s, const mgk_star* d_stars, ui
             stats->steps += k.steps;
             stats->wide_attempts += k.wide_attempts;
             stats->refine_evals += k.refine_evals;
-            stats->crossings += k.refine_count + k.escape_count;
+            stats->crossings += k.refine_count + k.escape_count + k.crossings_prev;
             stats->resumed += k.resume_count;
             stats->reflections += k.reflections;
             for (int i = 0; i < MGK_RAY_CLASSES; ++i) stats->class_count[i] += k.class_count[i];
@@ -931,6 +940,10 @@ ChunkBuffers chunk_buffers(void* A, const Layout& L, Counters* cnt) {
     B.hits = at<void>(A, L.hits);
     B.refine = at<void>(A, L.refine);
     B.resume = at<void>(A, L.resume);
+    if (L.cont) {
+        B.cont[0] = at<void>(A, L.cont0);
+        B.cont[1] = at<void>(A, L.cont1);
+    }
     B.xyz_ray = at<float>(A, L.xyz);
     B.counters = cnt;
     return B;
@@ -1124,7 +1137,7 @@ MGK_API mgk_result mgk_render_surrogate(mgk_context* ctx, mgk_surrogate* net, co
             stats->steps += k.steps;
             stats->wide_attempts += k.wide_attempts;
             stats->refine_evals += k.refine_evals;
-            stats->crossings += k.refine_count + k.escape_count;
+            stats->crossings += k.refine_count + k.escape_count + k.crossings_prev;
             stats->resumed += k.resume_count;
             stats->reflections += k.reflections;
             stats->fallback_rays += k.fallback_count;

@@ -542,19 +542,20 @@ struct Bounce {
 // thin disk (located crossing inside [r_in, r_out]) unless a room event comes
 // first on the chord, room walls and light, escape radius, horizon, step cap.
 // y_end receives the located crossing for disk, light and sky hits, and the
-// restart state after a reflection (pt and c0 then change too).
-template <int METRIC, Fuse F, class T>
+// restart state after a reflection (pt and c0 then change too).  ROOM =
+// false compiles the room tests out (scenes without the room).
+template <int METRIC, Fuse F, class T, bool ROOM>
 __device__ __forceinline__ Term<T> resolve(const DevScene<T>& P, const S7<T>& y0, const S7<T>& y1, T& pt, T h,
                                            T& c0, uint32_t steps, Bounce& bn, S7<T>& y_end, uint32_t& evals) {
     Term<T> o{MGK_RAY_ALIVE, T(0), T(0), T(0), T(0), T(0)};
     y_end = y1;
     bn.reflected = false;
     RoomEvent<T> ev{T(2), -1, 0, false};
-    if (P.room_on) {
+    if constexpr (ROOM) {
         const T a0[3] = {y0.x, y0.y, y0.z}, a1[3] = {y1.x, y1.y, y1.z};
         ev = room_chord<T>(P.room_lo, P.room_hi, P.light_lo, P.light_hi, a0, a1);
     }
-    if (disk_candidate<F, T>(P, y0, y1) && !(ev.axis >= 0 && ev.t < y0.y / (y0.y - y1.y))) {
+    if (disk_candidate<F, T>(P, y0, y1) && !(ROOM && ev.axis >= 0 && ev.t < y0.y / (y0.y - y1.y))) {
         S7<T> ys = refine<METRIC, F, T>(1, y0, y1, pt, h, T(0), P.m, evals);
         T rh = kerr_schild_r(ys.x, ys.y, ys.z, P.kerr_a);
         if (rh >= P.disk_r_in && rh <= P.disk_r_out) {
@@ -566,7 +567,7 @@ __device__ __forceinline__ Term<T> resolve(const DevScene<T>& P, const S7<T>& y0
             return o;
         }
     }
-    if (ev.axis >= 0) {
+    if (ROOM && ev.axis >= 0) {
         const T* face = ev.light ? (ev.side ? P.light_hi : P.light_lo) : (ev.side ? P.room_hi : P.room_lo);
         const S7<T> ys = ev.t > T(0) ? refine<METRIC, F, T>(ev.axis, y0, y1, pt, h, face[ev.axis], P.m, evals) : y0;
         y_end = ys;

@@ -17,6 +17,10 @@ struct Counters {
     unsigned long long refine_evals;
     unsigned long long class_count[MGK_RAY_CLASSES];
     unsigned long long reflections;  // room-wall reflections
+    unsigned long long crossings_prev;  // crossing-queue entries of earlier passes (room scenes)
+    uint32_t cont_count[2];  // room scenes: entries in the two continuation queues
+    uint32_t cont_head;      // next continuation-queue index handed to a warp
+    uint32_t pad0;
     uint32_t queue_head;    // next queue index handed to a warp
     uint32_t hit_count;     // entries in the hit queue
     uint32_t refine_count;  // disk-crossing entries (from the front of the crossing queue)
@@ -62,6 +66,7 @@ struct ChunkBuffers {
     void* hits;            // HitEntry<T>[n]
     void* refine;          // RefineEntry<T>[n]
     void* resume;          // ResumeEntry<T>[n]
+    void* cont[2] = {nullptr, nullptr};  // room scenes: ResumeEntry<T>[n] each, alternating passes
     float* xyz_ray;        // 3 floats per ray
     Counters* counters;
     const uint32_t* ray_ids = nullptr;  // queue position -> ray index (null: identity)

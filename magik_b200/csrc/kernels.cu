@@ -226,25 +226,38 @@ template <class T> __device__ __forceinline__ S7<T> s7(const T* v) {
 
 // -------------------------------------------------------------- integrate
 // Persistent: every warp loops until the queue is drained.  A lane whose
-// step ends near the disk plane crossing or beyond the escape radius hands
-// the step to the crossing queue; in MIXED mode a lane entering the FP64
-// band hands its ray to the resume queue.  Both pushes are warp-ballot
-// compactions with one atomic per warp.
-template <int METRIC, int MODE>
+// step ends near the disk plane crossing, beyond the escape radius or (room
+// scene) outside the room or near the light hands the step to the crossing
+// queue; in MIXED mode a lane entering the FP64 band hands its ray to the
+// resume queue.  Both pushes are warp-ballot compactions with one atomic per
+// warp.
+//  KIND 0: the camera-ray queue (qx, qp, qc; nq rays), no room.
+//  KIND 1: the camera-ray queue of a room scene (room pre-test on).
+//  KIND 2: a room scene's continuation queue of whole ray states (rays
+//          reflected by the previous pass's crossing kernel), cont_in with
+//          cnt->cont_count[sel] entries; nq is then only the chunk's queue
+//          capacity.
+template <int METRIC, int MODE, int KIND>
 __global__ void __launch_bounds__(kIntegrateThreads, MODE == MGK_PRECISION_F64 ? kIntegrateMinBlocksF64 : MGK_INTEGRATE_MIN_BLOCKS)
     k_integrate(const DevScene<typename ModeT<MODE>::T> P, uint32_t nq, const void* __restrict__ qx,
                 const void* __restrict__ qp, const void* __restrict__ qc,
                 RefineEntry<typename ModeT<MODE>::T>* refq, ResumeEntry<typename ModeT<MODE>::T>* resq,
-                mgk_ray_result* res, Counters* cnt, const uint32_t* __restrict__ ray_ids) {
+                mgk_ray_result* res, Counters* cnt, const uint32_t* __restrict__ ray_ids,
+                const ResumeEntry<typename ModeT<MODE>::T>* __restrict__ cont_in, uint32_t sel) {
     using T = typename ModeT<MODE>::T;
     constexpr Fuse F = ModeT<MODE>::F;
+    constexpr bool CONT = KIND == 2, ROOM = KIND != 0;
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
+    // rays in the input queue; its head counter
+    const uint32_t n_in = CONT ? min(cnt->cont_count[sel], nq) : nq;
+    uint32_t* const head = CONT ? &cnt->cont_head : &cnt->queue_head;
 
     bool alive = false;
     S7<T> y{};
     T pt = 0, c0 = 0, h = 0;
     uint32_t ray = 0, steps = 0, tries = 0, att = 0;
+    uint32_t evals = 0, bounces = 0;  // carried by continued rays (zero for camera rays)
     uint32_t cbeg = 0, cend = 0;
     bool drained = false;
     uint32_t n_att = 0, n_steps = 0;  // per lane: below 2^32 (a lane runs at most max_steps x n_max per ray)
@@ -260,14 +273,14 @@ __global__ void __launch_bounds__(kIntegrateThreads, MODE == MGK_PRECISION_F64 ?
             uint32_t nb = 0, ne = 0;
             if (need > rem && !drained) {
                 uint32_t got = 0;
-                if (lane == 0) got = atomicAdd(&cnt->queue_head, kChunk);
+                if (lane == 0) got = atomicAdd(head, kChunk);
                 got = __shfl_sync(kFull, got, 0);
-                if (got >= nq) {
+                if (got >= n_in) {
                     drained = true;
                 } else {
                     nb = got;
-                    ne = min(got + kChunk, nq);
-                    if (ne == nq) drained = true;
+                    ne = min(got + kChunk, n_in);
+                    if (ne == n_in) drained = true;
                 }
             }
             if (!alive) {
@@ -276,15 +289,23 @@ __global__ void __launch_bounds__(kIntegrateThreads, MODE == MGK_PRECISION_F64 ?
                 if (rank < rem) idx = cbeg + rank;
                 else if (rank - rem < ne - nb) idx = nb + (rank - rem);
                 if (idx != ~0u) {
-                    T a[4], b[4];
-                    q_load(qx, idx, a);
-                    q_load(qp, idx, b);
-                    y = S7<T>{a[0], a[1], a[2], a[3], b[0], b[1], b[2]};
-                    pt = b[3];
-                    c0 = reinterpret_cast<const T*>(qc)[idx];
-                    h = P.h0;
-                    ray = ray_ids ? ray_ids[idx] : idx;
-                    steps = 0; tries = 0; att = 0;
+                    if constexpr (CONT) {
+                        const ResumeEntry<T> e = cont_in[idx];
+                        y = s7(e.y);
+                        pt = e.pt; c0 = e.c0; h = e.h;
+                        ray = e.ray; steps = e.steps; att = e.attempts; evals = e.evals; bounces = e.bounces;
+                    } else {
+                        T a[4], b[4];
+                        q_load(qx, idx, a);
+                        q_load(qp, idx, b);
+                        y = S7<T>{a[0], a[1], a[2], a[3], b[0], b[1], b[2]};
+                        pt = b[3];
+                        c0 = reinterpret_cast<const T*>(qc)[idx];
+                        h = P.h0;
+                        ray = ray_ids ? ray_ids[idx] : idx;
+                        steps = 0; att = 0;
+                    }
+                    tries = 0;
                     alive = true;
                     if constexpr (MODE == MGK_PRECISION_MIXED && METRIC != MGK_METRIC_MINKOWSKI)
                         to_band = in_band(P, y.x, y.y, y.z);
@@ -318,7 +339,8 @@ __global__ void __launch_bounds__(kIntegrateThreads, MODE == MGK_PRECISION_F64 ?
                 ++steps; ++n_steps;
                 y = y1;
                 T r2 = radius2<F>(y1);
-                disk = disk_candidate<F, T>(P, y0, y1) || room_candidate<T>(P, y0, y1);
+                disk = disk_candidate<F, T>(P, y0, y1);
+                if constexpr (ROOM) disk = disk || room_candidate<T>(P, y0, y1);
                 cross = disk || r2 >= P.escape_r2;
                 if (!cross) {
                     cls = plain_terminal<METRIC, F, T>(P, y1, r2, steps);
@@ -335,7 +357,7 @@ __global__ void __launch_bounds__(kIntegrateThreads, MODE == MGK_PRECISION_F64 ?
         if (cls != MGK_RAY_ALIVE) {
             if (res) {
                 Term<T> t{cls, T(0), T(0), T(0), T(0), T(0)};
-                write_result<T>(res, ray, y, pt, t, steps, att, MODE == MGK_PRECISION_F64 ? att : 0u, 0u, 0u);
+                write_result<T>(res, ray, y, pt, t, steps, att, MODE == MGK_PRECISION_F64 ? att : 0u, evals, bounces);
             }
             ++n_cls[cls];
         }
@@ -353,12 +375,12 @@ __global__ void __launch_bounds__(kIntegrateThreads, MODE == MGK_PRECISION_F64 ?
                 e.pt = pt; e.h = h_used; e.h_next = h; e.c0 = c0;
                 e.ray = ray; e.steps = steps; e.attempts = att;
                 e.wide = MODE == MGK_PRECISION_F64 ? att : 0u;
-                e.evals = 0; e.bounces = 0; e.pad[0] = e.pad[1] = 0;
+                e.evals = evals; e.bounces = bounces; e.pad[0] = e.pad[1] = 0;
                 refq[slot] = e;
             }
             if constexpr (MODE == MGK_PRECISION_MIXED) {
                 uint32_t bslot = warp_push(to_band, &cnt->resume_count, nq, &cnt->status);
-                if (bslot != ~0u) store_resume<T>(resq, bslot, y, pt, h, c0, ray, steps, att, 0u, 0u, 0u);
+                if (bslot != ~0u) store_resume<T>(resq, bslot, y, pt, h, c0, ray, steps, att, 0u, evals, bounces);
             }
         }
         if (cls != MGK_RAY_ALIVE || cross || to_band) alive = false;
@@ -565,15 +587,18 @@ __global__ void __launch_bounds__(kIntegrateThreads, MGK_X2_MIN_BLOCKS)
 }
 
 // -------------------------------------------------------------- crossings
-// One thread per handed-off step: locate the disk / escape crossing, then
-// emit the hit, or send the ray on to the tail kernel when the disk
-// candidate missed and nothing else ended it.
-template <int METRIC, int MODE>
+// One thread per handed-off step: locate the disk / escape / room crossing,
+// then emit the hit, or send the ray on when nothing ended it (a disk or
+// light candidate that missed, a reflected ray): to the continuation queue
+// contq (room scenes, counted by *cont_count) for the next integrator pass,
+// else to the tail kernel's resume queue.
+template <int METRIC, int MODE, bool ROOM>
 __global__ void __launch_bounds__(128, MGK_REFINE_MIN_BLOCKS) k_refine(const DevScene<typename ModeT<MODE>::T> P,
                                                 const RefineEntry<typename ModeT<MODE>::T>* __restrict__ refq,
                                                 uint32_t cap, HitEntry<typename ModeT<MODE>::T>* hits,
                                                 ResumeEntry<typename ModeT<MODE>::T>* resq, mgk_ray_result* res,
-                                                Counters* cnt, uint32_t hit_cap) {
+                                                Counters* cnt, uint32_t hit_cap,
+                                                ResumeEntry<typename ModeT<MODE>::T>* contq, uint32_t* cont_count) {
     using T = typename ModeT<MODE>::T;
     constexpr Fuse F = ModeT<MODE>::F;
     const uint32_t nd = min(cnt->refine_count, cap);
@@ -601,14 +626,16 @@ __global__ void __launch_bounds__(128, MGK_REFINE_MIN_BLOCKS) k_refine(const Dev
             evals = e.evals;
             bn.count = e.bounces;
             bn.ray_id = P.ray_base + e.ray;
-            t = resolve<METRIC, F, T>(P, y0, y1, e.pt, e.h, e.c0, e.steps, bn, ye, evals);
+            t = resolve<METRIC, F, T, ROOM>(P, y0, y1, e.pt, e.h, e.c0, e.steps, bn, ye, evals);
             n_evals += evals - e.evals;
             n_refl += bn.reflected ? 1u : 0u;
         }
         // a ray that goes on (candidate missed, or reflected: restart with the first step size)
-        uint32_t rslot = warp_push(valid && t.cls == MGK_RAY_ALIVE, &cnt->resume_count, cap, &cnt->status);
+        ResumeEntry<T>* const oq = contq ? contq : resq;
+        uint32_t rslot = warp_push(valid && t.cls == MGK_RAY_ALIVE, contq ? cont_count : &cnt->resume_count, cap,
+                                   &cnt->status);
         if (rslot != ~0u)
-            store_resume<T>(resq, rslot, ye, e.pt, bn.reflected ? P.h0 : e.h_next, e.c0, e.ray, e.steps, e.attempts,
+            store_resume<T>(oq, rslot, ye, e.pt, bn.reflected ? P.h0 : e.h_next, e.c0, e.ray, e.steps, e.attempts,
                             e.wide, evals, bn.count);
         bool lit = valid && (t.cls == MGK_RAY_DISK || t.cls == MGK_RAY_ESCAPED || t.cls == MGK_RAY_LIGHT);
         uint32_t hslot = warp_push(lit, &cnt->hit_count, hit_cap, &cnt->status);
@@ -624,6 +651,18 @@ __global__ void __launch_bounds__(128, MGK_REFINE_MIN_BLOCKS) k_refine(const Dev
         if (n_cls[i]) atomicAdd(&cnt->class_count[i], (unsigned long long)n_cls[i]);
 }
 
+// Between two integrator passes of a room scene: the crossing queue's counts
+// go into the running total and restart at zero, as do the continuation
+// queue's head and the count of the queue the next pass's crossings write.
+__global__ void k_next_pass(Counters* cnt, uint32_t next_sel) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    cnt->crossings_prev += (unsigned long long)cnt->refine_count + cnt->escape_count;
+    cnt->refine_count = 0;
+    cnt->escape_count = 0;
+    cnt->cont_head = 0;
+    cnt->cont_count[next_sel] = 0;
+}
+
 // ------------------------------------------------------------------- tail
 // Resumed rays (MIXED rays inside the FP64 band, rays whose disk candidate
 // missed), run to termination.  Persistent like k_integrate: every lane
@@ -631,7 +670,7 @@ __global__ void __launch_bounds__(128, MGK_REFINE_MIN_BLOCKS) k_refine(const Dev
 // finished lanes from the resume queue in chunks, so that no lane waits for
 // the longest ray of its warp.  MIXED mode: FP64 attempts while within
 // MGK_WIDE_BAND of r_plus, FP32 otherwise.
-template <int METRIC, int MODE>
+template <int METRIC, int MODE, bool ROOM>
 __global__ void __launch_bounds__(128, 4) k_tail(const DevScene<typename ModeT<MODE>::T> P,
                                               const ResumeEntry<typename ModeT<MODE>::T>* __restrict__ resq,
                                               uint32_t cap, HitEntry<typename ModeT<MODE>::T>* hits,
@@ -724,7 +763,7 @@ __global__ void __launch_bounds__(128, 4) k_tail(const DevScene<typename ModeT<M
                 ++steps; ++n_steps;
                 S7<T> ye;
                 const uint32_t ev0 = evals;
-                t = resolve<METRIC, F, T>(P, y, y1, pt, h_used, c0, steps, bn, ye, evals);
+                t = resolve<METRIC, F, T, ROOM>(P, y, y1, pt, h_used, c0, steps, bn, ye, evals);
                 n_evals += evals - ev0;
                 y = ye;
                 if (bn.reflected) {
@@ -774,7 +813,9 @@ __global__ void __launch_bounds__(128, 4) k_tail(const DevScene<typename ModeT<M
 //    irradiance (device_color_utilities.cuh:22-29), spread over the bins by
 //    the Gaussian CDF differences at the bin edges
 //    (kernel_redistribute_radiance.cu:55-92).
-template <class T>
+//  ROOM: the scene has the room's light (a separate instantiation, so that
+//    scenes without it run the disk and star code alone).
+template <class T, bool ROOM>
 __global__ void __launch_bounds__(256) k_shade(const DevScene<T> P, const HitEntry<T>* __restrict__ hits,
                                                uint32_t cap, const Counters* cnt, const mgk_star* __restrict__ stars,
                                                StarGridDev grid, const float* __restrict__ d_w,
@@ -830,7 +871,7 @@ __global__ void __launch_bounds__(256) k_shade(const DevScene<T> P, const HitEnt
         if (h.cls == MGK_RAY_DISK) {
             // T(r) = T_in (r / r_in)^(-3/4)
             add(T(1), P.disk_T_in * exp2(T(-0.75) * log2(h.r_hit / P.disk_r_in)));
-        } else if (h.cls == MGK_RAY_LIGHT) {
+        } else if (ROOM && h.cls == MGK_RAY_LIGHT) {
             // white LED at the shifted wavelength, boosted by z^5
             // (matter_examples.cuh:67-76, bxdf_utilities.cuh:156-163)
             const T z2 = h.z * h.z, z5 = z2 * z2 * h.z;
@@ -1317,21 +1358,29 @@ cudaError_t launch_generate(const mgk_scene& s, const void* dev_scene, uint64_t 
     }
 }
 
-template <int METRIC, int MODE>
+template <int METRIC, int MODE, bool ROOM>
 static cudaError_t integ_t(const void* dsc, uint64_t first, uint32_t n, const ChunkBuffers& b, mgk_ray_result* res,
                            int sms, cudaStream_t st) {
     using T = typename ModeT<MODE>::T;
     DevScene<T> P = ds<T>(dsc);
     P.ray_base = first;
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_integrate<METRIC, MODE>, kIntegrateThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_integrate<METRIC, MODE, 0>, kIntegrateThreads, 0);
     if (per_sm < 1) per_sm = 1;
-    uint32_t blocks = uint32_t(sms * per_sm);
+    const uint32_t full = uint32_t(sms * per_sm);
+    uint32_t blocks = full;
     uint32_t need = (n + kIntegrateThreads - 1) / kIntegrateThreads;
     if (blocks > need) blocks = need;
     auto* refq = reinterpret_cast<RefineEntry<T>*>(b.refine);
     auto* resq = reinterpret_cast<ResumeEntry<T>*>(b.resume);
     auto* hits = reinterpret_cast<HitEntry<T>*>(b.hits);
+    ResumeEntry<T>* cont[2] = {reinterpret_cast<ResumeEntry<T>*>(b.cont[0]),
+                               reinterpret_cast<ResumeEntry<T>*>(b.cont[1])};
+    // room scenes with continuation queues: reflected rays go back through
+    // the integrator, one pass per reflection (plus one for rays whose light
+    // candidate missed); the last pass's crossing kernel sends what still
+    // goes on to the tail kernel
+    const uint32_t passes = (ROOM && cont[0] && cont[1]) ? P.room_limit + 1u : 0u;
     if constexpr (MGK_MIXED_X2 && MODE == MGK_PRECISION_MIXED && METRIC != MGK_METRIC_MINKOWSKI) {
         // two rays per thread: half the threads for the same rays
         per_sm = 0;
@@ -1343,33 +1392,52 @@ static cudaError_t integ_t(const void* dsc, uint64_t first, uint32_t n, const Ch
         k_integrate_x2<METRIC><<<blocks, kIntegrateThreads, 0, st>>>(P, n, b.qx, b.qp, b.qc, refq, resq, res,
                                                                      b.counters, b.ray_ids);
     } else {
-        k_integrate<METRIC, MODE><<<blocks, kIntegrateThreads, 0, st>>>(P, n, b.qx, b.qp, b.qc, refq, resq,
-                                                                       res, b.counters, b.ray_ids);
+        k_integrate<METRIC, MODE, ROOM ? 1 : 0><<<blocks, kIntegrateThreads, 0, st>>>(
+            P, n, b.qx, b.qp, b.qc, refq, resq, res, b.counters, b.ray_ids, nullptr, 0u);
     }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     const uint32_t hit_cap = b.hit_cap ? b.hit_cap : n;
     int refine_per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&refine_per_sm, k_refine<METRIC, MODE>, 128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&refine_per_sm, k_refine<METRIC, MODE, ROOM>, 128, 0);
     if (refine_per_sm < 1) refine_per_sm = 1;
-    k_refine<METRIC, MODE><<<sms * refine_per_sm * 2, 128, 0, st>>>(P, refq, n, hits, resq, res, b.counters,
-                                                                   hit_cap);
+    const uint32_t refine_blocks = uint32_t(sms * refine_per_sm * 2);
+    // pass p reads continuation queue p & 1 and its crossings write queue (p + 1) & 1
+    k_refine<METRIC, MODE, ROOM><<<refine_blocks, 128, 0, st>>>(P, refq, n, hits, resq, res, b.counters, hit_cap,
+                                                          passes ? cont[1] : nullptr, &b.counters->cont_count[1]);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
+    for (uint32_t p = 1; p <= passes; ++p) {
+        const uint32_t in = p & 1u, out = (p + 1u) & 1u;
+        k_next_pass<<<1, 32, 0, st>>>(b.counters, out);
+        k_integrate<METRIC, MODE, ROOM ? 2 : 0><<<full, kIntegrateThreads, 0, st>>>(
+            P, n, nullptr, nullptr, nullptr, refq, resq, res, b.counters, nullptr, cont[in], in);
+        k_refine<METRIC, MODE, ROOM><<<refine_blocks, 128, 0, st>>>(P, refq, n, hits, resq, res, b.counters, hit_cap,
+                                                              p < passes ? cont[out] : nullptr,
+                                                              &b.counters->cont_count[out]);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
     int tail_per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tail_per_sm, k_tail<METRIC, MODE>, 128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tail_per_sm, k_tail<METRIC, MODE, ROOM>, 128, 0);
     if (tail_per_sm < 1) tail_per_sm = 1;
-    k_tail<METRIC, MODE><<<sms * tail_per_sm, 128, 0, st>>>(P, resq, n, hits, res, b.counters, hit_cap);
+    k_tail<METRIC, MODE, ROOM><<<sms * tail_per_sm, 128, 0, st>>>(P, resq, n, hits, res, b.counters, hit_cap);
     return cudaGetLastError();
 }
 
 template <int MODE>
-static cudaError_t integ_m(int metric, const void* dsc, uint64_t first, uint32_t n, const ChunkBuffers& b,
+static cudaError_t integ_m(int metric, bool room, const void* dsc, uint64_t first, uint32_t n, const ChunkBuffers& b,
                            mgk_ray_result* res, int sms, cudaStream_t st) {
     switch (metric) {
-        case MGK_METRIC_KERR: return integ_t<MGK_METRIC_KERR, MODE>(dsc, first, n, b, res, sms, st);
-        case MGK_METRIC_SCHWARZSCHILD: return integ_t<MGK_METRIC_SCHWARZSCHILD, MODE>(dsc, first, n, b, res, sms, st);
-        default: return integ_t<MGK_METRIC_MINKOWSKI, MODE>(dsc, first, n, b, res, sms, st);
+        case MGK_METRIC_KERR:
+            return room ? integ_t<MGK_METRIC_KERR, MODE, true>(dsc, first, n, b, res, sms, st)
+                        : integ_t<MGK_METRIC_KERR, MODE, false>(dsc, first, n, b, res, sms, st);
+        case MGK_METRIC_SCHWARZSCHILD:
+            return room ? integ_t<MGK_METRIC_SCHWARZSCHILD, MODE, true>(dsc, first, n, b, res, sms, st)
+                        : integ_t<MGK_METRIC_SCHWARZSCHILD, MODE, false>(dsc, first, n, b, res, sms, st);
+        default:
+            return room ? integ_t<MGK_METRIC_MINKOWSKI, MODE, true>(dsc, first, n, b, res, sms, st)
+                        : integ_t<MGK_METRIC_MINKOWSKI, MODE, false>(dsc, first, n, b, res, sms, st);
     }
 }
 
@@ -1377,10 +1445,19 @@ cudaError_t launch_integrate(const mgk_scene& s, const void* dsc, uint64_t first
                              mgk_ray_result* res, int sms, cudaStream_t st) {
     if (n == 0) return cudaSuccess;
     switch (s.precision) {
-        case MGK_PRECISION_REF32: return integ_m<MGK_PRECISION_REF32>(s.metric, dsc, first, n, b, res, sms, st);
-        case MGK_PRECISION_MIXED: return integ_m<MGK_PRECISION_MIXED>(s.metric, dsc, first, n, b, res, sms, st);
-        default: return integ_m<MGK_PRECISION_F64>(s.metric, dsc, first, n, b, res, sms, st);
+        case MGK_PRECISION_REF32:
+            return integ_m<MGK_PRECISION_REF32>(s.metric, s.room_on != 0, dsc, first, n, b, res, sms, st);
+        case MGK_PRECISION_MIXED:
+            return integ_m<MGK_PRECISION_MIXED>(s.metric, s.room_on != 0, dsc, first, n, b, res, sms, st);
+        default: return integ_m<MGK_PRECISION_F64>(s.metric, s.room_on != 0, dsc, first, n, b, res, sms, st);
     }
+}
+
+template <class T, bool ROOM>
+static void shade_t(const void* dsc, uint64_t first, uint32_t n, const ChunkBuffers& b, const mgk_star* stars,
+                    StarGridDev grid, const float* d_w, float* film_spec, uint32_t blocks, cudaStream_t st) {
+    k_shade<T, ROOM><<<blocks, 256, 0, st>>>(ds<T>(dsc), reinterpret_cast<const HitEntry<T>*>(b.hits), n, b.counters,
+                                             stars, grid, d_w, b.xyz_ray, film_spec, first);
 }
 
 cudaError_t launch_shade(const mgk_scene& s, const void* dsc, uint64_t first, uint32_t n, const ChunkBuffers& b,
@@ -1388,12 +1465,14 @@ cudaError_t launch_shade(const mgk_scene& s, const void* dsc, uint64_t first, ui
                          cudaStream_t st) {
     if (n == 0) return cudaSuccess;
     uint32_t blocks = uint32_t(sms) * 8u;
-    if (s.precision == MGK_PRECISION_F64)
-        k_shade<double><<<blocks, 256, 0, st>>>(ds<double>(dsc), reinterpret_cast<const HitEntry<double>*>(b.hits),
-                                                n, b.counters, stars, grid, d_w, b.xyz_ray, film_spec, first);
-    else
-        k_shade<float><<<blocks, 256, 0, st>>>(ds<float>(dsc), reinterpret_cast<const HitEntry<float>*>(b.hits), n,
-                                               b.counters, stars, grid, d_w, b.xyz_ray, film_spec, first);
+    const bool room = s.room_on != 0;
+    if (s.precision == MGK_PRECISION_F64) {
+        if (room) shade_t<double, true>(dsc, first, n, b, stars, grid, d_w, film_spec, blocks, st);
+        else shade_t<double, false>(dsc, first, n, b, stars, grid, d_w, film_spec, blocks, st);
+    } else {
+        if (room) shade_t<float, true>(dsc, first, n, b, stars, grid, d_w, film_spec, blocks, st);
+        else shade_t<float, false>(dsc, first, n, b, stars, grid, d_w, film_spec, blocks, st);
+    }
     return cudaGetLastError();
 }
 
