@@ -139,6 +139,17 @@ typedef struct mgk_scene {
     double room_min[3], room_max[3];    /* (-40, -20, -40), (40, 20, 40) */
     double light_min[3], light_max[3];  /* (-20, 19, -20), (20, 21, 20) */
     double light_scale;                 /* white-LED spectral radiance scale, 7e5 */
+    /* Explicit camera (cam_explicit = 1) in place of the orbit camera
+     * (cam_r, cam_incl_rad): position and orientation as the reference's
+     * optical_system_settings hold them (optical_system_settings.h:33-34),
+     * in units of M; the observer moves with proper velocity cam_velocity
+     * (units of c) relative to the reference observer, in its tetrad with
+     * seeds x, y, z (rest_frame_four_velocity, relativity_utilities.cuh:163-173). */
+    uint32_t cam_explicit;
+    uint32_t reserved_cam;
+    double cam_pos[3];
+    double cam_axes[9];      /* columns right, up, back (the camera looks along -back) */
+    double cam_velocity[3];
 } mgk_scene;
 
 #define MGK_MAX_BINS 64
@@ -181,6 +192,8 @@ typedef struct mgk_ray_result {
     uint32_t bounces;       /* reflections off the room's walls */
 } mgk_ray_result;
 
+#define MGK_PASS_HISTORY 16
+
 /* Counters of one render. */
 typedef struct mgk_render_stats {
     uint64_t rays;
@@ -196,6 +209,16 @@ typedef struct mgk_render_stats {
     uint64_t fallback_rays;   /* surrogate renders: rays routed to RKF45 */
     double surrogate_ms;      /* surrogate renders: device time of network + routing */
     uint64_t reflections;     /* room scene: reflections off the walls */
+    /* Per integrator pass (room scenes run one pass per reflection; other
+     * scenes one pass), summed over the render's chunks; passes past
+     * MGK_PASS_HISTORY - 1 are added into the last entry. */
+    uint32_t n_passes;
+    uint32_t reserved_passes;
+    uint64_t pass_rays[MGK_PASS_HISTORY];       /* rays entering the pass */
+    uint64_t pass_crossings[MGK_PASS_HISTORY];  /* steps handed to the crossing kernel */
+    uint64_t pass_hits[MGK_PASS_HISTORY];       /* rays ending on an emitter (disk, sky, light) */
+    uint64_t pass_continued[MGK_PASS_HISTORY];  /* rays going on to the next pass */
+    uint64_t pass_to_tail[MGK_PASS_HISTORY];    /* rays handed to the tail kernel */
 } mgk_render_stats;
 
 typedef struct mgk_context mgk_context;

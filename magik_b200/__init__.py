@@ -431,3 +431,8 @@ def render_surrogate(ctx, net, scene, d_stars, d_film_xyz, conf_min=0.99, crit_f
                                     d_film_xyz.data_ptr(), C.byref(st), _stream_ptr(stream))
     _check(rc, "mgk_render_surrogate", ctx.handle)
     return st
+
+
+# the reference's render-manager API and the stage helpers (include/mgk_manager.h)
+from . import manager  # noqa: E402
+EXPORTS = EXPORTS + manager.MANAGER_EXPORTS

@@ -21,6 +21,7 @@ RAY_CLASSES = 6
 CLASS_NAMES = {0: "alive", 1: "disk", 2: "escaped", 3: "horizon", 4: "step_limit", 5: "light"}
 MASSIVE, MASSLESS = 0, 1
 MAX_BINS = 64
+PASS_HISTORY = 16
 SPECTRAL_BINS, SPECTRAL_SAMPLED = 0, 1
 CMF_ICDF_ENTRIES = 256
 WIDE_BAND = 0.05
@@ -44,6 +45,8 @@ class Scene(C.Structure):
         ("room_on", C.c_uint32), ("room_reflection_limit", C.c_uint32),
         ("room_min", C.c_double * 3), ("room_max", C.c_double * 3),
         ("light_min", C.c_double * 3), ("light_max", C.c_double * 3), ("light_scale", C.c_double),
+        ("cam_explicit", C.c_uint32), ("reserved_cam", C.c_uint32), ("cam_pos", C.c_double * 3),
+        ("cam_axes", C.c_double * 9), ("cam_velocity", C.c_double * 3),
     ]
 
     def copy(self):
@@ -108,7 +111,10 @@ class RenderStats(C.Structure):
                 ("class_count", C.c_uint64 * 6),
                 ("integrate_ms", C.c_double), ("total_ms", C.c_double), ("crossings", C.c_uint64),
                 ("resumed", C.c_uint64), ("fallback_rays", C.c_uint64), ("surrogate_ms", C.c_double),
-                ("reflections", C.c_uint64)]
+                ("reflections", C.c_uint64), ("n_passes", C.c_uint32), ("reserved_passes", C.c_uint32),
+                ("pass_rays", C.c_uint64 * PASS_HISTORY), ("pass_crossings", C.c_uint64 * PASS_HISTORY),
+                ("pass_hits", C.c_uint64 * PASS_HISTORY), ("pass_continued", C.c_uint64 * PASS_HISTORY),
+                ("pass_to_tail", C.c_uint64 * PASS_HISTORY)]
 
 
 class SampleLabel(C.Structure):
@@ -157,7 +163,7 @@ class TraceContainer(C.Structure):
                 ("steps", C.POINTER(TraceStep))]
 
 
-assert C.sizeof(Scene) == 328, C.sizeof(Scene)
+assert C.sizeof(Scene) == 456, C.sizeof(Scene)
 assert C.sizeof(Star) == 32
 assert C.sizeof(RayResult) == 128
 assert C.sizeof(TraceStep) == 60

@@ -16,8 +16,10 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmgk.so")
-SOURCES = ["kernels.cu", "api.cu", "static_scratch.cu", "mlp.cu", "mlp_tc.cu", "surrogate.cu", "display.cu"]
-HEADERS = ["dev_physics.cuh", "dev_pair.cuh", "dev_scene.cuh", "internal.h", os.path.join("..", "..", "include", "mgk.h")]
+SOURCES = ["kernels.cu", "api.cu", "static_scratch.cu", "mlp.cu", "mlp_tc.cu", "surrogate.cu", "display.cu",
+           "manager.cu"]
+HEADERS = ["dev_physics.cuh", "dev_pair.cuh", "dev_scene.cuh", "internal.h", os.path.join("..", "..", "include", "mgk.h"),
+           os.path.join("..", "..", "include", "mgk_manager.h")]
 
 NVCC_FLAGS = [
     "-std=c++17", "-O3", "-lineinfo",

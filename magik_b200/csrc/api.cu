@@ -76,8 +76,30 @@ mgk_result validate(const mgk_scene* s) {
     if (!(s->escape_radius > 0.0) || !(s->lambda_max_nm > s->lambda_min_nm) || !(s->lambda_min_nm > 0.0))
         return MGK_ERROR_INVALID_ARGUMENT;
     if (s->disk_r_out > 0.0 && !(s->disk_r_in > 0.0 && s->disk_r_in < s->disk_r_out)) return MGK_ERROR_INVALID_ARGUMENT;
-    if (!(s->focal_length_mm > 0.0) || !(s->sensor_diag_mm > 0.0) || !(s->cam_r > 0.0))
+    if (!(s->focal_length_mm > 0.0) || !(s->sensor_diag_mm > 0.0) || !(s->cam_explicit || s->cam_r > 0.0))
         return MGK_ERROR_INVALID_ARGUMENT;
+    if (s->cam_explicit > 1u) return MGK_ERROR_INVALID_ARGUMENT;
+    // the camera position (M)
+    double cam[3] = {0.0, s->cam_r * std::cos(s->cam_incl_rad), s->cam_r * std::sin(s->cam_incl_rad)};
+    if (s->cam_explicit) {
+        // finite position and velocity, orthonormal axes, outside the capture radius
+        const double* A = s->cam_axes;
+        for (int i = 0; i < 3; ++i) {
+            cam[i] = s->cam_pos[i];
+            if (!std::isfinite(cam[i]) || !std::isfinite(s->cam_velocity[i])) return MGK_ERROR_INVALID_ARGUMENT;
+            for (int j = 0; j < 3; ++j) {
+                const double d = A[3 * i] * A[3 * j] + A[3 * i + 1] * A[3 * j + 1] + A[3 * i + 2] * A[3 * j + 2];
+                if (!(std::fabs(d - (i == j ? 1.0 : 0.0)) <= 1e-6)) return MGK_ERROR_INVALID_ARGUMENT;
+            }
+        }
+        if (s->metric != MGK_METRIC_MINKOWSKI) {
+            const double a = s->metric == MGK_METRIC_KERR ? s->spin : 0.0;
+            const double R = cam[0] * cam[0] + cam[1] * cam[1] + cam[2] * cam[2] - a * a;
+            const double r = std::sqrt(0.5 * R + 0.5 * std::sqrt(R * R + 4.0 * a * a * cam[1] * cam[1]));
+            const double rh = (1.0 + std::sqrt(std::fmax(0.0, 1.0 - a * a))) * s->horizon_scalar;
+            if (!(r > rh)) return MGK_ERROR_INVALID_ARGUMENT;
+        }
+    }
     if (!(s->star_radius_rad > 0.0 && s->star_radius_rad <= 0.02)) return MGK_ERROR_INVALID_ARGUMENT;
     if (s->spectral_mode > MGK_SPECTRAL_SAMPLED) return MGK_UNKNOWN_ENUM_TYPE;
     if (s->spectral_mode == MGK_SPECTRAL_SAMPLED &&
@@ -94,7 +116,7 @@ mgk_result validate(const mgk_scene* s) {
                 return MGK_ERROR_INVALID_ARGUMENT;
         if (!(s->light_scale >= 0.0 && std::isfinite(s->light_scale)) || s->room_reflection_limit > 1024u)
             return MGK_ERROR_INVALID_ARGUMENT;
-        const double q[3] = {0.0, s->cam_r * std::cos(s->cam_incl_rad), s->cam_r * std::sin(s->cam_incl_rad)};
+        const double* q = cam;
         bool in_room = true, in_light = true;
         for (int a = 0; a < 3; ++a) {
             in_room = in_room && q[a] > s->room_min[a] && q[a] < s->room_max[a];
@@ -312,6 +334,33 @@ struct Layout {
     bool cont;
 };
 
+// Adds one chunk's per-pass record (m rays) to the render statistics: the
+// passes k_next_pass recorded, then the last pass from the final counts (its
+// hits include the tail kernel's).
+void add_pass_history(mgk_render_stats* st, const Counters& k, uint32_t m) {
+    const uint32_t recorded = std::min<uint32_t>(k.n_hist, MGK_PASS_HISTORY);
+    const uint32_t last = std::min<uint32_t>(k.n_hist, MGK_PASS_HISTORY - 1);
+    uint64_t cross[MGK_PASS_HISTORY] = {}, cont[MGK_PASS_HISTORY] = {}, hit[MGK_PASS_HISTORY] = {},
+             res[MGK_PASS_HISTORY] = {};
+    for (uint32_t e = 0; e < recorded; ++e) {
+        cross[e] = k.hist[e][0];
+        cont[e] = k.hist[e][1];
+        hit[e] = k.hist[e][2];
+        res[e] = k.hist[e][3];
+    }
+    cross[last] += uint64_t(k.refine_count) + k.escape_count;
+    hit[last] = k.hit_count;
+    res[last] = k.resume_count;
+    for (uint32_t e = 0; e <= last; ++e) {
+        st->pass_rays[e] += e == 0 ? m : cont[e - 1];
+        st->pass_crossings[e] += cross[e];
+        st->pass_hits[e] += hit[e] - (e ? hit[e - 1] : 0);
+        st->pass_continued[e] += cont[e];
+        st->pass_to_tail[e] += res[e] - (e ? res[e - 1] : 0);
+    }
+    st->n_passes = std::max<uint32_t>(st->n_passes, k.n_hist + 1u);
+}
+
 Layout make_layout(const mgk_scene& s, uint32_t chunk, uint32_t n_chunks, uint32_t n_stars, uint32_t gn) {
     const size_t T = s.precision == MGK_PRECISION_F64 ? 8 : 4;
     const bool f64 = s.precision == MGK_PRECISION_F64;
@@ -437,6 +486,8 @@ mgk_result run(mgk_context* ctx, const mgk_scene& s, const mgk_star* d_stars, ui
         std::memset(stats, 0, sizeof(*stats));
         stats->rays = n;
         uint32_t status = 0;
+        for (uint32_t c = 0; c < n_chunks; ++c)
+            add_pass_history(stats, h[c], uint32_t(std::min<uint64_t>(chunk, first + n - (first + uint64_t(c) * chunk))));
         for (auto& k : h) {
             stats->attempts += k.attempts;
             stats->steps += k.steps;
@@ -472,6 +523,7 @@ mgk_context* g_default[64] = {};
 
 namespace mgk {
 int context_device(mgk_context* ctx) { return ctx->device; }
+size_t context_device_bytes(mgk_context* ctx) { return ctx->arena_bytes + ctx->stage_bytes; }
 // Scene checks shared with the allocation-free entry point (static_scratch.cu).
 mgk_result validate_scene(const mgk_scene* s) { return validate(s); }
 }  // namespace mgk
@@ -962,7 +1014,8 @@ MGK_API mgk_result mgk_make_samples(mgk_context* ctx, const mgk_scene* base, uin
     mgk_result rc = validate(&s0);
     if (rc != MGK_SUCCESS) return rc;
     if (n_spin_buckets > 1024 || (n_spin_buckets && s0.escape_radius < 100.0)) return MGK_ERROR_INVALID_ARGUMENT;
-    if (s0.room_on) return MGK_ERROR_INVALID_ARGUMENT;  // the surrogate learns sky directions only
+    // the surrogate learns sky directions seen by the orbit camera's observer
+    if (s0.room_on || s0.cam_explicit) return MGK_ERROR_INVALID_ARGUMENT;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     MGK_CUDA(ctx, cudaSetDevice(ctx->device));
     const uint32_t chunk = std::min(n, kSampleChunk);
@@ -1039,7 +1092,8 @@ MGK_API mgk_result mgk_render_surrogate(mgk_context* ctx, mgk_surrogate* net, co
     mgk_result rc = validate(&s);
     if (rc != MGK_SUCCESS) return rc;
     if (s.precision == MGK_PRECISION_REF32) return MGK_ERROR_INVALID_ARGUMENT;
-    if (s.room_on) return MGK_ERROR_INVALID_ARGUMENT;  // the surrogate learns sky directions only
+    // the surrogate learns sky directions seen by the orbit camera's observer
+    if (s.room_on || s.cam_explicit) return MGK_ERROR_INVALID_ARGUMENT;
     if (n_stars && !d_stars) return MGK_ERROR_INVALID_POINTER;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     MGK_CUDA(ctx, cudaSetDevice(ctx->device));

@@ -144,10 +144,26 @@ inline SceneConsts scene_consts(const mgk_scene& s) {
     const double ms = s.mass_sign < 0 ? -1.0 : 1.0;
     double ci = std::cos(s.cam_incl_rad), si = std::sin(s.cam_incl_rad);
     V4<double> q{0.0, s.cam_r * ci, s.cam_r * si, 0.0};
-    c.cam_pos[0] = q.x; c.cam_pos[1] = q.y; c.cam_pos[2] = q.z; c.cam_pos[3] = q.t;
     V4<double> X{1, 0, 0, 0}, Y{0, si, -ci, 0}, Z{0, ci, si, 0};  // right, up, back
+    if (s.cam_explicit) {
+        q = V4<double>{s.cam_pos[0], s.cam_pos[1], s.cam_pos[2], 0.0};
+        X = V4<double>{s.cam_axes[0], s.cam_axes[1], s.cam_axes[2], 0.0};
+        Y = V4<double>{s.cam_axes[3], s.cam_axes[4], s.cam_axes[5], 0.0};
+        Z = V4<double>{s.cam_axes[6], s.cam_axes[7], s.cam_axes[8], 0.0};
+    }
+    c.cam_pos[0] = q.x; c.cam_pos[1] = q.y; c.cam_pos[2] = q.z; c.cam_pos[3] = q.t;
     V4<double> u = reference_observer<double>(metric, q.x, q.y, q.z, a, ms);
     Sym4<double> g = compute_g<double>(metric, q.x, q.y, q.z, a, ms);
+    const double* v = s.cam_velocity;
+    if (s.cam_explicit && (v[0] != 0.0 || v[1] != 0.0 || v[2] != 0.0)) {
+        // rest_frame_four_velocity (relativity_utilities.cuh:163-173): the proper
+        // velocity in the reference observer's tetrad, flipped when time reversed
+        Tetrad<double> e0 = build_tetrad<double>(g, V4<double>{1, 0, 0, 0}, V4<double>{0, 1, 0, 0},
+                                                 V4<double>{0, 0, 1, 0}, u);
+        const double f = s.time_reversed ? -1.0 : 1.0;
+        const double wx = f * v[0], wy = f * v[1], wz = f * v[2];
+        u = local_to_global<double>(e0, V4<double>{wx, wy, wz, std::sqrt(wx * wx + wy * wy + wz * wz + 1.0)});
+    }
     Tetrad<double> e = build_tetrad<double>(g, X, Y, Z, u);
     V4<double> cols[4] = {contract(g, e.x), contract(g, e.y), contract(g, e.z), contract(g, e.t)};
     for (int j = 0; j < 4; ++j) {

@@ -20,7 +20,10 @@ struct Counters {
     unsigned long long crossings_prev;  // crossing-queue entries of earlier passes (room scenes)
     uint32_t cont_count[2];  // room scenes: entries in the two continuation queues
     uint32_t cont_head;      // next continuation-queue index handed to a warp
-    uint32_t pad0;
+    uint32_t n_hist;         // passes recorded in hist
+    // per finished pass (k_next_pass): crossings, continued rays, and the hit
+    // and resume counts so far
+    uint32_t hist[MGK_PASS_HISTORY][4];
     uint32_t queue_head;    // next queue index handed to a warp
     uint32_t hit_count;     // entries in the hit queue
     uint32_t refine_count;  // disk-crossing entries (from the front of the crossing queue)
@@ -102,6 +105,8 @@ cudaError_t launch_route(const mgk_scene& s, const void* dev_scene, uint32_t bas
 cudaError_t surrogate_infer(mgk_surrogate* net, const float* feat, uint32_t n, float* out, cudaStream_t stream);
 uint32_t surrogate_status(mgk_surrogate* net);
 int context_device(mgk_context* ctx);
+size_t context_device_bytes(mgk_context* ctx);  // scratch arena and staging
+mgk_result validate_scene(const mgk_scene* s);   // mgk_render's scene checks
 cudaError_t launch_fma_probe(uint32_t blocks, uint32_t iters, float* sink, cudaStream_t stream);
 cudaError_t launch_check_rounding(int sm_count, unsigned long long* out, cudaStream_t stream);
 cudaError_t launch_trace_geodesic(const void* jobs, uint32_t n, void* steps, uint32_t* written, cudaStream_t stream);

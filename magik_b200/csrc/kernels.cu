@@ -656,6 +656,13 @@ __global__ void __launch_bounds__(128, MGK_REFINE_MIN_BLOCKS) k_refine(const Dev
 // queue's head and the count of the queue the next pass's crossings write.
 __global__ void k_next_pass(Counters* cnt, uint32_t next_sel) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    // the finished pass's record (the continuation queue it wrote is the other one)
+    const uint32_t k = min(cnt->n_hist, uint32_t(MGK_PASS_HISTORY - 1));
+    cnt->hist[k][0] += cnt->refine_count + cnt->escape_count;
+    cnt->hist[k][1] += cnt->cont_count[next_sel ^ 1u];
+    cnt->hist[k][2] = cnt->hit_count;
+    cnt->hist[k][3] = cnt->resume_count;
+    cnt->n_hist += 1u;
     cnt->crossings_prev += (unsigned long long)cnt->refine_count + cnt->escape_count;
     cnt->refine_count = 0;
     cnt->escape_count = 0;

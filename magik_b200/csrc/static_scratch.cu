@@ -31,8 +31,6 @@
 
 namespace mgk {
 
-mgk_result validate_scene(const mgk_scene* s);
-
 namespace {
 
 constexpr uint32_t kStaticMaxRays = 16384;

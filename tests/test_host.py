@@ -15,8 +15,10 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def header_functions():
-    text = open(os.path.join(ROOT, "include", "mgk.h")).read()
-    names = re.findall(r"MGK_API\s+[\w\s\*]+?\b(\w+)\s*\(", text)
+    names = []
+    for h in ("mgk.h", "mgk_manager.h"):
+        text = open(os.path.join(ROOT, "include", h)).read()
+        names += re.findall(r"MGK_API\s+[\w\s\*]+?\b(\w+)\s*\(", text)
     return sorted(set(names))
 
 
