@@ -19,6 +19,12 @@ namespace mgk {
 
 enum class Fuse { None, Fma };
 
+// 1: FP32 operations of the MIXED attempt that come in pairs run as f32x2
+// instructions (one issue slot per pair, each half rounded as the scalar).
+#ifndef MGK_PACKED_AXPY
+#define MGK_PACKED_AXPY 1
+#endif
+
 template <Fuse F> __device__ __forceinline__ float mad(float a, float b, float c) {
     if constexpr (F == Fuse::Fma) return __fmaf_rn(a, b, c);
     else return __fadd_rn(__fmul_rn(a, b), c);
@@ -232,6 +238,9 @@ __device__ __forceinline__ void rhs_schwarzschild(const S7<T>& s, T pt, T mass_s
 // so that with F = f (k.p), Ad = F/d, B = (k.p)^2 dq - F c y, Q = Ad G' + B and
 // E = F c r - (k.p)^2 2 a^2 r^3 y / f_den^2:
 //      dp_i/dl = Q dr_i + Ad U'_i + delta_iy E.
+// FP32 operations taken in f32x2 pairs (same rounding per half as the scalar form).
+template <class T> constexpr bool kPackFloat = MGK_PACKED_AXPY != 0 && sizeof(T) == 4;
+
 template <class T> __device__ __forceinline__ void rhs_kerr_fused(const S7<T>& s, T pt, const MP<T>& m, S7<T>& o) {
     constexpr Fuse F = Fuse::Fma;
     const T x = s.x, y = s.y, z = s.z, px = s.px, py = s.py, pz = s.pz;
@@ -246,22 +255,47 @@ template <class T> __device__ __forceinline__ void rhs_kerr_fused(const S7<T>& s
     const T rs = r * sigma;
     const T rsd = rs * d;
     const T inv_all = fused_rcp(rsd * f_den);  // ~r^9: finite for r below ~1.9e4 in float
-    const T inv_rsd = f_den * inv_all;
-    const T inv_fden = rsd * inv_all;
-    const T inv_d = rs * inv_rsd;
-    const T inv_rs = d * inv_rsd;
-    const T inv_r = sigma * inv_rs;
-    const T sxz = r_sq * inv_rs;
-    const T drx = x * sxz, dry = y * (d * inv_rs), drz = z * sxz;
+    T inv_rsd, inv_fden, inv_d, inv_rs, inv_r, sxz;
+    if constexpr (kPackFloat<T>) {  // products that share a factor, in pairs
+        const float2 p1 = __fmul2_rn(make_float2(f_den, rsd), make_float2(inv_all, inv_all));
+        inv_rsd = p1.x; inv_fden = p1.y;
+        const float2 p2 = __fmul2_rn(make_float2(rs, d), make_float2(inv_rsd, inv_rsd));
+        inv_d = p2.x; inv_rs = p2.y;
+        const float2 p3 = __fmul2_rn(make_float2(sigma, r_sq), make_float2(inv_rs, inv_rs));
+        inv_r = p3.x; sxz = p3.y;
+    } else {
+        inv_rsd = f_den * inv_all;
+        inv_fden = rsd * inv_all;
+        inv_d = rs * inv_rsd;
+        inv_rs = d * inv_rsd;
+        inv_r = sigma * inv_rs;
+        sxz = r_sq * inv_rs;
+    }
+    T drx, drz, kx, kz;
+    const T dry = y * (d * inv_rs);
     const T r_cu = r_sq * r;
     const T f_ = (T(2) * r_cu) * inv_fden;
     const T kx_num = mad<F>(r, x, -(a * z));
     const T kz_num = mad<F>(r, z, a * x);
-    const T kx = kx_num * inv_d, kz = kz_num * inv_d, ky = y * inv_r;
+    if constexpr (kPackFloat<T>) {  // (x, z) pairs: one f32x2 multiply for two
+        const float2 dr = __fmul2_rn(make_float2(x, z), make_float2(sxz, sxz));
+        const float2 kk = __fmul2_rn(make_float2(kx_num, kz_num), make_float2(inv_d, inv_d));
+        drx = dr.x; drz = dr.y; kx = kk.x; kz = kk.y;
+    } else {
+        drx = x * sxz; drz = z * sxz;
+        kx = kx_num * inv_d; kz = kz_num * inv_d;
+    }
+    const T ky = y * inv_r;
     const T S = mad<F>(pz, kz, px * kx);
     const T kTp = mad<F>(py, ky, S) - pt;
-    const T f_kTp = f_ * kTp;
-    const T kTp2 = kTp * kTp;
+    T f_kTp, kTp2;
+    if constexpr (kPackFloat<T>) {
+        const float2 p4 = __fmul2_rn(make_float2(f_, kTp), make_float2(kTp, kTp));
+        f_kTp = p4.x; kTp2 = p4.y;
+    } else {
+        f_kTp = f_ * kTp;
+        kTp2 = kTp * kTp;
+    }
     const T two_r = r + r;
     const T Gp = mad<F>(-two_r, S, mad<F>(pz, z, px * x));
     const T Ad = f_kTp * inv_d;
@@ -274,13 +308,21 @@ template <class T> __device__ __forceinline__ void rhs_kerr_fused(const S7<T>& s
     const T B = mad<F>(kTp2, dq, -(f_kTp * cy));
     const T E = mad<F>(-kTp2, ((m.two_a_sq * r_cu) * y) * inv_fden_sq, f_kTp * (c * r));
     const T Q = mad<F>(Ad, Gp, B);
-    o.x = mad<F>(-f_kTp, kx, px);
+    if constexpr (kPackFloat<T>) {
+        const float2 nf = make_float2(-f_kTp, -f_kTp);
+        const float2 oxz = __ffma2_rn(nf, make_float2(kx, kz), make_float2(px, pz));
+        const float2 au = __fmul2_rn(make_float2(Ad, Ad), make_float2(Ux, Uz));
+        const float2 opxz = __ffma2_rn(make_float2(Q, Q), make_float2(drx, drz), au);
+        o.x = oxz.x; o.z = oxz.y; o.px = opxz.x; o.pz = opxz.y;
+    } else {
+        o.x = mad<F>(-f_kTp, kx, px);
+        o.z = mad<F>(-f_kTp, kz, pz);
+        o.px = mad<F>(Q, drx, Ad * Ux);
+        o.pz = mad<F>(Q, drz, Ad * Uz);
+    }
     o.y = mad<F>(-f_kTp, ky, py);
-    o.z = mad<F>(-f_kTp, kz, pz);
     o.t = f_kTp - pt;
-    o.px = mad<F>(Q, drx, Ad * Ux);
     o.py = mad<F>(Q, dry, E);
-    o.pz = mad<F>(Q, drz, Ad * Uz);
 }
 
 // Schwarzschild, fused formulation: with a = 0, k = x/r, f = 2 m/r,
@@ -292,19 +334,34 @@ __device__ __forceinline__ void rhs_schwarzschild_fused(const S7<T>& s, T pt, T 
     const T x = s.x, y = s.y, z = s.z, px = s.px, py = s.py, pz = s.pz;
     const T r = fused_sqrt(mad<F>(z, z, mad<F>(y, y, x * x)));
     const T inv_r = fused_rcp(r);
-    const T kx = x * inv_r, ky = y * inv_r, kz = z * inv_r;
+    T kx, kz;
+    if constexpr (kPackFloat<T>) {
+        const float2 k = __fmul2_rn(make_float2(x, z), make_float2(inv_r, inv_r));
+        kx = k.x; kz = k.y;
+    } else {
+        kx = x * inv_r; kz = z * inv_r;
+    }
+    const T ky = y * inv_r;
     const T kp = mad<F>(pz, kz, mad<F>(py, ky, px * kx));
     const T kTp = kp - pt;
     const T fk = ((mass_sign * T(2)) * inv_r) * kTp;
-    o.x = mad<F>(-fk, kx, px);
-    o.y = mad<F>(-fk, ky, py);
-    o.z = mad<F>(-fk, kz, pz);
-    o.t = fk - pt;
     const T sc = fk * inv_r;
     const T q = mad<F>(T(0.5), kTp, kp);
-    o.px = sc * mad<F>(-kx, q, px);
+    if constexpr (kPackFloat<T>) {
+        // fma(-k, q, p) == fma(k, -q, p): negation is exact
+        const float2 K = make_float2(kx, kz), P = make_float2(px, pz);
+        const float2 oxz = __ffma2_rn(make_float2(-fk, -fk), K, P);
+        const float2 opxz = __fmul2_rn(make_float2(sc, sc), __ffma2_rn(K, make_float2(-q, -q), P));
+        o.x = oxz.x; o.z = oxz.y; o.px = opxz.x; o.pz = opxz.y;
+    } else {
+        o.x = mad<F>(-fk, kx, px);
+        o.z = mad<F>(-fk, kz, pz);
+        o.px = sc * mad<F>(-kx, q, px);
+        o.pz = sc * mad<F>(-kz, q, pz);
+    }
+    o.y = mad<F>(-fk, ky, py);
+    o.t = fk - pt;
     o.py = sc * mad<F>(-ky, q, py);
-    o.pz = sc * mad<F>(-kz, q, pz);
 }
 
 // Minkowski, metric_minkowski.cuh:8-13.
@@ -368,6 +425,20 @@ template <Fuse F, class T> __device__ __forceinline__ S7<T> axpy(T c, const S7<T
     return S7<T>{mad<F>(c, k.x, y.x), mad<F>(c, k.y, y.y), mad<F>(c, k.z, y.z), mad<F>(c, k.t, y.t),
                  mad<F>(c, k.px, y.px), mad<F>(c, k.py, y.py), mad<F>(c, k.pz, y.pz)};
 }
+#if MGK_PACKED_AXPY
+// The FP32 fused form as three packed f32x2 FMAs and one scalar: each half
+// rounds exactly as fmaf, for one issue slot per pair (the integrator is
+// bound by instruction issue).  The pairs (x, z) and (px, pz) are the ones
+// the fused Kerr RHS also works on.
+template <> __device__ __forceinline__ S7<float> axpy<Fuse::Fma, float>(float c, const S7<float>& k,
+                                                                        const S7<float>& y) {
+    const float2 cc = make_float2(c, c);
+    const float2 xz = __ffma2_rn(cc, make_float2(k.x, k.z), make_float2(y.x, y.z));
+    const float2 pxz = __ffma2_rn(cc, make_float2(k.px, k.pz), make_float2(y.px, y.pz));
+    const float2 yt = __ffma2_rn(cc, make_float2(k.y, k.t), make_float2(y.y, y.t));
+    return S7<float>{xz.x, yt.x, xz.y, yt.y, pxz.x, __fmaf_rn(c, k.py, y.py), pxz.y};
+}
+#endif
 template <class T> __device__ __forceinline__ S7<T> scl(T c, const S7<T>& k) {
     return S7<T>{c * k.x, c * k.y, c * k.z, c * k.t, c * k.px, c * k.py, c * k.pz};
 }
