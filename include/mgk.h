@@ -63,9 +63,10 @@ typedef int32_t mgk_result;
  *  REF32 - FP32 state and FP32 step control in the reference's exact operation
  *          order (no fused multiply-add): the kernels reproduce the reference
  *          CPU tracer's steps bit for bit.
- *  MIXED - FP32 state with fused multiply-add, FP64 error estimate and step
- *          control, whole attempts in FP64 within MGK_WIDE_BAND of the outer
- *          horizon.  The production mode.
+ *  MIXED - FP32 state with fused multiply-add, the step's error estimate
+ *          formed over the stage differences (exact cancellation of their
+ *          common part), whole attempts in FP64 within MGK_WIDE_BAND of the
+ *          outer horizon.  The production mode.
  *  F64   - FP64 everywhere (the accuracy reference run on the GPU). */
 #define MGK_PRECISION_REF32 0
 #define MGK_PRECISION_MIXED 1

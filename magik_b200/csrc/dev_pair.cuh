@@ -166,13 +166,23 @@ __device__ __forceinline__ void rkf45_stages_x2(const S7<F2>& y0, F2 pt, F2 h, c
                axpy2(ch(-C::b5, h), k[4], axpy2(ch(C::b4, h), k[3], axpy2(ch(C::b3, h), k[2], axpy2(ch(C::b1, h), k[0], y0)))));
 }
 
-// The unscaled FP64 error estimate of one slot (rkf45_error_unscaled of the
-// stages converted to double), rounded back to float.
+// The unscaled error estimate of one slot: rkf45_error_delta (or, with
+// MGK_MIXED_ERR_F32 = 0, rkf45_error_unscaled of the stages converted to
+// double, rounded back to float).
+// With MGK_MIXED_ERR_F32 the slot's estimate is rkf45_error_delta, as in the
+// one-ray kernel.
 template <int S> __device__ __forceinline__ S7<float> error_f64_slot(const S7<F2> k[6]) {
+#if MGK_MIXED_ERR_F32
+    S7<float> ks[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) ks[i] = slot_of<S>(k[i]);
+    return rkf45_error_delta(ks);
+#else
     S7<double> kd[6];
 #pragma unroll
     for (int i = 0; i < 6; ++i) kd[i] = cvt<double>(slot_of<S>(k[i]));
     return cvt<float>(rkf45_error_unscaled<double>(kd));
+#endif
 }
 
 // rcp_norm of both halves: the seed is integer arithmetic per half, the
@@ -183,7 +193,7 @@ __device__ __forceinline__ F2 rcp_norm2(F2 x) {
     return mul2(y, fma2(neg2(x), y, b2(2.0f)));
 }
 
-// control_mixed for two rays: FP64 error estimate per slot, packed norm,
+// control_mixed for two rays: the error estimate per slot, packed norm,
 // proposal per slot.
 __device__ __forceinline__ void control_mixed_x2(const S7<F2>& y0, const S7<F2>& y1, const S7<F2> k[6], F2 h,
                                                  const MP<float>& m, F2& h_next, bool ok[2]) {

@@ -575,15 +575,42 @@ template <class T> __device__ __forceinline__ S7<T> rkf45_error_unscaled(const S
                            axpy<Fuse::Fma>(C::e3, k[2], scl(C::e1, k[0])))));
 }
 
-// MIXED control: the error estimate (whose terms cancel badly in FP32) is
-// formed in FP64 from the FP32 stages; its norm and the proposal need only a
-// few digits and run in FP32.
+// The unscaled error estimate in FP32 over the stage differences: the
+// Fehlberg error weights sum to zero (-1/360 + 128/4275 + 2197/75240 - 1/50
+// - 2/55 = 0), so E = sum_j e_j (k_j - k_1).  Written this way the common
+// part of the stages cancels exactly (the differences are formed first, each
+// rounded relative to itself), and the FP32 rounding left in E is of order
+// 2^-24 h |dk/dlambda| instead of 2^-24 |k|: far below any tolerance the
+// step control works to.  The pairs run as f32x2 instructions.
+__device__ __forceinline__ S7<float> rkf45_error_delta(const S7<float> k[6]) {
+    using C = FB<float>;
+    auto dif = [](const S7<float>& a, const S7<float>& b) {
+        const float2 xz = __fadd2_rn(make_float2(a.x, a.z), make_float2(-b.x, -b.z));
+        const float2 pxz = __fadd2_rn(make_float2(a.px, a.pz), make_float2(-b.px, -b.pz));
+        const float2 yt = __fadd2_rn(make_float2(a.y, a.t), make_float2(-b.y, -b.t));
+        return S7<float>{xz.x, yt.x, xz.y, yt.y, pxz.x, a.py - b.py, pxz.y};
+    };
+    const S7<float> d3 = dif(k[2], k[0]), d4 = dif(k[3], k[0]), d5 = dif(k[4], k[0]), d6 = dif(k[5], k[0]);
+    return axpy<Fuse::Fma>(-C::e6, d6, axpy<Fuse::Fma>(-C::e5, d5, axpy<Fuse::Fma>(C::e4, d4, scl(C::e3, d3))));
+}
+
+// MIXED control: the error estimate (whose terms cancel badly when summed
+// directly in FP32) over the stage differences in FP32 (MGK_MIXED_ERR_F32,
+// the default) or summed directly in FP64; its norm and the proposal need
+// only a few digits and run in FP32.
+#ifndef MGK_MIXED_ERR_F32
+#define MGK_MIXED_ERR_F32 1
+#endif
 __device__ __forceinline__ void control_mixed(const S7<float>& y0, const S7<float>& y1, const S7<float> k[6],
                                               float h, const MP<float>& m, float& h_next, bool& ok) {
+#if MGK_MIXED_ERR_F32
+    S7<float> e = rkf45_error_delta(k);
+#else
     S7<double> kd[6];
 #pragma unroll
     for (int i = 0; i < 6; ++i) kd[i] = cvt<double>(k[i]);
     S7<float> e = cvt<float>(rkf45_error_unscaled<double>(kd));
+#endif
     float err = rms_error_mixed(e, y0, y1, h, m.abs_tol, m.rel_tol);
     float safe = err > 1e-30f ? err : 1e-30f;
     float hn = (0.9f * h) * inv_root5(safe);

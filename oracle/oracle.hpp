@@ -557,13 +557,36 @@ template <class T> inline GState<T> rkf45_error_unscaled(const GState<T> k[6]) {
                            axpy<Fuse::Fma>(C::e3, k[2], scale(C::e1, k[0])))));
 }
 
-// MIXED control: the error estimate in double from the float stages; its
-// norm and the proposal in float.
+// The unscaled estimate in float over the stage differences: the error
+// weights sum to zero, so E = e3 (k3 - k1) + e4 (k4 - k1) - e5 (k5 - k1)
+// - e6 (k6 - k1); the differences first, then the weighted sum with fma.
+inline GState<float> rkf45_error_delta(const GState<float> k[6]) {
+    using C = Fehlberg<float>;
+    auto dif = [](const GState<float>& a, const GState<float>& b) {
+        GState<float> d;
+        d.x = V4<float>{a.x.x - b.x.x, a.x.y - b.x.y, a.x.z - b.x.z, a.x.t - b.x.t};
+        d.p = V4<float>{a.p.x - b.p.x, a.p.y - b.p.y, a.p.z - b.p.z, a.p.t - b.p.t};
+        return d;
+    };
+    const GState<float> d3 = dif(k[2], k[0]), d4 = dif(k[3], k[0]), d5 = dif(k[4], k[0]), d6 = dif(k[5], k[0]);
+    return axpy<Fuse::Fma>(-C::e6, d6, axpy<Fuse::Fma>(-C::e5, d5, axpy<Fuse::Fma>(C::e4, d4, scale(C::e3, d3))));
+}
+
+// MIXED control: the error estimate over the stage differences in float
+// (rkf45_error_delta; summed directly in double when MGK_MIXED_ERR_F32 is 0);
+// its norm and the proposal in float.
+#ifndef MGK_MIXED_ERR_F32
+#define MGK_MIXED_ERR_F32 1
+#endif
 inline void control_mixed(const GState<float>& y0, const GState<float>& y1, const GState<float> k[6], float h,
                           const MetricParams<float>& m, float* h_next, bool* ok) {
+#if MGK_MIXED_ERR_F32
+    GState<float> e = rkf45_error_delta(k);
+#else
     GState<double> kd[6];
     for (int i = 0; i < 6; ++i) kd[i] = to_double(k[i]);
     GState<float> e = widen<float>(rkf45_error_unscaled<double>(kd));
+#endif
     float err = rms_error_mixed(e, y0, y1, h, m.abs_tol, m.rel_tol);
     float safe = err > 1e-30f ? err : 1e-30f;
     float hn = (0.9f * h) * inv_root5(safe);

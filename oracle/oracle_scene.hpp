@@ -15,7 +15,7 @@
 //    white-LED light (matter_examples.cuh:60-77, internal_math.h:2441-2509)
 //  * spectral -> XYZ with per-bin CMF weights (device_color_utilities.cuh:40-54)
 //
-// The "mixed" precision mode (FP32 state, FP64 step control, FP64 attempts
+// The "mixed" precision mode (FP32 state and step control, FP64 attempts
 // within 0.05 M of the outer horizon) is defined here exactly as the CUDA
 // kernels implement it, so that the two can be compared bit for bit.
 #pragma once
