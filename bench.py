@@ -34,7 +34,7 @@ sys.path.insert(0, ROOT)
 # ncu capture each of a smaller case (profiles/k_integrate_kerr_640x360x16.md,
 # profiles/k_mlp_infer_tc_1M_rows.md); the traffic grows with the units, so
 # the roofline scales it to the launch.
-INTEGRATE_DRAM_BYTES_PER_RAY = 613.4e6 / 3_686_400
+INTEGRATE_DRAM_BYTES_PER_RAY = 617.4e6 / 3_686_400
 MLP_DRAM_BYTES_PER_ROW = 44.2e6 / 1_048_576
 N_STARS = 100_000
 STAR_SEED = 0x57A25
