@@ -329,3 +329,26 @@ def test_room_scene_validation(ctx):
         with pytest.raises(M.MgkError) as e:
             ctx.render(s, None, film)
         assert e.value.code == abi.ERROR_INVALID_ARGUMENT, kw
+
+
+def test_render_pass_histories(ctx):
+    """Per-pass statistics: one pass without the room; with it, one pass per
+    reflection plus one, rays carried from each pass to the next, hits summing
+    to the emitter classes, crossings and tail hand-offs summing to the totals."""
+    import torch
+    s = small_scene()
+    film = torch.empty(s.width * s.height * 3, dtype=torch.float32, device="cuda")
+    st = ctx.render(s, None, film)
+    n = s.width * s.height * s.spp
+    assert st.n_passes == 1 and st.pass_rays[0] == n and st.pass_continued[0] == 0
+    assert st.pass_to_tail[0] == st.resumed and st.pass_crossings[0] == st.crossings
+    r = room_scene()
+    st = ctx.render(r, None, film)
+    L = r.room_reflection_limit
+    assert st.n_passes == L + 2 and st.pass_rays[0] == n
+    for p in range(st.n_passes - 1):
+        assert st.pass_rays[p + 1] == st.pass_continued[p]
+    cls = st.class_count
+    assert sum(st.pass_hits[:st.n_passes]) == cls[abi.RAY_LIGHT] + cls[abi.RAY_DISK] + cls[abi.RAY_ESCAPED]
+    assert sum(st.pass_crossings[:st.n_passes]) == st.crossings
+    assert sum(st.pass_to_tail[:st.n_passes]) == st.resumed
