@@ -64,6 +64,11 @@ __device__ __forceinline__ float rcp_approx(float b) {
     asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(b));
     return y;
 }
+__device__ __forceinline__ float ex2_approx(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
 __device__ __forceinline__ float msqrt(float a) {
     a = fmaxf(a, kSqrtFloor);
     const float y = rsqrt_approx(a);
