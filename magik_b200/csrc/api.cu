@@ -376,10 +376,11 @@ Layout make_layout(const mgk_scene& s, uint32_t chunk, uint32_t n_chunks, uint32
     L.hits = take(size_t(chunk) * hit);
     L.refine = take(size_t(chunk) * ref);
     L.resume = take(size_t(chunk) * rsm);
-    // room scenes: two continuation queues for the integrator's reflection passes
+    // continuation queues of the integrator's extra passes: two in room
+    // scenes (one pass per reflection), one otherwise (the disk misses)
     L.cont = s.room_on != 0;
     L.cont0 = take(L.cont ? size_t(chunk) * rsm : 0);
-    L.cont1 = take(L.cont ? size_t(chunk) * rsm : 0);
+    L.cont1 = take(size_t(chunk) * rsm);
     L.xyz = take(size_t(chunk) * 12);
     L.counters = take(size_t(n_chunks) * sizeof(Counters));
     size_t cells = n_stars ? size_t(6) * gn * gn : 0;
@@ -461,10 +462,8 @@ mgk_result run(mgk_context* ctx, const mgk_scene& s, const mgk_star* d_stars, ui
         B.hits = at<void>(A, L.hits);
         B.refine = at<void>(A, L.refine);
         B.resume = at<void>(A, L.resume);
-        if (L.cont) {
-            B.cont[0] = at<void>(A, L.cont0);
-            B.cont[1] = at<void>(A, L.cont1);
-        }
+        if (L.cont) B.cont[0] = at<void>(A, L.cont0);
+        B.cont[1] = at<void>(A, L.cont1);
         B.xyz_ray = ray_xyz ? ray_xyz + 3 * (b - first) : at<float>(A, L.xyz);
         B.counters = cnt_all + c;
         MGK_CUDA(ctx, launch_generate(s, table, b, m, B, st));
@@ -992,10 +991,8 @@ ChunkBuffers chunk_buffers(void* A, const Layout& L, Counters* cnt) {
     B.hits = at<void>(A, L.hits);
     B.refine = at<void>(A, L.refine);
     B.resume = at<void>(A, L.resume);
-    if (L.cont) {
-        B.cont[0] = at<void>(A, L.cont0);
-        B.cont[1] = at<void>(A, L.cont1);
-    }
+    if (L.cont) B.cont[0] = at<void>(A, L.cont0);
+    B.cont[1] = at<void>(A, L.cont1);
     B.xyz_ray = at<float>(A, L.xyz);
     B.counters = cnt;
     return B;

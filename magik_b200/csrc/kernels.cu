@@ -38,6 +38,11 @@
 namespace mgk {
 
 constexpr unsigned kFull = 0xffffffffu;
+// 1: scenes without the room continue disk-miss rays in one more pass of the
+// persistent integrator instead of the tail kernel.
+#ifndef MGK_MISS_PASS
+#define MGK_MISS_PASS 1
+#endif
 #ifndef MGK_INTEGRATE_THREADS
 #define MGK_INTEGRATE_THREADS 128
 #endif
@@ -237,6 +242,8 @@ template <class T> __device__ __forceinline__ S7<T> s7(const T* v) {
 //          reflected by the previous pass's crossing kernel), cont_in with
 //          cnt->cont_count[sel] entries; nq is then only the chunk's queue
 //          capacity.
+//  KIND 3: the continuation queue of a scene without the room (rays whose
+//          disk candidate missed the disk).
 template <int METRIC, int MODE, int KIND>
 __global__ void __launch_bounds__(kIntegrateThreads, MODE == MGK_PRECISION_F64 ? kIntegrateMinBlocksF64 : MGK_INTEGRATE_MIN_BLOCKS)
     k_integrate(const DevScene<typename ModeT<MODE>::T> P, uint32_t nq, const void* __restrict__ qx,
@@ -246,7 +253,7 @@ __global__ void __launch_bounds__(kIntegrateThreads, MODE == MGK_PRECISION_F64 ?
                 const ResumeEntry<typename ModeT<MODE>::T>* __restrict__ cont_in, uint32_t sel) {
     using T = typename ModeT<MODE>::T;
     constexpr Fuse F = ModeT<MODE>::F;
-    constexpr bool CONT = KIND == 2, ROOM = KIND != 0;
+    constexpr bool CONT = KIND >= 2, ROOM = KIND == 1 || KIND == 2;
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
     // rays in the input queue; its head counter
@@ -1394,11 +1401,14 @@ static cudaError_t integ_t(const void* dsc, uint64_t first, uint32_t n, const Ch
     auto* hits = reinterpret_cast<HitEntry<T>*>(b.hits);
     ResumeEntry<T>* cont[2] = {reinterpret_cast<ResumeEntry<T>*>(b.cont[0]),
                                reinterpret_cast<ResumeEntry<T>*>(b.cont[1])};
-    // room scenes with continuation queues: reflected rays go back through
-    // the integrator, one pass per reflection (plus one for rays whose light
-    // candidate missed); the last pass's crossing kernel sends what still
-    // goes on to the tail kernel
-    const uint32_t passes = (ROOM && cont[0] && cont[1]) ? P.room_limit + 1u : 0u;
+    // with continuation queues, rays that go on after the crossing kernel
+    // (room scenes: reflected rays and light misses; other scenes: disk
+    // misses) go back through the integrator: one pass per reflection plus
+    // one in room scenes, one pass otherwise; the last pass's crossing
+    // kernel sends what still goes on to the tail kernel
+    uint32_t passes = 0;
+    if constexpr (ROOM) passes = (cont[0] && cont[1]) ? P.room_limit + 1u : 0u;
+    else passes = (MGK_MISS_PASS && cont[1]) ? 1u : 0u;
     if constexpr (MGK_MIXED_X2 && MODE == MGK_PRECISION_MIXED && METRIC != MGK_METRIC_MINKOWSKI) {
         // two rays per thread: half the threads for the same rays
         per_sm = 0;
@@ -1428,7 +1438,7 @@ static cudaError_t integ_t(const void* dsc, uint64_t first, uint32_t n, const Ch
     for (uint32_t p = 1; p <= passes; ++p) {
         const uint32_t in = p & 1u, out = (p + 1u) & 1u;
         k_next_pass<<<1, 32, 0, st>>>(b.counters, out);
-        k_integrate<METRIC, MODE, ROOM ? 2 : 0><<<full, kIntegrateThreads, 0, st>>>(
+        k_integrate<METRIC, MODE, ROOM ? 2 : 3><<<full, kIntegrateThreads, 0, st>>>(
             P, n, nullptr, nullptr, nullptr, refq, resq, res, b.counters, nullptr, cont[in], in);
         k_refine<METRIC, MODE, ROOM><<<refine_blocks, 128, 0, st>>>(P, refq, n, hits, resq, res, b.counters, hit_cap,
                                                               p < passes ? cont[out] : nullptr,

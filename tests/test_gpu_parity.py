@@ -332,16 +332,19 @@ def test_room_scene_validation(ctx):
 
 
 def test_render_pass_histories(ctx):
-    """Per-pass statistics: one pass without the room; with it, one pass per
-    reflection plus one, rays carried from each pass to the next, hits summing
-    to the emitter classes, crossings and tail hand-offs summing to the totals."""
+    """Per-pass statistics: without the room two passes (the disk misses take
+    the second); with it one pass per reflection plus one; rays carried from
+    each pass to the next, hits summing to the emitter classes, crossings and
+    tail hand-offs summing to the totals."""
     import torch
     s = small_scene()
     film = torch.empty(s.width * s.height * 3, dtype=torch.float32, device="cuda")
     st = ctx.render(s, None, film)
     n = s.width * s.height * s.spp
-    assert st.n_passes == 1 and st.pass_rays[0] == n and st.pass_continued[0] == 0
-    assert st.pass_to_tail[0] == st.resumed and st.pass_crossings[0] == st.crossings
+    # the disk misses take one more pass of the integrator
+    assert st.n_passes == 2 and st.pass_rays[0] == n and st.pass_rays[1] == st.pass_continued[0] > 0
+    assert st.pass_continued[1] == 0
+    assert sum(st.pass_to_tail[:2]) == st.resumed and sum(st.pass_crossings[:2]) == st.crossings
     r = room_scene()
     st = ctx.render(r, None, film)
     L = r.room_reflection_limit
