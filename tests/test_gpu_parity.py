@@ -355,3 +355,55 @@ def test_render_pass_histories(ctx):
     assert sum(st.pass_hits[:st.n_passes]) == cls[abi.RAY_LIGHT] + cls[abi.RAY_DISK] + cls[abi.RAY_ESCAPED]
     assert sum(st.pass_crossings[:st.n_passes]) == st.crossings
     assert sum(st.pass_to_tail[:st.n_passes]) == st.resumed
+
+
+# --------------------------------------------------------------- edge cases
+def test_empty_and_single_ray_calls(ctx):
+    import torch
+    s = small_scene()
+    assert len(ctx.trace_rays(s, 0, 0)) == 0
+    assert len(ctx.shade_rays(s, None, M.xyz_weights(s.n_bins), 5, 0)) == 0
+    # the last ray of the frame alone
+    n = s.width * s.height * s.spp
+    compare_records(ctx.trace_rays(s, n - 1, 1), O.trace_rays(s, n - 1, 1))
+    # past the frame: refused
+    with pytest.raises(M.MgkError):
+        ctx.trace_rays(s, n - 1, 2)
+    # a 1 x 1 frame at one sample
+    t = small_scene(width=1, height=1, spp=1)
+    film = torch.empty(3, dtype=torch.float32, device="cuda")
+    ctx.render(t, None, film)
+    ref, _ = O.render_pixels(t, np.zeros(0, M.STAR_DTYPE), M.xyz_weights(t.n_bins), 0, 1)
+    assert np.allclose(film.cpu().numpy().reshape(1, 3).astype(np.float64), ref, rtol=1e-4, atol=0.0)
+
+
+@pytest.mark.parametrize("precision", [abi.PRECISION_REF32, abi.PRECISION_MIXED, abi.PRECISION_F64])
+def test_step_cap_and_camera_in_the_disk_plane(ctx, precision):
+    """Rays stopped by a small step cap, and a camera in the disk plane
+    (rays that start with y = 0, where the disk's chord test sees no sign
+    change): records equal to the oracle's."""
+    s = small_scene(precision=precision, max_steps=7)
+    n = s.width * s.height * s.spp
+    gpu = ctx.trace_rays(s, 0, n)
+    compare_records(gpu, O.trace_rays(s, 0, n))
+    assert (gpu["cls"] == abi.RAY_STEP_LIMIT).mean() > 0.5 and gpu["steps"].max() <= 7
+    e = small_scene(precision=precision, cam_incl_rad=math.pi / 2)
+    compare_records(ctx.trace_rays(e, 0, n), O.trace_rays(e, 0, n))
+
+
+def test_maximum_bins(ctx):
+    """MGK_MAX_BINS spectral bins, with the spectral film."""
+    import torch
+    s = small_scene(n_bins=abi.MAX_BINS, star_radius_rad=0.02, width=32, height=18)
+    stars = _stars(5000)
+    w = M.xyz_weights(s.n_bins)
+    npix = s.width * s.height
+    film = torch.empty(npix * 3, dtype=torch.float32, device="cuda")
+    spec = torch.empty(npix * s.n_bins, dtype=torch.float32, device="cuda")
+    ctx.render(s, torch.from_numpy(stars.view(np.uint8)).cuda(), film,
+               d_weights=torch.from_numpy(w.ravel()).cuda(), d_film_spectral=spec)
+    ref, _ = O.render_pixels(s, stars, w, 0, npix)
+    got = film.cpu().numpy().reshape(npix, 3).astype(np.float64)
+    assert _film_rel_err(got, ref).max() <= 1e-4
+    sp = spec.cpu().numpy().reshape(npix, s.n_bins).astype(np.float64)
+    assert _film_rel_err(sp @ w.astype(np.float64), got).max() <= 1e-4
