@@ -413,7 +413,10 @@ def run_display(args, ctx):
                     "ms_per_launch": ms,
                     "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s",
                                  "frac": gbs / peak if peak else None,
-                                 "peak_source": "MEASURED_PEAKS.json hbm_gbs, of measured"}}
+                                 "peak_source": "MEASURED_PEAKS.json hbm_gbs, of measured",
+                                 "note": ("instruction-bound, not HBM-bound: ncu 90 % issue, 3.7 % DRAM "
+                                          "(profiles/queues_film_display_640x360x16.md)") if key == "gt7" else
+                                         "24 bytes per pixel moved"}}
     return out
 
 
