@@ -522,6 +522,8 @@ def run_gpu(args, rank, world, local_rank):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "fp32 (fp64 attempts next to the horizon)",
         "data": "synthetic (seeded camera jitter and star catalogue)",
+        # one camera geodesic per pixel sample: samples/s equals geodesics/s
+        "samples_per_s": world * rays / (ms * 1e-3),
         "config": config_dict(s, {"parallelism": f"{world} sample slices of one frame, film sum-reduced into rank 0 (weak)"}),
         "e2e": {"value": world * rays / (e2e_ms * 1e-3), "unit": UNIT,
                 "h2d_bytes_per_step": int(h_stars.numel() + h_w.numel() * 4),
