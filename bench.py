@@ -146,8 +146,9 @@ class Clocks:
 # --------------------------------------------------------------- CPU legs
 def cpu_render_sample(s, stars, w, seconds, precision, reference=False):
     """Renders a strided sample of the frame's pixels on the host cores and
-    returns (geodesics/s, threads, description).  The sample is sized from a
-    short calibration run so that it takes about `seconds`."""
+    returns (geodesics/s, accepted RKF45 steps/s, threads, description).  The
+    sample is sized from a short calibration run so that it takes about
+    `seconds`."""
     from oracle import oracle_py as O
     s = s.copy()
     s.precision = precision
@@ -163,11 +164,12 @@ def cpu_render_sample(s, stars, w, seconds, precision, reference=False):
     n = int(min(npix, max(n_cal, rate * seconds)))
     stride = max(1, npix // n)
     t0 = time.perf_counter()
-    render(s, stars, w, 0, n, nthreads=threads, stride=stride)
+    _, counts = render(s, stars, w, 0, n, nthreads=threads, stride=stride)
     dt = time.perf_counter() - t0
     rays = n * s.spp
-    desc = (f"{n} of {npix} pixels (every {stride}th) x {s.spp} spp = {rays} geodesics in {dt:.1f} s")
-    return rays / dt, threads, desc
+    desc = (f"{n} of {npix} pixels (every {stride}th) x {s.spp} spp = {rays} geodesics, "
+            f"{counts['steps']} steps in {dt:.1f} s")
+    return rays / dt, counts["steps"] / dt, threads, desc
 
 
 # ------------------------------------------------------------------ arms
@@ -183,11 +185,12 @@ def run_reference(args, rank, world):
     use_ref = O.ref_available() and hasattr(O, "ref_render_pixels")
     kind = "reference" if use_ref else "port"
     per = max(2.0, min(args.cpu_seconds, 120.0 / max(1, args.steps + args.warmup)))
-    vals, desc, threads = [], "", 1
+    vals, svals, desc, threads = [], [], "", 1
     for i in range(args.warmup + args.steps):
-        v, threads, desc = cpu_render_sample(s, stars, w, per, M.abi.PRECISION_REF32, reference=use_ref)
+        v, sv, threads, desc = cpu_render_sample(s, stars, w, per, M.abi.PRECISION_REF32, reference=use_ref)
         if i >= args.warmup:
             vals.append(v)
+            svals.append(sv)
     value = statistics.mean(vals)
     what = ("the reference's own RKF45 (metric_kerr.cuh / internal_math.h compiled from its sources) per camera "
             "ray, with the disk, escape, star and spectral stages of the CPU oracle, which the reference lacks"
@@ -196,7 +199,8 @@ def run_reference(args, rank, world):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic (seeded)",
             "config": config_dict(s), "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads,
-                                                        "kind": kind, "sample": desc, "what": what},
+                                                        "kind": kind, "sample": desc, "what": what,
+                                                        "steps_per_s": statistics.mean(svals)},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
@@ -306,7 +310,28 @@ def run_surrogate(args, ctx, s, d_stars, d_w, film_mixed_ms, steps):
     }
 
 
-def run_stress(args, ctx, d_stars, d_w, peak):
+def split_rooflines(metric, st, integrate_ms, peaks):
+    """The integrator's two roofline lines for one frame: FP32 work (the
+    attempts taken in FP32 and the crossing sub-steps) over the FP32 peak, and
+    the FP64 attempts next to the horizon over the FP64 peak.  Both run inside
+    the same kernels, so the FP64 line gives the time its work needs at the
+    FP64 peak, its share of the integration time, and the fraction of the
+    combined bound (FP32 work / FP32 peak + FP64 work / FP64 peak)."""
+    from magik_b200 import flops as FL
+    t = integrate_ms * 1e-3
+    f32 = FL.render_flops(metric, st.attempts - st.wide_attempts, st.refine_evals)
+    f64 = st.wide_attempts * FL.attempt_flops(metric)
+    r32 = {"bound": "fp32", "achieved": f32 / t / 1e12, "peak": peaks["fp32"] / 1e12, "unit": "TFLOP/s",
+           "frac": f32 / t / peaks["fp32"]}
+    t64 = f64 / peaks["fp64"]
+    r64 = {"bound": "fp64", "flop": f64, "attempts": st.wide_attempts, "peak": peaks["fp64"] / 1e12,
+           "unit": "TFLOP/s", "ms_at_peak": t64 * 1e3, "share_of_integrate_time_at_peak": t64 / t,
+           "combined_frac": (f32 / peaks["fp32"] + t64) / t,
+           "peak_source": "measured in this run by mgk_fp64_peak (double FMA probe kernel)"}
+    return r32, r64
+
+
+def run_stress(args, ctx, d_stars, d_w, peaks):
     """BASELINE's refill-stress configuration: Kerr a = 0.998, observer at
     r = 20 M and 85 degrees, 3840x2160 at 64 spp (530,841,600 geodesics),
     up to 5e4 steps per ray, FP32 integration with the FP64 band near the
@@ -314,7 +339,6 @@ def run_stress(args, ctx, d_stars, d_w, peak):
     fraction of attempts taken in FP64 and the FP32 roofline."""
     import torch
     import magik_b200 as M
-    from magik_b200 import flops as FL
     s = M.scene_defaults(width=3840, height=2160, spp=args.stress_spp, spin=0.998, cam_r=20.0,
                          cam_incl_rad=85.0 * 3.141592653589793 / 180.0, max_steps=50_000)
     s.disk_r_in = M.isco_radius(0.998)
@@ -328,7 +352,7 @@ def run_stress(args, ctx, d_stars, d_w, peak):
     e1.synchronize()
     ms = e0.elapsed_time(e1)
     rays = s.width * s.height * s.spp
-    flop = FL.render_flops(s.metric, st.attempts, st.refine_evals)
+    r32, r64 = split_rooflines(s.metric, st, st.integrate_ms, peaks)
     return {"workload": f"kerr_a0.998_r20M_i85_fov60_3840x2160_{s.spp}spp_32bins_1e5stars_rtol1e-7",
             "value": rays / (ms * 1e-3), "unit": UNIT, "ms_per_frame": ms, "rays": rays,
             "attempts_per_ray": st.attempts / rays, "max_steps": s.max_steps,
@@ -336,12 +360,10 @@ def run_stress(args, ctx, d_stars, d_w, peak):
             "rays_resumed_in_tail": st.resumed, "step_limit_rays": int(st.class_count[4]),
             "classes": dict(zip(["alive", "disk", "escaped", "horizon", "step_limit", "light"],
                                 [int(c) for c in st.class_count])),
-            "roofline": {"bound": "fp32", "achieved": flop / (st.integrate_ms * 1e-3) / 1e12,
-                         "peak": peak / 1e12, "unit": "TFLOP/s",
-                         "frac": flop / (st.integrate_ms * 1e-3) / peak}}
+            "roofline": r32, "roofline_fp64": r64}
 
 
-def run_room(args, ctx, d_w, peak):
+def run_room(args, ctx, d_w, peaks):
     """The reference's box-and-light stage around the Kerr a = 0.9 hole
     (walls at x, z = +-40 M, floor and ceiling at y = -+20 M, white-LED light
     straddling the ceiling, up to 10 reflections, mirror walls normal to x,
@@ -352,7 +374,6 @@ def run_room(args, ctx, d_w, peak):
     of the same frame on the host cores."""
     import torch
     import magik_b200 as M
-    from magik_b200 import flops as FL
     s = M.scene_defaults(width=1920, height=1080, spp=4, room_on=1, cam_r=18.0,
                          cam_incl_rad=80.0 * 3.141592653589793 / 180.0, disk_r_out=0.0)
     film = torch.empty(s.width * s.height * 3, dtype=torch.float32, device=f"cuda:{ctx.device}")
@@ -367,7 +388,7 @@ def run_room(args, ctx, d_w, peak):
     e1.synchronize()
     ms = e0.elapsed_time(e1) / reps
     rays = s.width * s.height * s.spp
-    flop = FL.render_flops(s.metric, st.attempts, st.refine_evals)
+    r32, r64 = split_rooflines(s.metric, st, st.integrate_ms, peaks)
     out = {"workload": "room_kerr_a0.9_r18M_i80_fov60_1920x1080_4spp_32bins_10reflections",
            "value": rays / (ms * 1e-3), "unit": UNIT, "ms_per_frame": ms, "rays": rays,
            "segments_per_s": (rays + st.reflections) / (ms * 1e-3),
@@ -375,12 +396,12 @@ def run_room(args, ctx, d_w, peak):
            "classes": dict(zip(["alive", "disk", "escaped", "horizon", "step_limit", "light"],
                                [int(c) for c in st.class_count])),
            "film_finite": bool(torch.isfinite(film).all().item()),
-           "roofline": {"bound": "fp32", "achieved": flop / (st.integrate_ms * 1e-3) / 1e12,
-                        "peak": peak / 1e12, "unit": "TFLOP/s", "frac": flop / (st.integrate_ms * 1e-3) / peak}}
+           "roofline": r32, "roofline_fp64": r64}
     if not args.no_cpu_baseline:
-        v, thr, desc = cpu_render_sample(s, np.zeros(0, M.STAR_DTYPE), M.xyz_weights(s.n_bins), 3.0,
-                                         M.abi.PRECISION_MIXED)
-        out["cpu_port"] = {"value": v, "unit": UNIT, "cores": thr, "kind": "port", "sample": desc}
+        v, sv, thr, desc = cpu_render_sample(s, np.zeros(0, M.STAR_DTYPE), M.xyz_weights(s.n_bins), 3.0,
+                                             M.abi.PRECISION_MIXED)
+        out["cpu_port"] = {"value": v, "unit": UNIT, "cores": thr, "kind": "port", "sample": desc,
+                           "steps_per_s": sv}
     return out
 
 
@@ -451,6 +472,7 @@ def run_gpu(args, rank, world, local_rank):
     film = torch.empty(npix * 3, dtype=torch.float32, device=dev)
     flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)
     peak = ctx.fp32_peak()
+    peaks_fp = {"fp32": peak, "fp64": ctx.fp64_peak()}
 
     def barrier():
         if world > 1:
@@ -479,7 +501,7 @@ def run_gpu(args, rank, world, local_rank):
         e1.synchronize()
         times.append(e0.elapsed_time(e1))
         integ.append(st.integrate_ms)
-        flop.append(FL.render_flops(s.metric, st.attempts, st.refine_evals))
+        flop.append(FL.render_flops(s.metric, st.attempts - st.wide_attempts, st.refine_evals))
         st_last = st
     torch.cuda.synchronize()
     clk = clocks.stop()
@@ -537,7 +559,10 @@ def run_gpu(args, rank, world, local_rank):
                                     "MEASURED_PEAKS.json has no FP32 figure",
                      "flop_per_attempt": FL.attempt_flops(s.metric),
                      "flop_per_crossing_substep": FL.substep_flops(s.metric),
-                     "integrate_ms": ms_int},
+                     "integrate_ms": ms_int,
+                     "work": "attempts taken in FP32 and crossing sub-steps; the FP64 attempts are in roofline_fp64"},
+        "roofline_fp64": split_rooflines(s.metric, st_last, ms_int, peaks_fp)[1],
+        "steps_per_s": world * st_last.steps / (ms * 1e-3),
         "stats": {"attempts": st_last.attempts, "steps": st_last.steps, "refine_evals": st_last.refine_evals,
                   "wide_attempts": st_last.wide_attempts, "crossings": st_last.crossings,
                   "resumed": st_last.resumed,
@@ -549,9 +574,9 @@ def run_gpu(args, rank, world, local_rank):
         "film_finite": film_ok,
     }
     if world == 1 and not args.no_stress:
-        out["refill_stress"] = run_stress(args, ctx, d_stars, d_w, peak)
+        out["refill_stress"] = run_stress(args, ctx, d_stars, d_w, peaks_fp)
     if world == 1:
-        out["room"] = run_room(args, ctx, d_w, peak)
+        out["room"] = run_room(args, ctx, d_w, peaks_fp)
         out["display"] = run_display(args, ctx)
     if world == 1 and not args.no_surrogate:
         # runs after the timed region; its own timings are inside "surrogate"
@@ -559,11 +584,11 @@ def run_gpu(args, rank, world, local_rank):
     if world == 1 and not args.no_cpu_baseline:
         from oracle import oracle_py as O
         use_ref = O.ref_available()
-        v, thr, desc = cpu_render_sample(s, stars, w, args.cpu_seconds,
-                                         M.abi.PRECISION_REF32 if use_ref else M.abi.PRECISION_MIXED,
-                                         reference=use_ref)
+        v, sv, thr, desc = cpu_render_sample(s, stars, w, args.cpu_seconds,
+                                             M.abi.PRECISION_REF32 if use_ref else M.abi.PRECISION_MIXED,
+                                             reference=use_ref)
         out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": thr, "kind": "reference" if use_ref else "port",
-                               "sample": desc}
+                               "sample": desc, "steps_per_s": sv}
     return out
 
 

@@ -268,6 +268,11 @@ MGK_API mgk_result mgk_scene_constants(const mgk_scene* s, double* out32);
  * denominator of the integrator's roofline.  Synchronous. */
 MGK_API mgk_result mgk_fp32_peak(mgk_context* ctx, double* flops_per_s);
 
+/* Measured peak FP64 (non-tensor) throughput in FLOP/s, from the same probe
+ * with double FMA chains; the denominator of the roofline line of the FP64
+ * attempts next to the horizon.  Synchronous. */
+MGK_API mgk_result mgk_fp64_peak(mgk_context* ctx, double* flops_per_s);
+
 /* Self-check of the MIXED mode's square root and reciprocal (no counterpart
  * in the reference).  The fused RHS takes them from the hardware
  * approximations with one FMA correction each; they are defined as
@@ -492,6 +497,30 @@ MGK_API mgk_result mgk_surrogate_gradient(mgk_surrogate* net, const mgk_train_co
 MGK_API mgk_result mgk_surrogate_train(mgk_surrogate* net, const mgk_train_config* cfg, const float* d_features,
                                        const mgk_sample_label* d_labels, uint32_t n, float* h_epoch_loss,
                                        void* stream);
+/* Data-parallel training, one step at a time, for one rank of several that
+ * each hold a shard of the sample set: between mgk_surrogate_gradient_step and
+ * mgk_surrogate_adam_step the caller sums d_grad over the ranks (an all-reduce
+ * on the same stream), and every rank then takes the same Adam step.  With one
+ * rank, shuffle seed cfg->seed, rows [b B, (b + 1) B) of epoch e and progress
+ * (e nb + b) / (epochs nb) this is the loop of mgk_surrogate_train.
+ * mgk_surrogate_shuffle: the order of the n samples for one epoch (the
+ *   shuffle mgk_surrogate_train uses); synchronous.
+ * mgk_surrogate_gradient_step: forward and backward of rows [first, first + n)
+ *   of that order (n a multiple of 1024, the same n on every call for one
+ *   network); the gradient of the batch mean loss into d_grad
+ *   (mgk_surrogate_param_count floats), the batch mean loss added to
+ *   *d_loss_sum (device).  Asynchronous.
+ * mgk_surrogate_adam_step: one Adam step with gradient d_grad x grad_scale,
+ *   step size from cfg's cosine schedule at `progress` in [0, 1].
+ *   Asynchronous. */
+MGK_API mgk_result mgk_surrogate_shuffle(mgk_surrogate* net, uint64_t seed, uint32_t epoch, uint32_t n,
+                                         void* stream);
+MGK_API mgk_result mgk_surrogate_gradient_step(mgk_surrogate* net, const mgk_train_config* cfg,
+                                               const float* d_features, const mgk_sample_label* d_labels,
+                                               uint32_t first, uint32_t n, float* d_grad, float* d_loss_sum,
+                                               void* stream);
+MGK_API mgk_result mgk_surrogate_adam_step(mgk_surrogate* net, const mgk_train_config* cfg, const float* d_grad,
+                                           float grad_scale, double progress, void* stream);
 /* mgk_render with the surrogate in front of the integrator: every camera ray
  * goes through the network; rays whose confidence is below conf_min, or whose
  * impact parameter lies within crit_frac of the critical curve, are

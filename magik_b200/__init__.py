@@ -31,11 +31,12 @@ assert RESULT_DTYPE.itemsize == 128 and STAR_DTYPE.itemsize == 32 and STEP_DTYPE
 EXPORTS = [
     "mgk_context_create", "mgk_context_destroy", "mgk_last_error", "mgk_scene_defaults", "mgk_isco_radius",
     "mgk_xyz_weights", "mgk_star_catalog", "mgk_scene_constants", "mgk_render", "mgk_render_host",
-    "mgk_trace_rays", "mgk_shade_rays", "magik_trace_geodesic", "mgk_trace_geodesic_batch", "mgk_fp32_peak",
+    "mgk_trace_rays", "mgk_shade_rays", "magik_trace_geodesic", "mgk_trace_geodesic_batch", "mgk_fp32_peak", "mgk_fp64_peak",
     "mgk_check_rounding", "mgk_cmf_inverse_cdf", "mgk_display_defaults", "mgk_display_prepare", "mgk_display",
     "mgk_trace_rays_static", "mgk_train_defaults", "mgk_surrogate_param_count", "mgk_surrogate_create",
     "mgk_surrogate_destroy", "mgk_surrogate_get_params", "mgk_surrogate_set_params", "mgk_make_samples",
     "mgk_surrogate_forward", "mgk_surrogate_forward_tiled", "mgk_surrogate_status", "mgk_surrogate_gradient", "mgk_surrogate_train", "mgk_render_surrogate",
+    "mgk_surrogate_shuffle", "mgk_surrogate_gradient_step", "mgk_surrogate_adam_step",
 ]
 
 
@@ -75,6 +76,7 @@ def lib():
         L.mgk_trace_geodesic_batch.argtypes = [vp, P(abi.TraceContainer), P(abi.TraceInitialConditions),
                                                P(abi.TraceMetricParams), P(abi.TraceIntegratorParams), C.c_uint32]
         L.mgk_fp32_peak.argtypes = [vp, P(C.c_double)]
+        L.mgk_fp64_peak.argtypes = [vp, P(C.c_double)]
         L.mgk_check_rounding.argtypes = [vp, P(C.c_uint64)]
         L.mgk_cmf_inverse_cdf.argtypes = [C.c_double, C.c_double, P(C.c_float)]
         L.mgk_display_defaults.argtypes = [P(abi.DisplaySettings)]
@@ -97,6 +99,10 @@ def lib():
         L.mgk_surrogate_gradient.argtypes = [vp, P(abi.TrainConfig), vp, vp, C.c_uint32, P(C.c_float),
                                              P(C.c_float)]
         L.mgk_surrogate_train.argtypes = [vp, P(abi.TrainConfig), vp, vp, C.c_uint32, P(C.c_float), vp]
+        L.mgk_surrogate_shuffle.argtypes = [vp, C.c_uint64, C.c_uint32, C.c_uint32, vp]
+        L.mgk_surrogate_gradient_step.argtypes = [vp, P(abi.TrainConfig), vp, vp, C.c_uint32, C.c_uint32, vp, vp,
+                                                  vp]
+        L.mgk_surrogate_adam_step.argtypes = [vp, P(abi.TrainConfig), vp, C.c_float, C.c_double, vp]
         L.mgk_render_surrogate.argtypes = [vp, vp, P(Scene), vp, C.c_uint32, vp, C.c_float, C.c_float, vp,
                                            P(RenderStats), vp]
         for name in EXPORTS:
@@ -214,6 +220,12 @@ class Context:
         """Measured FP32 FLOP/s of this device (FMA probe)."""
         v = C.c_double(0)
         _check(lib().mgk_fp32_peak(self.handle, C.byref(v)), "mgk_fp32_peak", self.handle)
+        return v.value
+
+    def fp64_peak(self):
+        """Measured FP64 FLOP/s of this device (double FMA probe)."""
+        v = C.c_double(0)
+        _check(lib().mgk_fp64_peak(self.handle, C.byref(v)), "mgk_fp64_peak", self.handle)
         return v.value
 
     def check_rounding(self):
@@ -406,6 +418,26 @@ class Surrogate:
                                          d_feat.shape[0], losses.ctypes.data_as(C.POINTER(C.c_float)),
                                          _stream_ptr(stream)), "mgk_surrogate_train")
         return losses[: cfg.epochs]
+
+    # one training step at a time, for data-parallel training (magik_b200.dist)
+    @property
+    def param_count(self):
+        return surrogate_param_count()
+
+    def shuffle(self, seed, epoch, n, stream=None):
+        """The sample-set order of one epoch (mgk_surrogate_shuffle)."""
+        _check(lib().mgk_surrogate_shuffle(self.handle, seed, epoch, n, _stream_ptr(stream)), "mgk_surrogate_shuffle")
+
+    def gradient_step(self, cfg, d_feat, d_lab, first, n, d_grad, d_loss_sum, stream=None):
+        """Rows [first, first + n) of the order: gradient into d_grad, batch mean loss added to d_loss_sum."""
+        _check(lib().mgk_surrogate_gradient_step(self.handle, C.byref(cfg), d_feat.data_ptr(), d_lab.data_ptr(),
+                                                 first, n, d_grad.data_ptr(), d_loss_sum.data_ptr(),
+                                                 _stream_ptr(stream)), "mgk_surrogate_gradient_step")
+
+    def adam_step(self, cfg, d_grad, grad_scale, progress, stream=None):
+        """One Adam step with gradient d_grad x grad_scale at schedule position progress."""
+        _check(lib().mgk_surrogate_adam_step(self.handle, C.byref(cfg), d_grad.data_ptr(), grad_scale, progress,
+                                             _stream_ptr(stream)), "mgk_surrogate_adam_step")
 
 
 def make_samples(ctx, base, seed, n, n_spin_buckets=0, stream=None):

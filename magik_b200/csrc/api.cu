@@ -688,7 +688,10 @@ MGK_API mgk_result mgk_scene_constants(const mgk_scene* s, double* out) {
     return MGK_SUCCESS;
 }
 
-MGK_API mgk_result mgk_fp32_peak(mgk_context* ctx, double* flops_per_s) {
+// Best of three timed launches (after one untimed) of an FMA-chain probe:
+// blocks x 256 threads x iters loop trips x 16 FLOP per trip.
+static mgk_result probe_peak(mgk_context* ctx, cudaError_t (*launch)(uint32_t, uint32_t, void*),
+                             double* flops_per_s) {
     if (!ctx || !flops_per_s) return MGK_ERROR_INVALID_POINTER;
     MGK_CUDA(ctx, cudaSetDevice(ctx->device));
     mgk_result rc = ensure_arena(ctx, 4096);
@@ -700,7 +703,7 @@ MGK_API mgk_result mgk_fp32_peak(mgk_context* ctx, double* flops_per_s) {
     float best = 1e30f;
     for (int rep = 0; rep < 4; ++rep) {
         MGK_CUDA(ctx, cudaEventRecord(e0, nullptr));
-        MGK_CUDA(ctx, launch_fma_probe(blocks, iters, static_cast<float*>(ctx->arena), nullptr));
+        MGK_CUDA(ctx, launch(blocks, iters, ctx->arena));
         MGK_CUDA(ctx, cudaEventRecord(e1, nullptr));
         MGK_CUDA(ctx, cudaEventSynchronize(e1));
         float ms = 0.f;
@@ -711,6 +714,21 @@ MGK_API mgk_result mgk_fp32_peak(mgk_context* ctx, double* flops_per_s) {
     cudaEventDestroy(e1);
     *flops_per_s = double(blocks) * 256.0 * iters * 32.0 * 2.0 / (best * 1e-3);
     return MGK_SUCCESS;
+}
+
+static cudaError_t fp32_probe(uint32_t blocks, uint32_t iters, void* sink) {
+    return launch_fma_probe(blocks, iters, static_cast<float*>(sink), nullptr);
+}
+static cudaError_t fp64_probe(uint32_t blocks, uint32_t iters, void* sink) {
+    return launch_dfma_probe(blocks, iters, static_cast<double*>(sink), nullptr);
+}
+
+MGK_API mgk_result mgk_fp32_peak(mgk_context* ctx, double* flops_per_s) {
+    return probe_peak(ctx, fp32_probe, flops_per_s);
+}
+
+MGK_API mgk_result mgk_fp64_peak(mgk_context* ctx, double* flops_per_s) {
+    return probe_peak(ctx, fp64_probe, flops_per_s);
 }
 
 MGK_API mgk_result mgk_check_rounding(mgk_context* ctx, uint64_t mismatches[2]) {

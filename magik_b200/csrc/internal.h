@@ -108,6 +108,7 @@ int context_device(mgk_context* ctx);
 size_t context_device_bytes(mgk_context* ctx);  // scratch arena and staging
 mgk_result validate_scene(const mgk_scene* s);   // mgk_render's scene checks
 cudaError_t launch_fma_probe(uint32_t blocks, uint32_t iters, float* sink, cudaStream_t stream);
+cudaError_t launch_dfma_probe(uint32_t blocks, uint32_t iters, double* sink, cudaStream_t stream);
 cudaError_t launch_check_rounding(int sm_count, unsigned long long* out, cudaStream_t stream);
 cudaError_t launch_trace_geodesic(const void* jobs, uint32_t n, void* steps, uint32_t* written, cudaStream_t stream);
 

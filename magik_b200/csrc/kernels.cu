@@ -1319,6 +1319,23 @@ __global__ void __launch_bounds__(256) k_fma_probe(uint32_t iters, float seed, f
     if (r == 12345.f) sink[threadIdx.x] = r;
 }
 
+// Peak FP64 throughput, the same shape with double FMA chains: each loop trip
+// is 8 DFMA = 16 FLOP per thread.
+__global__ void __launch_bounds__(256) k_dfma_probe(uint32_t iters, double seed, double* sink) {
+    double a0 = seed + threadIdx.x, a1 = a0 + 1.0, a2 = a0 + 2.0, a3 = a0 + 3.0;
+    double a4 = a0 + 4.0, a5 = a0 + 5.0, a6 = a0 + 6.0, a7 = a0 + 7.0;
+    const double m = 0.999999999, c = 1e-12;
+    for (uint32_t i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            a0 = __fma_rn(a0, m, c); a1 = __fma_rn(a1, m, c); a2 = __fma_rn(a2, m, c); a3 = __fma_rn(a3, m, c);
+            a4 = __fma_rn(a4, m, c); a5 = __fma_rn(a5, m, c); a6 = __fma_rn(a6, m, c); a7 = __fma_rn(a7, m, c);
+        }
+    }
+    double r = ((a0 + a1) + (a2 + a3)) + ((a4 + a5) + (a6 + a7));
+    if (r == 12345.0) sink[threadIdx.x] = r;
+}
+
 // ----------------------------------------------------- rounding self-check
 // msqrt / mrcp (dev_physics.cuh) against their definitions, on every one of
 // the 2^32 float inputs: the definitions use the IEEE-rounded __fsqrt_rn and
@@ -1361,6 +1378,11 @@ cudaError_t launch_check_rounding(int sms, unsigned long long* out, cudaStream_t
 
 cudaError_t launch_fma_probe(uint32_t blocks, uint32_t iters, float* sink, cudaStream_t st) {
     k_fma_probe<<<blocks, 256, 0, st>>>(iters, 1.0f, sink);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_dfma_probe(uint32_t blocks, uint32_t iters, double* sink, cudaStream_t st) {
+    k_dfma_probe<<<blocks, 256, 0, st>>>(iters, 1.0, sink);
     return cudaGetLastError();
 }
 

@@ -341,7 +341,7 @@ __global__ void k_adam(float* __restrict__ p, const float* __restrict__ grad, fl
                        float* __restrict__ v, __nv_bfloat16* __restrict__ bf16_copy, int n, AdamStep a) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const float gi = grad[i];
+    const float gi = grad[i] * a.gscale;
     const float mi = a.b1 * m[i] + (1.f - a.b1) * gi;
     const float vi = a.b2 * v[i] + (1.f - a.b2) * gi * gi;
     m[i] = mi;

@@ -52,7 +52,8 @@ struct LossWeights {
 
 struct AdamStep {
     float lr, b1, b2, eps;
-    float c1, c2;  // 1 / (1 - b1^t), 1 / (1 - b2^t)
+    float c1, c2;     // 1 / (1 - b1^t), 1 / (1 - b2^t)
+    float gscale;     // the gradient is grad x gscale (1 / ranks after a sum over ranks)
 };
 
 cudaError_t launch_gemm(GemmKind kind, GemmArgs g, cudaStream_t st);

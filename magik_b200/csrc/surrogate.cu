@@ -60,6 +60,8 @@ struct mgk_surrogate {
     mgk_sample_label* blab = nullptr;
     uint32_t* perm = nullptr;
     uint32_t perm_n = 0;
+    std::vector<uint32_t> order;  // host copy of the latest mgk_surrogate_shuffle order
+    uint32_t order_n = 0;         // its length (rows mgk_surrogate_gradient_step may take)
     // inference buffers for batch `ib`
     int ib = 0;
     __nv_bfloat16 *ix0 = nullptr, *iha = nullptr, *ihb = nullptr;
@@ -169,11 +171,11 @@ cudaError_t forward(mgk_surrogate* s, const __nv_bfloat16* x0, int B, __nv_bfloa
 }
 
 // Loss, backward pass and gradient accumulation of the batch in the training
-// buffers (grad is zeroed first).
-cudaError_t backward(mgk_surrogate* s, int B, const LossWeights& w, cudaStream_t st) {
+// buffers (grad is zeroed first); the batch mean loss is added to *loss_acc.
+cudaError_t backward(mgk_surrogate* s, int B, const LossWeights& w, float* loss_acc, cudaStream_t st) {
     const Layout& L = s->L;
     cudaError_t e = cudaMemsetAsync(s->grad, 0, L.total * sizeof(float), st);
-    if (e == cudaSuccess) e = launch_loss(s->out, s->blab, B, w, s->dout, s->dout32, s->loss, st);
+    if (e == cudaSuccess) e = launch_loss(s->out, s->blab, B, w, s->dout, s->dout32, loss_acc, st);
     if (e != cudaSuccess) return e;
     const int ks = B >= 1024 && B % 1024 == 0 ? 1024 : B;
     // output layer
@@ -263,6 +265,26 @@ LossWeights loss_weights(const mgk_train_config& c) {
 }
 
 uint32_t host_hash(uint64_t seed, uint32_t a, uint32_t b) { return rng_u32(seed, 0x7E11u, a, b); }
+
+// The sample-set order of one epoch: Fisher-Yates with the counter-based hash.
+void epoch_order(std::vector<uint32_t>& perm, uint32_t n, uint64_t seed, uint32_t epoch) {
+    perm.resize(n);
+    for (uint32_t i = 0; i < n; ++i) perm[i] = i;
+    for (uint32_t i = n - 1; i > 0; --i) {
+        uint32_t j = uint32_t((uint64_t(host_hash(seed, epoch, i)) * (i + 1)) >> 32);
+        std::swap(perm[i], perm[j]);
+    }
+}
+
+// Step size of step `k` of `total` (cosine decay from lr to lr_final) and the
+// Adam constants after the network's step counter advanced to it.
+AdamStep adam_constants(const mgk_train_config& c, double prog, uint64_t step, float gscale) {
+    const float lr = float(double(c.lr_final) +
+                           0.5 * double(c.lr - c.lr_final) * (1.0 + std::cos(3.14159265358979323846 * prog)));
+    return AdamStep{lr, c.beta1, c.beta2, c.eps,
+                    float(1.0 / (1.0 - std::pow(double(c.beta1), double(step)))),
+                    float(1.0 / (1.0 - std::pow(double(c.beta2), double(step)))), gscale};
+}
 
 }  // namespace
 
@@ -395,11 +417,12 @@ MGK_API mgk_result mgk_surrogate_gradient(mgk_surrogate* s, const mgk_train_conf
     if (rc != MGK_SUCCESS) return rc;
     std::vector<uint32_t> perm(n);
     for (uint32_t i = 0; i < n; ++i) perm[i] = i;
+    s->order_n = 0;
     TRY(cudaMemcpyAsync(s->perm, perm.data(), size_t(n) * 4, cudaMemcpyHostToDevice, st));
     TRY(launch_gather(d_feat, d_lab, s->perm, 0, int(n), s->x0, s->blab, st));
     TRY(cudaMemsetAsync(s->loss, 0, 4, st));
     TRY(forward(s, s->x0, int(n), s->Z, s->H, s->out, st));
-    TRY(backward(s, int(n), loss_weights(*cfg), st));
+    TRY(backward(s, int(n), loss_weights(*cfg), s->loss, st));
     TRY(cudaMemcpyAsync(h_grad, s->grad, s->L.total * 4, cudaMemcpyDeviceToHost, st));
     float loss = 0.f;
     TRY(cudaMemcpyAsync(&loss, s->loss, 4, cudaMemcpyDeviceToHost, st));
@@ -425,25 +448,16 @@ MGK_API mgk_result mgk_surrogate_train(mgk_surrogate* s, const mgk_train_config*
     const uint32_t nb = n / B;
     std::vector<uint32_t> perm(n);
     for (uint32_t ep = 0; ep < cfg->epochs; ++ep) {
-        // Fisher-Yates with the counter-based hash
-        for (uint32_t i = 0; i < n; ++i) perm[i] = i;
-        for (uint32_t i = n - 1; i > 0; --i) {
-            uint32_t j = uint32_t((uint64_t(host_hash(cfg->seed, ep, i)) * (i + 1)) >> 32);
-            std::swap(perm[i], perm[j]);
-        }
+        epoch_order(perm, n, cfg->seed, ep);
+        s->order_n = 0;
         TRY(cudaMemcpyAsync(s->perm, perm.data(), size_t(n) * 4, cudaMemcpyHostToDevice, st));
         TRY(cudaMemsetAsync(s->loss, 0, 4, st));
         for (uint32_t b = 0; b < nb; ++b) {
             TRY(launch_gather(d_feat, d_lab, s->perm, int(b * B), int(B), s->x0, s->blab, st));
             TRY(forward(s, s->x0, int(B), s->Z, s->H, s->out, st));
-            TRY(backward(s, int(B), w, st));
+            TRY(backward(s, int(B), w, s->loss, st));
             ++s->step;
-            const double prog = double(ep * nb + b) / double(cfg->epochs * nb);
-            const float lr = float(double(cfg->lr_final) +
-                                   0.5 * double(cfg->lr - cfg->lr_final) * (1.0 + std::cos(3.14159265358979323846 * prog)));
-            AdamStep a{lr, cfg->beta1, cfg->beta2, cfg->eps,
-                       float(1.0 / (1.0 - std::pow(double(cfg->beta1), double(s->step)))),
-                       float(1.0 / (1.0 - std::pow(double(cfg->beta2), double(s->step))))};
+            const AdamStep a = adam_constants(*cfg, double(ep * nb + b) / double(cfg->epochs * nb), s->step, 1.0f);
             TRY(launch_adam(s->p, s->grad, s->m, s->v, s->wb, int(s->L.total), a, st));
             s->img_valid = false;
         }
@@ -452,6 +466,50 @@ MGK_API mgk_result mgk_surrogate_train(mgk_surrogate* s, const mgk_train_config*
         TRY(cudaStreamSynchronize(st));
         if (h_epoch_loss) h_epoch_loss[ep] = loss / float(nb);
     }
+    return MGK_SUCCESS;
+}
+
+MGK_API mgk_result mgk_surrogate_shuffle(mgk_surrogate* s, uint64_t seed, uint32_t epoch, uint32_t n, void* stream) {
+    if (!s) return MGK_ERROR_INVALID_POINTER;
+    if (n == 0) return MGK_ERROR_INVALID_ARGUMENT;
+    cudaSetDevice(s->device);
+    mgk_result rc = ensure_perm(s, n);
+    if (rc != MGK_SUCCESS) return rc;
+    epoch_order(s->order, n, seed, epoch);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    TRY(cudaMemcpyAsync(s->perm, s->order.data(), size_t(n) * 4, cudaMemcpyHostToDevice, st));
+    // the host copy of the order stays unchanged until the copy has read it
+    TRY(cudaStreamSynchronize(st));
+    s->order_n = n;
+    return MGK_SUCCESS;
+}
+
+MGK_API mgk_result mgk_surrogate_gradient_step(mgk_surrogate* s, const mgk_train_config* cfg, const float* d_feat,
+                                               const mgk_sample_label* d_lab, uint32_t first, uint32_t n,
+                                               float* d_grad, float* d_loss_sum, void* stream) {
+    if (!s || !cfg || !d_feat || !d_lab || !d_grad || !d_loss_sum) return MGK_ERROR_INVALID_POINTER;
+    if (n == 0 || n % 1024 || uint64_t(first) + n > s->order_n) return MGK_ERROR_INVALID_ARGUMENT;
+    cudaSetDevice(s->device);
+    mgk_result rc = ensure_train_buffers(s, int(n));
+    if (rc != MGK_SUCCESS) return rc;
+    if (s->tb != int(n)) return MGK_ERROR_INVALID_ARGUMENT;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    TRY(launch_gather(d_feat, d_lab, s->perm, int(first), int(n), s->x0, s->blab, st));
+    TRY(forward(s, s->x0, int(n), s->Z, s->H, s->out, st));
+    TRY(backward(s, int(n), loss_weights(*cfg), d_loss_sum, st));
+    TRY(cudaMemcpyAsync(d_grad, s->grad, s->L.total * 4, cudaMemcpyDeviceToDevice, st));
+    return MGK_SUCCESS;
+}
+
+MGK_API mgk_result mgk_surrogate_adam_step(mgk_surrogate* s, const mgk_train_config* cfg, const float* d_grad,
+                                           float grad_scale, double progress, void* stream) {
+    if (!s || !cfg || !d_grad) return MGK_ERROR_INVALID_POINTER;
+    if (!(progress >= 0.0 && progress <= 1.0)) return MGK_ERROR_INVALID_ARGUMENT;
+    cudaSetDevice(s->device);
+    ++s->step;
+    const AdamStep a = adam_constants(*cfg, progress, s->step, grad_scale);
+    TRY(launch_adam(s->p, d_grad, s->m, s->v, s->wb, int(s->L.total), a, static_cast<cudaStream_t>(stream)));
+    s->img_valid = false;
     return MGK_SUCCESS;
 }
 

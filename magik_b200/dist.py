@@ -47,3 +47,51 @@ def reduce_film(film, dst=0):
     if dist.get_rank() == dst:
         film.mul_(1.0 / world)
     return film
+
+
+def train_data_parallel(net, cfg, d_feat, d_lab, stream=None):
+    """Data-parallel Adam training of the deflection surrogate, one process
+    per GPU.  Every rank holds its own shard of the sample set (d_feat [n, 7],
+    d_lab [n], the same n on every rank) and takes cfg.batch / world rows of
+    it per step; the ranks' batch gradients are summed by an all-reduce (NCCL
+    over NVLink on GPUs) and the Adam step scales the sum by 1 / world, so each
+    step is a step on the union batch of cfg.batch rows and every rank keeps
+    the same parameters.  A rank shuffles its shard with frame_seed(cfg.seed,
+    rank): with one rank this is the loop of Surrogate.train
+    (mgk_surrogate_train).  Returns the mean batch loss of each epoch over all
+    ranks (numpy float32).
+
+    `net` is a Surrogate, or any object with its shuffle / gradient_step /
+    adam_step methods, a `param_count` and optionally a `grad_dtype` (float32
+    by default); d_feat and d_lab are tensors on the net's device."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    multi = dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1
+    world = dist.get_world_size() if multi else 1
+    rank = dist.get_rank() if multi else 0
+    if cfg.batch == 0 or cfg.batch % world or (cfg.batch // world) % 1024:
+        raise ValueError(f"batch {cfg.batch} is not {world} ranks x a multiple of 1024")
+    b = cfg.batch // world
+    n = int(d_feat.shape[0])
+    nb = n // b
+    if multi:  # the same number of steps on every rank, or the collectives would not pair up
+        t = torch.tensor([nb, -nb], dtype=torch.int64, device=d_feat.device)
+        dist.all_reduce(t, op=dist.ReduceOp.MIN)
+        if int(t[0]) != nb or -int(t[1]) != nb:
+            raise ValueError("the ranks' shards give different numbers of steps per epoch")
+    if nb == 0:
+        raise ValueError(f"{n} samples are fewer than one batch of {b} rows")
+    grad = torch.empty(int(net.param_count), dtype=getattr(net, "grad_dtype", torch.float32), device=d_feat.device)
+    loss = torch.zeros(max(int(cfg.epochs), 1), dtype=grad.dtype, device=d_feat.device)
+    seed = frame_seed(cfg.seed, rank)
+    for ep in range(int(cfg.epochs)):
+        net.shuffle(seed, ep, n, stream=stream)
+        for k in range(nb):
+            net.gradient_step(cfg, d_feat, d_lab, k * b, b, grad, loss[ep:ep + 1], stream=stream)
+            if multi:
+                dist.all_reduce(grad, op=dist.ReduceOp.SUM)
+            net.adam_step(cfg, grad, 1.0 / world, (ep * nb + k) / (int(cfg.epochs) * nb), stream=stream)
+    if multi:
+        dist.all_reduce(loss, op=dist.ReduceOp.SUM)
+    return (loss[: int(cfg.epochs)] / float(nb * world)).cpu().numpy().astype(np.float32)

@@ -273,25 +273,27 @@ int orc_shade_rays(const mgk_scene* s, const mgk_star* stars, uint32_t n_stars, 
 
 // Full pipeline for pixels first_pixel + i * pixel_stride, i < n_pixels:
 // trace every sample, shade, average.  xyz_out: 3 doubles per pixel.
-// attempts_out (may be NULL) receives the RKF45 attempt total.
+// attempts_out / steps_out (may be NULL) receive the RKF45 attempt and
+// accepted-step totals.
 int orc_render_pixels(const mgk_scene* s, const mgk_star* stars, uint32_t n_stars, const float* w,
                       uint64_t first_pixel, uint32_t n_pixels, uint64_t pixel_stride, const float* icdf,
-                      double* xyz_out, uint64_t* attempts_out, int nthreads) {
+                      double* xyz_out, uint64_t* attempts_out, uint64_t* steps_out, int nthreads) {
     if (s->spectral_mode == MGK_SPECTRAL_SAMPLED && !icdf) return 1;
     SceneConsts c = scene_consts(*s);
     StarIndex idx;
     idx.build(stars, n_stars, s->star_radius_rad);
     const uint32_t nb = s->n_bins, spp = s->spp;
     const double dl = (s->lambda_max_nm - s->lambda_min_nm) / nb;
-    std::atomic<uint64_t> att{0};
+    std::atomic<uint64_t> att{0}, stp{0};
     parallel_for(n_pixels, nthreads, [&](uint64_t i) {
         uint64_t pix = first_pixel + i * pixel_stride;
         double acc[3] = {0, 0, 0};
         float accf[3] = {0, 0, 0};
-        uint64_t a = 0;
+        uint64_t a = 0, n = 0;
         for (uint32_t smp = 0; smp < spp; ++smp) {
             RayResult r = trace_ray(*s, c, pix * spp + smp);
             a += r.attempts;
+            n += r.steps;
             if (s->precision == MGK_PRECISION_F64) {
                 double lam[MGK_MAX_BINS], spec[MGK_MAX_BINS], o[3];
                 for (uint32_t k = 0; k < nb; ++k) lam[k] = s->lambda_min_nm + (k + 0.5) * dl;
@@ -315,10 +317,12 @@ int orc_render_pixels(const mgk_scene* s, const mgk_star* stars, uint32_t n_star
             }
         }
         att += a;
+        stp += n;
         for (int k = 0; k < 3; ++k)
             xyz_out[3 * i + k] = s->precision == MGK_PRECISION_F64 ? acc[k] / spp : double(accf[k] / float(spp));
     });
     if (attempts_out) *attempts_out = att.load();
+    if (steps_out) *steps_out = stp.load();
     return 0;
 }
 

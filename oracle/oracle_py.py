@@ -43,7 +43,8 @@ def lib():
                                      C.POINTER(C.c_double), C.c_int]
         L.orc_render_pixels.argtypes = [C.POINTER(abi.Scene), C.POINTER(abi.Star), C.c_uint32,
                                         C.POINTER(C.c_float), C.c_uint64, C.c_uint32, C.c_uint64,
-                                        C.POINTER(C.c_float), C.POINTER(C.c_double), C.POINTER(C.c_uint64), C.c_int]
+                                        C.POINTER(C.c_float), C.POINTER(C.c_double), C.POINTER(C.c_uint64),
+                                        C.POINTER(C.c_uint64), C.c_int]
         L.orc_count_ops.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_uint64)]
         D3 = C.POINTER(C.c_double)
         F4 = C.POINTER(C.c_float)
@@ -73,7 +74,8 @@ def ref():
         R.ref_display_pixels.argtypes = [C.POINTER(abi.DisplaySettings), C.POINTER(C.c_float), C.c_uint32,
                                          C.POINTER(C.c_float)]
         R.ref_render_pixels.argtypes = [C.POINTER(abi.Scene), C.POINTER(abi.Star), C.c_uint32, C.POINTER(C.c_float),
-                                        C.c_uint64, C.c_uint32, C.c_uint64, C.POINTER(C.c_double), C.c_int]
+                                        C.c_uint64, C.c_uint32, C.c_uint64, C.POINTER(C.c_double),
+                                        C.POINTER(C.c_uint64), C.c_int]
         R.ref_render_pixels.restype = C.c_int
         R.ref_white_led.argtypes = [C.c_float]
         R.ref_white_led.restype = C.c_float
@@ -190,28 +192,31 @@ def render_pixels(scene, stars, weights, first_pixel, n_pixels, nthreads=None, s
     stars = np.ascontiguousarray(stars)
     w = np.ascontiguousarray(weights, dtype=np.float32)
     out = np.zeros((n_pixels, 3), dtype=np.float64)
-    att = C.c_uint64(0)
+    att, stp = C.c_uint64(0), C.c_uint64(0)
     keep, p = _icdf_ptr(scene, icdf)
     rc = lib().orc_render_pixels(C.byref(scene), stars.ctypes.data_as(C.POINTER(abi.Star)), len(stars),
                                  w.ctypes.data_as(C.POINTER(C.c_float)), first_pixel, n_pixels, stride, p,
-                                 out.ctypes.data_as(C.POINTER(C.c_double)), C.byref(att), nthreads or os.cpu_count())
+                                 out.ctypes.data_as(C.POINTER(C.c_double)), C.byref(att), C.byref(stp),
+                                 nthreads or os.cpu_count())
     assert rc == 0
     del keep
-    return out, att.value
+    return out, {"attempts": att.value, "steps": stp.value}
 
 
 def ref_render_pixels(scene, stars, weights, first_pixel, n_pixels, nthreads=None, stride=1):
     """Pixels rendered with the reference's own RKF45 step (oracle/_ref) inside
     the oracle's camera, termination and spectral stages; REF32 semantics.
-    Returns (xyz [n, 3] float64, None): the reference reports no retries."""
+    Returns (xyz [n, 3] float64, {"attempts": None, "steps": accepted steps}):
+    the reference reports no retries."""
     stars = np.ascontiguousarray(stars)
     w = np.ascontiguousarray(weights, dtype=np.float32)
     out = np.zeros((n_pixels, 3), dtype=np.float64)
+    stp = C.c_uint64(0)
     rc = ref().ref_render_pixels(C.byref(scene), stars.ctypes.data_as(C.POINTER(abi.Star)), len(stars),
                                  w.ctypes.data_as(C.POINTER(C.c_float)), first_pixel, n_pixels, stride,
-                                 out.ctypes.data_as(C.POINTER(C.c_double)), nthreads or os.cpu_count())
+                                 out.ctypes.data_as(C.POINTER(C.c_double)), C.byref(stp), nthreads or os.cpu_count())
     assert rc == 0, rc
-    return out, None
+    return out, {"attempts": None, "steps": stp.value}
 
 
 def count_ops(metric, fused):

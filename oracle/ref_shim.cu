@@ -292,10 +292,11 @@ extern "C" __attribute__((visibility("default"))) int ref_reflect_mirror(const m
 
 // Pixels [first, first + n*stride) of the scene (stride apart) rendered with
 // the reference's RKF45 step: mean XYZ per pixel into xyz_out (3 doubles per
-// pixel).  Kerr and Schwarzschild scenes; returns nonzero otherwise.
+// pixel); steps_out (may be NULL) receives the accepted-step total.  Kerr and
+// Schwarzschild scenes; returns nonzero otherwise.
 extern "C" __attribute__((visibility("default"))) int ref_render_pixels(
     const mgk_scene* s, const mgk_star* stars, uint32_t n_stars, const float* w, uint64_t first_pixel,
-    uint32_t n_pixels, uint64_t pixel_stride, double* xyz_out, int nthreads) {
+    uint32_t n_pixels, uint64_t pixel_stride, double* xyz_out, uint64_t* steps_out, int nthreads) {
     using namespace orc;
     if (!s || !xyz_out || (n_stars && !stars) || !w) return 2;
     if (s->metric != MGK_METRIC_KERR && s->metric != MGK_METRIC_SCHWARZSCHILD) return 1;
@@ -316,13 +317,16 @@ extern "C" __attribute__((visibility("default"))) int ref_render_pixels(
     ps.abs_tol = float(s->abs_tol);
     ps.rel_tol = float(s->rel_tol);
     ps.n_max = s->n_max_substep;
+    std::atomic<uint64_t> stp{0};
     ref_parallel_for(n_pixels, nthreads, [&](uint64_t i) {
         const uint64_t pix = first_pixel + i * pixel_stride;
         float acc[3] = {0, 0, 0};
+        uint64_t n = 0;
         for (uint32_t smp = 0; smp < spp; ++smp) {
             RayResult r = s->metric == MGK_METRIC_KERR
                               ? trace_ref<e_magik_spacetime_metric_types::KERR>(*s, c, pix * spp + smp, pk)
                               : trace_ref<e_magik_spacetime_metric_types::SCHWARZSCHILD>(*s, c, pix * spp + smp, ps);
+            n += r.steps;
             float lam[MGK_MAX_BINS], spec[MGK_MAX_BINS], o[3];
             for (uint32_t k = 0; k < nb; ++k) lam[k] = float(s->lambda_min_nm + (k + 0.5) * dl);
             Hit<float> h;
@@ -333,6 +337,8 @@ extern "C" __attribute__((visibility("default"))) int ref_render_pixels(
             for (int k = 0; k < 3; ++k) acc[k] += o[k];
         }
         for (int k = 0; k < 3; ++k) xyz_out[3 * i + k] = double(acc[k] / float(spp));
+        stp += n;
     });
+    if (steps_out) *steps_out = stp.load();
     return 0;
 }

@@ -72,6 +72,14 @@ def test_mixed_sqrt_and_reciprocal_match_their_definitions(ctx):
     assert ctx.check_rounding() == (0, 0)
 
 
+def test_peak_probes(ctx):
+    """The roofline denominators: FP32 and FP64 FMA throughput of this device
+    within the physical bounds of 148 SMs x 128 FP32 lanes at 2.1 GHz."""
+    p32, p64 = ctx.fp32_peak(), ctx.fp64_peak()
+    assert 1e13 < p32 < 148 * 128 * 2 * 2.1e9
+    assert 1e11 < p64 <= p32
+
+
 def test_trace_rays_offset_range(ctx):
     """A range that starts mid-frame and is not pixel aligned."""
     s = small_scene(spp=3)

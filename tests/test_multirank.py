@@ -59,3 +59,140 @@ def test_two_rank_weak_scaling_aggregation():
 def test_frame_seed_rank0_is_base():
     from magik_b200 import dist as D
     assert D.frame_seed(0x5EED, 0) == 0x5EED
+
+
+# ------------------------------------------- data-parallel surrogate training
+class _LinearNet:
+    """A linear least-squares model with the surrogate's step interface
+    (shuffle / gradient_step / adam_step): the host logic of the data-parallel
+    training loop without a GPU.  Its 'Adam step' is plain gradient descent on
+    the same cosine step-size schedule."""
+    grad_dtype = None  # set to torch.float64 on construction
+
+    def __init__(self, dim):
+        import torch
+        self.grad_dtype = torch.float64
+        self.w = torch.zeros(dim, dtype=torch.float64)
+        self.order = None
+
+    @property
+    def param_count(self):
+        return self.w.numel()
+
+    def shuffle(self, seed, epoch, n, stream=None):
+        import numpy as np
+        import torch
+        self.order = torch.from_numpy(np.random.default_rng([int(seed), int(epoch)]).permutation(n))
+
+    def gradient_step(self, cfg, feat, lab, first, n, grad, loss, stream=None):
+        rows = self.order[first:first + n]
+        X, y = feat[rows], lab[rows]
+        r = X @ self.w - y
+        grad.copy_((2.0 / n) * (X.T @ r))
+        loss += (r * r).mean()
+
+    def adam_step(self, cfg, grad, scale, progress, stream=None):
+        import math
+        lr = cfg.lr_final + 0.5 * (cfg.lr - cfg.lr_final) * (1.0 + math.cos(math.pi * progress))
+        self.w -= lr * (grad * scale)
+
+
+def _shard(rank, n=4096, dim=5):
+    import torch
+    g = torch.Generator().manual_seed(100 + rank)
+    X = torch.randn(n, dim, generator=g, dtype=torch.float64)
+    w_true = torch.arange(1, dim + 1, dtype=torch.float64)
+    return X, X @ w_true + 0.01 * torch.randn(n, generator=g, dtype=torch.float64)
+
+
+def _train_cfg():
+    from types import SimpleNamespace
+    return SimpleNamespace(batch=2048, epochs=3, seed=0x7EA1, lr=0.3, lr_final=0.05)
+
+
+def _union_batch_training(world, cfg):
+    """The expected run: every step a gradient step on the union of the
+    ranks' batches (the mean of the ranks' batch-mean gradients)."""
+    import math
+    import numpy as np
+    import torch
+    from magik_b200 import dist as D
+    shards = [_shard(r) for r in range(world)]
+    b = cfg.batch // world
+    n = shards[0][0].shape[0]
+    nb = n // b
+    w = torch.zeros(shards[0][0].shape[1], dtype=torch.float64)
+    losses = []
+    for ep in range(cfg.epochs):
+        orders = [torch.from_numpy(np.random.default_rng([D.frame_seed(cfg.seed, r), ep]).permutation(n))
+                  for r in range(world)]
+        tot = 0.0
+        for k in range(nb):
+            gs = []
+            for r, (X, y) in enumerate(shards):
+                rows = orders[r][k * b:(k + 1) * b]
+                res = X[rows] @ w - y[rows]
+                gs.append((2.0 / b) * (X[rows].T @ res))
+                tot += float((res * res).mean())
+            g = gs[0]
+            for h in gs[1:]:
+                g = g + h
+            lr = cfg.lr_final + 0.5 * (cfg.lr - cfg.lr_final) * (1.0 + math.cos(math.pi * (ep * nb + k) / (cfg.epochs * nb)))
+            w = w - lr * (g * (1.0 / world))
+        losses.append(tot / (nb * world))
+    return w, losses
+
+
+def _dp_worker(rank, world, port, q):
+    import datetime
+    import torch.distributed as dist
+    from magik_b200 import dist as D
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        net = _LinearNet(5)
+        X, y = _shard(rank)
+        losses = D.train_data_parallel(net, _train_cfg(), X, y)
+        q.put((rank, net.w.tolist(), [float(v) for v in losses]))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_rank_data_parallel_training_is_union_batch_training():
+    """Two gloo ranks with their own shards end with the same parameters,
+    those of training on the union batches, and report the mean loss of
+    both ranks' batches."""
+    import numpy as np
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_dp_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    out = sorted(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    w_want, loss_want = _union_batch_training(2, _train_cfg())
+    assert out[0][1] == out[1][1]  # every rank holds the same parameters
+    np.testing.assert_allclose(out[0][1], w_want.tolist(), rtol=1e-12, atol=1e-14)
+    np.testing.assert_allclose(out[0][2], loss_want, rtol=1e-6)
+    assert out[0][2][-1] < 0.1 * out[0][2][0]  # it trains
+
+
+def test_one_rank_data_parallel_training_and_batch_checks():
+    import numpy as np
+    from magik_b200 import dist as D
+    cfg = _train_cfg()
+    net = _LinearNet(5)
+    X, y = _shard(0)
+    losses = D.train_data_parallel(net, cfg, X, y)
+    w_want, loss_want = _union_batch_training(1, cfg)
+    np.testing.assert_allclose(net.w.numpy(), w_want.numpy(), rtol=1e-12, atol=1e-14)
+    np.testing.assert_allclose(losses, loss_want, rtol=1e-6)
+    cfg.batch = 1000
+    with pytest.raises(ValueError):
+        D.train_data_parallel(_LinearNet(5), cfg, X, y)
+    cfg.batch = 8192
+    with pytest.raises(ValueError):  # fewer samples than one batch
+        D.train_data_parallel(_LinearNet(5), cfg, X, y)

@@ -111,10 +111,14 @@ def test_oracle_render_matches_reference_step_render(metric):
     stars = M.star_catalog(0x57A25, 20000)
     w = M.xyz_weights(s.n_bins)
     n = s.width * s.height
-    a, _ = O.render_pixels(s, stars, w, 0, n, nthreads=4)
-    b, _ = O.ref_render_pixels(s, stars, w, 0, n, nthreads=4)
+    a, ca = O.render_pixels(s, stars, w, 0, n, nthreads=4)
+    b, cb = O.ref_render_pixels(s, stars, w, 0, n, nthreads=4)
     assert np.mean(np.all(a == b, axis=1)) >= 0.98
     assert np.abs(a - b).sum() <= 1e-5 * np.abs(a).sum()
+    # the step totals the CPU baselines report: the per-ray records summed
+    rec = O.trace_rays(s, 0, n)
+    assert ca["steps"] == int(rec["steps"].sum()) and ca["attempts"] == int(rec["attempts"].sum())
+    assert abs(cb["steps"] - ca["steps"]) <= 1e-3 * ca["steps"]
 
 
 def test_reference_inverse_cdf_golden():
