@@ -835,17 +835,24 @@ __global__ void __launch_bounds__(256) k_shade(const DevScene<T> P, const HitEnt
                                                StarGridDev grid, const float* __restrict__ d_w,
                                                float* __restrict__ xyz_ray, float* __restrict__ film_spec,
                                                uint64_t first_ray) {
-    __shared__ float sw[3 * MGK_MAX_BINS];
-    __shared__ T sa[MGK_MAX_BINS], sb[MGK_MAX_BINS];
+    // per bin: the XYZ weights as one 16-byte and the Planck factors as one
+    // 8- or 16-byte shared-memory load
+    struct alignas(2 * sizeof(T)) PlanckAB { T a, b; };
+    __shared__ float4 sw[MGK_MAX_BINS];
+    __shared__ PlanckAB sab[MGK_MAX_BINS];
     __shared__ float sicdf[MGK_CMF_ICDF_ENTRIES];
     const uint32_t nb = P.n_bins;
     const bool sampled = P.spectral_mode == MGK_SPECTRAL_SAMPLED;
-    for (uint32_t i = threadIdx.x; i < 3 * MGK_MAX_BINS; i += blockDim.x)
-        sw[i] = i < 3 * nb ? (d_w ? d_w[i] : P.xyz_w[i]) : 0.f;
     for (uint32_t i = threadIdx.x; i < MGK_MAX_BINS; i += blockDim.x) {
-        sa[i] = P.planck_a[i];
+        float4 w4 = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (i < nb) {
+            const float* src = d_w ? d_w : P.xyz_w;
+            w4 = make_float4(src[3 * i], src[3 * i + 1], src[3 * i + 2], 0.f);
+        }
+        sw[i] = w4;
         // float: b_k log2(e), for exp(b_k u) = 2^(b_k log2(e) u) in one ex2
-        sb[i] = std::is_same_v<T, float> ? T(P.planck_b[i] * T(1.4426950408889634)) : P.planck_b[i];
+        sab[i] = PlanckAB{P.planck_a[i],
+                          std::is_same_v<T, float> ? T(P.planck_b[i] * T(1.4426950408889634)) : P.planck_b[i]};
     }
     for (uint32_t i = threadIdx.x; i < MGK_CMF_ICDF_ENTRIES; i += blockDim.x) sicdf[i] = sampled ? P.cmf_icdf[i] : 0.f;
     __syncthreads();
@@ -876,20 +883,22 @@ __global__ void __launch_bounds__(256) k_shade(const DevScene<T> P, const HitEnt
                 return;
             }
             for (uint32_t k = 0; k < nb; ++k) {
+                const PlanckAB ab = sab[k];
                 float sv;
                 if constexpr (std::is_same_v<T, float>) {
                     // ex2.approx and the corrected reciprocal: a few ulp, far
                     // inside the film's 1e-4 (b_k u >= 0.2 for every emitter here,
                     // so e - 1 loses at most 2^-23 / 0.2 to cancellation).  e = 1
                     // or inf gives NaN, cleared by the clamp like the quotient's inf / 0.
-                    const float e = ex2_approx(sb[k] * u);
-                    sv = clamp_radiance<float>(amp * (sa[k] * mrcp(e - 1.0f)));
+                    const float e = ex2_approx(ab.b * u);
+                    sv = clamp_radiance<float>(amp * (ab.a * mrcp(e - 1.0f)));
                 } else {
-                    sv = float(clamp_radiance<T>(amp * (sa[k] / (exp(sb[k] * u) - T(1)))));
+                    sv = float(clamp_radiance<T>(amp * (ab.a / (exp(ab.b * u) - T(1)))));
                 }
-                X = __fmaf_rn(sv, sw[3 * k], X);
-                Y = __fmaf_rn(sv, sw[3 * k + 1], Y);
-                Z = __fmaf_rn(sv, sw[3 * k + 2], Z);
+                const float4 w = sw[k];
+                X = __fmaf_rn(sv, w.x, X);
+                Y = __fmaf_rn(sv, w.y, Y);
+                Z = __fmaf_rn(sv, w.z, Z);
                 if (spec) atomicAdd(spec + k, sv * P.inv_spp);
             }
         };
@@ -905,9 +914,10 @@ __global__ void __launch_bounds__(256) k_shade(const DevScene<T> P, const HitEnt
             } else {
                 for (uint32_t k = 0; k < nb; ++k) {
                     float sv = float(clamp_radiance<T>(white_led<T>(h.z * P.lambda[k]) * P.light_scale * z5));
-                    X = __fmaf_rn(sv, sw[3 * k], X);
-                    Y = __fmaf_rn(sv, sw[3 * k + 1], Y);
-                    Z = __fmaf_rn(sv, sw[3 * k + 2], Z);
+                    const float4 w = sw[k];
+                    X = __fmaf_rn(sv, w.x, X);
+                    Y = __fmaf_rn(sv, w.y, Y);
+                    Z = __fmaf_rn(sv, w.z, Z);
                     if (spec) atomicAdd(spec + k, sv * P.inv_spp);
                 }
             }
@@ -931,9 +941,10 @@ __global__ void __launch_bounds__(256) k_shade(const DevScene<T> P, const HitEnt
                     const T phi1 = T(0.5) * (T(1) + erf((e1 - lam) * P.inv_sigma_sqrt2));
                     const float sv = float(irr * (phi1 - phi0));
                     phi0 = phi1;
-                    X = __fmaf_rn(sv, sw[3 * k], X);
-                    Y = __fmaf_rn(sv, sw[3 * k + 1], Y);
-                    Z = __fmaf_rn(sv, sw[3 * k + 2], Z);
+                    const float4 w = sw[k];
+                    X = __fmaf_rn(sv, w.x, X);
+                    Y = __fmaf_rn(sv, w.y, Y);
+                    Z = __fmaf_rn(sv, w.z, Z);
                     if (spec) atomicAdd(spec + k, sv * P.inv_spp);
                 }
             }
