@@ -570,7 +570,9 @@ def run_gpu(args, rank, world, local_rank):
                                       [int(c) for c in st_last.class_count])),
                   "attempts_per_ray": st_last.attempts / rays},
         "clocks": clk,
-        "gpu_launches": 10 * args.steps,
+        # per frame: generate, integrate, refine, tail, shade, resolve; next-pass,
+        # integrate and refine for each continuation pass; four star-grid kernels
+        "gpu_launches": (6 + 3 * (int(st_last.n_passes) - 1) + 4) * args.steps,
         "film_finite": film_ok,
     }
     if world == 1 and not args.no_stress:
