@@ -449,7 +449,9 @@ def run_display(args, ctx):
                                  "peak_source": f"MEASURED_PEAKS.json hbm_gbs, {peak_src}",
                                  "note": ("instruction-bound, not HBM-bound: ncu 90 % issue, 3.7 % DRAM "
                                           "(profiles/queues_film_display_640x360x16.md)") if key == "gt7" else
-                                         "24 bytes per pixel moved"}}
+                                         ("24 bytes per pixel moved; three full-accuracy powf per pixel (the sRGB "
+                                          "encode) set the time, not the bytes "
+                                          "(profiles/queues_film_display_640x360x16.md)")}}
     return out
 
 
