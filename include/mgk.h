@@ -161,7 +161,7 @@ typedef struct mgk_scene {
  *  MGK_SPECTRAL_SAMPLED: the reference renderer's stochastic mode.  Each ray
  *    draws one wavelength from the CIE inverse CDF table
  *    (device_sensor_utilities.cuh:25-33; 256 entries, built like
- *    host_color_utilities.cuh:188-233 from the analytic colour-matching
+ *    host_color_utilities.cuh:188-233 from the tabulated CIE 1931
  *    functions), its radiance there carries the throughput 1/pdf, is turned
  *    into sensor irradiance (device_color_utilities.cuh:22-29) and spread over
  *    the bins with a Gaussian of redistribution_sigma_nm
@@ -245,16 +245,23 @@ MGK_API double mgk_isco_radius(double spin);
 
 /* ---------------------------------------------------- host utilities */
 /* Per-bin CIE 1931 XYZ weights w[3*k + c] for n_bins uniform bins over
- * [lambda_min, lambda_max], normalised like compute_normalized_isi_cmf_weights
- * (host_color_utilities.cuh:145-178); the colour-matching functions are the
- * multi-lobe Gaussian fit of Wyman, Sloan and Shirley (JCGT 2(2), 2013). */
+ * [lambda_min, lambda_max] (taken as float), computed in float from the
+ * tabulated CIE 1931 2-degree observer (1 nm, 360-830 nm) exactly as the
+ * reference's compute_normalized_isi_cmf_weights does
+ * (host_color_utilities.cuh:145-178, color_matching_functions.cuh:22-44). */
 MGK_API mgk_result mgk_xyz_weights(uint32_t n_bins, double lambda_min_nm, double lambda_max_nm, float* w_out);
+/* Opt-in: the same normalisation in double over the multi-lobe Gaussian fit
+ * of the CIE 1931 functions (Wyman, Sloan and Shirley, JCGT 2(2), 2013);
+ * within 1 % of the peak weight of mgk_xyz_weights.  No reference counterpart. */
+MGK_API mgk_result mgk_xyz_weights_analytic(uint32_t n_bins, double lambda_min_nm, double lambda_max_nm, float* w_out);
 /* The CIE inverse CDF table of the sampled spectral mode (MGK_SPECTRAL_SAMPLED)
  * for [lambda_min_nm, lambda_max_nm]: MGK_CMF_ICDF_ENTRIES wavelengths (nm) at
- * equidistant probabilities, built as the reference's
- * compute_tabulated_cmf_inverse_cdf (host_color_utilities.cuh:188-233,
- * floor 5 %) from the analytic colour-matching functions.  Host only. */
+ * equidistant probabilities, built in float from the tabulated CIE 1931
+ * functions as the reference's compute_tabulated_cmf_inverse_cdf
+ * (host_color_utilities.cuh:188-233, floor 5 %).  Host only. */
 MGK_API mgk_result mgk_cmf_inverse_cdf(double lambda_min_nm, double lambda_max_nm, float* table_out);
+/* Opt-in: the same table from the analytic fit (no reference counterpart). */
+MGK_API mgk_result mgk_cmf_inverse_cdf_analytic(double lambda_min_nm, double lambda_max_nm, float* table_out);
 
 /* Seeded star catalogue: directions uniform on the sphere, magnitudes uniform
  * in [0, 10] (fluxes log-uniform over four decades), temperatures uniform in
@@ -382,8 +389,8 @@ MGK_API void mgk_display_defaults(mgk_display_settings* ds);
 
 /* Host: the pipeline of the settings, as color_pipeline_descriptor_t::create
  * and the view transforms' make_params build it (the white point integrates
- * the blackbody against the analytic colour-matching functions at the 471
- * wavelengths of the reference's CIE table). */
+ * the blackbody against the tabulated CIE 1931 functions at their 471
+ * wavelengths, as compute_white_point_xyz does). */
 MGK_API mgk_result mgk_display_prepare(const mgk_display_settings* ds, mgk_display_pipeline* out);
 
 /* Device: n_pixels XYZ triples (d_xyz, e.g. an mgk_render film) -> display

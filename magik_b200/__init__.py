@@ -32,7 +32,7 @@ EXPORTS = [
     "mgk_context_create", "mgk_context_destroy", "mgk_last_error", "mgk_scene_defaults", "mgk_isco_radius",
     "mgk_xyz_weights", "mgk_star_catalog", "mgk_scene_constants", "mgk_render", "mgk_render_host",
     "mgk_trace_rays", "mgk_shade_rays", "magik_trace_geodesic", "mgk_trace_geodesic_batch", "mgk_fp32_peak", "mgk_fp64_peak",
-    "mgk_check_rounding", "mgk_cmf_inverse_cdf", "mgk_display_defaults", "mgk_display_prepare", "mgk_display",
+    "mgk_check_rounding", "mgk_cmf_inverse_cdf", "mgk_xyz_weights_analytic", "mgk_cmf_inverse_cdf_analytic", "mgk_display_defaults", "mgk_display_prepare", "mgk_display",
     "mgk_trace_rays_static", "mgk_train_defaults", "mgk_surrogate_param_count", "mgk_surrogate_create",
     "mgk_surrogate_destroy", "mgk_surrogate_get_params", "mgk_surrogate_set_params", "mgk_make_samples",
     "mgk_surrogate_forward", "mgk_surrogate_forward_tiled", "mgk_surrogate_status", "mgk_surrogate_gradient", "mgk_surrogate_train", "mgk_render_surrogate",
@@ -64,6 +64,7 @@ def lib():
         L.mgk_isco_radius.argtypes = [C.c_double]
         L.mgk_isco_radius.restype = C.c_double
         L.mgk_xyz_weights.argtypes = [C.c_uint32, C.c_double, C.c_double, P(C.c_float)]
+        L.mgk_xyz_weights_analytic.argtypes = [C.c_uint32, C.c_double, C.c_double, P(C.c_float)]
         L.mgk_star_catalog.argtypes = [C.c_uint64, C.c_uint32, vp]
         L.mgk_scene_constants.argtypes = [P(Scene), P(C.c_double)]
         L.mgk_render.argtypes = [vp, P(Scene), vp, C.c_uint32, vp, vp, vp, P(RenderStats), vp]
@@ -79,6 +80,7 @@ def lib():
         L.mgk_fp64_peak.argtypes = [vp, P(C.c_double)]
         L.mgk_check_rounding.argtypes = [vp, P(C.c_uint64)]
         L.mgk_cmf_inverse_cdf.argtypes = [C.c_double, C.c_double, P(C.c_float)]
+        L.mgk_cmf_inverse_cdf_analytic.argtypes = [C.c_double, C.c_double, P(C.c_float)]
         L.mgk_display_defaults.argtypes = [P(abi.DisplaySettings)]
         L.mgk_display_defaults.restype = None
         L.mgk_display_prepare.argtypes = [P(abi.DisplaySettings), P(abi.DisplayPipeline)]
@@ -134,17 +136,21 @@ def isco_radius(spin):
     return lib().mgk_isco_radius(float(spin))
 
 
-def xyz_weights(n_bins, lambda_min_nm=380.0, lambda_max_nm=780.0):
+def xyz_weights(n_bins, lambda_min_nm=380.0, lambda_max_nm=780.0, analytic=False):
+    """mgk_xyz_weights: per-bin XYZ weights (n_bins x 3) from the tabulated
+    CIE 1931 observer; `analytic` selects mgk_xyz_weights_analytic."""
     out = (C.c_float * (3 * n_bins))()
-    _check(lib().mgk_xyz_weights(n_bins, lambda_min_nm, lambda_max_nm, out), "mgk_xyz_weights")
+    fn = "mgk_xyz_weights_analytic" if analytic else "mgk_xyz_weights"
+    _check(getattr(lib(), fn)(n_bins, lambda_min_nm, lambda_max_nm, out), fn)
     return np.frombuffer(out, dtype=np.float32).reshape(n_bins, 3).copy()
 
 
-def cmf_inverse_cdf(lambda_min_nm=380.0, lambda_max_nm=780.0):
+def cmf_inverse_cdf(lambda_min_nm=380.0, lambda_max_nm=780.0, analytic=False):
     """mgk_cmf_inverse_cdf: the sampled spectral mode's CIE inverse CDF table
-    (256 wavelengths in nm)."""
+    (256 wavelengths in nm); `analytic` selects the table of the analytic fit."""
     out = (C.c_float * abi.CMF_ICDF_ENTRIES)()
-    _check(lib().mgk_cmf_inverse_cdf(lambda_min_nm, lambda_max_nm, out), "mgk_cmf_inverse_cdf")
+    fn = "mgk_cmf_inverse_cdf_analytic" if analytic else "mgk_cmf_inverse_cdf"
+    _check(getattr(lib(), fn)(lambda_min_nm, lambda_max_nm, out), fn)
     return np.frombuffer(out, dtype=np.float32).copy()
 
 

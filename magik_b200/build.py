@@ -18,7 +18,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmgk.so")
 SOURCES = ["kernels.cu", "api.cu", "static_scratch.cu", "mlp.cu", "mlp_tc.cu", "surrogate.cu", "display.cu",
            "manager.cu"]
-HEADERS = ["dev_physics.cuh", "dev_pair.cuh", "dev_scene.cuh", "internal.h", os.path.join("..", "..", "include", "mgk.h"),
+HEADERS = ["dev_physics.cuh", "dev_pair.cuh", "dev_scene.cuh", "internal.h", "cie1931_2deg.inc", os.path.join("..", "..", "include", "mgk.h"),
            os.path.join("..", "..", "include", "mgk_manager.h")]
 
 NVCC_FLAGS = [

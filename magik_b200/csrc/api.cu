@@ -131,7 +131,17 @@ mgk_result validate(const mgk_scene* s) {
     return MGK_SUCCESS;
 }
 
-// ----------------------------------------------------- CIE 1931 (analytic)
+// --------------------------------------------------------- CIE 1931 data
+// The CIE 1931 2-degree standard observer at 1 nm over 360-830 nm, the
+// published standard data the reference tabulates
+// (color_matching_functions.cuh:22-28).
+const float kCie1931[471][3] = {
+#include "cie1931_2deg.inc"
+};
+constexpr uint32_t kCieEntries = 471;
+constexpr float kCieMinNm = 360.0f, kCieMaxNm = 830.0f;
+
+// ------------------------------------------- CIE 1931 (analytic, opt-in)
 // Multi-lobe piecewise-Gaussian fit of the CIE 1931 2-degree observer from
 // Wyman, Sloan and Shirley, "Simple Analytic Approximations to the CIE XYZ
 // Color Matching Functions", JCGT 2(2), 2013.
@@ -139,7 +149,7 @@ double lobe(double l, double mu, double s1, double s2) {
     double t = (l - mu) / (l < mu ? s1 : s2);
     return std::exp(-0.5 * t * t);
 }
-void cmf_1931(double l, double out[3]) {
+void cmf_1931_fit(double l, double out[3]) {
     out[0] = 1.056 * lobe(l, 599.8, 37.9, 31.0) + 0.362 * lobe(l, 442.0, 16.0, 26.7) - 0.065 * lobe(l, 501.1, 20.4, 26.2);
     out[1] = 0.821 * lobe(l, 568.8, 46.9, 40.5) + 0.286 * lobe(l, 530.9, 16.3, 31.1);
     out[2] = 1.217 * lobe(l, 437.0, 11.8, 36.0) + 0.681 * lobe(l, 459.0, 26.0, 13.8);
@@ -164,28 +174,44 @@ uint32_t grid_n(double radius) {
 }  // namespace
 
 namespace mgk {
-void cmf_1931_values(double nm, double out[3]) { cmf_1931(nm, out); }
+// The tabulated CIE 1931 functions at `nm`, interpolated linearly between
+// the 1 nm entries in float and clamped to the table's ends, in the order of
+// operations of sample_equidistant_spectral_data and lerp
+// (color_matching_functions.cuh:35-44, internal_math.h:2040-2043).
+void cie1931_sample(float nm, float out[3]) {
+    const float spacing = (kCieMaxNm - kCieMinNm) / float(kCieEntries - 1);
+    const float fi = std::fmin(std::fmax((nm - kCieMinNm) / spacing, 0.0f), float(kCieEntries - 1));
+    const uint32_t lower = uint32_t(std::fmin(float(uint32_t(fi)), float(kCieEntries - 2)));
+    const float t = fi - float(lower);
+    for (int c = 0; c < 3; ++c) out[c] = (kCie1931[lower][c] * (1.0f - t)) + (kCie1931[lower + 1][c] * t);
+}
 
 // CIE inverse CDF table of the sampled spectral mode, as the reference builds
-// it (host_color_utilities.cuh:188-233) in float: the colour-matching
-// functions resampled at 471 points over [lmin, lmax] (the reference's 1 nm
-// CIE 1931 table has 471 entries), s = x + y + z, a trapezoid CDF with a
-// floor of 5 % of the mean of s per unit wavelength, normalised, inverted at
-// 256 equidistant probabilities by linear interpolation.
-void cmf_inverse_cdf_table(double lmin_d, double lmax_d, float* out) {
-    constexpr uint32_t n_entries = 471;
-    const uint32_t n = n_entries - 1;
+// it (host_color_utilities.cuh:188-233) in float: the tabulated functions
+// resampled at 471 points over [lmin, lmax], s = x + y + z, a trapezoid CDF
+// with a floor of 5 % of the mean of s per unit wavelength, normalised,
+// inverted at 256 equidistant probabilities by linear interpolation.  With
+// `fit` the analytic functions stand in for the table.
+void cmf_inverse_cdf_table(double lmin_d, double lmax_d, float* out, bool fit) {
+    const uint32_t n = kCieEntries - 1;
     const float lmin = float(lmin_d), lmax = float(lmax_d);
     const float dl = (lmax - lmin) / float(n);
-    std::vector<float> s(n_entries);
-    for (uint32_t i = 0; i < n_entries; ++i) {
-        double c[3];
-        cmf_1931(double(lmin + float(i) * dl), c);
-        s[i] = (float(c[0]) + float(c[1])) + float(c[2]);
+    std::vector<float> s(kCieEntries);
+    for (uint32_t i = 0; i < kCieEntries; ++i) {
+        const float nm = lmin + float(i) * dl;
+        float c[3];
+        if (fit) {
+            double d[3];
+            cmf_1931_fit(double(nm), d);
+            c[0] = float(d[0]); c[1] = float(d[1]); c[2] = float(d[2]);
+        } else {
+            cie1931_sample(nm, c);
+        }
+        s[i] = (c[0] + c[1]) + c[2];
     }
     float mean = 0.0f;
-    for (uint32_t i = 0; i < n_entries; ++i) mean += s[i];
-    mean /= float(n_entries);
+    for (uint32_t i = 0; i < kCieEntries; ++i) mean += s[i];
+    mean /= float(kCieEntries);
     const float floor = 0.05f * mean;
     std::vector<float> cdf(n + 1, 0.0f);
     for (uint32_t i = 0; i < n; ++i) cdf[i + 1] = cdf[i] + (0.5f * (s[i] + s[i + 1]) + floor) * dl;
@@ -625,11 +651,38 @@ MGK_API void mgk_scene_defaults(mgk_scene* s) {
     s->light_scale = 7.0e5;
 }
 
-MGK_API mgk_result mgk_xyz_weights(uint32_t n_bins, double lmin, double lmax, float* w_out) {
+MGK_API mgk_result mgk_xyz_weights(uint32_t n_bins, double lmin_d, double lmax_d, float* w_out) {
+    if (!w_out) return MGK_ERROR_INVALID_POINTER;
+    if (n_bins < 1 || n_bins > MGK_MAX_BINS || !(lmax_d > lmin_d)) return MGK_ERROR_INVALID_ARGUMENT;
+    // compute_normalized_isi_cmf_weights (host_color_utilities.cuh:145-178) in
+    // float over the tabulated functions: each bin midpoint-sampled at the
+    // table's 1 nm spacing, then normalised by sum(Y) and the bin width.
+    const float lmin = float(lmin_d), lmax = float(lmax_d);
+    const float bin = (lmax - lmin) / float(n_bins);
+    const float cmf_bin = (kCieMaxNm - kCieMinNm) / float(kCieEntries - 1);
+    const uint32_t sub = uint32_t(std::ceil(bin / cmf_bin));
+    const float dsub = bin / float(sub);
+    float sum_y = 0.0f;
+    for (uint32_t i = 0; i < n_bins; ++i) {
+        const float x0 = lmin + float(i) * bin;
+        float w[3] = {0.0f, 0.0f, 0.0f};
+        for (uint32_t j = 0; j < sub; ++j) {
+            float c[3];
+            cie1931_sample(x0 + (float(j) + 0.5f) * dsub, c);
+            for (int k = 0; k < 3; ++k) w[k] += c[k] * dsub;
+        }
+        for (int k = 0; k < 3; ++k) w_out[3 * i + k] = w[k];
+        sum_y += w[1];
+    }
+    const float scale = (1.0f / sum_y) * (1.0f / bin);
+    for (uint32_t i = 0; i < 3 * n_bins; ++i) w_out[i] *= scale;
+    return MGK_SUCCESS;
+}
+
+MGK_API mgk_result mgk_xyz_weights_analytic(uint32_t n_bins, double lmin, double lmax, float* w_out) {
     if (!w_out) return MGK_ERROR_INVALID_POINTER;
     if (n_bins < 1 || n_bins > MGK_MAX_BINS || !(lmax > lmin)) return MGK_ERROR_INVALID_ARGUMENT;
-    // host_color_utilities.cuh:145-178: midpoint sub-sampling of each bin at the
-    // 1 nm spacing of the tabulated CIE data, normalised by sum(Y) and bin width.
+    // the same normalisation in double over the analytic functions
     const double bin = (lmax - lmin) / n_bins;
     const uint32_t sub = uint32_t(std::ceil(bin / 1.0));
     const double dsub = bin / sub;
@@ -638,7 +691,7 @@ MGK_API mgk_result mgk_xyz_weights(uint32_t n_bins, double lmin, double lmax, fl
     for (uint32_t i = 0; i < n_bins; ++i) {
         for (uint32_t j = 0; j < sub; ++j) {
             double c[3];
-            cmf_1931(lmin + i * bin + (j + 0.5) * dsub, c);
+            cmf_1931_fit(lmin + i * bin + (j + 0.5) * dsub, c);
             for (int k = 0; k < 3; ++k) acc[3 * i + k] += c[k] * dsub;
         }
         sum_y += acc[3 * i + 1];
@@ -650,7 +703,14 @@ MGK_API mgk_result mgk_xyz_weights(uint32_t n_bins, double lmin, double lmax, fl
 MGK_API mgk_result mgk_cmf_inverse_cdf(double lmin, double lmax, float* table_out) {
     if (!table_out) return MGK_ERROR_INVALID_POINTER;
     if (!(lmax > lmin) || !(lmin > 0.0)) return MGK_ERROR_INVALID_ARGUMENT;
-    cmf_inverse_cdf_table(lmin, lmax, table_out);
+    cmf_inverse_cdf_table(lmin, lmax, table_out, false);
+    return MGK_SUCCESS;
+}
+
+MGK_API mgk_result mgk_cmf_inverse_cdf_analytic(double lmin, double lmax, float* table_out) {
+    if (!table_out) return MGK_ERROR_INVALID_POINTER;
+    if (!(lmax > lmin) || !(lmin > 0.0)) return MGK_ERROR_INVALID_ARGUMENT;
+    cmf_inverse_cdf_table(lmin, lmax, table_out, true);
     return MGK_SUCCESS;
 }
 

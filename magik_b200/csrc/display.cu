@@ -168,9 +168,9 @@ V3 white_point_xyz(float temperature, float tint) {
     float lam = 360.0f;
     const float step = (830.0f - 360.0f) / 470.0f;
     for (int i = 0; i < 471; ++i) {
-        double c[3];
-        cmf_1931_values(double(lam), c);
-        const V3 cm{float(c[0]), float(c[1]), float(c[2])};
+        float c[3];
+        cie1931_sample(lam, c);
+        const V3 cm{c[0], c[1], c[2]};
         const float p0 = planck_f(lam, temperature), p1 = planck_f(lam, temperature + 1.0f);
         b0 = V3{b0.x + cm.x * p0, b0.y + cm.y * p0, b0.z + cm.z * p0};
         b1 = V3{b1.x + cm.x * p1, b1.y + cm.y * p1, b1.z + cm.z * p1};

@@ -116,16 +116,18 @@ cudaError_t launch_trace_geodesic(const void* jobs, uint32_t n, void* steps, uin
 size_t dev_scene_size(const mgk_scene& s);
 // Fills the device-scene table (host memory, dev_scene_size bytes).
 void fill_dev_scene(const mgk_scene& s, const float* xyz_w, void* out);
-// The analytic CIE 1931 colour-matching functions (x, y, z) at nm (api.cu).
-void cmf_1931_values(double nm, double out[3]);
+// The tabulated CIE 1931 colour-matching functions (x, y, z) at nm, linearly
+// interpolated in float (api.cu).
+void cie1931_sample(float nm, float out[3]);
 // The colour resolve (display.cu).
 void display_defaults(mgk_display_settings* ds);
 mgk_result display_prepare(const mgk_display_settings& s, mgk_display_pipeline* out);
 cudaError_t launch_display(const mgk_display_pipeline& p, const float* xyz, uint64_t n, float* rgb,
                            cudaStream_t stream);
 // The CIE inverse CDF table of the sampled spectral mode (api.cu):
-// MGK_CMF_ICDF_ENTRIES wavelengths in nm.
-void cmf_inverse_cdf_table(double lmin_nm, double lmax_nm, float* out);
+// MGK_CMF_ICDF_ENTRIES wavelengths in nm, from the tabulated CIE 1931
+// functions (or the analytic fit with `fit`).
+void cmf_inverse_cdf_table(double lmin_nm, double lmax_nm, float* out, bool fit = false);
 
 // One geodesic of the reference-compatible trace API (host-prepared inputs).
 struct TraceJob {
