@@ -31,9 +31,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 # DRAM bytes per ray of k_integrate and per row of k_mlp_infer_tc, from one
-# ncu capture each of a smaller case (profiles/k_integrate_kerr_640x360x16.md,
-# profiles/k_mlp_infer_tc_1M_rows.md); the traffic grows with the units, so
-# the roofline scales it to the launch.
+# ncu capture each of a smaller case (640x360x16 rays; 2^20 rows); the
+# traffic grows with the units, so the roofline scales it to the launch.
 INTEGRATE_DRAM_BYTES_PER_RAY = 617.4e6 / 3_686_400
 MLP_DRAM_BYTES_PER_ROW = 44.2e6 / 1_048_576
 N_STARS = 100_000
@@ -71,20 +70,27 @@ def scene_config(M, rank=0):
     from magik_b200.dist import frame_seed
     s = M.scene_defaults()
     s.seed = frame_seed(0x5EED, rank)
+    _resize(s)
+    return s
+
+
+def _resize(s):
     if ARGS is not None:
         for k in ("width", "height", "spp"):
             v = getattr(ARGS, k)
             if v:
                 setattr(s, k, v)
-    return s
 
 
-def config_dict(s, extra=None):
+MIXED_PRECISION = "mixed (fp32 state and step control, fp64 attempts within 0.05 M of the horizon)"
+
+
+def config_dict(s, extra=None, precision=MIXED_PRECISION):
     name = WORKLOAD if (s.width, s.height, s.spp) == (1920, 1080, 16) else f"{WORKLOAD} resized to {s.width}x{s.height}x{s.spp}spp (profiling size)"
     d = {"workload": name, "metric_tensor": "kerr", "spin": s.spin, "width": s.width, "height": s.height,
          "spp": s.spp, "rays_per_frame": s.width * s.height * s.spp, "n_bins": s.n_bins, "stars": N_STARS,
          "rel_tol": s.rel_tol, "abs_tol": s.abs_tol,
-        "precision": "mixed (fp32 state and step control, fp64 attempts within 0.05 M of the horizon)",
+         "precision": precision,
          "l2": "a 512 MiB buffer is written between timed frames (frame traffic is also > L2)"}
     if extra:
         d.update(extra)
@@ -169,39 +175,61 @@ def cpu_render_sample(s, stars, w, seconds, precision, reference=False):
     rays = n * s.spp
     desc = (f"{n} of {npix} pixels (every {stride}th) x {s.spp} spp = {rays} geodesics, "
             f"{counts['steps']} steps in {dt:.1f} s")
+    cpu_render_sample.last_ms = dt * 1e3
     return rays / dt, counts["steps"] / dt, threads, desc
 
 
 # ------------------------------------------------------------------ arms
 def run_reference(args, rank, world):
-    """The reference arm: the reference's CPU geodesic integration on the host cores."""
+    """The reference arm: the reference's own RKF45 (metric_kerr.cuh /
+    internal_math.h compiled from its sources into oracle/_ref) per camera
+    ray on all host cores, with the reference's own CIE weights.  Everything
+    it needs comes from oracle/: the scene (the oracle's restatement of the
+    workload's defaults), the star catalogue and, where oracle/_ref is
+    absent, the oracle port in the reference's arithmetic.  It neither
+    imports the magik_b200 package nor loads libmgk.so.  Rank 0 alone runs."""
     if rank != 0:
         return None
-    import magik_b200 as M
     from oracle import oracle_py as O
-    s = scene_config(M)
-    stars = M.star_catalog(STAR_SEED, N_STARS)
-    w = M.xyz_weights(s.n_bins)
+    abi = O.abi
+    s = O.scene_defaults()
+    _resize(s)
+    stars = O.star_catalog(STAR_SEED, N_STARS)
     use_ref = O.ref_available() and hasattr(O, "ref_render_pixels")
+    if use_ref:
+        w = O.ref_cmf_weights(s.n_bins, s.lambda_min_nm, s.lambda_max_nm)
+    else:
+        w = np.load(os.path.join(ROOT, "tests", "golden", "ref_cmf_weights.npz"))[
+            f"w{s.n_bins}_{int(s.lambda_min_nm)}_{int(s.lambda_max_nm)}"]
     kind = "reference" if use_ref else "port"
     per = max(2.0, min(args.cpu_seconds, 120.0 / max(1, args.steps + args.warmup)))
-    vals, svals, desc, threads = [], [], "", 1
+    vals, svals, step_ms, desc, threads = [], [], [], "", 1
     for i in range(args.warmup + args.steps):
-        v, sv, threads, desc = cpu_render_sample(s, stars, w, per, M.abi.PRECISION_REF32, reference=use_ref)
+        v, sv, threads, desc = cpu_render_sample(s, stars, w, per, abi.PRECISION_REF32, reference=use_ref)
         if i >= args.warmup:
             vals.append(v)
             svals.append(sv)
+            step_ms.append(cpu_render_sample.last_ms)
     value = statistics.mean(vals)
+    rays = s.width * s.height * s.spp
     what = ("the reference's own RKF45 (metric_kerr.cuh / internal_math.h compiled from its sources) per camera "
-            "ray, with the disk, escape, star and spectral stages of the CPU oracle, which the reference lacks"
-            if use_ref else "the CPU oracle in REF32 arithmetic")
+            "ray, with the disk, escape, star and spectral stages of the CPU oracle, which the reference lacks, "
+            "and the reference's own CIE 1931 bin weights"
+            if use_ref else "the CPU oracle in REF32 arithmetic (the reference's operation order)")
+    precision = "fp32 (REF32: the reference's arithmetic and step control)"
     return {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+            "steps": args.steps, "warmup": args.warmup,
+            # each step renders a strided pixel sample of the frame (cpu_baseline.sample)
+            "ms_per_step": statistics.mean(step_ms), "ms_per_frame_equivalent": rays / value * 1e3,
+            "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic (seeded)",
-            "config": config_dict(s), "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads,
-                                                        "kind": kind, "sample": desc, "what": what,
-                                                        "steps_per_s": statistics.mean(svals)},
-            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "config": config_dict(s, precision=precision),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+                             "sample": desc + "; a step is one such sample; ms_per_frame_equivalent is the "
+                                       "time the whole frame takes at the sample's rate",
+                             "what": what, "steps_per_s": statistics.mean(svals)},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "package_imported": "magik_b200" in sys.modules}
 
 
 # The pool's earlier measurement of HBM copy bandwidth and cuBLAS BF16 burst
@@ -447,11 +475,10 @@ def run_display(args, ctx):
                     "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s",
                                  "frac": gbs / peak if peak else None,
                                  "peak_source": f"MEASURED_PEAKS.json hbm_gbs, {peak_src}",
-                                 "note": ("instruction-bound, not HBM-bound: ncu 90 % issue, 3.7 % DRAM "
-                                          "(profiles/queues_film_display_640x360x16.md)") if key == "gt7" else
+                                 "note": "instruction-bound, not HBM-bound: ncu 90 % issue, 3.7 % DRAM"
+                                         if key == "gt7" else
                                          ("24 bytes per pixel moved; three full-accuracy powf per pixel (the sRGB "
-                                          "encode) set the time, not the bytes "
-                                          "(profiles/queues_film_display_640x360x16.md)")}}
+                                          "encode) set the time, not the bytes")}}
     return out
 
 
@@ -555,8 +582,8 @@ def run_gpu(args, rank, world, local_rank):
         "roofline": {"bound": "fp32", "kernel": "k_integrate + k_refine + k_tail (one chunk)",
                      "achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "TFLOP/s",
                      "frac": achieved / peak, "traffic": INTEGRATE_DRAM_BYTES_PER_RAY * rays,
-                     "traffic_note": "bytes per launch of k_integrate: ncu DRAM bytes per ray of a 640x360x16 "
-                                     "capture x rays of this frame",
+                     "traffic_note": "bytes per launch of k_integrate: ncu DRAM bytes per ray of a "
+                                     "640x360x16 capture x rays of this frame",
                      "peak_source": "measured in this run by mgk_fp32_peak (FMA probe kernel); "
                                     "MEASURED_PEAKS.json has no FP32 figure",
                      "flop_per_attempt": FL.attempt_flops(s.metric),

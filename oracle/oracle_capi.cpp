@@ -195,6 +195,87 @@ int orc_trace_geodesic(magik_trace_geodesic_container_t* c, magik_trace_geodesic
     return pow_in_double ? trace_geodesic_ref<Ctl::RefD>(c, ic, mp, ip) : trace_geodesic_ref<Ctl::Ref>(c, ic, mp, ip);
 }
 
+// The benchmark workload's scene: the Kerr a = 0.9 view at r = 50 M and
+// 75 degrees, 1920x1080x16, 32 bins, rtol = atol = 1e-7, MIXED.  A
+// restatement of the library's defaults for the CPU legs that must not load
+// the library; tests check that both fill the same bytes.
+double orc_isco_radius(double a) {
+    // Bardeen, Press and Teukolsky (1972), prograde orbits, M = 1.
+    const double z1 = 1.0 + std::cbrt(1.0 - a * a) * (std::cbrt(1.0 + a) + std::cbrt(1.0 - a));
+    const double z2 = std::sqrt(3.0 * a * a + z1 * z1);
+    return 3.0 + z2 - std::sqrt((3.0 - z1) * (3.0 + z1 + 2.0 * z2));
+}
+
+void orc_scene_defaults(mgk_scene* s) {
+    std::memset(s, 0, sizeof(*s));
+    s->metric = MGK_METRIC_KERR;
+    s->precision = MGK_PRECISION_MIXED;
+    s->time_reversed = 1;
+    s->n_max_substep = 56;
+    s->spin = 0.9;
+    s->mass_sign = 1.0;
+    s->horizon_scalar = 1.01;
+    s->abs_tol = 1e-7;
+    s->rel_tol = 1e-7;
+    s->h_max = 1000.0;
+    s->max_steps = 10000;
+    s->n_bins = 32;
+    s->escape_radius = 1000.0;
+    s->disk_r_in = orc_isco_radius(0.9);
+    s->disk_r_out = 20.0;
+    s->disk_T_in = 1.0e4;
+    s->cam_r = 50.0;
+    s->cam_incl_rad = 75.0 * M_PI / 180.0;
+    s->sensor_diag_mm = 24.0;
+    s->focal_length_mm = 12.0 / std::tan(30.0 * M_PI / 180.0);
+    s->width = 1920;
+    s->height = 1080;
+    s->spp = 16;
+    s->seed = 0x5EEDull;
+    s->lambda_min_nm = 380.0;
+    s->lambda_max_nm = 780.0;
+    s->star_radius_rad = 2.0e-3;
+    s->spectral_mode = MGK_SPECTRAL_BINS;
+    s->iso = 500.0;
+    s->fps = 24.0;
+    s->shutter_angle_deg = 180.0;
+    s->redistribution_sigma_nm = 10.0;
+    s->room_on = 0;
+    s->room_reflection_limit = 10;
+    const double lo[3] = {-40.0, -20.0, -40.0}, hi[3] = {40.0, 20.0, 40.0};
+    const double llo[3] = {-20.0, 19.0, -20.0}, lhi[3] = {20.0, 21.0, 20.0};
+    for (int a = 0; a < 3; ++a) {
+        s->room_min[a] = lo[a]; s->room_max[a] = hi[a];
+        s->light_min[a] = llo[a]; s->light_max[a] = lhi[a];
+    }
+    s->light_scale = 7.0e5;
+}
+
+// The seeded star catalogue (a restatement of the library's): directions
+// uniform on the sphere, magnitudes uniform in [0, 10] relative to a 1e4 K
+// blackbody at 550 nm, temperatures uniform in 3000-30000 K.
+void orc_star_catalog(uint64_t seed, uint32_t n, mgk_star* out) {
+    auto planck = [](double nm, double T) {
+        const double h = 6.62607015E-34, c = 299792458.0, kb = 1.380649E-23;
+        const double wl = nm * 1e-9;
+        return (2.0 * h * c * c / std::pow(wl, 5)) / std::expm1(h * c / (wl * kb * T));
+    };
+    const double ref = planck(550.0, 1.0e4);
+    for (uint32_t i = 0; i < n; ++i) {
+        const double u0 = rng_unit(seed, 0x57A2u, i, 0), u1 = rng_unit(seed, 0x57A2u, i, 1);
+        const double u2 = rng_unit(seed, 0x57A2u, i, 2), u3 = rng_unit(seed, 0x57A2u, i, 3);
+        const double y = 2.0 * u0 - 1.0, ph = 2.0 * M_PI * u1, r = std::sqrt(std::max(0.0, 1.0 - y * y));
+        const double T = 3000.0 + 27000.0 * u3;
+        mgk_star& st = out[i];
+        std::memset(&st, 0, sizeof(st));
+        st.dir[0] = float(r * std::cos(ph));
+        st.dir[1] = float(y);
+        st.dir[2] = float(r * std::sin(ph));
+        st.amplitude = float(std::pow(10.0, -0.4 * (10.0 * u2)) * ref / planck(550.0, T));
+        st.temperature = float(T);
+    }
+}
+
 int orc_scene_constants(const mgk_scene* s, double* out) {
     SceneConsts c = scene_consts(*s);
     int k = 0;

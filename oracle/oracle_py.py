@@ -7,14 +7,33 @@ sources by oracle/Makefile (only present where the reference was available
 at build time).
 """
 import ctypes as C
+import importlib.util
 import os
 import subprocess
+import sys
 
 import numpy as np
 
-from magik_b200 import abi
-
 HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def _load_abi():
+    """The plain ctypes layouts of include/mgk.h (magik_b200/abi.py), loaded
+    by path so that the oracle, and the CPU legs that use it, run without
+    importing the magik_b200 package or loading libmgk.so.  The module is
+    registered under its package name, so a later `import magik_b200` shares
+    it (one set of ctypes classes)."""
+    name = "magik_b200.abi"
+    if name in sys.modules:
+        return sys.modules[name]
+    spec = importlib.util.spec_from_file_location(name, os.path.join(HERE, "..", "magik_b200", "abi.py"))
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+abi = _load_abi()
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libmagikref.so")
 
@@ -36,6 +55,12 @@ def lib():
                                          abi.TraceMetricParams, abi.TraceIntegratorParams, C.c_int]
         L.orc_trace_geodesic.restype = C.c_int
         L.orc_scene_constants.argtypes = [C.POINTER(abi.Scene), C.POINTER(C.c_double)]
+        L.orc_scene_defaults.argtypes = [C.POINTER(abi.Scene)]
+        L.orc_scene_defaults.restype = None
+        L.orc_isco_radius.argtypes = [C.c_double]
+        L.orc_isco_radius.restype = C.c_double
+        L.orc_star_catalog.argtypes = [C.c_uint64, C.c_uint32, C.POINTER(abi.Star)]
+        L.orc_star_catalog.restype = None
         L.orc_trace_rays.argtypes = [C.POINTER(abi.Scene), C.c_uint64, C.c_uint32, C.POINTER(abi.RayResult),
                                      C.c_int]
         L.orc_shade_rays.argtypes = [C.POINTER(abi.Scene), C.POINTER(abi.Star), C.c_uint32, C.POINTER(C.c_float),
@@ -84,6 +109,32 @@ def ref():
         R.ref_reflect_mirror.restype = C.c_int
         _ref = R
     return _ref
+
+
+def scene_defaults(**overrides):
+    """The benchmark workload's scene (the oracle's restatement of
+    mgk_scene_defaults), with field overrides."""
+    s = abi.Scene()
+    lib().orc_scene_defaults(C.byref(s))
+    for k, v in overrides.items():
+        if not hasattr(s, k):
+            raise AttributeError(k)
+        setattr(s, k, v)
+    return s
+
+
+def isco_radius(spin):
+    return lib().orc_isco_radius(float(spin))
+
+
+def star_catalog(seed, n):
+    """The seeded star catalogue (the oracle's restatement of mgk_star_catalog)."""
+    out = np.zeros(n, dtype=STAR_DTYPE)
+    lib().orc_star_catalog(seed, n, out.ctypes.data_as(C.POINTER(abi.Star)))
+    return out
+
+
+STAR_DTYPE = np.dtype([("dir", "<f4", 3), ("amplitude", "<f4"), ("temperature", "<f4"), ("reserved", "<f4", 3)])
 
 
 def new_container(n_steps):

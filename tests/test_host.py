@@ -288,3 +288,40 @@ def _jitter_dim(s, pixel, sample, dim):
     v = h32(v ^ pixel)
     v = h32(v ^ ((dim * 0x85EBCA6B + 1) & 0xFFFFFFFF))
     return (v >> 8) / 16777216.0
+
+
+def test_oracle_scene_and_star_catalog_equal_the_library():
+    """The CPU legs build the workload from oracle/ alone: its restated scene
+    defaults, ISCO radius and star catalogue are the library's bytes."""
+    assert bytes(O.scene_defaults()) == bytes(M.scene_defaults())
+    assert O.isco_radius(0.998) == M.isco_radius(0.998)
+    a = O.star_catalog(0x57A25, 5000)
+    b = M.star_catalog(0x57A25, 5000)
+    assert np.array_equal(a.view(np.uint8), b.view(np.uint8))
+
+
+def test_reference_arm_loads_neither_the_package_nor_libmgk():
+    """bench.py --impl reference runs the reference's code (or the oracle)
+    only: a fresh process that imports no magik_b200 module and maps no
+    libmgk.so, and reports a per-step time that its steps add up to."""
+    import json
+    import subprocess
+    import sys
+    code = ("import runpy, sys, json\n"
+            "sys.argv = ['bench.py', '--impl', 'reference', '--steps', '2', '--warmup', '0', '--cpu-seconds', '0.2',\n"
+            "            '--width', '64', '--height', '36', '--spp', '1']\n"
+            "try:\n"
+            "    runpy.run_path('bench.py', run_name='__main__')\n"
+            "except SystemExit:\n"
+            "    pass\n"
+            "maps = open('/proc/self/maps').read()\n"
+            "print(json.dumps({'libmgk': 'libmgk.so' in maps,\n"
+            "                  'pkg': sorted(m for m in sys.modules if m.startswith('magik_b200'))}))\n")
+    r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    lines = [json.loads(x) for x in r.stdout.strip().splitlines()]
+    line, probe = lines[0], lines[1]
+    assert line["impl"] == "reference" and line["value"] > 0
+    assert line["package_imported"] is False and probe["libmgk"] is False
+    assert probe["pkg"] in ([], ["magik_b200.abi"])  # the ctypes layouts, loaded by path
+    assert line["ms_per_step"] > 0 and "REF32" in line["config"]["precision"]
