@@ -415,8 +415,12 @@ MGK_API mgk_result mgk_trace_rays(mgk_context* ctx, const mgk_scene* s, uint64_t
  * MGK_STATIC_MAX_RAYS rays per call (more returns MGK_ERROR_INVALID_ARGUMENT).
  * Runs on the current device; its first call there looks up the array's
  * device address (cudaGetSymbolAddress) and should come before any stream
- * capture.  All calls share the array: calls whose work overlaps on the GPU
- * race, so issue them on one stream.  d_out as for mgk_trace_rays. */
+ * capture; calls must not span a cudaDeviceReset.  All calls share the
+ * array: calls whose work overlaps on the GPU race, so issue them on one
+ * stream.  d_out as for mgk_trace_rays.  There are no continuation queues in
+ * the array: rays that go on after a room reflection or a disk miss finish
+ * in the tail kernel instead of further integrator passes, with the same
+ * records. */
 #define MGK_STATIC_MAX_RAYS 16384
 MGK_API mgk_result mgk_trace_rays_static(const mgk_scene* s, uint64_t first_ray, uint32_t n_rays,
                                          mgk_ray_result* d_out, void* stream);

@@ -322,6 +322,9 @@ STATIC_MAX_RAYS = 16384
 def trace_rays_static(scene, first, n, d_out, stream=None):
     """mgk_trace_rays_static: traces camera rays [first, first+n) into the CUDA
     buffer d_out (n * 128 bytes) with no device allocation; n <= 16384."""
+    if d_out.numel() * d_out.element_size() < n * abi.RESULT_BYTES:
+        raise ValueError(f"d_out holds {d_out.numel() * d_out.element_size()} bytes, {n} records need "
+                         f"{n * abi.RESULT_BYTES}")
     _check(lib().mgk_trace_rays_static(C.byref(scene), first, n, d_out.data_ptr(), _stream_ptr(stream)),
            "mgk_trace_rays_static")
 

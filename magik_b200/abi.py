@@ -25,6 +25,7 @@ PASS_HISTORY = 16
 SPECTRAL_BINS, SPECTRAL_SAMPLED = 0, 1
 CMF_ICDF_ENTRIES = 256
 WIDE_BAND = 0.05
+RESULT_BYTES = 128  # sizeof(mgk_ray_result)
 
 
 class Scene(C.Structure):

@@ -880,7 +880,7 @@ MGK_API mgk_result mgk_trace_rays(mgk_context* ctx, const mgk_scene* s, uint64_t
                                   mgk_ray_result* d_out, void* stream) {
     if (!ctx || !s || !d_out) return MGK_ERROR_INVALID_POINTER;
     uint64_t total = uint64_t(s->width) * s->height * s->spp;
-    if (first_ray + n_rays > total) return MGK_ERROR_INVALID_ARGUMENT;
+    if (first_ray > total || n_rays > total - first_ray) return MGK_ERROR_INVALID_ARGUMENT;
     return run(ctx, *s, nullptr, 0, nullptr, first_ray, n_rays, d_out, nullptr, nullptr, nullptr, nullptr,
                static_cast<cudaStream_t>(stream), false);
 }
@@ -890,7 +890,7 @@ MGK_API mgk_result mgk_shade_rays(mgk_context* ctx, const mgk_scene* s, const mg
                                   void* stream) {
     if (!ctx || !s || !d_xyz) return MGK_ERROR_INVALID_POINTER;
     uint64_t total = uint64_t(s->width) * s->height * s->spp;
-    if (first_ray + n_rays > total) return MGK_ERROR_INVALID_ARGUMENT;
+    if (first_ray > total || n_rays > total - first_ray) return MGK_ERROR_INVALID_ARGUMENT;
     return run(ctx, *s, d_stars, n_stars, d_xyz_w, first_ray, n_rays, nullptr, d_xyz, nullptr, nullptr, nullptr,
                static_cast<cudaStream_t>(stream), true);
 }

@@ -16,11 +16,20 @@
 // to a kernel.  The device address comes from cudaGetSymbolAddress, taken
 // once per device (with that device current) by the first call there and
 // cached; that first call on a device should therefore come before any
-// stream capture.  Every call shares the one array and finds the previous call's
-// contents in it, so the counters are cleared at the start of each call.
-// Calls whose work overlaps on the GPU (different streams, or different
-// host threads on the same device) race on the array; callers serialise
-// them, for example by issuing them on one stream.
+// stream capture.  The cached address belongs to the device's current CUDA
+// context: calls must not span a cudaDeviceReset (which ends that context and
+// frees the module holding the array).  Every call shares the one array and
+// finds the previous call's contents in it, so the counters are cleared at
+// the start of each call.  Calls whose work overlaps on the GPU (different
+// streams, or different host threads on the same device) race on the array;
+// callers serialise them, for example by issuing them on one stream.
+//
+// The array holds no continuation queues.  mgk_trace_rays runs rays that go
+// on after a room reflection or a disk miss through further passes of the
+// persistent integrator; here those rays finish in the tail kernel instead.
+// Both integrate the same steps in the same arithmetic, so the records are
+// the same bytes (the no-allocation tests compare them, room scenes
+// included); only the kernel that takes the later steps differs.
 #include <cstring>
 #include <mutex>
 
@@ -40,25 +49,27 @@ struct StaticLayout {
     size_t qx, qp, qc, hits, refine, resume, xyz, counters, total;
 };
 
-size_t up256(size_t v) { return (v + 255) / 256 * 256; }
+constexpr size_t up256(size_t v) { return (v + 255) / 256 * 256; }
 
-StaticLayout static_layout(const mgk_scene& s, uint32_t n) {
-    const bool f64 = s.precision == MGK_PRECISION_F64;
+constexpr StaticLayout static_layout(bool f64, uint32_t n) {
     const size_t T = f64 ? 8 : 4;
     StaticLayout L{};
     size_t o = 0;
-    auto take = [&](size_t bytes) { size_t at = o; o = up256(o + bytes); return at; };
-    L.qx = take(size_t(n) * 4 * T);
-    L.qp = take(size_t(n) * 4 * T);
-    L.qc = take(size_t(n) * T);
-    L.hits = take(size_t(n) * (f64 ? sizeof(HitEntry<double>) : sizeof(HitEntry<float>)));
-    L.refine = take(size_t(n) * (f64 ? sizeof(RefineEntry<double>) : sizeof(RefineEntry<float>)));
-    L.resume = take(size_t(n) * (f64 ? sizeof(ResumeEntry<double>) : sizeof(ResumeEntry<float>)));
-    L.xyz = take(size_t(n) * 12);
-    L.counters = take(sizeof(Counters));
+    L.qx = o; o = up256(o + size_t(n) * 4 * T);
+    L.qp = o; o = up256(o + size_t(n) * 4 * T);
+    L.qc = o; o = up256(o + size_t(n) * T);
+    L.hits = o; o = up256(o + size_t(n) * (f64 ? sizeof(HitEntry<double>) : sizeof(HitEntry<float>)));
+    L.refine = o; o = up256(o + size_t(n) * (f64 ? sizeof(RefineEntry<double>) : sizeof(RefineEntry<float>)));
+    L.resume = o; o = up256(o + size_t(n) * (f64 ? sizeof(ResumeEntry<double>) : sizeof(ResumeEntry<float>)));
+    L.xyz = o; o = up256(o + size_t(n) * 12);
+    L.counters = o; o = up256(o + sizeof(Counters));
     L.total = o;
     return L;
 }
+
+// The documented limit must fit the array in both state widths.
+static_assert(static_layout(true, kStaticMaxRays).total <= kStaticBytes, "F64 layout exceeds the static scratch");
+static_assert(static_layout(false, kStaticMaxRays).total <= kStaticBytes, "FP32 layout exceeds the static scratch");
 
 std::mutex g_mu;
 void* g_addr[64] = {};
@@ -96,9 +107,9 @@ extern "C" MGK_API mgk_result mgk_trace_rays_static(const mgk_scene* s, uint64_t
     if (rc != MGK_SUCCESS) return rc;
     if (n_rays > kStaticMaxRays) return MGK_ERROR_INVALID_ARGUMENT;
     const uint64_t total = uint64_t(s->width) * s->height * s->spp;
-    if (first_ray + n_rays > total) return MGK_ERROR_INVALID_ARGUMENT;
+    if (first_ray > total || n_rays > total - first_ray) return MGK_ERROR_INVALID_ARGUMENT;
     if (n_rays == 0) return MGK_SUCCESS;
-    const StaticLayout L = static_layout(*s, n_rays);
+    const StaticLayout L = static_layout(s->precision == MGK_PRECISION_F64, n_rays);
     if (L.total > kStaticBytes) return MGK_ERROR_INVALID_ARGUMENT;
 
     int device = 0, sms = 0;

@@ -325,3 +325,11 @@ def test_reference_arm_loads_neither_the_package_nor_libmgk():
     assert line["package_imported"] is False and probe["libmgk"] is False
     assert probe["pkg"] in ([], ["magik_b200.abi"])  # the ctypes layouts, loaded by path
     assert line["ms_per_step"] > 0 and "REF32" in line["config"]["precision"]
+
+
+def test_static_entry_refuses_a_short_output_buffer():
+    """trace_rays_static checks d_out's size before it calls the library."""
+    import torch
+    s = M.scene_defaults(width=16, height=16, spp=1)
+    with pytest.raises(ValueError):
+        M.trace_rays_static(s, 0, 256, torch.empty(256 * 128 - 1, dtype=torch.uint8))

@@ -18,7 +18,7 @@ import pytest
 
 import magik_b200 as M
 from magik_b200 import abi
-from tests.conftest import small_scene
+from tests.conftest import room_scene, small_scene
 
 pytestmark = pytest.mark.gpu
 
@@ -42,6 +42,29 @@ def test_static_entry_matches_context_entry_on_two_calls(ctx, precision):
     # a different range right after: counters left by the previous call are cleared
     ref2 = ctx.trace_rays(s, 1000, 3000)
     assert np.array_equal(_static(s, 1000, 3000).view(np.uint8), ref2.view(np.uint8))
+
+
+@pytest.mark.parametrize("precision", [abi.PRECISION_MIXED, abi.PRECISION_F64])
+def test_static_entry_matches_context_entry_in_the_room(ctx, precision):
+    """Room scenes: mgk_trace_rays continues reflected rays in further
+    integrator passes, the static entry point in the tail kernel; the records
+    must still be the same bytes, on two calls in a row."""
+    s = room_scene(width=48, height=27, spp=2, precision=precision)
+    n = s.width * s.height * s.spp
+    ref = ctx.trace_rays(s, 0, n)
+    assert (ref["bounces"] > 0).mean() > 0.5  # most rays reflect at least once
+    for _ in range(2):
+        assert np.array_equal(_static(s, 0, n).view(np.uint8), ref.view(np.uint8))
+
+
+def test_static_entry_at_its_maximum_in_f64(ctx):
+    """The largest call (MGK_STATIC_MAX_RAYS rays) in the widest layout (F64,
+    ~7 MiB of the 8 MiB array) gives the context entry point's records."""
+    s = small_scene(width=128, height=64, spp=2, precision=abi.PRECISION_F64)
+    n = M.STATIC_MAX_RAYS
+    assert n == s.width * s.height * s.spp
+    ref = ctx.trace_rays(s, 0, n)
+    assert np.array_equal(_static(s, 0, n).view(np.uint8), ref.view(np.uint8))
 
 
 def test_static_entry_rejects_more_than_its_maximum():
