@@ -297,7 +297,15 @@ template <class T> struct Term {
 // secant iterations on the crossing function, each evaluating a fresh RK
 // sub-step of length s from y0 (explicit Euler for Minkowski), at most
 // MGK_REFINE_ITERS + 1 sub-steps.  This removes the chord error of linear
-// interpolation over a long step.
+// interpolation over a long step.  The escape sphere takes one sub-step, to
+// where the step's chord meets the sphere (the root of a quadratic): in the
+// far field the path departs from its chord by about one M over a step, so
+// the sub-step ends within ~1e-3 M of the sphere, and the escape direction is
+// taken at the escape radius itself (the remaining bending there changes by
+// ~2 M b / r^3 = 4e-8 rad per M).  Interpolating |x|^2 linearly instead put
+// the sub-step anywhere between ~0.85 R and R, which moved the measured
+// direction by the far-field bending in between (~5e-6 rad) from one step
+// sequence to another.
 template <int METRIC, Fuse F, class T>
 __device__ __forceinline__ S7<T> sub_step(const S7<T>& y0, T pt, T s, const MP<T>& m) {
     S7<T> y1;
@@ -320,6 +328,21 @@ template <Fuse F, class T> __device__ __forceinline__ T cross_g(int kind, const 
     return kind == 3 ? mad<F>(q.z, q.z, mad<F>(q.y, q.y, q.x * q.x)) - v : axis_of(q, kind) - v;
 }
 
+// Chord parameter t in (0, 1] where the chord y0 -> y1 meets the sphere
+// |x|^2 = |x0|^2 - g0 (g0 < 0: y0 inside): the positive root of
+// qa t^2 + 2 qb t + g0 = 0, in the cancellation-free form for either sign of
+// qb; `fallback` when the root is not in (0, 1].
+template <Fuse F, class T>
+__device__ __forceinline__ T chord_sphere(const S7<T>& y0, const S7<T>& y1, T g0, T fallback) {
+    const T dx = y1.x - y0.x, dy = y1.y - y0.y, dz = y1.z - y0.z;
+    const T qa = mad<F>(dz, dz, mad<F>(dy, dy, dx * dx));
+    const T qb = mad<F>(y0.z, dz, mad<F>(y0.y, dy, y0.x * dx));
+    const T disc = mad<F>(qb, qb, -(qa * g0));
+    const T sq = sqrt(disc > T(0) ? disc : T(0));
+    const T t = qb >= T(0) ? g0 / (-qb - sq) : (sq - qb) / qa;
+    return (t > T(0) && t <= T(1)) ? t : fallback;
+}
+
 // Disk: kind 1, v = 0; escape sphere: kind 3, v = R^2; room faces: planes.
 template <int METRIC, Fuse F, class T>
 __device__ __forceinline__ S7<T> refine(int kind, const S7<T>& y0, const S7<T>& y1, T pt, T h, T v, const MP<T>& m,
@@ -327,12 +350,13 @@ __device__ __forceinline__ S7<T> refine(int kind, const S7<T>& y0, const S7<T>& 
     T g0 = cross_g<F>(kind, y0, v), g1 = cross_g<F>(kind, y1, v);
     T s_prev = h, g_prev = g1;
     T s = h * (g0 / (g0 - g1));
+    if (kind == 3) s = h * chord_sphere<F>(y0, y1, g0, g0 / (g0 - g1));
     S7<T> ys = sub_step<METRIC, F, T>(y0, pt, s, m);
     ++evals;
     T gs = cross_g<F>(kind, ys, v);
-    // The escape sphere lies in the far field, where one sub-step to the chord
-    // estimate already puts the direction within 1e-9 of the located one;
-    // planes (the disk in strong field, the room's faces) iterate.
+    // The escape sphere lies in the far field, where one sub-step to the
+    // chord's intersection ends within ~1e-3 M of it; planes (the disk in
+    // strong field, the room's faces) iterate.
     const int iters = kind < 3 ? MGK_REFINE_ITERS : 0;
     for (int it = 0; it < iters; ++it) {
         T den = gs - g_prev;

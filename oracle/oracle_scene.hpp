@@ -231,12 +231,23 @@ inline GState<T> refine(int kind, const GState<T>& y0, const GState<T>& y1, T h,
     T g0 = g(y0), g1 = g(y1);
     T s_prev = h, g_prev = g1;
     T s = h * (g0 / (g0 - g1));
+    if (kind == 3) {
+        // the escape sphere: one sub-step to where the chord meets it (the
+        // positive root of qa t^2 + 2 qb t + g0 = 0), as the kernels do
+        const T dx = y1.x.x - y0.x.x, dy = y1.x.y - y0.x.y, dz = y1.x.z - y0.x.z;
+        const T qa = mad<F>(dz, dz, mad<F>(dy, dy, dx * dx));
+        const T qb = mad<F>(y0.x.z, dz, mad<F>(y0.x.y, dy, y0.x.x * dx));
+        const T disc = mad<F>(qb, qb, -(qa * g0));
+        const T sq = sq_root(disc > T(0) ? disc : T(0));
+        const T t = qb >= T(0) ? g0 / (-qb - sq) : (sq - qb) / qa;
+        s = h * ((t > T(0) && t <= T(1)) ? t : g0 / (g0 - g1));
+    }
     GState<T> ys = sub_step<F>(y0, s, m);
     ++*evals;
     T gs = g(ys);
-    // The escape sphere lies in the far field, where one sub-step to the chord
-    // estimate already puts the direction within 1e-9 of the located one;
-    // planes (the disk in strong field, the room's faces) iterate.
+    // The escape sphere lies in the far field, where one sub-step to the
+    // chord's intersection ends within ~1e-3 M of it; planes (the disk in
+    // strong field, the room's faces) iterate.
     const int iters = kind < 3 ? MGK_REFINE_ITERS : 0;
     for (int it = 0; it < iters; ++it) {
         T den = gs - g_prev;

@@ -17,6 +17,9 @@ class and accepted-step count of the same frame.
       from the ISCO, 32 bins, 1e5 seeded stars, rtol = atol = 1e-7, in FP64
       (the oracle the MIXED mode is checked against); 96 x 54 pixels x 2
       samples instead of 1920 x 1080 x 16.
+  c2conv  the same frame in FP64 at rtol = atol = 1e-11: the converged
+      image (its steps are 1e-10 apart from rtol 1e-12), against which the
+      error of the rtol = 1e-7 renders, FP64 and MIXED alike, is measured.
 
 tests/test_oracle_films.py checks that the oracle still renders these films
 (CPU) and that the library's F64 and MIXED renders agree with them (GPU).
@@ -47,7 +50,10 @@ def workloads():
                           escape_radius=1000.0, rel_tol=1e-8, abs_tol=1e-10, max_steps=10_000,
                           width=64, height=64, spp=1)
     c2 = M.scene_defaults(precision=abi.PRECISION_F64, width=96, height=54, spp=2)
-    return {"c1": (c1, np.zeros(0, M.STAR_DTYPE)), "c2": (c2, M.star_catalog(STAR_SEED, N_STARS))}
+    c2conv = M.scene_defaults(precision=abi.PRECISION_F64, width=96, height=54, spp=2, rel_tol=1e-11,
+                              abs_tol=1e-11)
+    stars = M.star_catalog(STAR_SEED, N_STARS)
+    return {"c1": (c1, np.zeros(0, M.STAR_DTYPE)), "c2": (c2, stars), "c2conv": (c2conv, stars)}
 
 
 def render(scene, stars):

@@ -49,8 +49,8 @@ def compare_records(gpu, orc, allow_frac=1e-3):
         same &= eq
     n_bad = int((~same).sum())
     assert n_bad <= max(1, int(allow_frac * len(gpu))), f"{n_bad} of {len(gpu)} rays differ"
-    # rays that differ (pow rounding) still agree in class
-    assert np.mean(gpu["cls"] == orc["cls"]) >= 1 - allow_frac
+    # rays that differ (pow rounding) still agree in class: the 99.99 % bar
+    assert np.mean(gpu["cls"] == orc["cls"]) >= 0.9999
     return n_bad
 
 

@@ -13,8 +13,19 @@ r = 50 M, 75 degrees, rtol = atol = 1e-7), and
   of the disk, or its conserved quantities within 2e-3 of the Kerr critical
   curve (the photon ring, where the geodesic flow amplifies a perturbation
   by about e^pi per half orbit);
-* disk radii, redshifts and escape directions agree to 1e-5 at the 99th
-  percentile.
+* escape directions and escape points (on the escape sphere) agree to 1e-6
+  at the 99th percentile and 2e-6 at the 99.9th (5.5e-7 and 9e-7 measured
+  on the oracle); the rays beyond that are strongly deflected ones (50 or
+  more steps, wrapping behind the hole), where the flow amplifies the FP32
+  rounding;
+* disk radii and redshifts agree to 1e-5 at the 99th percentile;
+* against the converged solution (F64 at rtol = atol = 1e-11): MIXED's
+  escape directions lie within 1e-6 at the 99th percentile, and its disk
+  radii and redshifts within 3x of F64's own error at rtol = 1e-7 at every
+  quantile up to the 99.9th (F64 at that tolerance is itself 1e-6 from the
+  converged disk radii at the 99th percentile; the two modes take different
+  step sequences, since at rtol = 1e-7 the FP32 stages' rounding moves the
+  error estimate by several percent).
 """
 import math
 
@@ -132,6 +143,43 @@ def test_mixed_against_f64_on_the_gpu(ctx):
     assert disk.sum() > 10000 and esc.sum() > 10000
     assert np.quantile(np.abs(a["r_hit"][disk] / b["r_hit"][disk] - 1), 0.99) < 1e-5
     assert np.quantile(np.abs(a["z"][disk] / b["z"][disk] - 1), 0.99) < 1e-5
-    assert np.quantile(np.abs(a["dir"][esc] - b["dir"][esc]).max(1), 0.99) < 1e-5
+    de = np.abs(a["dir"][esc] - b["dir"][esc]).max(1)
+    xe = np.linalg.norm(a["x"][esc][:, :3] - b["x"][esc][:, :3], axis=1) / np.linalg.norm(b["x"][esc][:, :3], axis=1)
+    print(f"escape direction MIXED vs F64: p99 {np.quantile(de, 0.99):.2e} p99.9 {np.quantile(de, 0.999):.2e} "
+          f"p99.99 {np.quantile(de, 0.9999):.2e}; escape point p99 {np.quantile(xe, 0.99):.2e}")
+    assert np.quantile(de, 0.99) <= 1e-6 and np.quantile(de, 0.999) <= 2e-6
+    assert np.quantile(xe, 0.99) <= 1e-6 and np.quantile(xe, 0.999) <= 2e-6
+    # the escape point lies on the escape sphere
+    assert np.abs(np.linalg.norm(a["x"][esc][:, :3], axis=1) / s32.escape_radius - 1).max() < 1e-5
     # the FP64 band ran: MIXED took FP64 attempts near the horizon
     assert a["wide_attempts"].sum() > 0
+
+
+def test_mixed_is_as_accurate_as_f64_at_the_same_tolerance(ctx):
+    conv = M.scene_defaults(width=WIDTH, height=HEIGHT, spp=SPP, precision=abi.PRECISION_F64,
+                            rel_tol=1e-11, abs_tol=1e-11)
+    s32 = M.scene_defaults(width=WIDTH, height=HEIGHT, spp=SPP, precision=abi.PRECISION_MIXED)
+    s64 = M.scene_defaults(width=WIDTH, height=HEIGHT, spp=SPP, precision=abi.PRECISION_F64)
+    n = WIDTH * HEIGHT * SPP
+    c = ctx.trace_rays(conv, 0, n)
+    a = ctx.trace_rays(s32, 0, n)
+    b = ctx.trace_rays(s64, 0, n)
+    assert (c["cls"] != abi.RAY_STEP_LIMIT).all()
+    same = (a["cls"] == c["cls"]) & (b["cls"] == c["cls"])
+    assert same.mean() >= 0.9999
+    disk = same & (c["cls"] == abi.RAY_DISK)
+    esc = same & (c["cls"] == abi.RAY_ESCAPED)
+    q = np.array([0.5, 0.9, 0.99, 0.999])
+
+    def err(r, field, sel):
+        if field == "dir":
+            return np.abs(r["dir"][sel] - c["dir"][sel]).max(1)
+        return np.abs(r[field][sel] / c[field][sel] - 1)
+
+    de_m, de_f = np.quantile(err(a, "dir", esc), q), np.quantile(err(b, "dir", esc), q)
+    print(f"dir vs converged: MIXED {np.array2string(de_m, precision=2)} F64@1e-7 {np.array2string(de_f, precision=2)}")
+    assert de_m[2] <= 1e-6
+    for field in ("r_hit", "z"):
+        em, ef = np.quantile(err(a, field, disk), q), np.quantile(err(b, field, disk), q)
+        print(f"{field} vs converged: MIXED {np.array2string(em, precision=2)} F64@1e-7 {np.array2string(ef, precision=2)}")
+        assert np.all(em <= 3.0 * ef + 1e-8), (field, em.tolist(), ef.tolist())

@@ -179,8 +179,9 @@ def test_null_condition_and_conserved_quantities(precision):
 
 
 def test_mixed_agrees_with_f64_physics():
-    """MIXED (FP32 state, FP64 error estimate) against F64 on the same rays:
-    termination class, located disk hits and escape directions."""
+    """MIXED (FP32 state and step control, FP64 attempts next to the horizon)
+    against F64 on the same rays: termination class, located disk hits and
+    escape directions."""
     kw = dict(width=64, height=36, spp=2)
     a = _trace(M.scene_defaults(precision=abi.PRECISION_MIXED, **kw))
     b = _trace(M.scene_defaults(precision=abi.PRECISION_F64, **kw))
@@ -190,7 +191,8 @@ def test_mixed_agrees_with_f64_physics():
     assert np.quantile(np.abs(a["r_hit"][disk] / b["r_hit"][disk] - 1), 0.99) < 1e-5
     assert np.quantile(np.abs(a["z"][disk] / b["z"][disk] - 1), 0.99) < 1e-5
     esc = same & (a["cls"] == abi.RAY_ESCAPED)
-    assert np.quantile(np.abs(a["dir"][esc] - b["dir"][esc]).max(1), 0.99) < 1e-5
+    # escape directions are taken on the escape sphere in both modes
+    assert np.quantile(np.abs(a["dir"][esc] - b["dir"][esc]).max(1), 0.99) < 1e-6
 
 
 def test_weak_field_deflection():
