@@ -8,6 +8,7 @@ import ctypes as C
 SUCCESS = 0
 ERROR_INVALID_POINTER = 2
 ERROR_HOST_TRACE_ALLOCATED_STEPS_AND_CAPACITY_MISMATCH = 102
+ERROR_UNKNOWN_METRIC = 707
 ERROR_UNKNOWN = 10000
 ERROR_INVALID_ARGUMENT = 10001
 ERROR_CUDA = 10002

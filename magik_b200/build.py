@@ -18,7 +18,12 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmgk.so")
 SOURCES = ["kernels.cu", "api.cu", "static_scratch.cu", "mlp.cu", "mlp_tc.cu", "surrogate.cu", "display.cu",
            "manager.cu"]
-HEADERS = ["dev_physics.cuh", "dev_pair.cuh", "dev_scene.cuh", "internal.h", "cie1931_2deg.inc", os.path.join("..", "..", "include", "mgk.h"),
+HEADERS = ["dev_physics.cuh", "dev_pair.cuh", "dev_scene.cuh", "internal.h", "cie1931_2deg.inc",
+           os.path.join("..", "src", "renderer", "relativity", "metric.cuh"),
+           os.path.join("..", "src", "renderer", "relativity", "metric_kerr.cuh"),
+           os.path.join("..", "src", "renderer", "relativity", "metric_schwarzschild.cuh"),
+           os.path.join("..", "src", "renderer", "relativity", "metric_minkowski.cuh"),
+           os.path.join("..", "src", "renderer", "bxdf", "matter.cuh"), os.path.join("..", "..", "include", "mgk.h"),
            os.path.join("..", "..", "include", "mgk_manager.h")]
 
 NVCC_FLAGS = [
@@ -46,14 +51,16 @@ def _stale():
 
 
 def build(force=False, verbose=False, out=None, defines=()):
-    """Compiles libmgk.so (or `out`, with extra -D `defines`)."""
+    """Compiles libmgk.so (or `out`, with extra -D `defines`); the sources
+    compile in parallel."""
+    from concurrent.futures import ThreadPoolExecutor
     lib = out or LIB
     if not force and out is None and not _stale():
         return LIB
-    objs = []
     bdir = os.path.join(os.path.dirname(lib) if out else HERE, "_build")
     os.makedirs(bdir, exist_ok=True)
-    for src in SOURCES:
+
+    def compile_one(src):
         obj = os.path.join(bdir, src.replace(".cu", ".o"))
         cmd = [nvcc(), *NVCC_FLAGS, *[f"-D{d}" for d in defines], "-c", os.path.join(CSRC, src), "-o", obj]
         r = subprocess.run(cmd, capture_output=True, text=True)
@@ -63,7 +70,10 @@ def build(force=False, verbose=False, out=None, defines=()):
             sys.stderr.write(r.stderr)
         with open(obj + ".ptxas.txt", "w") as f:
             f.write(r.stderr)
-        objs.append(obj)
+        return obj
+
+    with ThreadPoolExecutor(max_workers=min(len(SOURCES), os.cpu_count() or 1)) as pool:
+        objs = list(pool.map(compile_one, SOURCES))
     tmp = lib + ".tmp"
     cmd = [nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-cudart", "static",
            *objs, "-o", tmp]
@@ -72,6 +82,25 @@ def build(force=False, verbose=False, out=None, defines=()):
         raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
     os.replace(tmp, lib)
     return lib
+
+
+# A variant of the library with a user metric plugin compiled in (the
+# contract of src/renderer/relativity/metric.cuh): the test plugin of
+# tests/plugin/metric_schwarzschild_user.cuh under tag 16.
+USER_METRIC_HEADER = os.path.join(HERE, "..", "tests", "plugin", "metric_schwarzschild_user.cuh")
+USER_METRIC_LIB = os.path.join(HERE, "..", "tests", "plugin", "libmgk_user_metric.so")
+
+
+def user_metric_build(force=False):
+    """Builds USER_METRIC_LIB (when missing or older than its sources)."""
+    lib = os.path.abspath(USER_METRIC_LIB)
+    header = os.path.abspath(USER_METRIC_HEADER)
+    if not force and os.path.exists(lib):
+        t = os.path.getmtime(lib)
+        deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS] + [header, os.path.abspath(__file__)]
+        if all(os.path.getmtime(d) <= t for d in deps):
+            return lib
+    return build(out=lib, defines=(f'MGK_USER_METRIC_HEADER="{header}"',))
 
 
 if __name__ == "__main__":

@@ -66,7 +66,7 @@ mgk_result ensure_arena(mgk_context* ctx, size_t bytes) {
 
 mgk_result validate(const mgk_scene* s) {
     if (!s) return MGK_ERROR_INVALID_POINTER;
-    if (s->metric < 0 || s->metric > 2) return MGK_ERROR_UNKNOWN_METRIC;
+    if (!metric_supported(s->metric)) return MGK_ERROR_UNKNOWN_METRIC;
     if (s->precision < 0 || s->precision > 2) return MGK_UNKNOWN_ENUM_TYPE;
     if (s->n_max_substep < 1 || !(s->abs_tol > 0.0) || !(s->rel_tol >= 0.0) || !(s->h_max > 0.0))
         return MGK_ERROR_INVALID_ARGUMENT;
@@ -92,13 +92,16 @@ mgk_result validate(const mgk_scene* s) {
                 if (!(std::fabs(d - (i == j ? 1.0 : 0.0)) <= 1e-6)) return MGK_ERROR_INVALID_ARGUMENT;
             }
         }
-        if (s->metric != MGK_METRIC_MINKOWSKI) {
-            const double a = s->metric == MGK_METRIC_KERR ? s->spin : 0.0;
+        bool outside = true;
+        with_metric(s->metric, [&](auto mt) {
+            using MT = decltype(mt);
+            if (!MT::has_horizon) return;
+            const double a = MT::spin(*s);
             const double R = cam[0] * cam[0] + cam[1] * cam[1] + cam[2] * cam[2] - a * a;
             const double r = std::sqrt(0.5 * R + 0.5 * std::sqrt(R * R + 4.0 * a * a * cam[1] * cam[1]));
-            const double rh = (1.0 + std::sqrt(std::fmax(0.0, 1.0 - a * a))) * s->horizon_scalar;
-            if (!(r > rh)) return MGK_ERROR_INVALID_ARGUMENT;
-        }
+            outside = r > MT::outer_horizon(*s) * s->horizon_scalar;
+        });
+        if (!outside) return MGK_ERROR_INVALID_ARGUMENT;
     }
     if (!(s->star_radius_rad > 0.0 && s->star_radius_rad <= 0.02)) return MGK_ERROR_INVALID_ARGUMENT;
     if (s->spectral_mode > MGK_SPECTRAL_SAMPLED) return MGK_UNKNOWN_ENUM_TYPE;

@@ -15,9 +15,21 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#ifndef MGK_HD
+#define MGK_HD __host__ __device__ __forceinline__
+#endif
+
 namespace mgk {
 
 enum class Fuse { None, Fma };
+
+// Four-vectors (x, y, z, t) and symmetric 4x4 metrics.
+template <class T> struct V4 { T x, y, z, t; };
+template <class T> struct Sym4 { T tt, tx, ty, tz, xx, xy, xz, yy, yz, zz; };
+
+// The metric plugins (src/renderer/relativity/metric.cuh): metric<TAG> for
+// each supported MGK_METRIC_* tag.
+template <int TAG> struct metric;
 
 // 1: FP32 operations of the MIXED attempt that come in pairs run as f32x2
 // instructions (one issue slot per pair, each half rounded as the scalar).
@@ -375,40 +387,21 @@ template <class T> __device__ __forceinline__ void rhs_minkowski(const S7<T>& s,
     o.px = T(0); o.py = T(0); o.pz = T(0);
 }
 
+// The right-hand side and the capture test of the metric with tag METRIC,
+// through its plugin (metric<METRIC>::geodesic_rhs / in_domain).
 template <int METRIC, Fuse F, class T>
 __device__ __forceinline__ void rhs(const S7<T>& s, T pt, const MP<T>& m, S7<T>& o) {
-    if constexpr (METRIC == 2) {
-        if constexpr (F == Fuse::Fma) rhs_kerr_fused<T>(s, pt, m, o);
-        else rhs_kerr<F, T>(s, pt, m.spin, o);
-    } else if constexpr (METRIC == 1) {
-        if constexpr (F == Fuse::Fma) rhs_schwarzschild_fused<T>(s, pt, m.mass_sign, o);
-        else rhs_schwarzschild<F, T>(s, pt, m.mass_sign, o);
-    }
-    else rhs_minkowski<T>(s, pt, o);
+    metric<METRIC>::template geodesic_rhs<F, T>(s, pt, m, o);
+}
+template <int METRIC, class T> __device__ __forceinline__ bool in_domain(T x, T y, T z, const MP<T>& m) {
+    return metric<METRIC>::template in_domain<T>(x, y, z, m);
 }
 
-// kerr_schild_r, metric_kerr.cuh:8-13.
-template <class T> __device__ __forceinline__ T kerr_schild_r(T x, T y, T z, T a) {
+// kerr_schild_r, metric_kerr.cuh:8-13 (host or device).
+template <class T> MGK_HD T kerr_schild_r(T x, T y, T z, T a) {
     T R = (x * x + y * y + z * z - a * a);
     T r_squared = T(0.5) * R + T(0.5) * sqrt(R * R + T(4) * a * a * y * y);
     return sqrt(r_squared);
-}
-
-// Horizon test (true = captured): metric_kerr.cuh:169-175 (NaN r captures),
-// metric_schwarzschild.cuh:136-141, Minkowski never.
-template <int METRIC, class T> __device__ __forceinline__ bool in_domain(T x, T y, T z, const MP<T>& m) {
-    if constexpr (METRIC == 2) {
-        if (m.spin_abs_gt1 != T(0)) return false;
-        T r = kerr_schild_r(x, y, z, m.spin);
-        if (m.horizon < r) return false;
-        return true;
-    } else if constexpr (METRIC == 1) {
-        T r = sqrt(x * x + y * y + z * z);
-        if (m.mass_sign < T(0)) return r < T(1e-3);
-        return r <= m.horizon;
-    } else {
-        return false;
-    }
 }
 
 // ------------------------------------------------------------- RKF45

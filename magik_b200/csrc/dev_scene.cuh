@@ -14,13 +14,9 @@
 
 #include "dev_physics.cuh"
 #include "../../include/mgk.h"
-
-#define MGK_HD __host__ __device__ __forceinline__
+#include "../src/renderer/relativity/metric.cuh"
 
 namespace mgk {
-
-template <class T> struct V4 { T x, y, z, t; };
-template <class T> struct Sym4 { T tt, tx, ty, tz, xx, xy, xz, yy, yz, zz; };
 
 // ------------------------------------------------------------------ RNG
 // triplet_hash (internal_math.h:2027-2037) chained over (seed, stream, index, dim).
@@ -42,50 +38,6 @@ MGK_HD float rng_unit(uint64_t seed, uint32_t stream, uint32_t index, uint32_t d
 }
 
 // ------------------------------------------------------------- frames
-template <class T> MGK_HD T ks_r(T x, T y, T z, T a) {
-    T R = (x * x + y * y + z * z - a * a);
-    T r_squared = T(0.5) * R + T(0.5) * sqrt(R * R + T(4) * a * a * y * y);
-    return sqrt(r_squared);
-}
-
-// compute_g: metric_kerr.cuh:177-190, metric_schwarzschild.cuh:143-153.
-template <class T> MGK_HD Sym4<T> compute_g(int metric, T x, T y, T z, T a, T mass_sign) {
-    if (metric == MGK_METRIC_MINKOWSKI) return Sym4<T>{T(-1), 0, 0, 0, T(1), 0, 0, T(1), 0, T(1)};
-    T f, kx, ky, kz;
-    if (metric == MGK_METRIC_KERR) {
-        const T r = ks_r(x, y, z, a);
-        f = T(2) * r * r * r / (r * r * r * r + a * a * y * y);
-        kx = (r * x - a * z) / (r * r + a * a);
-        ky = y / r;
-        kz = (r * z + a * x) / (r * r + a * a);
-    } else {
-        const T r = sqrt(x * x + y * y + z * z);
-        f = T(2) * mass_sign / r;
-        kx = x / r; ky = y / r; kz = z / r;
-    }
-    return Sym4<T>{T(-1) + f, f * kx, f * ky, f * kz, T(1) + f * kx * kx, f * kx * ky, f * kx * kz,
-                   T(1) + f * ky * ky, f * ky * kz, T(1) + f * kz * kz};
-}
-
-// reference_observer: metric_kerr.cuh:207-226, metric_schwarzschild.cuh:167-171.
-template <class T> MGK_HD V4<T> reference_observer(int metric, T x, T y, T z, T a, T mass_sign) {
-    if (metric == MGK_METRIC_MINKOWSKI) return V4<T>{0, 0, 0, T(1)};
-    if (metric == MGK_METRIC_SCHWARZSCHILD) {
-        Sym4<T> g = compute_g<T>(metric, x, y, z, a, mass_sign);
-        return V4<T>{0, 0, 0, T(1) / sqrt(-g.tt)};
-    }
-    T r = ks_r(x, y, z, a);
-    T r_sq = r * r;
-    T a_sq = a * a;
-    T cos_theta = y / r;
-    T sin2_theta = T(1) - cos_theta * cos_theta;
-    T sigma = r_sq + a_sq * cos_theta * cos_theta;
-    T delta = r_sq - T(2) * r + a_sq;
-    T Lambda = (r_sq + a_sq) * (r_sq + a_sq) - a_sq * delta * sin2_theta;
-    T u_t = sqrt(Lambda / (delta * sigma));
-    T u_phi = T(2) * a * r / sqrt(Lambda * delta * sigma);
-    return V4<T>{z * u_phi, T(0), -x * u_phi, u_t};
-}
 
 // inner_product / contract, relativity_utilities.cuh:122-139.
 template <class T> MGK_HD T inner_product(const Sym4<T>& g, const V4<T>& u, const V4<T>& v) {
@@ -139,9 +91,7 @@ struct SceneConsts {
 
 inline SceneConsts scene_consts(const mgk_scene& s) {
     SceneConsts c{};
-    const int metric = s.metric;
     const double a = s.time_reversed ? -s.spin : s.spin;
-    const double ms = s.mass_sign < 0 ? -1.0 : 1.0;
     double ci = std::cos(s.cam_incl_rad), si = std::sin(s.cam_incl_rad);
     V4<double> q{0.0, s.cam_r * ci, s.cam_r * si, 0.0};
     V4<double> X{1, 0, 0, 0}, Y{0, si, -ci, 0}, Z{0, ci, si, 0};  // right, up, back
@@ -152,8 +102,17 @@ inline SceneConsts scene_consts(const mgk_scene& s) {
         Z = V4<double>{s.cam_axes[6], s.cam_axes[7], s.cam_axes[8], 0.0};
     }
     c.cam_pos[0] = q.x; c.cam_pos[1] = q.y; c.cam_pos[2] = q.z; c.cam_pos[3] = q.t;
-    V4<double> u = reference_observer<double>(metric, q.x, q.y, q.z, a, ms);
-    Sym4<double> g = compute_g<double>(metric, q.x, q.y, q.z, a, ms);
+    V4<double> u{};
+    Sym4<double> g{};
+    double r_plus = 0.0;
+    with_metric(s.metric, [&](auto mt) {
+        using MT = decltype(mt);
+        MP<double> m{};
+        MT::template make_params<double>(s, m);
+        u = MT::template reference_observer<double>(q.x, q.y, q.z, m);
+        g = MT::template compute_g<double>(q.x, q.y, q.z, m);
+        r_plus = MT::outer_horizon(s);
+    });
     const double* v = s.cam_velocity;
     if (s.cam_explicit && (v[0] != 0.0 || v[1] != 0.0 || v[2] != 0.0)) {
         // rest_frame_four_velocity (relativity_utilities.cuh:163-173): the proper
@@ -176,9 +135,7 @@ inline SceneConsts scene_consts(const mgk_scene& s) {
     c.pix_b = -tan_half;
     c.pix_c = -2.0 * tan_half / W;
     c.pix_d = tan_half * H / W;
-    double ap = metric == MGK_METRIC_KERR ? s.spin : 0.0;
-    double d1 = 1.0 - ap * ap;
-    c.r_plus = metric == MGK_METRIC_MINKOWSKI ? 0.0 : 1.0 + std::sqrt(d1 > 0.0 ? d1 : 0.0);
+    c.r_plus = r_plus;
     c.spin_t = a;
     c.omega_sign = s.time_reversed ? -1.0 : 1.0;
     return c;
@@ -260,11 +217,11 @@ template <class T> __device__ __forceinline__ T redshift_clamp(T z) {
 }
 
 // Circular Keplerian orbit at (x, 0, z), normalised in the integrated frame.
-template <class T>
-__device__ __forceinline__ V4<T> disk_velocity(T xh, T zh, T r, const DevScene<T>& P, int metric) {
+template <int METRIC, class T>
+__device__ __forceinline__ V4<T> disk_velocity(T xh, T zh, T r, const DevScene<T>& P) {
     T omega = P.omega_sign / (r * sqrt(r) + P.spin_phys);
     T vx = zh * omega, vz = -xh * omega;
-    Sym4<T> g = compute_g<T>(metric, xh, T(0), zh, P.m.spin, P.m.mass_sign);
+    Sym4<T> g = metric<METRIC>::template compute_g<T>(xh, T(0), zh, P.m);
     T n = g.tt + T(2) * (g.tx * vx + g.tz * vz) + g.xx * vx * vx + T(2) * g.xz * vx * vz + g.zz * vz * vz;
     T ut = T(1) / sqrt(-n);
     return V4<T>{vx * ut, T(0), vz * ut, ut};
@@ -285,6 +242,17 @@ template <class T> __device__ __forceinline__ T planck(T wavelength_nm, T temper
 template <class T> __device__ __forceinline__ T clamp_radiance(T v) {
     return (isnan(v) || isinf(v) || v < T(0)) ? T(0) : v;  // bxdf_utilities.cuh:158-159
 }
+
+// The matter plugins (src/renderer/bxdf/matter.cuh) use these two, defined
+// further down with the room and the star grid.
+template <class T> __device__ __forceinline__ T white_led(T x);
+MGK_HD uint32_t cube_cell(float dx, float dy, float dz, uint32_t n);
+
+}  // namespace mgk
+
+#include "../src/renderer/bxdf/matter.cuh"
+
+namespace mgk {
 
 // Termination record of a ray.
 template <class T> struct Term {
@@ -309,9 +277,9 @@ template <class T> struct Term {
 template <int METRIC, Fuse F, class T>
 __device__ __forceinline__ S7<T> sub_step(const S7<T>& y0, T pt, T s, const MP<T>& m) {
     S7<T> y1;
-    if constexpr (METRIC == MGK_METRIC_MINKOWSKI) {
+    if constexpr (metric<METRIC>::explicit_euler) {
         S7<T> f;
-        rhs_minkowski<T>(y0, pt, f);
+        rhs<METRIC, F, T>(y0, pt, m, f);
         y1 = axpy<F>(s, f, y0);
     } else {
         S7<T> k[6];
@@ -507,12 +475,11 @@ template <class T> MGK_HD void sphere_dir(uint64_t seed, uint32_t sample, uint32
 // normal), and mapped back to a null covariant momentum.  c0 becomes
 // (u . p_out) times the redshift at the wall, so that redshifts multiply
 // along the path.
-template <class T>
+template <int METRIC, class T>
 __device__ __forceinline__ void reflect_wall(const DevScene<T>& P, int axis, int side, const S7<T>& X, T& pt, T& c0,
                                              uint32_t bounce, uint64_t ray_id, S7<T>& out) {
-    const int metric = P.metric;
-    const Sym4<T> g = compute_g<T>(metric, X.x, X.y, X.z, P.m.spin, P.m.mass_sign);
-    const V4<T> u = reference_observer<T>(metric, X.x, X.y, X.z, P.m.spin, P.m.mass_sign);
+    const Sym4<T> g = metric<METRIC>::template compute_g<T>(X.x, X.y, X.z, P.m);
+    const V4<T> u = metric<METRIC>::template reference_observer<T>(X.x, X.y, X.z, P.m);
     const Tetrad<T> e = build_tetrad<T>(g, V4<T>{T(1), T(0), T(0), T(0)}, V4<T>{T(0), T(1), T(0), T(0)},
                                         V4<T>{T(0), T(0), T(1), T(0)}, u);
     const V4<T> p{X.px, X.py, X.pz, pt};
@@ -562,10 +529,13 @@ template <Fuse F, class T> __device__ __forceinline__ T radius2(const S7<T>& y) 
 // the exact horizon test; NaN positions always take it.
 template <int METRIC, Fuse F, class T>
 __device__ __forceinline__ uint32_t plain_terminal(const DevScene<T>& P, const S7<T>& y1, T r2, uint32_t steps) {
-    if constexpr (METRIC != MGK_METRIC_MINKOWSKI) {
-        T q = r2 - P.kerr_a * P.kerr_a;
-        if (!(q > T(4) * P.m.horizon * P.m.horizon) && in_domain<METRIC, T>(y1.x, y1.y, y1.z, P.m))
-            return MGK_RAY_HORIZON;
+    if constexpr (metric<METRIC>::has_horizon) {
+        bool test = true;
+        if constexpr (metric<METRIC>::ks_radius_bound) {
+            T q = r2 - P.kerr_a * P.kerr_a;
+            test = !(q > T(4) * P.m.horizon * P.m.horizon);
+        }
+        if (test && in_domain<METRIC, T>(y1.x, y1.y, y1.z, P.m)) return MGK_RAY_HORIZON;
     }
     if (steps >= P.max_steps) return MGK_RAY_STEP_LIMIT;
     return MGK_RAY_ALIVE;
@@ -599,7 +569,7 @@ __device__ __forceinline__ Term<T> resolve(const DevScene<T>& P, const S7<T>& y0
         S7<T> ys = refine<METRIC, F, T>(1, y0, y1, pt, h, T(0), P.m, evals);
         T rh = kerr_schild_r(ys.x, ys.y, ys.z, P.kerr_a);
         if (rh >= P.disk_r_in && rh <= P.disk_r_out) {
-            V4<T> u = disk_velocity<T>(ys.x, ys.z, rh, P, METRIC);
+            V4<T> u = matter<MGK_RAY_DISK>::template four_velocity<METRIC, T>(P, ys.x, ys.y, ys.z, rh);
             o.cls = MGK_RAY_DISK;
             o.z = redshift_clamp<T>(c0 / dot4(u, V4<T>{ys.px, ys.py, ys.pz, pt}));
             o.r_hit = rh;
@@ -613,7 +583,7 @@ __device__ __forceinline__ Term<T> resolve(const DevScene<T>& P, const S7<T>& y0
         y_end = ys;
         if (ev.light) {
             // absorbed: the light's spectrum at the redshift seen by its (static) observer
-            const V4<T> u = reference_observer<T>(P.metric, ys.x, ys.y, ys.z, P.m.spin, P.m.mass_sign);
+            const V4<T> u = matter<MGK_RAY_LIGHT>::template four_velocity<METRIC, T>(P, ys.x, ys.y, ys.z, T(0));
             o.cls = MGK_RAY_LIGHT;
             o.z = redshift_clamp<T>(c0 / dot4(u, V4<T>{ys.px, ys.py, ys.pz, pt}));
             return o;
@@ -625,7 +595,7 @@ __device__ __forceinline__ Term<T> resolve(const DevScene<T>& P, const S7<T>& y0
             o.cls = MGK_RAY_STEP_LIMIT;
             return o;
         }
-        reflect_wall<T>(P, ev.axis, ev.side, ys, pt, c0, bn.count, bn.ray_id, y_end);
+        reflect_wall<METRIC, T>(P, ev.axis, ev.side, ys, pt, c0, bn.count, bn.ray_id, y_end);
         bn.count += 1u;
         bn.reflected = true;
         if (steps >= P.max_steps) o.cls = MGK_RAY_STEP_LIMIT;
@@ -637,7 +607,8 @@ __device__ __forceinline__ Term<T> resolve(const DevScene<T>& P, const S7<T>& y0
         T pn = sqrt(mad<F>(ys.pz, ys.pz, mad<F>(ys.py, ys.py, ys.px * ys.px)));
         o.cls = MGK_RAY_ESCAPED;
         o.d0 = ys.px / pn; o.d1 = ys.py / pn; o.d2 = ys.pz / pn;
-        o.z = redshift_clamp<T>(c0 / pt);
+        static_assert(matter<MGK_RAY_ESCAPED>::at_infinity, "the sky is static at infinity");
+        o.z = redshift_clamp<T>(c0 / pt);  // u . p = p_t
         y_end = ys;
         return o;
     }

@@ -110,10 +110,10 @@ template <int METRIC, int MODE, class T>
 __device__ __forceinline__ void attempt(const DevScene<T>& P, const S7<T>& y, T pt, T h, S7<T>& y1, T& h_next,
                                         bool& ok) {
     constexpr Fuse F = ModeT<MODE>::F;
-    if constexpr (METRIC == MGK_METRIC_MINKOWSKI) {
+    if constexpr (metric<METRIC>::explicit_euler) {
         // explicit Euler with a fixed step, metric_minkowski.cuh:49-53
         S7<T> f;
-        rhs_minkowski<T>(y, pt, f);
+        rhs<METRIC, F, T>(y, pt, P.m, f);
         y1 = axpy<F>(h, f, y);
         h_next = h;
         ok = true;
@@ -152,7 +152,7 @@ __device__ __forceinline__ void attempt_wide(const DevScene<float>& P, const S7<
 __device__ __forceinline__ bool in_band(const DevScene<float>& P, float x, float y, float z) {
     float q = (x * x + y * y + z * z) - P.kerr_a * P.kerr_a;
     if (q > float(P.band_pre2)) return false;
-    double r = ks_r<double>(double(x), double(y), double(z), P.spin_d);
+    double r = kerr_schild_r<double>(double(x), double(y), double(z), P.spin_d);
     return r - P.r_plus < MGK_WIDE_BAND;
 }
 
@@ -314,7 +314,7 @@ __global__ void __launch_bounds__(kIntegrateThreads, MODE == MGK_PRECISION_F64 ?
                     }
                     tries = 0;
                     alive = true;
-                    if constexpr (MODE == MGK_PRECISION_MIXED && METRIC != MGK_METRIC_MINKOWSKI)
+                    if constexpr (MODE == MGK_PRECISION_MIXED && metric<METRIC>::has_horizon)
                         to_band = in_band(P, y.x, y.y, y.z);
                 }
             }
@@ -351,7 +351,7 @@ __global__ void __launch_bounds__(kIntegrateThreads, MODE == MGK_PRECISION_F64 ?
                 cross = disk || r2 >= P.escape_r2;
                 if (!cross) {
                     cls = plain_terminal<METRIC, F, T>(P, y1, r2, steps);
-                    if constexpr (MODE == MGK_PRECISION_MIXED && METRIC != MGK_METRIC_MINKOWSKI) {
+                    if constexpr (MODE == MGK_PRECISION_MIXED && metric<METRIC>::has_horizon) {
                         if (cls == MGK_RAY_ALIVE) to_band = in_band(P, y.x, y.y, y.z);
                     }
                 }
@@ -739,7 +739,7 @@ __global__ void __launch_bounds__(128, 4) k_tail(const DevScene<typename ModeT<M
                     bn.ray_id = P.ray_base + e.ray;
                     tries = 0;
                     if constexpr (MODE == MGK_PRECISION_MIXED)
-                        r_cur = ks_r<double>(double(y.x), double(y.y), double(y.z), P.spin_d);
+                        r_cur = kerr_schild_r<double>(double(y.x), double(y.y), double(y.z), P.spin_d);
                     alive = true;
                 }
             }
@@ -762,7 +762,7 @@ __global__ void __launch_bounds__(128, 4) k_tail(const DevScene<typename ModeT<M
             bool ok;
             const T h_used = h;
             bool w = false;
-            if constexpr (MODE == MGK_PRECISION_MIXED && METRIC != MGK_METRIC_MINKOWSKI) {
+            if constexpr (MODE == MGK_PRECISION_MIXED && metric<METRIC>::has_horizon) {
                 w = r_cur - P.r_plus < MGK_WIDE_BAND;
                 if (w) attempt_wide<METRIC>(P, y, pt, h, y1, hn, ok);
                 else attempt<METRIC, MODE, T>(P, y, pt, h, y1, hn, ok);
@@ -786,7 +786,7 @@ __global__ void __launch_bounds__(128, 4) k_tail(const DevScene<typename ModeT<M
                 }
                 if (t.cls != MGK_RAY_ALIVE) done = true;
                 else if constexpr (MODE == MGK_PRECISION_MIXED)
-                    r_cur = ks_r<double>(double(y.x), double(y.y), double(y.z), P.spin_d);
+                    r_cur = kerr_schild_r<double>(double(y.x), double(y.y), double(y.z), P.spin_d);
             }
         }
 
@@ -902,18 +902,19 @@ __global__ void __launch_bounds__(256) k_shade(const DevScene<T> P, const HitEnt
                 if (spec) atomicAdd(spec + k, sv * P.inv_spp);
             }
         };
+        // the emission of the matter the ray ended on (src/renderer/bxdf/matter.cuh)
         if (h.cls == MGK_RAY_DISK) {
-            // T(r) = T_in (r / r_in)^(-3/4)
-            add(T(1), P.disk_T_in * exp2(T(-0.75) * log2(h.r_hit / P.disk_r_in)));
+            matter<MGK_RAY_DISK>::blackbodies(P, h, stars, grid, add);
         } else if (ROOM && h.cls == MGK_RAY_LIGHT) {
-            // white LED at the shifted wavelength, boosted by z^5
+            // spectral radiance at the shifted wavelength, boosted by z^5
             // (matter_examples.cuh:67-76, bxdf_utilities.cuh:156-163)
+            using L = matter<MGK_RAY_LIGHT>;
             const T z2 = h.z * h.z, z5 = z2 * z2 * h.z;
             if (sampled) {
-                rad = clamp_radiance<T>(white_led<T>(h.z * lam) * P.light_scale * z5);
+                rad = clamp_radiance<T>(L::radiance<T>(P, h.z * lam) * z5);
             } else {
                 for (uint32_t k = 0; k < nb; ++k) {
-                    float sv = float(clamp_radiance<T>(white_led<T>(h.z * P.lambda[k]) * P.light_scale * z5));
+                    float sv = float(clamp_radiance<T>(L::radiance<T>(P, h.z * P.lambda[k]) * z5));
                     const float4 w = sw[k];
                     X = __fmaf_rn(sv, w.x, X);
                     Y = __fmaf_rn(sv, w.y, Y);
@@ -921,16 +922,8 @@ __global__ void __launch_bounds__(256) k_shade(const DevScene<T> P, const HitEnt
                     if (spec) atomicAdd(spec + k, sv * P.inv_spp);
                 }
             }
-        } else if (grid.n != 0u) {
-            const uint32_t cell = cube_cell(float(h.d0), float(h.d1), float(h.d2), grid.n);
-            const uint32_t j1 = grid.cell_start[cell + 1];
-            for (uint32_t j = grid.cell_start[cell]; j < j1; ++j) {
-                const mgk_star st = stars[grid.cell_stars[j]];
-                T dx = h.d0 - T(st.dir[0]), dy = h.d1 - T(st.dir[1]), dz = h.d2 - T(st.dir[2]);
-                T q = mad<Fuse::Fma>(dz, dz, mad<Fuse::Fma>(dy, dy, dx * dx)) * P.star_inv_r2;
-                if (q >= T(1)) continue;
-                add(T(st.amplitude) * ((T(1) - q) * (T(1) - q)), T(st.temperature));
-            }
+        } else {
+            matter<MGK_RAY_ESCAPED>::blackbodies(P, h, stars, grid, add);  // the hit queue holds no other class
         }
         if (sampled) {
             const T irr = (rad * tput) * P.sensor_gain;
@@ -975,22 +968,17 @@ __global__ void __launch_bounds__(256) k_resolve(uint64_t first_pixel, uint32_t 
 }
 
 // --------------------------------------------------------- trace_geodesic
-// host_trace_geodesic.cu:13-130 on the GPU, REF32 arithmetic, one thread per
-// geodesic; the observer set-up that needs sin/cos is done on the host.
-__global__ void __launch_bounds__(64) k_trace_geodesic(const TraceJob* __restrict__ jobs, uint32_t n,
-                                                       magik_trace_geodesic_step_t* steps_all, uint32_t* written) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const TraceJob J = jobs[i];
-    magik_trace_geodesic_step_t* st = steps_all + J.step_offset;
+// One geodesic of the reference trace in the metric with tag METRIC.
+template <int METRIC>
+__device__ __forceinline__ uint32_t trace_geodesic_one(const TraceJob& J, magik_trace_geodesic_step_t* st) {
+    using MT = metric<METRIC>;
     MP<float> m{};
     m.spin = J.spin; m.mass_sign = J.mass_sign; m.horizon = J.horizon; m.spin_abs_gt1 = J.spin_abs_gt1;
     m.h_max = 1000.0f; m.abs_tol = J.atol; m.rel_tol = J.rtol; m.n_max = uint32_t(J.n_max);
     set_spin_consts(m);
-    const int metric = J.metric;
     V4<float> x0{J.x0[0], J.x0[1], J.x0[2], J.x0[3]};
-    Sym4<float> g = compute_g<float>(metric, x0.x, x0.y, x0.z, J.spin, J.mass_sign);
-    V4<float> u_ref = reference_observer<float>(metric, x0.x, x0.y, x0.z, J.spin, J.mass_sign);
+    Sym4<float> g = MT::template compute_g<float>(x0.x, x0.y, x0.z, m);
+    V4<float> u_ref = MT::template reference_observer<float>(x0.x, x0.y, x0.z, m);
     V4<float> X{J.seed[0][0], J.seed[0][1], J.seed[0][2], J.seed[0][3]};
     V4<float> Yv{J.seed[1][0], J.seed[1][1], J.seed[1][2], J.seed[1][3]};
     V4<float> Z{J.seed[2][0], J.seed[2][1], J.seed[2][2], J.seed[2][3]};
@@ -1005,7 +993,7 @@ __global__ void __launch_bounds__(64) k_trace_geodesic(const TraceJob* __restric
     S7<float> y{x0.x, x0.y, x0.z, x0.t, p0.x, p0.y, p0.z};
     float pt = p0.t;
     const float contraction = dot4<float>(u, p0);
-    float h = metric == MGK_METRIC_MINKOWSKI ? 1000.0f : 1.0f;
+    float h = float(MT::initial_h_step());
     float aff = 0.0f;
     auto put = [&](uint32_t k, const S7<float>& s, const S7<float>& ds) {
         magik_trace_geodesic_step_t o;
@@ -1018,28 +1006,22 @@ __global__ void __launch_bounds__(64) k_trace_geodesic(const TraceJob* __restric
         o.delta_affine_parameter = h;
         st[k] = o;
     };
-    auto rhs_any = [&](const S7<float>& s, S7<float>& o) {
-        if (metric == MGK_METRIC_KERR) rhs_kerr<Fuse::None, float>(s, pt, m.spin, o);
-        else if (metric == MGK_METRIC_SCHWARZSCHILD) rhs_schwarzschild<Fuse::None, float>(s, pt, m.mass_sign, o);
-        else rhs_minkowski<float>(s, pt, o);
-    };
     S7<float> ys;
-    rhs_any(y, ys);
+    rhs<METRIC, Fuse::None, float>(y, pt, m, ys);
     put(0, y, ys);
     uint32_t nw = 1;
     while (nw < J.n_steps) {
         S7<float> y1;
         float h_taken = h;
-        if (metric == MGK_METRIC_MINKOWSKI) {
+        if constexpr (MT::explicit_euler) {
             S7<float> f;
-            rhs_minkowski<float>(y, pt, f);
+            rhs<METRIC, Fuse::None, float>(y, pt, m, f);
             y1 = axpy<Fuse::None>(h, f, y);
         } else {
             float temp_h = h;
             for (uint32_t a = 0; a < m.n_max; ++a) {
                 S7<float> k[6];
-                if (metric == MGK_METRIC_KERR) rkf45_stages<MGK_METRIC_KERR, Fuse::None, float>(y, pt, temp_h, m, y1, k);
-                else rkf45_stages<MGK_METRIC_SCHWARZSCHILD, Fuse::None, float>(y, pt, temp_h, m, y1, k);
+                rkf45_stages<METRIC, Fuse::None, float>(y, pt, temp_h, m, y1, k);
                 S7<float> er = rkf45_error<Fuse::None, float>(temp_h, k);
                 float err = rms_error<Fuse::None, float>(er, y, y1, m.abs_tol, m.rel_tol);
                 float safe = err > 1e-30f ? err : 1e-30f;
@@ -1051,18 +1033,27 @@ __global__ void __launch_bounds__(64) k_trace_geodesic(const TraceJob* __restric
             h = temp_h;
         }
         y = y1;
-        rhs_any(y, ys);
+        rhs<METRIC, Fuse::None, float>(y, pt, m, ys);
         aff = aff + h_taken;
         put(nw, y, ys);
         ++nw;
-        bool cap;
-        if (metric == MGK_METRIC_KERR) cap = in_domain<MGK_METRIC_KERR, float>(y.x, y.y, y.z, m);
-        else if (metric == MGK_METRIC_SCHWARZSCHILD) cap = in_domain<MGK_METRIC_SCHWARZSCHILD, float>(y.x, y.y, y.z, m);
-        else cap = false;
-        if (cap) break;
+        if (MT::has_horizon && in_domain<METRIC, float>(y.x, y.y, y.z, m)) break;
     }
     for (uint32_t k = 0; k < nw; ++k)
         for (int c = 0; c < 4; ++c) st[k].four_position[c] *= J.length_scale;
+    return nw;
+}
+
+// host_trace_geodesic.cu:13-130 on the GPU, REF32 arithmetic, one thread per
+// geodesic; the observer set-up that needs sin/cos is done on the host.
+__global__ void __launch_bounds__(64) k_trace_geodesic(const TraceJob* __restrict__ jobs, uint32_t n,
+                                                       magik_trace_geodesic_step_t* steps_all, uint32_t* written) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const TraceJob J = jobs[i];
+    magik_trace_geodesic_step_t* st = steps_all + J.step_offset;
+    uint32_t nw = 0;
+    with_metric(J.metric, [&](auto mt) { nw = trace_geodesic_one<decltype(mt)::tag>(J, st); });
     written[i] = nw;
 }
 
@@ -1103,12 +1094,15 @@ __global__ void __launch_bounds__(128) k_generate_samples(const DevScene<typenam
     const double ci = cos(incl), si = sin(incl);
     const double ct = u2, st = sqrt(fmax(0.0, 1.0 - ct * ct)), ph = 2.0 * 3.14159265358979323846 * u3;
     const double nx = st * cos(ph), ny = st * sin(ph), nz = -ct;
-    const int metric = P.metric;
-    const double a = P.spin_d, ms = double(P.m.mass_sign);
     V4<double> q{0.0, r_obs * ci, r_obs * si, 0.0};
     V4<double> X{1, 0, 0, 0}, Y{0, si, -ci, 0}, Z{0, ci, si, 0};
-    V4<double> u = reference_observer<double>(metric, q.x, q.y, q.z, a, ms);
-    Sym4<double> g = compute_g<double>(metric, q.x, q.y, q.z, a, ms);
+    V4<double> u{};
+    Sym4<double> g{};
+    with_metric(P.metric, [&](auto mt) {
+        using MT = decltype(mt);
+        u = MT::template reference_observer<double>(q.x, q.y, q.z, P.md);
+        g = MT::template compute_g<double>(q.x, q.y, q.z, P.md);
+    });
     Tetrad<double> e = build_tetrad<double>(g, X, Y, Z, u);
     V4<double> pu = local_to_global<double>(e, V4<double>{nx, ny, nz, 1.0});
     V4<double> p = contract<double>(g, pu);
@@ -1205,7 +1199,7 @@ cudaError_t launch_camera_features(const mgk_scene& s, const void* dsc, uint64_t
 __device__ __forceinline__ double critical_distance(double x, double y, double z, double px, double py, double pz,
                                                     double pt, double a) {
     const double E = -pt, L = z * px - x * pz;
-    const double r = ks_r<double>(x, y, z, a);
+    const double r = kerr_schild_r<double>(x, y, z, a);
     const double ct = y / r, st2 = fmax(1e-300, 1.0 - ct * ct), st = sqrt(st2);
     const double pth = (ct / st) * (x * px + z * pz) - r * st * py;
     const double Q = pth * pth + ct * ct * (L * L / st2 - a * a * E * E);
@@ -1442,7 +1436,7 @@ static cudaError_t integ_t(const void* dsc, uint64_t first, uint32_t n, const Ch
     uint32_t passes = 0;
     if constexpr (ROOM) passes = (cont[0] && cont[1]) ? P.room_limit + 1u : 0u;
     else passes = (MGK_MISS_PASS && cont[1]) ? 1u : 0u;
-    if constexpr (MGK_MIXED_X2 && MODE == MGK_PRECISION_MIXED && METRIC != MGK_METRIC_MINKOWSKI) {
+    if constexpr (MGK_MIXED_X2 && MODE == MGK_PRECISION_MIXED && (METRIC == MGK_METRIC_KERR || METRIC == MGK_METRIC_SCHWARZSCHILD)) {
         // two rays per thread: half the threads for the same rays
         per_sm = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_integrate_x2<METRIC>, kIntegrateThreads, 0);
@@ -1489,17 +1483,14 @@ static cudaError_t integ_t(const void* dsc, uint64_t first, uint32_t n, const Ch
 template <int MODE>
 static cudaError_t integ_m(int metric, bool room, const void* dsc, uint64_t first, uint32_t n, const ChunkBuffers& b,
                            mgk_ray_result* res, int sms, cudaStream_t st) {
-    switch (metric) {
-        case MGK_METRIC_KERR:
-            return room ? integ_t<MGK_METRIC_KERR, MODE, true>(dsc, first, n, b, res, sms, st)
-                        : integ_t<MGK_METRIC_KERR, MODE, false>(dsc, first, n, b, res, sms, st);
-        case MGK_METRIC_SCHWARZSCHILD:
-            return room ? integ_t<MGK_METRIC_SCHWARZSCHILD, MODE, true>(dsc, first, n, b, res, sms, st)
-                        : integ_t<MGK_METRIC_SCHWARZSCHILD, MODE, false>(dsc, first, n, b, res, sms, st);
-        default:
-            return room ? integ_t<MGK_METRIC_MINKOWSKI, MODE, true>(dsc, first, n, b, res, sms, st)
-                        : integ_t<MGK_METRIC_MINKOWSKI, MODE, false>(dsc, first, n, b, res, sms, st);
-    }
+    // the reference's dispatch_list over supported_metrics
+    cudaError_t e = cudaErrorInvalidValue;
+    with_metric(metric, [&](auto mt) {
+        constexpr int TAG = decltype(mt)::tag;
+        e = room ? integ_t<TAG, MODE, true>(dsc, first, n, b, res, sms, st)
+                 : integ_t<TAG, MODE, false>(dsc, first, n, b, res, sms, st);
+    });
+    return e;
 }
 
 cudaError_t launch_integrate(const mgk_scene& s, const void* dsc, uint64_t first, uint32_t n, const ChunkBuffers& b,
@@ -1559,40 +1550,27 @@ size_t dev_scene_size(const mgk_scene& s) {
 template <class T> static void fill_t(const mgk_scene& s, const float* xyz_w, DevScene<T>* P) {
     SceneConsts c = scene_consts(s);
     *P = DevScene<T>{};
-    const double a_t = s.time_reversed ? -s.spin : s.spin;
-    const bool kerr = s.metric == MGK_METRIC_KERR;
-    P->m.spin = T(kerr ? a_t : 0.0);
-    P->m.mass_sign = T(s.mass_sign < 0 ? -1.0 : 1.0);
-    // the reference's capture radius, evaluated in T like in_domain does
-    if (kerr) {
-        T a = T(a_t);
-        P->m.horizon = (T(1) + std::sqrt(T(1) - a * a)) * T(s.horizon_scalar);
-        P->m.spin_abs_gt1 = (a > T(1) || a < T(-1)) ? T(1) : T(0);
-    } else {
-        P->m.horizon = T(2) * T(s.horizon_scalar);
-        P->m.spin_abs_gt1 = T(0);
-    }
-    P->m.h_max = T(s.h_max);
-    P->m.abs_tol = T(s.abs_tol);
-    P->m.rel_tol = T(s.rel_tol);
-    P->m.n_max = s.n_max_substep;
-    P->md.spin = kerr ? a_t : 0.0;
-    P->md.mass_sign = s.mass_sign < 0 ? -1.0 : 1.0;
-    P->md.horizon = double(P->m.horizon);
-    P->md.spin_abs_gt1 = double(P->m.spin_abs_gt1);
-    P->md.h_max = s.h_max;
-    P->md.abs_tol = s.abs_tol;
-    P->md.rel_tol = s.rel_tol;
-    P->md.n_max = s.n_max_substep;
-    set_spin_consts(P->m);
-    set_spin_consts(P->md);
+    double spin = 0.0, h0 = 1.0;
+    with_metric(s.metric, [&](auto mt) {
+        using MT = decltype(mt);
+        // the metric's parameters (params_t / make_params) in T and in double;
+        // the FP64 attempts of the MIXED mode capture at the radius and with
+        // the flag the FP32 state uses
+        P->m = scene_params<MT, T>(s);
+        P->md = scene_params<MT, double>(s);
+        P->md.horizon = double(P->m.horizon);
+        P->md.spin_abs_gt1 = double(P->m.spin_abs_gt1);
+        spin = MT::spin(s);
+        h0 = MT::initial_h_step();
+    });
+    const double a_t = P->md.spin;  // the spin as integrated (0 for spherical metrics)
     for (int i = 0; i < 4; ++i) {
         P->cam[i] = T(c.cam_pos[i]);
         P->u_obs[i] = T(c.u_obs[i]);
         for (int j = 0; j < 4; ++j) P->M[i][j] = T(c.M[i][j]);
     }
     P->pix_a = T(c.pix_a); P->pix_b = T(c.pix_b); P->pix_c = T(c.pix_c); P->pix_d = T(c.pix_d);
-    P->h0 = s.metric == MGK_METRIC_MINKOWSKI ? T(1000) : T(1);
+    P->h0 = T(h0);
     P->disk_on = s.disk_r_out > 0.0 ? 1u : 0u;
     P->disk_r_in = T(s.disk_r_in);
     P->disk_r_out = T(s.disk_r_out);
@@ -1601,16 +1579,16 @@ template <class T> static void fill_t(const mgk_scene& s, const float* xyz_w, De
     P->disk_hi = T(1.02 * s.disk_r_out + 0.02);
     T er = T(s.escape_radius);
     P->escape_r2 = er * er;
-    P->spin_phys = T(kerr ? s.spin : 0.0);
+    P->spin_phys = T(spin);
     P->omega_sign = T(c.omega_sign);
-    P->kerr_a = T(kerr ? a_t : 0.0);
+    P->kerr_a = T(a_t);
     P->r_plus = c.r_plus;
     double pre = c.r_plus + MGK_WIDE_BAND + 0.01;
     P->band_pre2 = pre * pre;
     P->atol_d = s.abs_tol;
     P->rtol_d = s.rel_tol;
     P->hmax_d = s.h_max;
-    P->spin_d = kerr ? a_t : 0.0;
+    P->spin_d = a_t;
     T rr = T(s.star_radius_rad);
     P->star_inv_r2 = T(1) / (rr * rr);
     double dl = (s.lambda_max_nm - s.lambda_min_nm) / s.n_bins;

@@ -32,6 +32,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/mgk_manager.h"
+#include "../src/renderer/relativity/metric.cuh"
 #include "internal.h"
 
 namespace {
@@ -634,11 +635,12 @@ MGK_API mgk_result mgk_stage_apply(mgk_stage* s, const uint32_t* chunks, uint32_
 MGK_API mgk_result mgk_stage_scene(const mgk_stage* st, uint64_t seed, mgk_scene* out, mgk_display_settings* ds) {
     if (!st || !out || !ds) return MGK_ERROR_INVALID_POINTER;
     if (st->metric_type < 0 || st->metric_type > 2) return MGK_ERROR_UNKNOWN_METRIC;
-    const double G = 6.67430e-11, c = 299792458.0;
+    const double c = 299792458.0;
     const bool kerr = st->metric_type == MGK_METRIC_KERR, schw = st->metric_type == MGK_METRIC_SCHWARZSCHILD;
     const double mass = kerr ? st->kerr_mass : st->schwarzschild_mass;
-    // the metric's length scale (metric_*.cuh length_scale): M in metres
-    const double L = (kerr || schw) ? G * std::fabs(mass) / (c * c) : 1.0;
+    // the metric's length scale (metric<TAG>::length_scale): M in metres
+    double L = 0.0;
+    mgk::with_metric(st->metric_type, [&](auto mt) { L = decltype(mt)::length_scale(std::fabs(mass)); });
     if (!(L > 0.0) || !std::isfinite(L)) return MGK_ERROR_INVALID_ARGUMENT;
     mgk_scene s;
     mgk_scene_defaults(&s);
