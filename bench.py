@@ -11,10 +11,13 @@ step control with FP64 attempts next to the horizon (MIXED), escape radius
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
-Under torchrun every rank renders a sample slice of the frame (all pixels,
-its own jitter seed) and the films are sum-reduced into rank 0 inside the
-timed region: the work per GPU is fixed, so scaling is weak and the value is
-the total of all ranks.  Rank 0 prints one JSON line.
+Under torchrun the ranks share the one frame (--split spp, the default): rank
+r renders a contiguous slice of the 16 samples per pixel (all pixels, the same
+seed), and the films, weighted by their share of the samples, are
+sum-reduced into rank 0 inside the timed region; the total work is fixed, so
+scaling is strong.  --split seeds renders all 16 samples on every rank with
+its own seed instead (weak scaling: N x 16 samples per pixel).  The value is
+the geodesics of all ranks per second.  Rank 0 prints one JSON line.
 """
 import argparse
 import json
@@ -48,6 +51,8 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mgk", choices=["mgk", "reference"])
+    ap.add_argument("--split", default="spp", choices=["spp", "seeds"],
+                    help="multi-GPU split: sample slices of one frame (strong) or one frame per rank (weak)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU sample budget per measurement")
     # frame-size overrides for profiling captures (the default is the benchmark workload)
@@ -66,11 +71,18 @@ def parse_args():
 ARGS = None
 
 
-def scene_config(M, rank=0):
-    from magik_b200.dist import frame_seed
+def scene_config(M, rank=0, world=1):
+    """The scene a rank renders: the whole frame at one rank; with --split
+    spp its slice of the frame's samples, with --split seeds the whole frame
+    under its own seed."""
+    from magik_b200.dist import frame_seed, sample_slice
     s = M.scene_defaults()
-    s.seed = frame_seed(0x5EED, rank)
     _resize(s)
+    if ARGS is not None and ARGS.split == "seeds":
+        s.seed = frame_seed(0x5EED, rank)
+    else:
+        s.seed = 0x5EED
+        s.sample_offset, s.spp = sample_slice(s.spp, rank, world)
     return s
 
 
@@ -502,13 +514,24 @@ def run_gpu(args, rank, world, local_rank):
     import magik_b200 as M
     from magik_b200 import flops as FL
 
-    from magik_b200.dist import reduce_film
+    from magik_b200.dist import reduce_film, reduce_slices
     torch.cuda.set_device(local_rank)
     dev = f"cuda:{local_rank}"
     ctx = M.Context(local_rank)
-    s = scene_config(M, rank)
-    rays = s.width * s.height * s.spp
+    strong = args.split == "spp"
+    s = scene_config(M, rank, world)       # what this rank renders
+    s_frame = scene_config(M, 0, 1)        # the frame
+    rays = s.width * s.height * s.spp     # this rank's geodesics per step
     npix = s.width * s.height
+    total_rays = s_frame.width * s_frame.height * s_frame.spp * (1 if strong else world)
+
+    def combine(f):
+        # the one exchange step: the ranks' films into rank 0's
+        if world > 1:
+            if strong:
+                reduce_slices(f, s.spp, s_frame.spp)
+            else:
+                reduce_film(f)
     stars = M.star_catalog(STAR_SEED, N_STARS)
     w = M.xyz_weights(s.n_bins)
     d_stars = torch.from_numpy(stars.view(np.uint8)).to(dev)
@@ -539,8 +562,7 @@ def run_gpu(args, rank, world, local_rank):
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record()
         st = ctx.render(s, d_stars, film, d_weights=d_w, want_stats=True)
-        if world > 1:
-            reduce_film(film)  # the sample slices of all ranks into rank 0's image
+        combine(film)
         e1.record()
         e1.synchronize()
         times.append(e0.elapsed_time(e1))
@@ -556,15 +578,25 @@ def run_gpu(args, rank, world, local_rank):
     h_w = torch.from_numpy(w.ravel().copy()).pin_memory()
     h_film = torch.empty(npix * 3, dtype=torch.float32).pin_memory()
     e2e_times = []
-    if not args.no_e2e:
+    d_tmp = torch.empty_like(film) if world > 1 else None
+
+    def render_e2e():
         ctx.render_host(s, h_stars, h_film, h_weights=h_w, want_stats=False)
+        if world > 1:  # the host film through the same exchange step, back to rank 0's host
+            d_tmp.copy_(h_film, non_blocking=True)
+            combine(d_tmp)
+            if rank == 0:
+                h_film.copy_(d_tmp, non_blocking=True)
+
+    if not args.no_e2e:
+        render_e2e()
         for _ in range(max(1, min(args.steps, 3))):
             flush.fill_(1)
             torch.cuda.synchronize()
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record()
-            ctx.render_host(s, h_stars, h_film, h_weights=h_w, want_stats=False)
+            render_e2e()
             e1.record()
             e1.synchronize()
             e2e_times.append(e0.elapsed_time(e1))
@@ -576,22 +608,29 @@ def run_gpu(args, rank, world, local_rank):
     ms = statistics.mean(times)
     e2e_ms = statistics.mean(e2e_times)
     ms_int = statistics.mean(integ)
+    steps_all = float(st_last.steps)
     if world > 1:
-        from magik_b200.dist import max_over_ranks
+        from magik_b200.dist import max_over_ranks, sum_over_ranks
         ms, e2e_ms, ms_int = max_over_ranks([ms, e2e_ms, ms_int], device=dev)
+        steps_all = sum_over_ranks([steps_all], device=dev)[0]
     if rank != 0:
         return None
 
     achieved = statistics.mean(f / (t * 1e-3) for f, t in zip(flop, integ))
     out = {
-        "metric": METRIC, "value": world * rays / (ms * 1e-3), "unit": UNIT, "n_gpus": world,
+        "metric": METRIC, "value": total_rays / (ms * 1e-3), "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "fp32 (fp64 attempts next to the horizon)",
+        "scaling": "strong" if strong else "weak", "vs_baseline": None,
+        "dtype": "fp32 (fp64 attempts next to the horizon)",
         "data": "synthetic (seeded camera jitter and star catalogue)",
         # one camera geodesic per pixel sample: samples/s equals geodesics/s
-        "samples_per_s": world * rays / (ms * 1e-3),
-        "config": config_dict(s, {"parallelism": f"{world} sample slices of one frame, film sum-reduced into rank 0 (weak)"}),
-        "e2e": {"value": world * rays / (e2e_ms * 1e-3), "unit": UNIT,
+        "samples_per_s": total_rays / (ms * 1e-3),
+        "config": config_dict(s_frame, {"parallelism": (
+            f"{world} GPU(s): each renders {s.spp} of the frame's {s_frame.spp} samples per pixel "
+            f"(sample slices of one frame), films weighted and sum-reduced into rank 0 (strong)") if strong else (
+            f"{world} GPU(s): each renders the whole frame with its own seed, films averaged into rank 0 "
+            f"(weak: {world} x {s_frame.spp} samples per pixel)")}),
+        "e2e": {"value": total_rays / (e2e_ms * 1e-3), "unit": UNIT,
                 "h2d_bytes_per_step": int(h_stars.numel() + h_w.numel() * 4),
                 "d2h_bytes_per_step": int(h_film.numel() * 4)},
         "roofline": {"bound": "fp32", "kernel": "k_integrate + k_refine + k_tail (one chunk)",
@@ -606,7 +645,7 @@ def run_gpu(args, rank, world, local_rank):
                      "integrate_ms": ms_int,
                      "work": "attempts taken in FP32 and crossing sub-steps; the FP64 attempts are in roofline_fp64"},
         "roofline_fp64": split_rooflines(s.metric, st_last, ms_int, peaks_fp)[1],
-        "steps_per_s": world * st_last.steps / (ms * 1e-3),
+        "steps_per_s": steps_all / (ms * 1e-3),
         "stats": {"attempts": st_last.attempts, "steps": st_last.steps, "refine_evals": st_last.refine_evals,
                   "wide_attempts": st_last.wide_attempts, "crossings": st_last.crossings,
                   "resumed": st_last.resumed,

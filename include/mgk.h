@@ -147,7 +147,12 @@ typedef struct mgk_scene {
      * (units of c) relative to the reference observer, in its tetrad with
      * seeds x, y, z (rest_frame_four_velocity, relativity_utilities.cuh:163-173). */
     uint32_t cam_explicit;
-    uint32_t reserved_cam;
+    /* Sample slices of one frame: the scene's spp samples per pixel are the
+     * frame's samples sample_offset .. sample_offset + spp - 1 (their jitter
+     * and random numbers), so that renders of disjoint slices combine, in
+     * proportion to their spp, into the render of the whole frame.  0 by
+     * default; sample_offset + spp <= 2^32. */
+    uint32_t sample_offset;
     double cam_pos[3];
     double cam_axes[9];      /* columns right, up, back (the camera looks along -back) */
     double cam_velocity[3];

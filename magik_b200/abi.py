@@ -47,7 +47,7 @@ class Scene(C.Structure):
         ("room_on", C.c_uint32), ("room_reflection_limit", C.c_uint32),
         ("room_min", C.c_double * 3), ("room_max", C.c_double * 3),
         ("light_min", C.c_double * 3), ("light_max", C.c_double * 3), ("light_scale", C.c_double),
-        ("cam_explicit", C.c_uint32), ("reserved_cam", C.c_uint32), ("cam_pos", C.c_double * 3),
+        ("cam_explicit", C.c_uint32), ("sample_offset", C.c_uint32), ("cam_pos", C.c_double * 3),
         ("cam_axes", C.c_double * 9), ("cam_velocity", C.c_double * 3),
     ]
 

@@ -72,6 +72,7 @@ mgk_result validate(const mgk_scene* s) {
         return MGK_ERROR_INVALID_ARGUMENT;
     if (s->max_steps < 1 || s->n_bins < 1 || s->n_bins > MGK_MAX_BINS) return MGK_ERROR_INVALID_ARGUMENT;
     if (s->width < 1 || s->height < 1 || s->spp < 1) return MGK_ERROR_INVALID_ARGUMENT;
+    if (uint64_t(s->sample_offset) + s->spp > (1ull << 32)) return MGK_ERROR_INVALID_ARGUMENT;
     if (uint64_t(s->width) * s->height >= (1ull << 32)) return MGK_ERROR_INVALID_ARGUMENT;
     if (!(s->escape_radius > 0.0) || !(s->lambda_max_nm > s->lambda_min_nm) || !(s->lambda_min_nm > 0.0))
         return MGK_ERROR_INVALID_ARGUMENT;

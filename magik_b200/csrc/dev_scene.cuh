@@ -167,6 +167,7 @@ template <class T> struct DevScene {
     uint32_t width, height, spp, n_bins, max_steps, disk_on;
     int32_t metric;
     float inv_spp;
+    uint32_t sample_offset;  // the frame's index of this render's first sample
     // MGK_SPECTRAL_SAMPLED
     uint32_t spectral_mode;
     float cmf_icdf[MGK_CMF_ICDF_ENTRIES];  // CIE inverse CDF, nm
@@ -187,7 +188,7 @@ template <class T> struct DevScene {
 // the observer's tetrad -> covariant momentum; also c0 = u_obs . p.
 template <Fuse F, class T>
 __device__ __forceinline__ void camera_ray(const DevScene<T>& P, uint64_t ray_id, S7<T>& y, T& pt, T& c0) {
-    uint32_t pixel = uint32_t(ray_id / P.spp), sample = uint32_t(ray_id % P.spp);
+    uint32_t pixel = uint32_t(ray_id / P.spp), sample = uint32_t(ray_id % P.spp) + P.sample_offset;
     uint32_t px = pixel % P.width, py = pixel / P.width;
     T jx = T(rng_unit(P.seed, sample, pixel, 0));
     T jy = T(rng_unit(P.seed, sample, pixel, 1));
@@ -499,7 +500,7 @@ __device__ __forceinline__ void reflect_wall(const DevScene<T>& P, int axis, int
         const T k = T(2) * (d[0] * n[0] + d[1] * n[1] + d[2] * n[2]);
         o[0] = d[0] - k * n[0]; o[1] = d[1] - k * n[1]; o[2] = d[2] - k * n[2];
     } else {
-        const uint32_t pixel = uint32_t(ray_id / P.spp), sample = uint32_t(ray_id % P.spp);
+        const uint32_t pixel = uint32_t(ray_id / P.spp), sample = uint32_t(ray_id % P.spp) + P.sample_offset;
         T q[3];
         sphere_dir<T>(P.seed, sample, pixel, 8u + 64u * bounce, q);
         o[0] = q[0] + n[0]; o[1] = q[1] + n[1]; o[2] = q[2] + n[2];

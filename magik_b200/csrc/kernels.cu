@@ -865,7 +865,7 @@ __global__ void __launch_bounds__(256) k_shade(const DevScene<T> P, const HitEnt
         // sampled mode: the ray's wavelength, throughput and Planck factors there
         T lam = T(0), tput = T(0), a_s = T(0), b_s = T(0), rad = T(0);
         if (sampled) {
-            const uint32_t pixel = uint32_t(ray_id / P.spp), sample = uint32_t(ray_id % P.spp);
+            const uint32_t pixel = uint32_t(ray_id / P.spp), sample = uint32_t(ray_id % P.spp) + P.sample_offset;
             const float x = rng_unit(P.seed, sample, pixel, 2) * float(MGK_CMF_ICDF_ENTRIES - 1);
             const uint32_t k = uint32_t(fminf(x, float(MGK_CMF_ICDF_ENTRIES) - 2.0f));
             const float f = x - float(k);
@@ -1169,7 +1169,7 @@ __global__ void k_camera_features(const DevScene<T> P, uint64_t first_ray, uint3
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint64_t ray_id = first_ray + i;
-    const uint32_t pixel = uint32_t(ray_id / P.spp), sample = uint32_t(ray_id % P.spp);
+    const uint32_t pixel = uint32_t(ray_id / P.spp), sample = uint32_t(ray_id % P.spp) + P.sample_offset;
     const uint32_t px = pixel % P.width, py = pixel / P.width;
     const double sx = (double(px) + rng_unit(P.seed, sample, pixel, 0)) * double(P.pix_a) + double(P.pix_b);
     const double sy = (double(py) + rng_unit(P.seed, sample, pixel, 1)) * double(P.pix_c) + double(P.pix_d);
@@ -1607,6 +1607,7 @@ template <class T> static void fill_t(const mgk_scene& s, const float* xyz_w, De
     P->max_steps = s.max_steps;
     P->metric = s.metric;
     P->inv_spp = 1.0f / float(s.spp);
+    P->sample_offset = s.sample_offset;
     P->spectral_mode = s.spectral_mode;
     if (s.spectral_mode == MGK_SPECTRAL_SAMPLED) {
         cmf_inverse_cdf_table(s.lambda_min_nm, s.lambda_max_nm, P->cmf_icdf);

@@ -1,9 +1,42 @@
 """Multi-GPU plumbing of the render: one process per GPU over
-torch.distributed (NCCL on GPUs, gloo on CPU).  Rays are independent, so the
-frame is split into sample slices: every rank renders all pixels with its own
-jitter seed (a different set of samples of the same image) and the one
-exchange step is a sum-reduce of the XYZ films into rank 0, which divides by
-the number of ranks.  Timings are combined with a max over ranks."""
+torch.distributed (NCCL on GPUs, gloo on CPU).  Rays are independent, so a
+frame splits into sample slices, and the one exchange step is a sum-reduce of
+the XYZ films into rank 0.  Two splits:
+
+* strong (sample_slice / reduce_slices): the ranks share one frame.  Rank r
+  renders a contiguous slice of its spp samples per pixel (mgk_scene's
+  sample_offset and spp), all pixels, the same seed; each film, weighted by
+  its share of the samples, sums into the film of the whole frame.  N ranks
+  render the same frame N times faster.
+* weak (frame_seed / reduce_film): every rank renders all pixels and all spp
+  samples with its own jitter seed, and the mean of the films is the image at
+  N x spp samples per pixel.
+
+Timings are combined with a max over ranks."""
+
+
+def sample_slice(spp, rank, world):
+    """(sample_offset, count): the samples of a frame of `spp` samples per
+    pixel that `rank` of `world` renders in the strong split, contiguous and
+    as even as the division allows (every rank needs at least one)."""
+    spp, rank, world = int(spp), int(rank), int(world)
+    if world < 1 or not 0 <= rank < world or spp < world:
+        raise ValueError(f"{spp} samples per pixel do not split over {world} ranks")
+    base, extra = divmod(spp, world)
+    return rank * base + min(rank, extra), base + (1 if rank < extra else 0)
+
+
+def reduce_slices(film, count, spp, dst=0):
+    """The film of the whole frame into rank `dst`, in place: each rank's
+    film (the mean over its `count` of the frame's `spp` samples) weighted by
+    count / spp, then sum-reduced (NCCL over NVLink on GPUs).  The other
+    ranks' films are scratch afterwards.  Identity with one rank."""
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return film
+    film.mul_(float(count) / float(spp))
+    dist.reduce(film, dst=dst, op=dist.ReduceOp.SUM)
+    return film
 
 
 def frame_seed(base_seed, rank):

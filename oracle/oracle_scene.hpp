@@ -133,7 +133,7 @@ template <class T> struct RayInit { GState<T> y; T c0; T h0; };
 template <Fuse F, class T>
 inline RayInit<T> camera_ray(const mgk_scene& s, const SceneConsts& c, uint64_t ray_id) {
     uint32_t spp = s.spp;
-    uint32_t pixel = uint32_t(ray_id / spp), sample = uint32_t(ray_id % spp);
+    uint32_t pixel = uint32_t(ray_id / spp), sample = uint32_t(ray_id % spp) + s.sample_offset;
     uint32_t px = pixel % s.width, py = pixel / s.width;
     T jx = T(rng_unit(s.seed, sample, pixel, 0));
     T jy = T(rng_unit(s.seed, sample, pixel, 1));
@@ -406,7 +406,7 @@ inline GState<T> reflect_wall(const mgk_scene& s, const MetricParams<T>& m, int 
         for (int i = 0; i < 3; ++i) o[i] = d[i] - k * n[i];
     } else {
         T q[3];
-        sphere_dir<T>(s.seed, uint32_t(ray_id % s.spp), uint32_t(ray_id / s.spp), 8u + 64u * bounce, q);
+        sphere_dir<T>(s.seed, uint32_t(ray_id % s.spp) + s.sample_offset, uint32_t(ray_id / s.spp), 8u + 64u * bounce, q);
         for (int i = 0; i < 3; ++i) o[i] = q[i] + n[i];
         if (!(o[0] * o[0] + o[1] * o[1] + o[2] * o[2] > T(1e-12)))
             for (int i = 0; i < 3; ++i) o[i] = n[i];
@@ -691,7 +691,7 @@ inline void sampled_spectrum(const mgk_scene& s, const StarIndex* stars, const H
                              const float* icdf, T* spec) {
     const uint32_t nb = s.n_bins;
     for (uint32_t k = 0; k < nb; ++k) spec[k] = T(0);
-    const uint32_t pixel = uint32_t(ray_id / s.spp), sample = uint32_t(ray_id % s.spp);
+    const uint32_t pixel = uint32_t(ray_id / s.spp), sample = uint32_t(ray_id % s.spp) + s.sample_offset;
     const float x = rng_unit(s.seed, sample, pixel, 2) * float(MGK_CMF_ICDF_ENTRIES - 1);
     const uint32_t k0 = uint32_t(std::fmin(x, float(MGK_CMF_ICDF_ENTRIES) - 2.0f));
     const float f = x - float(k0);

@@ -196,3 +196,70 @@ def test_one_rank_data_parallel_training_and_batch_checks():
     cfg.batch = 8192
     with pytest.raises(ValueError):  # fewer samples than one batch
         D.train_data_parallel(_LinearNet(5), cfg, X, y)
+
+
+def _strong_worker(rank, world, port, q):
+    """One rank of bench.py's strong split with the CPU oracle standing in
+    for the GPU render: bench.scene_config gives the rank its slice of the
+    frame's samples, the oracle renders it, and dist.reduce_slices (the
+    exchange step of run_gpu) assembles the frame in rank 0."""
+    import argparse
+    import datetime
+    import sys
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, root)
+    import bench
+    import magik_b200 as M
+    from magik_b200 import dist as D
+    from oracle import oracle_py as O
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    try:
+        bench.ARGS = argparse.Namespace(split="spp", width=24, height=16, spp=6)
+        s = bench.scene_config(M, rank, world)
+        stars = M.star_catalog(0x57A25, 20000)
+        w = M.xyz_weights(s.n_bins)
+        film, _ = O.render_pixels(s, stars, w, 0, s.width * s.height, nthreads=2)
+        f = torch.from_numpy(np.ascontiguousarray(film, dtype=np.float64).ravel())
+        D.reduce_slices(f, s.spp, 6)
+        q.put((rank, int(s.sample_offset), int(s.spp), int(s.seed), f.numpy().tolist() if rank == 0 else None))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 4])
+def test_strong_split_assembles_the_one_rank_frame(world):
+    import numpy as np
+    import magik_b200 as M
+    from oracle import oracle_py as O
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_strong_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = sorted(q.get(timeout=300) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    # contiguous, disjoint slices of the 6 samples, one seed
+    offs = [(o[1], o[2]) for o in out]
+    assert sum(c for _, c in offs) == 6 and all(offs[i][0] + offs[i][1] == offs[i + 1][0] for i in range(world - 1))
+    assert len({o[3] for o in out}) == 1
+    s = M.scene_defaults(width=24, height=16, spp=6)
+    s.seed = out[0][3]
+    full, _ = O.render_pixels(s, M.star_catalog(0x57A25, 20000), M.xyz_weights(s.n_bins), 0, 24 * 16, nthreads=2)
+    got = np.array(out[0][4]).reshape(-1, 3)
+    assert np.abs(full).sum() > 0
+    np.testing.assert_allclose(got, full, rtol=1e-6, atol=1e-6 * np.abs(full).max())
+
+
+def test_sample_slice_bounds():
+    from magik_b200 import dist as D
+    assert [D.sample_slice(16, r, 8) for r in range(8)] == [(2 * r, 2) for r in range(8)]
+    assert [D.sample_slice(5, r, 2) for r in range(2)] == [(0, 3), (3, 2)]
+    with pytest.raises(ValueError):
+        D.sample_slice(2, 0, 4)
