@@ -50,6 +50,13 @@ __device__ __forceinline__ void mma_bf16(float* d, const uint32_t* a, uint32_t b
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
+// Element offset (in BF16 elements) of (row, col) inside a 128-row tile of
+// 16 columns in the tensor-core operand layout: 8-row groups 256 bytes apart,
+// 8-column groups 128 bytes apart.
+__host__ __device__ constexpr uint32_t tile16(uint32_t row, uint32_t col) {
+    return ((row >> 3) * 256u + (col >> 3) * 128u + (row & 7u) * 16u + (col & 7u) * 2u) / 2u;
+}
+
 __device__ __forceinline__ float silu(float z) { return z / (1.0f + expf(-z)); }
 __device__ __forceinline__ float silu_grad(float z) {
     float s = 1.0f / (1.0f + expf(-z));
@@ -260,6 +267,9 @@ __device__ __forceinline__ float sigmoidf_(float x) { return 1.0f / (1.0f + expf
 // Outputs: [0] disk logit, [1] escape logit (horizon logit fixed at 0),
 // [2] disk radius (scaled), [3] disk redshift, [4..6] escape direction,
 // [7] confidence logit.  See mlp.h for the label layout and the weights.
+// TILED: dout is written in the tensor-core tile layout (16 columns) of the
+// training kernels instead of row-major.
+template <bool TILED>
 __global__ void __launch_bounds__(256) k_loss(const float* __restrict__ out, const SampleLabel* __restrict__ lab,
                                               int B, LossWeights w, __nv_bfloat16* __restrict__ dout,
                                               float* __restrict__ dout32, float* __restrict__ loss_acc) {
@@ -303,7 +313,9 @@ __global__ void __launch_bounds__(256) k_loss(const float* __restrict__ out, con
         const float inv_b = 1.0f / float(B);
         for (int i = 0; i < MLP_OUT_PAD; ++i) {
             dout32[size_t(b) * MLP_OUT_PAD + i] = d[i] * inv_b;
-            dout[size_t(b) * MLP_OUT_PAD + i] = __float2bfloat16_rn(d[i] * inv_b);
+            const size_t o = TILED ? size_t(b >> 7) * 2048u + tile16(uint32_t(b) & 127u, uint32_t(i))
+                                   : size_t(b) * MLP_OUT_PAD + i;
+            dout[o] = __float2bfloat16_rn(d[i] * inv_b);
         }
     }
     // block reduction of the loss
@@ -319,7 +331,15 @@ __global__ void __launch_bounds__(256) k_loss(const float* __restrict__ out, con
 
 cudaError_t launch_loss(const float* out, const SampleLabel* lab, int B, LossWeights w, __nv_bfloat16* dout,
                         float* dout32, float* loss_acc, cudaStream_t st) {
-    k_loss<<<(B + 255) / 256, 256, 0, st>>>(out, lab, B, w, dout, dout32, loss_acc);
+    k_loss<false><<<(B + 255) / 256, 256, 0, st>>>(out, lab, B, w, dout, dout32, loss_acc);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_loss_tiled(const float* out, const SampleLabel* lab, int B, LossWeights w, void* dout_tiles,
+                              float* dout32, float* loss_acc, cudaStream_t st) {
+    if (B % 128) return cudaErrorInvalidValue;
+    k_loss<true><<<(B + 255) / 256, 256, 0, st>>>(out, lab, B, w, static_cast<__nv_bfloat16*>(dout_tiles), dout32,
+                                                 loss_acc);
     return cudaGetLastError();
 }
 
@@ -372,6 +392,35 @@ __global__ void k_gather(const float* __restrict__ feat, const SampleLabel* __re
 cudaError_t launch_gather(const float* feat, const SampleLabel* lab, const uint32_t* perm, int b0, int B,
                           __nv_bfloat16* x0, SampleLabel* blab, cudaStream_t st) {
     k_gather<<<(B + 255) / 256, 256, 0, st>>>(feat, lab, perm, b0, B, x0, blab);
+    return cudaGetLastError();
+}
+
+// The same batch with X0 in the tile layout of the training kernels: row i's
+// 16 BF16 values as two 16-byte groups of tile i / 128.
+__global__ void k_gather_tiled(const float* __restrict__ feat, const SampleLabel* __restrict__ lab,
+                               const uint32_t* __restrict__ perm, int b0, int B, __nv_bfloat16* __restrict__ x0,
+                               SampleLabel* __restrict__ blab) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= B) return;
+    const uint32_t s = perm[b0 + i];
+    __nv_bfloat162 v[MLP_IN_PAD / 2];
+#pragma unroll
+    for (int k = 0; k < MLP_IN_PAD / 2; ++k) {
+        const float a = 2 * k < MLP_IN ? feat[size_t(s) * MLP_IN + 2 * k] : 0.f;
+        const float b = 2 * k + 1 < MLP_IN ? feat[size_t(s) * MLP_IN + 2 * k + 1] : 0.f;
+        v[k] = __floats2bfloat162_rn(a, b);
+    }
+    __nv_bfloat16* t = x0 + size_t(i >> 7) * 2048u;
+    *reinterpret_cast<uint4*>(t + tile16(uint32_t(i) & 127u, 0)) = *reinterpret_cast<const uint4*>(&v[0]);
+    *reinterpret_cast<uint4*>(t + tile16(uint32_t(i) & 127u, 8)) = *reinterpret_cast<const uint4*>(&v[4]);
+    blab[i] = lab[s];
+}
+
+cudaError_t launch_gather_tiled(const float* feat, const SampleLabel* lab, const uint32_t* perm, int b0, int B,
+                                void* x0_tiles, SampleLabel* blab, cudaStream_t st) {
+    if (B % 128) return cudaErrorInvalidValue;
+    k_gather_tiled<<<(B + 255) / 256, 256, 0, st>>>(feat, lab, perm, b0, B, static_cast<__nv_bfloat16*>(x0_tiles),
+                                                     blab);
     return cudaGetLastError();
 }
 

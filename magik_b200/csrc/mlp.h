@@ -67,10 +67,42 @@ cudaError_t launch_gather(const float* feat, const SampleLabel* lab, const uint3
                           __nv_bfloat16* x0, SampleLabel* blab, cudaStream_t st);
 cudaError_t launch_features_bf16(const float* feat, uint32_t n, uint32_t rows, __nv_bfloat16* x0, cudaStream_t st);
 
+// The weight image of the tensor-core kernels (mlp_tc.cu, mlp_train_tc.cu):
+// 14 chunks, each stored K-major in the operand layout of the tensor cores.
+// Chunk 0 is W1 (256 x 16, 8-row stride 256 B), chunks 1-12 are W2..W4 in
+// slices of 64 input columns (256 x 64, 8-row stride 1024 B), chunk 13 is W5
+// (16 x 256, 8-row stride 4096 B).  W1..W4 are stored halved (exact in BF16).
+constexpr int MLP_IMAGE_CHUNKS = 14;
+__host__ __device__ constexpr uint32_t mlp_chunk_offset(int c) {
+    return c == 0 ? 0u : (c <= 12 ? 8192u + uint32_t(c - 1) * 32768u : 8192u + 12u * 32768u);
+}
+__host__ __device__ constexpr uint32_t mlp_chunk_bytes(int c) { return (c == 0 || c == 13) ? 8192u : 32768u; }
+constexpr uint32_t MLP_IMAGE_BYTES = 8192u + 12u * 32768u + 8192u;
+
 // Fused tensor-core inference (mlp_tc.cu).
 size_t mlp_image_bytes();
 cudaError_t launch_weight_image(const __nv_bfloat16* wb, void* img, cudaStream_t st);
 cudaError_t launch_mlp_infer_tc(const float* feat, uint32_t n, const void* img, const float* params, float* out,
                                 uint32_t* status, int sm_count, cudaStream_t st);
+
+// Tensor-core training (mlp_train_tc.cu) on tiled activations: 128-row tiles
+// in the operand layout (element (row, col) of tile t at
+// t * 256 * C + kmaj(row % 128, col, 16 C) bytes for C columns).
+cudaError_t launch_mlp_fwd_stash_tc(const void* img, const float* params, const void* x0_tiles, void* const* z,
+                                    void* const* h, float* out, uint32_t n_tiles, uint32_t* status, int sm_count,
+                                    cudaStream_t st);
+cudaError_t launch_mlp_bwd_dx_tc(const void* img, const void* dout_tiles, void* const* z, void* const* dz,
+                                 uint32_t n_tiles, uint32_t* status, int sm_count, cudaStream_t st);
+void mlp_dw_jobs(uint32_t n_tiles, int sm_count, uint32_t* heavy, uint32_t* light);
+size_t mlp_dw_partial_floats(uint32_t jobs);
+cudaError_t launch_mlp_dw_tc(void* const* dz, void* const* h, const void* x0_tiles, const void* dout_tiles,
+                             float* part, float* grad, uint32_t n_tiles, uint32_t jobs_heavy, uint32_t jobs_light,
+                             uint32_t* status, cudaStream_t st);
+// Batch assembly into tiled X0 (16 columns) and the loss writing the BF16
+// output gradient as tiles (mlp.cu).
+cudaError_t launch_gather_tiled(const float* feat, const SampleLabel* lab, const uint32_t* perm, int b0, int B,
+                                void* x0_tiles, SampleLabel* blab, cudaStream_t st);
+cudaError_t launch_loss_tiled(const float* out, const SampleLabel* lab, int B, LossWeights w, void* dout_tiles,
+                              float* dout32, float* loss_acc, cudaStream_t st);
 
 }  // namespace mgk

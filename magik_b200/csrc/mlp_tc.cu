@@ -39,9 +39,12 @@
 #include <cuda_runtime.h>
 
 #include "mlp.h"
+#include "tc_sm100.cuh"
 
 namespace mgk {
 namespace {
+
+using namespace tc;
 
 constexpr int TM = 128;                   // rows per tile
 // A bulk copy costs about the same time whatever its size up to 32 KB, so the
@@ -50,12 +53,10 @@ constexpr int N_SLOT = 2;
 constexpr uint32_t SLOT_BYTES = 32768;
 constexpr uint32_t A_BYTES = TM * MLP_HID * 2;  // 64 KB activation tile
 constexpr uint32_t A_SBO = 4096;                // 8-row group stride of the activation tile
-constexpr int N_CHUNKS = 14;                    // W1, W2 x4, W3 x4, W4 x4, W5
+constexpr int N_CHUNKS = MLP_IMAGE_CHUNKS;      // W1, W2 x4, W3 x4, W4 x4, W5
 constexpr int EPI_WARPS = 16;                   // 8 per buffer
 constexpr int THREADS = 32 * (2 + EPI_WARPS);
 constexpr uint32_t TMEM_COLS = 512;             // two 256-column accumulators
-constexpr uint32_t WAIT_LIMIT = 1u << 22;      // polls without a suspend hint
-constexpr uint32_t SLEEP_LIMIT = 4096;         // suspended waits of at most 1 ms each
 
 // Shared-memory map (dynamic, offsets from a 128-byte aligned base).
 constexpr uint32_t OFF_A = 0;                                // two activation tiles
@@ -68,140 +69,11 @@ static_assert(2 * N_SLOT + 5 <= 16, "barrier area");
 constexpr uint32_t SMEM_BYTES = OFF_MISC + 16 + 128;         // + alignment slack
 static_assert(SMEM_BYTES <= 232448, "shared memory");
 
-// Chunk c of the weight image: byte offset and size.  Chunk 0 is W1 (256 x 16,
-// 8-row stride 256 B), chunks 1-12 are W2..W4 in slices of 64 input columns
-// (256 x 64, stride 1024 B), chunk 13 is W5 (16 x 256, stride 4096 B).
-__host__ __device__ constexpr uint32_t chunk_offset(int c) {
-    return c == 0 ? 0u : (c <= 12 ? 8192u + uint32_t(c - 1) * 32768u : 8192u + 12u * 32768u);
-}
-__host__ __device__ constexpr uint32_t chunk_bytes(int c) { return (c == 0 || c == 13) ? 8192u : 32768u; }
-constexpr uint32_t IMAGE_BYTES = 8192u + 12u * 32768u + 8192u;
+// Chunk c of the weight image (mlp.h): byte offset and size.
+__host__ __device__ constexpr uint32_t chunk_offset(int c) { return mlp_chunk_offset(c); }
+__host__ __device__ constexpr uint32_t chunk_bytes(int c) { return mlp_chunk_bytes(c); }
+constexpr uint32_t IMAGE_BYTES = MLP_IMAGE_BYTES;
 
-__device__ __forceinline__ uint32_t smem_addr(const void* p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-// try_wait with a suspend-time hint: the thread sleeps until the phase
-// completes or about `ns` nanoseconds pass, instead of spinning.
-__device__ __forceinline__ bool mbar_try_sleep(uint32_t bar, uint32_t parity, uint32_t ns) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity), "r"(ns)
-        : "memory");
-    return ok != 0;
-}
-// Bounded wait for the completion of the phase with the given parity.  Gives
-// up (returns false) after SLEEP_LIMIT suspended tries (a few seconds) or
-// once another role has aborted.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile uint32_t* abort_flag) {
-    for (uint32_t it = 0; it < SLEEP_LIMIT; ++it) {
-        if (mbar_try_sleep(bar, parity, 1000000u)) return true;
-        if (*abort_flag) return false;
-    }
-    *abort_flag = 1u;
-    return false;
-}
-
-__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-                 "l"(src), "r"(bytes), "r"(bar)
-                 : "memory");
-}
-
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
-    return uint64_t((addr >> 4) & 0x3FFFu) | (uint64_t((lbo >> 4) & 0x3FFFu) << 16) |
-           (uint64_t((sbo >> 4) & 0x3FFFu) << 32) | (uint64_t(1) << 46);
-}
-// kind::f16 instruction descriptor: FP32 accumulator, BF16 A and B, both K-major.
-__host__ __device__ constexpr uint32_t idesc_bf16(uint32_t m, uint32_t n) {
-    return (1u << 4) | (1u << 7) | (1u << 10) | ((n >> 3) << 17) | ((m >> 4) << 24);
-}
-
-__device__ __forceinline__ void mma_bf16_ss(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-        "l"(a), "l"(b), "r"(idesc), "r"(acc)
-        : "memory");
-}
-__device__ __forceinline__ void mma_commit(uint32_t bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
-                 : "memory");
-}
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
-          "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
-          "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
-        : "r"(taddr));
-}
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-        : "r"(taddr));
-}
-__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
-// Waits for the outstanding TMEM loads; the registers are in-out operands so
-// that no use of them can be scheduled before the wait.
-__device__ __forceinline__ void tmem_wait_ld(uint32_t (&v)[32]) {
-    asm volatile("tcgen05.wait::ld.sync.aligned;"
-                 : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3]), "+r"(v[4]), "+r"(v[5]), "+r"(v[6]), "+r"(v[7]),
-                   "+r"(v[8]), "+r"(v[9]), "+r"(v[10]), "+r"(v[11]), "+r"(v[12]), "+r"(v[13]), "+r"(v[14]),
-                   "+r"(v[15]), "+r"(v[16]), "+r"(v[17]), "+r"(v[18]), "+r"(v[19]), "+r"(v[20]), "+r"(v[21]),
-                   "+r"(v[22]), "+r"(v[23]), "+r"(v[24]), "+r"(v[25]), "+r"(v[26]), "+r"(v[27]), "+r"(v[28]),
-                   "+r"(v[29]), "+r"(v[30]), "+r"(v[31])
-                 :
-                 : "memory");
-}
-__device__ __forceinline__ void tmem_wait_ld(uint32_t (&v)[16]) {
-    asm volatile("tcgen05.wait::ld.sync.aligned;"
-                 : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3]), "+r"(v[4]), "+r"(v[5]), "+r"(v[6]), "+r"(v[7]),
-                   "+r"(v[8]), "+r"(v[9]), "+r"(v[10]), "+r"(v[11]), "+r"(v[12]), "+r"(v[13]), "+r"(v[14]),
-                   "+r"(v[15])
-                 :
-                 : "memory");
-}
-
-__device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
-    __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
-    return *reinterpret_cast<uint32_t*>(&h);
-}
 // silu of a pair with u = z / 2:  z sigmoid(z) = u (1 + tanh u), in BF16x2.
 __device__ __forceinline__ uint32_t silu_half_pair(float u0, float u1) {
     const uint32_t u = pack_bf16(u0, u1);
@@ -227,10 +99,6 @@ __device__ __forceinline__ void epilogue_block(const uint32_t (&v)[32], const fl
     }
 }
 
-// Byte offset of element (row, k) in a K-major tile with 8-row stride sbo.
-__host__ __device__ constexpr uint32_t kmaj(uint32_t row, uint32_t k, uint32_t sbo) {
-    return (row >> 3) * sbo + (k >> 3) * 128u + (row & 7u) * 16u + (k & 7u) * 2u;
-}
 
 }  // namespace
 

@@ -3,6 +3,7 @@
 // kernels), inference and the routed render.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <new>
 #include <cstring>
 #include <vector>
@@ -55,6 +56,13 @@ struct mgk_surrogate {
     uint64_t step = 0;
     // training buffers for batch `tb`
     int tb = 0;
+    // the tensor-core training path (mlp_train_tc.cu): tiled activations and
+    // the weight-gradient partials; off (the mma.sync GEMMs of mlp.cu) when
+    // MGK_SURROGATE_TRAIN=mma was set at creation
+    bool train_tc = true;
+    void *tx0 = nullptr, *tZ[4] = {}, *tH[4] = {}, *tdZ[4] = {}, *tdout = nullptr;
+    float* dw_part = nullptr;
+    uint32_t dw_heavy = 0, dw_light = 0;
     __nv_bfloat16 *x0 = nullptr, *Z[4] = {}, *H[4] = {}, *dza = nullptr, *dzb = nullptr, *dout = nullptr;
     float *out = nullptr, *dout32 = nullptr, *loss = nullptr;
     mgk_sample_label* blab = nullptr;
@@ -110,6 +118,18 @@ mgk_result ensure_train_buffers(mgk_surrogate* s, int B) {
     TRY(dalloc(s, &s->dout32, size_t(B) * MLP_OUT_PAD * 4));
     TRY(dalloc(s, &s->loss, 64));
     TRY(dalloc(s, &s->blab, size_t(B) * sizeof(mgk_sample_label)));
+    if (s->train_tc) {
+        if (B % 128) return MGK_ERROR_INVALID_ARGUMENT;
+        TRY(dalloc(s, &s->tx0, size_t(B) * MLP_IN_PAD * 2));
+        for (int l = 0; l < 4; ++l) {
+            TRY(dalloc(s, &s->tZ[l], act));
+            TRY(dalloc(s, &s->tH[l], act));
+            TRY(dalloc(s, &s->tdZ[l], act));
+        }
+        TRY(dalloc(s, &s->tdout, size_t(B) * MLP_OUT_PAD * 2));
+        mlp_dw_jobs(uint32_t(B) / 128u, s->sm_count, &s->dw_heavy, &s->dw_light);
+        TRY(dalloc(s, &s->dw_part, mlp_dw_partial_floats(3 * s->dw_heavy + 2 * s->dw_light) * sizeof(float)));
+    }
     s->tb = B;
     return MGK_SUCCESS;
 }
@@ -168,6 +188,47 @@ cudaError_t forward(mgk_surrogate* s, const __nv_bfloat16* x0, int B, __nv_bfloa
     g.bias = s->p + L.b[4];
     g.out = out;
     return launch_gemm(GEMM_FWD_OUT, g, st);
+}
+
+// One gradient of the batch rows perm[b0 .. b0 + B) on the tensor-core
+// path: gather, forward with stash, loss, input gradients, weight gradients
+// (all of grad is written); the batch mean loss is added to *loss_acc.
+cudaError_t gradient_tc(mgk_surrogate* s, const float* feat, const mgk_sample_label* lab, int b0, int B,
+                        const LossWeights& w, float* loss_acc, cudaStream_t st) {
+    const Layout& L = s->L;
+    const uint32_t tiles = uint32_t(B) / 128u;
+    cudaError_t e = launch_gather_tiled(feat, lab, s->perm, b0, B, s->tx0, s->blab, st);
+    if (e == cudaSuccess && !s->img_valid) {
+        e = launch_weight_image(s->wb, s->img, st);
+        s->img_valid = e == cudaSuccess;
+    }
+    if (e == cudaSuccess)
+        e = launch_mlp_fwd_stash_tc(s->img, s->p, s->tx0, s->tZ, s->tH, s->out, tiles, s->status, s->sm_count, st);
+    if (e == cudaSuccess) e = launch_loss_tiled(s->out, s->blab, B, w, s->tdout, s->dout32, loss_acc, st);
+    if (e == cudaSuccess) e = launch_mlp_bwd_dx_tc(s->img, s->tdout, s->tZ, s->tdZ, tiles, s->status, s->sm_count, st);
+    if (e == cudaSuccess)
+        e = launch_mlp_dw_tc(s->tdZ, s->tH, s->tx0, s->tdout, s->dw_part, s->grad, tiles, s->dw_heavy, s->dw_light,
+                             s->status, st);
+    // the output bias gradient from the FP32 output gradient
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->grad + L.b[4], 0, MLP_OUT_PAD * sizeof(float), st);
+    if (e == cudaSuccess) e = launch_colsum_f32(s->dout32, B, MLP_OUT_PAD, s->grad + L.b[4], st);
+    return e;
+}
+
+// One gradient on the mma.sync path (mlp.cu): gather, forward, backward.
+cudaError_t backward(mgk_surrogate* s, int B, const LossWeights& w, float* loss_acc, cudaStream_t st);
+cudaError_t gradient_mma(mgk_surrogate* s, const float* feat, const mgk_sample_label* lab, int b0, int B,
+                         const LossWeights& w, float* loss_acc, cudaStream_t st) {
+    cudaError_t e = launch_gather(feat, lab, s->perm, b0, B, s->x0, s->blab, st);
+    if (e == cudaSuccess) e = forward(s, s->x0, B, s->Z, s->H, s->out, st);
+    if (e == cudaSuccess) e = backward(s, B, w, loss_acc, st);
+    return e;
+}
+
+cudaError_t gradient(mgk_surrogate* s, const float* feat, const mgk_sample_label* lab, int b0, int B,
+                     const LossWeights& w, float* loss_acc, cudaStream_t st) {
+    return s->train_tc ? gradient_tc(s, feat, lab, b0, B, w, loss_acc, st)
+                       : gradient_mma(s, feat, lab, b0, B, w, loss_acc, st);
 }
 
 // Loss, backward pass and gradient accumulation of the batch in the training
@@ -351,6 +412,7 @@ MGK_API mgk_result mgk_surrogate_create(mgk_context* ctx, uint64_t seed, mgk_sur
     s->ctx = ctx;
     s->device = context_device(ctx);
     s->L = param_layout();
+    if (const char* path = std::getenv("MGK_SURROGATE_TRAIN")) s->train_tc = std::strcmp(path, "mma") != 0;
     cudaSetDevice(s->device);
     const size_t n = s->L.total;
     if (dalloc(s, &s->p, n * 4) != cudaSuccess || dalloc(s, &s->grad, n * 4) != cudaSuccess ||
@@ -419,10 +481,8 @@ MGK_API mgk_result mgk_surrogate_gradient(mgk_surrogate* s, const mgk_train_conf
     for (uint32_t i = 0; i < n; ++i) perm[i] = i;
     s->order_n = 0;
     TRY(cudaMemcpyAsync(s->perm, perm.data(), size_t(n) * 4, cudaMemcpyHostToDevice, st));
-    TRY(launch_gather(d_feat, d_lab, s->perm, 0, int(n), s->x0, s->blab, st));
     TRY(cudaMemsetAsync(s->loss, 0, 4, st));
-    TRY(forward(s, s->x0, int(n), s->Z, s->H, s->out, st));
-    TRY(backward(s, int(n), loss_weights(*cfg), s->loss, st));
+    TRY(gradient(s, d_feat, d_lab, 0, int(n), loss_weights(*cfg), s->loss, st));
     TRY(cudaMemcpyAsync(h_grad, s->grad, s->L.total * 4, cudaMemcpyDeviceToHost, st));
     float loss = 0.f;
     TRY(cudaMemcpyAsync(&loss, s->loss, 4, cudaMemcpyDeviceToHost, st));
@@ -453,9 +513,7 @@ MGK_API mgk_result mgk_surrogate_train(mgk_surrogate* s, const mgk_train_config*
         TRY(cudaMemcpyAsync(s->perm, perm.data(), size_t(n) * 4, cudaMemcpyHostToDevice, st));
         TRY(cudaMemsetAsync(s->loss, 0, 4, st));
         for (uint32_t b = 0; b < nb; ++b) {
-            TRY(launch_gather(d_feat, d_lab, s->perm, int(b * B), int(B), s->x0, s->blab, st));
-            TRY(forward(s, s->x0, int(B), s->Z, s->H, s->out, st));
-            TRY(backward(s, int(B), w, s->loss, st));
+            TRY(gradient(s, d_feat, d_lab, int(b * B), int(B), w, s->loss, st));
             ++s->step;
             const AdamStep a = adam_constants(*cfg, double(ep * nb + b) / double(cfg->epochs * nb), s->step, 1.0f);
             TRY(launch_adam(s->p, s->grad, s->m, s->v, s->wb, int(s->L.total), a, st));
@@ -494,9 +552,7 @@ MGK_API mgk_result mgk_surrogate_gradient_step(mgk_surrogate* s, const mgk_train
     if (rc != MGK_SUCCESS) return rc;
     if (s->tb != int(n)) return MGK_ERROR_INVALID_ARGUMENT;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    TRY(launch_gather(d_feat, d_lab, s->perm, int(first), int(n), s->x0, s->blab, st));
-    TRY(forward(s, s->x0, int(n), s->Z, s->H, s->out, st));
-    TRY(backward(s, int(n), loss_weights(*cfg), d_loss_sum, st));
+    TRY(gradient(s, d_feat, d_lab, int(first), int(n), loss_weights(*cfg), d_loss_sum, st));
     TRY(cudaMemcpyAsync(d_grad, s->grad, s->L.total * 4, cudaMemcpyDeviceToDevice, st));
     return MGK_SUCCESS;
 }

@@ -141,6 +141,37 @@ def test_gradient_matches_oracle(ctx, n):
     del torch
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [1024, 65536])
+def test_tensor_core_gradient_equals_mma_path(ctx, n):
+    """The tcgen05 training kernels (mlp_train_tc.cu: forward with stash,
+    input gradients, split-K weight gradients) against the mma.sync GEMMs of
+    mlp.cu on the same batch: both round at the same points (BF16 Z, H and
+    dZ, FP32 accumulation); they differ by the SiLU evaluation (tanh.approx
+    against expf) and the summation order."""
+    import os
+    p = O.init_params(23)
+    f, lab = O.random_batch(n, 24)
+    cfg = M.train_defaults(batch=n)
+    grads = {}
+    for path in ("mma", "tc"):
+        os.environ["MGK_SURROGATE_TRAIN"] = path
+        try:
+            net = M.Surrogate(ctx, seed=7)
+        finally:
+            del os.environ["MGK_SURROGATE_TRAIN"]
+        net.set_params(p)
+        grads[path] = net.gradient(cfg, _dev(f), _dev(lab.view(np.int32).reshape(n, 8)))
+        assert net.status() == 0
+        net.close()
+    (l_m, g_m), (l_t, g_t) = grads["mma"], grads["tc"]
+    assert abs(l_t - l_m) <= 1e-3 * abs(l_m)
+    L, _ = O.layout()
+    for li, (wo, bo, n_out, n_in) in enumerate(L):
+        for lo, hi in ((wo, wo + n_out * n_in), (bo, bo + n_out)):
+            assert _rel(g_t[lo:hi], g_m[lo:hi]) <= 2e-2, (li, _rel(g_t[lo:hi], g_m[lo:hi]))
+
+
 def _samples(ctx, scene, n, seed):
     feat, lab = M.make_samples(ctx, scene, seed, n)
     return feat, lab
