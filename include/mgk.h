@@ -541,11 +541,24 @@ MGK_API mgk_result mgk_surrogate_adam_step(mgk_surrogate* net, const mgk_train_c
  * goes through the network; rays whose confidence is below conf_min, or whose
  * impact parameter lies within crit_frac of the critical curve, are
  * integrated with RKF45 (the scene's precision); the rest are shaded from the
- * network's outputs. */
+ * network's outputs.  (mgk_render_surrogate_routed with MGK_ROUTE_CONFIDENCE.) */
 MGK_API mgk_result mgk_render_surrogate(mgk_context* ctx, mgk_surrogate* net, const mgk_scene* s,
                                         const mgk_star* d_stars, uint32_t n_stars, const float* d_xyz_w,
                                         float conf_min, float crit_frac, float* d_film_xyz,
                                         mgk_render_stats* stats, void* stream);
+/* Routing of mgk_render_surrogate_routed (no reference counterpart).
+ *  MGK_ROUTE_CONFIDENCE: as mgk_render_surrogate.
+ *  MGK_ROUTE_CAPTURED: the network takes only the rays it classifies as
+ *    captured by the horizon with class probability >= conf_min (and > 1/2),
+ *    outside the crit_frac band of the critical curve; every other ray is
+ *    integrated.  A captured ray contributes no light, so the network's
+ *    regression outputs never reach the film: only a wrong class does. */
+#define MGK_ROUTE_CONFIDENCE 0u
+#define MGK_ROUTE_CAPTURED 1u
+MGK_API mgk_result mgk_render_surrogate_routed(mgk_context* ctx, mgk_surrogate* net, const mgk_scene* s,
+                                               const mgk_star* d_stars, uint32_t n_stars, const float* d_xyz_w,
+                                               float conf_min, float crit_frac, uint32_t route, float* d_film_xyz,
+                                               mgk_render_stats* stats, void* stream);
 
 /* ------------------------------------ reference-compatible trace API */
 /* Same types and layout as magik.h:583-648; when the reference's magik.h is

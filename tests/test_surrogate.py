@@ -296,3 +296,15 @@ def test_trained_surrogate_render_error_and_fallback(ctx):
     assert att[1] <= att[2] <= att[3] <= att[4] == plain_attempts
     # ... and what that costs in accuracy: the stricter the routing the closer to RKF45
     assert errs[4] <= errs[3] + 1e-6 <= errs[0] + 2e-6
+    # a routing point that gains without moving the film: the network takes
+    # the rays it classifies as captured (no light whatever its regression
+    # outputs); fewer attempts than plain RKF45 at a film error below 1e-3
+    film = torch.zeros_like(ref)
+    st = M.render_surrogate(ctx, net, s, d_stars, film, conf_min=0.99, crit_frac=0.02, route=M.ROUTE_CAPTURED)
+    fb_c = st.fallback_rays / (n_pix * s.spp)
+    rel_c = float((film - ref).abs().mean()) / float(ref.abs().mean())
+    rel_plain = float((plain - ref).abs().mean()) / float(ref.abs().mean())
+    print(f"captured routing: fallback {fb_c:.4f}, attempts {st.attempts} of {plain_attempts}, "
+          f"film error {rel_c:.2e} (plain {rel_plain:.2e})")
+    assert 0.0 < fb_c < 1.0 and st.attempts < plain_attempts
+    assert rel_c <= 1e-3
