@@ -345,12 +345,10 @@ def run_surrogate(args, ctx, s, d_stars, d_w, film_mixed_ms, steps):
     bf16_peak = peaks.get("bf16_tflops")
 
     points = []
-    for name, cm, cf, rt in (("spec routing: conf<0.99 or |b-b_c|/b_c<2% -> RKF45", 0.99, 0.02, M.ROUTE_CONFIDENCE),
-                             ("network only (no fallback)", -1.0, 0.0, M.ROUTE_CONFIDENCE),
-                             ("captured rays only: p(horizon)>=0.99 and |b-b_c|/b_c>=2% -> network", 0.99, 0.02,
-                              M.ROUTE_CAPTURED)):
+    for name, cm, cf in (("spec routing: conf<0.99 or |b-b_c|/b_c<2% -> RKF45", 0.99, 0.02),
+                         ("network only (no fallback)", -1.0, 0.0)):
         ms, st = timed(lambda: M.render_surrogate(ctx, net, s, d_stars, film, conf_min=cm, crit_frac=cf,
-                                                  d_weights=d_w, route=rt))
+                                                  d_weights=d_w))
         err = float((film - ref).abs().mean()) / scale
         err_conv = float((film - ref_conv).abs().mean()) / scale_conv
         points.append({"routing": name, "conf_min": cm, "crit_frac": cf, "value": rays / (ms * 1e-3),
@@ -423,12 +421,10 @@ def run_config5(args, ctx, net, d_stars, d_w):
            "rays": rays, "plain_rkf45": {"value": rays / (plain_ms * 1e-3), "unit": UNIT, "ms_per_frame": plain_ms,
                                          "xyz_rel_err_vs_fp64": plain_err},
            "points": []}
-    for name, cm, cf, rt in (("spec routing: conf<0.99 or |b-b_c|/b_c<2% -> RKF45", 0.99, 0.02, M.ROUTE_CONFIDENCE),
-                             ("network only (no fallback)", -1.0, 0.0, M.ROUTE_CONFIDENCE),
-                             ("captured rays only: p(horizon)>=0.99 and |b-b_c|/b_c>=2% -> network", 0.99, 0.02,
-                              M.ROUTE_CAPTURED)):
+    for name, cm, cf in (("spec routing: conf<0.99 or |b-b_c|/b_c<2% -> RKF45", 0.99, 0.02),
+                         ("network only (no fallback)", -1.0, 0.0)):
         ms, st = once(lambda: M.render_surrogate(ctx, net, s, d_stars, film, conf_min=cm, crit_frac=cf,
-                                                 d_weights=d_w, route=rt))
+                                                 d_weights=d_w))
         err = float((film - ref).abs().mean()) / scale
         out["points"].append({"routing": name, "value": rays / (ms * 1e-3), "unit": UNIT, "ms_per_frame": ms,
                               "fallback_fraction": st.fallback_rays / rays, "xyz_rel_err_vs_fp64": err,

@@ -520,7 +520,8 @@ MGK_API mgk_result mgk_surrogate_train(mgk_surrogate* net, const mgk_train_confi
  * rank, shuffle seed cfg->seed, rows [b B, (b + 1) B) of epoch e and progress
  * (e nb + b) / (epochs nb) this is the loop of mgk_surrogate_train.
  * mgk_surrogate_shuffle: the order of the n samples for one epoch (the
- *   shuffle mgk_surrogate_train uses); synchronous.
+ *   keyed permutation mgk_surrogate_train uses, computed on the device);
+ *   stream-ordered.
  * mgk_surrogate_gradient_step: forward and backward of rows [first, first + n)
  *   of that order (n a multiple of 1024, the same n on every call for one
  *   network); the gradient of the batch mean loss into d_grad
@@ -531,6 +532,12 @@ MGK_API mgk_result mgk_surrogate_train(mgk_surrogate* net, const mgk_train_confi
  *   Asynchronous. */
 MGK_API mgk_result mgk_surrogate_shuffle(mgk_surrogate* net, uint64_t seed, uint32_t epoch, uint32_t n,
                                          void* stream);
+/* The first n entries of the sample order of the latest shuffle (or of the
+ * latest epoch of mgk_surrogate_train), copied to the host; synchronous.
+ * The order is a keyed pseudo-random permutation: a 4-round Feistel network
+ * on the smallest even number of bits covering n, round keys from the
+ * counter-based hash of (seed, epoch), walked back into [0, n). */
+MGK_API mgk_result mgk_surrogate_order(mgk_surrogate* net, uint32_t* h_order, uint32_t n);
 MGK_API mgk_result mgk_surrogate_gradient_step(mgk_surrogate* net, const mgk_train_config* cfg,
                                                const float* d_features, const mgk_sample_label* d_labels,
                                                uint32_t first, uint32_t n, float* d_grad, float* d_loss_sum,
@@ -541,24 +548,11 @@ MGK_API mgk_result mgk_surrogate_adam_step(mgk_surrogate* net, const mgk_train_c
  * goes through the network; rays whose confidence is below conf_min, or whose
  * impact parameter lies within crit_frac of the critical curve, are
  * integrated with RKF45 (the scene's precision); the rest are shaded from the
- * network's outputs.  (mgk_render_surrogate_routed with MGK_ROUTE_CONFIDENCE.) */
+ * network's outputs. */
 MGK_API mgk_result mgk_render_surrogate(mgk_context* ctx, mgk_surrogate* net, const mgk_scene* s,
                                         const mgk_star* d_stars, uint32_t n_stars, const float* d_xyz_w,
                                         float conf_min, float crit_frac, float* d_film_xyz,
                                         mgk_render_stats* stats, void* stream);
-/* Routing of mgk_render_surrogate_routed (no reference counterpart).
- *  MGK_ROUTE_CONFIDENCE: as mgk_render_surrogate.
- *  MGK_ROUTE_CAPTURED: the network takes only the rays it classifies as
- *    captured by the horizon with class probability >= conf_min (and > 1/2),
- *    outside the crit_frac band of the critical curve; every other ray is
- *    integrated.  A captured ray contributes no light, so the network's
- *    regression outputs never reach the film: only a wrong class does. */
-#define MGK_ROUTE_CONFIDENCE 0u
-#define MGK_ROUTE_CAPTURED 1u
-MGK_API mgk_result mgk_render_surrogate_routed(mgk_context* ctx, mgk_surrogate* net, const mgk_scene* s,
-                                               const mgk_star* d_stars, uint32_t n_stars, const float* d_xyz_w,
-                                               float conf_min, float crit_frac, uint32_t route, float* d_film_xyz,
-                                               mgk_render_stats* stats, void* stream);
 
 /* ------------------------------------ reference-compatible trace API */
 /* Same types and layout as magik.h:583-648; when the reference's magik.h is

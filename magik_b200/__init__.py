@@ -35,8 +35,8 @@ EXPORTS = [
     "mgk_check_rounding", "mgk_cmf_inverse_cdf", "mgk_xyz_weights_analytic", "mgk_cmf_inverse_cdf_analytic", "mgk_display_defaults", "mgk_display_prepare", "mgk_display",
     "mgk_trace_rays_static", "mgk_train_defaults", "mgk_surrogate_param_count", "mgk_surrogate_create",
     "mgk_surrogate_destroy", "mgk_surrogate_get_params", "mgk_surrogate_set_params", "mgk_make_samples",
-    "mgk_surrogate_forward", "mgk_surrogate_forward_tiled", "mgk_surrogate_status", "mgk_surrogate_gradient", "mgk_surrogate_train", "mgk_render_surrogate", "mgk_render_surrogate_routed",
-    "mgk_surrogate_shuffle", "mgk_surrogate_gradient_step", "mgk_surrogate_adam_step",
+    "mgk_surrogate_forward", "mgk_surrogate_forward_tiled", "mgk_surrogate_status", "mgk_surrogate_gradient", "mgk_surrogate_train", "mgk_render_surrogate",
+    "mgk_surrogate_shuffle", "mgk_surrogate_order", "mgk_surrogate_gradient_step", "mgk_surrogate_adam_step",
 ]
 
 
@@ -102,13 +102,12 @@ def lib():
                                              P(C.c_float)]
         L.mgk_surrogate_train.argtypes = [vp, P(abi.TrainConfig), vp, vp, C.c_uint32, P(C.c_float), vp]
         L.mgk_surrogate_shuffle.argtypes = [vp, C.c_uint64, C.c_uint32, C.c_uint32, vp]
+        L.mgk_surrogate_order.argtypes = [vp, P(C.c_uint32), C.c_uint32]
         L.mgk_surrogate_gradient_step.argtypes = [vp, P(abi.TrainConfig), vp, vp, C.c_uint32, C.c_uint32, vp, vp,
                                                   vp]
         L.mgk_surrogate_adam_step.argtypes = [vp, P(abi.TrainConfig), vp, C.c_float, C.c_double, vp]
         L.mgk_render_surrogate.argtypes = [vp, vp, P(Scene), vp, C.c_uint32, vp, C.c_float, C.c_float, vp,
                                            P(RenderStats), vp]
-        L.mgk_render_surrogate_routed.argtypes = [vp, vp, P(Scene), vp, C.c_uint32, vp, C.c_float, C.c_float, C.c_uint32,
-                                                  vp, P(RenderStats), vp]
         for name in EXPORTS:
             fn = getattr(L, name)
             if fn.restype is C.c_int:  # ctypes default
@@ -439,6 +438,13 @@ class Surrogate:
         """The sample-set order of one epoch (mgk_surrogate_shuffle)."""
         _check(lib().mgk_surrogate_shuffle(self.handle, seed, epoch, n, _stream_ptr(stream)), "mgk_surrogate_shuffle")
 
+    def order(self, n):
+        """The first n entries of the latest sample order (mgk_surrogate_order)."""
+        out = np.zeros(n, np.uint32)
+        _check(lib().mgk_surrogate_order(self.handle, out.ctypes.data_as(C.POINTER(C.c_uint32)), n),
+               "mgk_surrogate_order")
+        return out
+
     def gradient_step(self, cfg, d_feat, d_lab, first, n, d_grad, d_loss_sum, stream=None):
         """Rows [first, first + n) of the order: gradient into d_grad, batch mean loss added to d_loss_sum."""
         _check(lib().mgk_surrogate_gradient_step(self.handle, C.byref(cfg), d_feat.data_ptr(), d_lab.data_ptr(),
@@ -463,20 +469,16 @@ def make_samples(ctx, base, seed, n, n_spin_buckets=0, stream=None):
     return feat[:n], lab[:n]
 
 
-ROUTE_CONFIDENCE, ROUTE_CAPTURED = 0, 1
-
-
 def render_surrogate(ctx, net, scene, d_stars, d_film_xyz, conf_min=0.99, crit_frac=0.02, d_weights=None,
-                     stream=None, route=ROUTE_CONFIDENCE):
-    """mgk_render_surrogate_routed (ROUTE_CONFIDENCE: mgk_render_surrogate);
-    returns the RenderStats."""
+                     stream=None):
+    """mgk_render_surrogate; returns the RenderStats."""
     n_stars = 0 if d_stars is None else d_stars.numel() * d_stars.element_size() // 32
     st = RenderStats()
-    rc = lib().mgk_render_surrogate_routed(ctx.handle, net.handle, C.byref(scene),
-                                           None if d_stars is None else d_stars.data_ptr(), n_stars,
-                                           None if d_weights is None else d_weights.data_ptr(), conf_min, crit_frac,
-                                           int(route), d_film_xyz.data_ptr(), C.byref(st), _stream_ptr(stream))
-    _check(rc, "mgk_render_surrogate_routed", ctx.handle)
+    rc = lib().mgk_render_surrogate(ctx.handle, net.handle, C.byref(scene),
+                                    None if d_stars is None else d_stars.data_ptr(), n_stars,
+                                    None if d_weights is None else d_weights.data_ptr(), conf_min, crit_frac,
+                                    d_film_xyz.data_ptr(), C.byref(st), _stream_ptr(stream))
+    _check(rc, "mgk_render_surrogate", ctx.handle)
     return st
 
 

@@ -1166,16 +1166,7 @@ MGK_API mgk_result mgk_make_samples(mgk_context* ctx, const mgk_scene* base, uin
 MGK_API mgk_result mgk_render_surrogate(mgk_context* ctx, mgk_surrogate* net, const mgk_scene* sp,
                                         const mgk_star* d_stars, uint32_t n_stars, const float* d_w, float conf_min,
                                         float crit_frac, float* film, mgk_render_stats* stats, void* stream) {
-    return mgk_render_surrogate_routed(ctx, net, sp, d_stars, n_stars, d_w, conf_min, crit_frac, MGK_ROUTE_CONFIDENCE,
-                                       film, stats, stream);
-}
-
-MGK_API mgk_result mgk_render_surrogate_routed(mgk_context* ctx, mgk_surrogate* net, const mgk_scene* sp,
-                                               const mgk_star* d_stars, uint32_t n_stars, const float* d_w,
-                                               float conf_min, float crit_frac, uint32_t route, float* film,
-                                               mgk_render_stats* stats, void* stream) {
     if (!ctx || !net || !sp || !film) return MGK_ERROR_INVALID_POINTER;
-    if (route > MGK_ROUTE_CAPTURED) return MGK_ERROR_INVALID_ARGUMENT;
     const mgk_scene& s = *sp;
     mgk_result rc = validate(&s);
     if (rc != MGK_SUCCESS) return rc;
@@ -1246,7 +1237,7 @@ MGK_API mgk_result mgk_render_surrogate_routed(mgk_context* ctx, mgk_surrogate* 
             const uint32_t k = std::min(kRouteBatch, m - r0);
             MGK_CUDA(ctx, launch_camera_features(s, table, b + r0, k, B, feat, st));
             MGK_CUDA(ctx, surrogate_infer(net, feat, k, out, st));
-            MGK_CUDA(ctx, launch_route(s, table, r0, k, m, out, feat, conf_min, crit_frac, route, B, ids, fq, st));
+            MGK_CUDA(ctx, launch_route(s, table, r0, k, m, out, feat, conf_min, crit_frac, B, ids, fq, st));
         }
         MGK_CUDA(ctx, cudaEventRecord(ev[1], st));
         Counters hc;

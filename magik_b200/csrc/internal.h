@@ -99,8 +99,8 @@ cudaError_t launch_labels(const mgk_ray_result* res, const float* feat, uint32_t
 cudaError_t launch_camera_features(const mgk_scene& s, const void* dev_scene, uint64_t first_ray, uint32_t n,
                                    const ChunkBuffers& b, float* feat, cudaStream_t stream);
 cudaError_t launch_route(const mgk_scene& s, const void* dev_scene, uint32_t base, uint32_t n, uint32_t cap,
-                         const float* out, const float* feat, float conf_min, float crit_frac, uint32_t route,
-                         const ChunkBuffers& b, uint32_t* fallback_ids, void* fallback_q, cudaStream_t stream);
+                         const float* out, const float* feat, float conf_min, float crit_frac, const ChunkBuffers& b,
+                         uint32_t* fallback_ids, void* fallback_q, cudaStream_t stream);
 // Inference of the surrogate network (surrogate.cu): 16 floats per row of out.
 cudaError_t surrogate_infer(mgk_surrogate* net, const float* feat, uint32_t n, float* out, cudaStream_t stream);
 uint32_t surrogate_status(mgk_surrogate* net);

@@ -1231,7 +1231,7 @@ template <int MODE>
 __global__ void __launch_bounds__(256) k_route(const DevScene<typename ModeT<MODE>::T> P, uint32_t base_ray, uint32_t n,
                                                uint32_t cap, const float* __restrict__ out,
                                                const float* __restrict__ feat, float conf_min,
-                                               float crit_frac, uint32_t route, const void* __restrict__ qx,
+                                               float crit_frac, const void* __restrict__ qx,
                                                const void* __restrict__ qp, const void* __restrict__ qc, void* fqx,
                                                void* fqp, void* fqc, uint32_t* fallback_ids,
                                                HitEntry<typename ModeT<MODE>::T>* hits, Counters* cnt) {
@@ -1252,17 +1252,7 @@ __global__ void __launch_bounds__(256) k_route(const DevScene<typename ModeT<MOD
             const float conf = 1.0f / (1.0f + expf(-o[7]));
             const double dc = critical_distance(double(a4[0]), double(a4[1]), double(a4[2]), double(b4[0]),
                                                 double(b4[1]), double(b4[2]), double(b4[3]), P.spin_d);
-            if (route == MGK_ROUTE_CONFIDENCE) {
-                fall = conf < conf_min || dc < double(crit_frac);
-            } else {
-                // MGK_ROUTE_CAPTURED: the network takes only rays it classifies
-                // as captured with probability >= conf_min (their emission is
-                // zero whatever the regression outputs)
-                const float mx = fmaxf(fmaxf(o[0], o[1]), 0.f);
-                const float e0 = expf(o[0] - mx), e1 = expf(o[1] - mx), e2 = expf(-mx);
-                const float p_h = e2 / (e0 + e1 + e2);
-                fall = !(p_h >= conf_min && p_h > 0.5f) || dc < double(crit_frac);
-            }
+            fall = conf < conf_min || dc < double(crit_frac);
             if (!fall) {
                 const int cls = (o[0] >= o[1] && o[0] >= 0.f) ? 0 : (o[1] >= 0.f ? 1 : 2);
                 if (cls == 0) {
@@ -1295,8 +1285,8 @@ __global__ void __launch_bounds__(256) k_route(const DevScene<typename ModeT<MOD
 }
 
 cudaError_t launch_route(const mgk_scene& s, const void* dsc, uint32_t base, uint32_t n, uint32_t cap,
-                         const float* out, const float* feat, float conf_min, float crit_frac, uint32_t route,
-                         const ChunkBuffers& b, uint32_t* fallback_ids, void* fallback_q, cudaStream_t st) {
+                         const float* out, const float* feat, float conf_min, float crit_frac, const ChunkBuffers& b,
+                         uint32_t* fallback_ids, void* fallback_q, cudaStream_t st) {
     if (n == 0) return cudaSuccess;
     const bool f64 = s.precision == MGK_PRECISION_F64;
     const size_t T = f64 ? 8 : 4;
@@ -1306,11 +1296,11 @@ cudaError_t launch_route(const mgk_scene& s, const void* dsc, uint32_t base, uin
     void* fqc = fq + size_t(cap) * 8 * T;
     const uint32_t blocks = (n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096;
     if (f64)
-        k_route<MGK_PRECISION_F64><<<blocks, 256, 0, st>>>(ds<double>(dsc), base, n, cap, out, feat, conf_min, crit_frac, route,
+        k_route<MGK_PRECISION_F64><<<blocks, 256, 0, st>>>(ds<double>(dsc), base, n, cap, out, feat, conf_min, crit_frac,
                                                            b.qx, b.qp, b.qc, fqx, fqp, fqc, fallback_ids,
                                                            reinterpret_cast<HitEntry<double>*>(b.hits), b.counters);
     else
-        k_route<MGK_PRECISION_MIXED><<<blocks, 256, 0, st>>>(ds<float>(dsc), base, n, cap, out, feat, conf_min, crit_frac, route,
+        k_route<MGK_PRECISION_MIXED><<<blocks, 256, 0, st>>>(ds<float>(dsc), base, n, cap, out, feat, conf_min, crit_frac,
                                                              b.qx, b.qp, b.qc, fqx, fqp, fqc, fallback_ids,
                                                              reinterpret_cast<HitEntry<float>*>(b.hits), b.counters);
     return cudaGetLastError();

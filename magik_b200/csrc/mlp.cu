@@ -424,6 +424,45 @@ cudaError_t launch_gather_tiled(const float* feat, const SampleLabel* lab, const
     return cudaGetLastError();
 }
 
+// The sample-set order of one epoch: perm[i] = P(i) for a keyed
+// pseudo-random permutation P of [0, n).  P is a 4-round balanced Feistel
+// network on the smallest even number of bits that covers n (a bijection of
+// that domain), its round function the MurmurHash3 finalizer (A. Appleby)
+// of the right half xor the round key; values outside [0, n) are walked on
+// through P until they fall inside ("cycle walking": the orbit of i under P
+// returns to i < n, so the walk ends, after fewer than 4 steps on average).
+__device__ __forceinline__ uint32_t fmix32(uint32_t h) {
+    h ^= h >> 16; h *= 0x85EBCA6Bu; h ^= h >> 13; h *= 0xC2B2AE35u; h ^= h >> 16;
+    return h;
+}
+__global__ void k_epoch_perm(uint32_t* __restrict__ perm, uint32_t n, uint32_t half_bits, uint4 key) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t mask = half_bits >= 32 ? 0xFFFFFFFFu : (1u << half_bits) - 1u;
+    const uint32_t k[4] = {key.x, key.y, key.z, key.w};
+    uint32_t x = i;
+    do {
+        uint32_t L = x >> half_bits, R = x & mask;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const uint32_t t = L ^ (fmix32(R ^ k[r]) & mask);
+            L = R;
+            R = t;
+        }
+        x = (L << half_bits) | R;
+    } while (x >= n);
+    perm[i] = x;
+}
+
+cudaError_t launch_epoch_perm(uint32_t* perm, uint32_t n, const uint32_t key[4], cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    uint32_t bits = 2;
+    while (bits < 32 && (uint64_t(1) << bits) < n) ++bits;
+    bits += bits & 1u;
+    k_epoch_perm<<<(n + 255) / 256, 256, 0, st>>>(perm, n, bits / 2, make_uint4(key[0], key[1], key[2], key[3]));
+    return cudaGetLastError();
+}
+
 // Inference input: n FP32 feature rows (7 floats) to BF16 rows of 16, rows
 // [n, rows) zero.
 __global__ void k_features_bf16(const float* __restrict__ feat, uint32_t n, uint32_t rows,

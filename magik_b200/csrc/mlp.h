@@ -98,6 +98,9 @@ size_t mlp_dw_partial_floats(uint32_t jobs);
 cudaError_t launch_mlp_dw_tc(void* const* dz, void* const* h, const void* x0_tiles, const void* dout_tiles,
                              float* part, float* grad, uint32_t n_tiles, uint32_t jobs_heavy, uint32_t jobs_light,
                              uint32_t* status, cudaStream_t st);
+// The sample-set order of one epoch (a keyed permutation of [0, n)) on the
+// device (mlp.cu).
+cudaError_t launch_epoch_perm(uint32_t* perm, uint32_t n, const uint32_t key[4], cudaStream_t st);
 // Batch assembly into tiled X0 (16 columns) and the loss writing the BF16
 // output gradient as tiles (mlp.cu).
 cudaError_t launch_gather_tiled(const float* feat, const SampleLabel* lab, const uint32_t* perm, int b0, int B,

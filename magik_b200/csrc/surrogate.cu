@@ -68,8 +68,7 @@ struct mgk_surrogate {
     mgk_sample_label* blab = nullptr;
     uint32_t* perm = nullptr;
     uint32_t perm_n = 0;
-    std::vector<uint32_t> order;  // host copy of the latest mgk_surrogate_shuffle order
-    uint32_t order_n = 0;         // its length (rows mgk_surrogate_gradient_step may take)
+    uint32_t order_n = 0;  // length of the latest mgk_surrogate_shuffle order (rows gradient_step may take)
     // inference buffers for batch `ib`
     int ib = 0;
     __nv_bfloat16 *ix0 = nullptr, *iha = nullptr, *ihb = nullptr;
@@ -325,16 +324,13 @@ LossWeights loss_weights(const mgk_train_config& c) {
     return LossWeights{c.w_cls, c.w_r, c.w_g, c.w_dir, c.w_conf, c.tol_r, c.tol_g, c.tol_dir};
 }
 
-uint32_t host_hash(uint64_t seed, uint32_t a, uint32_t b) { return rng_u32(seed, 0x7E11u, a, b); }
-
-// The sample-set order of one epoch: Fisher-Yates with the counter-based hash.
-void epoch_order(std::vector<uint32_t>& perm, uint32_t n, uint64_t seed, uint32_t epoch) {
-    perm.resize(n);
-    for (uint32_t i = 0; i < n; ++i) perm[i] = i;
-    for (uint32_t i = n - 1; i > 0; --i) {
-        uint32_t j = uint32_t((uint64_t(host_hash(seed, epoch, i)) * (i + 1)) >> 32);
-        std::swap(perm[i], perm[j]);
-    }
+// The sample-set order of one epoch into s->perm, on the device: the keyed
+// permutation of launch_epoch_perm with round keys from the counter-based
+// hash of (seed, epoch).
+cudaError_t epoch_order(mgk_surrogate* s, uint32_t n, uint64_t seed, uint32_t epoch, cudaStream_t st) {
+    uint32_t key[4];
+    for (uint32_t r = 0; r < 4; ++r) key[r] = rng_u32(seed, 0x7E11u, epoch, r);
+    return launch_epoch_perm(s->perm, n, key, st);
 }
 
 // Step size of step `k` of `total` (cosine decay from lr to lr_final) and the
@@ -506,11 +502,9 @@ MGK_API mgk_result mgk_surrogate_train(mgk_surrogate* s, const mgk_train_config*
     if (rc != MGK_SUCCESS) return rc;
     const LossWeights w = loss_weights(*cfg);
     const uint32_t nb = n / B;
-    std::vector<uint32_t> perm(n);
     for (uint32_t ep = 0; ep < cfg->epochs; ++ep) {
-        epoch_order(perm, n, cfg->seed, ep);
         s->order_n = 0;
-        TRY(cudaMemcpyAsync(s->perm, perm.data(), size_t(n) * 4, cudaMemcpyHostToDevice, st));
+        TRY(epoch_order(s, n, cfg->seed, ep, st));
         TRY(cudaMemsetAsync(s->loss, 0, 4, st));
         for (uint32_t b = 0; b < nb; ++b) {
             TRY(gradient(s, d_feat, d_lab, int(b * B), int(B), w, s->loss, st));
@@ -533,12 +527,16 @@ MGK_API mgk_result mgk_surrogate_shuffle(mgk_surrogate* s, uint64_t seed, uint32
     cudaSetDevice(s->device);
     mgk_result rc = ensure_perm(s, n);
     if (rc != MGK_SUCCESS) return rc;
-    epoch_order(s->order, n, seed, epoch);
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
-    TRY(cudaMemcpyAsync(s->perm, s->order.data(), size_t(n) * 4, cudaMemcpyHostToDevice, st));
-    // the host copy of the order stays unchanged until the copy has read it
-    TRY(cudaStreamSynchronize(st));
+    TRY(epoch_order(s, n, seed, epoch, static_cast<cudaStream_t>(stream)));
     s->order_n = n;
+    return MGK_SUCCESS;
+}
+
+MGK_API mgk_result mgk_surrogate_order(mgk_surrogate* s, uint32_t* h_order, uint32_t n) {
+    if (!s || !h_order) return MGK_ERROR_INVALID_POINTER;
+    if (n > s->perm_n) return MGK_ERROR_INVALID_ARGUMENT;
+    cudaSetDevice(s->device);
+    TRY(cudaMemcpy(h_order, s->perm, size_t(n) * 4, cudaMemcpyDeviceToHost));
     return MGK_SUCCESS;
 }
 

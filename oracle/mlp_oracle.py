@@ -204,3 +204,58 @@ def weights_of(cfg):
     get = (lambda k: cfg[k]) if isinstance(cfg, dict) else (lambda k: getattr(cfg, k))
     return dict(cls=get("w_cls"), r=get("w_r"), g=get("w_g"), dir=get("w_dir"), conf=get("w_conf"),
                 tol_r=get("tol_r"), tol_g=get("tol_g"), tol_dir=get("tol_dir"))
+
+
+# ----------------------------------------------------------- epoch order
+def _triplet_hash(x):
+    """triplet_hash (internal_math.h:2027-2037) on Python ints, 32 bits."""
+    m = 0xFFFFFFFF
+    x ^= x >> 17; x = (x * 0xED5AD4BB) & m; x ^= x >> 11; x = (x * 0xAC4C1B51) & m
+    x ^= x >> 15; x = (x * 0x31848BAB) & m; x ^= x >> 14
+    return x
+
+
+def rng_u32(seed, stream, index, dim):
+    """The counter-based hash chain of the library (dev_scene.cuh rng_u32)."""
+    m = 0xFFFFFFFF
+    h = _triplet_hash((seed & m) ^ 0x9E3779B9)
+    h = _triplet_hash(h ^ ((seed >> 32) & m))
+    h = _triplet_hash(h ^ stream)
+    h = _triplet_hash(h ^ index)
+    return _triplet_hash(h ^ ((dim * 0x85EBCA6B + 1) & m))
+
+
+def epoch_order(n, seed, epoch):
+    """The sample order of one epoch (a restatement of mlp.cu k_epoch_perm):
+    a 4-round balanced Feistel network on the smallest even number of bits
+    covering n, round function the MurmurHash3 finalizer of the right half
+    xor the round key rng_u32(seed, 0x7E11, epoch, r), cycle-walked into
+    [0, n).  Vectorised over the n indices."""
+    bits = 2
+    while bits < 32 and (1 << bits) < n:
+        bits += 1
+    bits += bits & 1
+    hb = bits // 2
+    mask = np.uint64((1 << hb) - 1)
+    keys = [np.uint64(rng_u32(seed, 0x7E11, epoch, r)) for r in range(4)]
+
+    def fmix(h):
+        h = h & np.uint64(0xFFFFFFFF)
+        h ^= h >> np.uint64(16); h = (h * np.uint64(0x85EBCA6B)) & np.uint64(0xFFFFFFFF)
+        h ^= h >> np.uint64(13); h = (h * np.uint64(0xC2B2AE35)) & np.uint64(0xFFFFFFFF)
+        h ^= h >> np.uint64(16)
+        return h
+
+    def P(x):
+        L, R = x >> np.uint64(hb), x & mask
+        for k in keys:
+            L, R = R, L ^ (fmix(R ^ k) & mask)
+        return (L << np.uint64(hb)) | R
+
+    x = P(np.arange(n, dtype=np.uint64))
+    out = x.copy()
+    todo = out >= n
+    while todo.any():
+        out[todo] = P(out[todo])
+        todo = out >= n
+    return out.astype(np.uint32)
