@@ -67,6 +67,8 @@ def parse_args():
     ap.add_argument("--stress-spp", type=int, default=64)
     ap.add_argument("--c5-spp", type=int, default=256,
                     help="samples per pixel of the 3840x2160 surrogate render (0 skips it)")
+    ap.add_argument("--train-only", action="store_true",
+                    help="time only the surrogate training loop (for profiling its kernels)")
     return ap.parse_args()
 
 
@@ -384,6 +386,34 @@ def run_surrogate(args, ctx, s, d_stars, d_w, film_mixed_ms, steps):
                                "peak_source": f"MEASURED_PEAKS.json bf16_tflops (cuBLAS burst), {peak_src}",
                                "flop_per_ray": 400_896, "rows": n_rows, "ms": fwd_ms},
     }
+
+
+def run_train_only(args, device):
+    """The surrogate training loop alone: --surrogate-samples FP64-labelled
+    samples of the training distribution, one warm-up epoch, then
+    --surrogate-epochs timed epochs at batch 65536 on the default tcgen05 path.
+    Prints the training FLOP rate (3 x 400,896 FLOP per sample per step)."""
+    import torch
+    import magik_b200 as M
+    torch.cuda.set_device(device)
+    with M.Context(device) as ctx:
+        s = M.scene_defaults(width=1920, height=1080, spp=1, precision=M.abi.PRECISION_F64)
+        feat, lab = M.make_samples(ctx, s, 0x5A3B, args.surrogate_samples, n_spin_buckets=16)
+        net = M.Surrogate(ctx, seed=3)
+        net.train(M.train_defaults(epochs=1), feat, lab)
+        cfg = M.train_defaults(epochs=args.surrogate_epochs)
+        torch.cuda.synchronize()
+        t0 = time.time()
+        losses = net.train(cfg, feat, lab)
+        torch.cuda.synchronize()
+        dt = time.time() - t0
+        assert net.status() == 0
+        net.close()
+    steps = args.surrogate_epochs * (args.surrogate_samples // cfg.batch)
+    return {"metric": "surrogate training FLOP/s", "value": steps * cfg.batch * 3 * 400_896 / dt / 1e12,
+            "unit": "TFLOP/s", "higher_is_better": True, "steps": steps, "us_per_step": dt / steps * 1e6,
+            "batch": cfg.batch, "samples": args.surrogate_samples, "epochs": args.surrogate_epochs,
+            "final_loss": float(losses[-1]), "dtype": "bf16", "data": "synthetic"}
 
 
 def run_config5(args, ctx, net, d_stars, d_w):
@@ -752,6 +782,9 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.train_only:
+        print(json.dumps(run_train_only(args, local_rank)), flush=True)
+        return 0
     if args.impl == "reference":
         out = run_reference(args, rank, world)
         if out is not None:

@@ -19,6 +19,7 @@
 #include <cuda_runtime.h>
 
 #include "mlp.h"
+#include "mlp_loss.cuh"
 
 namespace mgk {
 
@@ -261,61 +262,28 @@ cudaError_t launch_colsum(const __nv_bfloat16* X, int rows, int ld, int cols, fl
     return cudaGetLastError();
 }
 
-__device__ __forceinline__ float sigmoidf_(float x) { return 1.0f / (1.0f + expf(-x)); }
 
-// Loss of one batch and its gradient w.r.t. the 8 outputs (scaled by 1/B).
-// Outputs: [0] disk logit, [1] escape logit (horizon logit fixed at 0),
-// [2] disk radius (scaled), [3] disk redshift, [4..6] escape direction,
-// [7] confidence logit.  See mlp.h for the label layout and the weights.
-// TILED: dout is written in the tensor-core tile layout (16 columns) of the
-// training kernels instead of row-major.
-template <bool TILED>
+// Loss of one batch and its gradient w.r.t. the outputs (scaled by 1/B):
+// mlp_row_loss (mlp_loss.cuh) per row; dout in BF16 and dout32 in FP32,
+// row-major.
 __global__ void __launch_bounds__(256) k_loss(const float* __restrict__ out, const SampleLabel* __restrict__ lab,
                                               int B, LossWeights w, __nv_bfloat16* __restrict__ dout,
                                               float* __restrict__ dout32, float* __restrict__ loss_acc) {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     float l = 0.f;
     if (b < B) {
-        const float* o = out + size_t(b) * MLP_OUT_PAD;
-        const SampleLabel L = lab[b];
-        float d[MLP_OUT_PAD];
-        for (int i = 0; i < MLP_OUT_PAD; ++i) d[i] = 0.f;
-        // class cross-entropy over (disk, escape, horizon)
-        const float z0 = o[0], z1 = o[1], mx = fmaxf(fmaxf(z0, z1), 0.f);
-        const float e0 = expf(z0 - mx), e1 = expf(z1 - mx), e2 = expf(-mx), se = e0 + e1 + e2;
-        const float p0 = e0 / se, p1 = e1 / se, p2 = e2 / se;
-        const int c = L.cls;
-        l += w.cls * -logf(fmaxf(c == 0 ? p0 : (c == 1 ? p1 : p2), 1e-30f));
-        d[0] = w.cls * (p0 - (c == 0 ? 1.f : 0.f));
-        d[1] = w.cls * (p1 - (c == 1 ? 1.f : 0.f));
-        const int pred = (p0 >= p1 && p0 >= p2) ? 0 : (p1 >= p2 ? 1 : 2);
-        bool good = pred == c;
-        if (c == 0) {
-            const float er = o[2] - L.r, eg = o[3] - L.g;
-            l += w.r * er * er + w.g * eg * eg;
-            d[2] = 2.f * w.r * er;
-            d[3] = 2.f * w.g * eg;
-            good = good && fabsf(er) < w.tol_r && fabsf(eg) < w.tol_g;
-        } else if (c == 1) {
-            float ed = 0.f;
-            for (int i = 0; i < 3; ++i) {
-                const float e = o[4 + i] - L.dir[i];
-                ed += e * e;
-                d[4 + i] = 2.f * w.dir * e;
-            }
-            l += w.dir * ed;
-            good = good && ed < w.tol_dir * w.tol_dir;
+        float o[MLP_OUT_PAD], d[MLP_OUT_PAD];
+#pragma unroll
+        for (int i = 0; i < MLP_OUT_PAD; i += 4) {
+            const float4 v = *reinterpret_cast<const float4*>(out + size_t(b) * MLP_OUT_PAD + i);
+            o[i] = v.x; o[i + 1] = v.y; o[i + 2] = v.z; o[i + 3] = v.w;
         }
-        // confidence: BCE against "this prediction is within tolerance"
-        const float q = sigmoidf_(o[7]), t = good ? 1.f : 0.f;
-        l += w.conf * -(t * logf(fmaxf(q, 1e-30f)) + (1.f - t) * logf(fmaxf(1.f - q, 1e-30f)));
-        d[7] = w.conf * (q - t);
+        l = mlp_row_loss(o, lab[b], w, d);
         const float inv_b = 1.0f / float(B);
+#pragma unroll
         for (int i = 0; i < MLP_OUT_PAD; ++i) {
             dout32[size_t(b) * MLP_OUT_PAD + i] = d[i] * inv_b;
-            const size_t o = TILED ? size_t(b >> 7) * 2048u + tile16(uint32_t(b) & 127u, uint32_t(i))
-                                   : size_t(b) * MLP_OUT_PAD + i;
-            dout[o] = __float2bfloat16_rn(d[i] * inv_b);
+            dout[size_t(b) * MLP_OUT_PAD + i] = __float2bfloat16_rn(d[i] * inv_b);
         }
     }
     // block reduction of the loss
@@ -331,15 +299,7 @@ __global__ void __launch_bounds__(256) k_loss(const float* __restrict__ out, con
 
 cudaError_t launch_loss(const float* out, const SampleLabel* lab, int B, LossWeights w, __nv_bfloat16* dout,
                         float* dout32, float* loss_acc, cudaStream_t st) {
-    k_loss<false><<<(B + 255) / 256, 256, 0, st>>>(out, lab, B, w, dout, dout32, loss_acc);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_loss_tiled(const float* out, const SampleLabel* lab, int B, LossWeights w, void* dout_tiles,
-                              float* dout32, float* loss_acc, cudaStream_t st) {
-    if (B % 128) return cudaErrorInvalidValue;
-    k_loss<true><<<(B + 255) / 256, 256, 0, st>>>(out, lab, B, w, static_cast<__nv_bfloat16*>(dout_tiles), dout32,
-                                                 loss_acc);
+    k_loss<<<(B + 255) / 256, 256, 0, st>>>(out, lab, B, w, dout, dout32, loss_acc);
     return cudaGetLastError();
 }
 

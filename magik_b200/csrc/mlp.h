@@ -88,24 +88,27 @@ cudaError_t launch_mlp_infer_tc(const float* feat, uint32_t n, const void* img, 
 // Tensor-core training (mlp_train_tc.cu) on tiled activations: 128-row tiles
 // in the operand layout (element (row, col) of tile t at
 // t * 256 * C + kmaj(row % 128, col, 16 C) bytes for C columns).
+// Forward with stash of Z_1..Z_4; with labels (lab non-null) also the loss
+// (+= *loss_acc, the batch mean) and dOut tiles; out (FP32 [rows][16]) may be
+// null.
 cudaError_t launch_mlp_fwd_stash_tc(const void* img, const float* params, const void* x0_tiles, void* const* z,
-                                    void* const* h, float* out, uint32_t n_tiles, uint32_t* status, int sm_count,
+                                    float* out, const SampleLabel* lab, const LossWeights& w, void* dout_tiles,
+                                    float* loss_acc, uint32_t n_tiles, uint32_t* status, int sm_count,
                                     cudaStream_t st);
 cudaError_t launch_mlp_bwd_dx_tc(const void* img, const void* dout_tiles, void* const* z, void* const* dz,
                                  uint32_t n_tiles, uint32_t* status, int sm_count, cudaStream_t st);
 void mlp_dw_jobs(uint32_t n_tiles, int sm_count, uint32_t* heavy, uint32_t* light);
 size_t mlp_dw_partial_floats(uint32_t jobs);
-cudaError_t launch_mlp_dw_tc(void* const* dz, void* const* h, const void* x0_tiles, const void* dout_tiles,
+// Weight and bias gradients (all of W1..W5, b1..b5) from dZ_1..dZ_4, Z_1..Z_4,
+// X0 and dOut.
+cudaError_t launch_mlp_dw_tc(void* const* dz, void* const* z, const void* x0_tiles, const void* dout_tiles,
                              float* part, float* grad, uint32_t n_tiles, uint32_t jobs_heavy, uint32_t jobs_light,
                              uint32_t* status, cudaStream_t st);
 // The sample-set order of one epoch (a keyed permutation of [0, n)) on the
 // device (mlp.cu).
 cudaError_t launch_epoch_perm(uint32_t* perm, uint32_t n, const uint32_t key[4], cudaStream_t st);
-// Batch assembly into tiled X0 (16 columns) and the loss writing the BF16
-// output gradient as tiles (mlp.cu).
+// Batch assembly into tiled X0 (16 columns) (mlp.cu).
 cudaError_t launch_gather_tiled(const float* feat, const SampleLabel* lab, const uint32_t* perm, int b0, int B,
                                 void* x0_tiles, SampleLabel* blab, cudaStream_t st);
-cudaError_t launch_loss_tiled(const float* out, const SampleLabel* lab, int B, LossWeights w, void* dout_tiles,
-                              float* dout32, float* loss_acc, cudaStream_t st);
 
 }  // namespace mgk

@@ -5,8 +5,11 @@
 //  k_mlp_chain_tc<FWD>  forward with stash: all five layers of a 128-row
 //                       tile in one CTA (the structure of the fused
 //                       inference kernel), writing the pre-activations Z_l
-//                       and activations H_l = silu(Z_l) of layers 1-4 and
-//                       the FP32 outputs.
+//                       of layers 1-4 (the activations H_l = silu(Z_l) are
+//                       recomputed where the weight gradients need them),
+//                       then the loss of each row (mlp_loss.cuh) and the
+//                       BF16 output gradient dOut.  The FP32 outputs are
+//                       written only where asked for.
 //  k_mlp_chain_tc<BWD>  the input gradients of a tile through the layers:
 //                       dZ4 = (dOut W5) * silu'(Z4), dZ3 = (dZ4 W4) * silu'(Z3),
 //                       ... dZ1, the weights read as the transposes of the
@@ -15,8 +18,10 @@
 //                       dW5^T = H4^T dOut) over a range of batch tiles per
 //                       CTA (split K), both operands M/N-major views of the
 //                       stashed tiles, the partial in tensor memory, written
-//                       once per CTA; the CTA's idle warps sum the columns of
-//                       dZ_l for the bias gradients.
+//                       once per CTA.  The CTA's other warps turn each staged
+//                       Z_{l-1} into H_{l-1} = silu(Z_{l-1}) in shared memory
+//                       before its MMAs and sum the columns of dZ_l (dOut for
+//                       layer 5) for the bias gradients.
 //  k_mlp_dw_reduce      sums the CTAs' partials into the gradient vector (no
 //                       atomics: the gradient does not depend on the order in
 //                       which CTAs finish).
@@ -44,6 +49,7 @@
 #include <cuda_runtime.h>
 
 #include "mlp.h"
+#include "mlp_loss.cuh"
 #include "tc_sm100.cuh"
 
 namespace mgk {
@@ -71,7 +77,17 @@ __device__ __forceinline__ float silu_grad_f(float z) {
     return s * __fmaf_rn(z, 1.0f - s, 1.0f);
 }
 __device__ __forceinline__ float2 unpack_bf16(uint32_t v) {
-    return __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&v));
+    return make_float2(__uint_as_float(v << 16), __uint_as_float(v & 0xFFFF0000u));
+}
+// silu of both BF16 halves of a word, rounded back to BF16
+__device__ __forceinline__ uint32_t silu_bf16x2(uint32_t v) {
+    const float2 z = unpack_bf16(v);
+    return pack_bf16(silu_f(z.x), silu_f(z.y));
+}
+__device__ __forceinline__ void add_bf16x2(float& a, float& b, uint32_t v) {
+    const float2 f = unpack_bf16(v);
+    a += f.x;
+    b += f.y;
 }
 
 // ============================================================ chain kernel
@@ -120,8 +136,12 @@ struct ChainArgs {
     const float* params;       // FP32 parameters (biases)
     const unsigned char* in;   // FWD: X0 tiles (16 columns); BWD: dOut tiles (16 columns)
     unsigned char* z[4];       // Z_1..Z_4 tiles (FWD writes, BWD reads)
-    unsigned char* h[4];       // FWD: H_1..H_4 tiles; BWD: dZ_1..dZ_4 tiles (written)
-    float* out;                // FWD: outputs [rows][16] FP32
+    unsigned char* dz[4];      // BWD: dZ_1..dZ_4 tiles (written)
+    float* out;                // FWD: outputs [rows][16] FP32, or null
+    const SampleLabel* lab;    // FWD: the batch's labels for the fused loss
+    unsigned char* dout;       // FWD: dOut tiles (16 columns), d(loss)/d(out) / B in BF16
+    float* loss_acc;           // FWD: += the batch's mean loss
+    LossWeights w;
     uint32_t n_tiles;
     uint32_t* status;
 };
@@ -184,6 +204,15 @@ __global__ void __launch_bounds__(CH_THREADS, 1) k_mlp_chain_tc(ChainArgs g) {
                 for (int l = 0; l < S && ok; ++l)
                     for (int b = 0; b < 2 && ok; ++b) {
                         const Step st = step_of<DIR>(l);
+                        if constexpr (DIR == BWD) {
+                            // the Z tiles the epilogue reads for silu', one step ahead, into L2
+                            const uint32_t tile = blockIdx.x + (2 * p + uint32_t(b)) * gridDim.x;
+                            if (tile < n_tiles) {
+                                if (l == 0) bulk_prefetch_l2(g.z[3] + size_t(tile) * A_BYTES, A_BYTES);
+                                const unsigned char* zn = l == 0 ? g.z[2] : (l == 1 ? g.z[1] : g.z[0]);
+                                if (l + 1 < S) bulk_prefetch_l2(zn + size_t(tile) * A_BYTES, A_BYTES);
+                            }
+                        }
                         for (int ci = 0; ci < st.nc; ++ci, ++j) {
                             const uint32_t s = j % N_SLOT, use = j / N_SLOT;
                             if (use > 0 && !mbar_wait(bar_empty + 8 * s, (use - 1) & 1u, abort_flag)) {
@@ -247,6 +276,7 @@ __global__ void __launch_bounds__(CH_THREADS, 1) k_mlp_chain_tc(ChainArgs g) {
         const uint32_t bar_db = bar_d + 8 * buf, bar_ab = bar_a + 8 * buf;
         uint32_t dr = 0;
         bool ok = true;
+        float loss = 0.f;  // FWD: this thread's rows' loss
         for (uint32_t t = buf; t < 2 * my_pairs && ok; t += 2) {
             const uint32_t tile = blockIdx.x + t * gridDim.x;  // >= n_tiles for the empty tile
             const bool valid = tile < n_tiles;
@@ -263,7 +293,20 @@ __global__ void __launch_bounds__(CH_THREADS, 1) k_mlp_chain_tc(ChainArgs g) {
             }
             fence_proxy_async();
             mbar_arrive(bar_ab);
+            const size_t tile_off = size_t(tile) * A_BYTES;
             for (int l = 0; l < S; ++l) {
+                const int li = DIR == FWD ? l : 3 - l;  // the Z (dZ) index this step writes (reads)
+                unsigned char* const zl = li == 0 ? g.z[0] : (li == 1 ? g.z[1] : (li == 2 ? g.z[2] : g.z[3]));
+                unsigned char* const dzl = li == 0 ? g.dz[0] : (li == 1 ? g.dz[1] : (li == 2 ? g.dz[2] : g.dz[3]));
+                // BWD: the first block's Z, loaded while the MMAs run
+                uint4 zn[4];
+                if constexpr (DIR == BWD) {
+#pragma unroll
+                    for (int gq = 0; gq < 4; ++gq)
+                        zn[gq] = valid ? *reinterpret_cast<const uint4*>(zl + tile_off +
+                                                                          kmaj(row, half * 128 + 8 * gq, A_SBO))
+                                       : uint4{0u, 0u, 0u, 0u};
+                }
                 if (!mbar_wait(bar_db, dr & 1u, abort_flag)) { ok = false; break; }
                 ++dr;
                 tc_fence_after();
@@ -275,33 +318,37 @@ __global__ void __launch_bounds__(CH_THREADS, 1) k_mlp_chain_tc(ChainArgs g) {
                         tc_fence_before();
                         if (valid) {
                             const float* b5 = bias + 4 * MLP_HID;
-                            float4* o = reinterpret_cast<float4*>(g.out + (size_t(tile) * TM + row) * MLP_OUT_PAD);
+                            float o[MLP_OUT_PAD];
 #pragma unroll
-                            for (int k = 0; k < 4; ++k)
-                                o[k] = make_float4(__uint_as_float(v[4 * k]) + b5[4 * k],
-                                                   __uint_as_float(v[4 * k + 1]) + b5[4 * k + 1],
-                                                   __uint_as_float(v[4 * k + 2]) + b5[4 * k + 2],
-                                                   __uint_as_float(v[4 * k + 3]) + b5[4 * k + 3]);
+                            for (int k = 0; k < MLP_OUT_PAD; ++k) o[k] = __uint_as_float(v[k]) + b5[k];
+                            const uint32_t r = tile * TM + row;
+                            if (g.out) {
+                                float4* op = reinterpret_cast<float4*>(g.out + size_t(r) * MLP_OUT_PAD);
+#pragma unroll
+                                for (int k = 0; k < 4; ++k)
+                                    op[k] = make_float4(o[4 * k], o[4 * k + 1], o[4 * k + 2], o[4 * k + 3]);
+                            }
+                            if (g.lab) {
+                                float d[MLP_OUT_PAD];
+                                loss += mlp_row_loss(o, g.lab[r], g.w, d);
+                                const float inv_b = 1.0f / float(n_tiles * TM);
+                                uint32_t dv[8];
+#pragma unroll
+                                for (int k = 0; k < 8; ++k) dv[k] = pack_bf16(d[2 * k] * inv_b, d[2 * k + 1] * inv_b);
+                                unsigned char* dst = g.dout + size_t(tile) * X_TILE + kmaj(row, 0, X_SBO);
+                                *reinterpret_cast<uint4*>(dst) = uint4{dv[0], dv[1], dv[2], dv[3]};
+                                *reinterpret_cast<uint4*>(dst + 128) = uint4{dv[4], dv[5], dv[6], dv[7]};
+                            }
                         }
                     }
                     continue;
                 }
                 // 4 blocks of 32 columns of this warp's half
-                const int li = DIR == FWD ? l : 3 - l;  // the Z / H (dZ) index this step writes
-                const size_t tile_off = size_t(tile) * A_BYTES;
                 const float scale = (DIR == FWD || l > 0) ? 2.0f : 1.0f;  // layers 1-4 are stored halved
                 for (int blk = 0; blk < 4; ++blk) {
                     const uint32_t col = half * 128 + uint32_t(blk) * 32;
                     uint32_t v[32];
                     tmem_ld32(t_lane + col, v);
-                    uint4 zin[4];
-                    if constexpr (DIR == BWD) {
-#pragma unroll
-                        for (int gq = 0; gq < 4; ++gq)
-                            zin[gq] = valid ? *reinterpret_cast<const uint4*>(g.z[li] + tile_off +
-                                                                               kmaj(row, col + 8 * gq, A_SBO))
-                                            : uint4{0u, 0u, 0u, 0u};
-                    }
                     tmem_wait_ld(v);
 #pragma unroll
                     for (int gq = 0; gq < 4; ++gq) {
@@ -317,18 +364,31 @@ __global__ void __launch_bounds__(CH_THREADS, 1) k_mlp_chain_tc(ChainArgs g) {
                                 zv[e] = pack_bf16(z0, z1);
                                 hv[e] = pack_bf16(silu_f(z0), silu_f(z1));
                             } else {
-                                const uint32_t zw = (&zin[gq].x)[e];
+                                const uint32_t zw = e == 0 ? zn[gq].x : (e == 1 ? zn[gq].y : (e == 2 ? zn[gq].z : zn[gq].w));
                                 const float2 zf = unpack_bf16(zw);
                                 hv[e] = pack_bf16(a0 * silu_grad_f(zf.x), a1 * silu_grad_f(zf.y));
                                 zv[e] = 0u;
                             }
                         }
+                        // FWD: H into the next layer's operand, Z to the stash;
+                        // BWD: dZ into the next step's operand and to global memory
                         const uint4 h4 = uint4{hv[0], hv[1], hv[2], hv[3]};
                         if (l < S - 1) *reinterpret_cast<uint4*>(A + off) = h4;
                         if (valid) {
-                            *reinterpret_cast<uint4*>(g.h[li] + tile_off + off) = h4;
                             if constexpr (DIR == FWD)
-                                *reinterpret_cast<uint4*>(g.z[li] + tile_off + off) = uint4{zv[0], zv[1], zv[2], zv[3]};
+                                *reinterpret_cast<uint4*>(zl + tile_off + off) = uint4{zv[0], zv[1], zv[2], zv[3]};
+                            else
+                                *reinterpret_cast<uint4*>(dzl + tile_off + off) = h4;
+                        }
+                    }
+                    if constexpr (DIR == BWD) {
+                        // the next block's Z, loaded while this block's results drain
+                        if (blk < 3) {
+#pragma unroll
+                            for (int gq = 0; gq < 4; ++gq)
+                                zn[gq] = valid ? *reinterpret_cast<const uint4*>(zl + tile_off +
+                                                                                  kmaj(row, col + 32 + 8 * gq, A_SBO))
+                                               : uint4{0u, 0u, 0u, 0u};
                         }
                     }
                 }
@@ -337,6 +397,13 @@ __global__ void __launch_bounds__(CH_THREADS, 1) k_mlp_chain_tc(ChainArgs g) {
                     fence_proxy_async();
                     mbar_arrive(bar_ab);
                 }
+            }
+        }
+        if constexpr (DIR == FWD) {
+            if (half == 0 && g.loss_acc) {
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) loss += __shfl_xor_sync(0xFFFFFFFFu, loss, o);
+                if (lane == 0) atomicAdd(g.loss_acc, loss / float(n_tiles * TM));
             }
         }
     }
@@ -355,7 +422,9 @@ __global__ void __launch_bounds__(CH_THREADS, 1) k_mlp_chain_tc(ChainArgs g) {
 //   L = 4:    dW5^T = H4^T dOut   M = 256 (H4 columns), N = 16
 // Stages of 64 batch rows: half a tile of the A matrix (32 KB) and of the B
 // matrix (32 KB, or 2 KB for 16 columns); the M = 256 rows of the result in
-// two MMA halves of 128.
+// two MMA halves of 128.  H_L comes in as Z_L and is made in place.  A stage
+// passes full (the bulk copies landed) -> conv (the epilogue warps made H and
+// took the column sums) -> the MMAs -> empty (their commit).
 constexpr int DW_STAGES = 3;
 constexpr uint32_t DW_A_BYTES = 32768, DW_B_BYTES = 32768;
 constexpr uint32_t DW_STAGE = DW_A_BYTES + DW_B_BYTES;
@@ -363,13 +432,14 @@ constexpr int DW_EPI_WARPS = 8;
 constexpr int DW_THREADS = 32 * (2 + DW_EPI_WARPS);
 constexpr uint32_t DW_OFF_BAR = DW_STAGES * DW_STAGE;
 constexpr uint32_t DW_OFF_MISC = DW_OFF_BAR + 16 * 8;
-constexpr uint32_t DW_SMEM = DW_OFF_MISC + 16 + 128;
+constexpr uint32_t DW_OFF_RED = DW_OFF_MISC + 16;             // [8 warps][16] output-bias sums
+constexpr uint32_t DW_SMEM = DW_OFF_RED + DW_EPI_WARPS * 16 * 4 + 128;
 static_assert(DW_SMEM <= 232448, "shared memory");
 constexpr uint32_t DW_PART = MLP_HID * MLP_HID + MLP_HID;  // floats per job: the partial dW and bias sums
 
 struct DwArgs {
     const unsigned char* dz[4];  // dZ1..dZ4 tiles
-    const unsigned char* h[4];   // H1..H4 tiles
+    const unsigned char* z[4];   // Z1..Z4 tiles (H = silu(Z) is made in shared memory)
     const unsigned char* x0;     // X0 tiles (16 columns)
     const unsigned char* dout;   // dOut tiles (16 columns)
     float* part;                 // [jobs][DW_PART]
@@ -401,7 +471,8 @@ __global__ void __launch_bounds__(DW_THREADS, 1) k_mlp_dw_tc(DwArgs g) {
         reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
     const uint32_t sbase = smem_addr(smem);
     const uint32_t bar_full = sbase + DW_OFF_BAR, bar_empty = bar_full + DW_STAGES * 8;
-    const uint32_t bar_done = bar_empty + DW_STAGES * 8, bar_drain = bar_done + 8;
+    const uint32_t bar_conv = bar_empty + DW_STAGES * 8;
+    const uint32_t bar_done = bar_conv + DW_STAGES * 8, bar_drain = bar_done + 8;
     volatile uint32_t* tmem_slot = reinterpret_cast<volatile uint32_t*>(smem + DW_OFF_MISC);
     volatile uint32_t* abort_flag = reinterpret_cast<volatile uint32_t*>(smem + DW_OFF_MISC + 4);
 
@@ -412,9 +483,9 @@ __global__ void __launch_bounds__(DW_THREADS, 1) k_mlp_dw_tc(DwArgs g) {
     const bool wide = L >= 1 && L <= 3;     // N = 256
     const uint32_t n = wide ? 256u : 16u;
     const uint32_t tmem_cols = wide ? 512u : 32u;
-    const bool bias_sums = L <= 3;          // A = dZ: its column sums are the bias gradient
-    const unsigned char* Am = L == 4 ? g.h[3] : g.dz[L];
-    const unsigned char* Bm = L == 0 ? g.x0 : (L == 4 ? g.dout : g.h[L - 1]);
+    // the bias gradient: the column sums of A = dZ_L (L <= 3) or of B = dOut (L = 4)
+    const unsigned char* Am = L == 4 ? g.z[3] : (L == 0 ? g.dz[0] : (L == 1 ? g.dz[1] : (L == 2 ? g.dz[2] : g.dz[3])));
+    const unsigned char* Bm = L == 0 ? g.x0 : (L == 1 ? g.z[0] : (L == 2 ? g.z[1] : (L == 3 ? g.z[2] : g.dout)));
     const uint32_t a_tile = A_BYTES, b_tile = wide ? A_BYTES : X_TILE;
     const uint32_t b_half = b_tile / 2, b_lbo = wide ? A_SBO : X_SBO;
     const uint32_t n_stages = 2 * (t1 - t0);  // half tiles
@@ -422,7 +493,8 @@ __global__ void __launch_bounds__(DW_THREADS, 1) k_mlp_dw_tc(DwArgs g) {
     if (threadIdx.x == 0) {
         for (int s = 0; s < DW_STAGES; ++s) {
             mbar_init(bar_full + 8 * s, 1);
-            mbar_init(bar_empty + 8 * s, 1 + 32 * DW_EPI_WARPS);  // the MMA commit and every epilogue thread
+            mbar_init(bar_conv + 8 * s, 32 * DW_EPI_WARPS);  // every epilogue thread
+            mbar_init(bar_empty + 8 * s, 1);                 // the MMA commit
         }
         mbar_init(bar_done, 1);
         mbar_init(bar_drain, 1);
@@ -465,7 +537,7 @@ __global__ void __launch_bounds__(DW_THREADS, 1) k_mlp_dw_tc(DwArgs g) {
             const uint32_t idesc = idesc_bf16_major(TM, n, true, true);
             for (uint32_t j = 0; j < n_stages && ok; ++j) {
                 const uint32_t s = j % DW_STAGES, use = j / DW_STAGES;
-                if (!mbar_wait(bar_full + 8 * s, use & 1u, abort_flag)) { ok = false; break; }
+                if (!mbar_wait(bar_conv + 8 * s, use & 1u, abort_flag)) { ok = false; break; }
                 tc_fence_after();
                 const uint32_t sa = sbase + s * DW_STAGE, sb = sa + DW_A_BYTES;
                 // 64 rows of K: 4 steps of 16 rows, two 8-row groups each
@@ -483,24 +555,87 @@ __global__ void __launch_bounds__(DW_THREADS, 1) k_mlp_dw_tc(DwArgs g) {
             for (uint32_t it = 0; it < WAIT_LIMIT && !mbar_try(bar_drain, 0); ++it) {}
         }
     } else {
-        // column sums of each stage's A (dZ) half tile, then the partial out of TMEM
-        const uint32_t ew = warp - 2;           // 0..7
-        const uint32_t col = ew * 32 + lane;    // 0..255: this thread's column of A
-        float csum = 0.f;
+        // per stage: H = silu(Z) in place of the staged Z half tile, the
+        // column sums for the bias gradient; then the partial out of TMEM
+        const uint32_t ew = warp - 2;  // 0..7
+        const uint32_t et = threadIdx.x - 64;
+        // column sums: L <= 3, warp ew sums the 8-column groups 4 ew .. 4 ew + 3
+        // of A (lane: group 4 ew + lane % 4, row lane / 4 of each 8-row group);
+        // L = 4, warp ew the 8-row group ew of B (lanes 0-15: group lane / 8,
+        // row lane % 8)
+        float csum[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) csum[e] = 0.f;
         bool ok = true;
         for (uint32_t j = 0; j < n_stages && ok; ++j) {
             const uint32_t s = j % DW_STAGES, use = j / DW_STAGES;
             if (!mbar_wait(bar_full + 8 * s, use & 1u, abort_flag)) { ok = false; break; }
-            if (bias_sums) {
-                const unsigned char* a = smem + s * DW_STAGE;
-#pragma unroll 8
-                for (uint32_t r = 0; r < 64; ++r)
-                    csum += __bfloat162float(*reinterpret_cast<const __nv_bfloat16*>(a + kmaj(r, col, A_SBO)));
+            unsigned char* sa = smem + s * DW_STAGE;
+            unsigned char* sb = sa + DW_A_BYTES;
+            if (L >= 1) {
+                // the 32 KB half tile of Z (B for L = 1..3, A for L = 4) -> H
+                uint4* zt = reinterpret_cast<uint4*>(L == 4 ? sa : sb);
+#pragma unroll 2
+                for (uint32_t k = 0; k < DW_A_BYTES / 16 / (32 * DW_EPI_WARPS); ++k) {
+                    const uint4 v = zt[et + k * 32 * DW_EPI_WARPS];
+                    zt[et + k * 32 * DW_EPI_WARPS] =
+                        uint4{silu_bf16x2(v.x), silu_bf16x2(v.y), silu_bf16x2(v.z), silu_bf16x2(v.w)};
+                }
             }
-            mbar_arrive(bar_empty + 8 * s);
+            if (L <= 3) {
+                const unsigned char* a = sa + (4 * ew + (lane & 3u)) * 128u + (lane >> 2) * 16u;
+#pragma unroll
+                for (uint32_t rg = 0; rg < 8; ++rg) {
+                    const uint4 v = *reinterpret_cast<const uint4*>(a + rg * A_SBO);
+                    add_bf16x2(csum[0], csum[1], v.x);
+                    add_bf16x2(csum[2], csum[3], v.y);
+                    add_bf16x2(csum[4], csum[5], v.z);
+                    add_bf16x2(csum[6], csum[7], v.w);
+                }
+            } else if (lane < 16) {
+                const uint4 v = *reinterpret_cast<const uint4*>(sb + ew * X_SBO + (lane >> 3) * 128u + (lane & 7u) * 16u);
+                add_bf16x2(csum[0], csum[1], v.x);
+                add_bf16x2(csum[2], csum[3], v.y);
+                add_bf16x2(csum[4], csum[5], v.z);
+                add_bf16x2(csum[6], csum[7], v.w);
+            }
+            fence_proxy_async();
+            mbar_arrive(bar_conv + 8 * s);
         }
         float* part = g.part + size_t(blockIdx.x) * DW_PART;
-        if (bias_sums) part[MLP_HID * MLP_HID + col] = csum;
+        if (L <= 3) {
+            // sum over the 8 rows of a group (lanes of equal lane % 4)
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+                csum[e] += __shfl_xor_sync(0xFFFFFFFFu, csum[e], 4);
+                csum[e] += __shfl_xor_sync(0xFFFFFFFFu, csum[e], 8);
+                csum[e] += __shfl_xor_sync(0xFFFFFFFFu, csum[e], 16);
+            }
+            if (lane < 4) {
+                float* dst = part + MLP_HID * MLP_HID + (4 * ew + lane) * 8;
+#pragma unroll
+                for (int e = 0; e < 8; ++e) dst[e] = csum[e];
+            }
+        } else {
+            // over the rows of the group (lane % 8), then over the warps in order
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+                csum[e] += __shfl_xor_sync(0xFFFFFFFFu, csum[e], 1);
+                csum[e] += __shfl_xor_sync(0xFFFFFFFFu, csum[e], 2);
+                csum[e] += __shfl_xor_sync(0xFFFFFFFFu, csum[e], 4);
+            }
+            float* red = reinterpret_cast<float*>(smem + DW_OFF_RED);
+            if (lane == 0 || lane == 8) {
+#pragma unroll
+                for (int e = 0; e < 8; ++e) red[ew * 16 + (lane >> 3) * 8 + e] = csum[e];
+            }
+            asm volatile("bar.sync 1, %0;" ::"n"(32 * DW_EPI_WARPS) : "memory");
+            if (ew == 0 && lane < 16) {
+                float t = 0.f;
+                for (int k = 0; k < DW_EPI_WARPS; ++k) t += red[k * 16 + lane];
+                part[MLP_HID * MLP_HID + lane] = t;
+            }
+        }
         if (ok && mbar_wait(bar_done, 0, abort_flag)) {
             tc_fence_after();
             // a warp reads the TMEM lanes of its place in its warpgroup,
@@ -531,11 +666,11 @@ __global__ void __launch_bounds__(DW_THREADS, 1) k_mlp_dw_tc(DwArgs g) {
 }
 
 // grad = the sum of the jobs' partials: W1..W5 (W5 from its transpose) and
-// b1..b4; one thread per gradient element.
+// b1..b5; one thread per gradient element, the jobs summed in order.
 __global__ void __launch_bounds__(256) k_mlp_dw_reduce(const float* __restrict__ part, uint32_t jobs_heavy,
                                                        uint32_t jobs_light, float* __restrict__ grad) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    // element i of [W2 | W3 | W4 | W1 | W5 | b1 | b2 | b3 | b4]
+    // element i of [W2 | W3 | W4 | W1 | W5 | b1 | b2 | b3 | b4 | b5]
     constexpr uint32_t NW = MLP_HID * MLP_HID, NS = MLP_HID * MLP_IN_PAD;
     uint32_t j0, nj, src, dst;
     if (i < 3 * NW) {
@@ -553,10 +688,14 @@ __global__ void __launch_bounds__(256) k_mlp_dw_reduce(const float* __restrict__
         j0 = L == 0 ? 3 * jobs_heavy : (L - 1) * jobs_heavy;
         nj = L == 0 ? jobs_light : jobs_heavy;
         src = NW + c; dst = mlp_b_off(int(L)) + c;
+    } else if (i < 3 * NW + 2 * NS + 4 * MLP_HID + MLP_OUT_PAD) {
+        const uint32_t c = i - 3 * NW - 2 * NS - 4 * MLP_HID;  // b5 from the dOut column sums
+        j0 = 3 * jobs_heavy + jobs_light; nj = jobs_light; src = NW + c; dst = mlp_b_off(4) + c;
     } else {
         return;
     }
     float s = 0.f;
+#pragma unroll 4
     for (uint32_t k = 0; k < nj; ++k) s += part[size_t(j0 + k) * DW_PART + src];
     grad[dst] = s;
 }
@@ -567,7 +706,8 @@ __global__ void __launch_bounds__(256) k_mlp_dw_reduce(const float* __restrict__
 size_t mlp_dw_partial_floats(uint32_t jobs) { return size_t(jobs) * DW_PART; }
 
 cudaError_t launch_mlp_fwd_stash_tc(const void* img, const float* params, const void* x0_tiles, void* const* z,
-                                    void* const* h, float* out, uint32_t n_tiles, uint32_t* status, int sm_count,
+                                    float* out, const SampleLabel* lab, const LossWeights& w, void* dout_tiles,
+                                    float* loss_acc, uint32_t n_tiles, uint32_t* status, int sm_count,
                                     cudaStream_t st) {
     static bool attr = false;
     if (!attr) {
@@ -580,13 +720,15 @@ cudaError_t launch_mlp_fwd_stash_tc(const void* img, const float* params, const 
     a.img = static_cast<const unsigned char*>(img);
     a.params = params;
     a.in = static_cast<const unsigned char*>(x0_tiles);
-    for (int l = 0; l < 4; ++l) {
-        a.z[l] = static_cast<unsigned char*>(z[l]);
-        a.h[l] = static_cast<unsigned char*>(h[l]);
-    }
+    for (int l = 0; l < 4; ++l) a.z[l] = static_cast<unsigned char*>(z[l]);
     a.out = out;
+    a.lab = lab;
+    a.w = w;
+    a.dout = static_cast<unsigned char*>(dout_tiles);
+    a.loss_acc = loss_acc;
     a.n_tiles = n_tiles;
     a.status = status;
+    if (lab && !dout_tiles) return cudaErrorInvalidValue;
     const uint32_t grid = n_tiles < uint32_t(sm_count) ? n_tiles : uint32_t(sm_count);
     if (grid == 0) return cudaSuccess;
     k_mlp_chain_tc<FWD><<<grid, CH_THREADS, CH_SMEM, st>>>(a);
@@ -607,7 +749,7 @@ cudaError_t launch_mlp_bwd_dx_tc(const void* img, const void* dout_tiles, void* 
     a.in = static_cast<const unsigned char*>(dout_tiles);
     for (int l = 0; l < 4; ++l) {
         a.z[l] = static_cast<unsigned char*>(z[l]);
-        a.h[l] = static_cast<unsigned char*>(dz[l]);
+        a.dz[l] = static_cast<unsigned char*>(dz[l]);
     }
     a.n_tiles = n_tiles;
     a.status = status;
@@ -628,7 +770,7 @@ void mlp_dw_jobs(uint32_t n_tiles, int sm_count, uint32_t* heavy, uint32_t* ligh
     *light = l ? l : 1;
 }
 
-cudaError_t launch_mlp_dw_tc(void* const* dz, void* const* h, const void* x0_tiles, const void* dout_tiles,
+cudaError_t launch_mlp_dw_tc(void* const* dz, void* const* z, const void* x0_tiles, const void* dout_tiles,
                              float* part, float* grad, uint32_t n_tiles, uint32_t jobs_heavy, uint32_t jobs_light,
                              uint32_t* status, cudaStream_t st) {
     static bool attr = false;
@@ -640,7 +782,7 @@ cudaError_t launch_mlp_dw_tc(void* const* dz, void* const* h, const void* x0_til
     DwArgs a{};
     for (int l = 0; l < 4; ++l) {
         a.dz[l] = static_cast<const unsigned char*>(dz[l]);
-        a.h[l] = static_cast<const unsigned char*>(h[l]);
+        a.z[l] = static_cast<const unsigned char*>(z[l]);
     }
     a.x0 = static_cast<const unsigned char*>(x0_tiles);
     a.dout = static_cast<const unsigned char*>(dout_tiles);
@@ -654,7 +796,7 @@ cudaError_t launch_mlp_dw_tc(void* const* dz, void* const* h, const void* x0_til
     k_mlp_dw_tc<<<jobs, DW_THREADS, DW_SMEM, st>>>(a);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    const uint32_t n_out = 3 * MLP_HID * MLP_HID + 2 * MLP_HID * MLP_IN_PAD + 4 * MLP_HID;
+    const uint32_t n_out = 3 * MLP_HID * MLP_HID + 2 * MLP_HID * MLP_IN_PAD + 4 * MLP_HID + MLP_OUT_PAD;
     k_mlp_dw_reduce<<<(n_out + 255) / 256, 256, 0, st>>>(part, jobs_heavy, jobs_light, grad);
     return cudaGetLastError();
 }

@@ -60,7 +60,7 @@ struct mgk_surrogate {
     // the weight-gradient partials; off (the mma.sync GEMMs of mlp.cu) when
     // MGK_SURROGATE_TRAIN=mma was set at creation
     bool train_tc = true;
-    void *tx0 = nullptr, *tZ[4] = {}, *tH[4] = {}, *tdZ[4] = {}, *tdout = nullptr;
+    void *tx0 = nullptr, *tZ[4] = {}, *tdZ[4] = {}, *tdout = nullptr;
     float* dw_part = nullptr;
     uint32_t dw_heavy = 0, dw_light = 0;
     __nv_bfloat16 *x0 = nullptr, *Z[4] = {}, *H[4] = {}, *dza = nullptr, *dzb = nullptr, *dout = nullptr;
@@ -122,7 +122,6 @@ mgk_result ensure_train_buffers(mgk_surrogate* s, int B) {
         TRY(dalloc(s, &s->tx0, size_t(B) * MLP_IN_PAD * 2));
         for (int l = 0; l < 4; ++l) {
             TRY(dalloc(s, &s->tZ[l], act));
-            TRY(dalloc(s, &s->tH[l], act));
             TRY(dalloc(s, &s->tdZ[l], act));
         }
         TRY(dalloc(s, &s->tdout, size_t(B) * MLP_OUT_PAD * 2));
@@ -190,11 +189,11 @@ cudaError_t forward(mgk_surrogate* s, const __nv_bfloat16* x0, int B, __nv_bfloa
 }
 
 // One gradient of the batch rows perm[b0 .. b0 + B) on the tensor-core
-// path: gather, forward with stash, loss, input gradients, weight gradients
-// (all of grad is written); the batch mean loss is added to *loss_acc.
+// path: gather, forward with stash and loss, input gradients, weight
+// gradients (all of grad is written); the batch mean loss is added to
+// *loss_acc.
 cudaError_t gradient_tc(mgk_surrogate* s, const float* feat, const mgk_sample_label* lab, int b0, int B,
                         const LossWeights& w, float* loss_acc, cudaStream_t st) {
-    const Layout& L = s->L;
     const uint32_t tiles = uint32_t(B) / 128u;
     cudaError_t e = launch_gather_tiled(feat, lab, s->perm, b0, B, s->tx0, s->blab, st);
     if (e == cudaSuccess && !s->img_valid) {
@@ -202,15 +201,12 @@ cudaError_t gradient_tc(mgk_surrogate* s, const float* feat, const mgk_sample_la
         s->img_valid = e == cudaSuccess;
     }
     if (e == cudaSuccess)
-        e = launch_mlp_fwd_stash_tc(s->img, s->p, s->tx0, s->tZ, s->tH, s->out, tiles, s->status, s->sm_count, st);
-    if (e == cudaSuccess) e = launch_loss_tiled(s->out, s->blab, B, w, s->tdout, s->dout32, loss_acc, st);
+        e = launch_mlp_fwd_stash_tc(s->img, s->p, s->tx0, s->tZ, nullptr, s->blab, w, s->tdout, loss_acc, tiles,
+                                    s->status, s->sm_count, st);
     if (e == cudaSuccess) e = launch_mlp_bwd_dx_tc(s->img, s->tdout, s->tZ, s->tdZ, tiles, s->status, s->sm_count, st);
     if (e == cudaSuccess)
-        e = launch_mlp_dw_tc(s->tdZ, s->tH, s->tx0, s->tdout, s->dw_part, s->grad, tiles, s->dw_heavy, s->dw_light,
+        e = launch_mlp_dw_tc(s->tdZ, s->tZ, s->tx0, s->tdout, s->dw_part, s->grad, tiles, s->dw_heavy, s->dw_light,
                              s->status, st);
-    // the output bias gradient from the FP32 output gradient
-    if (e == cudaSuccess) e = cudaMemsetAsync(s->grad + L.b[4], 0, MLP_OUT_PAD * sizeof(float), st);
-    if (e == cudaSuccess) e = launch_colsum_f32(s->dout32, B, MLP_OUT_PAD, s->grad + L.b[4], st);
     return e;
 }
 
