@@ -33,7 +33,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-# DRAM bytes per ray of k_integrate and per row of k_mlp_infer_tc, from one
+# DRAM bytes per ray of k_integrate and per row of the fused inference, from one
 # ncu capture each of a smaller case (640x360x16 rays; 2^20 rows); the
 # traffic grows with the units, so the roofline scales it to the launch.
 INTEGRATE_DRAM_BYTES_PER_RAY = 617.4e6 / 3_686_400
@@ -67,8 +67,8 @@ def parse_args():
     ap.add_argument("--stress-spp", type=int, default=64)
     ap.add_argument("--c5-spp", type=int, default=256,
                     help="samples per pixel of the 3840x2160 surrogate render (0 skips it)")
-    ap.add_argument("--train-only", action="store_true",
-                    help="time only the surrogate training loop (for profiling its kernels)")
+    ap.add_argument("--surrogate-kernels", action="store_true",
+                    help="time only the surrogate's training loop and fused inference (for profiling their kernels)")
     return ap.parse_args()
 
 
@@ -379,7 +379,7 @@ def run_surrogate(args, ctx, s, d_stars, d_w, film_mixed_ms, steps):
                      "flop_count": "3 x 400,896 FLOP per sample per step (forward, input and weight gradients)",
                      "distribution": "observer r U[10,100] M, inclination U[0,90] deg, spin U[0,0.998] "
                                      "(16 launches), directions uniform on the forward hemisphere"},
-        "inference_roofline": {"bound": "tensor", "kernel": "k_mlp_infer_tc (tcgen05, fused 5 layers)",
+        "inference_roofline": {"bound": "tensor", "kernel": "k_mlp_chain_tc<INFER> (tcgen05, fused 5 layers)",
                                "achieved": fwd_tflops, "peak": bf16_peak, "unit": "TFLOP/s",
                                "frac": (fwd_tflops / bf16_peak) if bf16_peak else None,
                                "traffic": MLP_DRAM_BYTES_PER_ROW * n_rows,
@@ -388,11 +388,13 @@ def run_surrogate(args, ctx, s, d_stars, d_w, film_mixed_ms, steps):
     }
 
 
-def run_train_only(args, device):
-    """The surrogate training loop alone: --surrogate-samples FP64-labelled
-    samples of the training distribution, one warm-up epoch, then
-    --surrogate-epochs timed epochs at batch 65536 on the default tcgen05 path.
-    Prints the training FLOP rate (3 x 400,896 FLOP per sample per step)."""
+def run_surrogate_kernels(args, device):
+    """The surrogate's kernels alone: the training loop on
+    --surrogate-samples FP64-labelled samples of the training distribution
+    (one warm-up epoch, then --surrogate-epochs timed epochs at batch 65536 on
+    the default tcgen05 path; 3 x 400,896 FLOP per sample per step), then the
+    fused inference on 2^22 rows of the same samples (400,896 FLOP per row,
+    CUDA events over 5 launches after one)."""
     import torch
     import magik_b200 as M
     torch.cuda.set_device(device)
@@ -407,13 +409,25 @@ def run_train_only(args, device):
         losses = net.train(cfg, feat, lab)
         torch.cuda.synchronize()
         dt = time.time() - t0
+        x = feat[: min(1 << 22, feat.shape[0])].contiguous()
+        net.forward(x)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(5):
+            net.forward(x)
+        e1.record()
+        e1.synchronize()
+        infer_ms = e0.elapsed_time(e1) / 5
         assert net.status() == 0
         net.close()
     steps = args.surrogate_epochs * (args.surrogate_samples // cfg.batch)
     return {"metric": "surrogate training FLOP/s", "value": steps * cfg.batch * 3 * 400_896 / dt / 1e12,
             "unit": "TFLOP/s", "higher_is_better": True, "steps": steps, "us_per_step": dt / steps * 1e6,
             "batch": cfg.batch, "samples": args.surrogate_samples, "epochs": args.surrogate_epochs,
-            "final_loss": float(losses[-1]), "dtype": "bf16", "data": "synthetic"}
+            "final_loss": float(losses[-1]), "dtype": "bf16", "data": "synthetic",
+            "inference": {"rows": int(x.shape[0]), "ms": infer_ms,
+                          "tflops": int(x.shape[0]) * 400_896 / (infer_ms * 1e-3) / 1e12}}
 
 
 def run_config5(args, ctx, net, d_stars, d_w):
@@ -782,8 +796,8 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
-    if args.train_only:
-        print(json.dumps(run_train_only(args, local_rank)), flush=True)
+    if args.surrogate_kernels:
+        print(json.dumps(run_surrogate_kernels(args, local_rank)), flush=True)
         return 0
     if args.impl == "reference":
         out = run_reference(args, rank, world)

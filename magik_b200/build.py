@@ -18,7 +18,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmgk.so")
 SOURCES = ["kernels.cu", "api.cu", "static_scratch.cu", "mlp.cu", "mlp_tc.cu", "mlp_train_tc.cu", "surrogate.cu", "display.cu",
            "manager.cu"]
-HEADERS = ["dev_physics.cuh", "dev_pair.cuh", "dev_scene.cuh", "internal.h", "cie1931_2deg.inc", "mlp.h", "mlp_loss.cuh", "tc_sm100.cuh",
+HEADERS = ["dev_physics.cuh", "dev_pair.cuh", "dev_scene.cuh", "internal.h", "cie1931_2deg.inc", "mlp.h", "mlp_loss.cuh", "mlp_act.cuh", "tc_sm100.cuh",
            os.path.join("..", "src", "renderer", "relativity", "metric.cuh"),
            os.path.join("..", "src", "renderer", "relativity", "metric_kerr.cuh"),
            os.path.join("..", "src", "renderer", "relativity", "metric_schwarzschild.cuh"),

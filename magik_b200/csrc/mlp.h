@@ -79,13 +79,19 @@ __host__ __device__ constexpr uint32_t mlp_chunk_offset(int c) {
 __host__ __device__ constexpr uint32_t mlp_chunk_bytes(int c) { return (c == 0 || c == 13) ? 8192u : 32768u; }
 constexpr uint32_t MLP_IMAGE_BYTES = 8192u + 12u * 32768u + 8192u;
 
-// Fused tensor-core inference (mlp_tc.cu).
+// Fused tensor-core inference and the training chains (mlp_tc.cu).
 size_t mlp_image_bytes();
-cudaError_t launch_weight_image(const __nv_bfloat16* wb, void* img, cudaStream_t st);
+// The transposed image of the backward chain: W5^T (256 x 16, 8-row stride
+// 256 B), then W4^T, W3^T, W2^T in slices of 64 output columns (chunks 1-12
+// of the same offsets and shapes), halved like the forward image.
+size_t mlp_t_image_bytes();
+// Both images from the BF16 weights (img_t may be null).
+cudaError_t launch_weight_image(const __nv_bfloat16* wb, void* img, void* img_t, cudaStream_t st);
 cudaError_t launch_mlp_infer_tc(const float* feat, uint32_t n, const void* img, const float* params, float* out,
                                 uint32_t* status, int sm_count, cudaStream_t st);
 
-// Tensor-core training (mlp_train_tc.cu) on tiled activations: 128-row tiles
+// Tensor-core training (chains: mlp_tc.cu; weight gradients: mlp_train_tc.cu)
+// on tiled activations: 128-row tiles
 // in the operand layout (element (row, col) of tile t at
 // t * 256 * C + kmaj(row % 128, col, 16 C) bytes for C columns).
 // Forward with stash of Z_1..Z_4; with labels (lab non-null) also the loss
@@ -95,15 +101,21 @@ cudaError_t launch_mlp_fwd_stash_tc(const void* img, const float* params, const 
                                     float* out, const SampleLabel* lab, const LossWeights& w, void* dout_tiles,
                                     float* loss_acc, uint32_t n_tiles, uint32_t* status, int sm_count,
                                     cudaStream_t st);
-cudaError_t launch_mlp_bwd_dx_tc(const void* img, const void* dout_tiles, void* const* z, void* const* dz,
+cudaError_t launch_mlp_bwd_dx_tc(const void* img_t, const void* dout_tiles, void* const* z, void* const* dz,
                                  uint32_t n_tiles, uint32_t* status, int sm_count, cudaStream_t st);
-void mlp_dw_jobs(uint32_t n_tiles, int sm_count, uint32_t* heavy, uint32_t* light);
+// The weight-gradient kernel's CTAs: `heavy` per layer of W2..W4, `l0` for
+// W1 and b1, `l4` for W5 and b5, each job a contiguous range of batch tiles.
+struct DwJobs {
+    uint32_t heavy, l0, l4;
+    __host__ __device__ uint32_t total() const { return 3 * heavy + l0 + l4; }
+};
+DwJobs mlp_dw_jobs(uint32_t n_tiles, int sm_count);
 size_t mlp_dw_partial_floats(uint32_t jobs);
 // Weight and bias gradients (all of W1..W5, b1..b5) from dZ_1..dZ_4, Z_1..Z_4,
 // X0 and dOut.
 cudaError_t launch_mlp_dw_tc(void* const* dz, void* const* z, const void* x0_tiles, const void* dout_tiles,
-                             float* part, float* grad, uint32_t n_tiles, uint32_t jobs_heavy, uint32_t jobs_light,
-                             uint32_t* status, cudaStream_t st);
+                             float* part, float* grad, uint32_t n_tiles, const DwJobs& jobs, uint32_t* status,
+                             cudaStream_t st);
 // The sample-set order of one epoch (a keyed permutation of [0, n)) on the
 // device (mlp.cu).
 cudaError_t launch_epoch_perm(uint32_t* perm, uint32_t n, const uint32_t key[4], cudaStream_t st);

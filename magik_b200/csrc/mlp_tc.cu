@@ -1,35 +1,51 @@
-// Fused inference of the deflection surrogate on the 5th-generation tensor
-// cores: all five layers of a tile of 128 rows run in one CTA, accumulators
-// in tensor memory, activations resident in shared memory between layers.
-// Each CTA keeps two tiles in flight (buffers 0 and 1, two 256-column TMEM
-// accumulators) so that the epilogue of one tile overlaps the MMAs of the
-// other.
+// The layer chains of the deflection surrogate on the 5th-generation tensor
+// cores: all layers of a 128-row tile run in one CTA, accumulators in tensor
+// memory, activations resident in shared memory between layers.  One kernel
+// template, three chains:
 //
-//  warp 0      producer: streams the weight image in chunks of at most 32 KB
-//              into a 2-slot shared-memory ring (cp.async.bulk + mbarrier
-//              transaction counts), in the order the MMA warp consumes them.
-//  warp 1      allocates 512 TMEM columns; lane 0 issues tcgen05.mma
-//              (M = 128, K = 16 per instruction, N = 256 or 16), layer by
-//              layer alternating between the two tiles, and commits each
-//              chunk to its slot's "empty" barrier and each layer to the
-//              tile's "d_ready" barrier.
-//  warps 2..9  epilogue of buffer 0, warps 10..17 of buffer 1: tcgen05.ld
-//              of the accumulator (warp w reads TMEM lanes 32 (w % 4) ..;
-//              the first four warps of a buffer columns 0-127, the other four
-//              128-255), bias + SiLU, BF16 back into the tile's activations,
-//              or the 16 FP32 outputs of the last layer to global memory.
+//  INFER  inference: features (FP32) in, the 16 FP32 outputs out.
+//  FWD    training forward: X0 tiles in; the pre-activations Z_1..Z_4 to the
+//         stash, then each row's loss (mlp_loss.cuh) and the BF16 output
+//         gradient dOut / B; the FP32 outputs only where asked for.
+//  BWD    training input gradients: dOut tiles in;
+//         dZ4 = (dOut W5) * silu'(Z4), dZ3 = (dZ4 W4) * silu'(Z3), ... dZ1.
 //
-// SiLU is evaluated as u (1 + tanh u) with u = z / 2, on pairs of values in
-// BF16x2 (one tanh.approx.bf16x2 and one fma.rn.bf16x2 per pair, u rounded
-// to BF16 first: about one BF16 ulp of extra error on the activations).  The image holds the weights of the four SiLU layers halved (exact
-// in BF16) and the biases are staged halved, so u = accumulator + bias.
+// Each CTA is persistent (at most one per SM) and keeps two tiles in flight
+// (buffers 0 and 1, two 256-column TMEM accumulators), so the epilogue of one
+// overlaps the MMAs of the other.
+//
+//  warp 0       producer: streams the weight image in chunks of at most
+//               32 KB into a 3-slot shared-memory ring (cp.async.bulk +
+//               mbarrier transaction counts), in the order the MMA warp
+//               consumes them.  BWD: it also prefetches each step's Z tile
+//               into L2 a step ahead.
+//  warp 1       allocates 512 TMEM columns; lane 0 issues tcgen05.mma
+//               (M = 128, K = 16 per instruction, N = 256 or 16), step by
+//               step alternating between the two tiles, and commits each
+//               chunk to its slot's "empty" barrier and each step to the
+//               tile's "d_ready" barrier.
+//  warps 2..17  epilogue: all 16 warps take every step, in the MMA's order.
+//               Warp w reads TMEM lanes 32 (w % 4) .. (the rows of its lane
+//               quarter) and 64 of the 256 columns ((w - 2) / 4); the output
+//               layer's 16 columns go to the first four warps, and the next
+//               tile's input is loaded by the second four meanwhile.
+//
+// Weights: the image (mlp_chunk_offset, mlp.h) holds W1..W5 K-major for the
+// forward; the transposed image holds W5^T, W4^T, W3^T, W2^T K-major for the
+// backward, so both chains issue the same N = 256 MMAs.  Layers followed by
+// SiLU are stored halved (exact in BF16): the accumulator is z / 2 - b / 2.
+//
+// SiLU: INFER evaluates u (1 + tanh u), u = z / 2, in BF16x2 (one
+// tanh.approx.bf16x2 and one fma.rn.bf16x2 per pair, u rounded to BF16
+// first: about one BF16 ulp of extra error on the activations); FWD and BWD
+// in FP32 with tanh.approx.f32 (mlp_act.cuh), rounded to BF16 where stored.
 //
 // Operand layout in shared memory (both operands K-major, no swizzle): the
 // canonical 8 x 16-byte core matrices, element (row, k) of a tile at
 //   (row / 8) * SBO + (k / 8) * 128 + (row % 8) * 16 + (k % 8) * 2,
 // so a K step of 16 advances the descriptor start by 256 bytes.  The weight
-// image in global memory is stored chunk by chunk in exactly this layout, so
-// each chunk is one contiguous bulk copy.
+// images and the activation tiles in global memory are stored in exactly
+// this layout, so each chunk or tile is one contiguous bulk copy.
 //
 // Every wait on an mbarrier is bounded; on a timeout the kernel sets bit 1 of
 // *status, lets the other roles leave their loops, waits (bounded) for its
@@ -39,115 +55,158 @@
 #include <cuda_runtime.h>
 
 #include "mlp.h"
+#include "mlp_act.cuh"
+#include "mlp_loss.cuh"
 #include "tc_sm100.cuh"
 
 namespace mgk {
 namespace {
 
 using namespace tc;
+using namespace act;
 
-constexpr int TM = 128;                   // rows per tile
-// A bulk copy costs about the same time whatever its size up to 32 KB, so the
-// ring uses few large slots rather than many small ones.
-constexpr int N_SLOT = 2;
+constexpr int N_SLOT = 3;
 constexpr uint32_t SLOT_BYTES = 32768;
-constexpr uint32_t A_BYTES = TM * MLP_HID * 2;  // 64 KB activation tile
-constexpr uint32_t A_SBO = 4096;                // 8-row group stride of the activation tile
-constexpr int N_CHUNKS = MLP_IMAGE_CHUNKS;      // W1, W2 x4, W3 x4, W4 x4, W5
-constexpr int EPI_WARPS = 16;                   // 8 per buffer
+constexpr int EPI_WARPS = 16;
 constexpr int THREADS = 32 * (2 + EPI_WARPS);
 constexpr uint32_t TMEM_COLS = 512;             // two 256-column accumulators
+constexpr uint32_t IMAGE_BYTES = MLP_IMAGE_BYTES;
+constexpr uint32_t T_IMAGE_BYTES = 8192u + 12u * 32768u;  // W5^T, then W4^T, W3^T, W2^T in 64-column slices
 
 // Shared-memory map (dynamic, offsets from a 128-byte aligned base).
-constexpr uint32_t OFF_A = 0;                                // two activation tiles
-constexpr uint32_t OFF_W = OFF_A + 2 * A_BYTES;              // weight ring
-constexpr uint32_t OFF_BIAS = OFF_W + N_SLOT * SLOT_BYTES;   // b1..b4 halved, b5
-constexpr uint32_t N_BIAS = 4 * MLP_HID + MLP_OUT_PAD;
-constexpr uint32_t OFF_BAR = OFF_BIAS + N_BIAS * 4;          // full[2], empty[2], d_ready[2], a_ready[2], drain
-constexpr uint32_t OFF_MISC = OFF_BAR + 16 * 8;              // tmem base, abort flag
+constexpr uint32_t OFF_A = 0;                               // two activation tiles
+constexpr uint32_t OFF_W = OFF_A + 2 * A_BYTES;             // weight ring
+constexpr uint32_t OFF_BAR = OFF_W + N_SLOT * SLOT_BYTES;   // full[3], empty[3], d_ready[2], a_ready[2], drain
+constexpr uint32_t OFF_MISC = OFF_BAR + 16 * 8;             // tmem base, abort flag
 static_assert(2 * N_SLOT + 5 <= 16, "barrier area");
-constexpr uint32_t SMEM_BYTES = OFF_MISC + 16 + 128;         // + alignment slack
+constexpr uint32_t SMEM_BYTES = OFF_MISC + 16 + 128;        // + alignment slack
 static_assert(SMEM_BYTES <= 232448, "shared memory");
 
-// Chunk c of the weight image (mlp.h): byte offset and size.
-__host__ __device__ constexpr uint32_t chunk_offset(int c) { return mlp_chunk_offset(c); }
-__host__ __device__ constexpr uint32_t chunk_bytes(int c) { return mlp_chunk_bytes(c); }
-constexpr uint32_t IMAGE_BYTES = MLP_IMAGE_BYTES;
-
-// silu of a pair with u = z / 2:  z sigmoid(z) = u (1 + tanh u), in BF16x2.
-__device__ __forceinline__ uint32_t silu_half_pair(float u0, float u1) {
-    const uint32_t u = pack_bf16(u0, u1);
-    uint32_t t, h;
-    asm("tanh.approx.bf16x2 %0, %1;" : "=r"(t) : "r"(u));
-    asm("fma.rn.bf16x2 %0, %1, %2, %1;" : "=r"(h) : "r"(u), "r"(t));
-    return h;
-}
-
-// Bias + SiLU of 32 accumulator columns of one row into the activation tile.
-__device__ __forceinline__ void epilogue_block(const uint32_t (&v)[32], const float* hb, unsigned char* dst0) {
-#pragma unroll
-    for (int g = 0; g < 4; ++g) {
-        uint32_t pk[4];
-#pragma unroll
-        for (int e = 0; e < 4; e += 2) {
-            const int c = g * 8 + 2 * e;
-            const float4 bb = *reinterpret_cast<const float4*>(hb + c);
-            pk[e] = silu_half_pair(__uint_as_float(v[c]) + bb.x, __uint_as_float(v[c + 1]) + bb.y);
-            pk[e + 1] = silu_half_pair(__uint_as_float(v[c + 2]) + bb.z, __uint_as_float(v[c + 3]) + bb.w);
-        }
-        *reinterpret_cast<uint4*>(dst0 + g * 128) = uint4{pk[0], pk[1], pk[2], pk[3]};
-    }
-}
-
+enum { INFER = 0, FWD = 1, BWD = 2 };
 
 }  // namespace
 
-// Weight image for the fused kernel from the BF16 parameter copy (offsets of
-// the flat parameter vector, weights [out][in]).
-__global__ void k_weight_image(const __nv_bfloat16* __restrict__ wb, unsigned char* __restrict__ img) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;  // one BF16 element of the image
-    if (i >= IMAGE_BYTES / 2) return;
+// The two weight images from the BF16 parameter copy (weights [out][in]):
+// element i < IMAGE_BYTES / 2 of the forward image, the rest of the
+// transposed image (img_t may be null: then only the forward image).
+__global__ void k_weight_image(const __nv_bfloat16* __restrict__ wb, unsigned char* __restrict__ img,
+                               unsigned char* __restrict__ img_t) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;  // one BF16 element of an image
+    const bool tr = i >= IMAGE_BYTES / 2;
+    if (tr) {
+        i -= IMAGE_BYTES / 2;
+        if (img_t == nullptr || i >= T_IMAGE_BYTES / 2) return;
+    }
     const uint32_t byte = i * 2;
     int c = 0;
-    while (c < N_CHUNKS - 1 && byte >= chunk_offset(c + 1)) ++c;
-    const uint32_t o = byte - chunk_offset(c);
-    // invert kmaj for the chunk's shape
+    while (c < MLP_IMAGE_CHUNKS - 1 && byte >= mlp_chunk_offset(c + 1)) ++c;
+    const uint32_t o = byte - mlp_chunk_offset(c);
+    // invert kmaj for the chunk's shape: (row, k) of a K-major chunk
     uint32_t sbo, layer, k_base;
-    if (c == 0) { sbo = 256; layer = 0; k_base = 0; }
-    else if (c == 13) { sbo = 4096; layer = 4; k_base = 0; }
-    else { sbo = 1024; layer = 1 + (c - 1) / 4; k_base = 64 * ((c - 1) % 4); }
+    if (!tr) {
+        if (c == 0) { sbo = 256; layer = 0; k_base = 0; }
+        else if (c == 13) { sbo = 4096; layer = 4; k_base = 0; }
+        else { sbo = 1024; layer = 1 + (c - 1) / 4; k_base = 64 * ((c - 1) % 4); }
+    } else {
+        if (c == 0) { sbo = 256; layer = 4; k_base = 0; }
+        else { sbo = 1024; layer = 3 - (c - 1) / 4; k_base = 64 * ((c - 1) % 4); }
+    }
     const uint32_t grp = o / sbo, rem = o % sbo;
     const uint32_t kc = rem / 128, r2 = rem % 128;
     const uint32_t row = grp * 8 + r2 / 16, k = kc * 8 + (r2 % 16) / 2;
     const uint32_t in_dim = layer == 0 ? MLP_IN_PAD : MLP_HID;
-    const __nv_bfloat16 w = wb[mlp_w_off(int(layer)) + size_t(row) * in_dim + k_base + k];
+    // forward: row = output, k = input; transposed: row = input, k = output
+    const size_t e = tr ? size_t(k_base + k) * in_dim + row : size_t(row) * in_dim + k_base + k;
+    const __nv_bfloat16 w = wb[mlp_w_off(int(layer)) + e];
     // layers followed by SiLU are stored halved (exact: a power-of-two scale)
-    reinterpret_cast<__nv_bfloat16*>(img)[i] = layer < 4 ? __hmul(w, __float2bfloat16(0.5f)) : w;
+    const __nv_bfloat16 v = layer < 4 ? __hmul(w, __float2bfloat16(0.5f)) : w;
+    reinterpret_cast<__nv_bfloat16*>(tr ? img_t : img)[i] = v;
 }
 
-__global__ void __launch_bounds__(THREADS, 1)
-    k_mlp_infer_tc(const float* __restrict__ feat, uint32_t n, const unsigned char* __restrict__ img,
-                   const float* __restrict__ params, float* __restrict__ out, uint32_t* status) {
+namespace {
+
+struct ChainArgs {
+    const unsigned char* img;  // weight image (BWD: the transposed image)
+    const float* params;       // FP32 parameters (biases)
+    const float* feat;         // INFER: features [n_rows][7]
+    const unsigned char* in;   // FWD: X0 tiles; BWD: dOut tiles (16 columns)
+    unsigned char* z[4];       // Z_1..Z_4 tiles (FWD writes, BWD reads)
+    unsigned char* dz[4];      // BWD: dZ_1..dZ_4 tiles (written)
+    float* out;                // INFER, FWD: outputs [rows][16] FP32 (FWD: may be null)
+    const SampleLabel* lab;    // FWD: the batch's labels for the fused loss (may be null)
+    unsigned char* dout;       // FWD: dOut tiles, d(loss)/d(out) / B in BF16
+    float* loss_acc;           // FWD: += the batch's mean loss
+    LossWeights w;
+    uint32_t n_rows;
+    uint32_t n_tiles;
+    uint32_t* status;
+};
+
+// Step l of a tile: its weight chunks and the shape of their MMAs.  The
+// backward's steps (W5^T, W4^T, W3^T, W2^T of the transposed image) have the
+// forward's first four shapes.
+struct Step {
+    int c0, nc;      // first chunk, number of chunks
+    int ksteps;      // K steps of 16 per chunk
+    uint32_t n;      // MMA N
+    uint32_t b_sbo;  // 8-row stride of the chunk
+};
+__device__ __forceinline__ Step step_of(int l) {
+    if (l == 0) return Step{0, 1, 1, 256u, 256u};
+    if (l == 4) return Step{13, 1, 16, 16u, 4096u};
+    return Step{1 + 4 * (l - 1), 4, 4, 256u, 1024u};
+}
+
+// Epilogue of 32 accumulator columns of one row of a hidden layer: bias and
+// SiLU into the next step's operand (8-column groups 128 bytes apart from
+// `a`); FWD: Z to the stash at `zs` (null for the empty tile).
+template <int DIR>
+__device__ __forceinline__ void hidden_block(const uint32_t (&v)[32], const float* bl, unsigned char* a,
+                                             unsigned char* zs) {
+#pragma unroll
+    for (int gq = 0; gq < 4; ++gq) {
+        const float4 b0 = __ldg(reinterpret_cast<const float4*>(bl + gq * 8));
+        const float4 b1 = __ldg(reinterpret_cast<const float4*>(bl + gq * 8 + 4));
+        const float bb[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+        uint32_t hv[4], zv[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const int c = gq * 8 + 2 * e;
+            if constexpr (DIR == INFER) {
+                hv[e] = silu_half_pair(__uint_as_float(v[c]) + 0.5f * bb[2 * e],
+                                       __uint_as_float(v[c + 1]) + 0.5f * bb[2 * e + 1]);
+                zv[e] = 0u;
+            } else {
+                const float z0 = 2.0f * __uint_as_float(v[c]) + bb[2 * e];
+                const float z1 = 2.0f * __uint_as_float(v[c + 1]) + bb[2 * e + 1];
+                zv[e] = pack_bf16(z0, z1);
+                hv[e] = pack_bf16(silu_f(z0), silu_f(z1));
+            }
+        }
+        *reinterpret_cast<uint4*>(a + gq * 128) = uint4{hv[0], hv[1], hv[2], hv[3]};
+        if constexpr (DIR == FWD) {
+            if (zs) *reinterpret_cast<uint4*>(zs + gq * 128) = uint4{zv[0], zv[1], zv[2], zv[3]};
+        }
+    }
+}
+
+template <int DIR>
+__global__ void __launch_bounds__(THREADS, 1) k_mlp_chain_tc(ChainArgs g) {
+    constexpr int S = DIR == BWD ? MLP_LAYERS - 1 : MLP_LAYERS;  // steps per tile
     extern __shared__ unsigned char smem_raw[];
     unsigned char* smem =
         reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
     const uint32_t sbase = smem_addr(smem);
     const uint32_t bar_full = sbase + OFF_BAR, bar_empty = bar_full + N_SLOT * 8;
-    const uint32_t bar_d = bar_full + 2 * N_SLOT * 8, bar_a = bar_d + 2 * 8, bar_drain = bar_a + 2 * 8;
-    float* bias = reinterpret_cast<float*>(smem + OFF_BIAS);
+    const uint32_t bar_d = bar_empty + N_SLOT * 8, bar_a = bar_d + 2 * 8, bar_drain = bar_a + 2 * 8;
     volatile uint32_t* tmem_slot = reinterpret_cast<volatile uint32_t*>(smem + OFF_MISC);
     volatile uint32_t* abort_flag = reinterpret_cast<volatile uint32_t*>(smem + OFF_MISC + 4);
 
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t n_tiles = (n + TM - 1) / TM;
+    const uint32_t n_tiles = g.n_tiles;
     const uint32_t my_tiles = blockIdx.x < n_tiles ? (n_tiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
     const uint32_t my_pairs = (my_tiles + 1) / 2;  // an odd count ends with an empty tile in buffer 1
 
-    for (uint32_t i = threadIdx.x; i < N_BIAS; i += THREADS) {
-        const int l = i < 4 * MLP_HID ? int(i / MLP_HID) : 4;
-        const uint32_t k = i < 4 * MLP_HID ? i % MLP_HID : i - 4 * MLP_HID;
-        bias[i] = l < 4 ? 0.5f * params[mlp_b_off(l) + k] : params[mlp_b_off(l) + k];
-    }
     if (threadIdx.x == 0) {
         for (int s = 0; s < N_SLOT; ++s) {
             mbar_init(bar_full + 8 * s, 1);
@@ -155,7 +214,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         }
         for (int b = 0; b < 2; ++b) {
             mbar_init(bar_d + 8 * b, 1);
-            mbar_init(bar_a + 8 * b, 32 * EPI_WARPS / 2);
+            mbar_init(bar_a + 8 * b, 32 * EPI_WARPS);
         }
         mbar_init(bar_drain, 1);
         *abort_flag = 0u;
@@ -174,24 +233,32 @@ __global__ void __launch_bounds__(THREADS, 1)
 
     if (warp == 0) {
         // ------------------------------------------------------------ producer
-        // chunk order: per tile pair, per layer, per buffer, the layer's chunks
+        // chunk order: per tile pair, per step, per buffer, the step's chunks
         if (lane == 0) {
             uint32_t j = 0;
             bool ok = true;
             for (uint32_t p = 0; p < my_pairs && ok; ++p)
-                for (int l = 0; l < MLP_LAYERS && ok; ++l)
-                    for (int b = 0; b < 2 && ok; ++b) {
-                        const int c0 = l == 0 ? 0 : (l == 4 ? 13 : 1 + 4 * (l - 1));
-                        const int nc = (l == 0 || l == 4) ? 1 : 4;
-                        for (int ci = 0; ci < nc; ++ci, ++j) {
+                for (int l = 0; l < S && ok; ++l)
+                    for (uint32_t b = 0; b < 2 && ok; ++b) {
+                        const Step st = step_of(l);
+                        if constexpr (DIR == BWD) {
+                            // the Z tiles the epilogue reads for silu', one step ahead, into L2
+                            const uint32_t tile = blockIdx.x + (2 * p + b) * gridDim.x;
+                            if (tile < n_tiles) {
+                                if (l == 0) bulk_prefetch_l2(g.z[3] + size_t(tile) * A_BYTES, A_BYTES);
+                                const unsigned char* zn = l == 0 ? g.z[2] : (l == 1 ? g.z[1] : g.z[0]);
+                                if (l + 1 < S) bulk_prefetch_l2(zn + size_t(tile) * A_BYTES, A_BYTES);
+                            }
+                        }
+                        for (int ci = 0; ci < st.nc; ++ci, ++j) {
                             const uint32_t s = j % N_SLOT, use = j / N_SLOT;
                             if (use > 0 && !mbar_wait(bar_empty + 8 * s, (use - 1) & 1u, abort_flag)) {
                                 ok = false;
                                 break;
                             }
-                            const int c = c0 + ci;
-                            mbar_expect_tx(bar_full + 8 * s, chunk_bytes(c));
-                            bulk_g2s(sbase + OFF_W + s * SLOT_BYTES, img + chunk_offset(c), chunk_bytes(c),
+                            const int c = st.c0 + ci;
+                            mbar_expect_tx(bar_full + 8 * s, mlp_chunk_bytes(c));
+                            bulk_g2s(sbase + OFF_W + s * SLOT_BYTES, g.img + mlp_chunk_offset(c), mlp_chunk_bytes(c),
                                      bar_full + 8 * s);
                         }
                     }
@@ -208,26 +275,24 @@ __global__ void __launch_bounds__(THREADS, 1)
             uint32_t j = 0, ar[2] = {0u, 0u};
             bool ok = true;
             for (uint32_t p = 0; p < my_pairs && ok; ++p)
-                for (int l = 0; l < MLP_LAYERS && ok; ++l)
+                for (int l = 0; l < S && ok; ++l)
                     for (uint32_t b = 0; b < 2 && ok; ++b) {
                         if (!mbar_wait(bar_a + 8 * b, ar[b] & 1u, abort_flag)) { ok = false; break; }
                         ++ar[b];
                         tc_fence_after();
-                        const int nc = (l == 0 || l == 4) ? 1 : 4;
-                        const uint32_t idesc = idesc_bf16(TM, l == 4 ? MLP_OUT_PAD : MLP_HID);
-                        const uint32_t b_sbo = l == 0 ? 256u : (l == 4 ? 4096u : 1024u);
-                        const int ksteps = l == 0 ? 1 : (l == 4 ? 16 : 4);
+                        const Step st = step_of(l);
+                        const uint32_t idesc = idesc_bf16(TM, st.n);
                         const uint32_t a_base = sbase + OFF_A + b * A_BYTES;
                         const uint32_t d = tmem + b * 256u;
-                        for (int ci = 0; ci < nc; ++ci, ++j) {
+                        for (int ci = 0; ci < st.nc; ++ci, ++j) {
                             const uint32_t s = j % N_SLOT, use = j / N_SLOT;
                             if (!mbar_wait(bar_full + 8 * s, use & 1u, abort_flag)) { ok = false; break; }
                             tc_fence_after();
                             const uint32_t wslot = sbase + OFF_W + s * SLOT_BYTES;
-                            for (int ks = 0; ks < ksteps; ++ks) {
-                                const uint32_t kk = uint32_t(ci * ksteps + ks);  // K step within the layer
+                            for (int ks = 0; ks < st.ksteps; ++ks) {
+                                const uint32_t kk = uint32_t(ci * st.ksteps + ks);  // K step within the layer
                                 const uint64_t a = smem_desc(a_base + kk * 256u, 128u, A_SBO);
-                                const uint64_t bd = smem_desc(wslot + uint32_t(ks) * 256u, 128u, b_sbo);
+                                const uint64_t bd = smem_desc(wslot + uint32_t(ks) * 256u, 128u, st.b_sbo);
                                 mma_bf16_ss(d, a, bd, idesc, kk > 0 ? 1u : 0u);
                             }
                             mma_commit(bar_empty + 8 * s);
@@ -240,102 +305,248 @@ __global__ void __launch_bounds__(THREADS, 1)
         }
     } else {
         // ------------------------------------------------------------ epilogue
-        const uint32_t buf = (warp - 2) >> 3, q = warp & 3u, half = ((warp - 2) >> 2) & 1u;
+        const uint32_t ew = warp - 2, q = warp & 3u, cq = ew >> 2;  // lane quarter, column quarter
         const uint32_t row = q * 32 + lane;
-        const uint32_t t_lane = tmem + ((q * 32u) << 16) + buf * 256u;
-        unsigned char* A = smem + OFF_A + buf * A_BYTES;
-        const uint32_t bar_db = bar_d + 8 * buf, bar_ab = bar_a + 8 * buf;
-        uint32_t dr = 0;
-        bool ok = true;
-        for (uint32_t t = buf; t < 2 * my_pairs && ok; t += 2) {
-            const uint32_t tile = blockIdx.x + t * gridDim.x;  // >= n_tiles for the empty tile
-            const uint32_t g_row = tile * TM + row;
-            const bool valid = tile < n_tiles && g_row < n;
-            // layer-1 input: features -> BF16, K padded to 16
-            if (half == 0) {
-                float f[8];
+        const uint32_t t_q = tmem + ((q * 32u) << 16);
+        // the 16-column input of tile t into buffer b's activation tile, by
+        // the warps of column quarter 1 (one row each)
+        auto load_input = [&](uint32_t t, uint32_t b) {
+            if (cq != 1) return;
+            const uint32_t tile = blockIdx.x + t * gridDim.x;
+            unsigned char* A = smem + OFF_A + b * A_BYTES;
+            uint4 c0 = uint4{0u, 0u, 0u, 0u}, c1 = c0;
+            if constexpr (DIR == INFER) {
+                const uint32_t r = tile * TM + row;
+                if (tile < n_tiles && r < g.n_rows) {
+                    float f[8];
 #pragma unroll
-                for (int k = 0; k < 8; ++k) f[k] = (valid && k < MLP_IN) ? feat[size_t(g_row) * MLP_IN + k] : 0.f;
-                *reinterpret_cast<uint4*>(A + kmaj(row, 0, A_SBO)) =
-                    uint4{pack_bf16(f[0], f[1]), pack_bf16(f[2], f[3]), pack_bf16(f[4], f[5]), pack_bf16(f[6], f[7])};
-                *reinterpret_cast<uint4*>(A + kmaj(row, 8, A_SBO)) = uint4{0u, 0u, 0u, 0u};
+                    for (int k = 0; k < 8; ++k) f[k] = k < MLP_IN ? g.feat[size_t(r) * MLP_IN + k] : 0.f;
+                    c0 = uint4{pack_bf16(f[0], f[1]), pack_bf16(f[2], f[3]), pack_bf16(f[4], f[5]),
+                               pack_bf16(f[6], f[7])};
+                }
+            } else if (tile < n_tiles) {
+                const unsigned char* src = g.in + size_t(tile) * X_TILE + kmaj(row, 0, X_SBO);
+                c0 = *reinterpret_cast<const uint4*>(src);
+                c1 = *reinterpret_cast<const uint4*>(src + 128);
             }
+            *reinterpret_cast<uint4*>(A + kmaj(row, 0, A_SBO)) = c0;
+            *reinterpret_cast<uint4*>(A + kmaj(row, 8, A_SBO)) = c1;
+        };
+        uint32_t dr[2] = {0u, 0u};
+        bool ok = true;
+        float loss = 0.f;  // FWD: the loss of this thread's rows
+        if (my_pairs > 0) {
+            load_input(0, 0);
+            load_input(1, 1);
             fence_proxy_async();
-            mbar_arrive(bar_ab);
-            for (int l = 0; l < MLP_LAYERS; ++l) {
-                if (!mbar_wait(bar_db, dr & 1u, abort_flag)) { ok = false; break; }
-                ++dr;
-                tc_fence_after();
-                if (l < 4) {
-                    // 4 blocks of 32 columns, TMEM loads double-buffered
-                    const float* hb = bias + l * MLP_HID + half * 128;
-                    const uint32_t tc = t_lane + half * 128;
-                    unsigned char* dst = A + kmaj(row, half * 128, A_SBO);
-                    uint32_t va[32], vb[32];
-                    tmem_ld32(tc, va);
-                    tmem_wait_ld(va);
-                    tmem_ld32(tc + 32, vb);
-                    epilogue_block(va, hb, dst);
-                    tmem_wait_ld(vb);
-                    tmem_ld32(tc + 64, va);
-                    epilogue_block(vb, hb + 32, dst + 4 * 128);
-                    tmem_wait_ld(va);
-                    tmem_ld32(tc + 96, vb);
-                    epilogue_block(va, hb + 64, dst + 8 * 128);
-                    tmem_wait_ld(vb);
-                    epilogue_block(vb, hb + 96, dst + 12 * 128);
-                    tc_fence_before();
-                    fence_proxy_async();
-                    mbar_arrive(bar_ab);
-                } else if (half == 0) {
-                    uint32_t v[16];
-                    tmem_ld16(t_lane, v);
-                    tmem_wait_ld(v);
-                    tc_fence_before();
-                    if (valid) {
-                        const float* b5 = bias + 4 * MLP_HID;
-                        float4* o = reinterpret_cast<float4*>(out + size_t(g_row) * MLP_OUT_PAD);
+            mbar_arrive(bar_a);
+            mbar_arrive(bar_a + 8);
+        }
+        for (uint32_t p = 0; p < my_pairs && ok; ++p)
+            for (int l = 0; l < S && ok; ++l)
+                for (uint32_t b = 0; b < 2 && ok; ++b) {
+                    const uint32_t t = 2 * p + b, tile = blockIdx.x + t * gridDim.x;
+                    const bool valid = tile < n_tiles;  // false for the empty tile
+                    const size_t tile_off = size_t(tile) * A_BYTES;
+                    unsigned char* const A = smem + OFF_A + b * A_BYTES;
+                    const uint32_t tb = t_q + b * 256u;
+                    const int li = DIR == BWD ? 3 - l : l;  // the Z (and dZ) of this step
+                    unsigned char* const zl = li == 0 ? g.z[0] : (li == 1 ? g.z[1] : (li == 2 ? g.z[2] : g.z[3]));
+                    // BWD: this warp's 64 columns of Z, loaded while the MMAs run
+                    uint4 zs[8];
+                    if constexpr (DIR == BWD) {
 #pragma unroll
-                        for (int g = 0; g < 4; ++g)
-                            o[g] = make_float4(__uint_as_float(v[4 * g]) + b5[4 * g],
-                                               __uint_as_float(v[4 * g + 1]) + b5[4 * g + 1],
-                                               __uint_as_float(v[4 * g + 2]) + b5[4 * g + 2],
-                                               __uint_as_float(v[4 * g + 3]) + b5[4 * g + 3]);
+                        for (int k = 0; k < 8; ++k)
+                            zs[k] = valid ? *reinterpret_cast<const uint4*>(zl + tile_off +
+                                                                            kmaj(row, cq * 64 + 8 * k, A_SBO))
+                                          : uint4{0u, 0u, 0u, 0u};
+                    }
+                    if (!mbar_wait(bar_d + 8 * b, dr[b] & 1u, abort_flag)) { ok = false; break; }
+                    ++dr[b];
+                    tc_fence_after();
+                    if constexpr (DIR == BWD) {
+                        // dZ_{li} = scale acc * silu'(Z_{li}); W5 is stored whole, W4..W2 halved
+                        const float scale = l > 0 ? 2.0f : 1.0f;
+                        unsigned char* const dzl =
+                            li == 0 ? g.dz[0] : (li == 1 ? g.dz[1] : (li == 2 ? g.dz[2] : g.dz[3]));
+#pragma unroll
+                        for (int blk = 0; blk < 4; ++blk) {
+                            const uint32_t col = cq * 64 + uint32_t(blk) * 16;
+                            uint32_t v[16];
+                            tmem_ld16(tb + col, v);
+                            tmem_wait_ld(v);
+#pragma unroll
+                            for (int gq = 0; gq < 2; ++gq) {
+                                const uint4 zq = zs[blk * 2 + gq];
+                                const uint32_t zw[4] = {zq.x, zq.y, zq.z, zq.w};
+                                uint32_t hv[4];
+#pragma unroll
+                                for (int e = 0; e < 4; ++e) {
+                                    const int c = gq * 8 + 2 * e;
+                                    const float2 zf = unpack_bf16(zw[e]);
+                                    hv[e] = pack_bf16(scale * __uint_as_float(v[c]) * silu_grad_f(zf.x),
+                                                      scale * __uint_as_float(v[c + 1]) * silu_grad_f(zf.y));
+                                }
+                                const uint32_t off = kmaj(row, col + 8 * gq, A_SBO);
+                                const uint4 h4 = uint4{hv[0], hv[1], hv[2], hv[3]};
+                                if (l < S - 1) *reinterpret_cast<uint4*>(A + off) = h4;
+                                if (valid) *reinterpret_cast<uint4*>(dzl + tile_off + off) = h4;
+                            }
+                        }
+                    } else if (l == 4) {
+                        // the outputs: bias; FWD: the loss and dOut
+                        if (cq == 0) {
+                            uint32_t v[16];
+                            tmem_ld16(tb, v);
+                            tmem_wait_ld(v);
+                            const uint32_t r = tile * TM + row;
+                            if (valid && r < g.n_rows) {
+                                const float4* b5 = reinterpret_cast<const float4*>(g.params + mlp_b_off(4));
+                                float o[MLP_OUT_PAD];
+#pragma unroll
+                                for (int k = 0; k < 4; ++k) {
+                                    const float4 bb = __ldg(b5 + k);
+                                    o[4 * k] = __uint_as_float(v[4 * k]) + bb.x;
+                                    o[4 * k + 1] = __uint_as_float(v[4 * k + 1]) + bb.y;
+                                    o[4 * k + 2] = __uint_as_float(v[4 * k + 2]) + bb.z;
+                                    o[4 * k + 3] = __uint_as_float(v[4 * k + 3]) + bb.w;
+                                }
+                                if (g.out) {
+                                    float4* op = reinterpret_cast<float4*>(g.out + size_t(r) * MLP_OUT_PAD);
+#pragma unroll
+                                    for (int k = 0; k < 4; ++k)
+                                        op[k] = make_float4(o[4 * k], o[4 * k + 1], o[4 * k + 2], o[4 * k + 3]);
+                                }
+                                if constexpr (DIR == FWD) {
+                                    if (g.lab) {
+                                        float d[MLP_OUT_PAD];
+                                        loss += mlp_row_loss(o, g.lab[r], g.w, d);
+                                        const float inv_b = 1.0f / float(g.n_rows);
+                                        uint32_t dv[8];
+#pragma unroll
+                                        for (int k = 0; k < 8; ++k)
+                                            dv[k] = pack_bf16(d[2 * k] * inv_b, d[2 * k + 1] * inv_b);
+                                        unsigned char* dst = g.dout + size_t(tile) * X_TILE + kmaj(row, 0, X_SBO);
+                                        *reinterpret_cast<uint4*>(dst) = uint4{dv[0], dv[1], dv[2], dv[3]};
+                                        *reinterpret_cast<uint4*>(dst + 128) = uint4{dv[4], dv[5], dv[6], dv[7]};
+                                    }
+                                }
+                            }
+                        }
+                    } else {
+                        // hidden layer: z = 2 acc + b (INFER: u = z / 2 = acc + b / 2), H = silu(z)
+                        // into the next step's operand; FWD: Z to the stash
+                        const float* bl = g.params + mlp_b_off(l) + cq * 64;
+                        unsigned char* const zt = (DIR == FWD && valid) ? zl + tile_off : nullptr;
+#pragma unroll
+                        for (int blk = 0; blk < 2; ++blk) {
+                            const uint32_t col = cq * 64 + uint32_t(blk) * 32;
+                            uint32_t v[32];
+                            tmem_ld32(tb + col, v);
+                            tmem_wait_ld(v);
+                            hidden_block<DIR>(v, bl + blk * 32, A + kmaj(row, col, A_SBO),
+                                              zt ? zt + kmaj(row, col, A_SBO) : nullptr);
+                        }
+                    }
+                    tc_fence_before();
+                    const bool last = l == S - 1, more = p + 1 < my_pairs;
+                    if (last && more) load_input(t + 2, b);
+                    if (!last || more) {
+                        fence_proxy_async();
+                        mbar_arrive(bar_a + 8 * b);
                     }
                 }
+        if constexpr (DIR == FWD) {
+            if (cq == 0 && g.loss_acc) {
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) loss += __shfl_xor_sync(0xFFFFFFFFu, loss, o);
+                if (lane == 0) atomicAdd(g.loss_acc, loss / float(g.n_rows));
             }
         }
     }
     __syncthreads();
-    if (*abort_flag && threadIdx.x == 0) atomicOr(status, 2u);
+    if (*abort_flag && threadIdx.x == 0) atomicOr(g.status, 2u);
     if (warp == 1) {
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
     }
 }
 
-size_t mlp_image_bytes() { return IMAGE_BYTES; }
+template <int DIR>
+cudaError_t launch_chain(const ChainArgs& a, int sm_count, cudaStream_t st) {
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(k_mlp_chain_tc<DIR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             SMEM_BYTES);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    const uint32_t grid = a.n_tiles < uint32_t(sm_count) ? a.n_tiles : uint32_t(sm_count);
+    if (grid == 0) return cudaSuccess;
+    k_mlp_chain_tc<DIR><<<grid, THREADS, SMEM_BYTES, st>>>(a);
+    return cudaGetLastError();
+}
 
-cudaError_t launch_weight_image(const __nv_bfloat16* wb, void* img, cudaStream_t st) {
-    const uint32_t n = IMAGE_BYTES / 2;
-    k_weight_image<<<(n + 255) / 256, 256, 0, st>>>(wb, static_cast<unsigned char*>(img));
+}  // namespace
+
+size_t mlp_image_bytes() { return IMAGE_BYTES; }
+size_t mlp_t_image_bytes() { return T_IMAGE_BYTES; }
+
+cudaError_t launch_weight_image(const __nv_bfloat16* wb, void* img, void* img_t, cudaStream_t st) {
+    const uint32_t n = (IMAGE_BYTES + (img_t ? T_IMAGE_BYTES : 0u)) / 2;
+    k_weight_image<<<(n + 255) / 256, 256, 0, st>>>(wb, static_cast<unsigned char*>(img),
+                                                     static_cast<unsigned char*>(img_t));
     return cudaGetLastError();
 }
 
 cudaError_t launch_mlp_infer_tc(const float* feat, uint32_t n, const void* img, const float* params, float* out,
                                 uint32_t* status, int sm_count, cudaStream_t st) {
     if (n == 0) return cudaSuccess;
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(k_mlp_infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
-        if (e != cudaSuccess) return e;
-        attr_set = true;
+    ChainArgs a{};
+    a.img = static_cast<const unsigned char*>(img);
+    a.params = params;
+    a.feat = feat;
+    a.out = out;
+    a.n_rows = n;
+    a.n_tiles = (n + TM - 1) / TM;
+    a.status = status;
+    return launch_chain<INFER>(a, sm_count, st);
+}
+
+cudaError_t launch_mlp_fwd_stash_tc(const void* img, const float* params, const void* x0_tiles, void* const* z,
+                                    float* out, const SampleLabel* lab, const LossWeights& w, void* dout_tiles,
+                                    float* loss_acc, uint32_t n_tiles, uint32_t* status, int sm_count,
+                                    cudaStream_t st) {
+    if (lab && !dout_tiles) return cudaErrorInvalidValue;
+    ChainArgs a{};
+    a.img = static_cast<const unsigned char*>(img);
+    a.params = params;
+    a.in = static_cast<const unsigned char*>(x0_tiles);
+    for (int l = 0; l < 4; ++l) a.z[l] = static_cast<unsigned char*>(z[l]);
+    a.out = out;
+    a.lab = lab;
+    a.w = w;
+    a.dout = static_cast<unsigned char*>(dout_tiles);
+    a.loss_acc = loss_acc;
+    a.n_rows = n_tiles * TM;
+    a.n_tiles = n_tiles;
+    a.status = status;
+    return launch_chain<FWD>(a, sm_count, st);
+}
+
+cudaError_t launch_mlp_bwd_dx_tc(const void* img_t, const void* dout_tiles, void* const* z, void* const* dz,
+                                 uint32_t n_tiles, uint32_t* status, int sm_count, cudaStream_t st) {
+    ChainArgs a{};
+    a.img = static_cast<const unsigned char*>(img_t);
+    a.in = static_cast<const unsigned char*>(dout_tiles);
+    for (int l = 0; l < 4; ++l) {
+        a.z[l] = static_cast<unsigned char*>(z[l]);
+        a.dz[l] = static_cast<unsigned char*>(dz[l]);
     }
-    const uint32_t tiles = (n + TM - 1) / TM;
-    const uint32_t grid = tiles < uint32_t(sm_count) ? tiles : uint32_t(sm_count);
-    k_mlp_infer_tc<<<grid, THREADS, SMEM_BYTES, st>>>(feat, n, static_cast<const unsigned char*>(img), params, out,
-                                                       status);
-    return cudaGetLastError();
+    a.n_rows = n_tiles * TM;
+    a.n_tiles = n_tiles;
+    a.status = status;
+    return launch_chain<BWD>(a, sm_count, st);
 }
 
 }  // namespace mgk

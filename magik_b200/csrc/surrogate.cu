@@ -62,7 +62,7 @@ struct mgk_surrogate {
     bool train_tc = true;
     void *tx0 = nullptr, *tZ[4] = {}, *tdZ[4] = {}, *tdout = nullptr;
     float* dw_part = nullptr;
-    uint32_t dw_heavy = 0, dw_light = 0;
+    DwJobs dw_jobs{};
     __nv_bfloat16 *x0 = nullptr, *Z[4] = {}, *H[4] = {}, *dza = nullptr, *dzb = nullptr, *dout = nullptr;
     float *out = nullptr, *dout32 = nullptr, *loss = nullptr;
     mgk_sample_label* blab = nullptr;
@@ -75,6 +75,7 @@ struct mgk_surrogate {
     float* iout = nullptr;
     // fused tensor-core inference: weight image (rebuilt after each update)
     void* img = nullptr;
+    void* img_t = nullptr;  // the transposed image of the training backward (tcgen05 path)
     bool img_valid = false;
     uint32_t* status = nullptr;  // bit 1: a bounded wait of the fused kernel gave up
     int sm_count = 0;
@@ -125,8 +126,10 @@ mgk_result ensure_train_buffers(mgk_surrogate* s, int B) {
             TRY(dalloc(s, &s->tdZ[l], act));
         }
         TRY(dalloc(s, &s->tdout, size_t(B) * MLP_OUT_PAD * 2));
-        mlp_dw_jobs(uint32_t(B) / 128u, s->sm_count, &s->dw_heavy, &s->dw_light);
-        TRY(dalloc(s, &s->dw_part, mlp_dw_partial_floats(3 * s->dw_heavy + 2 * s->dw_light) * sizeof(float)));
+        TRY(dalloc(s, &s->img_t, mlp_t_image_bytes()));
+        s->img_valid = false;  // both images are built from now on
+        s->dw_jobs = mlp_dw_jobs(uint32_t(B) / 128u, s->sm_count);
+        TRY(dalloc(s, &s->dw_part, mlp_dw_partial_floats(s->dw_jobs.total()) * sizeof(float)));
     }
     s->tb = B;
     return MGK_SUCCESS;
@@ -197,16 +200,15 @@ cudaError_t gradient_tc(mgk_surrogate* s, const float* feat, const mgk_sample_la
     const uint32_t tiles = uint32_t(B) / 128u;
     cudaError_t e = launch_gather_tiled(feat, lab, s->perm, b0, B, s->tx0, s->blab, st);
     if (e == cudaSuccess && !s->img_valid) {
-        e = launch_weight_image(s->wb, s->img, st);
+        e = launch_weight_image(s->wb, s->img, s->img_t, st);
         s->img_valid = e == cudaSuccess;
     }
     if (e == cudaSuccess)
         e = launch_mlp_fwd_stash_tc(s->img, s->p, s->tx0, s->tZ, nullptr, s->blab, w, s->tdout, loss_acc, tiles,
                                     s->status, s->sm_count, st);
-    if (e == cudaSuccess) e = launch_mlp_bwd_dx_tc(s->img, s->tdout, s->tZ, s->tdZ, tiles, s->status, s->sm_count, st);
+    if (e == cudaSuccess) e = launch_mlp_bwd_dx_tc(s->img_t, s->tdout, s->tZ, s->tdZ, tiles, s->status, s->sm_count, st);
     if (e == cudaSuccess)
-        e = launch_mlp_dw_tc(s->tdZ, s->tZ, s->tx0, s->tdout, s->dw_part, s->grad, tiles, s->dw_heavy, s->dw_light,
-                             s->status, st);
+        e = launch_mlp_dw_tc(s->tdZ, s->tZ, s->tx0, s->tdout, s->dw_part, s->grad, tiles, s->dw_jobs, s->status, st);
     return e;
 }
 
@@ -276,7 +278,7 @@ namespace mgk {
 // Inference: the fused tensor-core kernel over all n rows.
 cudaError_t surrogate_infer(mgk_surrogate* s, const float* feat, uint32_t n, float* out, cudaStream_t st) {
     if (!s->img_valid) {
-        cudaError_t e = launch_weight_image(s->wb, s->img, st);
+        cudaError_t e = launch_weight_image(s->wb, s->img, s->img_t, st);
         if (e != cudaSuccess) return e;
         s->img_valid = true;
     }
