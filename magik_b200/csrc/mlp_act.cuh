@@ -41,8 +41,9 @@ __device__ __forceinline__ float2 unpack_bf16(uint32_t v) {
 }
 // silu of both BF16 halves of a word, rounded back to BF16
 __device__ __forceinline__ uint32_t silu_bf16x2(uint32_t v) {
-    const float2 z = unpack_bf16(v);
-    return tc::pack_bf16(silu_f(z.x), silu_f(z.y));
+    const float2 u = __fmul2_rn(make_float2(0.5f, 0.5f), unpack_bf16(v));
+    const float2 h = __ffma2_rn(u, make_float2(tanh_approx(u.x), tanh_approx(u.y)), u);
+    return tc::pack_bf16(h.x, h.y);
 }
 __device__ __forceinline__ void add_bf16x2(float& a, float& b, uint32_t v) {
     const float2 f = unpack_bf16(v);

@@ -157,36 +157,71 @@ __device__ __forceinline__ Step step_of(int l) {
     return Step{1 + 4 * (l - 1), 4, 4, 256u, 1024u};
 }
 
-// Epilogue of 32 accumulator columns of one row of a hidden layer: bias and
-// SiLU into the next step's operand (8-column groups 128 bytes apart from
-// `a`); FWD: Z to the stash at `zs` (null for the empty tile).
+// Epilogue of 16 accumulator columns of one row of a hidden layer (INFER,
+// FWD): bias and SiLU into the next step's operand (8-column groups 128 bytes
+// apart from `a`); FWD: Z to the stash at `zs` (null for the empty tile).
+// Pairs of columns in FP32x2 arithmetic; z = 2 acc + b and u = acc + b / 2
+// are single roundings (the scalings by 2 and 1/2 are exact).
 template <int DIR>
-__device__ __forceinline__ void hidden_block(const uint32_t (&v)[32], const float* bl, unsigned char* a,
-                                             unsigned char* zs) {
+__device__ __forceinline__ void hidden16(const uint32_t (&v)[16], const float* bl, unsigned char* a,
+                                         unsigned char* zs) {
+    const float2 half2 = make_float2(0.5f, 0.5f), two2 = make_float2(2.0f, 2.0f);
 #pragma unroll
-    for (int gq = 0; gq < 4; ++gq) {
+    for (int gq = 0; gq < 2; ++gq) {
         const float4 b0 = __ldg(reinterpret_cast<const float4*>(bl + gq * 8));
         const float4 b1 = __ldg(reinterpret_cast<const float4*>(bl + gq * 8 + 4));
-        const float bb[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+        const float2 bp[4] = {make_float2(b0.x, b0.y), make_float2(b0.z, b0.w), make_float2(b1.x, b1.y),
+                              make_float2(b1.z, b1.w)};
         uint32_t hv[4], zv[4];
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
             const int c = gq * 8 + 2 * e;
+            const float2 acc = make_float2(__uint_as_float(v[c]), __uint_as_float(v[c + 1]));
             if constexpr (DIR == INFER) {
-                hv[e] = silu_half_pair(__uint_as_float(v[c]) + 0.5f * bb[2 * e],
-                                       __uint_as_float(v[c + 1]) + 0.5f * bb[2 * e + 1]);
+                const float2 u = __ffma2_rn(half2, bp[e], acc);
+                hv[e] = silu_half_pair(u.x, u.y);
                 zv[e] = 0u;
             } else {
-                const float z0 = 2.0f * __uint_as_float(v[c]) + bb[2 * e];
-                const float z1 = 2.0f * __uint_as_float(v[c + 1]) + bb[2 * e + 1];
-                zv[e] = pack_bf16(z0, z1);
-                hv[e] = pack_bf16(silu_f(z0), silu_f(z1));
+                const float2 z = __ffma2_rn(two2, acc, bp[e]);
+                zv[e] = pack_bf16(z.x, z.y);
+                const float2 u = __fmul2_rn(half2, z);
+                const float2 h = __ffma2_rn(u, make_float2(tanh_approx(u.x), tanh_approx(u.y)), u);
+                hv[e] = pack_bf16(h.x, h.y);
             }
         }
         *reinterpret_cast<uint4*>(a + gq * 128) = uint4{hv[0], hv[1], hv[2], hv[3]};
         if constexpr (DIR == FWD) {
             if (zs) *reinterpret_cast<uint4*>(zs + gq * 128) = uint4{zv[0], zv[1], zv[2], zv[3]};
         }
+    }
+}
+
+// Epilogue of 16 accumulator columns of one row of the backward:
+// dZ = scale acc * silu'(Z) for the BF16 Z of `z` (2 x 8 columns), into the
+// next step's operand at `a` (null at the last step) and to global memory at
+// `dz` (null for the empty tile).  silu'(z) = s (1 + z (1 - s)),
+// s = (1 + tanh(z / 2)) / 2, in FP32x2.
+__device__ __forceinline__ void backward16(const uint32_t (&v)[16], const uint4 (&z)[2], float scale,
+                                           unsigned char* a, unsigned char* dz) {
+    const float2 half2 = make_float2(0.5f, 0.5f), one2 = make_float2(1.0f, 1.0f), sc2 = make_float2(scale, scale);
+#pragma unroll
+    for (int gq = 0; gq < 2; ++gq) {
+        const uint32_t zw[4] = {z[gq].x, z[gq].y, z[gq].z, z[gq].w};
+        uint32_t hv[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const int c = gq * 8 + 2 * e;
+            const float2 zf = unpack_bf16(zw[e]);
+            const float2 u = __fmul2_rn(half2, zf);
+            const float2 s = __ffma2_rn(half2, make_float2(tanh_approx(u.x), tanh_approx(u.y)), half2);
+            const float2 g = __fmul2_rn(s, __ffma2_rn(zf, __fadd2_rn(one2, make_float2(-s.x, -s.y)), one2));
+            const float2 acc = make_float2(__uint_as_float(v[c]), __uint_as_float(v[c + 1]));
+            const float2 d = __fmul2_rn(__fmul2_rn(sc2, acc), g);
+            hv[e] = pack_bf16(d.x, d.y);
+        }
+        const uint4 h4 = uint4{hv[0], hv[1], hv[2], hv[3]};
+        if (a) *reinterpret_cast<uint4*>(a + gq * 128) = h4;
+        if (dz) *reinterpret_cast<uint4*>(dz + gq * 128) = h4;
     }
 }
 
@@ -352,11 +387,11 @@ __global__ void __launch_bounds__(THREADS, 1) k_mlp_chain_tc(ChainArgs g) {
                     const uint32_t tb = t_q + b * 256u;
                     const int li = DIR == BWD ? 3 - l : l;  // the Z (and dZ) of this step
                     unsigned char* const zl = li == 0 ? g.z[0] : (li == 1 ? g.z[1] : (li == 2 ? g.z[2] : g.z[3]));
-                    // BWD: this warp's 64 columns of Z, loaded while the MMAs run
-                    uint4 zs[8];
+                    // BWD: the first 32 of this warp's 64 columns of Z, loaded while the MMAs run
+                    uint4 zs[4];
                     if constexpr (DIR == BWD) {
 #pragma unroll
-                        for (int k = 0; k < 8; ++k)
+                        for (int k = 0; k < 4; ++k)
                             zs[k] = valid ? *reinterpret_cast<const uint4*>(zl + tile_off +
                                                                             kmaj(row, cq * 64 + 8 * k, A_SBO))
                                           : uint4{0u, 0u, 0u, 0u};
@@ -365,34 +400,37 @@ __global__ void __launch_bounds__(THREADS, 1) k_mlp_chain_tc(ChainArgs g) {
                     ++dr[b];
                     tc_fence_after();
                     if constexpr (DIR == BWD) {
-                        // dZ_{li} = scale acc * silu'(Z_{li}); W5 is stored whole, W4..W2 halved
+                        // dZ_{li} = scale acc * silu'(Z_{li}); W5 is stored whole, W4..W2 halved;
+                        // 4 blocks of 16 columns
                         const float scale = l > 0 ? 2.0f : 1.0f;
                         unsigned char* const dzl =
                             li == 0 ? g.dz[0] : (li == 1 ? g.dz[1] : (li == 2 ? g.dz[2] : g.dz[3]));
+                        const uint32_t c0 = cq * 64;
+                        unsigned char* const an = l < S - 1 ? A + kmaj(row, c0, A_SBO) : nullptr;
+                        unsigned char* const dn = valid ? dzl + tile_off + kmaj(row, c0, A_SBO) : nullptr;
+                        const uint4 z0[2] = {zs[0], zs[1]}, z1[2] = {zs[2], zs[3]};
+                        uint32_t v[16];
+                        tmem_ld16(tb + c0, v);
+                        tmem_wait_ld(v);
+                        backward16(v, z0, scale, an, dn);
+                        // the last 32 columns' Z, while the second block runs
+                        uint4 z2[2], z3[2];
 #pragma unroll
-                        for (int blk = 0; blk < 4; ++blk) {
-                            const uint32_t col = cq * 64 + uint32_t(blk) * 16;
-                            uint32_t v[16];
-                            tmem_ld16(tb + col, v);
-                            tmem_wait_ld(v);
-#pragma unroll
-                            for (int gq = 0; gq < 2; ++gq) {
-                                const uint4 zq = zs[blk * 2 + gq];
-                                const uint32_t zw[4] = {zq.x, zq.y, zq.z, zq.w};
-                                uint32_t hv[4];
-#pragma unroll
-                                for (int e = 0; e < 4; ++e) {
-                                    const int c = gq * 8 + 2 * e;
-                                    const float2 zf = unpack_bf16(zw[e]);
-                                    hv[e] = pack_bf16(scale * __uint_as_float(v[c]) * silu_grad_f(zf.x),
-                                                      scale * __uint_as_float(v[c + 1]) * silu_grad_f(zf.y));
-                                }
-                                const uint32_t off = kmaj(row, col + 8 * gq, A_SBO);
-                                const uint4 h4 = uint4{hv[0], hv[1], hv[2], hv[3]};
-                                if (l < S - 1) *reinterpret_cast<uint4*>(A + off) = h4;
-                                if (valid) *reinterpret_cast<uint4*>(dzl + tile_off + off) = h4;
-                            }
+                        for (int k = 0; k < 2; ++k) {
+                            z2[k] = valid ? *reinterpret_cast<const uint4*>(zl + tile_off + kmaj(row, c0 + 32 + 8 * k, A_SBO))
+                                          : uint4{0u, 0u, 0u, 0u};
+                            z3[k] = valid ? *reinterpret_cast<const uint4*>(zl + tile_off + kmaj(row, c0 + 48 + 8 * k, A_SBO))
+                                          : uint4{0u, 0u, 0u, 0u};
                         }
+                        tmem_ld16(tb + c0 + 16, v);
+                        tmem_wait_ld(v);
+                        backward16(v, z1, scale, an ? an + 256 : nullptr, dn ? dn + 256 : nullptr);
+                        tmem_ld16(tb + c0 + 32, v);
+                        tmem_wait_ld(v);
+                        backward16(v, z2, scale, an ? an + 512 : nullptr, dn ? dn + 512 : nullptr);
+                        tmem_ld16(tb + c0 + 48, v);
+                        tmem_wait_ld(v);
+                        backward16(v, z3, scale, an ? an + 768 : nullptr, dn ? dn + 768 : nullptr);
                     } else if (l == 4) {
                         // the outputs: bias; FWD: the loss and dOut
                         if (cq == 0) {
@@ -437,16 +475,24 @@ __global__ void __launch_bounds__(THREADS, 1) k_mlp_chain_tc(ChainArgs g) {
                         // hidden layer: z = 2 acc + b (INFER: u = z / 2 = acc + b / 2), H = silu(z)
                         // into the next step's operand; FWD: Z to the stash
                         const float* bl = g.params + mlp_b_off(l) + cq * 64;
-                        unsigned char* const zt = (DIR == FWD && valid) ? zl + tile_off : nullptr;
-#pragma unroll
-                        for (int blk = 0; blk < 2; ++blk) {
-                            const uint32_t col = cq * 64 + uint32_t(blk) * 32;
-                            uint32_t v[32];
-                            tmem_ld32(tb + col, v);
-                            tmem_wait_ld(v);
-                            hidden_block<DIR>(v, bl + blk * 32, A + kmaj(row, col, A_SBO),
-                                              zt ? zt + kmaj(row, col, A_SBO) : nullptr);
-                        }
+                        // 4 blocks of 16 columns, the TMEM load of the next block in flight
+                        // while a block is processed
+                        const uint32_t c0 = cq * 64;
+                        unsigned char* const an = A + kmaj(row, c0, A_SBO);
+                        unsigned char* const zn = (DIR == FWD && valid) ? zl + tile_off + kmaj(row, c0, A_SBO) : nullptr;
+                        uint32_t va[16], vb[16];
+                        tmem_ld16(tb + c0, va);
+                        tmem_wait_ld(va);
+                        tmem_ld16(tb + c0 + 16, vb);
+                        hidden16<DIR>(va, bl, an, zn);
+                        tmem_wait_ld(vb);
+                        tmem_ld16(tb + c0 + 32, va);
+                        hidden16<DIR>(vb, bl + 16, an + 256, zn ? zn + 256 : nullptr);
+                        tmem_wait_ld(va);
+                        tmem_ld16(tb + c0 + 48, vb);
+                        hidden16<DIR>(va, bl + 32, an + 512, zn ? zn + 512 : nullptr);
+                        tmem_wait_ld(vb);
+                        hidden16<DIR>(vb, bl + 48, an + 768, zn ? zn + 768 : nullptr);
                     }
                     tc_fence_before();
                     const bool last = l == S - 1, more = p + 1 < my_pairs;
