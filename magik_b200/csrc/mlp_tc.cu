@@ -14,6 +14,16 @@
 // (buffers 0 and 1, two 256-column TMEM accumulators), so the epilogue of one
 // overlaps the MMAs of the other.
 //
+// PAIR (opt-in, MGK_SURROGATE_PAIRS=1): clusters of two CTAs run
+// cta_group::2 MMAs of M = 256 issued by the even CTA; each CTA holds its 128
+// rows of the activation tile and half of every weight chunk (N rows
+// 128 rank ..), its accumulator rows in its own tensor memory.  The odd CTA
+// forwards the landing of its chunk halves and the writing of its activation
+// rows to the even CTA's peer_full / peer_a barriers (remote mbarrier
+// arrivals at cluster scope); the MMA commits arrive on the barriers of both
+// CTAs (multicast); both CTAs meet at a cluster barrier after setting up
+// their barriers and before freeing their memory.
+//
 //  warp 0       producer: streams the weight image in chunks of at most
 //               32 KB into a 3-slot shared-memory ring (cp.async.bulk +
 //               mbarrier transaction counts), in the order the MMA warp
@@ -51,6 +61,7 @@
 // *status, lets the other roles leave their loops, waits (bounded) for its
 // own bulk copies and MMAs, frees its TMEM and returns.
 #include <cstdint>
+#include <cstdlib>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -65,22 +76,29 @@ namespace {
 using namespace tc;
 using namespace act;
 
-constexpr int N_SLOT = 3;
-constexpr uint32_t SLOT_BYTES = 32768;
 constexpr int EPI_WARPS = 16;
 constexpr int THREADS = 32 * (2 + EPI_WARPS);
 constexpr uint32_t TMEM_COLS = 512;             // two 256-column accumulators
 constexpr uint32_t IMAGE_BYTES = MLP_IMAGE_BYTES;
 constexpr uint32_t T_IMAGE_BYTES = 8192u + 12u * 32768u;  // W5^T, then W4^T, W3^T, W2^T in 64-column slices
 
-// Shared-memory map (dynamic, offsets from a 128-byte aligned base).
-constexpr uint32_t OFF_A = 0;                               // two activation tiles
-constexpr uint32_t OFF_W = OFF_A + 2 * A_BYTES;             // weight ring
-constexpr uint32_t OFF_BAR = OFF_W + N_SLOT * SLOT_BYTES;   // full[3], empty[3], d_ready[2], a_ready[2], drain
-constexpr uint32_t OFF_MISC = OFF_BAR + 16 * 8;             // tmem base, abort flag
-static_assert(2 * N_SLOT + 5 <= 16, "barrier area");
-constexpr uint32_t SMEM_BYTES = OFF_MISC + 16 + 128;        // + alignment slack
-static_assert(SMEM_BYTES <= 232448, "shared memory");
+// The weight ring and the shared-memory map (dynamic, offsets from a
+// 128-byte aligned base) of a single CTA (PAIR = false: whole chunks, 3
+// slots of 32 KB) and of a CTA of a pair (its half of each chunk, 6 slots of
+// 16 KB).  Barriers: full[slots], empty[slots], d_ready[2], a_ready[2],
+// drain; for a pair also peer_full[slots] and peer_a[2] (the other CTA's
+// chunk halves landed, its activation rows written).
+template <bool PAIR> struct Layout {
+    static constexpr int slots = PAIR ? 6 : 3;
+    static constexpr uint32_t slot_bytes = PAIR ? 16384u : 32768u;
+    static constexpr uint32_t off_a = 0;                                  // two activation tiles
+    static constexpr uint32_t off_w = off_a + 2 * A_BYTES;                // weight ring
+    static constexpr uint32_t off_bar = off_w + slots * slot_bytes;
+    static constexpr uint32_t n_bar = (PAIR ? 3 : 2) * slots + (PAIR ? 7 : 5);
+    static constexpr uint32_t off_misc = off_bar + ((n_bar * 8 + 127) / 128) * 128;  // tmem base, abort flag
+    static constexpr uint32_t smem_bytes = off_misc + 16 + 128;          // + alignment slack
+    static_assert(smem_bytes <= 232448, "shared memory");
+};
 
 enum { INFER = 0, FWD = 1, BWD = 2 };
 
@@ -225,22 +243,37 @@ __device__ __forceinline__ void backward16(const uint32_t (&v)[16], const uint4 
     }
 }
 
-template <int DIR>
+template <int DIR, bool PAIR>
 __global__ void __launch_bounds__(THREADS, 1) k_mlp_chain_tc(ChainArgs g) {
     constexpr int S = DIR == BWD ? MLP_LAYERS - 1 : MLP_LAYERS;  // steps per tile
+    using LY = Layout<PAIR>;
+    constexpr int N_SLOT = LY::slots;
+    constexpr uint32_t SLOT_BYTES = LY::slot_bytes, OFF_A = LY::off_a, OFF_W = LY::off_w, OFF_MISC = LY::off_misc;
     extern __shared__ unsigned char smem_raw[];
     unsigned char* smem =
         reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
     const uint32_t sbase = smem_addr(smem);
-    const uint32_t bar_full = sbase + OFF_BAR, bar_empty = bar_full + N_SLOT * 8;
+    const uint32_t bar_full = sbase + LY::off_bar, bar_empty = bar_full + N_SLOT * 8;
     const uint32_t bar_d = bar_empty + N_SLOT * 8, bar_a = bar_d + 2 * 8, bar_drain = bar_a + 2 * 8;
+    const uint32_t bar_pfull = bar_drain + 8, bar_pa = bar_pfull + N_SLOT * 8;  // PAIR only
     volatile uint32_t* tmem_slot = reinterpret_cast<volatile uint32_t*>(smem + OFF_MISC);
     volatile uint32_t* abort_flag = reinterpret_cast<volatile uint32_t*>(smem + OFF_MISC + 4);
 
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t n_tiles = g.n_tiles;
-    const uint32_t my_tiles = blockIdx.x < n_tiles ? (n_tiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
-    const uint32_t my_pairs = (my_tiles + 1) / 2;  // an odd count ends with an empty tile in buffer 1
+    // work units: 128-row tiles, or for a pair 256-row tiles whose rows
+    // 0-127 belong to the even CTA (rank 0, which issues the MMAs) and
+    // 128-255 to the odd one
+    const uint32_t rank = PAIR ? cluster_ctarank() : 0u;
+    const uint32_t unit = PAIR ? blockIdx.x >> 1 : blockIdx.x, n_units = PAIR ? gridDim.x >> 1 : gridDim.x;
+    const uint32_t units = PAIR ? (n_tiles + 1) / 2 : n_tiles;
+    const uint32_t my_units = unit < units ? (units - 1 - unit) / n_units + 1 : 0;
+    const uint32_t my_pairs = (my_units + 1) / 2;  // an odd count ends with an empty unit in buffer 1
+    // the 128-row tile of this CTA in buffer b of pair p
+    auto tile_of = [&](uint32_t p, uint32_t b) {
+        const uint32_t u = unit + (2 * p + b) * n_units;
+        return PAIR ? 2 * u + rank : u;
+    };
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < N_SLOT; ++s) {
@@ -252,14 +285,27 @@ __global__ void __launch_bounds__(THREADS, 1) k_mlp_chain_tc(ChainArgs g) {
             mbar_init(bar_a + 8 * b, 32 * EPI_WARPS);
         }
         mbar_init(bar_drain, 1);
+        if constexpr (PAIR) {
+            for (int s = 0; s < N_SLOT; ++s) mbar_init(bar_pfull + 8 * s, 1);
+            for (int b = 0; b < 2; ++b) mbar_init(bar_pa + 8 * b, EPI_WARPS);
+        }
         *abort_flag = 0u;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
+    // a pair: both CTAs' barriers are initialised before either signals the other's
+    if constexpr (PAIR) cluster_sync();
     if (warp == 1) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sbase + OFF_MISC),
-                     "r"(TMEM_COLS)
-                     : "memory");
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+        if constexpr (PAIR) {
+            asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sbase + OFF_MISC),
+                         "r"(TMEM_COLS)
+                         : "memory");
+            asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+        } else {
+            asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sbase + OFF_MISC),
+                         "r"(TMEM_COLS)
+                         : "memory");
+            asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+        }
     }
     tc_fence_before();
     __syncthreads();
@@ -278,7 +324,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_mlp_chain_tc(ChainArgs g) {
                         const Step st = step_of(l);
                         if constexpr (DIR == BWD) {
                             // the Z tiles the epilogue reads for silu', one step ahead, into L2
-                            const uint32_t tile = blockIdx.x + (2 * p + b) * gridDim.x;
+                            const uint32_t tile = tile_of(p, b);
                             if (tile < n_tiles) {
                                 if (l == 0) bulk_prefetch_l2(g.z[3] + size_t(tile) * A_BYTES, A_BYTES);
                                 const unsigned char* zn = l == 0 ? g.z[2] : (l == 1 ? g.z[1] : g.z[0]);
@@ -291,9 +337,11 @@ __global__ void __launch_bounds__(THREADS, 1) k_mlp_chain_tc(ChainArgs g) {
                                 ok = false;
                                 break;
                             }
+                            // a pair: this CTA's half of the chunk, the N rows (B columns) 128 rank ..
                             const int c = st.c0 + ci;
-                            mbar_expect_tx(bar_full + 8 * s, mlp_chunk_bytes(c));
-                            bulk_g2s(sbase + OFF_W + s * SLOT_BYTES, g.img + mlp_chunk_offset(c), mlp_chunk_bytes(c),
+                            const uint32_t bytes = PAIR ? mlp_chunk_bytes(c) / 2 : mlp_chunk_bytes(c);
+                            mbar_expect_tx(bar_full + 8 * s, bytes);
+                            bulk_g2s(sbase + OFF_W + s * SLOT_BYTES, g.img + mlp_chunk_offset(c) + rank * bytes, bytes,
                                      bar_full + 8 * s);
                         }
                     }
@@ -306,48 +354,73 @@ __global__ void __launch_bounds__(THREADS, 1) k_mlp_chain_tc(ChainArgs g) {
         }
     } else if (warp == 1) {
         // ----------------------------------------------------------------- MMA
-        if (lane == 0) {
+        if (lane == 0 && rank == 0) {
             uint32_t j = 0, ar[2] = {0u, 0u};
             bool ok = true;
             for (uint32_t p = 0; p < my_pairs && ok; ++p)
                 for (int l = 0; l < S && ok; ++l)
                     for (uint32_t b = 0; b < 2 && ok; ++b) {
                         if (!mbar_wait(bar_a + 8 * b, ar[b] & 1u, abort_flag)) { ok = false; break; }
+                        if (PAIR && !mbar_wait_cluster(bar_pa + 8 * b, ar[b] & 1u, abort_flag)) { ok = false; break; }
                         ++ar[b];
                         tc_fence_after();
                         const Step st = step_of(l);
-                        const uint32_t idesc = idesc_bf16(TM, st.n);
+                        const uint32_t idesc = idesc_bf16(PAIR ? 2 * TM : TM, st.n);
                         const uint32_t a_base = sbase + OFF_A + b * A_BYTES;
                         const uint32_t d = tmem + b * 256u;
                         for (int ci = 0; ci < st.nc; ++ci, ++j) {
                             const uint32_t s = j % N_SLOT, use = j / N_SLOT;
                             if (!mbar_wait(bar_full + 8 * s, use & 1u, abort_flag)) { ok = false; break; }
+                            if (PAIR && !mbar_wait_cluster(bar_pfull + 8 * s, use & 1u, abort_flag)) { ok = false; break; }
                             tc_fence_after();
                             const uint32_t wslot = sbase + OFF_W + s * SLOT_BYTES;
                             for (int ks = 0; ks < st.ksteps; ++ks) {
                                 const uint32_t kk = uint32_t(ci * st.ksteps + ks);  // K step within the layer
                                 const uint64_t a = smem_desc(a_base + kk * 256u, 128u, A_SBO);
                                 const uint64_t bd = smem_desc(wslot + uint32_t(ks) * 256u, 128u, st.b_sbo);
-                                mma_bf16_ss(d, a, bd, idesc, kk > 0 ? 1u : 0u);
+                                if constexpr (PAIR) mma_bf16_ss_pair(d, a, bd, idesc, kk > 0 ? 1u : 0u);
+                                else mma_bf16_ss(d, a, bd, idesc, kk > 0 ? 1u : 0u);
                             }
-                            mma_commit(bar_empty + 8 * s);
+                            if constexpr (PAIR) mma_commit_pair(bar_empty + 8 * s);
+                            else mma_commit(bar_empty + 8 * s);
                         }
-                        if (ok) mma_commit(bar_d + 8 * b);
+                        if (ok) {
+                            if constexpr (PAIR) mma_commit_pair(bar_d + 8 * b);
+                            else mma_commit(bar_d + 8 * b);
+                        }
                     }
             // all MMAs issued by this thread are complete before TMEM is freed
-            mma_commit(bar_drain);
+            if constexpr (PAIR) mma_commit_pair(bar_drain);
+            else mma_commit(bar_drain);
             for (uint32_t it = 0; it < WAIT_LIMIT && !mbar_try(bar_drain, 0); ++it) {}
+        } else if (PAIR && lane == 0) {
+            // the odd CTA of a pair: each of its chunk halves, once landed, to
+            // the even CTA's peer_full; at the end the even CTA's last commit
+            // (drain: no MMA reads this CTA's memory any more)
+            uint32_t j = 0;
+            bool ok = true;
+            for (uint32_t p = 0; p < my_pairs && ok; ++p)
+                for (int l = 0; l < S && ok; ++l)
+                    for (uint32_t b = 0; b < 2 && ok; ++b) {
+                        const Step st = step_of(l);
+                        for (int ci = 0; ci < st.nc; ++ci, ++j) {
+                            const uint32_t s = j % N_SLOT, use = j / N_SLOT;
+                            if (!mbar_wait(bar_full + 8 * s, use & 1u, abort_flag)) { ok = false; break; }
+                            mbar_arrive_remote(mapa_shared(bar_pfull + 8 * s, 0));
+                        }
+                    }
+            for (uint32_t it = 0; it < SLEEP_LIMIT && !mbar_try_sleep(bar_drain, 0, 1000000u); ++it) {}
         }
     } else {
         // ------------------------------------------------------------ epilogue
         const uint32_t ew = warp - 2, q = warp & 3u, cq = ew >> 2;  // lane quarter, column quarter
         const uint32_t row = q * 32 + lane;
         const uint32_t t_q = tmem + ((q * 32u) << 16);
-        // the 16-column input of tile t into buffer b's activation tile, by
-        // the warps of column quarter 1 (one row each)
-        auto load_input = [&](uint32_t t, uint32_t b) {
+        // the 16-column input of the tile of pair p, buffer b into buffer b's
+        // activation tile, by the warps of column quarter 1 (one row each)
+        auto load_input = [&](uint32_t p, uint32_t b) {
             if (cq != 1) return;
-            const uint32_t tile = blockIdx.x + t * gridDim.x;
+            const uint32_t tile = tile_of(p, b);
             unsigned char* A = smem + OFF_A + b * A_BYTES;
             uint4 c0 = uint4{0u, 0u, 0u, 0u}, c1 = c0;
             if constexpr (DIR == INFER) {
@@ -367,20 +440,33 @@ __global__ void __launch_bounds__(THREADS, 1) k_mlp_chain_tc(ChainArgs g) {
             *reinterpret_cast<uint4*>(A + kmaj(row, 0, A_SBO)) = c0;
             *reinterpret_cast<uint4*>(A + kmaj(row, 8, A_SBO)) = c1;
         };
+        // buffer b's activation rows of this CTA are written: a single CTA
+        // (or the even CTA of a pair) arrives on its a_ready, each warp of
+        // the odd CTA once on the even CTA's peer_a
+        auto arrive_a = [&](uint32_t b) {
+            if constexpr (PAIR) {
+                if (rank != 0) {
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive_remote(mapa_shared(bar_pa + 8 * b, 0));
+                    return;
+                }
+            }
+            mbar_arrive(bar_a + 8 * b);
+        };
         uint32_t dr[2] = {0u, 0u};
         bool ok = true;
         float loss = 0.f;  // FWD: the loss of this thread's rows
         if (my_pairs > 0) {
             load_input(0, 0);
-            load_input(1, 1);
+            load_input(0, 1);
             fence_proxy_async();
-            mbar_arrive(bar_a);
-            mbar_arrive(bar_a + 8);
+            arrive_a(0);
+            arrive_a(1);
         }
         for (uint32_t p = 0; p < my_pairs && ok; ++p)
             for (int l = 0; l < S && ok; ++l)
                 for (uint32_t b = 0; b < 2 && ok; ++b) {
-                    const uint32_t t = 2 * p + b, tile = blockIdx.x + t * gridDim.x;
+                    const uint32_t tile = tile_of(p, b);
                     const bool valid = tile < n_tiles;  // false for the empty tile
                     const size_t tile_off = size_t(tile) * A_BYTES;
                     unsigned char* const A = smem + OFF_A + b * A_BYTES;
@@ -496,10 +582,10 @@ __global__ void __launch_bounds__(THREADS, 1) k_mlp_chain_tc(ChainArgs g) {
                     }
                     tc_fence_before();
                     const bool last = l == S - 1, more = p + 1 < my_pairs;
-                    if (last && more) load_input(t + 2, b);
+                    if (last && more) load_input(p + 1, b);
                     if (!last || more) {
                         fence_proxy_async();
-                        mbar_arrive(bar_a + 8 * b);
+                        arrive_a(b);
                     }
                 }
         if constexpr (DIR == FWD) {
@@ -511,26 +597,72 @@ __global__ void __launch_bounds__(THREADS, 1) k_mlp_chain_tc(ChainArgs g) {
         }
     }
     __syncthreads();
+    // a pair: neither CTA leaves (freeing the shared memory the other
+    // signals) before both are done
+    if constexpr (PAIR) cluster_sync();
     if (*abort_flag && threadIdx.x == 0) atomicOr(g.status, 2u);
     if (warp == 1) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+        if constexpr (PAIR)
+            asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+        else
+            asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
     }
+}
+
+// The chains run as single CTAs (cta_group::1) unless MGK_SURROGATE_PAIRS=1
+// selects CTA pairs (cta_group::2: each SM streams half of every weight
+// chunk).  Both give the same bits; on B200 the pairs measured slower (the
+// even CTA's bulk copies landed 5-7 thousand cycles after issue against
+// 1.5-2 thousand in the odd CTA, and its MMA thread waited on them).
+bool use_pairs() {
+    const char* v = std::getenv("MGK_SURROGATE_PAIRS");
+    return v && v[0] == '1';
 }
 
 template <int DIR>
 cudaError_t launch_chain(const ChainArgs& a, int sm_count, cudaStream_t st) {
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(k_mlp_chain_tc<DIR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             SMEM_BYTES);
-        if (e != cudaSuccess) return e;
-        attr = true;
+    if (a.n_tiles == 0) return cudaSuccess;
+    if (!use_pairs()) {
+        static bool attr = false;
+        if (!attr) {
+            cudaError_t e = cudaFuncSetAttribute(k_mlp_chain_tc<DIR, false>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, Layout<false>::smem_bytes);
+            if (e != cudaSuccess) return e;
+            attr = true;
+        }
+        const uint32_t grid = a.n_tiles < uint32_t(sm_count) ? a.n_tiles : uint32_t(sm_count);
+        k_mlp_chain_tc<DIR, false><<<grid, THREADS, Layout<false>::smem_bytes, st>>>(a);
+        return cudaGetLastError();
     }
-    const uint32_t grid = a.n_tiles < uint32_t(sm_count) ? a.n_tiles : uint32_t(sm_count);
-    if (grid == 0) return cudaSuccess;
-    k_mlp_chain_tc<DIR><<<grid, THREADS, SMEM_BYTES, st>>>(a);
-    return cudaGetLastError();
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 2;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.blockDim = dim3(THREADS, 1, 1);
+    cfg.dynamicSmemBytes = Layout<true>::smem_bytes;
+    cfg.stream = st;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    // as many pairs as fit on the device at once (one CTA per SM)
+    static int max_pairs = 0;
+    if (max_pairs == 0) {
+        cudaError_t e = cudaFuncSetAttribute(k_mlp_chain_tc<DIR, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             Layout<true>::smem_bytes);
+        if (e != cudaSuccess) return e;
+        cfg.gridDim = dim3(2 * uint32_t(sm_count / 2), 1, 1);
+        int n = 0;
+        e = cudaOccupancyMaxActiveClusters(&n, k_mlp_chain_tc<DIR, true>, &cfg);
+        if (e != cudaSuccess) return e;
+        if (n < 1) return cudaErrorInvalidConfiguration;
+        max_pairs = n;
+    }
+    const uint32_t units = (a.n_tiles + 1) / 2;
+    const uint32_t pairs = units < uint32_t(max_pairs) ? units : uint32_t(max_pairs);
+    cfg.gridDim = dim3(2 * pairs, 1, 1);
+    return cudaLaunchKernelEx(&cfg, k_mlp_chain_tc<DIR, true>, a);
 }
 
 }  // namespace

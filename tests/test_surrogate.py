@@ -108,6 +108,37 @@ def test_forward_matches_oracle(ctx, n, path):
 
 
 @pytest.mark.gpu
+def test_cta_pair_chains_equal_single_cta(ctx):
+    """The chains as CTA pairs (MGK_SURROGATE_PAIRS=1: cta_group::2 MMAs of
+    M = 256, each SM holding half of every weight chunk) against single CTAs
+    (the default): the same inference outputs and the same gradient and
+    loss, on an odd tile count with a ragged last tile."""
+    import os
+    net = M.Surrogate(ctx, seed=7)
+    net.set_params(O.init_params(41))
+    f, lab = O.random_batch(70_001, 42)
+    x = _dev(f)
+    n = 65536
+    cfg = M.train_defaults(batch=n)
+    d_lab = _dev(lab[:n].view(np.int32).reshape(n, 8))
+    res = {}
+    try:
+        for mode in ("0", "1"):
+            os.environ["MGK_SURROGATE_PAIRS"] = mode
+            out = net.forward(x).cpu().numpy()
+            loss, g = net.gradient(cfg, x[:n].contiguous(), d_lab)
+            res[mode] = (out, loss, g)
+    finally:
+        del os.environ["MGK_SURROGATE_PAIRS"]
+    (o0, l0, g0), (o1, l1, g1) = res["0"], res["1"]
+    assert np.array_equal(o0, o1), np.abs(o0 - o1).max()
+    assert np.array_equal(g0, g1), np.abs(g0 - g1).max()
+    assert abs(l0 - l1) <= 1e-6 * abs(l0)
+    assert net.status() == 0
+    net.close()
+
+
+@pytest.mark.gpu
 def test_fused_forward_many_tiles_per_block(ctx):
     """300,000 rows: every block of the persistent fused kernel runs many
     tiles, so the weight ring and all barrier phases wrap around; the result
