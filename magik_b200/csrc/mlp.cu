@@ -51,12 +51,6 @@ __device__ __forceinline__ void mma_bf16(float* d, const uint32_t* a, uint32_t b
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
-// Element offset (in BF16 elements) of (row, col) inside a 128-row tile of
-// 16 columns in the tensor-core operand layout: 8-row groups 256 bytes apart,
-// 8-column groups 128 bytes apart.
-__host__ __device__ constexpr uint32_t tile16(uint32_t row, uint32_t col) {
-    return ((row >> 3) * 256u + (col >> 3) * 128u + (row & 7u) * 16u + (col & 7u) * 2u) / 2u;
-}
 
 __device__ __forceinline__ float silu(float z) { return z / (1.0f + expf(-z)); }
 __device__ __forceinline__ float silu_grad(float z) {
@@ -318,7 +312,8 @@ cudaError_t launch_colsum_f32(const float* X, int rows, int cols, float* out, cu
 
 // Adam on n FP32 parameters; bf16_copy (may be null) receives the new weights.
 __global__ void k_adam(float* __restrict__ p, const float* __restrict__ grad, float* __restrict__ m,
-                       float* __restrict__ v, __nv_bfloat16* __restrict__ bf16_copy, int n, AdamStep a) {
+                       float* __restrict__ v, __nv_bfloat16* __restrict__ bf16_copy, __nv_bfloat16* __restrict__ img,
+                       __nv_bfloat16* __restrict__ img_t, int n, AdamStep a) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float gi = grad[i] * a.gscale;
@@ -328,12 +323,22 @@ __global__ void k_adam(float* __restrict__ p, const float* __restrict__ grad, fl
     v[i] = vi;
     const float pi = p[i] - a.lr * (mi * a.c1) / (sqrtf(vi * a.c2) + a.eps);
     p[i] = pi;
-    if (bf16_copy) bf16_copy[i] = __float2bfloat16_rn(pi);
+    const __nv_bfloat16 h = __float2bfloat16_rn(pi);
+    if (bf16_copy) bf16_copy[i] = h;
+    if (img) {
+        uint32_t f, t;
+        bool halved;
+        mlp_image_offsets(uint32_t(i), &f, &t, &halved);
+        const __nv_bfloat16 w = halved ? __hmul(h, __float2bfloat16(0.5f)) : h;
+        if (f != ~0u) img[f / 2] = w;
+        if (img_t && t != ~0u) img_t[t / 2] = w;
+    }
 }
 
-cudaError_t launch_adam(float* p, const float* g, float* m, float* v, __nv_bfloat16* copy, int n, AdamStep a,
-                        cudaStream_t st) {
-    k_adam<<<(n + 255) / 256, 256, 0, st>>>(p, g, m, v, copy, n, a);
+cudaError_t launch_adam(float* p, const float* g, float* m, float* v, __nv_bfloat16* copy, void* img, void* img_t,
+                        int n, AdamStep a, cudaStream_t st) {
+    k_adam<<<(n + 255) / 256, 256, 0, st>>>(p, g, m, v, copy, static_cast<__nv_bfloat16*>(img),
+                                             static_cast<__nv_bfloat16*>(img_t), n, a);
     return cudaGetLastError();
 }
 
@@ -352,35 +357,6 @@ __global__ void k_gather(const float* __restrict__ feat, const SampleLabel* __re
 cudaError_t launch_gather(const float* feat, const SampleLabel* lab, const uint32_t* perm, int b0, int B,
                           __nv_bfloat16* x0, SampleLabel* blab, cudaStream_t st) {
     k_gather<<<(B + 255) / 256, 256, 0, st>>>(feat, lab, perm, b0, B, x0, blab);
-    return cudaGetLastError();
-}
-
-// The same batch with X0 in the tile layout of the training kernels: row i's
-// 16 BF16 values as two 16-byte groups of tile i / 128.
-__global__ void k_gather_tiled(const float* __restrict__ feat, const SampleLabel* __restrict__ lab,
-                               const uint32_t* __restrict__ perm, int b0, int B, __nv_bfloat16* __restrict__ x0,
-                               SampleLabel* __restrict__ blab) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= B) return;
-    const uint32_t s = perm[b0 + i];
-    __nv_bfloat162 v[MLP_IN_PAD / 2];
-#pragma unroll
-    for (int k = 0; k < MLP_IN_PAD / 2; ++k) {
-        const float a = 2 * k < MLP_IN ? feat[size_t(s) * MLP_IN + 2 * k] : 0.f;
-        const float b = 2 * k + 1 < MLP_IN ? feat[size_t(s) * MLP_IN + 2 * k + 1] : 0.f;
-        v[k] = __floats2bfloat162_rn(a, b);
-    }
-    __nv_bfloat16* t = x0 + size_t(i >> 7) * 2048u;
-    *reinterpret_cast<uint4*>(t + tile16(uint32_t(i) & 127u, 0)) = *reinterpret_cast<const uint4*>(&v[0]);
-    *reinterpret_cast<uint4*>(t + tile16(uint32_t(i) & 127u, 8)) = *reinterpret_cast<const uint4*>(&v[4]);
-    blab[i] = lab[s];
-}
-
-cudaError_t launch_gather_tiled(const float* feat, const SampleLabel* lab, const uint32_t* perm, int b0, int B,
-                                void* x0_tiles, SampleLabel* blab, cudaStream_t st) {
-    if (B % 128) return cudaErrorInvalidValue;
-    k_gather_tiled<<<(B + 255) / 256, 256, 0, st>>>(feat, lab, perm, b0, B, static_cast<__nv_bfloat16*>(x0_tiles),
-                                                     blab);
     return cudaGetLastError();
 }
 

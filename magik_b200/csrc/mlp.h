@@ -61,8 +61,10 @@ cudaError_t launch_colsum(const __nv_bfloat16* X, int rows, int ld, int cols, fl
 cudaError_t launch_colsum_f32(const float* X, int rows, int cols, float* out, cudaStream_t st);
 cudaError_t launch_loss(const float* out, const SampleLabel* lab, int B, LossWeights w, __nv_bfloat16* dout,
                         float* dout32, float* loss_acc, cudaStream_t st);
-cudaError_t launch_adam(float* p, const float* g, float* m, float* v, __nv_bfloat16* copy, int n, AdamStep a,
-                        cudaStream_t st);
+// Adam on the n FP32 parameters; the new values in BF16 into `copy` and,
+// where given, into the forward and transposed weight images.
+cudaError_t launch_adam(float* p, const float* g, float* m, float* v, __nv_bfloat16* copy, void* img, void* img_t,
+                        int n, AdamStep a, cudaStream_t st);
 cudaError_t launch_gather(const float* feat, const SampleLabel* lab, const uint32_t* perm, int b0, int B,
                           __nv_bfloat16* x0, SampleLabel* blab, cudaStream_t st);
 cudaError_t launch_features_bf16(const float* feat, uint32_t n, uint32_t rows, __nv_bfloat16* x0, cudaStream_t st);
@@ -78,6 +80,32 @@ __host__ __device__ constexpr uint32_t mlp_chunk_offset(int c) {
 }
 __host__ __device__ constexpr uint32_t mlp_chunk_bytes(int c) { return (c == 0 || c == 13) ? 8192u : 32768u; }
 constexpr uint32_t MLP_IMAGE_BYTES = 8192u + 12u * 32768u + 8192u;
+// Where parameter i (flat index) sits in the forward image and in the
+// transposed image of the backward (mlp_t_image_bytes): byte offsets, ~0u
+// where it has none (the biases; W1 in the transposed image).  *halved: the
+// images hold it halved (the layers followed by SiLU).
+__host__ __device__ inline void mlp_image_offsets(uint32_t i, uint32_t* f, uint32_t* t, bool* halved) {
+    *f = *t = ~0u;
+    *halved = false;
+    int l = 0;
+    while (l < MLP_LAYERS && !(i >= mlp_w_off(l) && i < mlp_b_off(l))) ++l;
+    if (l == MLP_LAYERS) return;
+    auto kmaj = [](uint32_t row, uint32_t k, uint32_t sbo) {
+        return (row >> 3) * sbo + (k >> 3) * 128u + (row & 7u) * 16u + (k & 7u) * 2u;
+    };
+    const uint32_t e = i - mlp_w_off(l), in_dim = l == 0 ? MLP_IN_PAD : MLP_HID;
+    const uint32_t out = e / in_dim, in = e % in_dim;
+    *halved = l < 4;
+    if (l == 0) {
+        *f = kmaj(out, in, 256);
+    } else if (l == 4) {
+        *f = mlp_chunk_offset(13) + kmaj(out, in, 4096);
+        *t = kmaj(in, out, 256);
+    } else {
+        *f = mlp_chunk_offset(1 + 4 * (l - 1) + int(in / 64)) + kmaj(out, in % 64, 1024);
+        *t = mlp_chunk_offset(1 + 4 * (3 - l) + int(out / 64)) + kmaj(in, out % 64, 1024);
+    }
+}
 
 // Fused tensor-core inference and the training chains (mlp_tc.cu).
 size_t mlp_image_bytes();
@@ -94,13 +122,14 @@ cudaError_t launch_mlp_infer_tc(const float* feat, uint32_t n, const void* img, 
 // on tiled activations: 128-row tiles
 // in the operand layout (element (row, col) of tile t at
 // t * 256 * C + kmaj(row % 128, col, 16 C) bytes for C columns).
-// Forward with stash of Z_1..Z_4; with labels (lab non-null) also the loss
-// (+= *loss_acc, the batch mean) and dOut tiles; out (FP32 [rows][16]) may be
-// null.
-cudaError_t launch_mlp_fwd_stash_tc(const void* img, const float* params, const void* x0_tiles, void* const* z,
-                                    float* out, const SampleLabel* lab, const LossWeights& w, void* dout_tiles,
-                                    float* loss_acc, uint32_t n_tiles, uint32_t* status, int sm_count,
-                                    cudaStream_t st);
+// Forward with stash of Z_1..Z_4 of the batch perm[b0 .. b0 + 128 n_tiles)
+// of the sample set (feat [.][7], lab), writing its X0 tiles; with labels
+// (lab non-null) also the loss (+= *loss_acc, the batch mean) and dOut tiles;
+// out (FP32 [rows][16]) may be null.
+cudaError_t launch_mlp_fwd_stash_tc(const void* img, const float* params, const float* feat, const uint32_t* perm,
+                                    uint32_t b0, void* x0_tiles, void* const* z, float* out, const SampleLabel* lab,
+                                    const LossWeights& w, void* dout_tiles, float* loss_acc, uint32_t n_tiles,
+                                    uint32_t* status, int sm_count, cudaStream_t st);
 cudaError_t launch_mlp_bwd_dx_tc(const void* img_t, const void* dout_tiles, void* const* z, void* const* dz,
                                  uint32_t n_tiles, uint32_t* status, int sm_count, cudaStream_t st);
 // The weight-gradient kernel's CTAs: `heavy` per layer of W2..W4, `l0` for
@@ -119,8 +148,5 @@ cudaError_t launch_mlp_dw_tc(void* const* dz, void* const* z, const void* x0_til
 // The sample-set order of one epoch (a keyed permutation of [0, n)) on the
 // device (mlp.cu).
 cudaError_t launch_epoch_perm(uint32_t* perm, uint32_t n, const uint32_t key[4], cudaStream_t st);
-// Batch assembly into tiled X0 (16 columns) (mlp.cu).
-cudaError_t launch_gather_tiled(const float* feat, const SampleLabel* lab, const uint32_t* perm, int b0, int B,
-                                void* x0_tiles, SampleLabel* blab, cudaStream_t st);
 
 }  // namespace mgk

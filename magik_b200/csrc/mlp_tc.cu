@@ -4,9 +4,11 @@
 // template, three chains:
 //
 //  INFER  inference: features (FP32) in, the 16 FP32 outputs out.
-//  FWD    training forward: X0 tiles in; the pre-activations Z_1..Z_4 to the
-//         stash, then each row's loss (mlp_loss.cuh) and the BF16 output
-//         gradient dOut / B; the FP32 outputs only where asked for.
+//  FWD    training forward: the batch's rows gathered from the sample set
+//         through the epoch's order (X0 also to global memory for the weight
+//         gradients); the pre-activations Z_1..Z_4 to the stash, then each
+//         row's loss (mlp_loss.cuh) and the BF16 output gradient dOut / B;
+//         the FP32 outputs only where asked for.
 //  BWD    training input gradients: dOut tiles in;
 //         dZ4 = (dOut W5) * silu'(Z4), dZ3 = (dZ4 W4) * silu'(Z3), ... dZ1.
 //
@@ -146,12 +148,15 @@ namespace {
 struct ChainArgs {
     const unsigned char* img;  // weight image (BWD: the transposed image)
     const float* params;       // FP32 parameters (biases)
-    const float* feat;         // INFER: features [n_rows][7]
-    const unsigned char* in;   // FWD: X0 tiles; BWD: dOut tiles (16 columns)
+    const float* feat;         // INFER: features [n_rows][7]; FWD: the sample set's features
+    const uint32_t* perm;      // FWD: the batch is rows perm[b0 ..] of the sample set
+    uint32_t b0;
+    unsigned char* x0;         // FWD: the batch's X0 tiles (16 columns, BF16), written
+    const unsigned char* in;   // BWD: dOut tiles (16 columns)
     unsigned char* z[4];       // Z_1..Z_4 tiles (FWD writes, BWD reads)
     unsigned char* dz[4];      // BWD: dZ_1..dZ_4 tiles (written)
     float* out;                // INFER, FWD: outputs [rows][16] FP32 (FWD: may be null)
-    const SampleLabel* lab;    // FWD: the batch's labels for the fused loss (may be null)
+    const SampleLabel* lab;    // FWD: the sample set's labels for the fused loss (may be null)
     unsigned char* dout;       // FWD: dOut tiles, d(loss)/d(out) / B in BF16
     float* loss_acc;           // FWD: += the batch's mean loss
     LossWeights w;
@@ -423,14 +428,20 @@ __global__ void __launch_bounds__(THREADS, 1) k_mlp_chain_tc(ChainArgs g) {
             const uint32_t tile = tile_of(p, b);
             unsigned char* A = smem + OFF_A + b * A_BYTES;
             uint4 c0 = uint4{0u, 0u, 0u, 0u}, c1 = c0;
-            if constexpr (DIR == INFER) {
+            if constexpr (DIR != BWD) {
                 const uint32_t r = tile * TM + row;
                 if (tile < n_tiles && r < g.n_rows) {
+                    const size_t src = DIR == FWD ? size_t(g.perm[g.b0 + r]) : size_t(r);
                     float f[8];
 #pragma unroll
-                    for (int k = 0; k < 8; ++k) f[k] = k < MLP_IN ? g.feat[size_t(r) * MLP_IN + k] : 0.f;
+                    for (int k = 0; k < 8; ++k) f[k] = k < MLP_IN ? g.feat[src * MLP_IN + k] : 0.f;
                     c0 = uint4{pack_bf16(f[0], f[1]), pack_bf16(f[2], f[3]), pack_bf16(f[4], f[5]),
                                pack_bf16(f[6], f[7])};
+                    if constexpr (DIR == FWD) {
+                        unsigned char* dst = g.x0 + size_t(tile) * X_TILE + kmaj(row, 0, X_SBO);
+                        *reinterpret_cast<uint4*>(dst) = c0;
+                        *reinterpret_cast<uint4*>(dst + 128) = c1;
+                    }
                 }
             } else if (tile < n_tiles) {
                 const unsigned char* src = g.in + size_t(tile) * X_TILE + kmaj(row, 0, X_SBO);
@@ -544,7 +555,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_mlp_chain_tc(ChainArgs g) {
                                 if constexpr (DIR == FWD) {
                                     if (g.lab) {
                                         float d[MLP_OUT_PAD];
-                                        loss += mlp_row_loss(o, g.lab[r], g.w, d);
+                                        loss += mlp_row_loss(o, g.lab[g.perm[g.b0 + r]], g.w, d);
                                         const float inv_b = 1.0f / float(g.n_rows);
                                         uint32_t dv[8];
 #pragma unroll
@@ -691,15 +702,18 @@ cudaError_t launch_mlp_infer_tc(const float* feat, uint32_t n, const void* img, 
     return launch_chain<INFER>(a, sm_count, st);
 }
 
-cudaError_t launch_mlp_fwd_stash_tc(const void* img, const float* params, const void* x0_tiles, void* const* z,
-                                    float* out, const SampleLabel* lab, const LossWeights& w, void* dout_tiles,
-                                    float* loss_acc, uint32_t n_tiles, uint32_t* status, int sm_count,
-                                    cudaStream_t st) {
+cudaError_t launch_mlp_fwd_stash_tc(const void* img, const float* params, const float* feat, const uint32_t* perm,
+                                    uint32_t b0, void* x0_tiles, void* const* z, float* out, const SampleLabel* lab,
+                                    const LossWeights& w, void* dout_tiles, float* loss_acc, uint32_t n_tiles,
+                                    uint32_t* status, int sm_count, cudaStream_t st) {
     if (lab && !dout_tiles) return cudaErrorInvalidValue;
     ChainArgs a{};
     a.img = static_cast<const unsigned char*>(img);
     a.params = params;
-    a.in = static_cast<const unsigned char*>(x0_tiles);
+    a.feat = feat;
+    a.perm = perm;
+    a.b0 = b0;
+    a.x0 = static_cast<unsigned char*>(x0_tiles);
     for (int l = 0; l < 4; ++l) a.z[l] = static_cast<unsigned char*>(z[l]);
     a.out = out;
     a.lab = lab;

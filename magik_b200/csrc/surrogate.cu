@@ -192,20 +192,20 @@ cudaError_t forward(mgk_surrogate* s, const __nv_bfloat16* x0, int B, __nv_bfloa
 }
 
 // One gradient of the batch rows perm[b0 .. b0 + B) on the tensor-core
-// path: gather, forward with stash and loss, input gradients, weight
-// gradients (all of grad is written); the batch mean loss is added to
+// path: forward (gathering the rows) with stash and loss, input gradients,
+// weight gradients (all of grad is written); the batch mean loss is added to
 // *loss_acc.
 cudaError_t gradient_tc(mgk_surrogate* s, const float* feat, const mgk_sample_label* lab, int b0, int B,
                         const LossWeights& w, float* loss_acc, cudaStream_t st) {
     const uint32_t tiles = uint32_t(B) / 128u;
-    cudaError_t e = launch_gather_tiled(feat, lab, s->perm, b0, B, s->tx0, s->blab, st);
-    if (e == cudaSuccess && !s->img_valid) {
+    cudaError_t e = cudaSuccess;
+    if (!s->img_valid) {
         e = launch_weight_image(s->wb, s->img, s->img_t, st);
         s->img_valid = e == cudaSuccess;
     }
     if (e == cudaSuccess)
-        e = launch_mlp_fwd_stash_tc(s->img, s->p, s->tx0, s->tZ, nullptr, s->blab, w, s->tdout, loss_acc, tiles,
-                                    s->status, s->sm_count, st);
+        e = launch_mlp_fwd_stash_tc(s->img, s->p, feat, s->perm, uint32_t(b0), s->tx0, s->tZ, nullptr, lab, w,
+                                    s->tdout, loss_acc, tiles, s->status, s->sm_count, st);
     if (e == cudaSuccess) e = launch_mlp_bwd_dx_tc(s->img_t, s->tdout, s->tZ, s->tdZ, tiles, s->status, s->sm_count, st);
     if (e == cudaSuccess)
         e = launch_mlp_dw_tc(s->tdZ, s->tZ, s->tx0, s->tdout, s->dw_part, s->grad, tiles, s->dw_jobs, s->status, st);
@@ -508,8 +508,9 @@ MGK_API mgk_result mgk_surrogate_train(mgk_surrogate* s, const mgk_train_config*
             TRY(gradient(s, d_feat, d_lab, int(b * B), int(B), w, s->loss, st));
             ++s->step;
             const AdamStep a = adam_constants(*cfg, double(ep * nb + b) / double(cfg->epochs * nb), s->step, 1.0f);
-            TRY(launch_adam(s->p, s->grad, s->m, s->v, s->wb, int(s->L.total), a, st));
-            s->img_valid = false;
+            // the weight images follow the update (every weight is rewritten)
+            TRY(launch_adam(s->p, s->grad, s->m, s->v, s->wb, s->img, s->img_t, int(s->L.total), a, st));
+            s->img_valid = true;
         }
         float loss = 0.f;
         TRY(cudaMemcpyAsync(&loss, s->loss, 4, cudaMemcpyDeviceToHost, st));
@@ -560,8 +561,9 @@ MGK_API mgk_result mgk_surrogate_adam_step(mgk_surrogate* s, const mgk_train_con
     cudaSetDevice(s->device);
     ++s->step;
     const AdamStep a = adam_constants(*cfg, progress, s->step, grad_scale);
-    TRY(launch_adam(s->p, d_grad, s->m, s->v, s->wb, int(s->L.total), a, static_cast<cudaStream_t>(stream)));
-    s->img_valid = false;
+    TRY(launch_adam(s->p, d_grad, s->m, s->v, s->wb, s->img, s->img_t, int(s->L.total), a,
+                    static_cast<cudaStream_t>(stream)));
+    s->img_valid = true;
     return MGK_SUCCESS;
 }
 
