@@ -342,6 +342,56 @@ cudaError_t launch_adam(float* p, const float* g, float* m, float* v, __nv_bfloa
     return cudaGetLastError();
 }
 
+// Adam with the constants of the current step of a counted run.  Every block
+// reads ctr->step before it counts itself done, so the last block's advance
+// comes after all reads.
+__global__ void k_adam_counted(float* __restrict__ p, const float* __restrict__ grad, float* __restrict__ m,
+                               float* __restrict__ v, __nv_bfloat16* __restrict__ bf16_copy,
+                               __nv_bfloat16* __restrict__ img, __nv_bfloat16* __restrict__ img_t, int n,
+                               const AdamStep* __restrict__ table, TrainCounters* ctr) {
+    __shared__ AdamStep a;
+    const uint32_t step = *reinterpret_cast<volatile uint32_t*>(&ctr->step);
+    if (threadIdx.x == 0) a = table[step];
+    __syncthreads();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const float gi = grad[i] * a.gscale;
+        const float mi = a.b1 * m[i] + (1.f - a.b1) * gi;
+        const float vi = a.b2 * v[i] + (1.f - a.b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        const float pi = p[i] - a.lr * (mi * a.c1) / (sqrtf(vi * a.c2) + a.eps);
+        p[i] = pi;
+        const __nv_bfloat16 h = __float2bfloat16_rn(pi);
+        if (bf16_copy) bf16_copy[i] = h;
+        if (img) {
+            uint32_t f, t;
+            bool halved;
+            mlp_image_offsets(uint32_t(i), &f, &t, &halved);
+            const __nv_bfloat16 w = halved ? __hmul(h, __float2bfloat16(0.5f)) : h;
+            if (f != ~0u) img[f / 2] = w;
+            if (img_t && t != ~0u) img_t[t / 2] = w;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&ctr->done, 1u) == gridDim.x - 1) {
+            ctr->done = 0u;
+            ctr->step = step + 1u;
+            ctr->batch += 1u;
+            __threadfence();
+        }
+    }
+}
+
+cudaError_t launch_adam_counted(float* p, const float* g, float* m, float* v, __nv_bfloat16* copy, void* img,
+                                void* img_t, int n, const AdamStep* table, TrainCounters* ctr, cudaStream_t st) {
+    k_adam_counted<<<(n + 255) / 256, 256, 0, st>>>(p, g, m, v, copy, static_cast<__nv_bfloat16*>(img),
+                                                     static_cast<__nv_bfloat16*>(img_t), n, table, ctr);
+    return cudaGetLastError();
+}
+
 // Batch assembly: rows perm[b0 + i] of the sample set.
 __global__ void k_gather(const float* __restrict__ feat, const SampleLabel* __restrict__ lab,
                          const uint32_t* __restrict__ perm, int b0, int B, __nv_bfloat16* __restrict__ x0,
@@ -371,9 +421,7 @@ __device__ __forceinline__ uint32_t fmix32(uint32_t h) {
     h ^= h >> 16; h *= 0x85EBCA6Bu; h ^= h >> 13; h *= 0xC2B2AE35u; h ^= h >> 16;
     return h;
 }
-__global__ void k_epoch_perm(uint32_t* __restrict__ perm, uint32_t n, uint32_t half_bits, uint4 key) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+__device__ __forceinline__ uint32_t feistel_index(uint32_t i, uint32_t n, uint32_t half_bits, uint4 key) {
     const uint32_t mask = half_bits >= 32 ? 0xFFFFFFFFu : (1u << half_bits) - 1u;
     const uint32_t k[4] = {key.x, key.y, key.z, key.w};
     uint32_t x = i;
@@ -387,7 +435,31 @@ __global__ void k_epoch_perm(uint32_t* __restrict__ perm, uint32_t n, uint32_t h
         }
         x = (L << half_bits) | R;
     } while (x >= n);
-    perm[i] = x;
+    return x;
+}
+__global__ void k_epoch_perm(uint32_t* __restrict__ perm, uint32_t n, uint32_t half_bits, uint4 key) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) perm[i] = feistel_index(i, n, half_bits, key);
+}
+
+__global__ void k_epoch_begin(TrainCounters* ctr) {
+    ctr->batch = 0u;
+    ctr->epoch += 1u;
+}
+__global__ void k_epoch_perm_counted(uint32_t* __restrict__ perm, uint32_t n, uint32_t half_bits,
+                                     const uint4* __restrict__ keys, const TrainCounters* ctr) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) perm[i] = feistel_index(i, n, half_bits, keys[ctr->epoch - 1u]);
+}
+
+cudaError_t launch_epoch_begin(uint32_t* perm, uint32_t n, const uint4* keys, TrainCounters* ctr, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    k_epoch_begin<<<1, 1, 0, st>>>(ctr);
+    uint32_t bits = 2;
+    while (bits < 32 && (uint64_t(1) << bits) < n) ++bits;
+    bits += bits & 1u;
+    k_epoch_perm_counted<<<(n + 255) / 256, 256, 0, st>>>(perm, n, bits / 2, keys, ctr);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_epoch_perm(uint32_t* perm, uint32_t n, const uint32_t key[4], cudaStream_t st) {

@@ -50,6 +50,16 @@ struct LossWeights {
     float tol_r, tol_g, tol_dir;  // "good prediction" bounds for the confidence target
 };
 
+// Device-side position of a training run whose steps are replayed from a
+// CUDA graph (mgk_surrogate_train): the kernels read where they are from
+// here instead of from their arguments.
+struct TrainCounters {
+    uint32_t step;   // global step: index into the table of Adam constants
+    uint32_t done;   // blocks of the Adam kernel finished in this step (the last one advances)
+    uint32_t batch;  // batch within the epoch
+    uint32_t epoch;  // epochs begun
+};
+
 struct AdamStep {
     float lr, b1, b2, eps;
     float c1, c2;     // 1 / (1 - b1^t), 1 / (1 - b2^t)
@@ -65,6 +75,13 @@ cudaError_t launch_loss(const float* out, const SampleLabel* lab, int B, LossWei
 // where given, into the forward and transposed weight images.
 cudaError_t launch_adam(float* p, const float* g, float* m, float* v, __nv_bfloat16* copy, void* img, void* img_t,
                         int n, AdamStep a, cudaStream_t st);
+// The same with the constants of step ctr->step from `table`; the last block
+// to finish advances ctr->step and ctr->batch.
+cudaError_t launch_adam_counted(float* p, const float* g, float* m, float* v, __nv_bfloat16* copy, void* img,
+                                void* img_t, int n, const AdamStep* table, TrainCounters* ctr, cudaStream_t st);
+// Begins an epoch of a counted run: ctr->batch = 0, ++ctr->epoch, and the
+// epoch's order perm[0, n) from keys[ctr->epoch - 1].
+cudaError_t launch_epoch_begin(uint32_t* perm, uint32_t n, const uint4* keys, TrainCounters* ctr, cudaStream_t st);
 cudaError_t launch_gather(const float* feat, const SampleLabel* lab, const uint32_t* perm, int b0, int B,
                           __nv_bfloat16* x0, SampleLabel* blab, cudaStream_t st);
 cudaError_t launch_features_bf16(const float* feat, uint32_t n, uint32_t rows, __nv_bfloat16* x0, cudaStream_t st);
@@ -126,10 +143,12 @@ cudaError_t launch_mlp_infer_tc(const float* feat, uint32_t n, const void* img, 
 // of the sample set (feat [.][7], lab), writing its X0 tiles; with labels
 // (lab non-null) also the loss (+= *loss_acc, the batch mean) and dOut tiles;
 // out (FP32 [rows][16]) may be null.
+// With ctr non-null the batch is batch ctr->batch of the epoch (b0 is added)
+// and the loss goes to loss_acc[ctr->epoch - 1].
 cudaError_t launch_mlp_fwd_stash_tc(const void* img, const float* params, const float* feat, const uint32_t* perm,
                                     uint32_t b0, void* x0_tiles, void* const* z, float* out, const SampleLabel* lab,
                                     const LossWeights& w, void* dout_tiles, float* loss_acc, uint32_t n_tiles,
-                                    uint32_t* status, int sm_count, cudaStream_t st);
+                                    const TrainCounters* ctr, uint32_t* status, int sm_count, cudaStream_t st);
 cudaError_t launch_mlp_bwd_dx_tc(const void* img_t, const void* dout_tiles, void* const* z, void* const* dz,
                                  uint32_t n_tiles, uint32_t* status, int sm_count, cudaStream_t st);
 // The weight-gradient kernel's CTAs: `heavy` per layer of W2..W4, `l0` for

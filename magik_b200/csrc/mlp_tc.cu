@@ -159,6 +159,8 @@ struct ChainArgs {
     const SampleLabel* lab;    // FWD: the sample set's labels for the fused loss (may be null)
     unsigned char* dout;       // FWD: dOut tiles, d(loss)/d(out) / B in BF16
     float* loss_acc;           // FWD: += the batch's mean loss
+    const TrainCounters* ctr;  // FWD, counted run: the batch is batch ctr->batch (b0 added), the loss
+                               // goes to loss_acc[ctr->epoch - 1]
     LossWeights w;
     uint32_t n_rows;
     uint32_t n_tiles;
@@ -274,6 +276,9 @@ __global__ void __launch_bounds__(THREADS, 1) k_mlp_chain_tc(ChainArgs g) {
     const uint32_t units = PAIR ? (n_tiles + 1) / 2 : n_tiles;
     const uint32_t my_units = unit < units ? (units - 1 - unit) / n_units + 1 : 0;
     const uint32_t my_pairs = (my_units + 1) / 2;  // an odd count ends with an empty unit in buffer 1
+    // FWD: the batch's first row in the order, and where its loss goes
+    const uint32_t b0 = g.b0 + (DIR == FWD && g.ctr ? g.ctr->batch * g.n_rows : 0u);
+    float* const loss_dst = DIR == FWD && g.loss_acc ? g.loss_acc + (g.ctr ? g.ctr->epoch - 1u : 0u) : nullptr;
     // the 128-row tile of this CTA in buffer b of pair p
     auto tile_of = [&](uint32_t p, uint32_t b) {
         const uint32_t u = unit + (2 * p + b) * n_units;
@@ -431,7 +436,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_mlp_chain_tc(ChainArgs g) {
             if constexpr (DIR != BWD) {
                 const uint32_t r = tile * TM + row;
                 if (tile < n_tiles && r < g.n_rows) {
-                    const size_t src = DIR == FWD ? size_t(g.perm[g.b0 + r]) : size_t(r);
+                    const size_t src = DIR == FWD ? size_t(g.perm[b0 + r]) : size_t(r);
                     float f[8];
 #pragma unroll
                     for (int k = 0; k < 8; ++k) f[k] = k < MLP_IN ? g.feat[src * MLP_IN + k] : 0.f;
@@ -555,7 +560,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_mlp_chain_tc(ChainArgs g) {
                                 if constexpr (DIR == FWD) {
                                     if (g.lab) {
                                         float d[MLP_OUT_PAD];
-                                        loss += mlp_row_loss(o, g.lab[g.perm[g.b0 + r]], g.w, d);
+                                        loss += mlp_row_loss(o, g.lab[g.perm[b0 + r]], g.w, d);
                                         const float inv_b = 1.0f / float(g.n_rows);
                                         uint32_t dv[8];
 #pragma unroll
@@ -600,10 +605,10 @@ __global__ void __launch_bounds__(THREADS, 1) k_mlp_chain_tc(ChainArgs g) {
                     }
                 }
         if constexpr (DIR == FWD) {
-            if (cq == 0 && g.loss_acc) {
+            if (cq == 0 && loss_dst) {
 #pragma unroll
                 for (int o = 16; o > 0; o >>= 1) loss += __shfl_xor_sync(0xFFFFFFFFu, loss, o);
-                if (lane == 0) atomicAdd(g.loss_acc, loss / float(g.n_rows));
+                if (lane == 0) atomicAdd(loss_dst, loss / float(g.n_rows));
             }
         }
     }
@@ -705,7 +710,7 @@ cudaError_t launch_mlp_infer_tc(const float* feat, uint32_t n, const void* img, 
 cudaError_t launch_mlp_fwd_stash_tc(const void* img, const float* params, const float* feat, const uint32_t* perm,
                                     uint32_t b0, void* x0_tiles, void* const* z, float* out, const SampleLabel* lab,
                                     const LossWeights& w, void* dout_tiles, float* loss_acc, uint32_t n_tiles,
-                                    uint32_t* status, int sm_count, cudaStream_t st) {
+                                    const TrainCounters* ctr, uint32_t* status, int sm_count, cudaStream_t st) {
     if (lab && !dout_tiles) return cudaErrorInvalidValue;
     ChainArgs a{};
     a.img = static_cast<const unsigned char*>(img);
@@ -720,6 +725,7 @@ cudaError_t launch_mlp_fwd_stash_tc(const void* img, const float* params, const 
     a.w = w;
     a.dout = static_cast<unsigned char*>(dout_tiles);
     a.loss_acc = loss_acc;
+    a.ctr = ctr;
     a.n_rows = n_tiles * TM;
     a.n_tiles = n_tiles;
     a.status = status;

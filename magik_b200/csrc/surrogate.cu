@@ -80,6 +80,23 @@ struct mgk_surrogate {
     uint32_t* status = nullptr;  // bit 1: a bounded wait of the fused kernel gave up
     int sm_count = 0;
     std::vector<void*> owned;
+    // mgk_surrogate_train on the tensor-core path: the run's position on the
+    // device, its tables (Adam constants per step, order keys per epoch), the
+    // epoch losses, and the CUDA graph of one epoch with the key it was
+    // captured for
+    TrainCounters* ctr = nullptr;
+    AdamStep* adam_table = nullptr;
+    uint4* keys = nullptr;
+    float* epoch_loss = nullptr;
+    uint32_t table_cap = 0, epoch_cap = 0;
+    cudaStream_t capture_stream = nullptr;
+    cudaGraphExec_t epoch_graph = nullptr;
+    struct GraphKey {
+        const void *feat, *lab;
+        uint32_t n, B;
+        LossWeights w;
+        const void *table, *keys, *loss;
+    } graph_key{};
 };
 
 namespace {
@@ -196,7 +213,7 @@ cudaError_t forward(mgk_surrogate* s, const __nv_bfloat16* x0, int B, __nv_bfloa
 // weight gradients (all of grad is written); the batch mean loss is added to
 // *loss_acc.
 cudaError_t gradient_tc(mgk_surrogate* s, const float* feat, const mgk_sample_label* lab, int b0, int B,
-                        const LossWeights& w, float* loss_acc, cudaStream_t st) {
+                        const LossWeights& w, float* loss_acc, cudaStream_t st, const TrainCounters* ctr = nullptr) {
     const uint32_t tiles = uint32_t(B) / 128u;
     cudaError_t e = cudaSuccess;
     if (!s->img_valid) {
@@ -205,7 +222,7 @@ cudaError_t gradient_tc(mgk_surrogate* s, const float* feat, const mgk_sample_la
     }
     if (e == cudaSuccess)
         e = launch_mlp_fwd_stash_tc(s->img, s->p, feat, s->perm, uint32_t(b0), s->tx0, s->tZ, nullptr, lab, w,
-                                    s->tdout, loss_acc, tiles, s->status, s->sm_count, st);
+                                    s->tdout, loss_acc, tiles, ctr, s->status, s->sm_count, st);
     if (e == cudaSuccess) e = launch_mlp_bwd_dx_tc(s->img_t, s->tdout, s->tZ, s->tdZ, tiles, s->status, s->sm_count, st);
     if (e == cudaSuccess)
         e = launch_mlp_dw_tc(s->tdZ, s->tZ, s->tx0, s->tdout, s->dw_part, s->grad, tiles, s->dw_jobs, s->status, st);
@@ -341,6 +358,113 @@ AdamStep adam_constants(const mgk_train_config& c, double prog, uint64_t step, f
                     float(1.0 / (1.0 - std::pow(double(c.beta2), double(step)))), gscale};
 }
 
+// Training on the tensor-core path as a counted run: the tables of the run
+// go to the device, epoch 0 runs as ordinary launches (which also set up the
+// kernels' attributes), the later epochs replay a CUDA graph of one epoch
+// (the epoch's order, then per batch: forward, backward, weight gradients,
+// Adam), captured once and kept while the data, shapes, loss weights and
+// tables stay the same.  No host synchronisation between epochs; the epoch
+// losses are read at the end.
+cudaError_t train_counted(mgk_surrogate* s, const mgk_train_config& cfg, const float* feat,
+                          const mgk_sample_label* lab, uint32_t n, float* h_epoch_loss, cudaStream_t st) {
+    const uint32_t B = cfg.batch, nb = n / B, E = cfg.epochs;
+    const LossWeights w = loss_weights(cfg);
+    if (E == 0) return cudaSuccess;
+    if (!s->ctr) {
+        cudaError_t e = dalloc(s, &s->ctr, sizeof(TrainCounters));
+        if (e != cudaSuccess) return e;
+    }
+    // room for at least 64 epochs, so that shorter runs reuse the tables
+    // (and the captured graph) of longer ones
+    const uint32_t cap_e = std::max<uint32_t>(64u, E);
+    if (cap_e * nb > s->table_cap || cap_e > s->epoch_cap) {
+        cudaFree(s->adam_table);
+        cudaFree(s->keys);
+        cudaFree(s->epoch_loss);
+        s->adam_table = nullptr;
+        s->keys = nullptr;
+        s->epoch_loss = nullptr;
+        s->table_cap = s->epoch_cap = 0;
+        cudaError_t e = cudaMalloc(&s->adam_table, size_t(cap_e) * nb * sizeof(AdamStep));
+        if (e == cudaSuccess) e = cudaMalloc(&s->keys, size_t(cap_e) * sizeof(uint4));
+        if (e == cudaSuccess) e = cudaMalloc(&s->epoch_loss, size_t(cap_e) * sizeof(float));
+        if (e != cudaSuccess) return e;
+        s->table_cap = cap_e * nb;
+        s->epoch_cap = cap_e;
+    }
+    std::vector<AdamStep> table(size_t(E) * nb);
+    for (uint32_t k = 0; k < E * nb; ++k)
+        table[k] = adam_constants(cfg, double(k) / double(E * nb), s->step + k + 1, 1.0f);
+    std::vector<uint4> keys(E);
+    for (uint32_t ep = 0; ep < E; ++ep)
+        keys[ep] = make_uint4(rng_u32(cfg.seed, 0x7E11u, ep, 0), rng_u32(cfg.seed, 0x7E11u, ep, 1),
+                              rng_u32(cfg.seed, 0x7E11u, ep, 2), rng_u32(cfg.seed, 0x7E11u, ep, 3));
+    cudaError_t e = cudaStreamSynchronize(st);  // the tables are not in use
+    if (e == cudaSuccess) e = cudaMemcpy(s->adam_table, table.data(), table.size() * sizeof(AdamStep),
+                                         cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(s->keys, keys.data(), keys.size() * sizeof(uint4), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->ctr, 0, sizeof(TrainCounters), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->epoch_loss, 0, size_t(E) * sizeof(float), st);
+    if (e == cudaSuccess && !s->img_valid) {
+        e = launch_weight_image(s->wb, s->img, s->img_t, st);
+        s->img_valid = e == cudaSuccess;
+    }
+    // one epoch's launches on stream q
+    auto epoch = [&](cudaStream_t q) {
+        cudaError_t r = launch_epoch_begin(s->perm, n, s->keys, s->ctr, q);
+        for (uint32_t b = 0; b < nb && r == cudaSuccess; ++b) {
+            r = gradient_tc(s, feat, lab, 0, int(B), w, s->epoch_loss, q, s->ctr);
+            if (r == cudaSuccess)
+                r = launch_adam_counted(s->p, s->grad, s->m, s->v, s->wb, s->img, s->img_t, int(s->L.total),
+                                        s->adam_table, s->ctr, q);
+        }
+        return r;
+    };
+    if (e == cudaSuccess) e = epoch(st);
+    // MGK_SURROGATE_GRAPH=0: every epoch as ordinary launches
+    const char* gv = std::getenv("MGK_SURROGATE_GRAPH");
+    if (gv && gv[0] == '0')
+        for (uint32_t ep = 1; ep < E && e == cudaSuccess; ++ep) e = epoch(st);
+    else if (e == cudaSuccess && E > 1) {
+        mgk_surrogate::GraphKey key{};
+        key.feat = feat;
+        key.lab = lab;
+        key.n = n;
+        key.B = B;
+        key.w = w;
+        key.table = s->adam_table;
+        key.keys = s->keys;
+        key.loss = s->epoch_loss;
+        if (!s->epoch_graph || std::memcmp(&key, &s->graph_key, sizeof(key)) != 0) {
+            if (s->epoch_graph) {
+                cudaGraphExecDestroy(s->epoch_graph);
+                s->epoch_graph = nullptr;
+            }
+            if (!s->capture_stream) e = cudaStreamCreateWithFlags(&s->capture_stream, cudaStreamNonBlocking);
+            cudaGraph_t graph = nullptr;
+            if (e == cudaSuccess) e = cudaStreamBeginCapture(s->capture_stream, cudaStreamCaptureModeThreadLocal);
+            if (e == cudaSuccess) {
+                const cudaError_t r = epoch(s->capture_stream);
+                e = cudaStreamEndCapture(s->capture_stream, &graph);
+                if (e == cudaSuccess) e = r;
+            }
+            if (e == cudaSuccess) e = cudaGraphInstantiate(&s->epoch_graph, graph, 0);
+            if (graph) cudaGraphDestroy(graph);
+            if (e == cudaSuccess) s->graph_key = key;
+        }
+        for (uint32_t ep = 1; ep < E && e == cudaSuccess; ++ep) e = cudaGraphLaunch(s->epoch_graph, st);
+    }
+    std::vector<float> loss(E, 0.f);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(loss.data(), s->epoch_loss, size_t(E) * 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return e;
+    s->step += uint64_t(E) * nb;
+    s->img_valid = true;  // the Adam kernels wrote the weight images
+    if (h_epoch_loss)
+        for (uint32_t ep = 0; ep < E; ++ep) h_epoch_loss[ep] = loss[ep] / float(nb);
+    return cudaSuccess;
+}
+
 }  // namespace
 
 extern "C" {
@@ -371,6 +495,11 @@ MGK_API uint64_t mgk_surrogate_param_count(void) { return param_layout().total; 
 MGK_API mgk_result mgk_surrogate_destroy(mgk_surrogate* s) {
     if (!s) return MGK_ERROR_INVALID_POINTER;
     cudaSetDevice(s->device);
+    if (s->epoch_graph) cudaGraphExecDestroy(s->epoch_graph);
+    if (s->capture_stream) cudaStreamDestroy(s->capture_stream);
+    cudaFree(s->adam_table);
+    cudaFree(s->keys);
+    cudaFree(s->epoch_loss);
     for (void* q : s->owned) cudaFree(q);
     delete s;
     return MGK_SUCCESS;
@@ -498,6 +627,10 @@ MGK_API mgk_result mgk_surrogate_train(mgk_surrogate* s, const mgk_train_config*
     if (s->tb != int(B)) return MGK_ERROR_INVALID_ARGUMENT;
     rc = ensure_perm(s, n);
     if (rc != MGK_SUCCESS) return rc;
+    if (s->train_tc) {
+        TRY(train_counted(s, *cfg, d_feat, d_lab, n, h_epoch_loss, st));
+        return MGK_SUCCESS;
+    }
     const LossWeights w = loss_weights(*cfg);
     const uint32_t nb = n / B;
     for (uint32_t ep = 0; ep < cfg->epochs; ++ep) {
