@@ -342,20 +342,31 @@ cudaError_t launch_adam(float* p, const float* g, float* m, float* v, __nv_bfloa
     return cudaGetLastError();
 }
 
-// Adam with the constants of the current step of a counted run.  Every block
-// reads ctr->step before it counts itself done, so the last block's advance
-// comes after all reads.
-__global__ void k_adam_counted(float* __restrict__ p, const float* __restrict__ grad, float* __restrict__ m,
-                               float* __restrict__ v, __nv_bfloat16* __restrict__ bf16_copy,
-                               __nv_bfloat16* __restrict__ img, __nv_bfloat16* __restrict__ img_t, int n,
-                               const AdamStep* __restrict__ table, TrainCounters* ctr) {
+// Adam with the constants of the current step of a counted run.  Every
+// block reads ctr->step before it counts itself done, so the last block's
+// advance comes after all reads.
+__global__ void k_adam_counted(float* __restrict__ p, const float* __restrict__ grad, const float* __restrict__ part,
+                               DwJobs jobs, float* __restrict__ m, float* __restrict__ v,
+                               __nv_bfloat16* __restrict__ bf16_copy, __nv_bfloat16* __restrict__ img,
+                               __nv_bfloat16* __restrict__ img_t, int n, const AdamStep* __restrict__ table,
+                               TrainCounters* ctr) {
     __shared__ AdamStep a;
     const uint32_t step = *reinterpret_cast<volatile uint32_t*>(&ctr->step);
     if (threadIdx.x == 0) a = table[step];
     __syncthreads();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) {
-        const float gi = grad[i] * a.gscale;
+        float gs;
+        if (part) {
+            uint32_t j0, nj, src;
+            mlp_dw_source(uint32_t(i), jobs, &j0, &nj, &src);
+            gs = 0.f;
+#pragma unroll 4
+            for (uint32_t k = 0; k < nj; ++k) gs += part[size_t(j0 + k) * MLP_DW_PART + src];
+        } else {
+            gs = grad[i];
+        }
+        const float gi = gs * a.gscale;
         const float mi = a.b1 * m[i] + (1.f - a.b1) * gi;
         const float vi = a.b2 * v[i] + (1.f - a.b2) * gi * gi;
         m[i] = mi;
@@ -385,9 +396,10 @@ __global__ void k_adam_counted(float* __restrict__ p, const float* __restrict__ 
     }
 }
 
-cudaError_t launch_adam_counted(float* p, const float* g, float* m, float* v, __nv_bfloat16* copy, void* img,
-                                void* img_t, int n, const AdamStep* table, TrainCounters* ctr, cudaStream_t st) {
-    k_adam_counted<<<(n + 255) / 256, 256, 0, st>>>(p, g, m, v, copy, static_cast<__nv_bfloat16*>(img),
+cudaError_t launch_adam_counted(float* p, const float* g, const float* part, const DwJobs& jobs, float* m, float* v,
+                                __nv_bfloat16* copy, void* img, void* img_t, int n, const AdamStep* table,
+                                TrainCounters* ctr, cudaStream_t st) {
+    k_adam_counted<<<(n + 255) / 256, 256, 0, st>>>(p, g, part, jobs, m, v, copy, static_cast<__nv_bfloat16*>(img),
                                                      static_cast<__nv_bfloat16*>(img_t), n, table, ctr);
     return cudaGetLastError();
 }

@@ -50,6 +50,13 @@ struct LossWeights {
     float tol_r, tol_g, tol_dir;  // "good prediction" bounds for the confidence target
 };
 
+// The weight-gradient kernel's CTAs: `heavy` per layer of W2..W4, `l0` for
+// W1 and b1, `l4` for W5 and b5, each job a contiguous range of batch tiles.
+struct DwJobs {
+    uint32_t heavy, l0, l4;
+    __host__ __device__ uint32_t total() const { return 3 * heavy + l0 + l4; }
+};
+
 // Device-side position of a training run whose steps are replayed from a
 // CUDA graph (mgk_surrogate_train): the kernels read where they are from
 // here instead of from their arguments.
@@ -77,8 +84,11 @@ cudaError_t launch_adam(float* p, const float* g, float* m, float* v, __nv_bfloa
                         int n, AdamStep a, cudaStream_t st);
 // The same with the constants of step ctr->step from `table`; the last block
 // to finish advances ctr->step and ctr->batch.
-cudaError_t launch_adam_counted(float* p, const float* g, float* m, float* v, __nv_bfloat16* copy, void* img,
-                                void* img_t, int n, const AdamStep* table, TrainCounters* ctr, cudaStream_t st);
+// With `part` non-null the gradient is summed from the weight-gradient
+// partials (mlp_dw_source) instead of read from g.
+cudaError_t launch_adam_counted(float* p, const float* g, const float* part, const DwJobs& jobs, float* m, float* v,
+                                __nv_bfloat16* copy, void* img, void* img_t, int n, const AdamStep* table,
+                                TrainCounters* ctr, cudaStream_t st);
 // Begins an epoch of a counted run: ctr->batch = 0, ++ctr->epoch, and the
 // epoch's order perm[0, n) from keys[ctr->epoch - 1].
 cudaError_t launch_epoch_begin(uint32_t* perm, uint32_t n, const uint4* keys, TrainCounters* ctr, cudaStream_t st);
@@ -151,19 +161,31 @@ cudaError_t launch_mlp_fwd_stash_tc(const void* img, const float* params, const 
                                     const TrainCounters* ctr, uint32_t* status, int sm_count, cudaStream_t st);
 cudaError_t launch_mlp_bwd_dx_tc(const void* img_t, const void* dout_tiles, void* const* z, void* const* dz,
                                  uint32_t n_tiles, uint32_t* status, int sm_count, cudaStream_t st);
-// The weight-gradient kernel's CTAs: `heavy` per layer of W2..W4, `l0` for
-// W1 and b1, `l4` for W5 and b5, each job a contiguous range of batch tiles.
-struct DwJobs {
-    uint32_t heavy, l0, l4;
-    __host__ __device__ uint32_t total() const { return 3 * heavy + l0 + l4; }
-};
 DwJobs mlp_dw_jobs(uint32_t n_tiles, int sm_count);
+// A job's partial sums: the 256 x 256 (or 256 x 16) weight-gradient block
+// row-major, then the 256 (or 16) bias-gradient sums.
+constexpr uint32_t MLP_DW_PART = MLP_HID * MLP_HID + MLP_HID;
+// Where the gradient of parameter i is in the partials: the sum over jobs
+// j0 .. j0 + nj - 1 of part[j * MLP_DW_PART + src].
+__host__ __device__ inline void mlp_dw_source(uint32_t i, const DwJobs& jobs, uint32_t* j0, uint32_t* nj,
+                                              uint32_t* src) {
+    const uint32_t j_l0 = 3 * jobs.heavy, j_l4 = j_l0 + jobs.l0;  // first job of W1 / b1 and of W5 / b5
+    int l = 0;
+    while (l < MLP_LAYERS - 1 && i >= mlp_w_off(l + 1)) ++l;
+    const bool bias = i >= mlp_b_off(l);
+    const uint32_t e = bias ? i - mlp_b_off(l) : i - mlp_w_off(l);
+    *j0 = l == 0 ? j_l0 : (l == 4 ? j_l4 : (l - 1) * jobs.heavy);
+    *nj = l == 0 ? jobs.l0 : (l == 4 ? jobs.l4 : jobs.heavy);
+    if (bias) *src = MLP_HID * MLP_HID + e;
+    else if (l == 4) *src = (e % MLP_HID) * MLP_OUT_PAD + e / MLP_HID;  // dW5 [16][256] from dW5^T [256][16]
+    else *src = e;
+}
 size_t mlp_dw_partial_floats(uint32_t jobs);
 // Weight and bias gradients (all of W1..W5, b1..b5) from dZ_1..dZ_4, Z_1..Z_4,
-// X0 and dOut.
+// X0 and dOut: the jobs' partials, and (reduce) their sums into grad.
 cudaError_t launch_mlp_dw_tc(void* const* dz, void* const* z, const void* x0_tiles, const void* dout_tiles,
                              float* part, float* grad, uint32_t n_tiles, const DwJobs& jobs, uint32_t* status,
-                             cudaStream_t st);
+                             cudaStream_t st, bool reduce = true);
 // The sample-set order of one epoch (a keyed permutation of [0, n)) on the
 // device (mlp.cu).
 cudaError_t launch_epoch_perm(uint32_t* perm, uint32_t n, const uint32_t key[4], cudaStream_t st);

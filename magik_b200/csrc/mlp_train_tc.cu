@@ -65,7 +65,7 @@ constexpr uint32_t DW_OFF_MISC = DW_OFF_BAR + 16 * 8;
 constexpr uint32_t DW_OFF_RED = DW_OFF_MISC + 16;             // [8 row groups][16] output-bias sums
 constexpr uint32_t DW_SMEM = DW_OFF_RED + 8 * 16 * 4 + 128;
 static_assert(DW_SMEM <= 232448, "shared memory");
-constexpr uint32_t DW_PART = MLP_HID * MLP_HID + MLP_HID;  // floats per job: the partial dW and bias sums
+constexpr uint32_t DW_PART = MLP_DW_PART;  // floats per job: the partial dW and bias sums
 
 struct DwArgs {
     const unsigned char* dz[4];  // dZ1..dZ4 tiles
@@ -301,40 +301,18 @@ __global__ void __launch_bounds__(DW_THREADS, 1) k_mlp_dw_tc(DwArgs g) {
     }
 }
 
-// grad = the sum of the jobs' partials: W1..W5 (W5 from its transpose) and
-// b1..b5; one thread per gradient element, the jobs summed in order.
+// grad = the sum of the jobs' partials, one thread per parameter, the jobs
+// summed in order (mlp_dw_source).
 __global__ void __launch_bounds__(256) k_mlp_dw_reduce(const float* __restrict__ part, DwJobs jobs,
                                                        float* __restrict__ grad) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    // element i of [W2 | W3 | W4 | W1 | W5 | b1 | b2 | b3 | b4 | b5]
-    constexpr uint32_t NW = MLP_HID * MLP_HID, NS = MLP_HID * MLP_IN_PAD;
-    const uint32_t j_l0 = 3 * jobs.heavy, j_l4 = j_l0 + jobs.l0;  // first job of W1 / b1 and of W5 / b5
-    uint32_t j0, nj, src, dst;
-    if (i < 3 * NW) {
-        const uint32_t L = 1 + i / NW, e = i % NW;
-        j0 = (L - 1) * jobs.heavy; nj = jobs.heavy; src = e; dst = mlp_w_off(int(L)) + e;
-    } else if (i < 3 * NW + NS) {
-        const uint32_t e = i - 3 * NW;  // dW1 [256][16]
-        j0 = j_l0; nj = jobs.l0; src = e; dst = mlp_w_off(0) + e;
-    } else if (i < 3 * NW + 2 * NS) {
-        const uint32_t e = i - 3 * NW - NS;  // dW5 [16][256] from dW5^T [256][16]
-        const uint32_t o = e / MLP_HID, in = e % MLP_HID;
-        j0 = j_l4; nj = jobs.l4; src = in * MLP_OUT_PAD + o; dst = mlp_w_off(4) + e;
-    } else if (i < 3 * NW + 2 * NS + 4 * MLP_HID) {
-        const uint32_t e = i - 3 * NW - 2 * NS, L = e / MLP_HID, c = e % MLP_HID;
-        j0 = L == 0 ? j_l0 : (L - 1) * jobs.heavy;
-        nj = L == 0 ? jobs.l0 : jobs.heavy;
-        src = NW + c; dst = mlp_b_off(int(L)) + c;
-    } else if (i < 3 * NW + 2 * NS + 4 * MLP_HID + MLP_OUT_PAD) {
-        const uint32_t c = i - 3 * NW - 2 * NS - 4 * MLP_HID;  // b5 from the dOut column sums
-        j0 = j_l4; nj = jobs.l4; src = NW + c; dst = mlp_b_off(4) + c;
-    } else {
-        return;
-    }
+    if (i >= MLP_PARAMS) return;
+    uint32_t j0, nj, src;
+    mlp_dw_source(i, jobs, &j0, &nj, &src);
     float s = 0.f;
 #pragma unroll 4
     for (uint32_t k = 0; k < nj; ++k) s += part[size_t(j0 + k) * DW_PART + src];
-    grad[dst] = s;
+    grad[i] = s;
 }
 
 }  // namespace
@@ -358,7 +336,7 @@ DwJobs mlp_dw_jobs(uint32_t n_tiles, int sm_count) {
 
 cudaError_t launch_mlp_dw_tc(void* const* dz, void* const* z, const void* x0_tiles, const void* dout_tiles,
                              float* part, float* grad, uint32_t n_tiles, const DwJobs& jobs, uint32_t* status,
-                             cudaStream_t st) {
+                             cudaStream_t st, bool reduce) {
     static bool attr = false;
     if (!attr) {
         cudaError_t e = cudaFuncSetAttribute(k_mlp_dw_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, DW_SMEM);
@@ -380,8 +358,8 @@ cudaError_t launch_mlp_dw_tc(void* const* dz, void* const* z, const void* x0_til
     k_mlp_dw_tc<<<jobs.total(), DW_THREADS, DW_SMEM, st>>>(a);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    const uint32_t n_out = 3 * MLP_HID * MLP_HID + 2 * MLP_HID * MLP_IN_PAD + 4 * MLP_HID + MLP_OUT_PAD;
-    k_mlp_dw_reduce<<<(n_out + 255) / 256, 256, 0, st>>>(part, jobs, grad);
+    if (!reduce) return cudaSuccess;
+    k_mlp_dw_reduce<<<(MLP_PARAMS + 255) / 256, 256, 0, st>>>(part, jobs, grad);
     return cudaGetLastError();
 }
 

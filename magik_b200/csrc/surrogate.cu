@@ -213,7 +213,8 @@ cudaError_t forward(mgk_surrogate* s, const __nv_bfloat16* x0, int B, __nv_bfloa
 // weight gradients (all of grad is written); the batch mean loss is added to
 // *loss_acc.
 cudaError_t gradient_tc(mgk_surrogate* s, const float* feat, const mgk_sample_label* lab, int b0, int B,
-                        const LossWeights& w, float* loss_acc, cudaStream_t st, const TrainCounters* ctr = nullptr) {
+                        const LossWeights& w, float* loss_acc, cudaStream_t st, const TrainCounters* ctr = nullptr,
+                        bool reduce = true) {
     const uint32_t tiles = uint32_t(B) / 128u;
     cudaError_t e = cudaSuccess;
     if (!s->img_valid) {
@@ -225,7 +226,8 @@ cudaError_t gradient_tc(mgk_surrogate* s, const float* feat, const mgk_sample_la
                                     s->tdout, loss_acc, tiles, ctr, s->status, s->sm_count, st);
     if (e == cudaSuccess) e = launch_mlp_bwd_dx_tc(s->img_t, s->tdout, s->tZ, s->tdZ, tiles, s->status, s->sm_count, st);
     if (e == cudaSuccess)
-        e = launch_mlp_dw_tc(s->tdZ, s->tZ, s->tx0, s->tdout, s->dw_part, s->grad, tiles, s->dw_jobs, s->status, st);
+        e = launch_mlp_dw_tc(s->tdZ, s->tZ, s->tx0, s->tdout, s->dw_part, s->grad, tiles, s->dw_jobs, s->status, st,
+                             reduce);
     return e;
 }
 
@@ -413,10 +415,11 @@ cudaError_t train_counted(mgk_surrogate* s, const mgk_train_config& cfg, const f
     auto epoch = [&](cudaStream_t q) {
         cudaError_t r = launch_epoch_begin(s->perm, n, s->keys, s->ctr, q);
         for (uint32_t b = 0; b < nb && r == cudaSuccess; ++b) {
-            r = gradient_tc(s, feat, lab, 0, int(B), w, s->epoch_loss, q, s->ctr);
+            // the gradient stays in the weight-gradient partials; Adam sums them
+            r = gradient_tc(s, feat, lab, 0, int(B), w, s->epoch_loss, q, s->ctr, false);
             if (r == cudaSuccess)
-                r = launch_adam_counted(s->p, s->grad, s->m, s->v, s->wb, s->img, s->img_t, int(s->L.total),
-                                        s->adam_table, s->ctr, q);
+                r = launch_adam_counted(s->p, s->grad, s->dw_part, s->dw_jobs, s->m, s->v, s->wb, s->img, s->img_t,
+                                        int(s->L.total), s->adam_table, s->ctr, q);
         }
         return r;
     };
