@@ -351,6 +351,7 @@ __global__ void k_adam_counted(float* __restrict__ p, const float* __restrict__ 
                                __nv_bfloat16* __restrict__ img_t, int n, const AdamStep* __restrict__ table,
                                TrainCounters* ctr) {
     __shared__ AdamStep a;
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     const uint32_t step = *reinterpret_cast<volatile uint32_t*>(&ctr->step);
     if (threadIdx.x == 0) a = table[step];
     __syncthreads();
@@ -361,7 +362,7 @@ __global__ void k_adam_counted(float* __restrict__ p, const float* __restrict__ 
             uint32_t j0, nj, src;
             mlp_dw_source(uint32_t(i), jobs, &j0, &nj, &src);
             gs = 0.f;
-#pragma unroll 4
+#pragma unroll 8
             for (uint32_t k = 0; k < nj; ++k) gs += part[size_t(j0 + k) * MLP_DW_PART + src];
         } else {
             gs = grad[i];
@@ -385,6 +386,7 @@ __global__ void k_adam_counted(float* __restrict__ p, const float* __restrict__ 
         }
     }
     __syncthreads();
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     if (threadIdx.x == 0) {
         __threadfence();
         if (atomicAdd(&ctr->done, 1u) == gridDim.x - 1) {
@@ -398,9 +400,20 @@ __global__ void k_adam_counted(float* __restrict__ p, const float* __restrict__ 
 
 cudaError_t launch_adam_counted(float* p, const float* g, const float* part, const DwJobs& jobs, float* m, float* v,
                                 __nv_bfloat16* copy, void* img, void* img_t, int n, const AdamStep* table,
-                                TrainCounters* ctr, cudaStream_t st) {
-    k_adam_counted<<<(n + 255) / 256, 256, 0, st>>>(p, g, part, jobs, m, v, copy, static_cast<__nv_bfloat16*>(img),
-                                                     static_cast<__nv_bfloat16*>(img_t), n, table, ctr);
+                                TrainCounters* ctr, cudaStream_t st, bool pdl) {
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.gridDim = dim3((n + 255) / 256, 1, 1);
+    cfg.blockDim = dim3(256, 1, 1);
+    cfg.stream = st;
+    cfg.attrs = at;
+    cfg.numAttrs = pdl ? 1 : 0;
+    cudaError_t e = cudaLaunchKernelEx(&cfg, k_adam_counted, p, g, part, jobs, m, v, copy,
+                                       static_cast<__nv_bfloat16*>(img), static_cast<__nv_bfloat16*>(img_t), n,
+                                       table, ctr);
+    if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }
 

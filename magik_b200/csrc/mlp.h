@@ -85,10 +85,12 @@ cudaError_t launch_adam(float* p, const float* g, float* m, float* v, __nv_bfloa
 // The same with the constants of step ctr->step from `table`; the last block
 // to finish advances ctr->step and ctr->batch.
 // With `part` non-null the gradient is summed from the weight-gradient
-// partials (mlp_dw_source) instead of read from g.
+// partials (mlp_dw_source) instead of read from g.  pdl (here and in the
+// tensor-core launchers): launched as a programmatic dependent of the
+// previous kernel in the stream, its set-up overlapping that kernel's tail.
 cudaError_t launch_adam_counted(float* p, const float* g, const float* part, const DwJobs& jobs, float* m, float* v,
                                 __nv_bfloat16* copy, void* img, void* img_t, int n, const AdamStep* table,
-                                TrainCounters* ctr, cudaStream_t st);
+                                TrainCounters* ctr, cudaStream_t st, bool pdl = false);
 // Begins an epoch of a counted run: ctr->batch = 0, ++ctr->epoch, and the
 // epoch's order perm[0, n) from keys[ctr->epoch - 1].
 cudaError_t launch_epoch_begin(uint32_t* perm, uint32_t n, const uint4* keys, TrainCounters* ctr, cudaStream_t st);
@@ -158,9 +160,10 @@ cudaError_t launch_mlp_infer_tc(const float* feat, uint32_t n, const void* img, 
 cudaError_t launch_mlp_fwd_stash_tc(const void* img, const float* params, const float* feat, const uint32_t* perm,
                                     uint32_t b0, void* x0_tiles, void* const* z, float* out, const SampleLabel* lab,
                                     const LossWeights& w, void* dout_tiles, float* loss_acc, uint32_t n_tiles,
-                                    const TrainCounters* ctr, uint32_t* status, int sm_count, cudaStream_t st);
+                                    const TrainCounters* ctr, uint32_t* status, int sm_count, cudaStream_t st,
+                                    bool pdl = false);
 cudaError_t launch_mlp_bwd_dx_tc(const void* img_t, const void* dout_tiles, void* const* z, void* const* dz,
-                                 uint32_t n_tiles, uint32_t* status, int sm_count, cudaStream_t st);
+                                 uint32_t n_tiles, uint32_t* status, int sm_count, cudaStream_t st, bool pdl = false);
 DwJobs mlp_dw_jobs(uint32_t n_tiles, int sm_count);
 // A job's partial sums: the 256 x 256 (or 256 x 16) weight-gradient block
 // row-major, then the 256 (or 16) bias-gradient sums.
@@ -185,7 +188,7 @@ size_t mlp_dw_partial_floats(uint32_t jobs);
 // X0 and dOut: the jobs' partials, and (reduce) their sums into grad.
 cudaError_t launch_mlp_dw_tc(void* const* dz, void* const* z, const void* x0_tiles, const void* dout_tiles,
                              float* part, float* grad, uint32_t n_tiles, const DwJobs& jobs, uint32_t* status,
-                             cudaStream_t st, bool reduce = true);
+                             cudaStream_t st, bool reduce = true, bool pdl = false);
 // The sample-set order of one epoch (a keyed permutation of [0, n)) on the
 // device (mlp.cu).
 cudaError_t launch_epoch_perm(uint32_t* perm, uint32_t n, const uint32_t key[4], cudaStream_t st);

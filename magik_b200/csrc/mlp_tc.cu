@@ -276,9 +276,6 @@ __global__ void __launch_bounds__(THREADS, 1) k_mlp_chain_tc(ChainArgs g) {
     const uint32_t units = PAIR ? (n_tiles + 1) / 2 : n_tiles;
     const uint32_t my_units = unit < units ? (units - 1 - unit) / n_units + 1 : 0;
     const uint32_t my_pairs = (my_units + 1) / 2;  // an odd count ends with an empty unit in buffer 1
-    // FWD: the batch's first row in the order, and where its loss goes
-    const uint32_t b0 = g.b0 + (DIR == FWD && g.ctr ? g.ctr->batch * g.n_rows : 0u);
-    float* const loss_dst = DIR == FWD && g.loss_acc ? g.loss_acc + (g.ctr ? g.ctr->epoch - 1u : 0u) : nullptr;
     // the 128-row tile of this CTA in buffer b of pair p
     auto tile_of = [&](uint32_t p, uint32_t b) {
         const uint32_t u = unit + (2 * p + b) * n_units;
@@ -321,6 +318,11 @@ __global__ void __launch_bounds__(THREADS, 1) k_mlp_chain_tc(ChainArgs g) {
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
+    // everything above overlaps the previous kernel's tail when launched as its dependent
+    grid_dependency_wait();
+    // FWD: the batch's first row in the order, and where its loss goes
+    const uint32_t b0 = g.b0 + (DIR == FWD && g.ctr ? g.ctr->batch * g.n_rows : 0u);
+    float* const loss_dst = DIR == FWD && g.loss_acc ? g.loss_acc + (g.ctr ? g.ctr->epoch - 1u : 0u) : nullptr;
 
     if (warp == 0) {
         // ------------------------------------------------------------ producer
@@ -613,6 +615,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_mlp_chain_tc(ChainArgs g) {
         }
     }
     __syncthreads();
+    grid_dependents_go();
     // a pair: neither CTA leaves (freeing the shared memory the other
     // signals) before both are done
     if constexpr (PAIR) cluster_sync();
@@ -636,8 +639,10 @@ bool use_pairs() {
     return v && v[0] == '1';
 }
 
+// pdl: launched as a programmatic dependent of the previous kernel in the
+// stream (its set-up overlaps that kernel's tail).
 template <int DIR>
-cudaError_t launch_chain(const ChainArgs& a, int sm_count, cudaStream_t st) {
+cudaError_t launch_chain(const ChainArgs& a, int sm_count, cudaStream_t st, bool pdl = false) {
     if (a.n_tiles == 0) return cudaSuccess;
     if (!use_pairs()) {
         static bool attr = false;
@@ -648,8 +653,17 @@ cudaError_t launch_chain(const ChainArgs& a, int sm_count, cudaStream_t st) {
             attr = true;
         }
         const uint32_t grid = a.n_tiles < uint32_t(sm_count) ? a.n_tiles : uint32_t(sm_count);
-        k_mlp_chain_tc<DIR, false><<<grid, THREADS, Layout<false>::smem_bytes, st>>>(a);
-        return cudaGetLastError();
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        at[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.gridDim = dim3(grid, 1, 1);
+        cfg.blockDim = dim3(THREADS, 1, 1);
+        cfg.dynamicSmemBytes = Layout<false>::smem_bytes;
+        cfg.stream = st;
+        cfg.attrs = at;
+        cfg.numAttrs = pdl ? 1 : 0;
+        return cudaLaunchKernelEx(&cfg, k_mlp_chain_tc<DIR, false>, a);
     }
     cudaLaunchConfig_t cfg = {};
     cudaLaunchAttribute attr[1];
@@ -710,7 +724,8 @@ cudaError_t launch_mlp_infer_tc(const float* feat, uint32_t n, const void* img, 
 cudaError_t launch_mlp_fwd_stash_tc(const void* img, const float* params, const float* feat, const uint32_t* perm,
                                     uint32_t b0, void* x0_tiles, void* const* z, float* out, const SampleLabel* lab,
                                     const LossWeights& w, void* dout_tiles, float* loss_acc, uint32_t n_tiles,
-                                    const TrainCounters* ctr, uint32_t* status, int sm_count, cudaStream_t st) {
+                                    const TrainCounters* ctr, uint32_t* status, int sm_count, cudaStream_t st,
+                                    bool pdl) {
     if (lab && !dout_tiles) return cudaErrorInvalidValue;
     ChainArgs a{};
     a.img = static_cast<const unsigned char*>(img);
@@ -729,11 +744,11 @@ cudaError_t launch_mlp_fwd_stash_tc(const void* img, const float* params, const 
     a.n_rows = n_tiles * TM;
     a.n_tiles = n_tiles;
     a.status = status;
-    return launch_chain<FWD>(a, sm_count, st);
+    return launch_chain<FWD>(a, sm_count, st, pdl);
 }
 
 cudaError_t launch_mlp_bwd_dx_tc(const void* img_t, const void* dout_tiles, void* const* z, void* const* dz,
-                                 uint32_t n_tiles, uint32_t* status, int sm_count, cudaStream_t st) {
+                                 uint32_t n_tiles, uint32_t* status, int sm_count, cudaStream_t st, bool pdl) {
     ChainArgs a{};
     a.img = static_cast<const unsigned char*>(img_t);
     a.in = static_cast<const unsigned char*>(dout_tiles);
@@ -744,7 +759,7 @@ cudaError_t launch_mlp_bwd_dx_tc(const void* img_t, const void* dout_tiles, void
     a.n_rows = n_tiles * TM;
     a.n_tiles = n_tiles;
     a.status = status;
-    return launch_chain<BWD>(a, sm_count, st);
+    return launch_chain<BWD>(a, sm_count, st, pdl);
 }
 
 }  // namespace mgk

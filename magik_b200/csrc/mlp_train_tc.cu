@@ -143,6 +143,8 @@ __global__ void __launch_bounds__(DW_THREADS, 1) k_mlp_dw_tc(DwArgs g) {
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
+    // everything above overlaps the previous kernel's tail when launched as its dependent
+    grid_dependency_wait();
 
     if (warp == 0) {
         if (lane == 0) {
@@ -294,6 +296,7 @@ __global__ void __launch_bounds__(DW_THREADS, 1) k_mlp_dw_tc(DwArgs g) {
         }
     }
     __syncthreads();
+    grid_dependents_go();
     if (*abort_flag && threadIdx.x == 0) atomicOr(g.status, 2u);
     if (warp == 1) {
         tc_fence_after();
@@ -336,7 +339,7 @@ DwJobs mlp_dw_jobs(uint32_t n_tiles, int sm_count) {
 
 cudaError_t launch_mlp_dw_tc(void* const* dz, void* const* z, const void* x0_tiles, const void* dout_tiles,
                              float* part, float* grad, uint32_t n_tiles, const DwJobs& jobs, uint32_t* status,
-                             cudaStream_t st, bool reduce) {
+                             cudaStream_t st, bool reduce, bool pdl) {
     static bool attr = false;
     if (!attr) {
         cudaError_t e = cudaFuncSetAttribute(k_mlp_dw_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, DW_SMEM);
@@ -355,8 +358,17 @@ cudaError_t launch_mlp_dw_tc(void* const* dz, void* const* z, const void* x0_til
     a.jobs = jobs;
     a.status = status;
     if (n_tiles == 0) return cudaSuccess;
-    k_mlp_dw_tc<<<jobs.total(), DW_THREADS, DW_SMEM, st>>>(a);
-    cudaError_t e = cudaGetLastError();
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.gridDim = dim3(jobs.total(), 1, 1);
+    cfg.blockDim = dim3(DW_THREADS, 1, 1);
+    cfg.dynamicSmemBytes = DW_SMEM;
+    cfg.stream = st;
+    cfg.attrs = at;
+    cfg.numAttrs = pdl ? 1 : 0;
+    cudaError_t e = cudaLaunchKernelEx(&cfg, k_mlp_dw_tc, a);
     if (e != cudaSuccess) return e;
     if (!reduce) return cudaSuccess;
     k_mlp_dw_reduce<<<(MLP_PARAMS + 255) / 256, 256, 0, st>>>(part, jobs, grad);

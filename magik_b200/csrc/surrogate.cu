@@ -214,7 +214,7 @@ cudaError_t forward(mgk_surrogate* s, const __nv_bfloat16* x0, int B, __nv_bfloa
 // *loss_acc.
 cudaError_t gradient_tc(mgk_surrogate* s, const float* feat, const mgk_sample_label* lab, int b0, int B,
                         const LossWeights& w, float* loss_acc, cudaStream_t st, const TrainCounters* ctr = nullptr,
-                        bool reduce = true) {
+                        bool reduce = true, bool pdl = false) {
     const uint32_t tiles = uint32_t(B) / 128u;
     cudaError_t e = cudaSuccess;
     if (!s->img_valid) {
@@ -223,11 +223,12 @@ cudaError_t gradient_tc(mgk_surrogate* s, const float* feat, const mgk_sample_la
     }
     if (e == cudaSuccess)
         e = launch_mlp_fwd_stash_tc(s->img, s->p, feat, s->perm, uint32_t(b0), s->tx0, s->tZ, nullptr, lab, w,
-                                    s->tdout, loss_acc, tiles, ctr, s->status, s->sm_count, st);
-    if (e == cudaSuccess) e = launch_mlp_bwd_dx_tc(s->img_t, s->tdout, s->tZ, s->tdZ, tiles, s->status, s->sm_count, st);
+                                    s->tdout, loss_acc, tiles, ctr, s->status, s->sm_count, st, pdl);
+    if (e == cudaSuccess)
+        e = launch_mlp_bwd_dx_tc(s->img_t, s->tdout, s->tZ, s->tdZ, tiles, s->status, s->sm_count, st, pdl);
     if (e == cudaSuccess)
         e = launch_mlp_dw_tc(s->tdZ, s->tZ, s->tx0, s->tdout, s->dw_part, s->grad, tiles, s->dw_jobs, s->status, st,
-                             reduce);
+                             reduce, pdl);
     return e;
 }
 
@@ -360,6 +361,12 @@ AdamStep adam_constants(const mgk_train_config& c, double prog, uint64_t step, f
                     float(1.0 / (1.0 - std::pow(double(c.beta2), double(step)))), gscale};
 }
 
+// Programmatic dependent launches in the counted run unless MGK_SURROGATE_PDL=0.
+bool pdl_on() {
+    const char* v = std::getenv("MGK_SURROGATE_PDL");
+    return !(v && v[0] == '0');
+}
+
 // Training on the tensor-core path as a counted run: the tables of the run
 // go to the device, epoch 0 runs as ordinary launches (which also set up the
 // kernels' attributes), the later epochs replay a CUDA graph of one epoch
@@ -416,10 +423,12 @@ cudaError_t train_counted(mgk_surrogate* s, const mgk_train_config& cfg, const f
         cudaError_t r = launch_epoch_begin(s->perm, n, s->keys, s->ctr, q);
         for (uint32_t b = 0; b < nb && r == cudaSuccess; ++b) {
             // the gradient stays in the weight-gradient partials; Adam sums them
-            r = gradient_tc(s, feat, lab, 0, int(B), w, s->epoch_loss, q, s->ctr, false);
+            // each kernel a programmatic dependent of the one before (the
+            // first forward of the epoch follows the order's kernel)
+            r = gradient_tc(s, feat, lab, 0, int(B), w, s->epoch_loss, q, s->ctr, false, pdl_on());
             if (r == cudaSuccess)
                 r = launch_adam_counted(s->p, s->grad, s->dw_part, s->dw_jobs, s->m, s->v, s->wb, s->img, s->img_t,
-                                        int(s->L.total), s->adam_table, s->ctr, q);
+                                        int(s->L.total), s->adam_table, s->ctr, q, pdl_on());
         }
         return r;
     };

@@ -107,6 +107,15 @@ __device__ __forceinline__ void mma_commit(uint32_t bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
                  : "memory");
 }
+// Programmatic dependent launch.  grid_dependency_wait: waits until the
+// grids this one depends on have completed and their memory is visible
+// (returns at once for a kernel launched without the dependency).
+// grid_dependents_go: lets the grids that depend on this one be scheduled
+// once every CTA of this grid has said so or left (their CTAs take SMs as
+// this grid's CTAs leave, and wait in grid_dependency_wait).
+__device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void grid_dependents_go() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // ---------------------------------------------------------- CTA pairs
 // The 2-CTA form (cta_group::2) of the tensor-core instructions: a cluster
 // of two CTAs on two SMs, an MMA of M = 256 issued by the even CTA whose A
