@@ -64,6 +64,7 @@
 // own bulk copies and MMAs, frees its TMEM and returns.
 #include <cstdint>
 #include <cstdlib>
+#include <cstring>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -629,6 +630,441 @@ __global__ void __launch_bounds__(THREADS, 1) k_mlp_chain_tc(ChainArgs g) {
     }
 }
 
+// ------------------------------------------------------------------------
+// The chains with the activations in tensor memory (opt-in,
+// MGK_SURROGATE_CHAIN=tmem; measured slower than the shared-memory kernel).
+//
+// Each tile's layer input is the MMA's A operand in tensor memory (A[m][k]
+// at lane m, column k / 2), its accumulator an N-half of 128 columns: per
+// buffer b, columns 256 b .. + 127 hold the accumulator and 256 b + 128 ..
+// + 255 the 256 BF16 activations of the tile's rows.  A hidden layer runs
+// as two MMA groups per tile (output columns 0-127, then 128-255), in the
+// order (half 0: tile 0, tile 1), (half 1: tile 0, tile 1), so the MMAs of
+// one group overlap the epilogue of the one before; each weight chunk stays
+// in shared memory for all four groups of its layer (half the weight stream
+// of the shared-memory kernel per tile), and the tensor core reads only the
+// weights from shared memory.  The epilogue of half 0 keeps its 32 columns
+// of BF16 results per row in registers until half 1 is done, then writes
+// the whole layer output into the tile's A columns with tcgen05.st.  Warps
+// 2-9 take tile 0's groups and warps 10-17 tile 1's, so the two tiles'
+// epilogues run side by side.
+//
+// Barriers: full / empty per weight slot; d_ready[b] (a group's MMAs are
+// complete), acc_free[b] (the epilogue has loaded the accumulator),
+// a_ready[b] (the tile's A columns hold the layer input), drain.
+namespace ta {
+constexpr int SLOTS = 6;
+constexpr uint32_t SLOT_BYTES = 32768;
+constexpr uint32_t OFF_W = 0;
+constexpr uint32_t OFF_BAR = OFF_W + SLOTS * SLOT_BYTES;
+constexpr uint32_t N_BAR = 2 * SLOTS + 7;
+constexpr uint32_t OFF_MISC = OFF_BAR + ((N_BAR * 8 + 127) / 128) * 128;
+constexpr uint32_t SMEM_BYTES = OFF_MISC + 16 + 128;
+static_assert(SMEM_BYTES <= 232448, "shared memory");
+}  // namespace ta
+
+// 16 accumulator columns of one row of a hidden layer (INFER, FWD) to 8
+// BF16x2 words of H (bias and SiLU as hidden16); FWD: Z to the stash at zs
+// (null for the empty tile).
+template <int DIR>
+__device__ __forceinline__ void hidden16_words(const uint32_t (&v)[16], const float* bl, unsigned char* zs,
+                                               uint32_t (&w)[8]) {
+    const float2 half2 = make_float2(0.5f, 0.5f), two2 = make_float2(2.0f, 2.0f);
+#pragma unroll
+    for (int gq = 0; gq < 2; ++gq) {
+        const float4 b0 = __ldg(reinterpret_cast<const float4*>(bl + gq * 8));
+        const float4 b1 = __ldg(reinterpret_cast<const float4*>(bl + gq * 8 + 4));
+        const float2 bp[4] = {make_float2(b0.x, b0.y), make_float2(b0.z, b0.w), make_float2(b1.x, b1.y),
+                              make_float2(b1.z, b1.w)};
+        uint32_t zv[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const int c = gq * 8 + 2 * e;
+            const float2 acc = make_float2(__uint_as_float(v[c]), __uint_as_float(v[c + 1]));
+            if constexpr (DIR == INFER) {
+                const float2 u = __ffma2_rn(half2, bp[e], acc);
+                w[gq * 4 + e] = silu_half_pair(u.x, u.y);
+                zv[e] = 0u;
+            } else {
+                const float2 z = __ffma2_rn(two2, acc, bp[e]);
+                zv[e] = pack_bf16(z.x, z.y);
+                const float2 u = __fmul2_rn(half2, z);
+                const float2 h = __ffma2_rn(u, make_float2(tanh_approx(u.x), tanh_approx(u.y)), u);
+                w[gq * 4 + e] = pack_bf16(h.x, h.y);
+            }
+        }
+        if constexpr (DIR == FWD) {
+            if (zs) *reinterpret_cast<uint4*>(zs + gq * 128) = uint4{zv[0], zv[1], zv[2], zv[3]};
+        }
+    }
+}
+
+// 16 accumulator columns of one row of the backward to 8 BF16x2 words of
+// dZ = scale acc * silu'(Z) (as backward16), also to global memory at dz
+// (null for the empty tile).
+__device__ __forceinline__ void backward16_words(const uint32_t (&v)[16], const uint4 (&z)[2], float scale,
+                                                 unsigned char* dz, uint32_t (&w)[8]) {
+    const float2 half2 = make_float2(0.5f, 0.5f), one2 = make_float2(1.0f, 1.0f), sc2 = make_float2(scale, scale);
+#pragma unroll
+    for (int gq = 0; gq < 2; ++gq) {
+        const uint32_t zw[4] = {z[gq].x, z[gq].y, z[gq].z, z[gq].w};
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const int c = gq * 8 + 2 * e;
+            const float2 zf = unpack_bf16(zw[e]);
+            const float2 u = __fmul2_rn(half2, zf);
+            const float2 s = __ffma2_rn(half2, make_float2(tanh_approx(u.x), tanh_approx(u.y)), half2);
+            const float2 gr = __fmul2_rn(s, __ffma2_rn(zf, __fadd2_rn(one2, make_float2(-s.x, -s.y)), one2));
+            const float2 acc = make_float2(__uint_as_float(v[c]), __uint_as_float(v[c + 1]));
+            const float2 d = __fmul2_rn(__fmul2_rn(sc2, acc), gr);
+            w[gq * 4 + e] = pack_bf16(d.x, d.y);
+        }
+        if (dz)
+            *reinterpret_cast<uint4*>(dz + gq * 128) = uint4{w[gq * 4], w[gq * 4 + 1], w[gq * 4 + 2], w[gq * 4 + 3]};
+    }
+}
+
+template <int DIR>
+__global__ void __launch_bounds__(THREADS, 1) k_mlp_chain_ta(ChainArgs g) {
+    constexpr int S = DIR == BWD ? MLP_LAYERS - 1 : MLP_LAYERS;  // steps per tile
+    constexpr int NS = ta::SLOTS;
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char* smem =
+        reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+    const uint32_t sbase = smem_addr(smem);
+    const uint32_t bar_full = sbase + ta::OFF_BAR, bar_empty = bar_full + NS * 8;
+    const uint32_t bar_d = bar_empty + NS * 8, bar_accf = bar_d + 16, bar_ardy = bar_accf + 16;
+    const uint32_t bar_drain = bar_ardy + 16;
+    volatile uint32_t* tmem_slot = reinterpret_cast<volatile uint32_t*>(smem + ta::OFF_MISC);
+    volatile uint32_t* abort_flag = reinterpret_cast<volatile uint32_t*>(smem + ta::OFF_MISC + 4);
+
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t n_tiles = g.n_tiles;
+    const uint32_t my_tiles = blockIdx.x < n_tiles ? (n_tiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+    const uint32_t my_pairs = (my_tiles + 1) / 2;  // an odd count ends with an empty tile in buffer 1
+    auto tile_of = [&](uint32_t p, uint32_t b) { return blockIdx.x + (2 * p + b) * gridDim.x; };
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < NS; ++s) {
+            mbar_init(bar_full + 8 * s, 1);
+            mbar_init(bar_empty + 8 * s, 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(bar_d + 8 * b, 1);
+            mbar_init(bar_accf + 8 * b, 32 * EPI_WARPS / 2);  // the buffer's 8 epilogue warps
+            mbar_init(bar_ardy + 8 * b, 32 * EPI_WARPS / 2);
+        }
+        mbar_init(bar_drain, 1);
+        *abort_flag = 0u;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sbase + ta::OFF_MISC),
+                     "r"(TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    // everything above overlaps the previous kernel's tail when launched as its dependent
+    grid_dependency_wait();
+    const uint32_t b0 = g.b0 + (DIR == FWD && g.ctr ? g.ctr->batch * g.n_rows : 0u);
+    float* const loss_dst = DIR == FWD && g.loss_acc ? g.loss_acc + (g.ctr ? g.ctr->epoch - 1u : 0u) : nullptr;
+
+    if (warp == 0) {
+        // ------------------------------------------------------------ producer
+        // each chunk once per tile pair and layer, in the MMA's order
+        if (lane == 0) {
+            uint32_t j = 0;
+            bool ok = true;
+            for (uint32_t p = 0; p < my_pairs && ok; ++p)
+                for (int l = 0; l < S && ok; ++l) {
+                    const Step st = step_of(l);
+                    if constexpr (DIR == BWD) {
+                        // the Z tiles the epilogue reads for silu', a step ahead, into L2
+                        for (uint32_t b = 0; b < 2; ++b) {
+                            const uint32_t tile = tile_of(p, b);
+                            if (tile < n_tiles) {
+                                if (l == 0) bulk_prefetch_l2(g.z[3] + size_t(tile) * A_BYTES, A_BYTES);
+                                const unsigned char* zn = l == 0 ? g.z[2] : (l == 1 ? g.z[1] : g.z[0]);
+                                if (l + 1 < S) bulk_prefetch_l2(zn + size_t(tile) * A_BYTES, A_BYTES);
+                            }
+                        }
+                    }
+                    for (int ci = 0; ci < st.nc; ++ci, ++j) {
+                        const uint32_t s = j % NS, use = j / NS;
+                        if (use > 0 && !mbar_wait(bar_empty + 8 * s, (use - 1) & 1u, abort_flag)) {
+                            ok = false;
+                            break;
+                        }
+                        const int c = st.c0 + ci;
+                        mbar_expect_tx(bar_full + 8 * s, mlp_chunk_bytes(c));
+                        bulk_g2s(sbase + ta::OFF_W + s * ta::SLOT_BYTES, g.img + mlp_chunk_offset(c), mlp_chunk_bytes(c),
+                                 bar_full + 8 * s);
+                    }
+                }
+            // drain: every issued copy has landed before the CTA may exit
+            const uint32_t first = j > NS ? j - NS : 0;
+            for (uint32_t k = first; k < j; ++k) {
+                const uint32_t s = k % NS, use = k / NS;
+                for (uint32_t it = 0; it < WAIT_LIMIT && !mbar_try(bar_full + 8 * s, use & 1u); ++it) {}
+            }
+        }
+    } else if (warp == 1) {
+        // ----------------------------------------------------------------- MMA
+        if (lane == 0) {
+            uint32_t j0 = 0, uses[2] = {0u, 0u}, ar[2] = {0u, 0u};
+            bool ok = true;
+            for (uint32_t p = 0; p < my_pairs && ok; ++p)
+                for (int l = 0; l < S && ok; ++l) {
+                    const Step st = step_of(l);
+                    const int nh = st.n == 16u ? 1 : 2;      // N halves of 128 (one group of 16 for W5)
+                    const uint32_t nn = st.n == 16u ? 16u : 128u;
+                    const uint32_t idesc = idesc_bf16(TM, nn);
+                    for (int h = 0; h < nh && ok; ++h)
+                        for (uint32_t b = 0; b < 2 && ok; ++b) {
+                            if (uses[b] > 0 && !mbar_wait(bar_accf + 8 * b, (uses[b] - 1) & 1u, abort_flag)) {
+                                ok = false;
+                                break;
+                            }
+                            ++uses[b];
+                            if (h == 0) {
+                                if (!mbar_wait(bar_ardy + 8 * b, ar[b] & 1u, abort_flag)) { ok = false; break; }
+                                ++ar[b];
+                            }
+                            tc_fence_after();
+                            const uint32_t d = tmem + b * 256u, a_col = tmem + b * 256u + 128u;
+                            for (int ci = 0; ci < st.nc; ++ci) {
+                                const uint32_t jj = j0 + uint32_t(ci), s = jj % NS;
+                                if (h == 0 && b == 0) {
+                                    if (!mbar_wait(bar_full + 8 * s, (jj / NS) & 1u, abort_flag)) { ok = false; break; }
+                                    tc_fence_after();
+                                }
+                                // this half's N rows of the chunk: 16 8-row groups in
+                                const uint32_t wslot = sbase + ta::OFF_W + s * ta::SLOT_BYTES + uint32_t(h) * 16u * st.b_sbo;
+                                for (int ks = 0; ks < st.ksteps; ++ks) {
+                                    const uint32_t kk = uint32_t(ci * st.ksteps + ks);  // K step within the layer
+                                    const uint64_t bd = smem_desc(wslot + uint32_t(ks) * 256u, 128u, st.b_sbo);
+                                    mma_bf16_ts(d, a_col + kk * 8u, bd, idesc, kk > 0 ? 1u : 0u);
+                                }
+                            }
+                            if (ok) mma_commit(bar_d + 8 * b);
+                        }
+                    // the layer's chunks are free once its four groups are done
+                    for (int ci = 0; ci < st.nc && ok; ++ci) mma_commit(bar_empty + 8 * ((j0 + uint32_t(ci)) % NS));
+                    j0 += uint32_t(st.nc);
+                }
+            // all MMAs issued by this thread are complete before TMEM is freed
+            mma_commit(bar_drain);
+            for (uint32_t it = 0; it < WAIT_LIMIT && !mbar_try(bar_drain, 0); ++it) {}
+        }
+    } else {
+        // ------------------------------------------------------------ epilogue
+        // warps 2-9 take buffer 0, warps 10-17 buffer 1, so the two tiles'
+        // epilogues run side by side; warp w: TMEM lanes 32 (w % 4) .. (its
+        // rows) and 64 of the 128 columns of each group
+        const uint32_t ew = warp - 2, b = ew >> 3, q = warp & 3u, cq = (ew >> 2) & 1u;
+        const uint32_t row = q * 32 + lane;
+        const uint32_t t_q = tmem + ((q * 32u) << 16);
+        const uint32_t acc = t_q + b * 256u, a_col = acc + 128u;
+        // the 16-column input of the tile of pair p into this buffer's A
+        // columns, by the warps of column half 1 (one row each)
+        auto load_input = [&](uint32_t p) {
+            if (cq != 1) return;
+            const uint32_t tile = tile_of(p, b);
+            uint4 c0 = uint4{0u, 0u, 0u, 0u}, c1 = c0;
+            if constexpr (DIR != BWD) {
+                const uint32_t r = tile * TM + row;
+                if (tile < n_tiles && r < g.n_rows) {
+                    const size_t src = DIR == FWD ? size_t(g.perm[b0 + r]) : size_t(r);
+                    float f[8];
+#pragma unroll
+                    for (int k = 0; k < 8; ++k) f[k] = k < MLP_IN ? g.feat[src * MLP_IN + k] : 0.f;
+                    c0 = uint4{pack_bf16(f[0], f[1]), pack_bf16(f[2], f[3]), pack_bf16(f[4], f[5]),
+                               pack_bf16(f[6], f[7])};
+                    if constexpr (DIR == FWD) {
+                        unsigned char* dst = g.x0 + size_t(tile) * X_TILE + kmaj(row, 0, X_SBO);
+                        *reinterpret_cast<uint4*>(dst) = c0;
+                        *reinterpret_cast<uint4*>(dst + 128) = c1;
+                    }
+                }
+            } else if (tile < n_tiles) {
+                const unsigned char* src = g.in + size_t(tile) * X_TILE + kmaj(row, 0, X_SBO);
+                c0 = *reinterpret_cast<const uint4*>(src);
+                c1 = *reinterpret_cast<const uint4*>(src + 128);
+            }
+            const uint32_t w8[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+            tmem_st8(a_col, w8);
+            tmem_wait_st();
+        };
+        auto arrive = [&](uint32_t bar) {
+            tc_fence_before();
+            mbar_arrive(bar);
+        };
+        uint32_t dr = 0;
+        uint32_t hold[32];  // half 0 of the layer output, until half 1 is done
+        bool ok = true;
+        float loss = 0.f;  // FWD: the loss of this thread's rows
+        if (my_pairs > 0) {
+            load_input(0);
+            arrive(bar_ardy + 8 * b);
+        }
+        for (uint32_t p = 0; p < my_pairs && ok; ++p)
+            for (int l = 0; l < S && ok; ++l) {
+                const Step st = step_of(l);
+                const int nh = st.n == 16u ? 1 : 2;
+                const int li = DIR == BWD ? 3 - l : l;  // the Z (and dZ) of this step
+                unsigned char* const zl = li == 0 ? g.z[0] : (li == 1 ? g.z[1] : (li == 2 ? g.z[2] : g.z[3]));
+                unsigned char* const dzl = li == 0 ? g.dz[0] : (li == 1 ? g.dz[1] : (li == 2 ? g.dz[2] : g.dz[3]));
+                const uint32_t tile = tile_of(p, b);
+                const bool valid = tile < n_tiles;  // false for the empty tile
+                const size_t tile_off = size_t(tile) * A_BYTES;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    if (h >= nh || !ok) break;
+                    const uint32_t col = uint32_t(h) * 128u + cq * 64u;  // this warp's first output column
+                    // BWD: the first block's Z, loaded while the MMAs run
+                    uint4 zs[2];
+                    if constexpr (DIR == BWD) {
+#pragma unroll
+                        for (int k = 0; k < 2; ++k)
+                            zs[k] = valid ? *reinterpret_cast<const uint4*>(zl + tile_off + kmaj(row, col + 8 * k, A_SBO))
+                                          : uint4{0u, 0u, 0u, 0u};
+                    }
+                    if (!mbar_wait(bar_d + 8 * b, dr & 1u, abort_flag)) { ok = false; break; }
+                    ++dr;
+                    tc_fence_after();
+                    if (DIR != BWD && l == 4) {
+                        // the outputs: bias; FWD: the loss and dOut
+                        if (cq == 0) {
+                            uint32_t v[16];
+                            tmem_ld16(acc, v);
+                            tmem_wait_ld(v);
+                            const uint32_t r = tile * TM + row;
+                            if (valid && r < g.n_rows) {
+                                const float4* b5 = reinterpret_cast<const float4*>(g.params + mlp_b_off(4));
+                                float o[MLP_OUT_PAD];
+#pragma unroll
+                                for (int k = 0; k < 4; ++k) {
+                                    const float4 bb = __ldg(b5 + k);
+                                    o[4 * k] = __uint_as_float(v[4 * k]) + bb.x;
+                                    o[4 * k + 1] = __uint_as_float(v[4 * k + 1]) + bb.y;
+                                    o[4 * k + 2] = __uint_as_float(v[4 * k + 2]) + bb.z;
+                                    o[4 * k + 3] = __uint_as_float(v[4 * k + 3]) + bb.w;
+                                }
+                                if (g.out) {
+                                    float4* op = reinterpret_cast<float4*>(g.out + size_t(r) * MLP_OUT_PAD);
+#pragma unroll
+                                    for (int k = 0; k < 4; ++k)
+                                        op[k] = make_float4(o[4 * k], o[4 * k + 1], o[4 * k + 2], o[4 * k + 3]);
+                                }
+                                if constexpr (DIR == FWD) {
+                                    if (g.lab) {
+                                        float dd[MLP_OUT_PAD];
+                                        loss += mlp_row_loss(o, g.lab[g.perm[b0 + r]], g.w, dd);
+                                        const float inv_b = 1.0f / float(g.n_rows);
+                                        uint32_t dv[8];
+#pragma unroll
+                                        for (int k = 0; k < 8; ++k)
+                                            dv[k] = pack_bf16(dd[2 * k] * inv_b, dd[2 * k + 1] * inv_b);
+                                        unsigned char* dst = g.dout + size_t(tile) * X_TILE + kmaj(row, 0, X_SBO);
+                                        *reinterpret_cast<uint4*>(dst) = uint4{dv[0], dv[1], dv[2], dv[3]};
+                                        *reinterpret_cast<uint4*>(dst + 128) = uint4{dv[4], dv[5], dv[6], dv[7]};
+                                    }
+                                }
+                            }
+                        }
+                        arrive(bar_accf + 8 * b);
+                    } else {
+                        // 64 columns in four blocks of 16
+                        const float scale = l > 0 ? 2.0f : 1.0f;  // BWD: W5 whole, W4..W2 halved
+                        unsigned char* const zt = (DIR == FWD && valid) ? zl + tile_off : nullptr;
+                        unsigned char* const dt = (DIR == BWD && valid) ? dzl + tile_off : nullptr;
+                        const bool write_a = h == 1 && l < S - 1;
+                        if (write_a) {
+                            // half 0 of the layer output into the tile's A columns (K = col -> column
+                            // col / 2); BWD reads it back from the dZ it wrote
+                            uint32_t h0[16];
+#pragma unroll
+                            for (int part = 0; part < 2; ++part) {
+                                if constexpr (DIR == BWD) {
+#pragma unroll
+                                    for (int k = 0; k < 4; ++k) {
+                                        const uint4 u = valid ? *reinterpret_cast<const uint4*>(
+                                                                    dzl + tile_off +
+                                                                    kmaj(row, cq * 64u + uint32_t(part) * 32u + 8u * k, A_SBO))
+                                                              : uint4{0u, 0u, 0u, 0u};
+                                        h0[4 * k] = u.x; h0[4 * k + 1] = u.y; h0[4 * k + 2] = u.z; h0[4 * k + 3] = u.w;
+                                    }
+                                } else {
+#pragma unroll
+                                    for (int k = 0; k < 16; ++k) h0[k] = hold[part * 16 + k];
+                                }
+                                tmem_st16(a_col + cq * 32u + uint32_t(part) * 16u, h0);
+                            }
+                        }
+#pragma unroll
+                        for (int blk = 0; blk < 4; ++blk) {
+                            uint32_t v[16];
+                            tmem_ld16(acc + cq * 64u + uint32_t(blk) * 16u, v);
+                            tmem_wait_ld(v);
+                            // the accumulator may be overwritten once all blocks are loaded
+                            if (blk == 3) arrive(bar_accf + 8 * b);
+                            const uint32_t c = col + uint32_t(blk) * 16u;
+                            uint32_t w8[8];
+                            if constexpr (DIR == BWD) {
+                                const uint4 z2[2] = {zs[0], zs[1]};
+                                if (blk < 3) {
+                                    // the next block's Z, while this one is processed
+#pragma unroll
+                                    for (int k = 0; k < 2; ++k)
+                                        zs[k] = valid ? *reinterpret_cast<const uint4*>(
+                                                            zl + tile_off + kmaj(row, c + 16 + 8 * k, A_SBO))
+                                                      : uint4{0u, 0u, 0u, 0u};
+                                }
+                                backward16_words(v, z2, scale, dt ? dt + kmaj(row, c, A_SBO) : nullptr, w8);
+                            } else {
+                                hidden16_words<DIR>(v, g.params + mlp_b_off(l) + c,
+                                                    zt ? zt + kmaj(row, c, A_SBO) : nullptr, w8);
+                            }
+                            if (h == 0) {
+                                if constexpr (DIR != BWD) {
+#pragma unroll
+                                    for (int k = 0; k < 8; ++k) hold[blk * 8 + k] = w8[k];
+                                }
+                            } else if (write_a) {
+                                tmem_st8(a_col + 64u + cq * 32u + uint32_t(blk) * 8u, w8);
+                            }
+                        }
+                        if (write_a) tmem_wait_st();
+                    }
+                    // after the layer's last group: the tile's A columns are ready
+                    if (h == nh - 1) {
+                        const bool last = l == S - 1, more = p + 1 < my_pairs;
+                        if (last && more) load_input(p + 1);
+                        if (!last || more) arrive(bar_ardy + 8 * b);
+                    }
+                }
+            }
+        if constexpr (DIR == FWD) {
+            if (cq == 0 && loss_dst) {
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) loss += __shfl_xor_sync(0xFFFFFFFFu, loss, o);
+                if (lane == 0) atomicAdd(loss_dst, loss / float(g.n_rows));
+            }
+        }
+    }
+    __syncthreads();
+    grid_dependents_go();
+    if (*abort_flag && threadIdx.x == 0) atomicOr(g.status, 2u);
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+    }
+}
+
 // The chains run as single CTAs (cta_group::1) unless MGK_SURROGATE_PAIRS=1
 // selects CTA pairs (cta_group::2: each SM streams half of every weight
 // chunk).  Both give the same bits; on B200 the pairs measured slower (the
@@ -641,9 +1077,39 @@ bool use_pairs() {
 
 // pdl: launched as a programmatic dependent of the previous kernel in the
 // stream (its set-up overlaps that kernel's tail).
+// The TMEM kernel (activations in tensor memory) instead of the
+// shared-memory one: MGK_SURROGATE_CHAIN=tmem.  Same bits; on B200 it
+// measured slower (inference 594 against 814-833 TFLOP/s, training chains
+// 68 + 77 against 60 + 63 us per step).
+bool use_tmem_chain() {
+    const char* v = std::getenv("MGK_SURROGATE_CHAIN");
+    return v && std::strcmp(v, "tmem") == 0;
+}
+
 template <int DIR>
 cudaError_t launch_chain(const ChainArgs& a, int sm_count, cudaStream_t st, bool pdl = false) {
     if (a.n_tiles == 0) return cudaSuccess;
+    if (!use_pairs() && use_tmem_chain()) {
+        static bool attr = false;
+        if (!attr) {
+            cudaError_t e = cudaFuncSetAttribute(k_mlp_chain_ta<DIR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 ta::SMEM_BYTES);
+            if (e != cudaSuccess) return e;
+            attr = true;
+        }
+        const uint32_t grid = a.n_tiles < uint32_t(sm_count) ? a.n_tiles : uint32_t(sm_count);
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        at[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.gridDim = dim3(grid, 1, 1);
+        cfg.blockDim = dim3(THREADS, 1, 1);
+        cfg.dynamicSmemBytes = ta::SMEM_BYTES;
+        cfg.stream = st;
+        cfg.attrs = at;
+        cfg.numAttrs = pdl ? 1 : 0;
+        return cudaLaunchKernelEx(&cfg, k_mlp_chain_ta<DIR>, a);
+    }
     if (!use_pairs()) {
         static bool attr = false;
         if (!attr) {

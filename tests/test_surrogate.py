@@ -108,12 +108,16 @@ def test_forward_matches_oracle(ctx, n, path):
 
 
 @pytest.mark.gpu
-def test_cta_pair_chains_equal_single_cta(ctx):
-    """The chains as CTA pairs (MGK_SURROGATE_PAIRS=1: cta_group::2 MMAs of
-    M = 256, each SM holding half of every weight chunk) against single CTAs
-    (the default): the same inference outputs and the same gradient and
-    loss, on an odd tile count with a ragged last tile."""
+@pytest.mark.parametrize("variant", [("MGK_SURROGATE_PAIRS", "1"), ("MGK_SURROGATE_CHAIN", "tmem")])
+def test_chain_variants_equal_default(ctx, variant):
+    """The opt-in chain kernels against the default (single CTAs, activations
+    in shared memory): CTA pairs (cta_group::2 MMAs of M = 256, each SM
+    holding half of every weight chunk) and the activations in tensor memory
+    (tcgen05.mma with A from TMEM, N-halves of 128).  The same inference
+    outputs and the same gradient, the loss to its summation order, on an odd
+    tile count with a ragged last tile."""
     import os
+    key, val = variant
     net = M.Surrogate(ctx, seed=7)
     net.set_params(O.init_params(41))
     f, lab = O.random_batch(70_001, 42)
@@ -123,14 +127,15 @@ def test_cta_pair_chains_equal_single_cta(ctx):
     d_lab = _dev(lab[:n].view(np.int32).reshape(n, 8))
     res = {}
     try:
-        for mode in ("0", "1"):
-            os.environ["MGK_SURROGATE_PAIRS"] = mode
+        for on in (False, True):
+            if on:
+                os.environ[key] = val
             out = net.forward(x).cpu().numpy()
             loss, g = net.gradient(cfg, x[:n].contiguous(), d_lab)
-            res[mode] = (out, loss, g)
+            res[on] = (out, loss, g)
     finally:
-        del os.environ["MGK_SURROGATE_PAIRS"]
-    (o0, l0, g0), (o1, l1, g1) = res["0"], res["1"]
+        os.environ.pop(key, None)
+    (o0, l0, g0), (o1, l1, g1) = res[False], res[True]
     assert np.array_equal(o0, o1), np.abs(o0 - o1).max()
     assert np.array_equal(g0, g1), np.abs(g0 - g1).max()
     assert abs(l0 - l1) <= 1e-6 * abs(l0)
