@@ -55,13 +55,17 @@ using namespace act;
 // two MMA halves of 128.  H_L comes in as Z_L and is made in place.  A stage
 // passes full (the bulk copies landed) -> conv (the epilogue warps made H and
 // took the column sums) -> the MMAs -> empty (their commit).
-constexpr int DW_STAGES = 3;
+// The ring: 3 stages of 64 KB for a 256-column layer, 5 of 36 KB for W1 and
+// W5 (whose B half tile is 2 KB), in the same 192 KB.
 constexpr uint32_t DW_A_BYTES = 32768, DW_B_BYTES = 32768;
-constexpr uint32_t DW_STAGE = DW_A_BYTES + DW_B_BYTES;
+constexpr uint32_t DW_RING = 3 * (DW_A_BYTES + DW_B_BYTES);
+constexpr int DW_MAX_SLOTS = 5;
+constexpr uint32_t DW_LIGHT_STAGE = DW_A_BYTES + 4096;
+static_assert(DW_MAX_SLOTS * DW_LIGHT_STAGE <= DW_RING, "light ring");
 constexpr int DW_EPI_WARPS = 16;
 constexpr int DW_THREADS = 32 * (2 + DW_EPI_WARPS);
-constexpr uint32_t DW_OFF_BAR = DW_STAGES * DW_STAGE;
-constexpr uint32_t DW_OFF_MISC = DW_OFF_BAR + 16 * 8;
+constexpr uint32_t DW_OFF_BAR = DW_RING;  // full, empty, conv per slot; done; drain
+constexpr uint32_t DW_OFF_MISC = DW_OFF_BAR + 32 * 8;
 constexpr uint32_t DW_OFF_RED = DW_OFF_MISC + 16;             // [8 row groups][16] output-bias sums
 constexpr uint32_t DW_SMEM = DW_OFF_RED + 8 * 16 * 4 + 128;
 static_assert(DW_SMEM <= 232448, "shared memory");
@@ -102,9 +106,9 @@ __global__ void __launch_bounds__(DW_THREADS, 1) k_mlp_dw_tc(DwArgs g) {
     unsigned char* smem =
         reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
     const uint32_t sbase = smem_addr(smem);
-    const uint32_t bar_full = sbase + DW_OFF_BAR, bar_empty = bar_full + DW_STAGES * 8;
-    const uint32_t bar_conv = bar_empty + DW_STAGES * 8;
-    const uint32_t bar_done = bar_conv + DW_STAGES * 8, bar_drain = bar_done + 8;
+    const uint32_t bar_full = sbase + DW_OFF_BAR, bar_empty = bar_full + DW_MAX_SLOTS * 8;
+    const uint32_t bar_conv = bar_empty + DW_MAX_SLOTS * 8;
+    const uint32_t bar_done = bar_conv + DW_MAX_SLOTS * 8, bar_drain = bar_done + 8;
     volatile uint32_t* tmem_slot = reinterpret_cast<volatile uint32_t*>(smem + DW_OFF_MISC);
     volatile uint32_t* abort_flag = reinterpret_cast<volatile uint32_t*>(smem + DW_OFF_MISC + 4);
 
@@ -121,9 +125,11 @@ __global__ void __launch_bounds__(DW_THREADS, 1) k_mlp_dw_tc(DwArgs g) {
     const uint32_t a_tile = A_BYTES, b_tile = wide ? A_BYTES : X_TILE;
     const uint32_t b_half = b_tile / 2, b_lbo = wide ? A_SBO : X_SBO;
     const uint32_t n_stages = 2 * (t1 - t0);  // half tiles
+    const uint32_t n_slot = wide ? 3u : uint32_t(DW_MAX_SLOTS);
+    const uint32_t stage = wide ? DW_A_BYTES + DW_B_BYTES : DW_LIGHT_STAGE;
 
     if (threadIdx.x == 0) {
-        for (int s = 0; s < DW_STAGES; ++s) {
+        for (int s = 0; s < DW_MAX_SLOTS; ++s) {
             mbar_init(bar_full + 8 * s, 1);
             mbar_init(bar_conv + 8 * s, 32 * DW_EPI_WARPS);  // every epilogue thread
             mbar_init(bar_empty + 8 * s, 1);                 // the MMA commit
@@ -151,17 +157,17 @@ __global__ void __launch_bounds__(DW_THREADS, 1) k_mlp_dw_tc(DwArgs g) {
             bool ok = true;
             uint32_t j = 0;
             for (; j < n_stages && ok; ++j) {
-                const uint32_t s = j % DW_STAGES, use = j / DW_STAGES;
+                const uint32_t s = j % n_slot, use = j / n_slot;
                 if (use > 0 && !mbar_wait(bar_empty + 8 * s, (use - 1) & 1u, abort_flag)) { ok = false; break; }
                 const uint32_t tile = t0 + j / 2, hf = j & 1u;
-                const uint32_t dst = sbase + s * DW_STAGE;
+                const uint32_t dst = sbase + s * stage;
                 mbar_expect_tx(bar_full + 8 * s, DW_A_BYTES + b_half);
                 bulk_g2s(dst, Am + size_t(tile) * a_tile + hf * DW_A_BYTES, DW_A_BYTES, bar_full + 8 * s);
                 bulk_g2s(dst + DW_A_BYTES, Bm + size_t(tile) * b_tile + hf * b_half, b_half, bar_full + 8 * s);
             }
-            const uint32_t first = j > DW_STAGES ? j - DW_STAGES : 0;
+            const uint32_t first = j > n_slot ? j - n_slot : 0;
             for (uint32_t k = first; k < j; ++k) {
-                const uint32_t s = k % DW_STAGES, use = k / DW_STAGES;
+                const uint32_t s = k % n_slot, use = k / n_slot;
                 for (uint32_t it = 0; it < WAIT_LIMIT && !mbar_try(bar_full + 8 * s, use & 1u); ++it) {}
             }
         }
@@ -170,10 +176,10 @@ __global__ void __launch_bounds__(DW_THREADS, 1) k_mlp_dw_tc(DwArgs g) {
             bool ok = true;
             const uint32_t idesc = idesc_bf16_major(TM, n, true, true);
             for (uint32_t j = 0; j < n_stages && ok; ++j) {
-                const uint32_t s = j % DW_STAGES, use = j / DW_STAGES;
+                const uint32_t s = j % n_slot, use = j / n_slot;
                 if (!mbar_wait(bar_conv + 8 * s, use & 1u, abort_flag)) { ok = false; break; }
                 tc_fence_after();
-                const uint32_t sa = sbase + s * DW_STAGE, sb = sa + DW_A_BYTES;
+                const uint32_t sa = sbase + s * stage, sb = sa + DW_A_BYTES;
                 // 64 rows of K: 4 steps of 16 rows, two 8-row groups each
                 for (uint32_t ks = 0; ks < 4; ++ks)
                     for (uint32_t mh = 0; mh < 2; ++mh) {
@@ -202,9 +208,9 @@ __global__ void __launch_bounds__(DW_THREADS, 1) k_mlp_dw_tc(DwArgs g) {
         for (int e = 0; e < 8; ++e) csum[e] = 0.f;
         bool ok = true;
         for (uint32_t j = 0; j < n_stages && ok; ++j) {
-            const uint32_t s = j % DW_STAGES, use = j / DW_STAGES;
+            const uint32_t s = j % n_slot, use = j / n_slot;
             if (!mbar_wait(bar_full + 8 * s, use & 1u, abort_flag)) { ok = false; break; }
-            unsigned char* sa = smem + s * DW_STAGE;
+            unsigned char* sa = smem + s * stage;
             unsigned char* sb = sa + DW_A_BYTES;
             if (L >= 1) {
                 // the 32 KB half tile of Z (B for L = 1..3, A for L = 4) -> H
@@ -325,10 +331,11 @@ size_t mlp_dw_partial_floats(uint32_t jobs) { return size_t(jobs) * DW_PART; }
 
 DwJobs mlp_dw_jobs(uint32_t n_tiles, int sm_count) {
     // CTAs in proportion to a tile's cost in each kind of job (measured on
-    // B200: 6.2, 3.4 and 4.2 thousand cycles per tile for a 256-column
-    // layer, W1 and W5), so that the jobs end together
+    // B200 from the spans of the jobs: 2.95, 1.55 and 1.90 us per tile for a
+    // 256-column layer, W1 and W5), so that the jobs end together
     const uint32_t sms = uint32_t(sm_count > 8 ? sm_count : 8);
-    uint32_t l4 = uint32_t(double(sms) * 4.2 / 26.2 + 0.5), l0 = uint32_t(double(sms) * 3.4 / 26.2 + 0.5);
+    const double unit = double(sms) / (3 * 2.95 + 1.55 + 1.90);
+    uint32_t l4 = uint32_t(unit * 1.90 + 0.5), l0 = uint32_t(unit * 1.55 + 0.5);
     uint32_t h = (sms - l0 - l4) / 3;
     DwJobs j;
     j.heavy = h < 1 ? 1 : (h > n_tiles ? n_tiles : h);
