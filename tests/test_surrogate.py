@@ -304,6 +304,34 @@ def test_data_parallel_loop_on_one_rank_is_train(ctx):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("switch", ["MGK_SURROGATE_GRAPH", "MGK_SURROGATE_PDL"])
+def test_counted_training_replay_equals_launches(ctx, switch):
+    """mgk_surrogate_train replays epochs after the first from a CUDA graph
+    and launches its kernels as programmatic dependents; with either turned
+    off (the same kernels as ordinary launches) it takes the same steps: the
+    same parameters bit for bit, the epoch losses to their summation order."""
+    import os
+    s = small_scene(width=128, height=64, spp=1, precision=abi.PRECISION_F64)
+    feat, lab = _samples(ctx, s, s.width * s.height * 2, 5)
+    cfg = M.train_defaults(batch=4096, epochs=3)
+    runs = []
+    for off in (False, True):
+        net = M.Surrogate(ctx, seed=3)
+        if off:
+            os.environ[switch] = "0"
+        try:
+            losses = net.train(cfg, feat, lab)
+        finally:
+            os.environ.pop(switch, None)
+        runs.append((net.get_params(), losses))
+        assert net.status() == 0
+        net.close()
+    (pa, la), (pb, lb) = runs
+    assert np.array_equal(pa, pb)
+    np.testing.assert_allclose(la, lb, rtol=1e-5)
+
+
+@pytest.mark.gpu
 def test_routed_render_all_fallback_equals_integrator(ctx):
     """conf_min above 1 sends every ray to RKF45: the film must equal mgk_render's."""
     import torch
