@@ -509,7 +509,15 @@ MGK_API mgk_result mgk_surrogate_gradient(mgk_surrogate* net, const mgk_train_co
                                           const mgk_sample_label* d_labels, uint32_t n, float* h_grad,
                                           float* h_loss);
 /* Adam training over the sample set; h_epoch_loss (may be NULL) receives the
- * mean batch loss of each epoch.  Synchronous. */
+ * mean batch loss of each epoch.  Synchronous.  On the tensor-core path the
+ * run is driven from the device (step and batch counters, tables of the
+ * Adam constants and order keys) and the epochs after the first replay a
+ * CUDA graph of one epoch, kept for later calls with the same data, shapes
+ * and loss weights; the host waits once, at the end.  Environment (read per
+ * call): MGK_SURROGATE_GRAPH=0 launches every epoch, MGK_SURROGATE_PDL=0
+ * launches without programmatic dependences, MGK_SURROGATE_PAIRS=1 and
+ * MGK_SURROGATE_CHAIN=tmem select the CTA-pair and tensor-memory layer
+ * chains (the same results; slower on B200). */
 MGK_API mgk_result mgk_surrogate_train(mgk_surrogate* net, const mgk_train_config* cfg, const float* d_features,
                                        const mgk_sample_label* d_labels, uint32_t n, float* h_epoch_loss,
                                        void* stream);
