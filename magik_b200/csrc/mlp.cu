@@ -14,12 +14,18 @@
 //  k_loss      loss and d(loss)/d(out) of a batch
 //  k_adam      Adam update of the FP32 master parameters and the BF16 copies
 //  k_gather    batch assembly (features, labels) from a permutation
+#include <algorithm>
 #include <cstdint>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include "mlp.h"
 #include "mlp_loss.cuh"
+#include "tc_sm100.cuh"
+
+#ifndef MGK_ADAM_BULK_ROWS
+#define MGK_ADAM_BULK_ROWS 40u
+#endif
 
 namespace mgk {
 
@@ -346,24 +352,52 @@ cudaError_t launch_adam(float* p, const float* g, float* m, float* v, __nv_bfloa
 // block reads ctr->step before it counts itself done, so the last block's
 // advance comes after all reads.
 __global__ void k_adam_counted(float* __restrict__ p, const float* __restrict__ grad, const float* __restrict__ part,
-                               DwJobs jobs, float* __restrict__ m, float* __restrict__ v,
+                               DwJobs jobs, uint32_t max_rows, float* __restrict__ m, float* __restrict__ v,
                                __nv_bfloat16* __restrict__ bf16_copy, __nv_bfloat16* __restrict__ img,
                                __nv_bfloat16* __restrict__ img_t, int n, const AdamStep* __restrict__ table,
                                TrainCounters* ctr) {
     __shared__ AdamStep a;
+    __shared__ __align__(8) uint64_t bar;
+    extern __shared__ __align__(16) float rows[];  // [jobs of this block's parameters][256]
     asm volatile("griddepcontrol.wait;" ::: "memory");
     const uint32_t step = *reinterpret_cast<volatile uint32_t*>(&ctr->step);
-    if (threadIdx.x == 0) a = table[step];
+    // the block's 256 parameters lie in one segment of the parameter vector
+    // (all segment boundaries are multiples of 256): where their partials
+    // are contiguous (all but W5's transpose), one thread brings the jobs'
+    // rows of 1 KB into shared memory with bulk copies
+    const uint32_t i0 = blockIdx.x * blockDim.x;
+    uint32_t j0, nj, src0, d0, d1, src1;
+    mlp_dw_source(i0, jobs, &j0, &nj, &src0);
+    mlp_dw_source(i0 + 1, jobs, &d0, &d1, &src1);
+    const bool bulk = part && blockDim.x == 256 && src1 == src0 + 1 && nj <= max_rows;
+    const uint32_t b_addr = tc::smem_addr(&bar);
+    if (threadIdx.x == 0) {
+        a = table[step];
+        if (bulk) {
+            tc::mbar_init(b_addr, 1);
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+            tc::mbar_expect_tx(b_addr, nj * 1024u);
+            for (uint32_t k = 0; k < nj; ++k)
+                tc::bulk_g2s(tc::smem_addr(rows + k * 256), part + size_t(j0 + k) * MLP_DW_PART + src0, 1024u, b_addr);
+        }
+    }
     __syncthreads();
+    bool landed = false;
+    if (bulk)
+        for (uint32_t it = 0; it < tc::SLEEP_LIMIT && !landed; ++it) landed = tc::mbar_try_sleep(b_addr, 0, 1000000u);
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) {
         float gs;
         if (part) {
-            uint32_t j0, nj, src;
-            mlp_dw_source(uint32_t(i), jobs, &j0, &nj, &src);
+            uint32_t pj0, pnj, src;
+            mlp_dw_source(uint32_t(i), jobs, &pj0, &pnj, &src);
             gs = 0.f;
+            if (landed) {
+                for (uint32_t k = 0; k < pnj; ++k) gs += rows[k * 256 + threadIdx.x];
+            } else {
 #pragma unroll 8
-            for (uint32_t k = 0; k < nj; ++k) gs += part[size_t(j0 + k) * MLP_DW_PART + src];
+                for (uint32_t k = 0; k < pnj; ++k) gs += part[size_t(pj0 + k) * MLP_DW_PART + src];
+            }
         } else {
             gs = grad[i];
         }
@@ -385,6 +419,9 @@ __global__ void k_adam_counted(float* __restrict__ p, const float* __restrict__ 
             if (img_t && t != ~0u) img_t[t / 2] = w;
         }
     }
+    // no copy may still be landing in this block's shared memory when it exits
+    if (bulk && !landed && threadIdx.x == 0)
+        for (uint32_t it = 0; it < tc::SLEEP_LIMIT && !tc::mbar_try_sleep(b_addr, 0, 1000000u); ++it) {}
     __syncthreads();
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     if (threadIdx.x == 0) {
@@ -405,12 +442,17 @@ cudaError_t launch_adam_counted(float* p, const float* g, const float* part, con
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     at[0].val.programmaticStreamSerializationAllowed = 1;
+    // room for the partial rows of the largest job kind (at most
+    // MGK_ADAM_BULK_ROWS rows of 1 KB; 0: every partial read directly)
+    const uint32_t max_rows =
+        part ? std::min<uint32_t>(MGK_ADAM_BULK_ROWS, std::max(jobs.heavy, std::max(jobs.l0, jobs.l4))) : 0u;
     cfg.gridDim = dim3((n + 255) / 256, 1, 1);
     cfg.blockDim = dim3(256, 1, 1);
+    cfg.dynamicSmemBytes = max_rows * 1024u;
     cfg.stream = st;
     cfg.attrs = at;
     cfg.numAttrs = pdl ? 1 : 0;
-    cudaError_t e = cudaLaunchKernelEx(&cfg, k_adam_counted, p, g, part, jobs, m, v, copy,
+    cudaError_t e = cudaLaunchKernelEx(&cfg, k_adam_counted, p, g, part, jobs, max_rows, m, v, copy,
                                        static_cast<__nv_bfloat16*>(img), static_cast<__nv_bfloat16*>(img_t), n,
                                        table, ctr);
     if (e != cudaSuccess) return e;
