@@ -162,6 +162,14 @@ cudaError_t launch_mlp_fwd_stash_tc(const void* img, const float* params, const 
                                     const LossWeights& w, void* dout_tiles, float* loss_acc, uint32_t n_tiles,
                                     const TrainCounters* ctr, uint32_t* status, int sm_count, cudaStream_t st,
                                     bool pdl = false);
+// The forward (as above, with labels) and the input-gradient chain in one
+// kernel: each tile's backward runs right after its forward, dOut handed
+// over in shared memory (and written to dout_tiles for the weight gradients).
+cudaError_t launch_mlp_fwd_bwd_tc(const void* img, const void* img_t, const float* params, const float* feat,
+                                  const uint32_t* perm, uint32_t b0, void* x0_tiles, void* const* z, void* const* dz,
+                                  const SampleLabel* lab, const LossWeights& w, void* dout_tiles, float* loss_acc,
+                                  uint32_t n_tiles, const TrainCounters* ctr, uint32_t* status, int sm_count,
+                                  cudaStream_t st, bool pdl = false);
 cudaError_t launch_mlp_bwd_dx_tc(const void* img_t, const void* dout_tiles, void* const* z, void* const* dz,
                                  uint32_t n_tiles, uint32_t* status, int sm_count, cudaStream_t st, bool pdl = false);
 DwJobs mlp_dw_jobs(uint32_t n_tiles, int sm_count);

@@ -103,7 +103,7 @@ template <bool PAIR> struct Layout {
     static_assert(smem_bytes <= 232448, "shared memory");
 };
 
-enum { INFER = 0, FWD = 1, BWD = 2 };
+enum { INFER = 0, FWD = 1, BWD = 2, FB = 3 };  // FB: forward then backward, per tile
 
 }  // namespace
 
@@ -147,7 +147,8 @@ __global__ void k_weight_image(const __nv_bfloat16* __restrict__ wb, unsigned ch
 namespace {
 
 struct ChainArgs {
-    const unsigned char* img;  // weight image (BWD: the transposed image)
+    const unsigned char* img;    // weight image (BWD: the transposed image)
+    const unsigned char* img_t;  // FB: the transposed image of the backward steps
     const float* params;       // FP32 parameters (biases)
     const float* feat;         // INFER: features [n_rows][7]; FWD: the sample set's features
     const uint32_t* perm;      // FWD: the batch is rows perm[b0 ..] of the sample set
@@ -253,7 +254,13 @@ __device__ __forceinline__ void backward16(const uint32_t (&v)[16], const uint4 
 
 template <int DIR, bool PAIR>
 __global__ void __launch_bounds__(THREADS, 1) k_mlp_chain_tc(ChainArgs g) {
-    constexpr int S = DIR == BWD ? MLP_LAYERS - 1 : MLP_LAYERS;  // steps per tile
+    // steps per tile: FB runs the forward's five, then the backward's four
+    constexpr int S = DIR == BWD ? MLP_LAYERS - 1 : (DIR == FB ? 2 * MLP_LAYERS - 1 : MLP_LAYERS);
+    constexpr bool FWDLIKE = DIR == FWD || DIR == FB;  // gathers its input, stashes Z, takes the loss
+    static_assert(!(PAIR && DIR == FB), "the forward-and-backward chain runs as single CTAs");
+    // step l of a tile: a backward step?  Its index within its chain
+    auto bwd_step = [](int l) { return DIR == BWD || (DIR == FB && l >= MLP_LAYERS); };
+    auto step_in = [](int l) { return DIR == FB && l >= MLP_LAYERS ? l - MLP_LAYERS : l; };
     using LY = Layout<PAIR>;
     constexpr int N_SLOT = LY::slots;
     constexpr uint32_t SLOT_BYTES = LY::slot_bytes, OFF_A = LY::off_a, OFF_W = LY::off_w, OFF_MISC = LY::off_misc;
@@ -322,8 +329,8 @@ __global__ void __launch_bounds__(THREADS, 1) k_mlp_chain_tc(ChainArgs g) {
     // everything above overlaps the previous kernel's tail when launched as its dependent
     grid_dependency_wait();
     // FWD: the batch's first row in the order, and where its loss goes
-    const uint32_t b0 = g.b0 + (DIR == FWD && g.ctr ? g.ctr->batch * g.n_rows : 0u);
-    float* const loss_dst = DIR == FWD && g.loss_acc ? g.loss_acc + (g.ctr ? g.ctr->epoch - 1u : 0u) : nullptr;
+    const uint32_t b0 = g.b0 + (FWDLIKE && g.ctr ? g.ctr->batch * g.n_rows : 0u);
+    float* const loss_dst = FWDLIKE && g.loss_acc ? g.loss_acc + (g.ctr ? g.ctr->epoch - 1u : 0u) : nullptr;
 
     if (warp == 0) {
         // ------------------------------------------------------------ producer
@@ -334,7 +341,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_mlp_chain_tc(ChainArgs g) {
             for (uint32_t p = 0; p < my_pairs && ok; ++p)
                 for (int l = 0; l < S && ok; ++l)
                     for (uint32_t b = 0; b < 2 && ok; ++b) {
-                        const Step st = step_of(l);
+                        const Step st = step_of(step_in(l));
                         if constexpr (DIR == BWD) {
                             // the Z tiles the epilogue reads for silu', one step ahead, into L2
                             const uint32_t tile = tile_of(p, b);
@@ -354,7 +361,8 @@ __global__ void __launch_bounds__(THREADS, 1) k_mlp_chain_tc(ChainArgs g) {
                             const int c = st.c0 + ci;
                             const uint32_t bytes = PAIR ? mlp_chunk_bytes(c) / 2 : mlp_chunk_bytes(c);
                             mbar_expect_tx(bar_full + 8 * s, bytes);
-                            bulk_g2s(sbase + OFF_W + s * SLOT_BYTES, g.img + mlp_chunk_offset(c) + rank * bytes, bytes,
+                            const unsigned char* img = DIR == FB && bwd_step(l) ? g.img_t : g.img;
+                            bulk_g2s(sbase + OFF_W + s * SLOT_BYTES, img + mlp_chunk_offset(c) + rank * bytes, bytes,
                                      bar_full + 8 * s);
                         }
                     }
@@ -377,7 +385,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_mlp_chain_tc(ChainArgs g) {
                         if (PAIR && !mbar_wait_cluster(bar_pa + 8 * b, ar[b] & 1u, abort_flag)) { ok = false; break; }
                         ++ar[b];
                         tc_fence_after();
-                        const Step st = step_of(l);
+                        const Step st = step_of(step_in(l));
                         const uint32_t idesc = idesc_bf16(PAIR ? 2 * TM : TM, st.n);
                         const uint32_t a_base = sbase + OFF_A + b * A_BYTES;
                         const uint32_t d = tmem + b * 256u;
@@ -415,7 +423,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_mlp_chain_tc(ChainArgs g) {
             for (uint32_t p = 0; p < my_pairs && ok; ++p)
                 for (int l = 0; l < S && ok; ++l)
                     for (uint32_t b = 0; b < 2 && ok; ++b) {
-                        const Step st = step_of(l);
+                        const Step st = step_of(step_in(l));
                         for (int ci = 0; ci < st.nc; ++ci, ++j) {
                             const uint32_t s = j % N_SLOT, use = j / N_SLOT;
                             if (!mbar_wait(bar_full + 8 * s, use & 1u, abort_flag)) { ok = false; break; }
@@ -439,13 +447,13 @@ __global__ void __launch_bounds__(THREADS, 1) k_mlp_chain_tc(ChainArgs g) {
             if constexpr (DIR != BWD) {
                 const uint32_t r = tile * TM + row;
                 if (tile < n_tiles && r < g.n_rows) {
-                    const size_t src = DIR == FWD ? size_t(g.perm[b0 + r]) : size_t(r);
+                    const size_t src = FWDLIKE ? size_t(g.perm[b0 + r]) : size_t(r);
                     float f[8];
 #pragma unroll
                     for (int k = 0; k < 8; ++k) f[k] = k < MLP_IN ? g.feat[src * MLP_IN + k] : 0.f;
                     c0 = uint4{pack_bf16(f[0], f[1]), pack_bf16(f[2], f[3]), pack_bf16(f[4], f[5]),
                                pack_bf16(f[6], f[7])};
-                    if constexpr (DIR == FWD) {
+                    if constexpr (FWDLIKE) {
                         unsigned char* dst = g.x0 + size_t(tile) * X_TILE + kmaj(row, 0, X_SBO);
                         *reinterpret_cast<uint4*>(dst) = c0;
                         *reinterpret_cast<uint4*>(dst + 128) = c1;
@@ -490,11 +498,13 @@ __global__ void __launch_bounds__(THREADS, 1) k_mlp_chain_tc(ChainArgs g) {
                     const size_t tile_off = size_t(tile) * A_BYTES;
                     unsigned char* const A = smem + OFF_A + b * A_BYTES;
                     const uint32_t tb = t_q + b * 256u;
-                    const int li = DIR == BWD ? 3 - l : l;  // the Z (and dZ) of this step
+                    const bool bw = bwd_step(l);
+                    const int sl = step_in(l);
+                    const int li = bw ? 3 - sl : sl;  // the Z (and dZ) of this step
                     unsigned char* const zl = li == 0 ? g.z[0] : (li == 1 ? g.z[1] : (li == 2 ? g.z[2] : g.z[3]));
                     // BWD: the first 32 of this warp's 64 columns of Z, loaded while the MMAs run
                     uint4 zs[4];
-                    if constexpr (DIR == BWD) {
+                    if (bw) {
 #pragma unroll
                         for (int k = 0; k < 4; ++k)
                             zs[k] = valid ? *reinterpret_cast<const uint4*>(zl + tile_off +
@@ -504,14 +514,14 @@ __global__ void __launch_bounds__(THREADS, 1) k_mlp_chain_tc(ChainArgs g) {
                     if (!mbar_wait(bar_d + 8 * b, dr[b] & 1u, abort_flag)) { ok = false; break; }
                     ++dr[b];
                     tc_fence_after();
-                    if constexpr (DIR == BWD) {
+                    if (bw) {
                         // dZ_{li} = scale acc * silu'(Z_{li}); W5 is stored whole, W4..W2 halved;
                         // 4 blocks of 16 columns
-                        const float scale = l > 0 ? 2.0f : 1.0f;
+                        const float scale = sl > 0 ? 2.0f : 1.0f;
                         unsigned char* const dzl =
                             li == 0 ? g.dz[0] : (li == 1 ? g.dz[1] : (li == 2 ? g.dz[2] : g.dz[3]));
                         const uint32_t c0 = cq * 64;
-                        unsigned char* const an = l < S - 1 ? A + kmaj(row, c0, A_SBO) : nullptr;
+                        unsigned char* const an = sl < MLP_LAYERS - 2 ? A + kmaj(row, c0, A_SBO) : nullptr;
                         unsigned char* const dn = valid ? dzl + tile_off + kmaj(row, c0, A_SBO) : nullptr;
                         const uint4 z0[2] = {zs[0], zs[1]}, z1[2] = {zs[2], zs[3]};
                         uint32_t v[16];
@@ -536,7 +546,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_mlp_chain_tc(ChainArgs g) {
                         tmem_ld16(tb + c0 + 48, v);
                         tmem_wait_ld(v);
                         backward16(v, z3, scale, an ? an + 768 : nullptr, dn ? dn + 768 : nullptr);
-                    } else if (l == 4) {
+                    } else if (sl == 4) {
                         // the outputs: bias; FWD: the loss and dOut
                         if (cq == 0) {
                             uint32_t v[16];
@@ -560,7 +570,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_mlp_chain_tc(ChainArgs g) {
                                     for (int k = 0; k < 4; ++k)
                                         op[k] = make_float4(o[4 * k], o[4 * k + 1], o[4 * k + 2], o[4 * k + 3]);
                                 }
-                                if constexpr (DIR == FWD) {
+                                if constexpr (FWDLIKE) {
                                     if (g.lab) {
                                         float d[MLP_OUT_PAD];
                                         loss += mlp_row_loss(o, g.lab[g.perm[b0 + r]], g.w, d);
@@ -572,6 +582,11 @@ __global__ void __launch_bounds__(THREADS, 1) k_mlp_chain_tc(ChainArgs g) {
                                         unsigned char* dst = g.dout + size_t(tile) * X_TILE + kmaj(row, 0, X_SBO);
                                         *reinterpret_cast<uint4*>(dst) = uint4{dv[0], dv[1], dv[2], dv[3]};
                                         *reinterpret_cast<uint4*>(dst + 128) = uint4{dv[4], dv[5], dv[6], dv[7]};
+                                        if constexpr (DIR == FB) {
+                                            // dOut is also the backward's first input
+                                            *reinterpret_cast<uint4*>(A + kmaj(row, 0, A_SBO)) = uint4{dv[0], dv[1], dv[2], dv[3]};
+                                            *reinterpret_cast<uint4*>(A + kmaj(row, 8, A_SBO)) = uint4{dv[4], dv[5], dv[6], dv[7]};
+                                        }
                                     }
                                 }
                             }
@@ -579,25 +594,25 @@ __global__ void __launch_bounds__(THREADS, 1) k_mlp_chain_tc(ChainArgs g) {
                     } else {
                         // hidden layer: z = 2 acc + b (INFER: u = z / 2 = acc + b / 2), H = silu(z)
                         // into the next step's operand; FWD: Z to the stash
-                        const float* bl = g.params + mlp_b_off(l) + cq * 64;
+                        const float* bl = g.params + mlp_b_off(sl) + cq * 64;
                         // 4 blocks of 16 columns, the TMEM load of the next block in flight
                         // while a block is processed
                         const uint32_t c0 = cq * 64;
                         unsigned char* const an = A + kmaj(row, c0, A_SBO);
-                        unsigned char* const zn = (DIR == FWD && valid) ? zl + tile_off + kmaj(row, c0, A_SBO) : nullptr;
+                        unsigned char* const zn = (FWDLIKE && valid) ? zl + tile_off + kmaj(row, c0, A_SBO) : nullptr;
                         uint32_t va[16], vb[16];
                         tmem_ld16(tb + c0, va);
                         tmem_wait_ld(va);
                         tmem_ld16(tb + c0 + 16, vb);
-                        hidden16<DIR>(va, bl, an, zn);
+                        hidden16<DIR == FB ? FWD : DIR>(va, bl, an, zn);
                         tmem_wait_ld(vb);
                         tmem_ld16(tb + c0 + 32, va);
-                        hidden16<DIR>(vb, bl + 16, an + 256, zn ? zn + 256 : nullptr);
+                        hidden16<DIR == FB ? FWD : DIR>(vb, bl + 16, an + 256, zn ? zn + 256 : nullptr);
                         tmem_wait_ld(va);
                         tmem_ld16(tb + c0 + 48, vb);
-                        hidden16<DIR>(va, bl + 32, an + 512, zn ? zn + 512 : nullptr);
+                        hidden16<DIR == FB ? FWD : DIR>(va, bl + 32, an + 512, zn ? zn + 512 : nullptr);
                         tmem_wait_ld(vb);
-                        hidden16<DIR>(vb, bl + 48, an + 768, zn ? zn + 768 : nullptr);
+                        hidden16<DIR == FB ? FWD : DIR>(vb, bl + 48, an + 768, zn ? zn + 768 : nullptr);
                     }
                     tc_fence_before();
                     const bool last = l == S - 1, more = p + 1 < my_pairs;
@@ -607,7 +622,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_mlp_chain_tc(ChainArgs g) {
                         arrive_a(b);
                     }
                 }
-        if constexpr (DIR == FWD) {
+        if constexpr (FWDLIKE) {
             if (cq == 0 && loss_dst) {
 #pragma unroll
                 for (int o = 16; o > 0; o >>= 1) loss += __shfl_xor_sync(0xFFFFFFFFu, loss, o);
@@ -1089,6 +1104,9 @@ bool use_tmem_chain() {
 template <int DIR>
 cudaError_t launch_chain(const ChainArgs& a, int sm_count, cudaStream_t st, bool pdl = false) {
     if (a.n_tiles == 0) return cudaSuccess;
+    // the forward-and-backward chain exists only as single CTAs in shared memory
+    constexpr bool ONLY_SMEM = DIR == FB;
+    if constexpr (!ONLY_SMEM) {
     if (!use_pairs() && use_tmem_chain()) {
         static bool attr = false;
         if (!attr) {
@@ -1110,7 +1128,8 @@ cudaError_t launch_chain(const ChainArgs& a, int sm_count, cudaStream_t st, bool
         cfg.numAttrs = pdl ? 1 : 0;
         return cudaLaunchKernelEx(&cfg, k_mlp_chain_ta<DIR>, a);
     }
-    if (!use_pairs()) {
+    }
+    if (ONLY_SMEM || !use_pairs()) {
         static bool attr = false;
         if (!attr) {
             cudaError_t e = cudaFuncSetAttribute(k_mlp_chain_tc<DIR, false>,
@@ -1131,6 +1150,7 @@ cudaError_t launch_chain(const ChainArgs& a, int sm_count, cudaStream_t st, bool
         cfg.numAttrs = pdl ? 1 : 0;
         return cudaLaunchKernelEx(&cfg, k_mlp_chain_tc<DIR, false>, a);
     }
+    if constexpr (!ONLY_SMEM) {
     cudaLaunchConfig_t cfg = {};
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -1159,6 +1179,8 @@ cudaError_t launch_chain(const ChainArgs& a, int sm_count, cudaStream_t st, bool
     const uint32_t pairs = units < uint32_t(max_pairs) ? units : uint32_t(max_pairs);
     cfg.gridDim = dim3(2 * pairs, 1, 1);
     return cudaLaunchKernelEx(&cfg, k_mlp_chain_tc<DIR, true>, a);
+    }
+    return cudaSuccess;
 }
 
 }  // namespace
@@ -1211,6 +1233,35 @@ cudaError_t launch_mlp_fwd_stash_tc(const void* img, const float* params, const 
     a.n_tiles = n_tiles;
     a.status = status;
     return launch_chain<FWD>(a, sm_count, st, pdl);
+}
+
+cudaError_t launch_mlp_fwd_bwd_tc(const void* img, const void* img_t, const float* params, const float* feat,
+                                  const uint32_t* perm, uint32_t b0, void* x0_tiles, void* const* z, void* const* dz,
+                                  const SampleLabel* lab, const LossWeights& w, void* dout_tiles, float* loss_acc,
+                                  uint32_t n_tiles, const TrainCounters* ctr, uint32_t* status, int sm_count,
+                                  cudaStream_t st, bool pdl) {
+    if (!lab || !dout_tiles) return cudaErrorInvalidValue;
+    ChainArgs a{};
+    a.img = static_cast<const unsigned char*>(img);
+    a.img_t = static_cast<const unsigned char*>(img_t);
+    a.params = params;
+    a.feat = feat;
+    a.perm = perm;
+    a.b0 = b0;
+    a.x0 = static_cast<unsigned char*>(x0_tiles);
+    for (int l = 0; l < 4; ++l) {
+        a.z[l] = static_cast<unsigned char*>(z[l]);
+        a.dz[l] = static_cast<unsigned char*>(dz[l]);
+    }
+    a.lab = lab;
+    a.w = w;
+    a.dout = static_cast<unsigned char*>(dout_tiles);
+    a.loss_acc = loss_acc;
+    a.ctr = ctr;
+    a.n_rows = n_tiles * TM;
+    a.n_tiles = n_tiles;
+    a.status = status;
+    return launch_chain<FB>(a, sm_count, st, pdl);
 }
 
 cudaError_t launch_mlp_bwd_dx_tc(const void* img_t, const void* dout_tiles, void* const* z, void* const* dz,

@@ -212,6 +212,16 @@ cudaError_t forward(mgk_surrogate* s, const __nv_bfloat16* x0, int B, __nv_bfloa
 // path: forward (gathering the rows) with stash and loss, input gradients,
 // weight gradients (all of grad is written); the batch mean loss is added to
 // *loss_acc.
+// The forward and backward chains as one kernel (each tile's backward right
+// after its forward) when MGK_SURROGATE_FUSED=1 and no chain variant other
+// than the shared-memory one is asked for.
+bool fused_chains() {
+    const char* f = std::getenv("MGK_SURROGATE_FUSED");
+    const char* p = std::getenv("MGK_SURROGATE_PAIRS");
+    const char* c = std::getenv("MGK_SURROGATE_CHAIN");
+    return (f && f[0] == '1') && !(p && p[0] == '1') && !(c && std::strcmp(c, "tmem") == 0);
+}
+
 cudaError_t gradient_tc(mgk_surrogate* s, const float* feat, const mgk_sample_label* lab, int b0, int B,
                         const LossWeights& w, float* loss_acc, cudaStream_t st, const TrainCounters* ctr = nullptr,
                         bool reduce = true, bool pdl = false) {
@@ -221,11 +231,17 @@ cudaError_t gradient_tc(mgk_surrogate* s, const float* feat, const mgk_sample_la
         e = launch_weight_image(s->wb, s->img, s->img_t, st);
         s->img_valid = e == cudaSuccess;
     }
-    if (e == cudaSuccess)
-        e = launch_mlp_fwd_stash_tc(s->img, s->p, feat, s->perm, uint32_t(b0), s->tx0, s->tZ, nullptr, lab, w,
-                                    s->tdout, loss_acc, tiles, ctr, s->status, s->sm_count, st, pdl);
-    if (e == cudaSuccess)
-        e = launch_mlp_bwd_dx_tc(s->img_t, s->tdout, s->tZ, s->tdZ, tiles, s->status, s->sm_count, st, pdl);
+    if (fused_chains()) {
+        if (e == cudaSuccess)
+            e = launch_mlp_fwd_bwd_tc(s->img, s->img_t, s->p, feat, s->perm, uint32_t(b0), s->tx0, s->tZ, s->tdZ, lab,
+                                      w, s->tdout, loss_acc, tiles, ctr, s->status, s->sm_count, st, pdl);
+    } else {
+        if (e == cudaSuccess)
+            e = launch_mlp_fwd_stash_tc(s->img, s->p, feat, s->perm, uint32_t(b0), s->tx0, s->tZ, nullptr, lab, w,
+                                        s->tdout, loss_acc, tiles, ctr, s->status, s->sm_count, st, pdl);
+        if (e == cudaSuccess)
+            e = launch_mlp_bwd_dx_tc(s->img_t, s->tdout, s->tZ, s->tdZ, tiles, s->status, s->sm_count, st, pdl);
+    }
     if (e == cudaSuccess)
         e = launch_mlp_dw_tc(s->tdZ, s->tZ, s->tx0, s->tdout, s->dw_part, s->grad, tiles, s->dw_jobs, s->status, st,
                              reduce, pdl);
