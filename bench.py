@@ -373,8 +373,9 @@ def run_surrogate(args, ctx, s, d_stars, d_w, film_mixed_ms, steps):
         "training": {"samples": args.surrogate_samples, "epochs": args.surrogate_epochs, "batch": cfg.batch,
                      "sample_generation_s": t_samples, "train_s": t_train,
                      "train_tflops": train_flop / t_train / 1e12, "epoch_loss": [float(v) for v in losses],
-                     "path": "tcgen05 (fused forward with stash, fused input-gradient chain, split-K weight "
-                             "gradients; activations in tensor-core tiles)",
+                     "path": "tcgen05 (one kernel per tile: forward with stash and loss, then the input-"
+                             "gradient chain; split-K weight gradients; Adam on device-side step counters; "
+                             "one CUDA graph per epoch)",
                      "mma_sync_path_tflops": mma_tflops,
                      "flop_count": "3 x 400,896 FLOP per sample per step (forward, input and weight gradients)",
                      "distribution": "observer r U[10,100] M, inclination U[0,90] deg, spin U[0,0.998] "

