@@ -351,6 +351,10 @@ cudaError_t launch_adam(float* p, const float* g, float* m, float* v, __nv_bfloa
 // Adam with the constants of the current step of a counted run.  Every
 // block reads ctr->step before it counts itself done, so the last block's
 // advance comes after all reads.
+// Launched as the dependent of the weight gradients, a block loads before
+// its griddepcontrol.wait what only earlier kernels wrote: the step counter
+// and constants, m, v and p (the Adam of the step before, whose completion
+// the kernels in between waited for); the partials after it.
 __global__ void k_adam_counted(float* __restrict__ p, const float* __restrict__ grad, const float* __restrict__ part,
                                DwJobs jobs, uint32_t max_rows, float* __restrict__ m, float* __restrict__ v,
                                __nv_bfloat16* __restrict__ bf16_copy, __nv_bfloat16* __restrict__ img,
@@ -359,8 +363,14 @@ __global__ void k_adam_counted(float* __restrict__ p, const float* __restrict__ 
     __shared__ AdamStep a;
     __shared__ __align__(8) uint64_t bar;
     extern __shared__ __align__(16) float rows[];  // [jobs of this block's parameters][256]
-    asm volatile("griddepcontrol.wait;" ::: "memory");
     const uint32_t step = *reinterpret_cast<volatile uint32_t*>(&ctr->step);
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    float m_old = 0.f, v_old = 0.f, p_old = 0.f;
+    if (i < n) {
+        m_old = m[i];
+        v_old = v[i];
+        p_old = p[i];
+    }
     // the block's 256 parameters lie in one segment of the parameter vector
     // (all segment boundaries are multiples of 256): where their partials
     // are contiguous (all but W5's transpose), one thread brings the jobs'
@@ -376,16 +386,18 @@ __global__ void k_adam_counted(float* __restrict__ p, const float* __restrict__ 
         if (bulk) {
             tc::mbar_init(b_addr, 1);
             asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-            tc::mbar_expect_tx(b_addr, nj * 1024u);
-            for (uint32_t k = 0; k < nj; ++k)
-                tc::bulk_g2s(tc::smem_addr(rows + k * 256), part + size_t(j0 + k) * MLP_DW_PART + src0, 1024u, b_addr);
         }
+    }
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    if (threadIdx.x == 0 && bulk) {
+        tc::mbar_expect_tx(b_addr, nj * 1024u);
+        for (uint32_t k = 0; k < nj; ++k)
+            tc::bulk_g2s(tc::smem_addr(rows + k * 256), part + size_t(j0 + k) * MLP_DW_PART + src0, 1024u, b_addr);
     }
     __syncthreads();
     bool landed = false;
     if (bulk)
         for (uint32_t it = 0; it < tc::SLEEP_LIMIT && !landed; ++it) landed = tc::mbar_try_sleep(b_addr, 0, 1000000u);
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) {
         float gs;
         if (part) {
@@ -402,11 +414,11 @@ __global__ void k_adam_counted(float* __restrict__ p, const float* __restrict__ 
             gs = grad[i];
         }
         const float gi = gs * a.gscale;
-        const float mi = a.b1 * m[i] + (1.f - a.b1) * gi;
-        const float vi = a.b2 * v[i] + (1.f - a.b2) * gi * gi;
+        const float mi = a.b1 * m_old + (1.f - a.b1) * gi;
+        const float vi = a.b2 * v_old + (1.f - a.b2) * gi * gi;
         m[i] = mi;
         v[i] = vi;
-        const float pi = p[i] - a.lr * (mi * a.c1) / (sqrtf(vi * a.c2) + a.eps);
+        const float pi = p_old - a.lr * (mi * a.c1) / (sqrtf(vi * a.c2) + a.eps);
         p[i] = pi;
         const __nv_bfloat16 h = __float2bfloat16_rn(pi);
         if (bf16_copy) bf16_copy[i] = h;

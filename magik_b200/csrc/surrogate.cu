@@ -96,6 +96,7 @@ struct mgk_surrogate {
         uint32_t n, B;
         LossWeights w;
         const void *table, *keys, *loss;
+        char env[96];  // the values of the switches that change which kernels an epoch launches
     } graph_key{};
 };
 
@@ -221,6 +222,19 @@ bool fused_chains() {
     const char* p = std::getenv("MGK_SURROGATE_PAIRS");
     const char* c = std::getenv("MGK_SURROGATE_CHAIN");
     return !(f && f[0] == '0') && !(p && p[0] == '1') && !(c && std::strcmp(c, "tmem") == 0);
+}
+
+// The values of the environment switches that choose the training kernels,
+// each followed by ';' (a captured epoch is replayed only under the same).
+void switch_values(char (&out)[96]) {
+    static const char* const names[] = {"MGK_SURROGATE_FUSED", "MGK_SURROGATE_PDL", "MGK_SURROGATE_PAIRS",
+                                        "MGK_SURROGATE_CHAIN"};
+    size_t k = 0;
+    for (const char* n : names) {
+        if (const char* v = std::getenv(n))
+            for (; *v && k + 2 < sizeof(out); ++v) out[k++] = *v;
+        if (k + 1 < sizeof(out)) out[k++] = ';';
+    }
 }
 
 cudaError_t gradient_tc(mgk_surrogate* s, const float* feat, const mgk_sample_label* lab, int b0, int B,
@@ -464,6 +478,7 @@ cudaError_t train_counted(mgk_surrogate* s, const mgk_train_config& cfg, const f
         key.table = s->adam_table;
         key.keys = s->keys;
         key.loss = s->epoch_loss;
+        switch_values(key.env);
         if (!s->epoch_graph || std::memcmp(&key, &s->graph_key, sizeof(key)) != 0) {
             if (s->epoch_graph) {
                 cudaGraphExecDestroy(s->epoch_graph);
