@@ -1101,6 +1101,24 @@ bool use_tmem_chain() {
     return v && std::strcmp(v, "tmem") == 0;
 }
 
+// The grid of the single-CTA chains, which take their tiles in pairs: the
+// fewest CTAs that leave the busiest one no more pairs than one CTA per SM
+// would (512 tiles on 148 SMs: 128 CTAs of two full pairs, not 148 of which
+// 80 stream the weights for an empty tile).  MGK_CHAIN_GRID=n asks for n
+// CTAs (at most one per SM and per tile).
+uint32_t chain_grid(uint32_t n_tiles, int sm_count) {
+    const uint32_t sms = uint32_t(sm_count > 0 ? sm_count : 1);
+    uint32_t grid = n_tiles < sms ? n_tiles : sms;
+    const uint32_t pairs = (n_tiles + 2 * grid - 1) / (2 * grid);  // of the busiest CTA
+    const uint32_t fewest = (n_tiles + 2 * pairs - 1) / (2 * pairs);
+    if (fewest < grid) grid = fewest;
+    if (const char* e = std::getenv("MGK_CHAIN_GRID")) {
+        const unsigned long v = std::strtoul(e, nullptr, 10);
+        if (v >= 1 && v <= sms) grid = v < n_tiles ? uint32_t(v) : n_tiles;
+    }
+    return grid;
+}
+
 template <int DIR>
 cudaError_t launch_chain(const ChainArgs& a, int sm_count, cudaStream_t st, bool pdl = false) {
     if (a.n_tiles == 0) return cudaSuccess;
@@ -1137,7 +1155,7 @@ cudaError_t launch_chain(const ChainArgs& a, int sm_count, cudaStream_t st, bool
             if (e != cudaSuccess) return e;
             attr = true;
         }
-        const uint32_t grid = a.n_tiles < uint32_t(sm_count) ? a.n_tiles : uint32_t(sm_count);
+        const uint32_t grid = chain_grid(a.n_tiles, sm_count);
         cudaLaunchConfig_t cfg = {};
         cudaLaunchAttribute at[1];
         at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
