@@ -516,7 +516,10 @@ MGK_API mgk_result mgk_surrogate_gradient(mgk_surrogate* net, const mgk_train_co
  * and loss weights; the host waits once, at the end.  Environment (read per
  * call): MGK_SURROGATE_GRAPH=0 launches every epoch, MGK_SURROGATE_PDL=0
  * launches without programmatic dependences, MGK_SURROGATE_FUSED=0 runs the
- * forward and backward chains as two kernels, MGK_SURROGATE_PAIRS=1 and
+ * forward and backward chains as two kernels, MGK_DW_CTAS=n runs the weight
+ * gradients on n CTAs (default 7/8 of the SMs; read when the training buffers
+ * are first sized), MGK_CHAIN_GRID=n the layer chains on n CTAs,
+ * MGK_SURROGATE_PAIRS=1 and
  * MGK_SURROGATE_CHAIN=tmem select the CTA-pair and tensor-memory layer
  * chains (the same results; slower on B200). */
 MGK_API mgk_result mgk_surrogate_train(mgk_surrogate* net, const mgk_train_config* cfg, const float* d_features,

@@ -146,7 +146,16 @@ mgk_result ensure_train_buffers(mgk_surrogate* s, int B) {
         TRY(dalloc(s, &s->tdout, size_t(B) * MLP_OUT_PAD * 2));
         TRY(dalloc(s, &s->img_t, mlp_t_image_bytes()));
         s->img_valid = false;  // both images are built from now on
-        s->dw_jobs = mlp_dw_jobs(uint32_t(B) / 128u, s->sm_count);
+        // the weight gradients on 7/8 of the SMs (129 of 148): on B200, 128
+        // CTAs took 197.8 us per training step against 201.3 with 148, 198.6
+        // with 112 and 202.6 with 96 (fewer CTAs contending for DRAM, fewer
+        // partials for Adam); MGK_DW_CTAS=n asks for n
+        int ctas = s->sm_count * 7 / 8;
+        if (const char* e = std::getenv("MGK_DW_CTAS")) {
+            const int v = std::atoi(e);
+            if (v > 0 && v <= s->sm_count) ctas = v;
+        }
+        s->dw_jobs = mlp_dw_jobs(uint32_t(B) / 128u, ctas);
         TRY(dalloc(s, &s->dw_part, mlp_dw_partial_floats(s->dw_jobs.total()) * sizeof(float)));
     }
     s->tb = B;
