@@ -518,7 +518,8 @@ MGK_API mgk_result mgk_surrogate_gradient(mgk_surrogate* net, const mgk_train_co
  * launches without programmatic dependences, MGK_SURROGATE_FUSED=0 runs the
  * forward and backward chains as two kernels, MGK_DW_CTAS=n runs the weight
  * gradients on n CTAs (default 7/8 of the SMs; read when the training buffers
- * are first sized), MGK_CHAIN_GRID=n the layer chains on n CTAs,
+ * are first sized), MGK_DW_JOBS=h,l0,l4 sets their jobs per 256-column layer,
+ * for W1 and for W5 instead, MGK_CHAIN_GRID=n the layer chains on n CTAs,
  * MGK_SURROGATE_PAIRS=1 and
  * MGK_SURROGATE_CHAIN=tmem select the CTA-pair and tensor-memory layer
  * chains (the same results; slower on B200). */

@@ -3,6 +3,7 @@
 // kernels), inference and the routed render.
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <new>
 #include <cstring>
@@ -156,6 +157,18 @@ mgk_result ensure_train_buffers(mgk_surrogate* s, int B) {
             if (v > 0 && v <= s->sm_count) ctas = v;
         }
         s->dw_jobs = mlp_dw_jobs(uint32_t(B) / 128u, ctas);
+        // MGK_DW_JOBS=h,l0,l4: the jobs per 256-column layer, for W1 and for
+        // W5 (each at most one per tile, together at most one CTA per SM)
+        if (const char* e = std::getenv("MGK_DW_JOBS")) {
+            unsigned h = 0, l0 = 0, l4 = 0;
+            const uint32_t tiles = uint32_t(B) / 128u;
+            if (std::sscanf(e, "%u,%u,%u", &h, &l0, &l4) == 3 && h >= 1 && l0 >= 1 && l4 >= 1 && h <= tiles &&
+                l0 <= tiles && l4 <= tiles && 3 * h + l0 + l4 <= unsigned(s->sm_count)) {
+                s->dw_jobs.heavy = h;
+                s->dw_jobs.l0 = l0;
+                s->dw_jobs.l4 = l4;
+            }
+        }
         TRY(dalloc(s, &s->dw_part, mlp_dw_partial_floats(s->dw_jobs.total()) * sizeof(float)));
     }
     s->tb = B;
